@@ -1,0 +1,150 @@
+/*
+ * pictor_b200.h -- C ABI of the B200 (sm_100a) particle-in-cell step.
+ *
+ * The reference has no plugin API: src/MAIN.F90 calls argument-less Fortran
+ * subroutines under `#ifdef gpu` (MAIN.F90:20-28, 53-55, 67-69, 91-93,
+ * 113-116, 128-130, 161-163, 173-175, 189-191, 223-233, 250-252, 263-265)
+ * that work on module globals (vars.F90, src/var_gpu.F90).  Each entry point
+ * below replaces one of those subroutines; a Fortran module binds them with
+ * ISO_C_BINDING.  Plain pointers and sizes only.
+ *
+ * Layout on the host side is the reference's: fields are column-major
+ * (mx,my,mz) double arrays with 2 low and 3 high ghost layers (mx = nx+5,
+ * mz = 1 in 2D; src/comm/subdomains/subdomains.F90:42-50); particles are the
+ * SoA q,x,y,z,u,v,w (double) + flv (int32) of vars.F90:43-45 with absolute
+ * local cell coordinates, interior [3, m-2), 2D z in [1,2) and flv = 0 marking
+ * a hole.
+ *
+ * Every call returns PIC_OK (0) or a negative PIC_ERR_* code; the Fortran shim
+ * maps a nonzero code to the reference's Abort(code)
+ * (src/comm/communication.F90:96-102).  One host thread drives a handle; the
+ * library owns all device memory and its CUDA stream.
+ */
+#ifndef PICTOR_B200_H
+#define PICTOR_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIC_MAX_FLVR 15
+
+enum {
+    PIC_OK = 0,
+    PIC_ERR_INVALID = -1,   /* bad argument or configuration                   */
+    PIC_ERR_OOM = -2,       /* device allocation failed                        */
+    PIC_ERR_OVERFLOW = -3,  /* particle capacity exceeded (cf. particles_gpu.F90:21, Abort(12)) */
+    PIC_ERR_NAN = -4,       /* non-finite value met                             */
+    PIC_ERR_TIMEOUT = -5,   /* a bounded device wait gave up                   */
+    PIC_ERR_CUDA = -6,      /* CUDA runtime error                              */
+    PIC_ERR_RANGE = -7,     /* particle outside the ghost frame of the grid    */
+    PIC_ERR_NOGPU = -8      /* no CUDA device                                  */
+};
+
+enum { PIC_GEOM_CARTESIAN = 0, PIC_GEOM_CYLINDRICAL = 1 };
+enum { PIC_FDTD_YEE = 0, PIC_FDTD_LEHE = 1 };
+/* PIC_PREC_FP64: the reference layout and arithmetic (drop-in).
+   PIC_PREC_FP32: FP32 particles with cell-relative positions and FP32 fields. */
+enum { PIC_PREC_FP64 = 0, PIC_PREC_FP32 = 1 };
+
+/* Runtime form of parameters.F90 + the setup's species table.  Replaces the
+   compile-time module parameters read by the GPU kernels (src/var_gpu.F90). */
+typedef struct {
+    int32_t nx, ny, nz;          /* interior cells (parameters.F90:6-8); nz ignored in 2D  */
+    int32_t dims;                /* 2 or 3 (Makefile THREE_DIMS)                          */
+    int32_t geom;                /* PIC_GEOM_*                                             */
+    int32_t fdtd;                /* PIC_FDTD_* (Makefile FDTD=Lehe)                       */
+    int32_t precision;           /* PIC_PREC_*                                             */
+    int32_t nflvr;               /* species count (vars.F90:92)                           */
+    double c;                    /* Courant number (parameters.F90:20)                    */
+    double qi;                   /* charge unit from InitScale (initialise.F90:46)        */
+    double bext[3];              /* Bx_ext0, By_ext0, Bz_ext0 (vars.F90:25)               */
+    double qm[PIC_MAX_FLVR + 1]; /* flvrqm, index 1..nflvr (vars.F90:87)                  */
+    int32_t reorder_period;      /* prtl_reorder_period (parameters.F90:71); 0 = never    */
+    int32_t curr_filter;         /* passes of the (1/4,1/2,1/4) filter (parameters.F90:22) */
+    int64_t capacity;            /* particle slots on the device (gpu_prtl_arr_size)      */
+    /* cylindrical (geom = PIC_GEOM_CYLINDRICAL): r of the first interior x cell
+       (xborders(procxind) + rshift, cyl_common.F90:23) and whether the axis is
+       in the domain (parameters.F90:65). */
+    double rmin;
+    int32_t inc_axis;
+    int32_t reserved[7];
+} pic_config;
+
+typedef struct pic_handle pic_handle;
+
+/* Library version, for the Fortran side to check at InitAll_gpu. */
+int pic_version(void);
+
+/* Create / destroy a simulation handle.  Replaces InitAll_gpu's allocations
+   (src/init/initialise_gpu.F90:9-150). */
+int pic_create(const pic_config *cfg, pic_handle **out);
+void pic_destroy(pic_handle *h);
+
+/* Host <-> device copies (InitAll_gpu, CopyGPUDataToHostForOutput
+   src/mem/particles_gpu.F90:569-581).  Field arrays are (mx,my,mz)
+   column-major doubles; any pointer may be NULL to skip that array. */
+int pic_load_fields(pic_handle *h, const double *Ex, const double *Ey, const double *Ez,
+                    const double *Bx, const double *By, const double *Bz);
+int pic_fetch_fields(pic_handle *h, double *Ex, double *Ey, double *Ez,
+                     double *Bx, double *By, double *Bz, double *Jx, double *Jy, double *Jz);
+/* Current host -> device, as smoothen_current_gpu_OnHost does around the
+   host filter (src/maxwell/fields_gpu.F90:120-131). */
+int pic_load_current(pic_handle *h, const double *Jx, const double *Jy, const double *Jz);
+int pic_load_particles(pic_handle *h, int64_t n, const double *q, const double *x, const double *y,
+                       const double *z, const double *u, const double *v, const double *w,
+                       const int32_t *flv);
+/* Writes the used_prtl_arr_size slots (holes included); *n receives the count.
+   Host arrays must hold pic_particle_count() entries. */
+int pic_fetch_particles(pic_handle *h, int64_t *n, double *q, double *x, double *y, double *z,
+                        double *u, double *v, double *w, int32_t *flv);
+int pic_particle_count(pic_handle *h, int64_t *used);
+
+/* Generate the Weibel set-up (setup_weibel.F90:17-61; init_prtl.F90:177-221;
+   prob_dist.F90:13-70,223-254) on the device, with Philox-4x32-10 keyed by
+   seed in place of gfortran's random_number.  epc = trials per cell per call,
+   density = acceptance threshold, drift = beam |v| along x, temp = 2kT/mc^2. */
+int pic_init_weibel(pic_handle *h, double epc, double density, double drift,
+                    double temp_ion, double temp_elc, uint32_t seed);
+
+/* Phases of one time step, in MAIN.F90 order. */
+int pic_update_b_half(pic_handle *h);      /* UpdateBfieldHalfGPU + SendRecvFlds(B)  (em_update_gpu.F90:44) */
+int pic_move_deposit(pic_handle *h);       /* MoveDepositPrtlGPU (movdep_gpu.F90:14-49)                     */
+int pic_exchange_particles(pic_handle *h); /* ExchangePrtlGPU + AppendParticles (loadprtlout.F90:13-106, comm_prtl.F90:11-30) */
+int pic_update_e(pic_handle *h);           /* UpdateEfieldGPU + SendRecvFlds(E) (em_update_gpu.F90:12-42)    */
+int pic_fold_current(pic_handle *h);       /* UpdateCurrentsAllEdgesGPU / UpdateCurrentAllFaces (comm_fld.F90:15-72) */
+int pic_add_current(pic_handle *h);        /* AddCurrentGPU + EMfldExchangeGPU (em_update_gpu.F90:92-109)    */
+int pic_reset_current(pic_handle *h);      /* ResetCurrentGPU (fields_gpu.F90:61-65)                        */
+int pic_reorder(pic_handle *h);            /* ReorderPrtlGPU / ReorderPrtlArr (mem_prtl.F90:166-301)        */
+/* Current filter passes (smoothen_current, current.F90:19-163). */
+int pic_filter_current(pic_handle *h);
+
+/* nsteps full steps of MAIN.F90:42-284 (reorder every reorder_period steps,
+   counted from the handle's step counter), captured once as a CUDA graph. */
+int pic_step(pic_handle *h, int32_t nsteps);
+int pic_set_step(pic_handle *h, int64_t t);
+
+/* Diagnostics (savedata_routines.F90:265-348), FP64 accumulation on device:
+   out[0] = sum |B|^2, out[1] = sum |E|^2 over the interior (CalcFldEnergy),
+   out[2] = max |divE - rho| over interior nodes, out[3] = max |rho_+|,
+   out[4..4+nflvr-1] = kinetic energy per species (CalcPrtlEnergy). */
+int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout);
+
+/* Device error word accumulated by the kernels since the last call (bit set of
+   PIC_DEVERR_*); cleared by the call. */
+enum { PIC_DEVERR_RANGE = 1, PIC_DEVERR_OVERFLOW = 2, PIC_DEVERR_NAN = 4 };
+int pic_device_errors(pic_handle *h, int32_t *bits);
+
+/* Text for an error code. */
+const char *pic_error_string(int code);
+
+/* Stream the handle launches on (cudaStream_t as void*), for callers that
+   order their own device work after the library's. */
+void *pic_stream(pic_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

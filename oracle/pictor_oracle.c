@@ -1,0 +1,920 @@
+/*
+ * pictor_oracle.c -- CPU restatement (FP64) of PICTOR's Cartesian PIC step.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker for the CUDA path, never part of it.
+ * Parity against the reference itself is UNPINNED (the reference is Fortran,
+ * has no tests or golden vectors, and cannot be compiled here); the
+ * restatement is pinned to hand-derived known-answer vectors instead.
+ *
+ * Every routine follows the reference loop for loop and keeps its order of
+ * floating-point operations (Fortran evaluates a+b+c as (a+b)+c and a*b*c as
+ * (a*b)*c), so that with -ffp-contract=off the results are those of the
+ * reference CPU build compiled without FMA contraction.  File:line citations
+ * are relative to the reference project root.
+ */
+#include "pictor_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* 1-based (i,j,k) -> 0-based column-major offset. */
+#define ID(g, i, j, k) ((int64_t)((i) - 1) + (int64_t)(g)->mx * ((int64_t)((j) - 1) + (int64_t)(g)->my * (int64_t)((k) - 1)))
+
+static const double PI_PSN = 3.14159265358979323846264; /* vars.F90:224 */
+
+void orc_grid_init(orc_grid *g)
+{
+    g->mx = g->nx + 5;
+    g->my = g->ny + 5;
+    g->mz = (g->dims == 2) ? 1 : g->nz + 5;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Field solver: em_update.F90 (Yee) and em_update_lehe.F90 (Lehe)            */
+/* ------------------------------------------------------------------------- */
+
+/* em_update_lehe.F90:8-25 (Fortran parameters; grid_dx=dy=dz=1). */
+void orc_lehe_coefficients(const orc_grid *g, double o[12])
+{
+    const double c = g->c;
+    const double cinv = 1.0 / c;                         /* vars.F90:222 */
+    const double beta_xy = 0.125 * (1.0 * 1.0);
+    const double beta_xz = 0.125 * (1.0 * 1.0);
+    const double beta_yx = 0.125, beta_yz = 0.0, beta_zx = 0.125, beta_zy = 0.0;
+    const double s = sin((0.5 * PI_PSN) * c);
+    const double delta_x = 0.25 * (1.0 - (cinv * cinv) * (s * s));
+    const double delta_y = 0.0, delta_z = 0.0;
+    double ax, ay, az;
+    if (g->dims == 3) {
+        ax = ((1.0 - 2.0 * beta_xy) - 2.0 * beta_xz) - 3.0 * delta_x;
+        ay = ((1.0 - 2.0 * beta_yx) - 2.0 * beta_yz) - 3.0 * delta_y;
+        az = ((1.0 - 2.0 * beta_zx) - 2.0 * beta_zy) - 3.0 * delta_z;
+    } else {
+        ax = (1.0 - 2.0 * beta_xy) - 3.0 * delta_x;
+        ay = (1.0 - 2.0 * beta_yx) - 3.0 * delta_y;
+        az = 1.0;
+    }
+    o[0] = ax; o[1] = ay; o[2] = az;
+    o[3] = beta_xy; o[4] = beta_xz; o[5] = beta_yx; o[6] = beta_yz; o[7] = beta_zx; o[8] = beta_zy;
+    o[9] = delta_x; o[10] = delta_y; o[11] = delta_z;
+}
+
+/* em_update_lehe.F90:223-258 (inv_d = 1). */
+static double gradX(const orc_grid *g, const double *L, const double *F, int i, int j, int k)
+{
+    double r = L[0] * (F[ID(g, i + 1, j, k)] - F[ID(g, i, j, k)]);
+    r = r + L[3] * (F[ID(g, i + 1, j + 1, k)] - F[ID(g, i, j + 1, k)]);
+    r = r + L[3] * (F[ID(g, i + 1, j - 1, k)] - F[ID(g, i, j - 1, k)]);
+    if (g->dims == 3) {
+        r = r + L[4] * (F[ID(g, i + 1, j, k + 1)] - F[ID(g, i, j, k + 1)]);
+        r = r + L[4] * (F[ID(g, i + 1, j, k - 1)] - F[ID(g, i, j, k - 1)]);
+    }
+    r = r + L[9] * (F[ID(g, i + 2, j, k)] - F[ID(g, i - 1, j, k)]);
+    return r;
+}
+
+static double gradY(const orc_grid *g, const double *L, const double *F, int i, int j, int k)
+{
+    double r = L[1] * (F[ID(g, i, j + 1, k)] - F[ID(g, i, j, k)]);
+    r = r + L[5] * (F[ID(g, i + 1, j + 1, k)] - F[ID(g, i + 1, j, k)]);
+    r = r + L[5] * (F[ID(g, i - 1, j + 1, k)] - F[ID(g, i - 1, j, k)]);
+    if (g->dims == 3) {
+        r = r + L[6] * (F[ID(g, i, j + 1, k + 1)] - F[ID(g, i, j, k + 1)]);
+        r = r + L[6] * (F[ID(g, i, j + 1, k - 1)] - F[ID(g, i, j, k - 1)]);
+    }
+    r = r + L[10] * (F[ID(g, i, j + 2, k)] - F[ID(g, i, j - 1, k)]);
+    return r;
+}
+
+static double gradZ(const orc_grid *g, const double *L, const double *F, int i, int j, int k)
+{
+    double r = L[2] * (F[ID(g, i, j, k + 1)] - F[ID(g, i, j, k)]);
+    r = r + L[7] * (F[ID(g, i + 1, j, k + 1)] - F[ID(g, i + 1, j, k)]);
+    r = r + L[7] * (F[ID(g, i - 1, j, k + 1)] - F[ID(g, i - 1, j, k)]);
+    r = r + L[8] * (F[ID(g, i, j + 1, k + 1)] - F[ID(g, i, j + 1, k)]);
+    r = r + L[8] * (F[ID(g, i, j - 1, k + 1)] - F[ID(g, i, j - 1, k)]);
+    r = r + L[11] * (F[ID(g, i, j, k + 2)] - F[ID(g, i, j, k - 1)]);
+    return r;
+}
+
+/* em_update.F90:41-77 (Yee) / em_update_lehe.F90:191-221 (Lehe). */
+void orc_update_b_half(const orc_grid *g, orc_fields *f)
+{
+    const double h = (g->c * 0.5) * 1.0; /* fld_halfc, vars.F90:221 */
+    const double *Ex = f->Ex, *Ey = f->Ey, *Ez = f->Ez;
+    double *Bx = f->Bx, *By = f->By, *Bz = f->Bz;
+    if (g->fdtd == 0) {
+        const int k1 = g->dims == 3 ? 2 : 1, k2 = g->dims == 3 ? g->mz - 1 : 1;
+        for (int k = k1; k <= k2; k++)
+            for (int j = 2; j <= g->my - 1; j++)
+                for (int i = 2; i <= g->mx - 1; i++) {
+                    const int64_t c0 = ID(g, i, j, k);
+                    if (g->dims == 3) {
+                        Bx[c0] = (Bx[c0] - h * (Ez[ID(g, i, j + 1, k)] - Ez[c0])) + h * (Ey[ID(g, i, j, k + 1)] - Ey[c0]);
+                        By[c0] = (By[c0] - h * (Ex[ID(g, i, j, k + 1)] - Ex[c0])) + h * (Ez[ID(g, i + 1, j, k)] - Ez[c0]);
+                        Bz[c0] = (Bz[c0] - h * (Ey[ID(g, i + 1, j, k)] - Ey[c0])) + h * (Ex[ID(g, i, j + 1, k)] - Ex[c0]);
+                    } else {
+                        Bx[c0] = Bx[c0] - h * (Ez[ID(g, i, j + 1, k)] - Ez[c0]);
+                        By[c0] = By[c0] + h * (Ez[ID(g, i + 1, j, k)] - Ez[c0]);
+                        Bz[c0] = (Bz[c0] - h * (Ey[ID(g, i + 1, j, k)] - Ey[c0])) + h * (Ex[ID(g, i, j + 1, k)] - Ex[c0]);
+                    }
+                }
+    } else {
+        double L[12];
+        orc_lehe_coefficients(g, L);
+        const int k1 = g->dims == 3 ? 3 : 1, k2 = g->dims == 3 ? g->mz - 3 : 1;
+        for (int k = k1; k <= k2; k++)
+            for (int j = 3; j <= g->my - 3; j++)
+                for (int i = 3; i <= g->mx - 3; i++) {
+                    const int64_t c0 = ID(g, i, j, k);
+                    if (g->dims == 3) {
+                        Bx[c0] = (Bx[c0] - h * gradY(g, L, Ez, i, j, k)) + h * gradZ(g, L, Ey, i, j, k);
+                        By[c0] = (By[c0] - h * gradZ(g, L, Ex, i, j, k)) + h * gradX(g, L, Ez, i, j, k);
+                        Bz[c0] = (Bz[c0] - h * gradX(g, L, Ey, i, j, k)) + h * gradY(g, L, Ex, i, j, k);
+                    } else {
+                        Bx[c0] = Bx[c0] - h * gradY(g, L, Ez, i, j, k);
+                        By[c0] = By[c0] + h * gradX(g, L, Ez, i, j, k);
+                        Bz[c0] = (Bz[c0] - h * gradX(g, L, Ey, i, j, k)) + h * gradY(g, L, Ex, i, j, k);
+                    }
+                }
+    }
+}
+
+/* em_update.F90:9-39 (Yee loops 2..m-1) / em_update_lehe.F90:146-187 (3..m-3). */
+void orc_update_e(const orc_grid *g, orc_fields *f)
+{
+    const double fc = g->c * 1.0; /* fldc, vars.F90:220 */
+    double *Ex = f->Ex, *Ey = f->Ey, *Ez = f->Ez;
+    const double *Bx = f->Bx, *By = f->By, *Bz = f->Bz;
+    const int lo = g->fdtd == 0 ? 2 : 3;
+    const int k1 = g->dims == 3 ? lo : 1, k2 = g->dims == 3 ? (g->fdtd == 0 ? g->mz - 1 : g->mz - 3) : 1;
+    const int jhi = g->fdtd == 0 ? g->my - 1 : g->my - 3, ihi = g->fdtd == 0 ? g->mx - 1 : g->mx - 3;
+    for (int k = k1; k <= k2; k++)
+        for (int j = lo; j <= jhi; j++)
+            for (int i = lo; i <= ihi; i++) {
+                const int64_t c0 = ID(g, i, j, k);
+                if (g->dims == 3) {
+                    Ex[c0] = (Ex[c0] + fc * (Bz[c0] - Bz[ID(g, i, j - 1, k)])) - fc * (By[c0] - By[ID(g, i, j, k - 1)]);
+                    Ey[c0] = (Ey[c0] + fc * (Bx[c0] - Bx[ID(g, i, j, k - 1)])) - fc * (Bz[c0] - Bz[ID(g, i - 1, j, k)]);
+                    Ez[c0] = (Ez[c0] + fc * (By[c0] - By[ID(g, i - 1, j, k)])) - fc * (Bx[c0] - Bx[ID(g, i, j - 1, k)]);
+                } else {
+                    Ex[c0] = Ex[c0] + fc * (Bz[c0] - Bz[ID(g, i, j - 1, k)]);
+                    Ey[c0] = Ey[c0] - fc * (Bz[c0] - Bz[ID(g, i - 1, j, k)]);
+                    Ez[c0] = (Ez[c0] + fc * (By[c0] - By[ID(g, i - 1, j, k)])) - fc * (Bx[c0] - Bx[ID(g, i, j - 1, k)]);
+                }
+            }
+}
+
+/* em_update.F90:79-102 (identical in em_update_lehe.F90:264-287). */
+void orc_add_current(const orc_grid *g, orc_fields *f)
+{
+    const int k1 = g->dims == 3 ? 3 : 1, k2 = g->dims == 3 ? g->mz - 3 : 1;
+    for (int k = k1; k <= k2; k++)
+        for (int j = 3; j <= g->my - 3; j++)
+            for (int i = 3; i <= g->mx - 3; i++) {
+                const int64_t c0 = ID(g, i, j, k);
+                f->Ex[c0] = f->Ex[c0] - (f->Jx[c0] * 1.0) * 1.0;
+                f->Ey[c0] = f->Ey[c0] - (f->Jy[c0] * 1.0) * 1.0;
+                f->Ez[c0] = f->Ez[c0] - (f->Jz[c0] * 1.0) * 1.0;
+            }
+}
+
+void orc_reset_current(const orc_grid *g, orc_fields *f)
+{
+    const size_t n = (size_t)g->mx * g->my * g->mz;
+    memset(f->Jx, 0, n * sizeof(double));
+    memset(f->Jy, 0, n * sizeof(double));
+    memset(f->Jz, 0, n * sizeof(double));
+}
+
+/* ------------------------------------------------------------------------- */
+/* Periodic single-rank halo copy and current fold (comm_fld.F90)            */
+/* ------------------------------------------------------------------------- */
+
+/* Copy along one axis: high ghosts m-2..m <- 3..5, low ghosts 1..2 <- m-4..m-3
+   (layer map of subdomains.F90:592-612 with the neighbour being this rank).
+   lo/hi give the index ranges of the two other axes. */
+static void halo_axis(const orc_grid *g, double *F, int axis, const int lo[3], const int hi[3])
+{
+    const int m = axis == 0 ? g->mx : axis == 1 ? g->my : g->mz;
+    for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+            for (int i = lo[0]; i <= hi[0]; i++) {
+                int idx[3] = {i, j, k};
+                if (idx[axis] != 1) continue; /* iterate the layer axis below */
+                for (int l = 0; l < 3; l++) {
+                    int d[3] = {i, j, k}, s[3] = {i, j, k};
+                    d[axis] = m - 2 + l; s[axis] = 3 + l;
+                    F[ID(g, d[0], d[1], d[2])] = F[ID(g, s[0], s[1], s[2])];
+                }
+                for (int l = 0; l < 2; l++) {
+                    int d[3] = {i, j, k}, s[3] = {i, j, k};
+                    d[axis] = 1 + l; s[axis] = m - 4 + l;
+                    F[ID(g, d[0], d[1], d[2])] = F[ID(g, s[0], s[1], s[2])];
+                }
+            }
+}
+
+/* comm_fld.F90:75-130: y faces (x range 3..mx-3), then z faces (3D), then x
+   faces over the full y,z range. */
+void orc_send_recv_flds(const orc_grid *g, double *Fx, double *Fy, double *Fz)
+{
+    double *F[3] = {Fx, Fy, Fz};
+    for (int c = 0; c < 3; c++) {
+        int lo[3] = {3, 1, 1}, hi[3] = {g->mx - 3, 1, g->mz};
+        halo_axis(g, F[c], 1, lo, hi);
+        if (g->dims == 3) {
+            int lo2[3] = {3, 1, 1}, hi2[3] = {g->mx - 3, g->my, 1};
+            halo_axis(g, F[c], 2, lo2, hi2);
+        }
+        int lo3[3] = {1, 1, 1}, hi3[3] = {1, g->my, g->mz};
+        halo_axis(g, F[c], 0, lo3, hi3);
+    }
+}
+
+/* Fold along one axis: 3..5 += m-2..m and m-4..m-3 += 1..2 (AddBuffToFld,
+   comm_fld.F90:288-307, with the neighbour being this rank). */
+static void fold_axis(const orc_grid *g, double *F, int axis, const int lo[3], const int hi[3])
+{
+    const int m = axis == 0 ? g->mx : axis == 1 ? g->my : g->mz;
+    for (int k = lo[2]; k <= hi[2]; k++)
+        for (int j = lo[1]; j <= hi[1]; j++)
+            for (int i = lo[0]; i <= hi[0]; i++) {
+                double buf_hi[3], buf_lo[2];
+                for (int l = 0; l < 3; l++) {
+                    int s[3] = {i, j, k};
+                    s[axis] = m - 2 + l;
+                    buf_hi[l] = F[ID(g, s[0], s[1], s[2])];
+                }
+                for (int l = 0; l < 2; l++) {
+                    int s[3] = {i, j, k};
+                    s[axis] = 1 + l;
+                    buf_lo[l] = F[ID(g, s[0], s[1], s[2])];
+                }
+                for (int l = 0; l < 3; l++) {
+                    int d[3] = {i, j, k};
+                    d[axis] = 3 + l;
+                    F[ID(g, d[0], d[1], d[2])] = F[ID(g, d[0], d[1], d[2])] + buf_hi[l];
+                }
+                for (int l = 0; l < 2; l++) {
+                    int d[3] = {i, j, k};
+                    d[axis] = m - 4 + l;
+                    F[ID(g, d[0], d[1], d[2])] = F[ID(g, d[0], d[1], d[2])] + buf_lo[l];
+                }
+            }
+}
+
+/* comm_fld.F90:15-33: x faces (full y,z), then y faces (x 3..mx-3), then z. */
+void orc_update_current_all_faces(const orc_grid *g, double *Jx, double *Jy, double *Jz)
+{
+    double *F[3] = {Jx, Jy, Jz};
+    for (int c = 0; c < 3; c++) {
+        int lo[3] = {1, 1, 1}, hi[3] = {1, g->my, g->mz};
+        fold_axis(g, F[c], 0, lo, hi);
+    }
+    for (int c = 0; c < 3; c++) {
+        int lo[3] = {3, 1, 1}, hi[3] = {g->mx - 3, 1, g->mz};
+        fold_axis(g, F[c], 1, lo, hi);
+    }
+    if (g->dims == 3)
+        for (int c = 0; c < 3; c++) {
+            int lo[3] = {3, 1, 1}, hi[3] = {g->mx - 3, g->my, 1};
+            fold_axis(g, F[c], 2, lo, hi);
+        }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Mover + deposit: movdep.F90:12-258, movdep_routines.F90:6-311             */
+/* ------------------------------------------------------------------------- */
+
+/* GatherVecEfld / GatherVecBfld, movdep_routines.F90:6-223: node values of a
+   component at the 4 (2D) or 8 (3D) corners of cell (i,j,k), corner order
+   nn = (0,0,0),(1,0,0),(0,1,0),(1,1,0),(0,0,1),... */
+static void node_values(const orc_grid *g, const orc_fields *f, int i, int j, int k, double V[6][8])
+{
+    const int nc = g->dims == 3 ? 8 : 4;
+    for (int nn = 0; nn < nc; nn++) {
+        const int a = i + (nn & 1), b = j + ((nn >> 1) & 1), c = k + ((nn >> 2) & 1);
+        V[0][nn] = (f->Ex[ID(g, a - 1, b, c)] + f->Ex[ID(g, a, b, c)]) * 0.5;
+        V[1][nn] = (f->Ey[ID(g, a, b - 1, c)] + f->Ey[ID(g, a, b, c)]) * 0.5;
+        if (g->dims == 3) {
+            V[2][nn] = (f->Ez[ID(g, a, b, c - 1)] + f->Ez[ID(g, a, b, c)]) * 0.5;
+            V[3][nn] = (((f->Bx[ID(g, a, b - 1, c - 1)] + f->Bx[ID(g, a, b, c - 1)]) + f->Bx[ID(g, a, b - 1, c)]) + f->Bx[ID(g, a, b, c)]) * 0.25 + g->bext[0];
+            V[4][nn] = (((f->By[ID(g, a - 1, b, c - 1)] + f->By[ID(g, a - 1, b, c)]) + f->By[ID(g, a, b, c - 1)]) + f->By[ID(g, a, b, c)]) * 0.25 + g->bext[1];
+        } else {
+            V[2][nn] = f->Ez[ID(g, a, b, c)];
+            V[3][nn] = (f->Bx[ID(g, a, b - 1, c)] + f->Bx[ID(g, a, b, c)]) * 0.5 + g->bext[0];
+            V[4][nn] = (f->By[ID(g, a - 1, b, c)] + f->By[ID(g, a, b, c)]) * 0.5 + g->bext[1];
+        }
+        V[5][nn] = (((f->Bz[ID(g, a - 1, b - 1, c)] + f->Bz[ID(g, a - 1, b, c)]) + f->Bz[ID(g, a, b - 1, c)]) + f->Bz[ID(g, a, b, c)]) * 0.25 + g->bext[2];
+    }
+}
+
+typedef struct {
+    int64_t cell;  /* VecJ column (1-based short_arr_ind)                */
+    double val[12];
+} vecj_contrib;
+
+/* The 8 (2D) or 12 (3D) VecJ entries of one zigzag segment, with the
+   wtF/Jwt tables of vars.F90:328-355 expanded.  Products are left to right
+   as in movdep.F90:209,233. */
+static void segment_values(int dims, double Fx, double Fy, double Fz, double Wx, double Wy, double Wz, double out[12])
+{
+    if (dims == 2) {
+        out[0] = ((Fx * 1.0) * (1.0 - Wy)) * 1.0;
+        out[1] = ((Fx * 1.0) * Wy) * 1.0;
+        out[2] = ((Fy * (1.0 - Wx)) * 1.0) * 1.0;
+        out[3] = ((Fy * Wx) * 1.0) * 1.0;
+        out[4] = ((Fz * (1.0 - Wx)) * (1.0 - Wy)) * 1.0;
+        out[5] = ((Fz * Wx) * (1.0 - Wy)) * 1.0;
+        out[6] = ((Fz * (1.0 - Wx)) * Wy) * 1.0;
+        out[7] = ((Fz * Wx) * Wy) * 1.0;
+    } else {
+        out[0] = ((Fx * 1.0) * (1.0 - Wy)) * (1.0 - Wz);
+        out[1] = ((Fx * 1.0) * Wy) * (1.0 - Wz);
+        out[2] = ((Fx * 1.0) * (1.0 - Wy)) * Wz;
+        out[3] = ((Fx * 1.0) * Wy) * Wz;
+        out[4] = ((Fy * (1.0 - Wx)) * 1.0) * (1.0 - Wz);
+        out[5] = ((Fy * Wx) * 1.0) * (1.0 - Wz);
+        out[6] = ((Fy * (1.0 - Wx)) * 1.0) * Wz;
+        out[7] = ((Fy * Wx) * 1.0) * Wz;
+        out[8] = ((Fz * (1.0 - Wx)) * (1.0 - Wy)) * 1.0;
+        out[9] = ((Fz * Wx) * (1.0 - Wy)) * 1.0;
+        out[10] = ((Fz * (1.0 - Wx)) * Wy) * 1.0;
+        out[11] = ((Fz * Wx) * Wy) * 1.0;
+    }
+}
+
+/* Per-particle body of movdep.F90:68-249.  Appends the two deposit segments
+   to VecJ (thread slice vj). */
+static void move_one(const orc_grid *g, orc_particles *p, const orc_fields *f, int64_t n, double *vj)
+{
+    const int nc = g->dims == 3 ? 8 : 4, nj = g->dims == 3 ? 12 : 8;
+    const double c = g->c, sqc = c * c, cinv = 1.0 / c;
+    const double x0 = p->x[n], y0 = p->y[n], z0 = p->z[n];
+    const double qm = p->flv[n] == 0 ? 0.0 : g->flvrqm[p->flv[n]] * 0.5;     /* :74-80 */
+    const int ip0 = (int)x0, jp0 = (int)y0, kp0 = (int)z0;                     /* :89-91 */
+    const double dx = x0 - ip0, dy = y0 - jp0;
+    double wt[8];
+    if (g->dims == 3) {
+        const double dz = z0 - kp0;
+        for (int nn = 0; nn < 8; nn++) {
+            const double wx = (nn & 1) ? (0.0 + 1.0 * dx) : (1.0 + -1.0 * dx);
+            const double wy = (nn & 2) ? (0.0 + 1.0 * dy) : (1.0 + -1.0 * dy);
+            const double wz = (nn & 4) ? (0.0 + 1.0 * dz) : (1.0 + -1.0 * dz);
+            wt[nn] = (wx * wy) * wz;
+        }
+    } else {
+        for (int nn = 0; nn < 4; nn++) {
+            const double wx = (nn & 1) ? (0.0 + 1.0 * dx) : (1.0 + -1.0 * dx);
+            const double wy = (nn & 2) ? (0.0 + 1.0 * dy) : (1.0 + -1.0 * dy);
+            wt[nn] = wx * wy;
+        }
+    }
+    double V[6][8];
+    node_values(g, f, ip0, jp0, g->dims == 3 ? kp0 : 1, V);
+    double pE[3] = {0, 0, 0}, pB[3] = {0, 0, 0};
+    for (int nn = 0; nn < nc; nn++) {                                          /* :116-129 */
+        pE[0] = pE[0] + wt[nn] * V[0][nn];
+        pE[1] = pE[1] + wt[nn] * V[1][nn];
+        pE[2] = pE[2] + wt[nn] * V[2][nn];
+        pB[0] = pB[0] + wt[nn] * V[3][nn];
+        pB[1] = pB[1] + wt[nn] * V[4][nn];
+        pB[2] = pB[2] + wt[nn] * V[5][nn];
+    }
+    for (int d = 0; d < 3; d++) { pE[d] = pE[d] * qm; pB[d] = pB[d] * qm; } /* :134-139 */
+
+    /* Boris push, movdep.F90:143-173 */
+    double u0 = c * p->u[n] + pE[0];
+    double v0 = c * p->v[n] + pE[1];
+    double w0 = c * p->w[n] + pE[2];
+    double gg = 1.0 / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+    const double bx = gg * pB[0], by = gg * pB[1], bz = gg * pB[2];
+    const double ff = 2.0 / (((1.0 + bx * bx) + by * by) + bz * bz);
+    const double u1 = ((u0 + v0 * bz) - w0 * by) * ff;
+    const double v1 = ((v0 + w0 * bx) - u0 * bz) * ff;
+    const double w1 = ((w0 + u0 * by) - v0 * bx) * ff;
+    u0 = ((u0 + v1 * bz) - w1 * by) + pE[0];
+    v0 = ((v0 + w1 * bx) - u1 * bz) + pE[1];
+    w0 = ((w0 + u1 * by) - v1 * bx) + pE[2];
+    p->u[n] = u0 * cinv;
+    p->v[n] = v0 * cinv;
+    p->w[n] = w0 * cinv;
+    gg = sqc / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+    const double x1 = p->x[n] + (p->u[n] * gg) * 1.0;
+    const double y1 = p->y[n] + (p->v[n] * gg) * 1.0;
+    const double z1 = p->z[n] + (p->w[n] * gg) * 1.0;
+    p->x[n] = x1; p->y[n] = y1; p->z[n] = z1;
+
+    /* zigzag deposit, movdep.F90:177-237 */
+    const int ip = (int)x1, jp = (int)y1, kp = (int)z1;
+    const double xr = fmin((double)((ip0 < ip ? ip0 : ip) + 1), fmax((double)(ip0 > ip ? ip0 : ip), 0.5 * (x0 + x1)));
+    const double yr = fmin((double)((jp0 < jp ? jp0 : jp) + 1), fmax((double)(jp0 > jp ? jp0 : jp), 0.5 * (y0 + y1)));
+    const double zr = fmin((double)((kp0 < kp ? kp0 : kp) + 1), fmax((double)(kp0 > kp ? kp0 : kp), 0.5 * (z0 + z1)));
+    const double qthis = p->q[n] * g->qi;
+    double seg[12];
+    {
+        const double Fx1 = qthis * (xr - x0), Fy1 = qthis * (yr - y0), Fz1 = qthis * (zr - z0);
+        const double Wx1 = 0.5 * (x0 + xr) - ip0, Wy1 = 0.5 * (y0 + yr) - jp0;
+        const double Wz1 = g->dims == 3 ? 0.5 * (z0 + zr) - kp0 : 0.0;
+        const int64_t cell = g->dims == 3 ? ID(g, ip0, jp0, kp0) : ID(g, ip0, jp0, 1);
+        segment_values(g->dims, Fx1, Fy1, Fz1, Wx1, Wy1, Wz1, seg);
+        for (int nn = 0; nn < nj; nn++) vj[cell * nj + nn] = vj[cell * nj + nn] + seg[nn];
+    }
+    {
+        const double Fx2 = qthis * (x1 - xr), Fy2 = qthis * (y1 - yr), Fz2 = qthis * (z1 - zr);
+        const double Wx2 = 0.5 * (x1 + xr) - ip, Wy2 = 0.5 * (y1 + yr) - jp;
+        const double Wz2 = g->dims == 3 ? 0.5 * (z1 + zr) - kp : 0.0;
+        const int64_t cell = g->dims == 3 ? ID(g, ip, jp, kp) : ID(g, ip, jp, 1);
+        segment_values(g->dims, Fx2, Fy2, Fz2, Wx2, Wy2, Wz2, seg);
+        for (int nn = 0; nn < nj; nn++) vj[cell * nj + nn] = vj[cell * nj + nn] + seg[nn];
+    }
+    /* 2D periodic z, movdep.F90:241-249 (zmin=1, zmax=2, zlen=1) */
+    if (g->dims == 2) {
+        if (p->z[n] > 2.0) p->z[n] = p->z[n] - 1.0;
+        else if (p->z[n] < 1.0) p->z[n] = 1.0 + p->z[n];
+    }
+}
+
+/* ReduceCurrentMatrix scatter, movdep_routines.F90:262-308 (thread slices
+   already summed into vj). */
+static void reduce_current_matrix(const orc_grid *g, const double *vj, orc_fields *f)
+{
+    double *Jx = f->Jx, *Jy = f->Jy, *Jz = f->Jz;
+    if (g->dims == 3) {
+        for (int k = 1; k <= g->mz - 1; k++)
+            for (int j = 1; j <= g->my - 1; j++)
+                for (int i = 1; i <= g->mx - 1; i++) {
+                    const double *v = vj + ID(g, i, j, k) * 12;
+                    Jx[ID(g, i, j, k)] += v[0];
+                    Jx[ID(g, i, j + 1, k)] += v[1];
+                    Jx[ID(g, i, j, k + 1)] += v[2];
+                    Jx[ID(g, i, j + 1, k + 1)] += v[3];
+                    Jy[ID(g, i, j, k)] += v[4];
+                    Jy[ID(g, i + 1, j, k)] += v[5];
+                    Jy[ID(g, i, j, k + 1)] += v[6];
+                    Jy[ID(g, i + 1, j, k + 1)] += v[7];
+                    Jz[ID(g, i, j, k)] += v[8];
+                    Jz[ID(g, i + 1, j, k)] += v[9];
+                    Jz[ID(g, i, j + 1, k)] += v[10];
+                    Jz[ID(g, i + 1, j + 1, k)] += v[11];
+                }
+    } else {
+        for (int j = 1; j <= g->my - 1; j++)
+            for (int i = 1; i <= g->mx - 1; i++) {
+                const double *v = vj + ID(g, i, j, 1) * 8;
+                Jx[ID(g, i, j, 1)] += v[0];
+                Jx[ID(g, i, j + 1, 1)] += v[1];
+                Jy[ID(g, i, j, 1)] += v[2];
+                Jy[ID(g, i + 1, j, 1)] += v[3];
+                Jz[ID(g, i, j, 1)] += v[4];
+                Jz[ID(g, i + 1, j, 1)] += v[5];
+                Jz[ID(g, i, j + 1, 1)] += v[6];
+                Jz[ID(g, i + 1, j + 1, 1)] += v[7];
+            }
+    }
+}
+
+void orc_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f)
+{
+    const int nj = g->dims == 3 ? 12 : 8;
+    const size_t ncell = (size_t)g->mx * g->my * g->mz;
+    double *vj = (double *)calloc(ncell * nj, sizeof(double));
+    orc_reset_current(g, f); /* J is zero whenever the deposit starts (current.F90:13-17) */
+#ifdef _OPENMP
+    int nthreads = omp_get_max_threads();
+#else
+    int nthreads = 1;
+#endif
+    if (nthreads <= 1 || p->used < 4096) {
+        for (int64_t n = 0; n < p->used; n++) move_one(g, p, f, n, vj);
+    } else {
+#ifdef _OPENMP
+        /* OPEN_MP path of movdep.F90:57-66: blocks of 32 particles, one private
+           VecJ per thread, summed in thread order (movdep_routines.F90:251-255). */
+        double *priv = (double *)calloc((size_t)nthreads * ncell * nj, sizeof(double));
+        const int64_t nblocks = (p->used + 31) / 32;
+#pragma omp parallel
+        {
+            double *mine = priv + (size_t)omp_get_thread_num() * ncell * nj;
+#pragma omp for schedule(static)
+            for (int64_t b = 0; b < nblocks; b++) {
+                const int64_t e = (b + 1) * 32 < p->used ? (b + 1) * 32 : p->used;
+                for (int64_t n = b * 32; n < e; n++) move_one(g, p, f, n, mine);
+            }
+#pragma omp for schedule(static)
+            for (int64_t cidx = 0; cidx < (int64_t)ncell; cidx++)
+                for (int t = 0; t < nthreads; t++)
+                    for (int nn = 0; nn < nj; nn++) vj[cidx * nj + nn] += priv[((size_t)t * ncell + cidx) * nj + nn];
+        }
+        free(priv);
+#endif
+    }
+    reduce_current_matrix(g, vj, f);
+    free(vj);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Particle wrap: loadprtlout.F90:13-106, comm_prtl.F90:11-66                */
+/* ------------------------------------------------------------------------- */
+
+/* RemovePrtl, loadprtlout.F90:164-181 */
+static void remove_prtl(const orc_grid *g, orc_particles *p, int64_t n)
+{
+    p->q[n] = 0; p->flv[n] = 0; p->u[n] = 0; p->v[n] = 0; p->w[n] = 0;
+    p->x[n] = 3.8; p->y[n] = 3.8; p->z[n] = g->dims == 3 ? 3.8 : 1.5;
+}
+
+int orc_exchange_particles(const orc_grid *g, orc_particles *p)
+{
+    const double xmin = 3.0, xmax = (double)(g->mx - 2), ymin = 3.0, ymax = (double)(g->my - 2);
+    const double zmin = g->dims == 3 ? 3.0 : 1.0, zmax = g->dims == 3 ? (double)(g->mz - 2) : 2.0;
+    const double len[3] = {xmax - xmin, ymax - ymin, zmax - zmin};
+    const int nfaces = g->dims == 3 ? 6 : 4;
+    int64_t *lists[6];
+    int64_t cnt[6] = {0, 0, 0, 0, 0, 0};
+    double (*saved)[8] = NULL; /* q,x,y,z,u,v,w,flv of each leaver */
+    int64_t nsaved = 0;
+    for (int fc = 0; fc < 6; fc++) lists[fc] = NULL;
+    /* count pass is folded into the scan: grow arrays as needed */
+    int64_t cap_saved = 1024;
+    saved = (double (*)[8])malloc((size_t)cap_saved * sizeof(*saved));
+    for (int fc = 0; fc < nfaces; fc++) lists[fc] = (int64_t *)malloc((size_t)cap_saved * sizeof(int64_t));
+    int64_t cap_list[6] = {cap_saved, cap_saved, cap_saved, cap_saved, cap_saved, cap_saved};
+
+    for (int64_t i = 0; i < p->used; i++) {
+        if (p->flv[i] == 0) continue;
+        double x = p->x[i], y = p->y[i], z = p->z[i];
+#define SEND(fc)                                                                              \
+    do {                                                                                      \
+        if (nsaved == cap_saved) {                                                            \
+            cap_saved *= 2;                                                                   \
+            saved = (double (*)[8])realloc(saved, (size_t)cap_saved * sizeof(*saved));        \
+        }                                                                                     \
+        saved[nsaved][0] = p->q[i]; saved[nsaved][1] = p->x[i]; saved[nsaved][2] = p->y[i];   \
+        saved[nsaved][3] = p->z[i]; saved[nsaved][4] = p->u[i]; saved[nsaved][5] = p->v[i];   \
+        saved[nsaved][6] = p->w[i]; saved[nsaved][7] = (double)p->flv[i];                    \
+        if (cnt[fc] == cap_list[fc]) {                                                        \
+            cap_list[fc] *= 2;                                                                \
+            lists[fc] = (int64_t *)realloc(lists[fc], (size_t)cap_list[fc] * sizeof(int64_t)); \
+        }                                                                                     \
+        lists[fc][cnt[fc]++] = nsaved++;                                                      \
+        remove_prtl(g, p, i);                                                                 \
+        x = p->x[i]; y = p->y[i]; z = p->z[i];                                                \
+    } while (0)
+        if (x < xmin) {                                                       /* :31-41 */
+            if ((y <= (ymax + xmin) - x) && (y >= (ymin - xmin) + x)) {
+                if (g->dims == 2 || ((z <= (zmax + xmin) - x) && (z >= (zmin - xmin) + x))) SEND(0);
+            }
+        } else if (x > xmax) {                                                /* :42-53 */
+            if ((y <= (ymax - xmax) + x) && (y >= (ymin + xmax) - x)) {
+                if (g->dims == 2 || ((z <= (zmax - xmax) + x) && (z >= (zmin + xmax) - x))) SEND(1);
+            }
+        }
+        if (y < ymin) {                                                       /* :54-64 */
+            if ((y < (ymin - xmin) + x) && (y < (ymin + xmax) - x)) {
+                if (g->dims == 2 || ((z >= (zmin - ymin) + y) && (z <= (zmax + ymin) - y))) SEND(2);
+            }
+        } else if (y > ymax) {                                                /* :65-76 */
+            if ((y > (ymax + xmin) - x) && (y > (ymax - xmax) + x)) {
+                if (g->dims == 2 || ((z >= (zmin + ymax) - y) && (z <= (zmax - ymax) + y))) SEND(3);
+            }
+        }
+        if (g->dims == 3) {
+            if (z < zmin) {                                                   /* :79-86 */
+                if ((z < (zmin - xmin) + x) && (z < (zmin + xmax) - x))
+                    if ((z < (zmin - ymin) + y) && (z < (zmin + ymax) - y)) SEND(4);
+            } else if (z > zmax) {                                            /* :87-95 */
+                if ((z > (zmax + xmin) - x) && (z > (zmax - xmax) + x))
+                    if ((z > (zmax + ymin) - y) && (z > (zmax - ymax) + y)) SEND(5);
+            }
+        }
+#undef SEND
+    }
+    int64_t total = 0;
+    for (int fc = 0; fc < nfaces; fc++) total += cnt[fc];
+    int rc = 0;
+    if (p->used + total > p->capacity) {
+        rc = -1;
+    } else {
+        /* AppendParticles order: recv(1)..recv(n) hold send(2),send(1),send(4),... */
+        static const int order[6] = {1, 0, 3, 2, 5, 4};
+        for (int o = 0; o < nfaces; o++) {
+            const int fc = order[o];
+            const int axis = fc / 2;
+            for (int64_t m = 0; m < cnt[fc]; m++) {
+                const double *s = saved[lists[fc][m]];
+                double pos[3] = {s[1], s[2], s[3]};
+                /* CopyTransferPrtl subtracts the send list shift (len on high
+                   faces), InsertPrtls adds the recv list shift (len on the
+                   receiving high list): low faces end up +len, high faces -len. */
+                if (fc % 2 == 0) pos[axis] = (pos[axis] - 0.0) + len[axis];
+                else pos[axis] = (pos[axis] - len[axis]) + 0.0;
+                const int64_t d = p->used++;
+                p->q[d] = s[0]; p->x[d] = pos[0]; p->y[d] = pos[1]; p->z[d] = pos[2];
+                p->u[d] = s[4]; p->v[d] = s[5]; p->w[d] = s[6]; p->flv[d] = (int32_t)s[7];
+            }
+        }
+    }
+    for (int fc = 0; fc < nfaces; fc++) free(lists[fc]);
+    free(saved);
+    return rc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* ReorderPrtlArr, mem_prtl.F90:166-301 (serial: stable)                     */
+/* ------------------------------------------------------------------------- */
+void orc_reorder(const orc_grid *g, orc_particles *p, int64_t *perm)
+{
+    const size_t ncell = (size_t)g->mx * g->my * g->mz;
+    int64_t *pcount = (int64_t *)calloc(ncell, sizeof(int64_t));
+    int64_t np = 0;
+    for (int64_t n = 0; n < p->used; n++)                                         /* :178-190 */
+        if (p->flv[n] != 0) {
+            const int i = (int)floor(p->x[n]), j = (int)floor(p->y[n]);
+            const int k = g->dims == 3 ? (int)floor(p->z[n]) : 1;
+            pcount[ID(g, i, j, k)]++;
+            np++;
+        }
+    int64_t offset = 0;                                                           /* :199-214 */
+    for (size_t cidx = 0; cidx < ncell; cidx++) {
+        const int64_t t = pcount[cidx];
+        pcount[cidx] = offset;
+        offset += t;
+    }
+    double *tmp = (double *)malloc((size_t)(np > 0 ? np : 1) * sizeof(double));
+    int32_t *tmpi = (int32_t *)malloc((size_t)(np > 0 ? np : 1) * sizeof(int32_t));
+    int64_t *dest = (int64_t *)malloc((size_t)(p->used > 0 ? p->used : 1) * sizeof(int64_t));
+    for (int64_t n = 0; n < p->used; n++) {                                       /* :238-272 */
+        dest[n] = -1;
+        if (p->flv[n] != 0) {
+            const int i = (int)floor(p->x[n]), j = (int)floor(p->y[n]);
+            const int k = g->dims == 3 ? (int)floor(p->z[n]) : 1;
+            dest[n] = pcount[ID(g, i, j, k)]++;
+        }
+    }
+    double *arrs[7] = {p->q, p->x, p->y, p->z, p->u, p->v, p->w};
+    for (int a = 0; a < 7; a++) {
+        for (int64_t n = 0; n < p->used; n++)
+            if (dest[n] >= 0) tmp[dest[n]] = arrs[a][n];
+        memcpy(arrs[a], tmp, (size_t)np * sizeof(double));
+    }
+    for (int64_t n = 0; n < p->used; n++)
+        if (dest[n] >= 0) {
+            tmpi[dest[n]] = p->flv[n];
+            if (perm) perm[dest[n]] = n;
+        }
+    memcpy(p->flv, tmpi, (size_t)np * sizeof(int32_t));
+    for (int64_t n = np; n < p->used; n++) { p->q[n] = 0; p->flv[n] = 0; }      /* :274-277 */
+    p->used = np;
+    free(pcount); free(tmp); free(tmpi); free(dest);
+}
+
+/* ------------------------------------------------------------------------- */
+/* One time step, src/MAIN.F90:42-284                                        */
+/* ------------------------------------------------------------------------- */
+int orc_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period)
+{
+    orc_update_b_half(g, f);                                   /* :49-56 */
+    orc_send_recv_flds(g, f->Bx, f->By, f->Bz);                /* :58 */
+    orc_move_deposit(g, p, f);                                 /* :63-71 */
+    int rc = orc_exchange_particles(g, p);                     /* :86-94 + :145-150 */
+    orc_update_b_half(g, f);                                   /* :101-111 */
+    orc_send_recv_flds(g, f->Bx, f->By, f->Bz);
+    orc_update_e(g, f);
+    orc_send_recv_flds(g, f->Ex, f->Ey, f->Ez);
+    orc_update_current_all_faces(g, f->Jx, f->Jy, f->Jz);      /* :124 */
+    orc_add_current(g, f);                                     /* :170-172 */
+    orc_send_recv_flds(g, f->Ex, f->Ey, f->Ez);                /* :184 */
+    if (reorder_period > 0 && t % reorder_period == 0) orc_reorder(g, p, NULL); /* :259-265 */
+    return rc;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Diagnostics: savedata_routines.F90:265-348                                */
+/* ------------------------------------------------------------------------- */
+void orc_field_energy(const orc_grid *g, const orc_fields *f, double out[2])
+{
+    double eb = 0, ee = 0;
+    const int k1 = g->dims == 3 ? 3 : 1, k2 = g->dims == 3 ? g->mz - 3 : 1;
+    for (int k = k1; k <= k2; k++)
+        for (int j = 3; j <= g->my - 3; j++)
+            for (int i = 3; i <= g->mx - 3; i++) {
+                const int64_t c0 = ID(g, i, j, k);
+                eb = eb + ((f->Bx[c0] * f->Bx[c0] + f->By[c0] * f->By[c0]) + f->Bz[c0] * f->Bz[c0]);
+                ee = ee + ((f->Ex[c0] * f->Ex[c0] + f->Ey[c0] * f->Ey[c0]) + f->Ez[c0] * f->Ez[c0]);
+            }
+    out[0] = eb;
+    out[1] = ee;
+}
+
+void orc_particle_energy(const orc_grid *g, const orc_particles *p, double masse, double massi, double *energy)
+{
+    const double c = g->c;
+    const double mec2 = (masse * c) * c;
+    (void)massi;
+    for (int64_t n = 0; n < p->used; n++) {
+        if (p->flv[n] == 0) continue;
+        const double gm = sqrt(((1.0 + p->u[n] * p->u[n]) + p->v[n] * p->v[n]) + p->w[n] * p->w[n]);
+        const int fl = p->flv[n];
+        /* weight wtp = |q| for the loaders here (charge = weight * FlvrCharge) */
+        const double wt = fabs(p->q[n]);
+        if (p->q[n] > 0) energy[fl - 1] += (((gm - 1.0) * wt) * (p->q[n] * g->qi / g->flvrqm[fl])) * c * c;
+        if (p->q[n] < 0) energy[fl - 1] += ((gm - 1.0) * wt) * mec2;
+    }
+}
+
+static int wrap_node(int idx, int n)
+{
+    int r = (idx - 3) % n;
+    if (r < 0) r += n;
+    return 3 + r;
+}
+
+double orc_gauss_residual(const orc_grid *g, const orc_fields *f, const orc_particles *p, double *rho_max)
+{
+    const size_t ncell = (size_t)g->mx * g->my * g->mz;
+    double *rho = (double *)calloc(ncell, sizeof(double));
+    double *rho_pos = (double *)calloc(ncell, sizeof(double));
+    for (int64_t n = 0; n < p->used; n++) {
+        if (p->flv[n] == 0) continue;
+        const double q = p->q[n] * g->qi;
+        const int i = (int)floor(p->x[n]), j = (int)floor(p->y[n]);
+        const double dx = p->x[n] - i, dy = p->y[n] - j;
+        const int k = g->dims == 3 ? (int)floor(p->z[n]) : 1;
+        const double dz = g->dims == 3 ? p->z[n] - k : 0.0;
+        const int nc = g->dims == 3 ? 8 : 4;
+        for (int nn = 0; nn < nc; nn++) {
+            const double w = ((nn & 1) ? dx : 1.0 - dx) * ((nn & 2) ? dy : 1.0 - dy) * ((nn & 4) ? dz : 1.0 - dz);
+            const int a = wrap_node(i + (nn & 1), g->nx), b = wrap_node(j + ((nn >> 1) & 1), g->ny);
+            const int cc = g->dims == 3 ? wrap_node(k + ((nn >> 2) & 1), g->nz) : 1;
+            rho[ID(g, a, b, cc)] += q * w;
+            if (q > 0) rho_pos[ID(g, a, b, cc)] += q * w;
+        }
+    }
+    double res = 0, rmax = 0;
+    const int k1 = g->dims == 3 ? 3 : 1, k2 = g->dims == 3 ? g->mz - 3 : 1;
+    for (int k = k1; k <= k2; k++)
+        for (int j = 3; j <= g->my - 3; j++)
+            for (int i = 3; i <= g->mx - 3; i++) {
+                double div = (f->Ex[ID(g, i, j, k)] - f->Ex[ID(g, i - 1, j, k)]) + (f->Ey[ID(g, i, j, k)] - f->Ey[ID(g, i, j - 1, k)]);
+                if (g->dims == 3) div = div + (f->Ez[ID(g, i, j, k)] - f->Ez[ID(g, i, j, k - 1)]);
+                const double r = fabs(div - rho[ID(g, i, j, k)]);
+                if (r > res) res = r;
+                if (fabs(rho_pos[ID(g, i, j, k)]) > rmax) rmax = fabs(rho_pos[ID(g, i, j, k)]);
+            }
+    free(rho);
+    free(rho_pos);
+    if (rho_max) *rho_max = rmax;
+    return res;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Synthetic inputs: Philox-4x32-10 in place of gfortran random_number       */
+/* ------------------------------------------------------------------------- */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        const uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        const uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        c0 = hi1 ^ c1 ^ k0;
+        c1 = lo1;
+        c2 = hi0 ^ c3 ^ k1;
+        c3 = lo0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+double orc_u01(uint32_t hi, uint32_t lo)
+{
+    const uint64_t b = (((uint64_t)hi << 32) | lo) >> 11;
+    return (double)b * (1.0 / 9007199254740992.0);
+}
+
+/* prob_dist.F90:34-54 */
+void orc_maxbolt_table(int n, double *X, double *P)
+{
+    const double dX = (15.0 - 0.0) / (double)(n - 1);
+    for (int i = 1; i <= n; i++) X[i - 1] = dX * (double)(i - 1);
+    double s = 0;
+    P[0] = 0;
+    for (int i = 2; i <= n; i++) {
+        s = s + sqrt(X[i - 1]) * exp(-X[i - 1]);
+        P[i - 1] = s;
+    }
+    for (int i = 0; i < n; i++) P[i] = P[i] / s;
+}
+
+/* prob_dist.F90:85-105 (1-based result) */
+static int binary_search(int n, const double *A, double val)
+{
+    int imin = 1, imax = n, imid = (imin + imax) / 2, search = 1;
+    while (search) {
+        const int prev = imid;
+        if (A[imid - 1] >= val) imax = imid;
+        if (A[imid - 1] <= val) imin = imid;
+        imid = (imin + imax) / 2;
+        if (imin + 1 >= imax) search = 0;
+        if (imid == prev) search = 0;
+    }
+    return imin;
+}
+
+/* prob_dist.F90:72-83 */
+static double inv_pdf(const double *X, const double *P, double pdf, int idx)
+{
+    if (P[idx] == P[idx - 1]) return X[idx - 1];
+    return X[idx - 1] + (X[idx] - X[idx - 1]) * ((pdf - P[idx - 1]) / (P[idx] - P[idx - 1]));
+}
+
+/* prob_dist.F90:223-254 */
+static void add_drift_vel(double *u, double *v, double *w, double vx, double vy, double vz)
+{
+    const double drift = sqrt((vx * vx + vy * vy) + vz * vz);
+    double beta, gamma;
+    if (fabs(drift) < 1.0) {
+        beta = drift;
+        gamma = 1.0 / sqrt((1.0 - drift) * (1.0 + drift));
+    } else {
+        gamma = fabs(drift);
+        beta = sqrt((drift - 1.0) * (drift + 1.0)) / drift;
+    }
+    double d[3] = {vx, vy, vz};
+    const double mag = sqrt((d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]);
+    if (mag == 0) d[0] = d[1] = d[2] = 0;
+    else { d[0] = d[0] / mag; d[1] = d[1] / mag; d[2] = d[2] / mag; }
+    const double gm = sqrt(((1.0 + *u * *u) + *v * *v) + *w * *w);
+    const double projn = (*u * d[0] + *v * d[1]) + *w * d[2];
+    *u = (*u + ((gamma - 1.0) * projn) * d[0]) + ((gamma * beta) * gm) * d[0];
+    *v = (*v + ((gamma - 1.0) * projn) * d[1]) + ((gamma * beta) * gm) * d[1];
+    *w = (*w + ((gamma - 1.0) * projn) * d[2]) + ((gamma * beta) * gm) * d[2];
+}
+
+int64_t orc_load_weibel(const orc_weibel *wb, orc_particles *p)
+{
+    enum { NT = 10000 };
+    static double X[NT], P[NT];
+    orc_maxbolt_table(NT, X, P);
+    const uint32_t key[2] = {wb->seed, 0x50494354u};
+    const double x1 = 0, x2 = wb->nx, y1 = 0, y2 = wb->ny, z1 = 0, z2 = wb->dims == 3 ? wb->nz : 1;
+    const double zmin = wb->dims == 3 ? 3.0 : 1.0;
+    /* init_prtl.F90:190 */
+    const int64_t ntrial = (int64_t)(wb->epc * fmax(0.0, x2 - x1) * fmax(0.0, y2 - y1) * fmax(0.0, z2 - z1));
+    p->used = 0;
+    for (uint32_t call = 0; call < 2; call++) {
+        for (int64_t n = 0; n < ntrial; n++) {
+            uint32_t r[4], ctr[4] = {(uint32_t)n, call, 0, 0};
+            orc_philox4x32_10(ctr, key, r);
+            const double r1 = orc_u01(r[0], r[1]), r2 = orc_u01(r[2], r[3]);
+            ctr[2] = 1;
+            orc_philox4x32_10(ctr, key, r);
+            const double r3 = orc_u01(r[0], r[1]), racpt = orc_u01(r[2], r[3]);
+            const double xg = x1 + r1 * (x2 - x1), yg = y1 + r2 * (y2 - y1), zg = z1 + r3 * (z2 - z1);
+            if (!(racpt <= wb->density)) continue;                         /* :209 */
+            const double xl = (xg - 0.0) + 3.0, yl = (yg - 0.0) + 3.0, zl = (zg - 0.0) + zmin;
+            for (int s = 0; s < 2; s++) {                                  /* InsertPrtl_PSP */
+                const double temp = s == 0 ? wb->temp_ion : wb->temp_elc;
+                ctr[2] = 2 + s;
+                orc_philox4x32_10(ctr, key, r);
+                const double rmb = orc_u01(r[0], r[1]), riso2 = orc_u01(r[2], r[3]);
+                ctr[2] = 4 + s;
+                orc_philox4x32_10(ctr, key, r);
+                const double riso3 = orc_u01(r[0], r[1]);
+                /* GetVelGamma_MaxBolt, prob_dist.F90:13-30 */
+                const int idx = binary_search(NT, P, rmb);
+                double beta = inv_pdf(X, P, rmb, idx);
+                beta = sqrt(beta * temp);
+                if (beta >= 1.0) beta = 0.0;
+                const double gamma = 1.0 / sqrt((1.0 + beta) * (1.0 - beta));
+                /* iso3vel, prob_dist.F90:56-70 */
+                const double ct = 2.0 * riso2 - 1.0;
+                const double st = sqrt(1.0 - ct * ct);
+                const double phi = (2.0 * PI_PSN) * riso3;
+                double u = (gamma * beta) * ct;
+                double v = ((gamma * beta) * st) * cos(phi);
+                double w = ((gamma * beta) * st) * sin(phi);
+                /* setup_weibel.F90:23-24: call 0 drifts flavour 1 left and
+                   flavour 2 right, call 1 the reverse. */
+                const double sgn = ((call == 0) == (s == 0)) ? -1.0 : 1.0;
+                add_drift_vel(&u, &v, &w, sgn * wb->drift, 0.0, 0.0);
+                if (p->used >= p->capacity) return -1;
+                const int64_t d = p->used++;
+                p->x[d] = xl; p->y[d] = yl; p->z[d] = zl;
+                p->u[d] = u; p->v[d] = v; p->w[d] = w;
+                p->q[d] = (1.0 * (s == 0 ? 1.0 : -1.0)) * 1.0;             /* :161 */
+                p->flv[d] = s + 1;
+            }
+        }
+    }
+    return p->used;
+}

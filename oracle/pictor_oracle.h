@@ -1,0 +1,127 @@
+/*
+ * pictor_oracle.h -- CPU restatement (FP64, serial) of PICTOR's Cartesian
+ * particle-in-cell time step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker that the CUDA path
+ * in pictor_b200/ is compared against.  Nothing in the product links it,
+ * loads it or calls it; only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference arm of bench.py do.
+ *
+ * Parity status: the reference is Fortran (h5pfc + mpi_f08 + HDF5) and ships
+ * no tests, golden vectors or fixtures, and no Fortran compiler exists in
+ * this image, so this restatement cannot be checked against outputs of the
+ * reference itself: parity against the reference is UNPINNED.  The
+ * restatement is pinned instead to hand-derived known-answer vectors
+ * (single-particle zigzag deposits, Boris gyration, Philox-4x32-10 published
+ * vectors, Yee/Lehe stencil values) committed under tests/golden/.
+ *
+ * Layout conventions follow the reference exactly: fields are column-major
+ * (mx,my,mz) arrays with 2 low and 3 high ghost layers (mx = nx+5;
+ * src/comm/subdomains/subdomains.F90:42-50), indices are 1-based in the
+ * comments and 0-based in memory; particle positions are absolute local cell
+ * coordinates with the interior in [3, m-2) (subdomains.F90:52-67).
+ */
+#ifndef PICTOR_ORACLE_H
+#define PICTOR_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_MAX_FLVR 8
+
+typedef struct {
+    int dims;               /* 2 or 3 (Makefile THREE_DIMS / -DtwoD)            */
+    int nx, ny, nz;         /* interior cells (nz ignored in 2D)                */
+    int mx, my, mz;         /* nx+5, ny+5, nz+5 (mz=1 in 2D)                    */
+    int fdtd;               /* 0 = Yee (em_update.F90), 1 = Lehe (em_update_lehe.F90) */
+    int nflvr;              /* number of species                               */
+    double c;               /* Courant number, parameters.F90:20               */
+    double qi;              /* InitScale charge unit, initialise.F90:46         */
+    double bext[3];         /* Bx_ext0, By_ext0, Bz_ext0 (vars.F90:25)          */
+    double flvrqm[ORC_MAX_FLVR + 1]; /* q/m per flavour, index 1..nflvr         */
+} orc_grid;
+
+/* Particle SoA in the reference layout (vars.F90:43-45). */
+typedef struct {
+    double *q, *x, *y, *z, *u, *v, *w;
+    int32_t *flv;
+    int64_t used;           /* used_prtl_arr_size                              */
+    int64_t capacity;       /* prtl_arr_size                                   */
+} orc_particles;
+
+typedef struct {
+    double *Ex, *Ey, *Ez, *Bx, *By, *Bz, *Jx, *Jy, *Jz;
+} orc_fields;
+
+/* Fill mx,my,mz from nx,ny,nz,dims. */
+void orc_grid_init(orc_grid *g);
+
+/* em_update.F90 / em_update_lehe.F90 */
+void orc_update_b_half(const orc_grid *g, orc_fields *f);
+void orc_update_e(const orc_grid *g, orc_fields *f);
+void orc_add_current(const orc_grid *g, orc_fields *f);
+/* Lehe coefficients (em_update_lehe.F90:8-25): out[0..8] =
+   alpha_x, alpha_y, alpha_z, beta_xy, beta_xz, beta_yx, beta_yz, beta_zx, beta_zy,
+   out[9..11] = delta_x, delta_y, delta_z. */
+void orc_lehe_coefficients(const orc_grid *g, double out[12]);
+
+/* comm_fld.F90 SendRecvFlds on a single periodic rank. */
+void orc_send_recv_flds(const orc_grid *g, double *Fx, double *Fy, double *Fz);
+/* comm_fld.F90 UpdateCurrentAllFaces on a single periodic rank. */
+void orc_update_current_all_faces(const orc_grid *g, double *Jx, double *Jy, double *Jz);
+/* current.F90 ResetCurrent */
+void orc_reset_current(const orc_grid *g, orc_fields *f);
+
+/* movdep.F90 MoveDepositPrtl (gather, Boris push, zigzag deposit, reduce). */
+void orc_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f);
+
+/* loadprtlout.F90 LoadPrtlOutliers + comm_prtl.F90 AppendParticles on a single
+   periodic rank.  Returns 0, or -1 when the particle capacity is exceeded. */
+int orc_exchange_particles(const orc_grid *g, orc_particles *p);
+
+/* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
+   If perm is non-NULL it receives, for each output slot, the input slot. */
+void orc_reorder(const orc_grid *g, orc_particles *p, int64_t *perm);
+
+/* One time step of src/MAIN.F90:42-284 (single rank, periodic, curr_filter=0,
+   no setup hooks).  t is the step counter used by the reorder period test. */
+int orc_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period);
+
+/* savedata_routines.F90 CalcFldEnergy (sums, not halved): out[0]=sum|B|^2,
+   out[1]=sum|E|^2 over the interior 3..m-3. */
+void orc_field_energy(const orc_grid *g, const orc_fields *f, double out[2]);
+/* savedata_routines.F90 CalcPrtlEnergy: energy[flv-1] per species. */
+void orc_particle_energy(const orc_grid *g, const orc_particles *p, double masse, double massi, double *energy);
+/* L-infinity norm over interior nodes of divE - rho, with divE as in
+   savedata_routines.F90:329-348 (backward differences) and rho the CIC
+   deposit of q*qi at nodes folded periodically.  rho_max receives max|rho| of
+   the positive species alone (a scale for the residual). */
+double orc_gauss_residual(const orc_grid *g, const orc_fields *f, const orc_particles *p, double *rho_max);
+
+/* Philox-4x32-10 (Salmon et al., SC'11). */
+void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+double orc_u01(uint32_t hi, uint32_t lo);
+
+/* Weibel loader: two InitPrtl calls as in setup_weibel.F90:23-24, positions
+   by init_prtl.F90:177-221, momenta by prob_dist.F90:13-70,223-254.
+   The gfortran random_number stream is replaced by Philox-4x32-10 keyed by
+   seed.  Returns the number of particles written, or -1 on overflow. */
+typedef struct {
+    int dims, nx, ny, nz;
+    double epc;             /* trials per unit volume per call                  */
+    double density;         /* acceptance threshold Den() (setup_weibel:46-49) */
+    double drift;           /* |v| of the beams along x (beta if <1, gamma if >1) */
+    double temp_ion, temp_elc; /* Temp = 2 kT/mc^2 per species (prob_dist:12)    */
+    uint32_t seed;
+} orc_weibel;
+int64_t orc_load_weibel(const orc_weibel *w, orc_particles *p);
+/* The Maxwell-Boltzmann inverse-CDF tables of prob_dist.F90:34-54 (N=10000). */
+void orc_maxbolt_table(int n, double *x_table, double *pdf_table);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

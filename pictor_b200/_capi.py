@@ -1,0 +1,134 @@
+"""ctypes binding of ``include/pictor_b200.h``.
+
+The library is the product: there is no CPU fallback.  Loading raises when
+``libpictor_b200.so`` is absent, and every entry point raises ``PicError`` on
+a nonzero return code.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import build as _build
+
+MAX_FLVR = 15
+
+PIC_OK = 0
+ERRORS = {
+    -1: "PIC_ERR_INVALID", -2: "PIC_ERR_OOM", -3: "PIC_ERR_OVERFLOW", -4: "PIC_ERR_NAN",
+    -5: "PIC_ERR_TIMEOUT", -6: "PIC_ERR_CUDA", -7: "PIC_ERR_RANGE", -8: "PIC_ERR_NOGPU",
+}
+GEOM = {"cartesian": 0, "cylindrical": 1}
+FDTD = {"yee": 0, "lehe": 1}
+PRECISION = {"fp64": 0, "fp32": 1}
+
+
+class PicError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where}: {ERRORS.get(code, code)} ({_lib_error_string(code)})")
+
+
+class Config(C.Structure):
+    """pic_config: the runtime form of parameters.F90 + the species table."""
+
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("dims", C.c_int32), ("geom", C.c_int32), ("fdtd", C.c_int32), ("precision", C.c_int32),
+        ("nflvr", C.c_int32),
+        ("c", C.c_double), ("qi", C.c_double), ("bext", C.c_double * 3),
+        ("qm", C.c_double * (MAX_FLVR + 1)),
+        ("reorder_period", C.c_int32), ("curr_filter", C.c_int32),
+        ("capacity", C.c_int64),
+        ("rmin", C.c_double), ("inc_axis", C.c_int32), ("reserved", C.c_int32 * 7),
+    ]
+
+
+_LIB = None
+
+
+def library_path() -> str:
+    return _build.LIB
+
+
+def lib() -> C.CDLL:
+    """Load libpictor_b200.so (built in-tree); raises if it is missing."""
+    global _LIB
+    if _LIB is None:
+        path = library_path()
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: run pictor_b200.build.build() (nvcc) first")
+        L = C.CDLL(path)
+        _declare(L)
+        _LIB = L
+    return _LIB
+
+
+def _lib_error_string(code: int) -> str:
+    try:
+        return lib().pic_error_string(code).decode()
+    except Exception:  # the library itself may be what failed to load
+        return "?"
+
+
+PD = C.POINTER(C.c_double)
+PI32 = C.POINTER(C.c_int32)
+PI64 = C.POINTER(C.c_int64)
+H = C.c_void_p
+
+# name -> (restype, argtypes); every symbol declared in include/pictor_b200.h
+SIGNATURES = {
+    "pic_version": (C.c_int, []),
+    "pic_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "pic_destroy": (None, [H]),
+    "pic_load_fields": (C.c_int, [H] + [PD] * 6),
+    "pic_fetch_fields": (C.c_int, [H] + [PD] * 9),
+    "pic_load_current": (C.c_int, [H] + [PD] * 3),
+    "pic_load_particles": (C.c_int, [H, C.c_int64] + [PD] * 7 + [PI32]),
+    "pic_fetch_particles": (C.c_int, [H, PI64] + [PD] * 7 + [PI32]),
+    "pic_particle_count": (C.c_int, [H, PI64]),
+    "pic_init_weibel": (C.c_int, [H, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_uint32]),
+    "pic_update_b_half": (C.c_int, [H]),
+    "pic_move_deposit": (C.c_int, [H]),
+    "pic_exchange_particles": (C.c_int, [H]),
+    "pic_update_e": (C.c_int, [H]),
+    "pic_fold_current": (C.c_int, [H]),
+    "pic_add_current": (C.c_int, [H]),
+    "pic_reset_current": (C.c_int, [H]),
+    "pic_reorder": (C.c_int, [H]),
+    "pic_filter_current": (C.c_int, [H]),
+    "pic_step": (C.c_int, [H, C.c_int32]),
+    "pic_set_step": (C.c_int, [H, C.c_int64]),
+    "pic_diagnostics": (C.c_int, [H, C.c_double, PD, C.c_int32]),
+    "pic_device_errors": (C.c_int, [H, PI32]),
+    "pic_error_string": (C.c_char_p, [C.c_int]),
+    "pic_stream": (C.c_void_p, [H]),
+}
+
+
+def _declare(L: C.CDLL) -> None:
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def check(code: int, where: str) -> None:
+    if code != PIC_OK:
+        raise PicError(code, where)
+
+
+def dptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and (a.flags["C_CONTIGUOUS"] or a.flags["F_CONTIGUOUS"]), "float64 contiguous array required"
+    return a.ctypes.data_as(PD)
+
+
+def iptr(a: np.ndarray | None):
+    if a is None:
+        return None
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"], "int32 contiguous array required"
+    return a.ctypes.data_as(PI32)

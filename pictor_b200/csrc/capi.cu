@@ -1,0 +1,746 @@
+// capi.cu -- the C ABI of include/pictor_b200.h: handle lifetime, host <->
+// device copies, the phase entry points that replace the reference's
+// `#ifdef gpu` subroutines, and the CUDA-graph step loop.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels.cuh"
+
+using namespace pic;
+
+struct pic_handle {
+    pic_config cfg;
+    GridP g;
+    cudaStream_t s = nullptr;
+    bool fp32 = false;
+    void *E[3] = {}, *B[3] = {}, *J[3] = {};
+    void *Jtmp = nullptr;
+    PartF64 p64[2] = {};
+    PartF32 p32[2] = {};
+    int cur = 0;
+    long long capacity = 0;
+    Counters *cnt = nullptr;
+    int *err = nullptr;
+    SortScratch sc = {};
+    double *tab_x = nullptr, *tab_p = nullptr;
+    int ntab = 10000;
+    double *diag_partials = nullptr;
+    int diag_blocks = 0;
+    double *diag_out = nullptr;
+    double *rho = nullptr, *rho_pos = nullptr;
+    long long t = 0;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+int cuda_status(cudaError_t e)
+{
+    if (e == cudaSuccess) return PIC_OK;
+    if (e == cudaErrorMemoryAllocation) return PIC_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return PIC_ERR_NOGPU;
+    return PIC_ERR_CUDA;
+}
+
+#define CK(x)                                   \
+    do {                                        \
+        cudaError_t e_ = (x);                   \
+        if (e_ != cudaSuccess) return cuda_status(e_); \
+    } while (0)
+
+template <typename T>
+int dalloc(pic_handle *h, T **p, size_t n)
+{
+    void *q = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(&q, n * sizeof(T));
+    if (e != cudaSuccess) return cuda_status(e);
+    h->allocs.push_back(q);
+    *p = (T *)q;
+    return PIC_OK;
+}
+
+// Lehe coefficients, em_update_lehe.F90:8-25 (grid_dx = dy = dz = 1).
+void lehe_coefficients(int dims, double c, double *o)
+{
+    const double pi = 3.14159265358979323846264;
+    const double cinv = 1.0 / c;
+    const double bxy = 0.125 * (1.0 * 1.0), bxz = 0.125 * (1.0 * 1.0);
+    const double byx = 0.125, byz = 0.0, bzx = 0.125, bzy = 0.0;
+    const double s = std::sin((0.5 * pi) * c);
+    const double dxl = 0.25 * (1.0 - (cinv * cinv) * (s * s));
+    const double dyl = 0.0, dzl = 0.0;
+    if (dims == 3) {
+        o[0] = ((1.0 - 2.0 * bxy) - 2.0 * bxz) - 3.0 * dxl;
+        o[1] = ((1.0 - 2.0 * byx) - 2.0 * byz) - 3.0 * dyl;
+        o[2] = ((1.0 - 2.0 * bzx) - 2.0 * bzy) - 3.0 * dzl;
+    } else {
+        o[0] = (1.0 - 2.0 * bxy) - 3.0 * dxl;
+        o[1] = (1.0 - 2.0 * byx) - 3.0 * dyl;
+        o[2] = 1.0;
+    }
+    o[3] = bxy; o[4] = bxz; o[5] = byx; o[6] = byz; o[7] = bzx; o[8] = bzy;
+    o[9] = dxl; o[10] = dyl; o[11] = dzl;
+}
+
+// Init_MaxBolt_Table, prob_dist.F90:34-54.
+void maxbolt_table(int n, std::vector<double> &X, std::vector<double> &P)
+{
+    X.assign(n, 0.0);
+    P.assign(n, 0.0);
+    const double dX = (15.0 - 0.0) / (double)(n - 1);
+    for (int i = 1; i <= n; i++) X[i - 1] = dX * (double)(i - 1);
+    double s = 0;
+    for (int i = 2; i <= n; i++) {
+        s = s + std::sqrt(X[i - 1]) * std::exp(-X[i - 1]);
+        P[i - 1] = s;
+    }
+    for (int i = 0; i < n; i++) P[i] = P[i] / s;
+}
+
+int check_device_errors(pic_handle *h)
+{
+    int bits = 0;
+    CK(cudaMemcpyAsync(&bits, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    if (bits & PIC_DEVERR_OVERFLOW) return PIC_ERR_OVERFLOW;
+    if (bits & PIC_DEVERR_RANGE) return PIC_ERR_RANGE;
+    if (bits & PIC_DEVERR_NAN) return PIC_ERR_NAN;
+    return PIC_OK;
+}
+
+// Finish a synchronous entry point: launch errors, stream errors, device error word.
+int finish(pic_handle *h)
+{
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(h->s));
+    return check_device_errors(h);
+}
+
+template <typename T>
+void field_ptrs(pic_handle *h, T *E[3], T *B[3], T *J[3])
+{
+    for (int c = 0; c < 3; c++) {
+        E[c] = (T *)h->E[c];
+        B[c] = (T *)h->B[c];
+        J[c] = (T *)h->J[c];
+    }
+}
+
+// The launches of one full step (MAIN.F90:42-284), enqueued on h->s.  Reads
+// `cur` and, when reorder is set, leaves the particles in buffer cur^1.
+void enqueue_step(pic_handle *h, int cur, bool reorder)
+{
+    const GridP &g = h->g;
+    const bool filt = h->cfg.curr_filter > 0;
+    if (!h->fp32) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_bhalf<double>(g, E, B, h->s);                                      // :49-58
+        launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);  // :63-71
+        launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s); // :86-94, :145-150
+        launch_bhalf<double>(g, E, B, h->s);                                      // :101-105
+        if (!filt) {
+            launch_efield<double>(g, 1, E, B, J, h->s);                           // :108-110, :124, :170-184
+        } else {
+            launch_fold<double>(g, J, h->s);
+            for (int k = 0; k < h->cfg.curr_filter; k++) launch_filter<double>(g, J, (double *)h->Jtmp, h->s);
+            launch_efield<double>(g, 3, E, B, J, h->s);
+            for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(double), h->s);
+        }
+        if (reorder) launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+    } else {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_bhalf<float>(g, E, B, h->s);
+        launch_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
+        launch_bhalf<float>(g, E, B, h->s);
+        if (!filt) {
+            launch_efield<float>(g, 1, E, B, J, h->s);
+        } else {
+            launch_fold<float>(g, J, h->s);
+            for (int k = 0; k < h->cfg.curr_filter; k++) launch_filter<float>(g, J, (float *)h->Jtmp, h->s);
+            launch_efield<float>(g, 3, E, B, J, h->s);
+            for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(float), h->s);
+        }
+        if (reorder) launch_reorder_f32(g, h->p32[cur], h->p32[cur ^ 1], h->cnt, h->sc, h->capacity, h->s);
+    }
+}
+
+int get_graph(pic_handle *h, int cur, bool reorder, cudaGraphExec_t *out)
+{
+    cudaGraphExec_t &ge = h->graph[reorder ? 1 : 0][cur];
+    if (!ge) {
+        cudaGraph_t graph = nullptr;
+        CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
+        enqueue_step(h, cur, reorder);
+        cudaError_t e = cudaStreamEndCapture(h->s, &graph);
+        if (e != cudaSuccess) return cuda_status(e);
+        e = cudaGraphInstantiate(&ge, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            ge = nullptr;
+            return cuda_status(e);
+        }
+    }
+    *out = ge;
+    return PIC_OK;
+}
+
+size_t field_bytes(const pic_handle *h) { return (size_t)h->g.ncell * (h->fp32 ? sizeof(float) : sizeof(double)); }
+
+int alloc_particles(pic_handle *h)
+{
+    const size_t n = (size_t)h->capacity;
+    for (int b = 0; b < 2; b++) {
+        if (!h->fp32) {
+            PartF64 &p = h->p64[b];
+            int r;
+            if ((r = dalloc(h, &p.q, n)) || (r = dalloc(h, &p.x, n)) || (r = dalloc(h, &p.y, n)) ||
+                (r = dalloc(h, &p.z, n)) || (r = dalloc(h, &p.u, n)) || (r = dalloc(h, &p.v, n)) ||
+                (r = dalloc(h, &p.w, n)) || (r = dalloc(h, &p.flv, n)))
+                return r;
+        } else {
+            PartF32 &p = h->p32[b];
+            int r;
+            if ((r = dalloc(h, &p.key, n)) || (r = dalloc(h, &p.dx, n)) || (r = dalloc(h, &p.dy, n)) ||
+                (h->g.dims == 3 && (r = dalloc(h, &p.dz, n))) || (r = dalloc(h, &p.ux, n)) ||
+                (r = dalloc(h, &p.uy, n)) || (r = dalloc(h, &p.uz, n)) || (r = dalloc(h, &p.w, n)))
+                return r;
+        }
+    }
+    return PIC_OK;
+}
+
+// Temporary FP64 particle buffers for converting FP32 state in chunks.
+constexpr long long kConvChunk = 1ll << 24;
+
+struct TmpF64 {
+    PartF64 p = {};
+    void *base = nullptr;
+    int alloc(long long n)
+    {
+        const size_t sz = (size_t)n * (7 * sizeof(double) + sizeof(int32_t));
+        cudaError_t e = cudaMalloc(&base, sz);
+        if (e != cudaSuccess) return cuda_status(e);
+        double *d = (double *)base;
+        p.q = d; p.x = d + n; p.y = d + 2 * n; p.z = d + 3 * n; p.u = d + 4 * n; p.v = d + 5 * n; p.w = d + 6 * n;
+        p.flv = (int32_t *)(d + 7 * n);
+        return PIC_OK;
+    }
+    ~TmpF64()
+    {
+        if (base) cudaFree(base);
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int pic_version(void) { return 10000; }
+
+const char *pic_error_string(int code)
+{
+    switch (code) {
+        case PIC_OK: return "ok";
+        case PIC_ERR_INVALID: return "invalid argument or configuration";
+        case PIC_ERR_OOM: return "device memory allocation failed";
+        case PIC_ERR_OVERFLOW: return "particle capacity exceeded";
+        case PIC_ERR_NAN: return "non-finite value";
+        case PIC_ERR_TIMEOUT: return "bounded device wait timed out";
+        case PIC_ERR_CUDA: return "CUDA runtime error";
+        case PIC_ERR_RANGE: return "particle outside the ghost frame of the grid";
+        case PIC_ERR_NOGPU: return "no CUDA device";
+        default: return "unknown error";
+    }
+}
+
+void pic_destroy(pic_handle *h)
+{
+    if (!h) return;
+    if (h->s) cudaStreamSynchronize(h->s);
+    for (auto &row : h->graph)
+        for (auto &ge : row)
+            if (ge) cudaGraphExecDestroy(ge);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->s) cudaStreamDestroy(h->s);
+    delete h;
+}
+
+int pic_create(const pic_config *cfg, pic_handle **out)
+{
+    if (!cfg || !out) return PIC_ERR_INVALID;
+    *out = nullptr;
+    const pic_config &c = *cfg;
+    if (c.dims != 2 && c.dims != 3) return PIC_ERR_INVALID;
+    if (c.geom != PIC_GEOM_CARTESIAN) return PIC_ERR_INVALID;
+    if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
+    if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
+    if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
+    if (c.nflvr < 1 || c.nflvr > PIC_MAX_FLVR) return PIC_ERR_INVALID;
+    if (!(c.c > 0.0 && c.c < 1.0) || c.capacity < 1 || c.capacity >= (1ll << 32) - 1) return PIC_ERR_INVALID;
+    if (c.curr_filter < 0 || c.reorder_period < 0) return PIC_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return PIC_ERR_NOGPU;
+    }
+    pic_handle *h = new pic_handle();
+    h->cfg = c;
+    h->fp32 = c.precision == PIC_PREC_FP32;
+    GridP &g = h->g;
+    std::memset(&g, 0, sizeof(g));
+    g.dims = c.dims;
+    g.nx = c.nx;
+    g.ny = c.ny;
+    g.nz = c.dims == 3 ? c.nz : 1;
+    g.mx = c.nx + 5;
+    g.my = c.ny + 5;
+    g.mz = c.dims == 3 ? c.nz + 5 : 1;
+    g.fdtd = c.fdtd;
+    g.sy = g.mx;
+    g.sz = (long long)g.mx * g.my;
+    g.ncell = g.sz * g.mz;
+    if (g.ncell >= (1ll << kFlvShift) - 1) {
+        delete h;
+        return PIC_ERR_INVALID;
+    }
+    g.c = c.c;
+    g.h = (c.c * 0.5) * 1.0;   // fld_halfc, vars.F90:221
+    g.fc = c.c * 1.0;          // fldc, vars.F90:220
+    g.sqc = c.c * c.c;         // vars.F90:223
+    g.cinv = 1.0 / c.c;        // vars.F90:222
+    g.qi = c.qi;
+    for (int d = 0; d < 3; d++) g.bext[d] = c.bext[d];
+    lehe_coefficients(c.dims, c.c, g.lehe);
+    g.qm[0] = 0.0;
+    for (int f = 1; f <= PIC_MAX_FLVR; f++) g.qm[f] = f <= c.nflvr ? c.qm[f] : 0.0;
+    // subdomains.F90:52-67
+    g.xmin = 3.0;
+    g.xmax = (double)(g.mx - 2);
+    g.ymin = 3.0;
+    g.ymax = (double)(g.my - 2);
+    g.zmin = c.dims == 3 ? 3.0 : 1.0;
+    g.zmax = c.dims == 3 ? (double)(g.mz - 2) : 2.0;
+    g.xlen = g.xmax - g.xmin;
+    g.ylen = g.ymax - g.ymin;
+    g.zlen = g.zmax - g.zmin;
+    h->capacity = c.capacity;
+
+    int r = PIC_OK;
+    if (cudaStreamCreateWithFlags(&h->s, cudaStreamNonBlocking) != cudaSuccess) r = PIC_ERR_CUDA;
+    const size_t fb = field_bytes(h);
+    for (int k = 0; k < 3 && !r; k++) {
+        if ((r = dalloc(h, (char **)&h->E[k], fb))) break;
+        if ((r = dalloc(h, (char **)&h->B[k], fb))) break;
+        if ((r = dalloc(h, (char **)&h->J[k], fb))) break;
+    }
+    if (!r && c.curr_filter > 0) r = dalloc(h, (char **)&h->Jtmp, fb);
+    if (!r) r = alloc_particles(h);
+    if (!r) r = dalloc(h, &h->cnt, 1);
+    if (!r) r = dalloc(h, &h->err, 1);
+    if (!r) {
+        SortScratch &sc = h->sc;
+        sc.ntiles = sort_tiles(h->capacity);
+        sc.scan_tmp_len = scan_tmp_len(256 * sc.ntiles);
+        if ((r = dalloc(h, &sc.key[0], (size_t)h->capacity)) || (r = dalloc(h, &sc.key[1], (size_t)h->capacity)) ||
+            (r = dalloc(h, &sc.idx[0], (size_t)h->capacity)) || (r = dalloc(h, &sc.idx[1], (size_t)h->capacity)) ||
+            (r = dalloc(h, &sc.hist, 256 * sc.ntiles)) || (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
+        }
+    }
+    if (!r) {
+        h->diag_blocks = field_energy_blocks(g);
+        if (!(r = dalloc(h, &h->diag_partials, 2 * (size_t)h->diag_blocks))) r = dalloc(h, &h->diag_out, 64);
+    }
+    if (!r) {
+        std::vector<double> X, P;
+        maxbolt_table(h->ntab, X, P);
+        if (!(r = dalloc(h, &h->tab_x, h->ntab)) && !(r = dalloc(h, &h->tab_p, h->ntab))) {
+            cudaMemcpy(h->tab_x, X.data(), X.size() * sizeof(double), cudaMemcpyHostToDevice);
+            cudaMemcpy(h->tab_p, P.data(), P.size() * sizeof(double), cudaMemcpyHostToDevice);
+        }
+    }
+    if (!r) {
+        for (int k = 0; k < 3; k++) {
+            cudaMemsetAsync(h->E[k], 0, fb, h->s);
+            cudaMemsetAsync(h->B[k], 0, fb, h->s);
+            cudaMemsetAsync(h->J[k], 0, fb, h->s);
+        }
+        cudaMemsetAsync(h->cnt, 0, sizeof(Counters), h->s);
+        cudaMemsetAsync(h->err, 0, sizeof(int), h->s);
+        r = finish(h);
+    }
+    if (r) {
+        pic_destroy(h);
+        return r;
+    }
+    *out = h;
+    return PIC_OK;
+}
+
+void *pic_stream(pic_handle *h) { return h ? (void *)h->s : nullptr; }
+
+int pic_load_fields(pic_handle *h, const double *Ex, const double *Ey, const double *Ez, const double *Bx,
+                    const double *By, const double *Bz)
+{
+    if (!h) return PIC_ERR_INVALID;
+    const double *src[6] = {Ex, Ey, Ez, Bx, By, Bz};
+    void *dst[6] = {h->E[0], h->E[1], h->E[2], h->B[0], h->B[1], h->B[2]};
+    const size_t n = (size_t)h->g.ncell;
+    std::vector<float> tmp;
+    for (int k = 0; k < 6; k++) {
+        if (!src[k]) continue;
+        if (!h->fp32) {
+            CK(cudaMemcpyAsync(dst[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice, h->s));
+            CK(cudaStreamSynchronize(h->s));
+        } else {
+            tmp.resize(n);
+            for (size_t i = 0; i < n; i++) tmp[i] = (float)src[k][i];
+            CK(cudaMemcpyAsync(dst[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->s));
+            CK(cudaStreamSynchronize(h->s));
+        }
+    }
+    return finish(h);
+}
+
+int pic_load_current(pic_handle *h, const double *Jx, const double *Jy, const double *Jz)
+{
+    if (!h) return PIC_ERR_INVALID;
+    const double *src[3] = {Jx, Jy, Jz};
+    const size_t n = (size_t)h->g.ncell;
+    std::vector<float> tmp;
+    for (int k = 0; k < 3; k++) {
+        if (!src[k]) continue;
+        if (!h->fp32) {
+            CK(cudaMemcpyAsync(h->J[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice, h->s));
+        } else {
+            tmp.resize(n);
+            for (size_t i = 0; i < n; i++) tmp[i] = (float)src[k][i];
+            CK(cudaMemcpyAsync(h->J[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->s));
+        }
+        CK(cudaStreamSynchronize(h->s));
+    }
+    return finish(h);
+}
+
+int pic_fetch_fields(pic_handle *h, double *Ex, double *Ey, double *Ez, double *Bx, double *By, double *Bz, double *Jx,
+                     double *Jy, double *Jz)
+{
+    if (!h) return PIC_ERR_INVALID;
+    double *dst[9] = {Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz};
+    void *src[9] = {h->E[0], h->E[1], h->E[2], h->B[0], h->B[1], h->B[2], h->J[0], h->J[1], h->J[2]};
+    const size_t n = (size_t)h->g.ncell;
+    std::vector<float> tmp;
+    CK(cudaStreamSynchronize(h->s));
+    for (int k = 0; k < 9; k++) {
+        if (!dst[k]) continue;
+        if (!h->fp32) {
+            CK(cudaMemcpyAsync(dst[k], src[k], n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+        } else {
+            tmp.resize(n);
+            CK(cudaMemcpyAsync(tmp.data(), src[k], n * sizeof(float), cudaMemcpyDeviceToHost, h->s));
+            CK(cudaStreamSynchronize(h->s));
+            for (size_t i = 0; i < n; i++) dst[k][i] = (double)tmp[i];
+        }
+    }
+    return finish(h);
+}
+
+int pic_particle_count(pic_handle *h, int64_t *used)
+{
+    if (!h || !used) return PIC_ERR_INVALID;
+    long long u = 0;
+    CK(cudaMemcpyAsync(&u, &h->cnt->used, sizeof(long long), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaStreamSynchronize(h->s));
+    *used = u;
+    return PIC_OK;
+}
+
+int pic_load_particles(pic_handle *h, int64_t n, const double *q, const double *x, const double *y, const double *z,
+                       const double *u, const double *v, const double *w, const int32_t *flv)
+{
+    if (!h || n < 0 || n > h->capacity || (n > 0 && (!q || !x || !y || !z || !u || !v || !w || !flv)))
+        return PIC_ERR_INVALID;
+    const double *src[7] = {q, x, y, z, u, v, w};
+    if (!h->fp32) {
+        PartF64 &p = h->p64[h->cur];
+        double *dst[7] = {p.q, p.x, p.y, p.z, p.u, p.v, p.w};
+        for (int k = 0; k < 7; k++)
+            if (n) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->s));
+        if (n) CK(cudaMemcpyAsync(p.flv, flv, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s));
+    } else {
+        TmpF64 tmp;
+        const long long chunk = n < kConvChunk ? (n > 0 ? n : 1) : kConvChunk;
+        int r = tmp.alloc(chunk);
+        if (r) return r;
+        for (long long o = 0; o < n; o += chunk) {
+            const long long m = (n - o) < chunk ? (n - o) : chunk;
+            double *dst[7] = {tmp.p.q, tmp.p.x, tmp.p.y, tmp.p.z, tmp.p.u, tmp.p.v, tmp.p.w};
+            for (int k = 0; k < 7; k++)
+                CK(cudaMemcpyAsync(dst[k], src[k] + o, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, h->s));
+            CK(cudaMemcpyAsync(tmp.p.flv, flv + o, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, h->s));
+            PartF32 d = h->p32[h->cur];
+            d.key += o; d.dx += o; d.dy += o; if (d.dz) d.dz += o;
+            d.ux += o; d.uy += o; d.uz += o; d.w += o;
+            launch_f64_to_f32(h->g, tmp.p, d, m, h->err, h->s);
+            CK(cudaStreamSynchronize(h->s));
+        }
+    }
+    Counters c0 = {};
+    c0.used = n;
+    c0.np = n;
+    CK(cudaMemcpyAsync(h->cnt, &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->s));
+    return finish(h);
+}
+
+int pic_fetch_particles(pic_handle *h, int64_t *nout, double *q, double *x, double *y, double *z, double *u, double *v,
+                        double *w, int32_t *flv)
+{
+    if (!h) return PIC_ERR_INVALID;
+    int64_t n = 0;
+    int r = pic_particle_count(h, &n);
+    if (r) return r;
+    if (nout) *nout = n;
+    double *dst[7] = {q, x, y, z, u, v, w};
+    if (!h->fp32) {
+        PartF64 &p = h->p64[h->cur];
+        const double *src[7] = {p.q, p.x, p.y, p.z, p.u, p.v, p.w};
+        for (int k = 0; k < 7; k++)
+            if (dst[k] && n) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+        if (flv && n) CK(cudaMemcpyAsync(flv, p.flv, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
+    } else {
+        TmpF64 tmp;
+        const long long chunk = n < kConvChunk ? (n > 0 ? n : 1) : kConvChunk;
+        r = tmp.alloc(chunk);
+        if (r) return r;
+        for (long long o = 0; o < n; o += chunk) {
+            const long long m = (n - o) < chunk ? (n - o) : chunk;
+            PartF32 sp = h->p32[h->cur];
+            sp.key += o; sp.dx += o; sp.dy += o; if (sp.dz) sp.dz += o;
+            sp.ux += o; sp.uy += o; sp.uz += o; sp.w += o;
+            launch_f32_to_f64(h->g, sp, tmp.p, m, h->s);
+            const double *src[7] = {tmp.p.q, tmp.p.x, tmp.p.y, tmp.p.z, tmp.p.u, tmp.p.v, tmp.p.w};
+            for (int k = 0; k < 7; k++)
+                if (dst[k]) CK(cudaMemcpyAsync(dst[k] + o, src[k], (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, h->s));
+            if (flv) CK(cudaMemcpyAsync(flv + o, tmp.p.flv, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
+            CK(cudaStreamSynchronize(h->s));
+        }
+    }
+    return finish(h);
+}
+
+int pic_init_weibel(pic_handle *h, double epc, double density, double drift, double temp_ion, double temp_elc,
+                    uint32_t seed)
+{
+    if (!h || !(epc > 0) || h->cfg.nflvr < 2) return PIC_ERR_INVALID;
+    WeibelParams w;
+    w.epc = epc;
+    w.density = density;
+    w.drift = drift;
+    w.temp[0] = temp_ion;
+    w.temp[1] = temp_elc;
+    w.seed = seed;
+    // init_prtl.F90:190: Nprtl = epc * (x2-x1)*(y2-y1)*(z2-z1), truncated
+    const double vol = (double)h->g.nx * (double)h->g.ny * (h->g.dims == 3 ? (double)h->g.nz : 1.0);
+    w.ntrial = (long long)(epc * vol);
+    if (w.ntrial <= 0 || 2 * w.ntrial >= (1ll << 32)) return PIC_ERR_INVALID;
+    const PartF64 *p64 = h->fp32 ? nullptr : &h->p64[h->cur];
+    const PartF32 *p32 = h->fp32 ? &h->p32[h->cur] : nullptr;
+    CK(cudaMemsetAsync(h->cnt, 0, sizeof(Counters), h->s));
+    int r = launch_weibel(h->g, w, h->tab_x, h->tab_p, h->ntab, p64, p32, h->cnt, h->sc, h->capacity, h->err, h->s);
+    if (r) return r;
+    return finish(h);
+}
+
+// --- phases --------------------------------------------------------------
+
+int pic_update_b_half(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_bhalf<float>(h->g, E, B, h->s);
+    } else {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_bhalf<double>(h->g, E, B, h->s);
+    }
+    return finish(h);
+}
+
+int pic_reset_current(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
+    return finish(h);
+}
+
+int pic_move_deposit(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
+    if (h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
+    } else {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_move_deposit_f64(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s);
+    }
+    return finish(h);
+}
+
+int pic_exchange_particles(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (!h->fp32) launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s);
+    return finish(h);
+}
+
+int pic_update_e(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_efield<float>(h->g, 0, E, B, J, h->s);
+    } else {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_efield<double>(h->g, 0, E, B, J, h->s);
+    }
+    return finish(h);
+}
+
+int pic_fold_current(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_fold<float>(h->g, J, h->s);
+    } else {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_fold<double>(h->g, J, h->s);
+    }
+    return finish(h);
+}
+
+int pic_filter_current(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (!h->Jtmp) {
+        int r = dalloc(h, (char **)&h->Jtmp, field_bytes(h));
+        if (r) return r;
+    }
+    for (int k = 0; k < h->cfg.curr_filter; k++) {
+        if (h->fp32) {
+            float *E[3], *B[3], *J[3];
+            field_ptrs(h, E, B, J);
+            launch_filter<float>(h->g, J, (float *)h->Jtmp, h->s);
+        } else {
+            double *E[3], *B[3], *J[3];
+            field_ptrs(h, E, B, J);
+            launch_filter<double>(h->g, J, (double *)h->Jtmp, h->s);
+        }
+    }
+    return finish(h);
+}
+
+int pic_add_current(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_efield<float>(h->g, 2, E, B, J, h->s);
+    } else {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_efield<double>(h->g, 2, E, B, J, h->s);
+    }
+    return finish(h);
+}
+
+int pic_reorder(pic_handle *h)
+{
+    if (!h) return PIC_ERR_INVALID;
+    if (h->fp32) launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->s);
+    else launch_reorder_f64(h->g, h->p64[h->cur], h->p64[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+    h->cur ^= 1;
+    return finish(h);
+}
+
+int pic_set_step(pic_handle *h, int64_t t)
+{
+    if (!h) return PIC_ERR_INVALID;
+    h->t = t;
+    return PIC_OK;
+}
+
+int pic_step(pic_handle *h, int32_t nsteps)
+{
+    if (!h || nsteps < 0) return PIC_ERR_INVALID;
+    // J must be zero when a deposit starts; inside the loop the E update
+    // consumes and clears it.
+    for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
+    for (int32_t i = 0; i < nsteps; i++) {
+        h->t += 1;
+        const bool reorder = h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0;
+        cudaGraphExec_t ge = nullptr;
+        int r = get_graph(h, h->cur, reorder, &ge);
+        if (r) return r;
+        CK(cudaGraphLaunch(ge, h->s));
+        if (reorder) h->cur ^= 1;
+    }
+    return finish(h);
+}
+
+int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout)
+{
+    if (!h || !out || nout < 4) return PIC_ERR_INVALID;
+    const GridP &g = h->g;
+    if (!h->rho) {
+        int r;
+        if ((r = dalloc(h, &h->rho, (size_t)g.ncell)) || (r = dalloc(h, &h->rho_pos, (size_t)g.ncell))) return r;
+    }
+    CK(cudaMemsetAsync(h->diag_out, 0, 64 * sizeof(double), h->s));
+    launch_field_energy(g, h->E, h->B, h->fp32, h->diag_partials, h->diag_blocks, h->diag_out, h->s);
+    if (h->fp32) {
+        const float *E[3] = {(const float *)h->E[0], (const float *)h->E[1], (const float *)h->E[2]};
+        launch_gauss_f32(g, h->p32[h->cur], h->cnt, E, h->rho, h->rho_pos, h->diag_out + 2, h->s);
+        launch_particle_energy_f32(g, h->p32[h->cur], h->cnt, masse, h->diag_out + 4, h->s);
+    } else {
+        const double *E[3] = {(const double *)h->E[0], (const double *)h->E[1], (const double *)h->E[2]};
+        launch_gauss_f64(g, h->p64[h->cur], h->cnt, E, h->rho, h->rho_pos, h->diag_out + 2, h->s);
+        launch_particle_energy_f64(g, h->p64[h->cur], h->cnt, masse, h->diag_out + 4, h->s);
+    }
+    double tmp[64];
+    CK(cudaMemcpyAsync(tmp, h->diag_out, sizeof(tmp), cudaMemcpyDeviceToHost, h->s));
+    int r = finish(h);
+    const int n = nout < 4 + h->cfg.nflvr ? nout : 4 + h->cfg.nflvr;
+    for (int i = 0; i < n; i++) out[i] = tmp[i];
+    return r;
+}
+
+int pic_device_errors(pic_handle *h, int32_t *bits)
+{
+    if (!h || !bits) return PIC_ERR_INVALID;
+    int b = 0;
+    CK(cudaMemcpyAsync(&b, h->err, sizeof(int), cudaMemcpyDeviceToHost, h->s));
+    CK(cudaMemsetAsync(h->err, 0, sizeof(int), h->s));
+    CK(cudaStreamSynchronize(h->s));
+    *bits = b;
+    return PIC_OK;
+}
+
+}  // extern "C"

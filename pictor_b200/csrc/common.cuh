@@ -1,0 +1,61 @@
+// common.cuh -- shared device-side definitions of the B200 PIC step.
+//
+// Grid layout (both precisions): column-major (mx,my,mz) with 2 low and 3 high
+// ghost layers per axis (mx = nx+5; mz = 1 in 2D), as in the reference
+// (src/comm/subdomains/subdomains.F90:42-50).  Indices in comments are 1-based
+// like the reference; memory offsets are 0-based.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pictor_b200.h"
+
+namespace pic {
+
+constexpr int kThreads = 256;         // threads per CTA for streaming kernels
+constexpr int kSMs = 148;             // B200 SM count (2 dies x 74)
+
+// Scalar parameters every kernel needs, passed by value (fits in the 4 KB
+// kernel parameter space).
+struct GridP {
+    int dims, nx, ny, nz, mx, my, mz;
+    int fdtd;
+    long long ncell;                  // mx*my*mz
+    long long sy, sz;                 // strides of j and k: mx, mx*my
+    double c, h, fc, sqc, cinv, qi;   // Courant, fld_halfc, fldc, c^2, 1/c, qi
+    double bext[3];
+    double lehe[12];                  // alpha_x..z, beta_xy,xz,yx,yz,zx,zy, delta_x..z
+    double qm[PIC_MAX_FLVR + 1];      // flvrqm (index 0 = hole -> 0)
+    // particle bounds (subdomains.F90:52-67)
+    double xmin, xmax, ymin, ymax, zmin, zmax, xlen, ylen, zlen;
+};
+
+__host__ __device__ inline long long cidx(const GridP &g, int i, int j, int k)
+{
+    return (long long)(i - 1) + g.sy * (long long)(j - 1) + g.sz * (long long)(k - 1);
+}
+
+// Periodic image of a (possibly ghost) 1-based index along an axis with m
+// entries and n = m-5 interior cells: ghosts 1,2 -> m-4,m-3 and m-2..m -> 3..5
+// (the layer map of subdomains.F90:592-612 with a single periodic rank).
+__host__ __device__ inline int wrap_index(int i, int m)
+{
+    const int n = m - 5;
+    if (i < 3) return i + n;
+    if (i > m - 3) return i - n;
+    return i;
+}
+
+// Error bits written by kernels (never __trap): see PIC_DEVERR_*.
+__device__ inline void raise_error(int *err, int bit) { atomicOr(err, bit); }
+
+// Device-side particle counters shared by the step kernels.
+struct Counters {
+    long long used;        // used_prtl_arr_size
+    long long np;          // live particles (after a reorder)
+    long long append;      // particles appended by the last exchange
+    long long scratch[5];
+};
+
+}  // namespace pic

@@ -1,0 +1,85 @@
+// kernels.cuh -- host launchers of the device kernels (one declaration per
+// kernel family; definitions in fields.cu, mover.cu, particles.cu, diag.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace pic {
+
+// Particle arrays in the reference layout (vars.F90:43-45).
+struct PartF64 {
+    double *q, *x, *y, *z, *u, *v, *w;
+    int32_t *flv;
+};
+
+// FP32 cell-relative particles: key = (flv << 28) | linear ghosted cell index;
+// offsets in [0,1) from the cell's lower corner; momenta gamma*v/c; w = q.
+// In 2D dz is not stored (the out-of-plane position never enters the 2D step).
+struct PartF32 {
+    uint32_t *key;
+    float *dx, *dy, *dz, *ux, *uy, *uz, *w;
+};
+
+constexpr int kFlvShift = 28;
+constexpr uint32_t kCellMask = (1u << kFlvShift) - 1u;
+
+// fields.cu
+template <typename T> void launch_bhalf(const GridP &g, T *const E[3], T *const B[3], cudaStream_t s);
+template <typename T> void launch_efield(const GridP &g, int mode, T *const E[3], T *const B[3], T *const J[3], cudaStream_t s);
+template <typename T> void launch_fold(const GridP &g, T *const J[3], cudaStream_t s);
+template <typename T> void launch_filter(const GridP &g, T *const J[3], T *tmp, cudaStream_t s);
+
+// mover.cu
+void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s);
+void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
+                             float *const B[3], float *const J[3], int *err, cudaStream_t s);
+
+// particles.cu
+struct SortScratch {
+    uint32_t *key[2];
+    uint32_t *idx[2];
+    uint32_t *hist;       // 256 * ntiles
+    uint32_t *scan_tmp;   // partial sums of the scan
+    size_t ntiles;
+    size_t scan_tmp_len;
+};
+size_t sort_tiles(long long capacity);
+size_t scan_tmp_len(size_t n);
+// Exchange (wrap) of the reference layout: holes + append in AppendParticles order.
+void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch &sc, long long capacity, int *err,
+                         cudaStream_t s);
+// Stable cell-key reorder (ReorderPrtlArr).  The payload is gathered into
+// `out`, after which the caller swaps `p` and `out`.
+void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Counters *cnt, SortScratch &sc,
+                        long long capacity, int *err, cudaStream_t s);
+void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, SortScratch &sc,
+                        long long capacity, cudaStream_t s);
+// Reference layout <-> FP32 cell-relative conversion.
+void launch_f64_to_f32(const GridP &g, const PartF64 &in, const PartF32 &out, long long n, int *err, cudaStream_t s);
+void launch_f32_to_f64(const GridP &g, const PartF32 &in, const PartF64 &out, long long n, cudaStream_t s);
+// Device Weibel loader.
+struct WeibelParams {
+    double epc, density, drift, temp[2];
+    uint32_t seed;
+    long long ntrial;
+};
+int launch_weibel(const GridP &g, const WeibelParams &w, const double *table_x, const double *table_p, int ntable,
+                  const PartF64 *p64, const PartF32 *p32, Counters *cnt, SortScratch &sc, long long capacity,
+                  int *err, cudaStream_t s);
+void scan_exclusive_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *tmp, uint32_t *total, cudaStream_t s);
+
+// diag.cu
+void launch_field_energy(const GridP &g, const void *const E[3], const void *const B[3], bool fp32, double *partials,
+                         int nblocks, double *out2, cudaStream_t s);
+int field_energy_blocks(const GridP &g);
+void launch_particle_energy_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double masse, double *out,
+                                cudaStream_t s);
+void launch_particle_energy_f32(const GridP &g, const PartF32 &p, const Counters *cnt, double masse, double *out,
+                                cudaStream_t s);
+void launch_gauss_f64(const GridP &g, const PartF64 &p, const Counters *cnt, const double *const E[3], double *rho,
+                      double *rho_pos, double *out2, cudaStream_t s);
+void launch_gauss_f32(const GridP &g, const PartF32 &p, const Counters *cnt, const float *const E[3], double *rho,
+                      double *rho_pos, double *out2, cudaStream_t s);
+
+}  // namespace pic

@@ -1,0 +1,327 @@
+// mover.cu -- fused gather / relativistic Boris push / zigzag current deposit.
+//
+// Reference: src/movdep/movdep.F90:12-258 (CPU loop the FP64 path restates),
+// src/movdep/movdep_routines.F90:6-223 (node-averaged fields),
+// src/movdep/movdep_gpu.F90:56-334 (the reference's own CUDA Fortran kernel),
+// weight tables vars.F90:322-356.
+//
+// FP64 path: the reference layout and arithmetic.  The node averages that the
+// reference stages in VecE*/VecB* are recomputed per particle from the field
+// arrays with the same expressions, so interpolated fields, momenta and
+// positions equal the serial CPU build bit for bit.  Currents go to J with
+// FP64 atomics (order-dependent in the last bits only).
+//
+// FP32 path: cell-relative positions (cell index + offset in [0,1)) so FP32
+// keeps full sub-cell resolution anywhere in the box; the periodic wrap is an
+// integer update of the cell index inside the kernel (no holes, no append).
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace pic {
+
+// ---------------------------------------------------------------------------
+// Shared helpers
+// ---------------------------------------------------------------------------
+
+// Node-averaged field components at the 4 (2D) / 8 (3D) corners of the cell
+// whose lower corner is at offset c0, interpolated with weights wt[]
+// (GatherVecEfld/GatherVecBfld + movdep.F90:116-129).
+template <typename T, int DIMS>
+__device__ __forceinline__ void gather(const GridP &g, const T *__restrict__ Ex, const T *__restrict__ Ey,
+                                       const T *__restrict__ Ez, const T *__restrict__ Bx, const T *__restrict__ By,
+                                       const T *__restrict__ Bz, long long c0, const T *wt, T pE[3], T pB[3])
+{
+    const long long sy = g.sy, sz = g.sz;
+    const T half = (T)0.5, quarter = (T)0.25;
+    const T b0 = (T)g.bext[0], b1 = (T)g.bext[1], b2 = (T)g.bext[2];
+    pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = (T)0;
+#pragma unroll
+    for (int nn = 0; nn < (DIMS == 3 ? 8 : 4); nn++) {
+        const long long nd = c0 + (nn & 1) + ((nn >> 1) & 1) * sy + ((nn >> 2) & 1) * sz;
+        const T vex = (__ldg(Ex + nd - 1) + __ldg(Ex + nd)) * half;
+        const T vey = (__ldg(Ey + nd - sy) + __ldg(Ey + nd)) * half;
+        T vez, vbx, vby;
+        if (DIMS == 3) {
+            vez = (__ldg(Ez + nd - sz) + __ldg(Ez + nd)) * half;
+            vbx = (((__ldg(Bx + nd - sy - sz) + __ldg(Bx + nd - sz)) + __ldg(Bx + nd - sy)) + __ldg(Bx + nd)) * quarter + b0;
+            vby = (((__ldg(By + nd - 1 - sz) + __ldg(By + nd - 1)) + __ldg(By + nd - sz)) + __ldg(By + nd)) * quarter + b1;
+        } else {
+            vez = __ldg(Ez + nd);
+            vbx = (__ldg(Bx + nd - sy) + __ldg(Bx + nd)) * half + b0;
+            vby = (__ldg(By + nd - 1) + __ldg(By + nd)) * half + b1;
+        }
+        const T vbz = (((__ldg(Bz + nd - 1 - sy) + __ldg(Bz + nd - 1)) + __ldg(Bz + nd - sy)) + __ldg(Bz + nd)) * quarter + b2;
+        pE[0] = pE[0] + wt[nn] * vex;
+        pE[1] = pE[1] + wt[nn] * vey;
+        pE[2] = pE[2] + wt[nn] * vez;
+        pB[0] = pB[0] + wt[nn] * vbx;
+        pB[1] = pB[1] + wt[nn] * vby;
+        pB[2] = pB[2] + wt[nn] * vbz;
+    }
+}
+
+// Interpolation weights (vars.F90:323-326, 339-344): corner nn uses
+// (1-d) for a 0 bit and d for a 1 bit of nn, multiplied x, y, z left to right.
+template <typename T, int DIMS>
+__device__ __forceinline__ void weights(T dx, T dy, T dz, T *wt)
+{
+#pragma unroll
+    for (int nn = 0; nn < (DIMS == 3 ? 8 : 4); nn++) {
+        const T wx = (nn & 1) ? ((T)0 + (T)1 * dx) : ((T)1 + (T)-1 * dx);
+        const T wy = (nn & 2) ? ((T)0 + (T)1 * dy) : ((T)1 + (T)-1 * dy);
+        if (DIMS == 3) {
+            const T wz = (nn & 4) ? ((T)0 + (T)1 * dz) : ((T)1 + (T)-1 * dz);
+            wt[nn] = (wx * wy) * wz;
+        } else {
+            wt[nn] = wx * wy;
+        }
+    }
+}
+
+// Relativistic Boris rotation, movdep.F90:143-167.  On entry u,v,w hold
+// gamma*v/c; pE, pB are already scaled by q/m * 0.5.  Returns the new
+// momenta (u,v,w) and g = c^2/sqrt(c^2+|c u|^2).
+template <typename T>
+__device__ __forceinline__ void boris(T c, T sqc, T cinv, const T pE[3], const T pB[3], T &u, T &v, T &w, T &gout)
+{
+    T u0 = c * u + pE[0];
+    T v0 = c * v + pE[1];
+    T w0 = c * w + pE[2];
+    const T gg = (T)1 / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+    const T bx = gg * pB[0], by = gg * pB[1], bz = gg * pB[2];
+    const T ff = (T)2 / ((((T)1 + bx * bx) + by * by) + bz * bz);
+    const T u1 = ((u0 + v0 * bz) - w0 * by) * ff;
+    const T v1 = ((v0 + w0 * bx) - u0 * bz) * ff;
+    const T w1 = ((w0 + u0 * by) - v0 * bx) * ff;
+    u0 = ((u0 + v1 * bz) - w1 * by) + pE[0];
+    v0 = ((v0 + w1 * bx) - u1 * bz) + pE[1];
+    w0 = ((w0 + u1 * by) - v1 * bx) + pE[2];
+    u = u0 * cinv;
+    v = v0 * cinv;
+    w = w0 * cinv;
+    gout = sqc / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+}
+
+// The 8 (2D) / 12 (3D) VecJ entries of one zigzag segment
+// (movdep.F90:209,233 with the tables of vars.F90:328-355 expanded).
+template <typename T, int DIMS>
+__device__ __forceinline__ void segment(T Fx, T Fy, T Fz, T Wx, T Wy, T Wz, T *o)
+{
+    if (DIMS == 2) {
+        o[0] = ((Fx * (T)1) * ((T)1 - Wy)) * (T)1;
+        o[1] = ((Fx * (T)1) * Wy) * (T)1;
+        o[2] = ((Fy * ((T)1 - Wx)) * (T)1) * (T)1;
+        o[3] = ((Fy * Wx) * (T)1) * (T)1;
+        o[4] = ((Fz * ((T)1 - Wx)) * ((T)1 - Wy)) * (T)1;
+        o[5] = ((Fz * Wx) * ((T)1 - Wy)) * (T)1;
+        o[6] = ((Fz * ((T)1 - Wx)) * Wy) * (T)1;
+        o[7] = ((Fz * Wx) * Wy) * (T)1;
+    } else {
+        o[0] = ((Fx * (T)1) * ((T)1 - Wy)) * ((T)1 - Wz);
+        o[1] = ((Fx * (T)1) * Wy) * ((T)1 - Wz);
+        o[2] = ((Fx * (T)1) * ((T)1 - Wy)) * Wz;
+        o[3] = ((Fx * (T)1) * Wy) * Wz;
+        o[4] = ((Fy * ((T)1 - Wx)) * (T)1) * ((T)1 - Wz);
+        o[5] = ((Fy * Wx) * (T)1) * ((T)1 - Wz);
+        o[6] = ((Fy * ((T)1 - Wx)) * (T)1) * Wz;
+        o[7] = ((Fy * Wx) * (T)1) * Wz;
+        o[8] = ((Fz * ((T)1 - Wx)) * ((T)1 - Wy)) * (T)1;
+        o[9] = ((Fz * Wx) * ((T)1 - Wy)) * (T)1;
+        o[10] = ((Fz * ((T)1 - Wx)) * Wy) * (T)1;
+        o[11] = ((Fz * Wx) * Wy) * (T)1;
+    }
+}
+
+// Scatter of VecJ entries onto the cell edges, movdep_routines.F90:276-303.
+template <typename T, int DIMS>
+__device__ __forceinline__ void scatter(const GridP &g, T *Jx, T *Jy, T *Jz, long long c0, const T *o)
+{
+    const long long sy = g.sy, sz = g.sz;
+    if (DIMS == 2) {
+        atomicAdd(Jx + c0, o[0]);
+        atomicAdd(Jx + c0 + sy, o[1]);
+        atomicAdd(Jy + c0, o[2]);
+        atomicAdd(Jy + c0 + 1, o[3]);
+        atomicAdd(Jz + c0, o[4]);
+        atomicAdd(Jz + c0 + 1, o[5]);
+        atomicAdd(Jz + c0 + sy, o[6]);
+        atomicAdd(Jz + c0 + 1 + sy, o[7]);
+    } else {
+        atomicAdd(Jx + c0, o[0]);
+        atomicAdd(Jx + c0 + sy, o[1]);
+        atomicAdd(Jx + c0 + sz, o[2]);
+        atomicAdd(Jx + c0 + sy + sz, o[3]);
+        atomicAdd(Jy + c0, o[4]);
+        atomicAdd(Jy + c0 + 1, o[5]);
+        atomicAdd(Jy + c0 + sz, o[6]);
+        atomicAdd(Jy + c0 + 1 + sz, o[7]);
+        atomicAdd(Jz + c0, o[8]);
+        atomicAdd(Jz + c0 + 1, o[9]);
+        atomicAdd(Jz + c0 + sy, o[10]);
+        atomicAdd(Jz + c0 + 1 + sy, o[11]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// FP64, reference layout
+// ---------------------------------------------------------------------------
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_move_f64(GridP g, PartF64 p, const Counters *__restrict__ cnt,
+                                                       const double *__restrict__ Ex, const double *__restrict__ Ey,
+                                                       const double *__restrict__ Ez, const double *__restrict__ Bx,
+                                                       const double *__restrict__ By, const double *__restrict__ Bz,
+                                                       double *Jx, double *Jy, double *Jz, int *err)
+{
+    const long long used = cnt->used;
+    const double c = g.c, sqc = g.sqc, cinv = g.cinv, qi = g.qi;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
+        const int flv = p.flv[n];
+        if (flv == 0) continue;  // hole: moves nothing, deposits zero
+        const double x0 = p.x[n], y0 = p.y[n], z0 = p.z[n];
+        if (flv < 0 || flv > PIC_MAX_FLVR || !(x0 >= 2.0 && x0 < (double)(g.mx - 1)) ||
+            !(y0 >= 2.0 && y0 < (double)(g.my - 1)) || (DIMS == 3 && !(z0 >= 2.0 && z0 < (double)(g.mz - 1)))) {
+            raise_error(err, PIC_DEVERR_RANGE);
+            continue;
+        }
+        const double qm = g.qm[flv] * 0.5;                                      // movdep.F90:78
+        const int ip0 = (int)x0, jp0 = (int)y0, kp0 = (int)z0;                  // :89-91
+        double wt[8];
+        weights<double, DIMS>(x0 - ip0, y0 - jp0, z0 - kp0, wt);
+        double pE[3], pB[3];
+        gather<double, DIMS>(g, Ex, Ey, Ez, Bx, By, Bz, cidx(g, ip0, jp0, DIMS == 3 ? kp0 : 1), wt, pE, pB);
+        for (int d = 0; d < 3; d++) {                                           // :134-139
+            pE[d] = pE[d] * qm;
+            pB[d] = pB[d] * qm;
+        }
+        double u = p.u[n], v = p.v[n], w = p.w[n], gg;
+        boris<double>(c, sqc, cinv, pE, pB, u, v, w, gg);
+        const double x1 = x0 + (u * gg) * 1.0, y1 = y0 + (v * gg) * 1.0, z1 = z0 + (w * gg) * 1.0; // :169-171
+        // zigzag deposit, movdep.F90:177-237
+        const int ip = (int)x1, jp = (int)y1, kp = (int)z1;
+        const double xr = fmin((double)(min(ip0, ip) + 1), fmax((double)max(ip0, ip), 0.5 * (x0 + x1)));
+        const double yr = fmin((double)(min(jp0, jp) + 1), fmax((double)max(jp0, jp), 0.5 * (y0 + y1)));
+        const double zr = fmin((double)(min(kp0, kp) + 1), fmax((double)max(kp0, kp), 0.5 * (z0 + z1)));
+        const double qthis = p.q[n] * qi;
+        double o[12];
+        segment<double, DIMS>(qthis * (xr - x0), qthis * (yr - y0), qthis * (zr - z0), 0.5 * (x0 + xr) - ip0,
+                              0.5 * (y0 + yr) - jp0, DIMS == 3 ? 0.5 * (z0 + zr) - kp0 : 0.0, o);
+        scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip0, jp0, DIMS == 3 ? kp0 : 1), o);
+        segment<double, DIMS>(qthis * (x1 - xr), qthis * (y1 - yr), qthis * (z1 - zr), 0.5 * (x1 + xr) - ip,
+                              0.5 * (y1 + yr) - jp, DIMS == 3 ? 0.5 * (z1 + zr) - kp : 0.0, o);
+        scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip, jp, DIMS == 3 ? kp : 1), o);
+        p.u[n] = u;
+        p.v[n] = v;
+        p.w[n] = w;
+        p.x[n] = x1;
+        p.y[n] = y1;
+        double zn = z1;
+        if (DIMS == 2) {  // movdep.F90:241-249 (zmin=1, zmax=2, zlen=1)
+            if (zn > 2.0) zn = zn - 1.0;
+            else if (zn < 1.0) zn = 1.0 + zn;
+        }
+        p.z[n] = zn;
+    }
+}
+
+void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s)
+{
+    const int grid = kSMs * 16;
+    if (g.dims == 3)
+        k_move_f64<3><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+    else
+        k_move_f64<2><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+}
+
+// ---------------------------------------------------------------------------
+// FP32, cell-relative
+// ---------------------------------------------------------------------------
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_move_f32(GridP g, PartF32 p, const Counters *__restrict__ cnt,
+                                                       const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                                       const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                                       const float *__restrict__ By, const float *__restrict__ Bz,
+                                                       float *Jx, float *Jy, float *Jz, int *err)
+{
+    const long long used = cnt->used;
+    const float c = (float)g.c, sqc = (float)g.sqc, cinv = (float)g.cinv, qi = (float)g.qi;
+    const int mx = g.mx, my = g.my, mz = g.mz;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
+        const uint32_t key = p.key[n];
+        const int flv = (int)(key >> kFlvShift);
+        if (flv == 0) continue;
+        const int cell = (int)(key & kCellMask);
+        const int i = cell % mx + 1, jk = cell / mx, j = jk % my + 1, k = jk / my + 1;
+        if (i < 3 || i > mx - 3 || j < 3 || j > my - 3 || (DIMS == 3 && (k < 3 || k > mz - 3)) || (DIMS == 2 && k != 1)) {
+            raise_error(err, PIC_DEVERR_RANGE);
+            continue;
+        }
+        const float dx = p.dx[n], dy = p.dy[n], dz = DIMS == 3 ? p.dz[n] : 0.f;
+        const float qm = (float)g.qm[flv] * 0.5f;
+        float wt[8];
+        weights<float, DIMS>(dx, dy, dz, wt);
+        float pE[3], pB[3];
+        gather<float, DIMS>(g, Ex, Ey, Ez, Bx, By, Bz, (long long)cell, wt, pE, pB);
+        for (int d = 0; d < 3; d++) {
+            pE[d] = pE[d] * qm;
+            pB[d] = pB[d] * qm;
+        }
+        float u = p.ux[n], v = p.uy[n], w = p.uz[n], gg;
+        boris<float>(c, sqc, cinv, pE, pB, u, v, w, gg);
+        // displacement in cell units; positions relative to this cell's corner
+        const float x1 = dx + u * gg, y1 = dy + v * gg, z1 = dz + w * gg;
+        const int sx = (int)floorf(x1), sy = (int)floorf(y1), sz = DIMS == 3 ? (int)floorf(z1) : 0;
+        // zigzag relay point with ip0 = 0, ip = s (movdep.F90:183-185)
+        const float xr = fminf((float)(min(0, sx) + 1), fmaxf((float)max(0, sx), 0.5f * (dx + x1)));
+        const float yr = fminf((float)(min(0, sy) + 1), fmaxf((float)max(0, sy), 0.5f * (dy + y1)));
+        const float qthis = p.w[n] * qi;
+        float o[12];
+        float Fz1, Fz2, Wz1 = 0.f, Wz2 = 0.f;
+        if (DIMS == 3) {
+            const float zr = fminf((float)(min(0, sz) + 1), fmaxf((float)max(0, sz), 0.5f * (dz + z1)));
+            Fz1 = qthis * (zr - dz);
+            Fz2 = qthis * (z1 - zr);
+            Wz1 = 0.5f * (dz + zr);
+            Wz2 = 0.5f * (z1 + zr) - (float)sz;
+        } else {
+            // out-of-plane motion: no cell crossing, the relay point is the midpoint
+            Fz1 = qthis * (0.5f * (w * gg));
+            Fz2 = Fz1;
+        }
+        segment<float, DIMS>(qthis * (xr - dx), qthis * (yr - dy), Fz1, 0.5f * (dx + xr), 0.5f * (dy + yr), Wz1, o);
+        scatter<float, DIMS>(g, Jx, Jy, Jz, (long long)cell, o);
+        const long long c1 = (long long)cell + sx + (long long)sy * g.sy + (long long)sz * g.sz;
+        segment<float, DIMS>(qthis * (x1 - xr), qthis * (y1 - yr), Fz2, 0.5f * (x1 + xr) - (float)sx,
+                             0.5f * (y1 + yr) - (float)sy, Wz2, o);
+        scatter<float, DIMS>(g, Jx, Jy, Jz, c1, o);
+        // new offsets and periodic cell index
+        float nx = x1 - (float)sx, ny = y1 - (float)sy, nz = z1 - (float)sz;
+        int ni = i + sx, nj = j + sy, nk = k + sz;
+        if (nx >= 1.f) { nx -= 1.f; ni += 1; }
+        if (ny >= 1.f) { ny -= 1.f; nj += 1; }
+        if (DIMS == 3 && nz >= 1.f) { nz -= 1.f; nk += 1; }
+        ni = wrap_index(ni, mx);
+        nj = wrap_index(nj, my);
+        if (DIMS == 3) nk = wrap_index(nk, mz);
+        const uint32_t ncell = (uint32_t)((ni - 1) + mx * ((nj - 1) + my * (nk - 1)));
+        p.key[n] = ((uint32_t)flv << kFlvShift) | ncell;
+        p.dx[n] = nx;
+        p.dy[n] = ny;
+        if (DIMS == 3) p.dz[n] = nz;
+        p.ux[n] = u;
+        p.uy[n] = v;
+        p.uz[n] = w;
+    }
+}
+
+void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
+                             float *const B[3], float *const J[3], int *err, cudaStream_t s)
+{
+    const int grid = kSMs * 16;
+    if (g.dims == 3)
+        k_move_f32<3><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+    else
+        k_move_f32<2><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+}
+
+}  // namespace pic

@@ -1,0 +1,257 @@
+"""Host-side mirror of the reference's GPU entry points for the PIC step.
+
+The reference's drop-in boundary is the set of argument-less subroutines that
+``src/MAIN.F90`` calls under ``#ifdef gpu``; they act on module globals.
+``Simulation`` owns one ``pic_handle`` (the device state those globals
+describe) and exposes each of those subroutines under its reference name,
+with a snake_case alias.  Arrays cross the boundary in the reference's layout:
+fields are Fortran-ordered ``(mx, my, mz)`` float64 arrays with 2 low and 3
+high ghost layers, particles are the SoA ``q,x,y,z,u,v,w`` (float64) and
+``flv`` (int32) with absolute local cell coordinates.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _capi
+from ._capi import check, dptr, iptr
+
+
+def init_scale(c: float, c_ompe: float, epc: float, g0: float = 1.0, mi_me: float = 1.0) -> dict:
+    """InitScale (src/init/initialise.F90:44-53) plus the default species
+    table of AllocatePrtlVars (initialise.F90:84-87): flavour 1 = ions
+    (q/m = 1/mi), flavour 2 = electrons (q/m = -1)."""
+    me, mi = 1.0, mi_me
+    ompe = c / c_ompe
+    qi = (g0 * (ompe * ompe)) / ((float(epc) / 1.0) * (1.0 + me / mi))
+    qe = -qi
+    return {"ompe": ompe, "qi": qi, "qe": qe, "qmi": 1.0 / mi, "qme": -1.0,
+            "masse": abs(qe) * me, "massi": qi * mi}
+
+
+@dataclass
+class PicConfig:
+    """Runtime form of parameters.F90 (grid, Courant number, species, periods)."""
+
+    nx: int
+    ny: int
+    nz: int = 1
+    dims: int = 2
+    c: float = 0.45
+    qi: float = 1.0
+    qm: tuple = (1.0, -1.0)
+    fdtd: str = "yee"
+    precision: str = "fp64"
+    geom: str = "cartesian"
+    bext: tuple = (0.0, 0.0, 0.0)
+    reorder_period: int = 20
+    curr_filter: int = 0
+    capacity: int = 1 << 20
+    rmin: float = 0.0
+    inc_axis: int = 1
+
+    def to_struct(self) -> _capi.Config:
+        s = _capi.Config()
+        s.nx, s.ny, s.nz = self.nx, self.ny, (self.nz if self.dims == 3 else 1)
+        s.dims = self.dims
+        s.geom = _capi.GEOM[self.geom]
+        s.fdtd = _capi.FDTD[self.fdtd]
+        s.precision = _capi.PRECISION[self.precision]
+        s.nflvr = len(self.qm)
+        s.c, s.qi = self.c, self.qi
+        for d in range(3):
+            s.bext[d] = self.bext[d]
+        for i, v in enumerate(self.qm):
+            s.qm[i + 1] = v
+        s.reorder_period = self.reorder_period
+        s.curr_filter = self.curr_filter
+        s.capacity = int(self.capacity)
+        s.rmin = self.rmin
+        s.inc_axis = self.inc_axis
+        return s
+
+    @property
+    def shape(self):
+        return (self.nx + 5, self.ny + 5, (self.nz + 5) if self.dims == 3 else 1)
+
+
+@dataclass
+class Particles:
+    """Reference-layout particle arrays (vars.F90:43-45)."""
+
+    q: np.ndarray
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    flv: np.ndarray
+
+    NAMES = ("q", "x", "y", "z", "u", "v", "w", "flv")
+
+    @classmethod
+    def empty(cls, n: int) -> "Particles":
+        return cls(*(np.zeros(n) for _ in range(7)), np.zeros(n, dtype=np.int32))
+
+    def __len__(self):
+        return len(self.x)
+
+
+@dataclass
+class Fields:
+    """Fortran-ordered (mx,my,mz) float64 field arrays."""
+
+    Ex: np.ndarray
+    Ey: np.ndarray
+    Ez: np.ndarray
+    Bx: np.ndarray
+    By: np.ndarray
+    Bz: np.ndarray
+    Jx: np.ndarray = field(default=None)
+    Jy: np.ndarray = field(default=None)
+    Jz: np.ndarray = field(default=None)
+
+    @classmethod
+    def zeros(cls, shape) -> "Fields":
+        return cls(*(np.zeros(shape, order="F") for _ in range(9)))
+
+
+class Simulation:
+    """One single-rank periodic PIC run on the GPU (one pic_handle)."""
+
+    def __init__(self, cfg: PicConfig):
+        self.cfg = cfg
+        self.L = _capi.lib()
+        h = C.c_void_p()
+        check(self.L.pic_create(C.byref(cfg.to_struct()), C.byref(h)), "pic_create")
+        self.h = h
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pic_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- host <-> device (InitAll_gpu, CopyGPUDataToHostForOutput) ----------
+    def load_fields(self, f: Fields) -> None:
+        check(self.L.pic_load_fields(self.h, dptr(f.Ex), dptr(f.Ey), dptr(f.Ez), dptr(f.Bx), dptr(f.By), dptr(f.Bz)),
+              "pic_load_fields")
+
+    def load_current(self, Jx: np.ndarray, Jy: np.ndarray, Jz: np.ndarray) -> None:
+        check(self.L.pic_load_current(self.h, dptr(Jx), dptr(Jy), dptr(Jz)), "pic_load_current")
+
+    def fetch_fields(self, with_current: bool = True) -> Fields:
+        f = Fields.zeros(self.cfg.shape)
+        J = (dptr(f.Jx), dptr(f.Jy), dptr(f.Jz)) if with_current else (None, None, None)
+        check(self.L.pic_fetch_fields(self.h, dptr(f.Ex), dptr(f.Ey), dptr(f.Ez), dptr(f.Bx), dptr(f.By), dptr(f.Bz), *J),
+              "pic_fetch_fields")
+        return f
+
+    def load_particles(self, p: Particles) -> None:
+        arrs = [np.ascontiguousarray(getattr(p, k), dtype=np.float64) for k in Particles.NAMES[:7]]
+        flv = np.ascontiguousarray(p.flv, dtype=np.int32)
+        check(self.L.pic_load_particles(self.h, len(flv), *[dptr(a) for a in arrs], iptr(flv)), "pic_load_particles")
+
+    def particle_count(self) -> int:
+        n = C.c_int64()
+        check(self.L.pic_particle_count(self.h, C.byref(n)), "pic_particle_count")
+        return n.value
+
+    def fetch_particles(self) -> Particles:
+        n = self.particle_count()
+        p = Particles.empty(n)
+        got = C.c_int64()
+        check(self.L.pic_fetch_particles(self.h, C.byref(got), *[dptr(getattr(p, k)) for k in Particles.NAMES[:7]],
+                                         iptr(p.flv)), "pic_fetch_particles")
+        return p
+
+    def init_weibel(self, epc: float, density: float, drift: float, temp_ion: float, temp_elc: float,
+                    seed: int = 2930) -> int:
+        """InitSetup of setup_weibel.F90 generated on the device (Philox-4x32-10)."""
+        check(self.L.pic_init_weibel(self.h, epc, density, drift, temp_ion, temp_elc, seed), "pic_init_weibel")
+        return self.particle_count()
+
+    # -- phases of MAIN.F90 (reference names) -------------------------------
+    def UpdateBfieldHalfGPU(self):
+        """em_update_gpu.F90:44 + SendRecvFlds(B)."""
+        check(self.L.pic_update_b_half(self.h), "pic_update_b_half")
+
+    def MoveDepositPrtlGPU(self):
+        """movdep_gpu.F90:14-49 (J cleared first, as ResetCurrent leaves it)."""
+        check(self.L.pic_move_deposit(self.h), "pic_move_deposit")
+
+    def ExchangePrtlGPU(self):
+        """LoadPrtlOutliers + AppendParticles on one periodic rank."""
+        check(self.L.pic_exchange_particles(self.h), "pic_exchange_particles")
+
+    def UpdateEfieldGPU(self):
+        """em_update_gpu.F90:12-42 + SendRecvFlds(E)."""
+        check(self.L.pic_update_e(self.h), "pic_update_e")
+
+    def UpdateCurrentsAllEdgesGPU(self):
+        """UpdateCurrentAllFaces (comm_fld.F90:15-33): fold ghost J onto images."""
+        check(self.L.pic_fold_current(self.h), "pic_fold_current")
+
+    def smoothen_current_gpu(self):
+        """smoothen_current (current.F90:19-30): curr_filter filter passes."""
+        check(self.L.pic_filter_current(self.h), "pic_filter_current")
+
+    def AddCurrentGPU(self):
+        """em_update_gpu.F90:92-109 + EMfldExchangeGPU."""
+        check(self.L.pic_add_current(self.h), "pic_add_current")
+
+    def ResetCurrentGPU(self):
+        check(self.L.pic_reset_current(self.h), "pic_reset_current")
+
+    def ReorderPrtlGPU(self):
+        """ReorderPrtlArr (mem_prtl.F90:166-301): stable cell-key sort."""
+        check(self.L.pic_reorder(self.h), "pic_reorder")
+
+    update_b_half = UpdateBfieldHalfGPU
+    move_deposit = MoveDepositPrtlGPU
+    exchange_particles = ExchangePrtlGPU
+    update_e = UpdateEfieldGPU
+    fold_current = UpdateCurrentsAllEdgesGPU
+    filter_current = smoothen_current_gpu
+    add_current = AddCurrentGPU
+    reset_current = ResetCurrentGPU
+    reorder = ReorderPrtlGPU
+
+    def step(self, nsteps: int = 1) -> None:
+        """nsteps full steps of MAIN.F90:42-284 as one CUDA graph per step."""
+        check(self.L.pic_step(self.h, int(nsteps)), "pic_step")
+
+    def set_step(self, t: int) -> None:
+        check(self.L.pic_set_step(self.h, int(t)), "pic_set_step")
+
+    def diagnostics(self, masse: float = 1.0) -> dict:
+        n = 4 + len(self.cfg.qm)
+        out = np.zeros(n)
+        check(self.L.pic_diagnostics(self.h, masse, dptr(out), n), "pic_diagnostics")
+        return {"B2": out[0], "E2": out[1], "Benergy": 0.5 * out[0], "Eenergy": 0.5 * out[1],
+                "gauss_linf": out[2], "rho_max": out[3], "kinetic": out[4:].copy()}
+
+    def device_errors(self) -> int:
+        b = C.c_int32()
+        check(self.L.pic_device_errors(self.h, C.byref(b)), "pic_device_errors")
+        return b.value
+
+    @property
+    def stream(self) -> int:
+        return self.L.pic_stream(self.h)

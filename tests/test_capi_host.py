@@ -1,0 +1,83 @@
+"""Host-side checks of the C ABI that need no GPU: the in-tree library loads,
+exports every entry point include/pictor_b200.h declares, and the ctypes
+mirror of pic_config has the C layout."""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "pictor_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(pic_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_entry_point():
+    from pictor_b200 import _capi, build
+
+    build.build()
+    L = C.CDLL(_capi.library_path())
+    names = declared_functions()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    # and the Python binding declares exactly these
+    assert sorted(_capi.SIGNATURES) == names
+
+
+def test_error_strings_without_gpu():
+    from pictor_b200 import _capi
+
+    L = _capi.lib()
+    assert L.pic_error_string(0) == b"ok"
+    assert b"capacity" in L.pic_error_string(-3)
+    assert L.pic_version() >= 10000
+
+
+def test_config_struct_layout_matches_c():
+    from pictor_b200 import _capi
+
+    fields = [f[0] for f in _capi.Config._fields_]
+    prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"pictor_b200.h\"\nint main(){printf(\"%zu\\n\", sizeof(pic_config));"
+    for f in fields:
+        prog += f'printf("%zu\\n", offsetof(pic_config, {f}));'
+    prog += "return 0;}\n"
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "t.c")
+        exe = os.path.join(d, "t")
+        open(c, "w").write(prog)
+        subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
+    assert out[0] == C.sizeof(_capi.Config)
+    for f, off in zip(fields, out[1:]):
+        assert getattr(_capi.Config, f).offset == off, f
+
+
+def test_create_without_gpu_fails_cleanly():
+    """With no CUDA device the library reports PIC_ERR_NOGPU (never a CPU fallback)."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from pictor_b200 import PicConfig, PicError, Simulation
+
+    with pytest.raises(PicError) as e:
+        Simulation(PicConfig(nx=8, ny=8))
+    assert e.value.code in (-8, -6)
+
+
+def test_invalid_configs_rejected_before_device_use():
+    from pictor_b200 import PicConfig, PicError, Simulation
+
+    for bad in (PicConfig(nx=3, ny=8), PicConfig(nx=8, ny=8, c=1.5), PicConfig(nx=8, ny=8, dims=4),
+                PicConfig(nx=8, ny=8, qm=()), PicConfig(nx=8, ny=8, capacity=0)):
+        with pytest.raises(PicError) as e:
+            Simulation(bad)
+        assert e.value.code == -1

@@ -1,0 +1,191 @@
+"""Pins the CPU restatement (the oracle) to hand-derived known answers
+(tests/golden/known_answers.json, made by make_known_answers.py without the
+oracle) and to the discrete invariants of the reference algorithm."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "known_answers.json")))
+
+
+def test_philox_published_vectors():
+    for v in GOLD["philox"]:
+        assert list(O.philox(v["ctr"], v["key"])) == v["out"]
+
+
+@pytest.mark.parametrize("case", GOLD["deposit"]["cases"], ids=lambda c: c["name"])
+def test_single_particle_zigzag_deposit(case):
+    d = GOLD["deposit"]
+    g = O.make_grid(2, 16, 12, c=d["c"], qi=d["qi"])
+    p = O.Particles.from_arrays(8, q=[d["q"]], x=[case["x0"]], y=[case["y0"]], z=[1.5], u=[case["u"]], v=[0.0],
+                                w=[0.0], flv=[1])
+    o = O.Oracle(g, p)
+    o.move_deposit()
+    assert o.p.x[0] == pytest.approx(case["x1"], abs=1e-14)
+    assert o.p.y[0] == case["y0"] and o.p.u[0] == case["u"]
+    expect = {}
+    for comp, i, j, val in case["J"]:
+        expect[(comp, i, j)] = val
+    for comp in ("Jx", "Jy", "Jz"):
+        a = getattr(o.f, comp)
+        nz = {(comp, i + 1, j + 1): a[i, j, 0] for i, j in zip(*np.nonzero(a[:, :, 0]))}
+        want = {k: v for k, v in expect.items() if k[0] == comp}
+        assert set(nz) == set(want), (comp, nz, want)
+        for k, v in want.items():
+            assert nz[k] == pytest.approx(v, abs=1e-14), k
+
+
+def test_boris_gyration_phase_and_invariant():
+    b = GOLD["boris"]
+    g = O.make_grid(2, 16, 16, c=b["c"], qi=0.0, qm=(1.0, b["qm"]), bext=(0.0, 0.0, b["Bz"]))
+    p = O.Particles.from_arrays(4, q=[-1.0], x=[10.5], y=[10.5], z=[1.5], u=[b["u0"]], v=[0.0], w=[0.0], flv=[2])
+    o = O.Oracle(g, p)
+    angles = []
+    for _ in range(10):
+        o.move_deposit()
+        o.p.x[0], o.p.y[0] = 10.5, 10.5  # keep it in place: only the momentum rotation is tested
+        angles.append(math.atan2(o.p.v[0], o.p.u[0]))
+        assert math.hypot(o.p.u[0], o.p.v[0]) == pytest.approx(b["umag"], rel=1e-14)
+    dphi = np.diff(np.unwrap(angles))
+    assert np.allclose(np.abs(dphi), b["phase_per_step"], rtol=1e-12)
+
+
+@pytest.mark.parametrize("fdtd", ["yee"])
+def test_yee_vacuum_dispersion(fdtd):
+    y = GOLD["yee"]
+    nx, m, c = y["nx"], y["m"], y["c"]
+    g = O.make_grid(2, nx, 5, c=c, fdtd=fdtd)
+    k = 2 * math.pi * m / nx
+    i = np.arange(1, g.mx + 1)
+    th = k * (i - 3)
+    cols = []
+    for init in ("E", "B"):
+        f = O.Fields(g)
+        if init == "E":
+            f.Ey[...] = np.cos(th)[:, None, None]
+        else:
+            f.Bz[...] = np.cos(th + k / 2)[:, None, None]
+        o = O.Oracle(g, O.Particles(1), f)
+        o.send_recv_flds("E"); o.send_recv_flds("B")
+        o.update_b_half(); o.send_recv_flds("B")
+        o.update_b_half(); o.send_recv_flds("B")
+        o.update_e(); o.send_recv_flds("E")
+        sl = slice(2, g.mx - 3)
+        a = 2 / nx * np.sum(o.f.Ey[sl, 3, 0] * np.exp(-1j * th[sl]))
+        bb = 2 / nx * np.sum(o.f.Bz[sl, 3, 0] * np.exp(-1j * (th[sl] + k / 2)))
+        cols.append((a, bb))
+    trace = cols[0][0] + cols[1][1]
+    assert abs(trace.imag) < 1e-12
+    assert trace.real == pytest.approx(y["trace"], abs=1e-12)
+
+
+def test_periodic_wrap_appends_shifted_copy():
+    w = GOLD["wrap"]
+    g = O.make_grid(2, w["nx"], w["ny"])
+    p = O.Particles.from_arrays(8, q=[1.0, -1.0], x=[w["x"], 8.2], y=[w["y"], 8.2], z=[w["z"], 1.2],
+                                u=[0.1, 0.2], v=[0.0, 0.0], w=[0.0, 0.0], flv=[1, 2])
+    o = O.Oracle(g, p)
+    assert o.exchange_particles() == 0
+    assert o.p.used == 3
+    assert (o.p.x[0], o.p.y[0], o.p.z[0]) == tuple(w["hole"]) and o.p.flv[0] == 0 and o.p.q[0] == 0
+    assert o.p.x[2] == pytest.approx(w["x_new"], abs=1e-15) and o.p.y[2] == w["y"] and o.p.flv[2] == 1
+    assert o.p.x[1] == 8.2
+
+
+def test_reorder_is_stable_counting_sort():
+    g = O.make_grid(2, 16, 12)
+    rng = np.random.default_rng(0)
+    n = 500
+    x = rng.integers(3, g.mx - 2, n) + rng.random(n)
+    y = rng.integers(3, g.my - 2, n) + rng.random(n)
+    flv = rng.integers(0, 3, n).astype(np.int32)
+    p = O.Particles.from_arrays(n + 8, q=np.arange(n, dtype=float), x=x, y=y, z=np.full(n, 1.5), u=np.zeros(n),
+                                v=np.zeros(n), w=np.zeros(n), flv=flv)
+    o = O.Oracle(g, p)
+    perm = o.reorder()
+    live = np.nonzero(flv != 0)[0]
+    key = (np.floor(y[live]).astype(int) - 1) * g.mx + np.floor(x[live]).astype(int)
+    expect = live[np.argsort(key, kind="stable")]
+    assert np.array_equal(perm, expect)
+    assert o.p.used == live.size
+    assert np.array_equal(o.p.q[: o.p.used], expect.astype(float))
+
+
+@pytest.mark.parametrize("dims,fdtd", [(2, "yee"), (2, "lehe"), (3, "yee"), (3, "lehe")])
+def test_charge_conservation_gauss_residual(dims, fdtd):
+    """2D: the zigzag deposit conserves charge exactly, so divE - rho stays at
+    round-off.  3D: the reference's weights (vars.F90:346-355) are products of
+    segment-midpoint weights and lack the dy*dz/12 cross term of exact
+    conservation, so the residual grows at O(d^3) per move (small, nonzero)."""
+    nx, ny, nz = (24, 20, 1) if dims == 2 else (8, 8, 8)
+    qi = O.init_scale(0.45, 2.0, 8)[0]
+    g = O.make_grid(dims, nx, ny, nz, c=0.45, qi=qi, fdtd=fdtd)
+    p = O.load_weibel(dims, nx, ny, nz, epc=8 if dims == 2 else 4, drift=0.5, temp=0.005, seed=11)
+    o = O.Oracle(g, p)
+    r0, rmax = o.gauss_residual()
+    assert r0 == 0.0 and rmax > 0
+    for t in range(1, 31):
+        assert o.step(t, reorder_period=10) == 0
+    r, rmax = o.gauss_residual()
+    if dims == 2:
+        assert r <= 1e-13 * rmax
+    else:
+        assert 0 < r <= 1e-2 * rmax
+
+
+@pytest.mark.parametrize("move", [(0.3, 0, 0), (0, 0.3, 0), (0, 0, 0.3), (0.9, 0, 0), (0, 0, -0.9)])
+def test_3d_axis_moves_conserve_charge_exactly(move):
+    """A 3D move along one axis (crossing or not) conserves charge exactly;
+    a static partner of opposite charge makes rho vanish at t=0."""
+    g = O.make_grid(3, 8, 8, 8, c=0.45, qi=1.0, qm=(1.0, 0.0))
+    p = O.Particles.from_arrays(4, q=[1.0, -1.0], x=[6.9, 6.9], y=[6.5, 6.5], z=[6.1, 6.1], u=[move[0], 0],
+                                v=[move[1], 0], w=[move[2], 0], flv=[1, 2])
+    o = O.Oracle(g, p)
+    o.move_deposit(); o.fold_current(); o.add_current(); o.send_recv_flds("E")
+    r, rm = o.gauss_residual()
+    assert r <= 1e-15 and rm > 0
+
+
+def test_3d_diagonal_move_residual_is_the_missing_cross_term():
+    """Known answer for the 3D weights: a diagonal move inside one cell leaves
+    a node residual bounded by 3*|q dx dy dz|/12 and not below |q dx dy dz|/12/2."""
+    g = O.make_grid(3, 8, 8, 8, c=0.45, qi=1.0, qm=(1.0, 0.0))
+    p = O.Particles.from_arrays(4, q=[1.0, -1.0], x=[6.2, 6.2], y=[6.7, 6.7], z=[6.4, 6.4], u=[0.2, 0],
+                                v=[-0.3, 0], w=[0.1, 0], flv=[1, 2])
+    o = O.Oracle(g, p)
+    o.move_deposit()
+    d = abs((o.p.x[0] - 6.2) * (o.p.y[0] - 6.7) * (o.p.z[0] - 6.4)) / 12
+    o.fold_current(); o.add_current(); o.send_recv_flds("E")
+    r, _ = o.gauss_residual()
+    assert d / 2 <= r <= 3 * d + 1e-15
+
+
+def test_lehe_coefficients():
+    g = O.make_grid(2, 16, 16, c=0.45, fdtd="lehe")
+    L = O.lehe_coefficients(g)
+    dx = 0.25 * (1 - (1 / 0.45) ** 2 * math.sin(math.pi * 0.45 / 2) ** 2)
+    assert L[9] == pytest.approx(dx, rel=1e-15)
+    assert L[0] == pytest.approx(1 - 0.25 - 3 * dx, rel=1e-15)
+    assert L[1] == 0.75 and L[2] == 1.0
+    g3 = O.make_grid(3, 8, 8, 8, c=0.45, fdtd="lehe")
+    L3 = O.lehe_coefficients(g3)
+    assert L3[0] == pytest.approx(1 - 0.5 - 3 * dx, rel=1e-15) and L3[1] == 0.75 and L3[2] == 0.75
+
+
+def test_weibel_loader_statistics():
+    p = O.load_weibel(2, 64, 64, epc=16, drift=0.5, temp=0.005, seed=2930)
+    v = p.view()
+    n = p.used
+    assert abs(n - 2 * 16 * 64 * 64) < 5 * math.sqrt(2 * 16 * 64 * 64)
+    # pairs are co-located (rho = 0 at t = 0) and alternate flavour 1, 2
+    assert np.array_equal(v["x"][0::2], v["x"][1::2]) and np.array_equal(v["flv"][0::2], np.ones(n // 2))
+    # beams drift +-0.5c along x: mean gamma*beta of flavour-1 particles of each call
+    gb = 0.5 / math.sqrt(1 - 0.25)
+    ux = v["u"]
+    assert np.mean(np.abs(ux)) == pytest.approx(gb, rel=0.02)
+    assert np.all((v["x"] >= 3) & (v["x"] < 67) & (v["y"] >= 3) & (v["y"] < 67) & (v["z"] >= 1) & (v["z"] < 2))
