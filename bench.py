@@ -1,0 +1,414 @@
+"""Throughput of the PIC step on B200: particle-steps/s.
+
+Default workload: the 3D Cartesian Weibel run in the FP32 cell-relative form
+(512x256x256 cells, 8 particles per cell per species in two counter-streaming
+e+- beams at +-0.3c, thermal spread 0.02c, Courant 0.45, periodic), with
+synthetic inputs generated from Philox-4x32-10 on the device.  The same seed
+is also stepped in the FP64 reference form; their throughput ratio and field
+/ total energy difference are reported beside the headline.
+
+One JSON line on stdout (rank 0).  Under torchrun every rank runs its own
+replica (seed + rank): weak scaling with no data-path collective; the timed
+region is bracketed by a barrier and the max over ranks is taken.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200 (FP32/batched vs plain FP64) at stated energy error"
+
+WORKLOADS = {
+    # configs: the 3D FP32 Weibel run (headline) and the 2D FP64 Weibel run
+    "weibel3d_fp32": dict(dims=3, nx=512, ny=256, nz=256, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
+                          precision="fp32"),
+    "weibel2d_fp64": dict(dims=2, nx=256, ny=256, nz=1, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0,
+                          precision="fp64"),
+}
+SEED = 2930
+
+
+def bytes_per_particle(dims: int, precision: str) -> int:
+    """Algorithmic bytes per particle-step: each SoA field read once and the
+    updated ones written once."""
+    if precision == "fp32":
+        return 60 if dims == 3 else 52
+    return 108
+
+
+def bytes_per_cell_mover(precision: str) -> int:
+    """Grid bytes of the mover per interior cell: gather of 6 field components
+    + deposit of 3 current components."""
+    return 9 * (4 if precision == "fp32" else 8)
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.device = device
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    import torch
+
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(ws, value: float) -> float:
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(ws, value: float) -> float:
+    if ws == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def make_sim(wl: dict, precision: str, extra_capacity: float = 1.04):
+    from pictor_b200 import PicConfig, Simulation, init_scale
+
+    sc = init_scale(wl["c"], wl["c_ompe"], wl["epc"])
+    vol = wl["nx"] * wl["ny"] * (wl["nz"] if wl["dims"] == 3 else 1)
+    cap = int(2 * wl["epc"] * vol * extra_capacity) + (1 << 16)
+    cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=wl["nz"], dims=wl["dims"], c=wl["c"], qi=sc["qi"],
+                    precision=precision, capacity=cap, reorder_period=20)
+    return Simulation(cfg), sc
+
+
+def timed_steps(sim, steps: int, ws: int, profile: bool):
+    """K steps bracketed by barrier + synchronize; CUDA events on the
+    library's stream.  Returns (ms total, phase times, launches)."""
+    import torch
+
+    stream = torch.cuda.ExternalStream(sim.stream)
+    sim.profile(profile)
+    sim.phase_times()
+    sim.launch_count()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    phases = sim.phase_times() if profile else None
+    launches = sim.launch_count()
+    sim.profile(False)
+    return ms, phases, launches
+
+
+def energies(sim, sc) -> dict:
+    d = sim.diagnostics(sc["masse"])
+    return {"field": 0.5 * (d["B2"] + d["E2"]), "B": 0.5 * d["B2"], "kinetic": float(sum(d["kinetic"])),
+            "gauss_linf": d["gauss_linf"], "rho_max": d["rho_max"]}
+
+
+def cpu_sample(wl: dict, target_s: float = 12.0, threads: int | None = None):
+    """The reference CPU step (C restatement, OpenMP over 32-particle blocks
+    as the reference's OPEN_MP build) on a bounded sub-box of the workload
+    with the same physics; returns particle-steps/s and what was timed."""
+    from oracle import oracle as O
+
+    if threads:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    dims = wl["dims"]
+    if dims == 3:
+        nx, ny, nz = 96, 48, 48
+    else:
+        nx, ny, nz = 256, 256, 1
+    qi = O.init_scale(wl["c"], wl["c_ompe"], wl["epc"])[0]
+    g = O.make_grid(dims, nx, ny, nz, c=wl["c"], qi=qi)
+    p = O.load_weibel(dims, nx, ny, nz, epc=wl["epc"], drift=wl["drift"], temp=wl["temp"], seed=SEED)
+    o = O.Oracle(g, p, openmp=True)
+    o.step(1)
+    n_steps, t0, t = 0, time.perf_counter(), 1
+    while True:
+        t += 1
+        o.step(t)
+        n_steps += 1
+        el = time.perf_counter() - t0
+        if el >= target_s or n_steps >= 200:
+            break
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return {"value": p.used * n_steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "port",
+            "sample": f"{'x'.join(map(str, (nx, ny, nz)[:dims]))} cells, {p.used} particles, {n_steps} steps "
+                      f"(same physics and seed), FP64, C restatement of the reference CPU path with OpenMP"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU algorithm (C restatement of the
+    Fortran CPU path; the Fortran build is not available here) on the host."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = WORKLOADS[args.workload]
+    from oracle import oracle as O
+
+    O.build()
+    base = cpu_sample(wl, target_s=max(5.0, min(60.0, 3.0 * args.steps)))
+    line = {
+        "metric": METRIC, "value": base["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, **{k: v for k, v in wl.items()}, "seed": SEED},
+        "cpu_baseline": base,
+        "e2e": {"value": base["value"], "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="weibel3d_fp32")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) run")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    from pictor_b200 import build
+
+    build.build()
+    ws, rank, local = dist_setup(args.gpus)
+    wl = WORKLOADS[args.workload]
+    prec = wl["precision"]
+    seed = SEED + rank
+    peak, peak_kind = measured_peaks()
+
+    # ---- headline: the workload in its own precision, inputs resident -----
+    sim, sc = make_sim(wl, prec)
+    n_p = sim.init_weibel(wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], seed)
+    sim.reorder()                      # ReorderPrtl at Startups (MAIN.F90:307)
+    sim.step(args.warmup)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, phases, launches = timed_steps(sim, args.steps, ws, profile=True)
+    clk = clocks.stop()
+    e32 = energies(sim, sc)
+    ms_max = max_over_ranks(ws, ms)
+    n_tot = sum_over_ranks(ws, float(n_p))
+    value = n_tot * args.steps / (ms_max * 1e-3)
+
+    n_cells = wl["nx"] * wl["ny"] * (wl["nz"] if wl["dims"] == 3 else 1)
+    move_ms = phases["ms"]["move"] / max(phases["steps"], 1)
+    bytes_move = n_p * bytes_per_particle(wl["dims"], prec) + n_cells * bytes_per_cell_mover(prec)
+    achieved = bytes_move / (move_ms * 1e-3) / 1e9
+    step_bytes = (n_p * bytes_per_particle(wl["dims"], prec) + n_cells * 24 * (4 if prec == "fp32" else 8))
+    sim.close()
+    del sim
+
+    # ---- FP64 reference form on the same seed -------------------------------
+    fp64 = None
+    if not args.no_fp64 and prec == "fp32":
+        sim64, _ = make_sim(wl, "fp64")
+        sim64.init_weibel(wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], seed)
+        sim64.reorder()
+        sim64.step(args.warmup)
+        ms64, ph64, _ = timed_steps(sim64, args.steps, ws, profile=True)
+        e64 = energies(sim64, sc)
+        ms64 = max_over_ranks(ws, ms64)
+        v64 = n_tot * args.steps / (ms64 * 1e-3)
+        fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "speedup_fp32_over_fp64": value / v64,
+                "field_energy_rel_err": abs(e32["field"] - e64["field"]) / max(abs(e64["field"]), 1e-300),
+                "total_energy_rel_err": abs((e32["field"] + e32["kinetic"]) - (e64["field"] + e64["kinetic"]))
+                / max(abs(e64["field"] + e64["kinetic"]), 1e-300),
+                "field_energy_fp64": e64["field"], "field_energy_fp32": e32["field"],
+                "gauss_linf_over_rho": e64["gauss_linf"] / max(e64["rho_max"], 1e-300),
+                "move_ms": ph64["ms"]["move"] / max(ph64["steps"], 1)}
+        sim64.close()
+        del sim64
+
+    # ---- end to end through the C ABI with host buffers ---------------------
+    e2e = None
+    if not args.no_e2e:
+        sim, sc = make_sim(wl, prec)
+        sim.init_weibel(wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], seed)
+        host = sim.fetch_particles()  # reference-layout FP64 host arrays
+        pinned = {}
+        for k in ("q", "x", "y", "z", "u", "v", "w", "flv"):
+            a = getattr(host, k)
+            t = torch.from_numpy(a).pin_memory()
+            pinned[k] = t
+        del host
+        from pictor_b200 import Particles
+
+        hp = Particles(*(pinned[k].numpy() for k in ("q", "x", "y", "z", "u", "v", "w", "flv")))
+        stream = torch.cuda.ExternalStream(sim.stream)
+        sim.load_particles(hp)
+        sim.reorder()
+        sim.step(args.warmup)
+        barrier(ws)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.load_particles(hp)                 # host -> device: the run's particle state
+        sim.reorder()                          # ReorderPrtl at Startups
+        sim.step(args.steps)
+        d = sim.diagnostics(sc["masse"])       # device -> host: energies, Gauss residual
+        f = sim.fetch_fields(with_current=False)  # device -> host: the fields
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) * 1e3
+        barrier(ws)
+        ms_e2e = max_over_ranks(ws, max(wall, e0.elapsed_time(e1)))
+        h2d = n_p * (7 * 8 + 4)
+        d2h = 6 * (wl["nx"] + 5) * (wl["ny"] + 5) * ((wl["nz"] + 5) if wl["dims"] == 3 else 1) * 8 + 8 * len(d["kinetic"]) + 32
+        e2e = {"value": n_tot * args.steps / (ms_e2e * 1e-3), "unit": "particle-steps/s",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "ms": ms_e2e, "includes": "pic_load_particles from pinned FP64 host arrays + K steps + "
+                                          "pic_diagnostics + pic_fetch_fields"}
+        sim.close()
+        del sim, f
+
+    # ---- CPU baseline (rank 0, N=1) -----------------------------------------
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle as O
+
+        O.build()
+        cpu = cpu_sample(wl)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if prec == "fp32" else "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "cells": [wl["nx"], wl["ny"], wl["nz"]][: wl["dims"]],
+                       "particles_per_gpu": n_p, "particles_per_cell_per_species": wl["epc"],
+                       "drift_c": wl["drift"], "thermal_c": math.sqrt(wl["temp"] / 2), "courant": wl["c"],
+                       "c_ompe": wl["c_ompe"], "reorder_period": 20, "seed": SEED, "parallelism": f"replicas{ws}",
+                       "l2": "inputs larger than L2 (particle state >> 126 MB)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "k_move_f32" if prec == "fp32" else "k_move_f64",
+                         "algorithmic_bytes_per_launch": bytes_move, "launch_ms": move_ms,
+                         "peak_kind": peak_kind, "step_algorithmic_GBs": step_bytes / (ms_max / args.steps * 1e-3) / 1e9},
+            "phases_ms_per_step": {k: v / max(phases["steps"], 1) for k, v in phases["ms"].items()},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "energy": {k: e32[k] for k in ("field", "kinetic", "gauss_linf", "rho_max")},
+        }
+        if fp64:
+            line["fp64"] = fp64
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -137,6 +137,26 @@ int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout);
 enum { PIC_DEVERR_RANGE = 1, PIC_DEVERR_OVERFLOW = 2, PIC_DEVERR_NAN = 4 };
 int pic_device_errors(pic_handle *h, int32_t *bits);
 
+/* Phases of pic_step, in step order. */
+enum {
+    PIC_PHASE_BHALF1 = 0, /* UpdateBfieldHalf + halo before the push     */
+    PIC_PHASE_MOVE,       /* MoveDepositPrtl                               */
+    PIC_PHASE_EXCHANGE,   /* particle wrap (FP64 layout)                   */
+    PIC_PHASE_BHALF2,     /* second UpdateBfieldHalf + halo                */
+    PIC_PHASE_EFIELD,     /* UpdateEfield + fold + AddCurrent + halo       */
+    PIC_PHASE_REORDER,    /* ReorderPrtl (every reorder_period steps)      */
+    PIC_PHASE_COUNT
+};
+/* Profiling (the reference's per-phase timers, MAIN.F90:440-452 and
+   communication.F90:69-94, on the device): while enabled, pic_step launches
+   phases eagerly with a CUDA event pair around each; pic_phase_times returns
+   the summed milliseconds and kernel launches per phase and the number of
+   profiled steps, then resets them. */
+int pic_profile(pic_handle *h, int32_t enable);
+int pic_phase_times(pic_handle *h, double *ms, int64_t *launches, int32_t n, int64_t *steps);
+/* Kernels launched by pic_step since the last call (graph or eager). */
+int pic_launch_count(pic_handle *h, int64_t *launches);
+
 /* Text for an error code. */
 const char *pic_error_string(int code);
 

@@ -84,6 +84,9 @@ def _declare(L: C.CDLL) -> None:
     L.orc_lehe_coefficients.argtypes = [P(Grid), P(C.c_double)]
     L.orc_send_recv_flds.argtypes = [P(Grid)] + [P(C.c_double)] * 3
     L.orc_update_current_all_faces.argtypes = [P(Grid)] + [P(C.c_double)] * 3
+    L.orc_filter_current.argtypes = [P(Grid)] + [P(C.c_double)] * 3 + [C.c_int]
+    L.orc_step_filtered.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int, C.c_int]
+    L.orc_step_filtered.restype = C.c_int
     L.orc_move_deposit.argtypes = [P(Grid), P(_Particles), P(_Fields)]
     L.orc_exchange_particles.argtypes = [P(Grid), P(_Particles)]
     L.orc_exchange_particles.restype = C.c_int
@@ -225,6 +228,13 @@ class Oracle:
 
     def fold_current(self):
         self.L.orc_update_current_all_faces(C.byref(self.g), _dp(self.f.Jx), _dp(self.f.Jy), _dp(self.f.Jz))
+
+    def filter_current(self, passes: int):
+        self.L.orc_filter_current(C.byref(self.g), _dp(self.f.Jx), _dp(self.f.Jy), _dp(self.f.Jz), int(passes))
+
+    def step_filtered(self, t: int, reorder_period: int, curr_filter: int) -> int:
+        fs = self.f.struct()
+        return self._call_p(self.L.orc_step_filtered, C.byref(fs), int(t), int(reorder_period), int(curr_filter))
 
     def move_deposit(self):
         fs = self.f.struct()

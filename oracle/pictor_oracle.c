@@ -287,6 +287,54 @@ void orc_update_current_all_faces(const orc_grid *g, double *Jx, double *Jy, dou
         }
 }
 
+/* current.F90:55-163 MovingAverageFilter on one periodic rank: before each
+   axis pass the halo of that axis is refreshed (SendRecvFldsYZ / ZX / XY),
+   then F = wtm1*F(-1) + wt0*F + wtp1*F(+1) over 2..m-2 (2D k = 1). */
+static void moving_average_axis(const orc_grid *g, double *F, int axis)
+{
+    const size_t n = (size_t)g->mx * g->my * g->mz;
+    double *tmp = (double *)malloc(n * sizeof(double));
+    memcpy(tmp, F, n * sizeof(double));
+    const int k1 = g->dims == 3 ? 2 : 1, k2 = g->dims == 3 ? g->mz - 2 : 1;
+    for (int k = k1; k <= k2; k++)
+        for (int j = 2; j <= g->my - 2; j++)
+            for (int i = 2; i <= g->mx - 2; i++) {
+                int lo[3] = {i, j, k}, hi[3] = {i, j, k};
+                lo[axis] -= 1;
+                hi[axis] += 1;
+                tmp[ID(g, i, j, k)] = (0.25 * F[ID(g, lo[0], lo[1], lo[2])] + 0.5 * F[ID(g, i, j, k)]) +
+                                      0.25 * F[ID(g, hi[0], hi[1], hi[2])];
+            }
+    for (int k = k1; k <= k2; k++)
+        for (int j = 2; j <= g->my - 2; j++)
+            for (int i = 2; i <= g->mx - 2; i++) F[ID(g, i, j, k)] = tmp[ID(g, i, j, k)];
+    free(tmp);
+}
+
+void orc_filter_current(const orc_grid *g, double *Jx, double *Jy, double *Jz, int passes)
+{
+    double *F[3] = {Jx, Jy, Jz};
+    for (int ps = 0; ps < passes; ps++) {                        /* smoothen_current, current.F90:19-30 */
+        for (int c = 0; c < 3; c++) {
+            int lo[3] = {1, 1, 1}, hi[3] = {1, g->my, g->mz};
+            halo_axis(g, F[c], 0, lo, hi);                       /* SendRecvFldsYZ */
+        }
+        for (int c = 0; c < 3; c++) moving_average_axis(g, F[c], 0);
+        for (int c = 0; c < 3; c++) {
+            int lo[3] = {3, 1, 1}, hi[3] = {g->mx - 3, 1, g->mz};
+            halo_axis(g, F[c], 1, lo, hi);                       /* SendRecvFldsZX */
+        }
+        for (int c = 0; c < 3; c++) moving_average_axis(g, F[c], 1);
+        if (g->dims == 3) {
+            for (int c = 0; c < 3; c++) {
+                int lo[3] = {3, 1, 1}, hi[3] = {g->mx - 3, g->my, 1};
+                halo_axis(g, F[c], 2, lo, hi);                   /* SendRecvFldsXY */
+            }
+            for (int c = 0; c < 3; c++) moving_average_axis(g, F[c], 2);
+        }
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* Mover + deposit: movdep.F90:12-258, movdep_routines.F90:6-311             */
 /* ------------------------------------------------------------------------- */
@@ -677,6 +725,24 @@ void orc_reorder(const orc_grid *g, orc_particles *p, int64_t *perm)
 /* ------------------------------------------------------------------------- */
 /* One time step, src/MAIN.F90:42-284                                        */
 /* ------------------------------------------------------------------------- */
+int orc_step_filtered(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period, int curr_filter)
+{
+    orc_update_b_half(g, f);
+    orc_send_recv_flds(g, f->Bx, f->By, f->Bz);
+    orc_move_deposit(g, p, f);
+    int rc = orc_exchange_particles(g, p);
+    orc_update_b_half(g, f);
+    orc_send_recv_flds(g, f->Bx, f->By, f->Bz);
+    orc_update_e(g, f);
+    orc_send_recv_flds(g, f->Ex, f->Ey, f->Ez);
+    orc_update_current_all_faces(g, f->Jx, f->Jy, f->Jz);
+    orc_filter_current(g, f->Jx, f->Jy, f->Jz, curr_filter);  /* MAIN.F90:156-165 */
+    orc_add_current(g, f);
+    orc_send_recv_flds(g, f->Ex, f->Ey, f->Ez);
+    if (reorder_period > 0 && t % reorder_period == 0) orc_reorder(g, p, NULL);
+    return rc;
+}
+
 int orc_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period)
 {
     orc_update_b_half(g, f);                                   /* :49-56 */

@@ -72,6 +72,8 @@ void orc_lehe_coefficients(const orc_grid *g, double out[12]);
 void orc_send_recv_flds(const orc_grid *g, double *Fx, double *Fy, double *Fz);
 /* comm_fld.F90 UpdateCurrentAllFaces on a single periodic rank. */
 void orc_update_current_all_faces(const orc_grid *g, double *Jx, double *Jy, double *Jz);
+/* current.F90 smoothen_current (curr_filter passes of MovingAverageFilter). */
+void orc_filter_current(const orc_grid *g, double *Jx, double *Jy, double *Jz, int passes);
 /* current.F90 ResetCurrent */
 void orc_reset_current(const orc_grid *g, orc_fields *f);
 
@@ -89,6 +91,8 @@ void orc_reorder(const orc_grid *g, orc_particles *p, int64_t *perm);
 /* One time step of src/MAIN.F90:42-284 (single rank, periodic, curr_filter=0,
    no setup hooks).  t is the step counter used by the reorder period test. */
 int orc_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period);
+/* orc_step with curr_filter passes of the current filter (MAIN.F90:156-165). */
+int orc_step_filtered(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period, int curr_filter);
 
 /* savedata_routines.F90 CalcFldEnergy (sums, not halved): out[0]=sum|B|^2,
    out[1]=sum|E|^2 over the interior 3..m-3. */

@@ -20,6 +20,7 @@ ERRORS = {
     -1: "PIC_ERR_INVALID", -2: "PIC_ERR_OOM", -3: "PIC_ERR_OVERFLOW", -4: "PIC_ERR_NAN",
     -5: "PIC_ERR_TIMEOUT", -6: "PIC_ERR_CUDA", -7: "PIC_ERR_RANGE", -8: "PIC_ERR_NOGPU",
 }
+PHASES = ("bhalf1", "move", "exchange", "bhalf2", "efield", "reorder")
 GEOM = {"cartesian": 0, "cylindrical": 1}
 FDTD = {"yee": 0, "lehe": 1}
 PRECISION = {"fp64": 0, "fp32": 1}
@@ -103,6 +104,9 @@ SIGNATURES = {
     "pic_set_step": (C.c_int, [H, C.c_int64]),
     "pic_diagnostics": (C.c_int, [H, C.c_double, PD, C.c_int32]),
     "pic_device_errors": (C.c_int, [H, PI32]),
+    "pic_profile": (C.c_int, [H, C.c_int32]),
+    "pic_phase_times": (C.c_int, [H, PD, PI64, C.c_int32, PI64]),
+    "pic_launch_count": (C.c_int, [H, PI64]),
     "pic_error_string": (C.c_char_p, [C.c_int]),
     "pic_stream": (C.c_void_p, [H]),
 }

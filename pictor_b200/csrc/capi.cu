@@ -34,8 +34,23 @@ struct pic_handle {
     double *rho = nullptr, *rho_pos = nullptr;
     long long t = 0;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    int graph_kernels[2][2] = {{0, 0}, {0, 0}};
+    bool profiling = false;
+    double phase_ms[PIC_PHASE_COUNT] = {};
+    long long phase_launches[PIC_PHASE_COUNT] = {};
+    long long prof_steps = 0;
+    long long launches = 0;   // kernels launched by pic_step since the last pic_launch_count
+    // FP32 spatial tiles (valid while `sorted`: set by a reorder, cleared by loads)
+    Tiling tiles = {};
+    bool sorted = false;
     std::vector<void *> allocs;
 };
+
+static thread_local long long g_launches = 0;
+
+namespace pic {
+void count_launches(int n) { g_launches += n; }
+}  // namespace pic
 
 namespace {
 
@@ -132,44 +147,84 @@ void field_ptrs(pic_handle *h, T *E[3], T *B[3], T *J[3])
     }
 }
 
-// The launches of one full step (MAIN.F90:42-284), enqueued on h->s.  Reads
-// `cur` and, when reorder is set, leaves the particles in buffer cur^1.
-void enqueue_step(pic_handle *h, int cur, bool reorder)
+// One phase of a full step (MAIN.F90:42-284), enqueued on h->s; reads
+// buffer `cur` and, for the reorder phase, leaves the particles in cur^1.
+// Returns the number of kernels it launched.
+int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
 {
     const GridP &g = h->g;
     const bool filt = h->cfg.curr_filter > 0;
+    g_launches = 0;
     if (!h->fp32) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_bhalf<double>(g, E, B, h->s);                                      // :49-58
-        launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);  // :63-71
-        launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s); // :86-94, :145-150
-        launch_bhalf<double>(g, E, B, h->s);                                      // :101-105
-        if (!filt) {
-            launch_efield<double>(g, 1, E, B, J, h->s);                           // :108-110, :124, :170-184
-        } else {
-            launch_fold<double>(g, J, h->s);
-            for (int k = 0; k < h->cfg.curr_filter; k++) launch_filter<double>(g, J, (double *)h->Jtmp, h->s);
-            launch_efield<double>(g, 3, E, B, J, h->s);
-            for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(double), h->s);
+        switch (phase) {
+            case PIC_PHASE_BHALF1:  // MAIN.F90:49-58
+            case PIC_PHASE_BHALF2:  // MAIN.F90:101-105
+                launch_bhalf<double>(g, E, B, h->s);
+                break;
+            case PIC_PHASE_MOVE:  // MAIN.F90:63-71
+                launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);
+                break;
+            case PIC_PHASE_EXCHANGE:  // MAIN.F90:86-94 + 145-150
+                launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s);
+                break;
+            case PIC_PHASE_EFIELD:  // MAIN.F90:108-110, 124, 158, 170-184
+                if (!filt) {
+                    launch_efield<double>(g, 1, E, B, J, h->s);
+                } else {
+                    launch_fold<double>(g, J, h->s);
+                    for (int k = 0; k < h->cfg.curr_filter; k++) launch_filter<double>(g, J, (double *)h->Jtmp, h->s);
+                    launch_efield<double>(g, 3, E, B, J, h->s);
+                    for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(double), h->s);
+                }
+                break;
+            case PIC_PHASE_REORDER:  // MAIN.F90:259-265
+                if (reorder)
+                    launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+                break;
         }
-        if (reorder) launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
     } else {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_bhalf<float>(g, E, B, h->s);
-        launch_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
-        launch_bhalf<float>(g, E, B, h->s);
-        if (!filt) {
-            launch_efield<float>(g, 1, E, B, J, h->s);
-        } else {
-            launch_fold<float>(g, J, h->s);
-            for (int k = 0; k < h->cfg.curr_filter; k++) launch_filter<float>(g, J, (float *)h->Jtmp, h->s);
-            launch_efield<float>(g, 3, E, B, J, h->s);
-            for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(float), h->s);
+        switch (phase) {
+            case PIC_PHASE_BHALF1:
+            case PIC_PHASE_BHALF2:
+                launch_bhalf<float>(g, E, B, h->s);
+                break;
+            case PIC_PHASE_MOVE:
+                if (h->sorted)
+                    launch_move_deposit_f32_tiled(g, h->p32[cur], h->tiles.tile_start, h->tiles.ntiles, E, B, J, h->err,
+                                                  h->s);
+                else
+                    launch_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
+                break;
+            case PIC_PHASE_EXCHANGE:  // the FP32 form wraps inside the mover
+                break;
+            case PIC_PHASE_EFIELD:
+                if (!filt) {
+                    launch_efield<float>(g, 1, E, B, J, h->s);
+                } else {
+                    launch_fold<float>(g, J, h->s);
+                    for (int k = 0; k < h->cfg.curr_filter; k++) launch_filter<float>(g, J, (float *)h->Jtmp, h->s);
+                    launch_efield<float>(g, 3, E, B, J, h->s);
+                    for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(float), h->s);
+                }
+                break;
+            case PIC_PHASE_REORDER:
+                if (reorder)
+                    launch_reorder_f32(g, h->p32[cur], h->p32[cur ^ 1], h->cnt, h->sc, h->capacity, &h->tiles, h->s);
+                break;
         }
-        if (reorder) launch_reorder_f32(g, h->p32[cur], h->p32[cur ^ 1], h->cnt, h->sc, h->capacity, h->s);
     }
+    return (int)g_launches;
+}
+
+int enqueue_step(pic_handle *h, int cur, bool reorder)
+{
+    int n = 0;
+    for (int ph = 0; ph < PIC_PHASE_COUNT; ph++) n += enqueue_phase(h, cur, reorder, ph);
+    return n;
 }
 
 int get_graph(pic_handle *h, int cur, bool reorder, cudaGraphExec_t *out)
@@ -178,7 +233,7 @@ int get_graph(pic_handle *h, int cur, bool reorder, cudaGraphExec_t *out)
     if (!ge) {
         cudaGraph_t graph = nullptr;
         CK(cudaStreamBeginCapture(h->s, cudaStreamCaptureModeThreadLocal));
-        enqueue_step(h, cur, reorder);
+        h->graph_kernels[reorder ? 1 : 0][cur] = enqueue_step(h, cur, reorder);
         cudaError_t e = cudaStreamEndCapture(h->s, &graph);
         if (e != cudaSuccess) return cuda_status(e);
         e = cudaGraphInstantiate(&ge, graph, 0);
@@ -190,6 +245,54 @@ int get_graph(pic_handle *h, int cur, bool reorder, cudaGraphExec_t *out)
     }
     *out = ge;
     return PIC_OK;
+}
+
+// pic_step with an event pair around every phase of every step (no graphs).
+int step_profiled(pic_handle *h, int32_t nsteps)
+{
+    const int NE = PIC_PHASE_COUNT + 1;
+    std::vector<cudaEvent_t> ev((size_t)nsteps * NE);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    int rc = PIC_OK;
+    for (int32_t i = 0; i < nsteps && rc == PIC_OK; i++) {
+        h->t += 1;
+        const bool reorder = h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0;
+        cudaEvent_t *e = &ev[(size_t)i * NE];
+        cudaEventRecord(e[0], h->s);
+        for (int ph = 0; ph < PIC_PHASE_COUNT; ph++) {
+            h->phase_launches[ph] += enqueue_phase(h, h->cur, reorder, ph);
+            cudaEventRecord(e[ph + 1], h->s);
+        }
+        if (reorder) {
+            h->cur ^= 1;
+            if (h->fp32) h->sorted = true;  // eager launches: no graph to drop
+        }
+        h->prof_steps += 1;
+        if (cudaGetLastError() != cudaSuccess) rc = PIC_ERR_CUDA;
+    }
+    if (cudaStreamSynchronize(h->s) != cudaSuccess) rc = PIC_ERR_CUDA;
+    for (int32_t i = 0; i < nsteps && rc == PIC_OK; i++)
+        for (int ph = 0; ph < PIC_PHASE_COUNT; ph++) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ev[(size_t)i * NE + ph], ev[(size_t)i * NE + ph + 1]);
+            h->phase_ms[ph] += ms;
+        }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return rc;
+}
+
+// The FP32 mover variant is baked into the step graphs: drop them when the
+// tile ranges become valid or stale.
+void set_sorted(pic_handle *h, bool sorted)
+{
+    if (h->sorted == sorted) return;
+    h->sorted = sorted;
+    for (auto &row : h->graph)
+        for (auto &ge : row)
+            if (ge) {
+                cudaGraphExecDestroy(ge);
+                ge = nullptr;
+            }
 }
 
 size_t field_bytes(const pic_handle *h) { return (size_t)h->g.ncell * (h->fp32 ? sizeof(float) : sizeof(double)); }
@@ -343,6 +446,16 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     }
     if (!r && c.curr_filter > 0) r = dalloc(h, (char **)&h->Jtmp, fb);
     if (!r) r = alloc_particles(h);
+    if (!r && h->fp32) {
+        // tile width: about 2048 particles per tile at the configured fill
+        const double ppc = (double)h->capacity / ((double)g.nx * g.ny * g.nz);
+        int w = 8;
+        while (w < g.nx && w * 2 * ppc <= 2048.0) w *= 2;
+        h->tiles.width = w < g.nx ? w : g.nx;
+        h->tiles.per_row = (g.nx + h->tiles.width - 1) / h->tiles.width;
+        h->tiles.ntiles = h->tiles.per_row * g.ny * g.nz;
+        r = dalloc(h, &h->tiles.tile_start, (size_t)h->tiles.ntiles + 1);
+    }
     if (!r) r = dalloc(h, &h->cnt, 1);
     if (!r) r = dalloc(h, &h->err, 1);
     if (!r) {
@@ -496,6 +609,7 @@ int pic_load_particles(pic_handle *h, int64_t n, const double *q, const double *
     c0.used = n;
     c0.np = n;
     CK(cudaMemcpyAsync(h->cnt, &c0, sizeof(Counters), cudaMemcpyHostToDevice, h->s));
+    set_sorted(h, false);
     return finish(h);
 }
 
@@ -553,6 +667,7 @@ int pic_init_weibel(pic_handle *h, double epc, double density, double drift, dou
     const PartF64 *p64 = h->fp32 ? nullptr : &h->p64[h->cur];
     const PartF32 *p32 = h->fp32 ? &h->p32[h->cur] : nullptr;
     CK(cudaMemsetAsync(h->cnt, 0, sizeof(Counters), h->s));
+    set_sorted(h, false);
     int r = launch_weibel(h->g, w, h->tab_x, h->tab_p, h->ntab, p64, p32, h->cnt, h->sc, h->capacity, h->err, h->s);
     if (r) return r;
     return finish(h);
@@ -674,9 +789,10 @@ int pic_add_current(pic_handle *h)
 int pic_reorder(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->fp32) launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->s);
+    if (h->fp32) launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->sc, h->capacity, &h->tiles, h->s);
     else launch_reorder_f64(h->g, h->p64[h->cur], h->p64[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
     h->cur ^= 1;
+    set_sorted(h, h->fp32);
     return finish(h);
 }
 
@@ -693,6 +809,15 @@ int pic_step(pic_handle *h, int32_t nsteps)
     // J must be zero when a deposit starts; inside the loop the E update
     // consumes and clears it.
     for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
+    if (h->profiling) {
+        const long long before = [&] { long long n = 0; for (long long v : h->phase_launches) n += v; return n; }();
+        int r = step_profiled(h, nsteps);
+        long long after = 0;
+        for (long long v : h->phase_launches) after += v;
+        h->launches += after - before;
+        if (r) return r;
+        return finish(h);
+    }
     for (int32_t i = 0; i < nsteps; i++) {
         h->t += 1;
         const bool reorder = h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0;
@@ -700,7 +825,14 @@ int pic_step(pic_handle *h, int32_t nsteps)
         int r = get_graph(h, h->cur, reorder, &ge);
         if (r) return r;
         CK(cudaGraphLaunch(ge, h->s));
-        if (reorder) h->cur ^= 1;
+        h->launches += h->graph_kernels[reorder ? 1 : 0][h->cur];
+        if (reorder) {
+            h->cur ^= 1;
+            if (h->fp32 && !h->sorted) {  // tile ranges are valid from now on
+                CK(cudaStreamSynchronize(h->s));
+                set_sorted(h, true);
+            }
+        }
     }
     return finish(h);
 }
@@ -730,6 +862,37 @@ int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout)
     const int n = nout < 4 + h->cfg.nflvr ? nout : 4 + h->cfg.nflvr;
     for (int i = 0; i < n; i++) out[i] = tmp[i];
     return r;
+}
+
+int pic_profile(pic_handle *h, int32_t enable)
+{
+    if (!h) return PIC_ERR_INVALID;
+    h->profiling = enable != 0;
+    return PIC_OK;
+}
+
+int pic_phase_times(pic_handle *h, double *ms, int64_t *launches, int32_t n, int64_t *steps)
+{
+    if (!h || n < 0) return PIC_ERR_INVALID;
+    for (int i = 0; i < n && i < PIC_PHASE_COUNT; i++) {
+        if (ms) ms[i] = h->phase_ms[i];
+        if (launches) launches[i] = h->phase_launches[i];
+    }
+    if (steps) *steps = h->prof_steps;
+    for (int i = 0; i < PIC_PHASE_COUNT; i++) {
+        h->phase_ms[i] = 0;
+        h->phase_launches[i] = 0;
+    }
+    h->prof_steps = 0;
+    return PIC_OK;
+}
+
+int pic_launch_count(pic_handle *h, int64_t *launches)
+{
+    if (!h || !launches) return PIC_ERR_INVALID;
+    *launches = h->launches;
+    h->launches = 0;
+    return PIC_OK;
 }
 
 int pic_device_errors(pic_handle *h, int32_t *bits)

@@ -47,6 +47,10 @@ __host__ __device__ inline int wrap_index(int i, int m)
     return i;
 }
 
+// Kernel-launch accounting (for the launch count a benchmark reports): every
+// host launcher adds the number of kernels it enqueued.
+void count_launches(int n);
+
 // Error bits written by kernels (never __trap): see PIC_DEVERR_*.
 __device__ inline void raise_error(int *err, int bit) { atomicOr(err, bit); }
 

@@ -90,6 +90,8 @@ void launch_field_energy(const GridP &g, const void *const E[3], const void *con
             g, (const double *)E[0], (const double *)E[1], (const double *)E[2], (const double *)B[0],
             (const double *)B[1], (const double *)B[2], partials);
     k_sum_partials<<<1, 32, 0, s>>>(partials, nblocks, out2);
+    count_launches(1);
+    count_launches(1);
 }
 
 // ---------------------------------------------------------------------------
@@ -146,12 +148,14 @@ void launch_particle_energy_f64(const GridP &g, const PartF64 &p, const Counters
                                 cudaStream_t s)
 {
     k_pe_f64<<<kSMs * 4, kDiagThreads, 0, s>>>(g, p, cnt, masse, out);
+    count_launches(1);
 }
 
 void launch_particle_energy_f32(const GridP &g, const PartF32 &p, const Counters *cnt, double masse, double *out,
                                 cudaStream_t s)
 {
     k_pe_f32<<<kSMs * 4, kDiagThreads, 0, s>>>(g, p, cnt, masse, out);
+    count_launches(1);
 }
 
 // ---------------------------------------------------------------------------
@@ -231,7 +235,9 @@ void launch_gauss_f64(const GridP &g, const PartF64 &p, const Counters *cnt, con
     cudaMemsetAsync(rho_pos, 0, (size_t)g.ncell * sizeof(double), s);
     cudaMemsetAsync(out2, 0, 2 * sizeof(double), s);
     k_rho_f64<<<kSMs * 8, 256, 0, s>>>(g, p, cnt, rho, rho_pos);
+    count_launches(1);
     k_gauss_max<double><<<field_energy_blocks(g), kDiagThreads, 0, s>>>(g, E[0], E[1], E[2], rho, rho_pos, out2);
+    count_launches(1);
 }
 
 void launch_gauss_f32(const GridP &g, const PartF32 &p, const Counters *cnt, const float *const E[3], double *rho,
@@ -241,7 +247,9 @@ void launch_gauss_f32(const GridP &g, const PartF32 &p, const Counters *cnt, con
     cudaMemsetAsync(rho_pos, 0, (size_t)g.ncell * sizeof(double), s);
     cudaMemsetAsync(out2, 0, 2 * sizeof(double), s);
     k_rho_f32<<<kSMs * 8, 256, 0, s>>>(g, p, cnt, rho, rho_pos);
+    count_launches(1);
     k_gauss_max<float><<<field_energy_blocks(g), kDiagThreads, 0, s>>>(g, E[0], E[1], E[2], rho, rho_pos, out2);
+    count_launches(1);
 }
 
 }  // namespace pic

@@ -303,6 +303,7 @@ void launch_bhalf(const GridP &g, T *const E[3], T *const B[3], cudaStream_t s)
         if (g.fdtd == PIC_FDTD_YEE) k_bhalf<T, 2, PIC_FDTD_YEE><<<grid, block, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2]);
         else k_bhalf<T, 2, PIC_FDTD_LEHE><<<grid, block, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2]);
     }
+    count_launches(1);
 }
 
 template <typename T>
@@ -322,6 +323,7 @@ void launch_efield(const GridP &g, int mode, T *const E[3], T *const B[3], T *co
         else LE(2, 3);
     }
 #undef LE
+    count_launches(1);
 }
 
 template <typename T>
@@ -330,6 +332,7 @@ void launch_fold(const GridP &g, T *const J[3], cudaStream_t s)
     const dim3 grid = interior_grid(g), block(32, 8, 1);
     if (g.dims == 3) k_fold<T, 3><<<grid, block, 0, s>>>(g, J[0], J[1], J[2]);
     else k_fold<T, 2><<<grid, block, 0, s>>>(g, J[0], J[1], J[2]);
+    count_launches(1);
 }
 
 template <typename T>
@@ -344,6 +347,7 @@ void launch_filter(const GridP &g, T *const J[3], T *tmp, cudaStream_t s)
             cudaMemcpyAsync(J[c], tmp, bytes, cudaMemcpyDeviceToDevice, s);
         }
     }
+    count_launches(3 * g.dims);
 }
 
 template void launch_bhalf<double>(const GridP &, double *const[3], double *const[3], cudaStream_t);

@@ -34,6 +34,9 @@ void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *c
                              double *const B[3], double *const J[3], int *err, cudaStream_t s);
 void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
                              float *const B[3], float *const J[3], int *err, cudaStream_t s);
+// Tiled FP32 mover: one CTA per spatial tile (tile_start[ntiles+1] particle ranges).
+void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const uint32_t *tile_start, int ntiles,
+                                   float *const E[3], float *const B[3], float *const J[3], int *err, cudaStream_t s);
 
 // particles.cu
 struct SortScratch {
@@ -53,8 +56,14 @@ void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch 
 // `out`, after which the caller swaps `p` and `out`.
 void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Counters *cnt, SortScratch &sc,
                         long long capacity, int *err, cudaStream_t s);
+// Tiles: row segments of `width` interior cells, S = ceil(nx/width) per (j,k)
+// row; tile_start (ntiles + 1 entries) receives each tile's first particle.
+struct Tiling {
+    uint32_t *tile_start;
+    int width, per_row, ntiles;
+};
 void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, SortScratch &sc,
-                        long long capacity, cudaStream_t s);
+                        long long capacity, const Tiling *tiles, cudaStream_t s);
 // Reference layout <-> FP32 cell-relative conversion.
 void launch_f64_to_f32(const GridP &g, const PartF64 &in, const PartF32 &out, long long n, int *err, cudaStream_t s);
 void launch_f32_to_f64(const GridP &g, const PartF32 &in, const PartF64 &out, long long n, cudaStream_t s);

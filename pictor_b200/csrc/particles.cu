@@ -105,8 +105,10 @@ void scan_exclusive_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *t
     uint32_t *sums = tmp;
     uint32_t *rest = tmp + nb + 1;
     k_scan_block<<<(unsigned)nb, kScanBlock, 0, s>>>(in, out, n, sums, nullptr);
+    count_launches(1);
     scan_exclusive_u32(sums, sums, nb, rest, total, s);
     k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, n, sums);
+    count_launches(1);
 }
 
 // ---------------------------------------------------------------------------
@@ -198,9 +200,11 @@ static int radix_sort(SortScratch &sc, const long long *used, int nbits, size_t 
     for (int ps = 0; ps < passes; ps++) {
         const int shift = ps * bits;
         k_radix_hist<<<(unsigned)ntiles, 256, 0, s>>>(sc.key[cur], used, shift, mask, sc.hist, ntiles);
+        count_launches(1);
         scan_exclusive_u32(sc.hist, sc.hist, 256 * ntiles, sc.scan_tmp, nullptr, s);
         k_radix_scatter<<<(unsigned)ntiles, 256, 0, s>>>(sc.key[cur], sc.idx[cur], sc.key[cur ^ 1], sc.idx[cur ^ 1], used,
                                                          shift, mask, sc.hist, ntiles, ps == 0);
+        count_launches(1);
         cur ^= 1;
     }
     return cur;
@@ -318,21 +322,54 @@ void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Co
 {
     cudaMemsetAsync(&cnt->np, 0, sizeof(long long), s);
     k_keys_f64<<<stream_grid(capacity), kThreads, 0, s>>>(g, p, &cnt->used, sc.key[0], &cnt->np, err);
+    count_launches(1);
     const size_t ntiles = sort_tiles(capacity);
     const int r = radix_sort(sc, &cnt->used, key_bits(g.ncell), ntiles, s);
     k_gather_f64<<<stream_grid(capacity), kThreads, 0, s>>>(p, out, sc.idx[r], &cnt->used);
+    count_launches(1);
     k_set_used_np<<<1, 1, 0, s>>>(cnt);
+    count_launches(1);
+}
+
+// First particle of every tile in the sorted keys (lower bound of the tile's
+// first cell); tile ntiles ends at the live count.
+__global__ void k_tile_starts(GridP g, const uint32_t *__restrict__ keys, const Counters *__restrict__ cnt, Tiling t)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q > t.ntiles) return;
+    const long long n = cnt->np;
+    if (q == t.ntiles) {
+        t.tile_start[q] = (uint32_t)n;
+        return;
+    }
+    const int row = q / t.per_row, seg = q % t.per_row;
+    const int j = 3 + row % g.ny, k = g.dims == 3 ? 3 + row / g.ny : 1;
+    const uint32_t first = (uint32_t)cidx(g, 3 + seg * t.width, j, k);
+    long long lo = 0, hi = n;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (keys[mid] < first) lo = mid + 1;
+        else hi = mid;
+    }
+    t.tile_start[q] = (uint32_t)lo;
 }
 
 void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, SortScratch &sc,
-                        long long capacity, cudaStream_t s)
+                        long long capacity, const Tiling *tiles, cudaStream_t s)
 {
     cudaMemsetAsync(&cnt->np, 0, sizeof(long long), s);
     k_keys_f32<<<stream_grid(capacity), kThreads, 0, s>>>(g, p, &cnt->used, sc.key[0], &cnt->np);
+    count_launches(1);
     const size_t ntiles = sort_tiles(capacity);
     const int r = radix_sort(sc, &cnt->used, key_bits(g.ncell), ntiles, s);
     k_gather_f32<<<stream_grid(capacity), kThreads, 0, s>>>(p, out, sc.idx[r], &cnt->used, g.dims == 3);
+    count_launches(1);
     k_set_used_np<<<1, 1, 0, s>>>(cnt);
+    count_launches(1);
+    if (tiles) {
+        k_tile_starts<<<(tiles->ntiles + 1 + 255) / 256, 256, 0, s>>>(g, sc.key[r], cnt, *tiles);
+        count_launches(1);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -497,6 +534,8 @@ void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch 
     if (g.dims == 3) k_exch_scatter<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err);
     else k_exch_scatter<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err);
     k_exch_finish<<<1, 1, 0, s>>>(cnt, total, capacity);
+    count_launches(1);
+    count_launches(2);
 }
 
 // ---------------------------------------------------------------------------
@@ -553,11 +592,13 @@ __global__ void k_f32_to_f64(GridP g, PartF32 in, PartF64 out, long long n)
 void launch_f64_to_f32(const GridP &g, const PartF64 &in, const PartF32 &out, long long n, int *err, cudaStream_t s)
 {
     if (n > 0) k_f64_to_f32<<<stream_grid(n), kThreads, 0, s>>>(g, in, out, n, err);
+    count_launches(n > 0 ? 1 : 0);
 }
 
 void launch_f32_to_f64(const GridP &g, const PartF32 &in, const PartF64 &out, long long n, cudaStream_t s)
 {
     if (n > 0) k_f32_to_f64<<<stream_grid(n), kThreads, 0, s>>>(g, in, out, n);
+    count_launches(n > 0 ? 1 : 0);
 }
 
 // ---------------------------------------------------------------------------
@@ -797,11 +838,14 @@ int launch_weibel(const GridP &g, const WeibelParams &w, const double *X, const 
     if (ntiles > 256 * sc.ntiles) return PIC_ERR_OVERFLOW;
     uint32_t *total = sc.scan_tmp + sc.scan_tmp_len - 1;
     k_weibel_count<<<(unsigned)ntiles, 256, 0, s>>>(w, sc.hist, ntot);
+    count_launches(1);
     scan_exclusive_u32(sc.hist, sc.hist, ntiles, sc.scan_tmp, total, s);
     PartF64 a = p64 ? *p64 : PartF64{};
     PartF32 b = p32 ? *p32 : PartF32{};
     k_weibel_fill<<<(unsigned)ntiles, 256, 0, s>>>(g, w, X, P, nt, a, b, p32 != nullptr, sc.hist, total, ntot, capacity, err);
+    count_launches(1);
     k_weibel_finish<<<1, 1, 0, s>>>(cnt, total, capacity);
+    count_launches(1);
     return PIC_OK;
 }
 

@@ -1,0 +1,239 @@
+! pictor_b200_gpu.F90 -- ISO_C_BINDING shim that lets PICTOR's unchanged
+! MAIN.F90 drive libpictor_b200.so.  Build PICTOR with -Dgpu and this file in
+! place of the CUDA Fortran sources of src/movdep, src/maxwell, src/mem,
+! src/init/initialise_gpu.F90 and src/comm/comm_fld_gpu.F90: it provides the
+! modules MAIN.F90 uses under `#ifdef gpu` (MAIN.F90:20-28) and the
+! argument-less subroutines it calls (MAIN.F90:53-55, 67-69, 91-93, 113-116,
+! 128-130, 161-163, 173-175, 189-191, 223-233, 250-252, 263-265).
+!
+! State stays in the reference's module globals (vars.F90); the library owns
+! the device copies.  Host arrays move only in InitAll_gpu and at output
+! steps (CopyGPUDataToHostForOutput), as in src/mem/particles_gpu.F90:569-581.
+
+module pictor_b200_capi
+   use iso_c_binding
+   implicit none
+
+   integer(c_int), parameter :: PIC_MAX_FLVR = 15
+
+   type, bind(C) :: pic_config
+      integer(c_int32_t) :: nx, ny, nz, dims, geom, fdtd, precision, nflvr
+      real(c_double) :: c, qi, bext(3), qm(0:PIC_MAX_FLVR)
+      integer(c_int32_t) :: reorder_period, curr_filter
+      integer(c_int64_t) :: capacity
+      real(c_double) :: rmin
+      integer(c_int32_t) :: inc_axis, reserved(7)
+   end type pic_config
+
+   interface
+      integer(c_int) function pic_create(cfg, h) bind(C, name="pic_create")
+         import :: c_int, c_ptr, pic_config
+         type(pic_config), intent(in) :: cfg
+         type(c_ptr), intent(out) :: h
+      end function
+      subroutine pic_destroy(h) bind(C, name="pic_destroy")
+         import :: c_ptr
+         type(c_ptr), value :: h
+      end subroutine
+      integer(c_int) function pic_load_fields(h, ex, ey, ez, bx, by, bz) bind(C, name="pic_load_fields")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: h
+         real(c_double), intent(in) :: ex(*), ey(*), ez(*), bx(*), by(*), bz(*)
+      end function
+      integer(c_int) function pic_fetch_fields(h, ex, ey, ez, bx, by, bz, jx, jy, jz) bind(C, name="pic_fetch_fields")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: h
+         real(c_double), intent(out) :: ex(*), ey(*), ez(*), bx(*), by(*), bz(*), jx(*), jy(*), jz(*)
+      end function
+      integer(c_int) function pic_load_particles(h, n, q, x, y, z, u, v, w, flv) bind(C, name="pic_load_particles")
+         import :: c_int, c_ptr, c_double, c_int64_t, c_int32_t
+         type(c_ptr), value :: h
+         integer(c_int64_t), value :: n
+         real(c_double), intent(in) :: q(*), x(*), y(*), z(*), u(*), v(*), w(*)
+         integer(c_int32_t), intent(in) :: flv(*)
+      end function
+      integer(c_int) function pic_fetch_particles(h, n, q, x, y, z, u, v, w, flv) bind(C, name="pic_fetch_particles")
+         import :: c_int, c_ptr, c_double, c_int64_t, c_int32_t
+         type(c_ptr), value :: h
+         integer(c_int64_t), intent(out) :: n
+         real(c_double), intent(out) :: q(*), x(*), y(*), z(*), u(*), v(*), w(*)
+         integer(c_int32_t), intent(out) :: flv(*)
+      end function
+      integer(c_int) function pic_particle_count(h, n) bind(C, name="pic_particle_count")
+         import :: c_int, c_ptr, c_int64_t
+         type(c_ptr), value :: h
+         integer(c_int64_t), intent(out) :: n
+      end function
+   end interface
+
+   ! the phase entry points share one signature: int f(pic_handle*)
+   interface
+      integer(c_int) function pic_update_b_half(h) bind(C, name="pic_update_b_half")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_move_deposit(h) bind(C, name="pic_move_deposit")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_exchange_particles(h) bind(C, name="pic_exchange_particles")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_update_e(h) bind(C, name="pic_update_e")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_fold_current(h) bind(C, name="pic_fold_current")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_filter_current(h) bind(C, name="pic_filter_current")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_add_current(h) bind(C, name="pic_add_current")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_reset_current(h) bind(C, name="pic_reset_current")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_reorder(h) bind(C, name="pic_reorder")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+   end interface
+
+   type(c_ptr), save :: pic_h = c_null_ptr
+
+contains
+
+   subroutine pic_check(code)
+      use communication, only: Abort   ! communication.F90:96-102
+      integer(c_int), intent(in) :: code
+      if (code .ne. 0) call Abort(int(100 - code))
+   end subroutine pic_check
+
+end module pictor_b200_capi
+
+! ---------------------------------------------------------------------------
+! Modules named as MAIN.F90 uses them under #ifdef gpu.
+! ---------------------------------------------------------------------------
+module var_gpu
+   use pictor_b200_capi
+end module var_gpu
+
+module initialise_gpu
+   use parameters
+   use vars
+   use pictor_b200_capi
+   implicit none
+contains
+   subroutine InitAll_gpu   ! replaces src/init/initialise_gpu.F90:9
+      type(pic_config) :: cfg
+      integer :: n
+      cfg%nx = mx - 5; cfg%ny = my - 5; cfg%nz = max(mz - 5, 1)
+#ifdef twoD
+      cfg%dims = 2
+#else
+      cfg%dims = 3
+#endif
+#ifdef cyl
+      cfg%geom = 1
+#else
+      cfg%geom = 0
+#endif
+#ifdef Lehe
+      cfg%fdtd = 1
+#else
+      cfg%fdtd = 0
+#endif
+      cfg%precision = 0
+      cfg%nflvr = Nflvr
+      cfg%c = c; cfg%qi = qi
+      cfg%bext = (/ Bx_ext0, By_ext0, Bz_ext0 /)
+      cfg%qm = 0
+      do n = 1, Nflvr
+         cfg%qm(n) = flvrqm(n)
+      end do
+      cfg%reorder_period = prtl_reorder_period
+      cfg%curr_filter = curr_filter
+      cfg%capacity = gpu_prtl_arr_size
+      cfg%rmin = 0; cfg%inc_axis = 1; cfg%reserved = 0
+      call pic_check(pic_create(cfg, pic_h))
+      call pic_check(pic_load_fields(pic_h, Ex, Ey, Ez, Bx, By, Bz))
+      call pic_check(pic_load_particles(pic_h, int(used_prtl_arr_size, c_int64_t), qp, xp, yp, zp, up, vp, wp, flvp))
+   end subroutine InitAll_gpu
+end module initialise_gpu
+
+module em_update_gpu
+   use pictor_b200_capi
+   implicit none
+contains
+   subroutine UpdateBfieldHalfGPU      ! em_update_gpu.F90:44 (+ halo)
+      call pic_check(pic_update_b_half(pic_h))
+   end subroutine
+   subroutine UpdateEfieldGPU          ! em_update_gpu.F90:12 (+ halo)
+      call pic_check(pic_update_e(pic_h))
+   end subroutine
+   subroutine AddCurrentGPU            ! em_update_gpu.F90:92 (+ halo)
+      call pic_check(pic_add_current(pic_h))
+   end subroutine
+end module em_update_gpu
+
+module movdep_gpu
+   use pictor_b200_capi
+   implicit none
+contains
+   subroutine MoveDepositPrtlGPU       ! movdep_gpu.F90:14
+      call pic_check(pic_move_deposit(pic_h))
+   end subroutine
+end module movdep_gpu
+
+module particles_gpu
+   use vars
+   use pictor_b200_capi
+   implicit none
+contains
+   subroutine ExchangePrtlGPU          ! LoadPrtlOutliers + AppendParticles on one periodic rank
+      call pic_check(pic_exchange_particles(pic_h))
+   end subroutine
+   subroutine ReorderPrtlGPU           ! particles_gpu.F90:416
+      if (modulo(t, prtl_reorder_period) .eq. 0) call pic_check(pic_reorder(pic_h))
+   end subroutine
+   subroutine CopyGPUDataToHostForOutput   ! particles_gpu.F90:569
+      integer(c_int64_t) :: n
+      call pic_check(pic_particle_count(pic_h, n))
+      if (n .gt. size(xp)) call ReshapePrtlArr(int(n) + 1000000)
+      call pic_check(pic_fetch_particles(pic_h, n, qp, xp, yp, zp, up, vp, wp, flvp))
+      used_prtl_arr_size = int(n)
+      call pic_check(pic_fetch_fields(pic_h, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz))
+   end subroutine
+   subroutine FinishSaveDataGPU
+   end subroutine
+end module particles_gpu
+
+module fields_gpu
+   use pictor_b200_capi
+   implicit none
+contains
+   subroutine ResetCurrentGPU          ! fields_gpu.F90:61
+      call pic_check(pic_reset_current(pic_h))
+   end subroutine
+   subroutine smoothen_current_gpu     ! fields_gpu.F90:120 (filter on the device)
+      call pic_check(pic_filter_current(pic_h))
+   end subroutine
+end module fields_gpu
+
+module comm_fld_gpu
+   use pictor_b200_capi
+   implicit none
+contains
+   subroutine UpdateCurrentsAllEdgesGPU    ! ghost current fold on one periodic rank
+      call pic_check(pic_fold_current(pic_h))
+   end subroutine
+   subroutine EMfldExchangeGPU             ! halo: done inside every field update
+   end subroutine
+end module comm_fld_gpu

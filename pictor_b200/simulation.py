@@ -247,6 +247,25 @@ class Simulation:
         return {"B2": out[0], "E2": out[1], "Benergy": 0.5 * out[0], "Eenergy": 0.5 * out[1],
                 "gauss_linf": out[2], "rho_max": out[3], "kinetic": out[4:].copy()}
 
+    def profile(self, enable: bool = True) -> None:
+        check(self.L.pic_profile(self.h, 1 if enable else 0), "pic_profile")
+
+    def phase_times(self) -> dict:
+        """Summed device milliseconds and kernel launches per phase of the
+        profiled pic_step calls (resets the accumulators)."""
+        n = len(_capi.PHASES)
+        ms = np.zeros(n)
+        launches = np.zeros(n, dtype=np.int64)
+        steps = C.c_int64()
+        check(self.L.pic_phase_times(self.h, dptr(ms), launches.ctypes.data_as(_capi.PI64), n, C.byref(steps)),
+              "pic_phase_times")
+        return {"steps": steps.value, "ms": dict(zip(_capi.PHASES, ms)), "launches": dict(zip(_capi.PHASES, launches))}
+
+    def launch_count(self) -> int:
+        n = C.c_int64()
+        check(self.L.pic_launch_count(self.h, C.byref(n)), "pic_launch_count")
+        return n.value
+
     def device_errors(self) -> int:
         b = C.c_int32()
         check(self.L.pic_device_errors(self.h, C.byref(b)), "pic_device_errors")

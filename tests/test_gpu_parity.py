@@ -176,3 +176,86 @@ def test_diagnostics_match_oracle():
         np.testing.assert_allclose([d["B2"], d["E2"]], [eb, ee], rtol=1e-9)
         res, rmax = o.gauss_residual()
         assert d["gauss_linf"] <= 1e-12 * rmax and res <= 1e-12 * rmax
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_current_filter_bit_exact(dims):
+    """smoothen_current (current.F90:19-163): two passes of the (1/4,1/2,1/4)
+    filter on a folded current; interior bit-exact, then a filtered full step."""
+    g, cfg = grid_and_config(dims=dims, curr_filter=2)
+    rng = np.random.default_rng(8)
+    J = [np.asfortranarray(rng.normal(scale=1e-3, size=O.grid_shape(g))) for _ in range(3)]
+    o = O.Oracle(g, O.Particles(1))
+    o.f.Jx[...], o.f.Jy[...], o.f.Jz[...] = J
+    with _sim(cfg) as s:
+        s.load_current(*J)
+        o.fold_current(); s.fold_current()
+        o.filter_current(2); s.filter_current()
+        gf = s.fetch_fields()
+        for n in ("Jx", "Jy", "Jz"):
+            assert np.array_equal(interior(getattr(gf, n), g), interior(getattr(o.f, n), g)), n
+
+
+def test_filtered_step_matches_oracle():
+    g, cfg = grid_and_config(dims=2, nx=24, ny=20, curr_filter=1, qi=0.00158203125, reorder_period=5)
+    p = O.load_weibel(2, 24, 20, epc=8, drift=0.5, temp=0.005, seed=5)
+    o = O.Oracle(g, p.copy())
+    with _sim(cfg) as s:
+        s.load_particles(to_gpu_particles(p))
+        o.step_filtered(1, 5, 1); s.step(1)
+        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+        for t in range(2, 8):
+            o.step_filtered(t, 5, 1); s.step(1)
+        gf = s.fetch_fields(with_current=False)
+        for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+            a, b = getattr(gf, n), getattr(o.f, n)
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * max(np.abs(b).max(), 1e-30), err_msg=n)
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_fp32_tiled_mover_matches_global_mover(dims):
+    """The tiled FP32 mover (shared-memory fields and current per tile) and the
+    per-particle FP32 mover give the same particles and the same current up to
+    the FP32 rounding of the summation order."""
+    nx, ny, nz = (48, 40, 1) if dims == 2 else (24, 16, 12)
+    g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, precision="fp32", qi=0.00158203125, capacity=1 << 18)
+    f = random_fields(g, seed=41, scale=0.02)
+    with _sim(cfg) as s:
+        s.init_weibel(8, 0.5, 0.4, 0.005, 0.005, 9)
+        s.reorder()                       # tiles valid -> tiled mover
+        sorted_p = s.fetch_particles()
+        s.load_fields(to_gpu_fields(f))
+        s.move_deposit()
+        a_p, a_f = s.fetch_particles(), s.fetch_fields()
+        s.load_particles(sorted_p)        # same state, tiles invalid -> per-particle mover
+        s.load_fields(to_gpu_fields(f))
+        s.move_deposit()
+        b_p, b_f = s.fetch_particles(), s.fetch_fields()
+    for k in ("x", "y", "z", "u", "v", "w"):
+        np.testing.assert_array_equal(getattr(a_p, k), getattr(b_p, k), err_msg=k)
+    for n in ("Jx", "Jy", "Jz"):
+        a, b = getattr(a_f, n), getattr(b_f, n)
+        np.testing.assert_allclose(a, b, rtol=0, atol=2e-6 * np.abs(b).max(), err_msg=n)
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_fp32_form_tracks_fp64(dims):
+    """FP32 cell-relative run vs the FP64 reference form from the same seed:
+    energies agree to the stated tolerance after 30 steps."""
+    nx, ny, nz = (64, 64, 1) if dims == 2 else (24, 24, 24)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, precision=prec, qi=0.00158203125, capacity=1 << 19)
+        with _sim(cfg) as s:
+            s.init_weibel(16 if dims == 2 else 4, 0.5, 0.5, 0.005, 0.005, 2930)
+            s.reorder()
+            s.step(30)
+            d = s.diagnostics(0.00158203125)
+            res[prec] = d
+    a, b = res["fp32"], res["fp64"]
+    tot32 = 0.5 * (a["B2"] + a["E2"]) + a["kinetic"].sum()
+    tot64 = 0.5 * (b["B2"] + b["E2"]) + b["kinetic"].sum()
+    assert abs(tot32 - tot64) <= 1e-5 * abs(tot64)
+    fe32, fe64 = a["B2"] + a["E2"], b["B2"] + b["E2"]
+    assert abs(fe32 - fe64) <= 1e-2 * fe64
+    assert a["gauss_linf"] <= (1e-4 if dims == 2 else 2e-2) * a["rho_max"]
