@@ -134,7 +134,7 @@ int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout);
 
 /* Device error word accumulated by the kernels since the last call (bit set of
    PIC_DEVERR_*); cleared by the call. */
-enum { PIC_DEVERR_RANGE = 1, PIC_DEVERR_OVERFLOW = 2, PIC_DEVERR_NAN = 4 };
+enum { PIC_DEVERR_RANGE = 1, PIC_DEVERR_OVERFLOW = 2, PIC_DEVERR_NAN = 4, PIC_DEVERR_SUBSTEP = 8 };
 int pic_device_errors(pic_handle *h, int32_t *bits);
 
 /* Phases of pic_step, in step order. */

@@ -103,6 +103,19 @@ def _declare(L: C.CDLL) -> None:
     L.orc_load_weibel.argtypes = [P(_Weibel), P(_Particles)]
     L.orc_load_weibel.restype = C.c_int64
     L.orc_maxbolt_table.argtypes = [C.c_int, P(C.c_double), P(C.c_double)]
+    for fn in ("orc_cyl_update_b_half", "orc_cyl_update_e", "orc_cyl_add_current"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Fields)]
+    L.orc_cyl_params.argtypes = [P(Grid), P(C.c_double)]
+    L.orc_cyl_send_recv_flds.argtypes = [P(Grid)] + [P(C.c_double)] * 3
+    L.orc_cyl_fold.argtypes = [P(Grid)] + [P(C.c_double)] * 3
+    L.orc_cyl_move_deposit.argtypes = [P(Grid), P(_Particles), P(_Fields)]
+    L.orc_cyl_exchange.argtypes = [P(Grid), P(_Particles)]
+    L.orc_cyl_exchange.restype = C.c_int
+    L.orc_cyl_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
+    L.orc_cyl_step.restype = C.c_int
+    L.orc_cyl_load_uniform.argtypes = [P(Grid), C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       C.c_uint32, P(_Particles)]
+    L.orc_cyl_load_uniform.restype = C.c_int64
 
 
 def _dp(a: np.ndarray):
@@ -264,6 +277,56 @@ class Oracle:
         ps = self.p.struct()
         r = self.L.orc_gauss_residual(C.byref(self.g), C.byref(fs), C.byref(ps), C.byref(rm))
         return r, rm.value
+
+
+class CylOracle(Oracle):
+    """The cylindrical (r, theta, z) restatement: same state, cylindrical phases."""
+
+    def update_b_half(self):
+        fs = self.f.struct()
+        self.L.orc_cyl_update_b_half(C.byref(self.g), C.byref(fs))
+
+    def update_e(self):
+        fs = self.f.struct()
+        self.L.orc_cyl_update_e(C.byref(self.g), C.byref(fs))
+
+    def add_current(self):
+        fs = self.f.struct()
+        self.L.orc_cyl_add_current(C.byref(self.g), C.byref(fs))
+
+    def send_recv_flds(self, which: str):
+        a = [getattr(self.f, which + c) for c in "xyz"]
+        self.L.orc_cyl_send_recv_flds(C.byref(self.g), *[_dp(x) for x in a])
+
+    def fold_current(self):
+        self.L.orc_cyl_fold(C.byref(self.g), _dp(self.f.Jx), _dp(self.f.Jy), _dp(self.f.Jz))
+
+    def move_deposit(self):
+        fs = self.f.struct()
+        self._call_p(self.L.orc_cyl_move_deposit, C.byref(fs))
+
+    def exchange_particles(self) -> int:
+        return self._call_p(self.L.orc_cyl_exchange)
+
+    def step(self, t: int, reorder_period: int = 20) -> int:
+        fs = self.f.struct()
+        return self._call_p(self.L.orc_cyl_step, C.byref(fs), int(t), int(reorder_period))
+
+    def params(self):
+        out = (C.c_double * 4)()
+        self.L.orc_cyl_params(C.byref(self.g), out)
+        return {"dtheta": out[0], "ax_perm_area": out[1], "inv_dtheta": out[2], "rshift": out[3]}
+
+
+def cyl_load_uniform(g: Grid, npx: int, npy: int, npz: int, density: float, temp: float, charge: float, flv: int,
+                     seed: int, capacity: int) -> Particles:
+    p = Particles(capacity)
+    ps = p.struct()
+    n = lib().orc_cyl_load_uniform(C.byref(g), npx, npy, npz, density, temp, charge, flv, seed, C.byref(ps))
+    if n < 0:
+        raise RuntimeError("capacity exceeded")
+    p.used = ps.used
+    return p
 
 
 def lehe_coefficients(g: Grid) -> np.ndarray:

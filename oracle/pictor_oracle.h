@@ -125,6 +125,23 @@ int64_t orc_load_weibel(const orc_weibel *w, orc_particles *p);
 /* The Maxwell-Boltzmann inverse-CDF tables of prob_dist.F90:34-54 (N=10000). */
 void orc_maxbolt_table(int n, double *x_table, double *pdf_table);
 
+/* ---- cylindrical (r, theta, z), pictor_oracle_cyl.c ---------------------
+   x = r (axis at x = 3.5), y = theta (ny cells over 2 pi), z; 3D only.
+   fdtd selects the B update: 0 = cyl_em_update.F90, 1 = cyl_em_update_lehe.F90. */
+void orc_cyl_params(const orc_grid *g, double out[4]);    /* dtheta, ax_perm_area, 1/dtheta, rshift */
+void orc_cyl_update_b_half(const orc_grid *g, orc_fields *f);
+void orc_cyl_update_e(const orc_grid *g, orc_fields *f);
+void orc_cyl_add_current(const orc_grid *g, orc_fields *f);
+void orc_cyl_send_recv_flds(const orc_grid *g, double *Fx, double *Fy, double *Fz);
+void orc_cyl_fold(const orc_grid *g, double *Jx, double *Jy, double *Jz);
+void orc_cyl_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f);
+int orc_cyl_exchange(const orc_grid *g, orc_particles *p);
+int orc_cyl_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period);
+int64_t orc_cyl_load_uniform(const orc_grid *g, int npx, int npy, int npz, double density, double temp, double charge,
+                             int flv, uint32_t seed, orc_particles *p);
+extern int orc_cyl_max_substeps;
+extern int64_t orc_cyl_substep_overruns;
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,28 @@ void lehe_coefficients(int dims, double c, double *o)
     o[9] = dxl; o[10] = dyl; o[11] = dzl;
 }
 
+// Lehe coefficients of cyl_em_update_lehe.F90:6-17 (grid_dx = dz = 1,
+// dtheta = 2 pi/ny): the extended stencil acts along z.
+void cyl_lehe_coefficients(double c, int ny, double *o)
+{
+    const double pi = 3.14159265358979323846264;
+    const double dtheta = 2.0 * pi / ny;
+    const double cinv = 1.0 / c;
+    o[3] = 0.0;
+    o[4] = 0.125;
+    o[5] = 0.0;
+    o[6] = 0.125;
+    o[7] = 0.125 * ((1.0 / 1.0) * (1.0 / 1.0));
+    o[8] = 0.125 * ((1.0 / (1.0 * dtheta)) * (1.0 / (1.0 * dtheta)));
+    o[9] = 0.0;
+    o[10] = 0.0;
+    const double s = std::sin((0.5 * pi) * c);
+    o[11] = 0.25 * (1.0 - (cinv * cinv) * (s * s));
+    o[0] = ((1.0 - 2.0 * o[3]) - 2.0 * o[4]) - 3.0 * o[9];
+    o[1] = ((1.0 - 2.0 * o[5]) - 2.0 * o[6]) - 3.0 * o[10];
+    o[2] = ((1.0 - 2.0 * o[7]) - 2.0 * o[8]) - 3.0 * o[11];
+}
+
 // Init_MaxBolt_Table, prob_dist.F90:34-54.
 void maxbolt_table(int n, std::vector<double> &X, std::vector<double> &P)
 {
@@ -126,6 +148,7 @@ int check_device_errors(pic_handle *h)
     if (bits & PIC_DEVERR_OVERFLOW) return PIC_ERR_OVERFLOW;
     if (bits & PIC_DEVERR_RANGE) return PIC_ERR_RANGE;
     if (bits & PIC_DEVERR_NAN) return PIC_ERR_NAN;
+    if (bits & PIC_DEVERR_SUBSTEP) return PIC_ERR_TIMEOUT;
     return PIC_OK;
 }
 
@@ -155,6 +178,33 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
     const GridP &g = h->g;
     const bool filt = h->cfg.curr_filter > 0;
     g_launches = 0;
+    if (g.geom == PIC_GEOM_CYLINDRICAL) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        switch (phase) {
+            case PIC_PHASE_BHALF1:  // cyl_em_update.F90:49-110 + halo
+            case PIC_PHASE_BHALF2:
+                launch_cyl_bhalf(g, E, B, h->s);
+                break;
+            case PIC_PHASE_MOVE:  // cyl_movdep_strang.F90:14-378
+                launch_cyl_move_deposit(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);
+                break;
+            case PIC_PHASE_EXCHANGE:
+                launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s);
+                break;
+            case PIC_PHASE_EFIELD:  // UpdateEfield, halo, fold, AddCurrent, halo, ResetCurrent
+                launch_cyl_efield(g, 0, E, B, J, h->s);
+                launch_cyl_fold(g, J, h->s);
+                launch_cyl_efield(g, 2, E, B, J, h->s);
+                for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(double), h->s);
+                break;
+            case PIC_PHASE_REORDER:
+                if (reorder)
+                    launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+                break;
+        }
+        return (int)g_launches;
+    }
     if (!h->fp32) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -382,7 +432,12 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     *out = nullptr;
     const pic_config &c = *cfg;
     if (c.dims != 2 && c.dims != 3) return PIC_ERR_INVALID;
-    if (c.geom != PIC_GEOM_CARTESIAN) return PIC_ERR_INVALID;
+    if (c.geom != PIC_GEOM_CARTESIAN && c.geom != PIC_GEOM_CYLINDRICAL) return PIC_ERR_INVALID;
+    // the cylindrical step exists in the reference's FP64 form, 3D, with the
+    // axis on this rank and no current filter
+    if (c.geom == PIC_GEOM_CYLINDRICAL &&
+        (c.dims != 3 || c.precision != PIC_PREC_FP64 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
+        return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
@@ -421,7 +476,10 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     g.cinv = 1.0 / c.c;        // vars.F90:222
     g.qi = c.qi;
     for (int d = 0; d < 3; d++) g.bext[d] = c.bext[d];
-    lehe_coefficients(c.dims, c.c, g.lehe);
+    if (c.geom == PIC_GEOM_CYLINDRICAL) cyl_lehe_coefficients(c.c, c.ny, g.lehe);
+    else lehe_coefficients(c.dims, c.c, g.lehe);
+    g.geom = c.geom;
+    g.closed_x = c.geom == PIC_GEOM_CYLINDRICAL;
     g.qm[0] = 0.0;
     for (int f = 1; f <= PIC_MAX_FLVR; f++) g.qm[f] = f <= c.nflvr ? c.qm[f] : 0.0;
     // subdomains.F90:52-67
@@ -678,7 +736,11 @@ int pic_init_weibel(pic_handle *h, double epc, double density, double drift, dou
 int pic_update_b_half(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->fp32) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_bhalf(h->g, E, B, h->s);
+    } else if (h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_bhalf<float>(h->g, E, B, h->s);
@@ -701,10 +763,18 @@ int pic_move_deposit(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
-    if (h->fp32) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_move_deposit(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s);
+    } else if (h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
+        if (h->sorted)
+            launch_move_deposit_f32_tiled(h->g, h->p32[h->cur], h->tiles.tile_start, h->tiles.ntiles, E, B, J, h->err,
+                                          h->s);
+        else
+            launch_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
     } else {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -723,7 +793,11 @@ int pic_exchange_particles(pic_handle *h)
 int pic_update_e(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->fp32) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_efield(h->g, 0, E, B, J, h->s);
+    } else if (h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_efield<float>(h->g, 0, E, B, J, h->s);
@@ -738,7 +812,11 @@ int pic_update_e(pic_handle *h)
 int pic_fold_current(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->fp32) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_fold(h->g, J, h->s);
+    } else if (h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_fold<float>(h->g, J, h->s);
@@ -752,7 +830,7 @@ int pic_fold_current(pic_handle *h)
 
 int pic_filter_current(pic_handle *h)
 {
-    if (!h) return PIC_ERR_INVALID;
+    if (!h || h->g.geom == PIC_GEOM_CYLINDRICAL) return PIC_ERR_INVALID;
     if (!h->Jtmp) {
         int r = dalloc(h, (char **)&h->Jtmp, field_bytes(h));
         if (r) return r;
@@ -774,7 +852,11 @@ int pic_filter_current(pic_handle *h)
 int pic_add_current(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->fp32) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_efield(h->g, 2, E, B, J, h->s);
+    } else if (h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_efield<float>(h->g, 2, E, B, J, h->s);

@@ -29,6 +29,8 @@ struct GridP {
     double qm[PIC_MAX_FLVR + 1];      // flvrqm (index 0 = hole -> 0)
     // particle bounds (subdomains.F90:52-67)
     double xmin, xmax, ymin, ymax, zmin, zmax, xlen, ylen, zlen;
+    int geom;                         // PIC_GEOM_*
+    int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
 };
 
 __host__ __device__ inline long long cidx(const GridP &g, int i, int j, int k)

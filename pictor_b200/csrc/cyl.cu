@@ -1,0 +1,537 @@
+// cyl.cu -- the cylindrical (r, theta, z) step in the reference's FP64 form.
+//
+// Reference: src/cyl/cyl_common.F90:19-32 (dtheta = 2 pi/ny, ax_perm_area =
+// 4/ny, rshift = -0.5), cyl_em_update.F90 (Yee with 1/r metrics, axis
+// treatment), cyl_em_update_lehe.F90 (Lehe, restated with its syntax fixed),
+// cyl_movdep_strang.F90 (Strang-split mover with a local Cartesian move,
+// adaptive near-axis sub-stepping, AxisCurrentBC), deposit.F90 (the scalar
+// deposit the sub-stepper uses).
+//
+// Set-up: the rank holds the axis (x = 3.5 is r = 0); theta (y) and z are
+// periodic, r is not (no halo or fold across the r faces, particles leaving at
+// r_max are dropped).  With the axis included the reference exchanges the y
+// faces before the z faces (indepLBaxis = 2), with the y faces over all x and
+// the interior z only.  Every kernel keeps the reference's loop ranges and
+// operation order; the file is compiled without FMA contraction, so fields,
+// momenta and positions equal the serial CPU build bit for bit.
+#include "common.cuh"
+#include "kernels.cuh"
+#include "particle_math.cuh"
+
+namespace pic {
+
+struct CylP {
+    double dtheta, ax_perm_area, inv_dtheta, rmin;
+};
+
+__device__ __forceinline__ double ldd(const double *p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// Fields
+// ---------------------------------------------------------------------------
+
+// Lehe directional differences of cyl_em_update_lehe.F90:255-289.
+__device__ __forceinline__ double lgx(const GridP &g, const double *F, long long c0)
+{
+    double r = g.lehe[0] * (ldd(F + c0 + 1) - ldd(F + c0));
+    r = r + g.lehe[4] * (ldd(F + c0 + 1 + g.sz) - ldd(F + c0 + g.sz));
+    r = r + g.lehe[4] * (ldd(F + c0 + 1 - g.sz) - ldd(F + c0 - g.sz));
+    return r;
+}
+__device__ __forceinline__ double lgx1(const GridP &g, const double *F, long long c0, double rp, double rr)
+{
+    double r = g.lehe[0] * (rp * ldd(F + c0 + 1) - rr * ldd(F + c0));
+    r = r + g.lehe[4] * (rp * ldd(F + c0 + 1 + g.sz) - rr * ldd(F + c0 + g.sz));
+    r = r + g.lehe[4] * (rp * ldd(F + c0 + 1 - g.sz) - rr * ldd(F + c0 - g.sz));
+    return r;
+}
+__device__ __forceinline__ double lgy(const GridP &g, const double *F, long long c0)
+{
+    double r = (g.lehe[1] * 1.0) * (ldd(F + c0 + g.sy) - ldd(F + c0));
+    r = r + (g.lehe[6] * 1.0) * (ldd(F + c0 + g.sy + g.sz) - ldd(F + c0 + g.sz));
+    r = r + (g.lehe[6] * 1.0) * (ldd(F + c0 + g.sy - g.sz) - ldd(F + c0 - g.sz));
+    return r;
+}
+__device__ __forceinline__ double lgz(const GridP &g, const double *F, long long c0)
+{
+    const long long sy = g.sy, sz = g.sz;
+    double r = g.lehe[2] * (ldd(F + c0 + sz) - ldd(F + c0));
+    r = r + g.lehe[7] * (ldd(F + c0 + 1 + sz) - ldd(F + c0 + 1));
+    r = r + g.lehe[7] * (ldd(F + c0 - 1 + sz) - ldd(F + c0 - 1));
+    r = r + g.lehe[8] * (ldd(F + c0 + sy + sz) - ldd(F + c0 + sy));
+    r = r + g.lehe[8] * (ldd(F + c0 - sy + sz) - ldd(F + c0 - sy));
+    r = r + g.lehe[11] * (ldd(F + c0 + 2 * sz) - ldd(F + c0 - sz));
+    return r;
+}
+
+// UpdateBfieldHalf main loop (cyl_em_update.F90:66-83): i 4..mx-1, j 1..my-1,
+// k 1..mz-1 (Lehe: k 2..mz-2, see the oracle for why).
+template <int FDTD>
+__global__ void k_cyl_bhalf(GridP g, CylP cp, const double *__restrict__ Ex, const double *__restrict__ Ey,
+                            const double *__restrict__ Ez, double *Bx, double *By, double *Bz)
+{
+    const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = (FDTD == PIC_FDTD_LEHE ? 2 : 1) + blockIdx.z;
+    if (i > g.mx - 1 || j > g.my - 1) return;
+    const double h = g.h, dtheta = cp.dtheta;
+    const double r = (((double)i - 3.0) + cp.rmin) * 1.0;
+    const double rp_half = r + 0.5 * 1.0, rp = r + 1.0;
+    const long long c0 = cidx(g, i, j, k);
+    const long long sy = g.sy, sz = g.sz;
+    if (FDTD == PIC_FDTD_YEE) {
+        Bx[c0] = (Bx[c0] - (h * (ldd(Ez + c0 + sy) - ldd(Ez + c0))) / (r * dtheta)) + (h * 1.0) * (ldd(Ey + c0 + sz) - ldd(Ey + c0));
+        By[c0] = (By[c0] - (h * 1.0) * (ldd(Ex + c0 + sz) - ldd(Ex + c0))) + (h * 1.0) * (ldd(Ez + c0 + 1) - ldd(Ez + c0));
+        Bz[c0] = Bz[c0] - (h * ((1.0 * (rp * ldd(Ey + c0 + 1) - r * ldd(Ey + c0))) - (ldd(Ex + c0 + sy) - ldd(Ex + c0)) / dtheta)) / rp_half;
+    } else {
+        Bx[c0] = (Bx[c0] - (h * lgy(g, Ez, c0)) / (r * dtheta)) + (h * 1.0) * lgz(g, Ey, c0);
+        By[c0] = (By[c0] - (h * 1.0) * lgz(g, Ex, c0)) + (h * 1.0) * lgx(g, Ez, c0);
+        Bz[c0] = Bz[c0] - (h * ((1.0 * lgx1(g, Ey, c0, rp, r)) - lgy(g, Ex, c0) / dtheta)) / rp_half;
+    }
+}
+
+// UpdateBzAxis (cyl_em_update.F90:231-246) + Bz(3,j,k) = Bz_ax(k): one
+// thread per k sums Ey(4,j,k) over j in the reference's order.
+__global__ void k_cyl_bz_axis(GridP g, CylP cp, const double *__restrict__ Ey, double *Bz)
+{
+    const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (k > g.mz - 1) return;
+    const double hax = g.h * cp.ax_perm_area;
+    double s = 0.0;
+    for (int j = 3; j <= g.my - 3; j++) s = s - hax * Ey[cidx(g, 4, j, k)];
+    const double v = Bz[cidx(g, 3, 3, k)] + s;
+    for (int j = 1; j <= g.my - 1; j++) Bz[cidx(g, 3, j, k)] = v;
+}
+
+__device__ __forceinline__ int axis_partner(const GridP &g, int j)
+{
+    int p = j + g.ny / 2;
+    if (p > g.my - 3) p -= g.ny;
+    return p;
+}
+
+// UpdateBFldAxis (cyl_em_update.F90:187-227), all j, k.
+__global__ void k_cyl_b_axis(GridP g, double *Bx, double *By, double *Bz)
+{
+    const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y;
+    if (j > g.my) return;
+    const int jpp = axis_partner(g, j);
+    By[cidx(g, 3, j, k)] = 0.5 * (By[cidx(g, 4, j, k)] - By[cidx(g, 4, jpp, k)]);
+    By[cidx(g, 2, j, k)] = -By[cidx(g, 4, jpp, k)];
+    Bx[cidx(g, 3, j, k)] = -Bx[cidx(g, 4, jpp, k)];
+    Bz[cidx(g, 2, j, k)] = Bz[cidx(g, 4, jpp, k)];
+}
+
+// UpdateEFldAxis (cyl_em_update.F90:143-185), all j, k.
+__global__ void k_cyl_e_axis(GridP g, double *Ex, double *Ey, double *Ez)
+{
+    const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y;
+    if (j > g.my) return;
+    const int jpp = axis_partner(g, j);
+    Ex[cidx(g, 3, j, k)] = 0.5 * (Ex[cidx(g, 4, j, k)] - Ex[cidx(g, 4, jpp, k)]);
+    Ex[cidx(g, 2, j, k)] = -Ex[cidx(g, 4, jpp, k)];
+    Ey[cidx(g, 3, j, k)] = -Ey[cidx(g, 4, jpp, k)];
+    Ez[cidx(g, 3, j, k)] = Ez[cidx(g, 4, jpp, k)];
+}
+
+// UpdateEfield (MODE 0, cyl_em_update.F90:24-41) or AddCurrent (MODE 2,
+// :128-137): i 4..mx-3, j, k 3..m-3.
+template <int MODE>
+__global__ void k_cyl_e(GridP g, CylP cp, double *Ex, double *Ey, double *Ez, const double *__restrict__ Bx,
+                        const double *__restrict__ By, const double *__restrict__ Bz, const double *__restrict__ Jx,
+                        const double *__restrict__ Jy, const double *__restrict__ Jz)
+{
+    const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = 3 + blockIdx.z;
+    if (i > g.mx - 3 || j > g.my - 3) return;
+    const double dtheta = cp.dtheta;
+    const double r = (((double)i - 3.0) + cp.rmin) * 1.0;
+    const double rp_half = r + 0.5 * 1.0, rm_half = r - 0.5 * 1.0;
+    const long long c0 = cidx(g, i, j, k);
+    if (MODE == 0) {
+        const double fc = g.fc;
+        Ex[c0] = (Ex[c0] + (fc * (ldd(Bz + c0) - ldd(Bz + c0 - g.sy))) / (rp_half * dtheta)) - (fc * 1.0) * (ldd(By + c0) - ldd(By + c0 - g.sz));
+        Ey[c0] = (Ey[c0] + (fc * 1.0) * (ldd(Bx + c0) - ldd(Bx + c0 - g.sz))) - (fc * 1.0) * (ldd(Bz + c0) - ldd(Bz + c0 - 1));
+        Ez[c0] = (Ez[c0] + ((fc * 1.0) * (rp_half * ldd(By + c0) - rm_half * ldd(By + c0 - 1))) / r) - (fc * (ldd(Bx + c0) - ldd(Bx + c0 - g.sy))) / (r * dtheta);
+    } else {
+        Ex[c0] = Ex[c0] - (ldd(Jx + c0) * 1.0) / (rp_half * dtheta);
+        Ey[c0] = Ey[c0] - (ldd(Jy + c0) * 1.0) * 1.0;
+        Ez[c0] = Ez[c0] - (ldd(Jz + c0) * 1.0) / (r * dtheta);
+    }
+}
+
+// Halo along y over x 1..mx and z 3..mz-3, then along z over all x, y.
+__global__ void k_cyl_halo_y(GridP g, double *F)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 3 + blockIdx.y;
+    if (i > g.mx) return;
+    const int m = g.my;
+    for (int l = 0; l < 3; l++) F[cidx(g, i, m - 2 + l, k)] = F[cidx(g, i, 3 + l, k)];
+    for (int l = 0; l < 2; l++) F[cidx(g, i, 1 + l, k)] = F[cidx(g, i, m - 4 + l, k)];
+}
+__global__ void k_cyl_halo_z(GridP g, double *F)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > g.mx) return;
+    const int m = g.mz;
+    for (int l = 0; l < 3; l++) F[cidx(g, i, j, m - 2 + l)] = F[cidx(g, i, j, 3 + l)];
+    for (int l = 0; l < 2; l++) F[cidx(g, i, j, 1 + l)] = F[cidx(g, i, j, m - 4 + l)];
+}
+
+// Current fold: z faces over all x, y, then y faces over x 1..mx, z 3..mz-3.
+__global__ void k_cyl_fold_z(GridP g, double *F)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > g.mx) return;
+    const int m = g.mz;
+    double hi3[3], lo2[2];
+    for (int l = 0; l < 3; l++) hi3[l] = F[cidx(g, i, j, m - 2 + l)];
+    for (int l = 0; l < 2; l++) lo2[l] = F[cidx(g, i, j, 1 + l)];
+    for (int l = 0; l < 3; l++) F[cidx(g, i, j, 3 + l)] = F[cidx(g, i, j, 3 + l)] + hi3[l];
+    for (int l = 0; l < 2; l++) F[cidx(g, i, j, m - 4 + l)] = F[cidx(g, i, j, m - 4 + l)] + lo2[l];
+}
+__global__ void k_cyl_fold_y(GridP g, double *F)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 3 + blockIdx.y;
+    if (i > g.mx) return;
+    const int m = g.my;
+    double hi3[3], lo2[2];
+    for (int l = 0; l < 3; l++) hi3[l] = F[cidx(g, i, m - 2 + l, k)];
+    for (int l = 0; l < 2; l++) lo2[l] = F[cidx(g, i, 1 + l, k)];
+    for (int l = 0; l < 3; l++) F[cidx(g, i, 3 + l, k)] = F[cidx(g, i, 3 + l, k)] + hi3[l];
+    for (int l = 0; l < 2; l++) F[cidx(g, i, m - 4 + l, k)] = F[cidx(g, i, m - 4 + l, k)] + lo2[l];
+}
+
+static CylP cyl_params(const GridP &g)
+{
+    CylP c;
+    const double pi = 3.14159265358979323846264;
+    c.dtheta = 2.0 * pi / g.ny;
+    c.ax_perm_area = 4.0 / g.ny;
+    c.inv_dtheta = 1.0 / c.dtheta;
+    c.rmin = 0.0 + -0.5;  // xborders(0) + rshift
+    return c;
+}
+
+static void halo(const GridP &g, double *const F[3], cudaStream_t s)
+{
+    for (int c = 0; c < 3; c++) {
+        k_cyl_halo_y<<<dim3((g.mx + 127) / 128, g.mz - 5), 128, 0, s>>>(g, F[c]);
+        k_cyl_halo_z<<<dim3((g.mx + 127) / 128, g.my), 128, 0, s>>>(g, F[c]);
+    }
+    count_launches(6);
+}
+
+void launch_cyl_bhalf(const GridP &g, double *const E[3], double *const B[3], cudaStream_t s)
+{
+    const CylP cp = cyl_params(g);
+    const int nk = g.fdtd == PIC_FDTD_LEHE ? g.mz - 3 : g.mz - 1;
+    const dim3 grid((g.mx - 4 + 31) / 32, (g.my - 1 + 7) / 8, nk), block(32, 8, 1);
+    if (g.fdtd == PIC_FDTD_LEHE) k_cyl_bhalf<PIC_FDTD_LEHE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
+    else k_cyl_bhalf<PIC_FDTD_YEE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
+    k_cyl_bz_axis<<<(g.mz + 127) / 128, 128, 0, s>>>(g, cp, E[1], B[2]);
+    k_cyl_b_axis<<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, B[0], B[1], B[2]);
+    count_launches(3);
+    halo(g, B, s);
+}
+
+void launch_cyl_efield(const GridP &g, int mode, double *const E[3], double *const B[3], double *const J[3], cudaStream_t s)
+{
+    const CylP cp = cyl_params(g);
+    const dim3 grid((g.mx - 6 + 31) / 32, (g.my - 5 + 7) / 8, g.mz - 5), block(32, 8, 1);
+    if (mode == 0) k_cyl_e<0><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
+    else k_cyl_e<2><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
+    k_cyl_e_axis<<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, E[0], E[1], E[2]);
+    count_launches(2);
+    halo(g, E, s);
+}
+
+void launch_cyl_fold(const GridP &g, double *const J[3], cudaStream_t s)
+{
+    for (int c = 0; c < 3; c++) k_cyl_fold_z<<<dim3((g.mx + 127) / 128, g.my), 128, 0, s>>>(g, J[c]);
+    for (int c = 0; c < 3; c++) k_cyl_fold_y<<<dim3((g.mx + 127) / 128, g.mz - 5), 128, 0, s>>>(g, J[c]);
+    count_launches(6);
+}
+
+// ---------------------------------------------------------------------------
+// Mover
+// ---------------------------------------------------------------------------
+
+// Interp_VecEM_GridPoints at (x, y, z): node averages of GatherVecEfld /
+// GatherVecBfld with the trilinear weights (3D).
+__device__ __forceinline__ void interp3(const GridP &g, const double *Ex, const double *Ey, const double *Ez,
+                                        const double *Bx, const double *By, const double *Bz, double x, double y,
+                                        double z, double pE[3], double pB[3])
+{
+    const int ip = (int)x, jp = (int)y, kp = (int)z;
+    const double dx = x - ip, dy = y - jp, dz = z - kp;
+    double wt[8];
+#pragma unroll
+    for (int nn = 0; nn < 8; nn++) {
+        const double wx = (nn & 1) ? (0.0 + 1.0 * dx) : (1.0 + -1.0 * dx);
+        const double wy = (nn & 2) ? (0.0 + 1.0 * dy) : (1.0 + -1.0 * dy);
+        const double wz = (nn & 4) ? (0.0 + 1.0 * dz) : (1.0 + -1.0 * dz);
+        wt[nn] = (wx * wy) * wz;
+    }
+    const long long sy = g.sy, sz = g.sz;
+    const long long c0 = cidx(g, ip, jp, kp);
+    pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.0;
+#pragma unroll
+    for (int nn = 0; nn < 8; nn++) {
+        const long long nd = c0 + (nn & 1) + ((nn >> 1) & 1) * sy + ((nn >> 2) & 1) * sz;
+        const double vex = (ldd(Ex + nd - 1) + ldd(Ex + nd)) * 0.5;
+        const double vey = (ldd(Ey + nd - sy) + ldd(Ey + nd)) * 0.5;
+        const double vez = (ldd(Ez + nd - sz) + ldd(Ez + nd)) * 0.5;
+        const double vbx = (((ldd(Bx + nd - sy - sz) + ldd(Bx + nd - sz)) + ldd(Bx + nd - sy)) + ldd(Bx + nd)) * 0.25 + g.bext[0];
+        const double vby = (((ldd(By + nd - 1 - sz) + ldd(By + nd - 1)) + ldd(By + nd - sz)) + ldd(By + nd)) * 0.25 + g.bext[1];
+        const double vbz = (((ldd(Bz + nd - 1 - sy) + ldd(Bz + nd - 1)) + ldd(Bz + nd - sy)) + ldd(Bz + nd)) * 0.25 + g.bext[2];
+        pE[0] = pE[0] + wt[nn] * vex;
+        pE[1] = pE[1] + wt[nn] * vey;
+        pE[2] = pE[2] + wt[nn] * vez;
+        pB[0] = pB[0] + wt[nn] * vbx;
+        pB[1] = pB[1] + wt[nn] * vby;
+        pB[2] = pB[2] + wt[nn] * vbz;
+    }
+}
+
+__device__ __forceinline__ void half_boris_d(double sqc, const double pE[3], const double pB[3], double &u0, double &v0,
+                                           double &w0)
+{
+    const double gg = 1.0 / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+    const double bx = gg * pB[0], by = gg * pB[1], bz = gg * pB[2];
+    const double ff = 2.0 / (((1.0 + bx * bx) + by * by) + bz * bz);
+    const double u1 = ((u0 + v0 * bz) - w0 * by) * ff;
+    const double v1 = ((v0 + w0 * bx) - u0 * bz) * ff;
+    const double w1 = ((w0 + u0 * by) - v0 * bx) * ff;
+    u0 = ((u0 + v1 * bz) - w1 * by) + pE[0];
+    v0 = ((v0 + w1 * bx) - u1 * bz) + pE[1];
+    w0 = ((w0 + u1 * by) - v1 * bx) + pE[2];
+}
+
+// DepositCurrentPIC (deposit.F90:11-103, 3D) with atomics.
+__device__ void deposit_pic(const GridP &g, double *Jx, double *Jy, double *Jz, double x0, double y0, double z0,
+                            double x, double y, double z, double q)
+{
+    const double qthis = q * g.qi;
+    const int i1 = (int)floor(x0), i2 = (int)floor(x), j1 = (int)floor(y0), j2 = (int)floor(y);
+    const int k1 = (int)floor(z0), k2 = (int)floor(z);
+    const double xr = fmin((double)(min(i1, i2) + 1), fmax((double)max(i1, i2), 0.5 * (x0 + x)));
+    const double yr = fmin((double)(min(j1, j2) + 1), fmax((double)max(j1, j2), 0.5 * (y0 + y)));
+    const double zr = fmin((double)(min(k1, k2) + 1), fmax((double)max(k1, k2), 0.5 * (z0 + z)));
+    const double Fx1 = qthis * (xr - x0), Fy1 = qthis * (yr - y0), Fz1 = qthis * (zr - z0);
+    const double Wx1 = 0.5 * (x0 + xr) - i1, Wy1 = 0.5 * (y0 + yr) - j1;
+    const double Wx2 = 0.5 * (x + xr) - i2, Wy2 = 0.5 * (y + yr) - j2;
+    const double Wz1 = 0.5 * (z0 + zr) - k1, Wz2 = 0.5 * (z + zr) - k2;
+    const double Fx2 = qthis * (x - xr), Fy2 = qthis * (y - yr), Fz2 = qthis * (z - zr);
+    atomicAdd(Jx + cidx(g, i1, j1, k1), (Fx1 * (1.0 - Wy1)) * (1.0 - Wz1));
+    atomicAdd(Jx + cidx(g, i1, j1 + 1, k1), (Fx1 * Wy1) * (1.0 - Wz1));
+    atomicAdd(Jx + cidx(g, i1, j1, k1 + 1), (Fx1 * (1.0 - Wy1)) * Wz1);
+    atomicAdd(Jx + cidx(g, i1, j1 + 1, k1 + 1), (Fx1 * Wy1) * Wz1);
+    atomicAdd(Jx + cidx(g, i2, j2, k2), (Fx2 * (1.0 - Wy2)) * (1.0 - Wz2));
+    atomicAdd(Jx + cidx(g, i2, j2 + 1, k2), (Fx2 * Wy2) * (1.0 - Wz2));
+    atomicAdd(Jx + cidx(g, i2, j2, k2 + 1), (Fx2 * (1.0 - Wy2)) * Wz2);
+    atomicAdd(Jx + cidx(g, i2, j2 + 1, k2 + 1), (Fx2 * Wy2) * Wz2);
+    atomicAdd(Jy + cidx(g, i1, j1, k1), (Fy1 * (1.0 - Wx1)) * (1.0 - Wz1));
+    atomicAdd(Jy + cidx(g, i1 + 1, j1, k1), (Fy1 * Wx1) * (1.0 - Wz1));
+    atomicAdd(Jy + cidx(g, i1, j1, k1 + 1), (Fy1 * (1.0 - Wx1)) * Wz1);
+    atomicAdd(Jy + cidx(g, i1 + 1, j1, k1 + 1), (Fy1 * Wx1) * Wz1);
+    atomicAdd(Jy + cidx(g, i2, j2, k2), (Fy2 * (1.0 - Wx2)) * (1.0 - Wz2));
+    atomicAdd(Jy + cidx(g, i2 + 1, j2, k2), (Fy2 * Wx2) * (1.0 - Wz2));
+    atomicAdd(Jy + cidx(g, i2, j2, k2 + 1), (Fy2 * (1.0 - Wx2)) * Wz2);
+    atomicAdd(Jy + cidx(g, i2 + 1, j2, k2 + 1), (Fy2 * Wx2) * Wz2);
+    atomicAdd(Jz + cidx(g, i1, j1, k1), (Fz1 * (1.0 - Wx1)) * (1.0 - Wy1));
+    atomicAdd(Jz + cidx(g, i1 + 1, j1, k1), (Fz1 * Wx1) * (1.0 - Wy1));
+    atomicAdd(Jz + cidx(g, i1, j1 + 1, k1), (Fz1 * (1.0 - Wx1)) * Wy1);
+    atomicAdd(Jz + cidx(g, i1 + 1, j1 + 1, k1), (Fz1 * Wx1) * Wy1);
+    atomicAdd(Jz + cidx(g, i2, j2, k2), (Fz2 * (1.0 - Wx2)) * (1.0 - Wy2));
+    atomicAdd(Jz + cidx(g, i2 + 1, j2, k2), (Fz2 * Wx2) * (1.0 - Wy2));
+    atomicAdd(Jz + cidx(g, i2, j2 + 1, k2), (Fz2 * (1.0 - Wx2)) * Wy2);
+    atomicAdd(Jz + cidx(g, i2 + 1, j2 + 1, k2), (Fz2 * Wx2) * Wy2);
+}
+
+constexpr int kMaxSubsteps = 100000;
+
+template <int DUMMY>
+__global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64 p, const Counters *__restrict__ cnt,
+                                                       const double *__restrict__ Ex, const double *__restrict__ Ey,
+                                                       const double *__restrict__ Ez, const double *__restrict__ Bx,
+                                                       const double *__restrict__ By, const double *__restrict__ Bz,
+                                                       double *Jx, double *Jy, double *Jz, int *err)
+{
+    const long long used = cnt->used;
+    const double c = g.c, sqc = g.sqc, cinv = g.cinv;
+    const double r_proc = cp.rmin - 3.0;  // xborders + rshift - xmin
+    const double ylen = g.ylen;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
+        const int flv = p.flv[n];
+        const double x0 = p.x[n], y0 = p.y[n], z0 = p.z[n];
+        if (flv < 0 || flv > PIC_MAX_FLVR || !(x0 >= 2.5 && x0 < (double)(g.mx - 1)) ||
+            !(y0 >= 2.0 && y0 < (double)(g.my - 1)) || !(z0 >= 2.0 && z0 < (double)(g.mz - 1))) {
+            raise_error(err, PIC_DEVERR_RANGE);
+            continue;
+        }
+        if (flv == 0) continue;  // a hole moves nowhere and deposits zero
+        double qthis = p.q[n] * g.qi;
+        const double ui = p.u[n], vi = p.v[n], wi = p.w[n];
+        const double qm = g.qm[flv] * 0.25;  // cyl_movdep_strang.F90:100
+        const int ip0 = (int)x0, jp0 = (int)y0, kp0 = (int)z0;
+        double pE[3], pB[3];
+        interp3(g, Ex, Ey, Ez, Bx, By, Bz, x0, y0, z0, pE, pB);
+        for (int d = 0; d < 3; d++) {
+            pE[d] = pE[d] * qm;
+            pB[d] = pB[d] * qm;
+        }
+        double u0 = c * ui + pE[0], v0 = c * vi + pE[1], w0 = c * wi + pE[2];
+        half_boris_d(sqc, pE, pB, u0, v0, w0);
+        double u1 = u0 * cinv, v1 = v0 * cinv;
+        const double gg = sqc / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+        const double r0 = (x0 + r_proc) * 1.0;
+        const double xx1 = r0 + u1 * gg, yy1 = v1 * gg;
+        double r1 = sqrt(xx1 * xx1 + yy1 * yy1);
+        double xn = r1 * 1.0 - r_proc;
+        double yn = y0 + atan(yy1 / xx1) * cp.inv_dtheta;
+        double zn = z0 + (wi * gg) * 1.0;  // z moves with this step's initial w (:202)
+        r1 = 1.0 / r1;
+        u1 = (r0 * u0 + ((u0 * u1) * gg + v0 * yy1)) * r1;
+        v1 = (v0 * r0) * r1;
+        if (x0 >= 4.5 && (!(xn >= 2.0 && xn < (double)(g.mx - 1)) || !(yn >= 2.0 && yn < (double)(g.my - 1)) ||
+                          !(zn >= 2.0 && zn < (double)(g.mz - 1)))) {
+            raise_error(err, PIC_DEVERR_RANGE);  // the azimuthal step left the ghost frame
+            continue;
+        }
+        const int ip = (int)xn, jp = (int)yn, kp = (int)zn;
+        if (x0 >= 4.5) {
+            interp3(g, Ex, Ey, Ez, Bx, By, Bz, xn, yn, zn, pE, pB);
+        } else {
+            pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.0;  // redone by the sub-stepper below
+        }
+        for (int d = 0; d < 3; d++) {
+            pE[d] = pE[d] * qm;
+            pB[d] = pB[d] * qm;
+        }
+        u0 = u1 + pE[0];
+        v0 = v1 + pE[1];
+        w0 = w0 + pE[2];
+        half_boris_d(sqc, pE, pB, u0, v0, w0);
+        double un = u0 * cinv, vn = v0 * cinv, wn = w0 * cinv;
+        if (x0 < 4.5) {
+            // SubStepMovDep (:404-438) from the step's initial state
+            qthis = 0.0;
+            xn = x0; yn = y0; zn = z0; un = ui; vn = vi; wn = wi;
+            double t = 0.0, dt = 1.0, sx0 = x0, sy0 = y0, sz0 = z0;
+            int tries = 0;
+            while (t < 1.0) {
+                if (++tries > kMaxSubsteps) {
+                    raise_error(err, PIC_DEVERR_SUBSTEP);
+                    break;
+                }
+                const double delt = (t + dt > 1.0) ? 1.0 - t : dt;
+                // MovePrtlAxis (:462-566)
+                interp3(g, Ex, Ey, Ez, Bx, By, Bz, sx0, sy0, sz0, pE, pB);
+                for (int d = 0; d < 3; d++) {
+                    pE[d] = (pE[d] * qm) * delt;
+                    pB[d] = (pB[d] * qm) * delt;
+                }
+                double a0 = c * un + pE[0], b0 = c * vn + pE[1], c0 = c * wn + pE[2];
+                half_boris_d(sqc, pE, pB, a0, b0, c0);
+                double a1 = a0 * cinv, b1 = b0 * cinv;
+                const double c1 = c0 * cinv;
+                const double g2 = sqc / sqrt(((sqc + a0 * a0) + b0 * b0) + c0 * c0);
+                const double rr0 = (sx0 - 3.5) * 1.0;
+                const double X1 = rr0 + (a1 * g2) * delt;
+                const double Y1 = (b1 * g2) * delt;
+                const double R1 = sqrt(X1 * X1 + Y1 * Y1);
+                const double dy = X1 > 0 ? atan(Y1 / X1) * cp.inv_dtheta : 0.0;
+                if (fabs(dy) > 0.45) {
+                    dt = dt * 0.5;
+                    continue;
+                }
+                double nx;
+                if (X1 > 0) {
+                    nx = R1 / 1.0 + 3.5;
+                    a1 = (rr0 * a0 + ((a0 * a1) * g2 * delt + b0 * Y1)) / R1;
+                    b1 = (b0 * rr0) / R1;
+                } else {
+                    nx = X1 / 1.0 + 3.5;
+                }
+                const double ny = yn + dy;
+                const double nz = zn + ((c1 * g2) * delt) * 1.0;
+                interp3(g, Ex, Ey, Ez, Bx, By, Bz, nx, ny, nz, pE, pB);
+                for (int d = 0; d < 3; d++) {
+                    pE[d] = (pE[d] * qm) * delt;
+                    pB[d] = (pB[d] * qm) * delt;
+                }
+                a0 = a1 + pE[0];
+                b0 = b1 + pE[1];
+                c0 = c0 + pE[2];
+                half_boris_d(sqc, pE, pB, a0, b0, c0);
+                xn = nx; yn = ny; zn = nz;
+                un = a0 * cinv; vn = b0 * cinv; wn = c0 * cinv;
+                t = t + delt;
+                deposit_pic(g, Jx, Jy, Jz, sx0, sy0, sz0, xn, yn, zn, p.q[n]);
+                // PrtlAxisBC (:450-460)
+                if (xn < 3.5) {
+                    xn = 3.5 + (3.5 - xn);
+                    yn = yn + g.ny / 2.0;
+                    un = -un;
+                    vn = -vn;
+                }
+                if (yn > g.ymax) yn = yn - g.ylen;
+                if (yn < g.ymin) yn = yn + g.ylen;
+                dt = dt * 1.7;
+                sx0 = xn; sy0 = yn; sz0 = zn;
+            }
+        }
+        // zigzag deposit; both segments use the start cell (:341)
+        const double xr = fmin((double)(min(ip0, ip) + 1), fmax((double)max(ip0, ip), 0.5 * (x0 + xn)));
+        const double yr = fmin((double)(min(jp0, jp) + 1), fmax((double)max(jp0, jp), 0.5 * (y0 + yn)));
+        const double zr = fmin((double)(min(kp0, kp) + 1), fmax((double)max(kp0, kp), 0.5 * (z0 + zn)));
+        if (qthis != 0.0) {
+            const long long cell = cidx(g, ip0, jp0, kp0);
+            double o[12], o2[12];
+            segment<double, 3>(qthis * (xr - x0), qthis * (yr - y0), qthis * (zr - z0), 0.5 * (x0 + xr) - ip0,
+                               0.5 * (y0 + yr) - jp0, 0.5 * (z0 + zr) - kp0, o);
+            segment<double, 3>(qthis * (xn - xr), qthis * (yn - yr), qthis * (zn - zr), 0.5 * (xn + xr) - ip,
+                               0.5 * (yn + yr) - jp, 0.5 * (zn + zr) - kp, o2);
+            for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
+            scatter<double, 3>(g, Jx, Jy, Jz, cell, o);
+        }
+        p.x[n] = xn;
+        p.y[n] = yn;
+        p.z[n] = zn;
+        p.u[n] = un;
+        p.v[n] = vn;
+        p.w[n] = wn;
+    }
+}
+
+// AxisCurrentBC (cyl_movdep_strang.F90:570-584), all j, k.
+__global__ void k_cyl_axis_current(GridP g, double *Jx, double *Jy, double *Jz)
+{
+    const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = 1 + blockIdx.y;
+    if (j > g.my) return;
+    Jy[cidx(g, 4, j, k)] = Jy[cidx(g, 4, j, k)] - Jy[cidx(g, 3, j, k)];
+    Jz[cidx(g, 4, j, k)] = Jz[cidx(g, 4, j, k)] - Jz[cidx(g, 3, j, k)];
+    Jx[cidx(g, 3, j, k)] = 0.0;
+    Jy[cidx(g, 2, j, k)] = 0.0;
+    Jz[cidx(g, 2, j, k)] = 0.0;
+}
+
+void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s)
+{
+    const CylP cp = cyl_params(g);
+    k_cyl_move<0><<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+    k_cyl_axis_current<<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
+    count_launches(2);
+}
+
+}  // namespace pic

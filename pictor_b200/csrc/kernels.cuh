@@ -29,6 +29,13 @@ template <typename T> void launch_efield(const GridP &g, int mode, T *const E[3]
 template <typename T> void launch_fold(const GridP &g, T *const J[3], cudaStream_t s);
 template <typename T> void launch_filter(const GridP &g, T *const J[3], T *tmp, cudaStream_t s);
 
+// cyl.cu (cylindrical FP64 form)
+void launch_cyl_bhalf(const GridP &g, double *const E[3], double *const B[3], cudaStream_t s);
+void launch_cyl_efield(const GridP &g, int mode, double *const E[3], double *const B[3], double *const J[3], cudaStream_t s);
+void launch_cyl_fold(const GridP &g, double *const J[3], cudaStream_t s);
+void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s);
+
 // mover.cu
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
                              double *const B[3], double *const J[3], int *err, cudaStream_t s);

@@ -410,10 +410,12 @@ __device__ __forceinline__ int outlier_face(const GridP &g, double x, double y, 
 }
 
 // AppendParticles walks recv(1..6), which hold what left through faces
-// 2,1,4,3,6,5: slot of a face in that order, -1 for none.
-__device__ __forceinline__ int append_slot(int face)
+// 2,1,4,3,6,5: slot of a face in that order, -1 for none.  Faces whose
+// neighbour is MPI_PROC_NULL (the r faces of a cylinder) append nothing.
+__device__ __forceinline__ int append_slot(const GridP &g, int face)
 {
-    return face == 0 ? -1 : ((face - 1) ^ 1);
+    if (face == 0 || (g.closed_x && face <= 2)) return -1;
+    return (face - 1) ^ 1;
 }
 
 template <int DIMS>
@@ -428,7 +430,7 @@ __global__ void __launch_bounds__(256) k_exch_count(GridP g, PartF64 p, const lo
     for (int r = 0; r < kTile / 256; r++) {
         const long long i = base + r * 256 + threadIdx.x;
         if (i < n && p.flv[i] != 0) {
-            const int s = append_slot(outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i]));
+            const int s = append_slot(g, outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i]));
             if (s >= 0) atomicAdd(&c[s], 1u);
         }
     }
@@ -454,7 +456,7 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
     const uint32_t lt = lanemask_lt();
     for (int r = 0; r < kWarpItems / 32; r++) {
         const long long i = wbase + r * 32 + lane;
-        const int s = (i < n && p.flv[i] != 0) ? append_slot(outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i])) : -1;
+        const int s = (i < n && p.flv[i] != 0) ? append_slot(g, outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i])) : -1;
         for (int f = 0; f < 6; f++) {
             const uint32_t b = __ballot_sync(0xffffffffu, s == f);
             if (lane == 0) wh[warp][f] += __popc(b);
@@ -477,7 +479,7 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
         const bool ok = i < n && p.flv[i] != 0;
         int face = 0;
         if (ok) face = outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i]);
-        const int s = append_slot(face);
+        const int s = append_slot(g, face);
         uint32_t pos = 0;
         for (int f = 0; f < 6; f++) {
             const uint32_t b = __ballot_sync(0xffffffffu, s == f);
@@ -503,6 +505,16 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
             p.w[d] = p.w[i];
             p.flv[d] = p.flv[i];
             // RemovePrtl, loadprtlout.F90:164-181
+            p.q[i] = 0.0;
+            p.flv[i] = 0;
+            p.u[i] = 0.0;
+            p.v[i] = 0.0;
+            p.w[i] = 0.0;
+            p.x[i] = 3.8;
+            p.y[i] = 3.8;
+            p.z[i] = DIMS == 3 ? 3.8 : 1.5;
+        } else if (face != 0) {
+            // sent to MPI_PROC_NULL: RemovePrtl without a matching append
             p.q[i] = 0.0;
             p.flv[i] = 0;
             p.u[i] = 0.0;

@@ -259,3 +259,104 @@ def test_fp32_form_tracks_fp64(dims):
     fe32, fe64 = a["B2"] + a["E2"], b["B2"] + b["E2"]
     assert abs(fe32 - fe64) <= 1e-2 * fe64
     assert a["gauss_linf"] <= (1e-4 if dims == 2 else 2e-2) * a["rho_max"]
+
+
+# ---------------------------------------------------------------------------
+# Cylindrical (r, theta, z) FP64 form vs the cylindrical restatement
+# ---------------------------------------------------------------------------
+def _cyl(fdtd="yee", nx=12, ny=8, nz=10, capacity=1 << 15, reorder_period=20):
+    from pictor_b200 import PicConfig
+
+    g = O.make_grid(3, nx, ny, nz, c=0.45, qi=0.01, fdtd=fdtd, qm=(1.0, -1.0))
+    cfg = PicConfig(nx=nx, ny=ny, nz=nz, dims=3, c=0.45, qi=0.01, qm=(1.0, -1.0), fdtd=fdtd, geom="cylindrical",
+                    capacity=capacity, reorder_period=reorder_period, rmin=-0.5, inc_axis=1)
+    return g, cfg
+
+
+def _cyl_particles(g, seed=3):
+    p = O.cyl_load_uniform(g, 1, 1, 1, 1.0, 2e-3, -1.0, 2, seed, 1 << 14)
+    rng = np.random.default_rng(seed)
+    n = p.used
+    # a few near-axis particles moving through the axis region, and some ions
+    k = min(40, n)
+    idx = rng.choice(n, k, replace=False)
+    p.x[idx] = 3.5 + rng.uniform(0.05, 1.0, k)
+    p.u[idx] = rng.uniform(-0.6, 0.6, k)
+    p.v[idx] = rng.uniform(-0.6, 0.6, k)
+    p.flv[idx[: k // 2]] = 1
+    p.q[idx[: k // 2]] *= -1.0
+    return p
+
+
+@pytest.mark.parametrize("fdtd", ["yee", "lehe"])
+def test_cyl_field_phases_bit_exact(fdtd):
+    g, cfg = _cyl(fdtd)
+    f = random_fields(g, seed=51, consistent_ghosts=False)
+    o = O.CylOracle(g, O.Particles(1), f.copy())
+    with _sim(cfg) as s:
+        s.load_fields(to_gpu_fields(f))
+        o.update_b_half(); o.send_recv_flds("B")
+        s.update_b_half()
+        gf = s.fetch_fields()
+        for n in ("Bx", "By", "Bz"):
+            assert np.array_equal(getattr(gf, n), getattr(o.f, n)), n
+        o.update_e(); o.send_recv_flds("E")
+        s.update_e()
+        gf = s.fetch_fields()
+        for n in ("Ex", "Ey", "Ez"):
+            assert np.array_equal(getattr(gf, n), getattr(o.f, n)), n
+        rng = np.random.default_rng(6)
+        J = [np.asfortranarray(rng.normal(scale=1e-3, size=O.grid_shape(g))) for _ in range(3)]
+        o.f.Jx[...], o.f.Jy[...], o.f.Jz[...] = J
+        s.load_current(*J)
+        o.fold_current(); s.fold_current()
+        gf = s.fetch_fields()
+        for n in ("Jx", "Jy", "Jz"):
+            assert np.array_equal(getattr(gf, n), getattr(o.f, n)), n
+        o.add_current(); o.send_recv_flds("E")
+        s.add_current()
+        gf = s.fetch_fields()
+        for n in ("Ex", "Ey", "Ez"):
+            assert np.array_equal(getattr(gf, n), getattr(o.f, n)), n
+
+
+def test_cyl_move_deposit_and_exchange_parity():
+    g, cfg = _cyl()
+    f = random_fields(g, seed=52, scale=0.02, consistent_ghosts=False)
+    p = _cyl_particles(g)
+    o = O.CylOracle(g, p.copy(), f.copy())
+    with _sim(cfg) as s:
+        s.load_fields(to_gpu_fields(f))
+        s.load_particles(to_gpu_particles(p))
+        o.move_deposit(); s.move_deposit()
+        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+        gf = s.fetch_fields()
+        for n in ("Jx", "Jy", "Jz"):
+            a, b = getattr(gf, n), getattr(o.f, n)
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * np.abs(b).max(), err_msg=n)
+        assert o.exchange_particles() == 0
+        s.exchange_particles()
+        assert s.particle_count() == o.p.used
+        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+
+
+@pytest.mark.parametrize("fdtd", ["yee", "lehe"])
+def test_cyl_full_steps_lockstep(fdtd):
+    g, cfg = _cyl(fdtd, reorder_period=4)
+    p = _cyl_particles(g, seed=4)
+    o = O.CylOracle(g, p.copy())
+    with _sim(cfg) as s:
+        s.load_particles(to_gpu_particles(p))
+        o.step(1); s.step(1)
+        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+        for t in range(2, 9):
+            o.step(t); s.step(1)
+        assert s.particle_count() == o.p.used
+        gp, v = s.fetch_particles(), o.p.view()
+        assert np.array_equal(gp.flv, v["flv"])
+        for k in ("x", "y", "z", "u", "v", "w"):
+            np.testing.assert_allclose(getattr(gp, k), v[k], rtol=1e-9, atol=1e-9, err_msg=k)
+        gf = s.fetch_fields(with_current=False)
+        for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+            a, b = getattr(gf, n), getattr(o.f, n)
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * max(np.abs(b).max(), 1e-30), err_msg=n)

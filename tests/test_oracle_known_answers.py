@@ -189,3 +189,55 @@ def test_weibel_loader_statistics():
     ux = v["u"]
     assert np.mean(np.abs(ux)) == pytest.approx(gb, rel=0.02)
     assert np.all((v["x"] >= 3) & (v["x"] < 67) & (v["y"] >= 3) & (v["y"] < 67) & (v["z"] >= 1) & (v["z"] < 2))
+
+
+# --- cylindrical restatement: hand-derived single-particle answers ----------
+def _cyl_one(x, y, z, u, v, w, ny=8):
+    g = O.make_grid(3, 16, ny, 12, c=0.45, qi=0.01)
+    p = O.Particles.from_arrays(8, q=[1.0], x=[x], y=[y], z=[z], u=[u], v=[v], w=[w], flv=[2])
+    o = O.CylOracle(g, p)
+    o.move_deposit()
+    return o
+
+
+def test_cyl_radial_move_is_straight():
+    o = _cyl_one(10.5, 5.5, 7.5, 0.3, 0.0, 0.0)
+    d = 0.3 / math.sqrt(1 + 0.09) * 0.45       # beta * c per step
+    assert o.p.x[0] == pytest.approx(10.5 + d, abs=1e-14)
+    assert o.p.y[0] == 5.5 and o.p.u[0] == pytest.approx(0.3, abs=1e-15)
+
+
+def test_cyl_azimuthal_move_conserves_angular_momentum():
+    ny = 8
+    o = _cyl_one(10.5, 5.5, 7.5, 0.0, 0.3, 0.0, ny)
+    r0 = 7.0
+    d = 0.3 / math.sqrt(1 + 0.09) * 0.45
+    r1 = math.sqrt(r0 * r0 + d * d)
+    assert o.p.x[0] - 3.5 == pytest.approx(r1, abs=1e-13)
+    assert o.p.y[0] == pytest.approx(5.5 + math.atan(d / r0) / (2 * math.pi / ny), abs=1e-13)
+    assert o.p.v[0] * (o.p.x[0] - 3.5) == pytest.approx(0.3 * r0, rel=1e-13)
+
+
+def test_cyl_axis_crossing_reflects_through_theta_pi():
+    """A particle driven through r = 0 by the sub-stepper comes out on the far
+    side: theta advanced by ny/2 cells, radial momentum reversed.  The
+    reference's crossing branch (cyl_movdep_strang.F90:525-527) keeps u1 in
+    units of gamma*v/c, so the final momentum carries a factor 1/c."""
+    ny = 8
+    o = _cyl_one(3.6, 5.5, 7.5, -0.5, 0.0, 0.0, ny)
+    assert o.p.y[0] == pytest.approx(5.5 + ny / 2, abs=1e-12)
+    assert o.p.x[0] > 3.5
+    assert o.p.u[0] == pytest.approx(0.5 / 0.45, rel=1e-12)
+
+
+def test_cyl_vacuum_fields_stay_bounded():
+    g = O.make_grid(3, 12, 8, 10, c=0.45, qi=0.0)
+    rng = np.random.default_rng(1)
+    f = O.Fields(g)
+    for n in ("Ex", "Ey", "Ez"):
+        getattr(f, n)[...] = rng.normal(scale=1e-2, size=O.grid_shape(g))
+    o = O.CylOracle(g, O.Particles(1), f)
+    for t in range(1, 30):
+        o.step(t)
+    e = o.field_energy()
+    assert np.isfinite(e[0]) and np.isfinite(e[1]) and e[0] + e[1] < 1e3
