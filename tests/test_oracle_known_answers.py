@@ -231,13 +231,18 @@ def test_cyl_axis_crossing_reflects_through_theta_pi():
 
 
 def test_cyl_vacuum_fields_stay_bounded():
-    g = O.make_grid(3, 12, 8, 10, c=0.45, qi=0.0)
+    """Vacuum run from a random interior E (ghost layers zero: the open r face
+    has no boundary condition here).  The near-axis cells have r*dtheta = 0.5
+    * 2pi/ny, so with ny = 8 the explicit scheme needs c below ~0.34; at
+    c = 0.3 the field energy stays bounded."""
+    g = O.make_grid(3, 12, 8, 10, c=0.3, qi=0.0)
     rng = np.random.default_rng(1)
     f = O.Fields(g)
     for n in ("Ex", "Ey", "Ez"):
-        getattr(f, n)[...] = rng.normal(scale=1e-2, size=O.grid_shape(g))
+        getattr(f, n)[3:g.mx - 3, 2:g.my - 3, 2:g.mz - 3] = rng.normal(scale=1e-2, size=(g.mx - 6, g.my - 5, g.mz - 5))
     o = O.CylOracle(g, O.Particles(1), f)
-    for t in range(1, 30):
+    e0 = sum(o.field_energy())
+    for t in range(1, 200):
         o.step(t)
-    e = o.field_energy()
-    assert np.isfinite(e[0]) and np.isfinite(e[1]) and e[0] + e[1] < 1e3
+    e = sum(o.field_energy())
+    assert np.isfinite(e) and e < 10 * e0
