@@ -36,6 +36,9 @@ WORKLOADS = {
                           precision="fp32"),
     "weibel2d_fp64": dict(dims=2, nx=256, ny=256, nz=1, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0,
                           precision="fp64"),
+    # a small case of the headline physics for profiler captures (particles 270 MB > L2)
+    "weibel3d_fp32_small": dict(dims=3, nx=128, ny=64, nz=64, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
+                                precision="fp32"),
 }
 SEED = 2930
 
