@@ -116,6 +116,7 @@ def _declare(L: C.CDLL) -> None:
     L.orc_cyl_load_uniform.argtypes = [P(Grid), C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_int,
                                        C.c_uint32, P(_Particles)]
     L.orc_cyl_load_uniform.restype = C.c_int64
+    L.orc_cyl_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
 
 
 def _dp(a: np.ndarray):
@@ -311,6 +312,12 @@ class CylOracle(Oracle):
     def step(self, t: int, reorder_period: int = 20) -> int:
         fs = self.f.struct()
         return self._call_p(self.L.orc_cyl_step, C.byref(fs), int(t), int(reorder_period))
+
+    def field_energy(self):
+        out = (C.c_double * 2)()
+        fs = self.f.struct()
+        self.L.orc_cyl_field_energy(C.byref(self.g), C.byref(fs), out)
+        return out[0], out[1]
 
     def params(self):
         out = (C.c_double * 4)()

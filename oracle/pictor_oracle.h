@@ -139,6 +139,7 @@ int orc_cyl_exchange(const orc_grid *g, orc_particles *p);
 int orc_cyl_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period);
 int64_t orc_cyl_load_uniform(const orc_grid *g, int npx, int npy, int npz, double density, double temp, double charge,
                              int flv, uint32_t seed, orc_particles *p);
+void orc_cyl_field_energy(const orc_grid *g, const orc_fields *f, double out[2]);
 extern int orc_cyl_max_substeps;
 extern int64_t orc_cyl_substep_overruns;
 

@@ -628,6 +628,25 @@ int orc_cyl_exchange(const orc_grid *g, orc_particles *p)
     return rc;
 }
 
+/* CalcFldEnergy_cyl, cyl_savedata_routines.F90:8-31 (not halved). */
+void orc_cyl_field_energy(const orc_grid *g, const orc_fields *f, double out[2])
+{
+    double P[4];
+    orc_cyl_params(g, P);
+    const double dtheta = P[0], rmin = 0.0 + P[3];
+    double eb = 0.0, ee = 0.0;
+    for (int k = 3; k <= g->mz - 3; k++)
+        for (int j = 3; j <= g->my - 3; j++)
+            for (int i = 4; i <= g->mx - 3; i++) {
+                const double r = ((double)i - 3.0) + rmin, rp = r + 0.5;
+                const int64_t c0 = ID(g, i, j, k);
+                eb = eb + ((r * (f->Bx[c0] * f->Bx[c0]) + rp * (f->By[c0] * f->By[c0])) + rp * (f->Bz[c0] * f->Bz[c0])) * dtheta;
+                ee = ee + ((rp * (f->Ex[c0] * f->Ex[c0]) + r * (f->Ey[c0] * f->Ey[c0])) + r * (f->Ez[c0] * f->Ez[c0])) * dtheta;
+            }
+    out[0] = eb;
+    out[1] = ee;
+}
+
 /* One cylindrical step in MAIN.F90 order (Yee or Lehe B update). */
 int orc_cyl_step(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period)
 {

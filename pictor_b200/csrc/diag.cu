@@ -50,13 +50,22 @@ __global__ void __launch_bounds__(kDiagThreads) k_field_energy_partial(GridP g, 
     __shared__ double red[kDiagThreads / 32];
     const long long nint = (long long)g.nx * g.ny * (g.dims == 3 ? g.nz : 1);
     double eb = 0, ee = 0;
+    const double dtheta = 2.0 * 3.14159265358979323846264 / g.ny;
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
         int i, j, k;
         interior_ijk(g, t, i, j, k);
         const long long c = cidx(g, i, j, k);
         const double bx = Bx[c], by = By[c], bz = Bz[c], ex = Ex[c], ey = Ey[c], ez = Ez[c];
-        eb += (bx * bx + by * by) + bz * bz;
-        ee += (ex * ex + ey * ey) + ez * ez;
+        if (g.geom == PIC_GEOM_CYLINDRICAL) {
+            // CalcFldEnergy_cyl (cyl_savedata_routines.F90:8-31): r weights, axis cell excluded
+            if (i < 4) continue;
+            const double r = ((double)i - 3.0) + -0.5, rp = r + 0.5;
+            eb += ((r * (bx * bx) + rp * (by * by)) + rp * (bz * bz)) * dtheta;
+            ee += ((rp * (ex * ex) + r * (ey * ey)) + r * (ez * ez)) * dtheta;
+        } else {
+            eb += (bx * bx + by * by) + bz * bz;
+            ee += (ex * ex + ey * ey) + ez * ez;
+        }
     }
     const double sb = block_sum(eb, red);
     const double se = block_sum(ee, red);

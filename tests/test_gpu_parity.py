@@ -360,3 +360,14 @@ def test_cyl_full_steps_lockstep(fdtd):
         for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
             a, b = getattr(gf, n), getattr(o.f, n)
             np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * max(np.abs(b).max(), 1e-30), err_msg=n)
+
+
+def test_cyl_field_energy_matches_oracle():
+    g, cfg = _cyl()
+    f = random_fields(g, seed=53, consistent_ghosts=False)
+    o = O.CylOracle(g, O.Particles(1), f.copy())
+    with _sim(cfg) as s:
+        s.load_fields(to_gpu_fields(f))
+        d = s.diagnostics()
+    eb, ee = o.field_energy()
+    np.testing.assert_allclose([d["B2"], d["E2"]], [eb, ee], rtol=1e-12)
