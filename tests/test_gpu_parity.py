@@ -114,10 +114,10 @@ def test_full_steps_lockstep(dims, fdtd):
     o = O.Oracle(g, p.copy())
     with _sim(cfg) as s:
         s.load_particles(to_gpu_particles(p))
-        o.step(1); s.step(1)
+        o.step(1, 5); s.step(1)
         assert_particles_equal(s.fetch_particles(), o.p, exact=True)
         for t in range(2, 13):
-            o.step(t); s.step(1)
+            o.step(t, 5); s.step(1)
         assert s.particle_count() == o.p.used
         gp = s.fetch_particles()
         v = o.p.view()
@@ -347,10 +347,10 @@ def test_cyl_full_steps_lockstep(fdtd):
     o = O.CylOracle(g, p.copy())
     with _sim(cfg) as s:
         s.load_particles(to_gpu_particles(p))
-        o.step(1); s.step(1)
+        o.step(1, 4); s.step(1)
         assert_particles_equal(s.fetch_particles(), o.p, exact=True)
         for t in range(2, 9):
-            o.step(t); s.step(1)
+            o.step(t, 4); s.step(1)
         assert s.particle_count() == o.p.used
         gp, v = s.fetch_particles(), o.p.view()
         assert np.array_equal(gp.flv, v["flv"])
