@@ -329,7 +329,13 @@ def test_cyl_move_deposit_and_exchange_parity():
         s.load_fields(to_gpu_fields(f))
         s.load_particles(to_gpu_particles(p))
         o.move_deposit(); s.move_deposit()
-        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+        # the azimuthal move calls atan (device vs libm: last-ulp differences), so
+        # positions agree to round-off; momenta and cells match
+        gp = s.fetch_particles()
+        assert_particles_equal(gp, o.p, exact=False, rtol=1e-13)
+        v = o.p.view()
+        for k in ("x", "y", "z"):
+            assert np.array_equal(np.floor(getattr(gp, k)), np.floor(v[k])), k
         gf = s.fetch_fields()
         for n in ("Jx", "Jy", "Jz"):
             a, b = getattr(gf, n), getattr(o.f, n)
@@ -337,7 +343,7 @@ def test_cyl_move_deposit_and_exchange_parity():
         assert o.exchange_particles() == 0
         s.exchange_particles()
         assert s.particle_count() == o.p.used
-        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+        assert_particles_equal(s.fetch_particles(), o.p, exact=False, rtol=1e-13)
 
 
 @pytest.mark.parametrize("fdtd", ["yee", "lehe"])
@@ -348,7 +354,7 @@ def test_cyl_full_steps_lockstep(fdtd):
     with _sim(cfg) as s:
         s.load_particles(to_gpu_particles(p))
         o.step(1, 4); s.step(1)
-        assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+        assert_particles_equal(s.fetch_particles(), o.p, exact=False, rtol=1e-13)
         for t in range(2, 9):
             o.step(t, 4); s.step(1)
         assert s.particle_count() == o.p.used
