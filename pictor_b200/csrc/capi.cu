@@ -465,7 +465,9 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     g.sy = g.mx;
     g.sz = (long long)g.mx * g.my;
     g.ncell = g.sz * g.mz;
-    if (g.ncell >= (1ll << kFlvShift) - 1) {
+    g.mx_magic = div_magic((unsigned)g.mx);
+    g.my_magic = div_magic((unsigned)g.my);
+    if (g.ncell >= (1ll << kFlvShift) - 1 || g.mx > 4096 || g.my > 4096) {
         delete h;
         return PIC_ERR_INVALID;
     }

@@ -31,7 +31,27 @@ struct GridP {
     double xmin, xmax, ymin, ymax, zmin, zmax, xlen, ylen, zlen;
     int geom;                         // PIC_GEOM_*
     int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
+    unsigned long long mx_magic, my_magic;  // ceil(2^40 / m): exact n/m for n < 2^28, m <= 4096
 };
+
+// n / d by multiply-shift (the magic of GridP); exact for n < 2^28, d <= 4096.
+__host__ __device__ inline unsigned long long div_magic(unsigned int d)
+{
+    return ((1ull << 40) + d - 1) / d;
+}
+__device__ __forceinline__ int fast_div(unsigned int n, unsigned long long magic)
+{
+    return (int)__umul64hi((unsigned long long)n << 24, magic);  // (n * magic) >> 40 without overflow
+}
+// (i,j,k), 1-based, of a linear ghosted cell index.
+__device__ __forceinline__ void decode_cell(const GridP &g, int cell, int &i, int &j, int &k)
+{
+    const int jk = fast_div((unsigned)cell, g.mx_magic);
+    i = cell - jk * g.mx + 1;
+    k = fast_div((unsigned)jk, g.my_magic);
+    j = jk - k * g.my + 1;
+    k += 1;
+}
 
 __host__ __device__ inline long long cidx(const GridP &g, int i, int j, int k)
 {

@@ -109,7 +109,8 @@ __device__ __forceinline__ void move_one_f32_global(const GridP &g, const PartF3
     const int flv = (int)(key >> kFlvShift);
     if (flv == 0) return;
     const int cell = (int)(key & kCellMask);
-    const int i = cell % mx + 1, jk = cell / mx, j = jk % my + 1, k = jk / my + 1;
+    int i, j, k;
+        decode_cell(g, cell, i, j, k);
     if (i < 3 || i > mx - 3 || j < 3 || j > my - 3 || (DIMS == 3 && (k < 3 || k > mz - 3)) || (DIMS == 2 && k != 1)) {
         raise_error(err, PIC_DEVERR_RANGE);
         return;
@@ -220,7 +221,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
             const uint32_t key = p.key[n];
             if ((key >> kFlvShift) == 0) continue;
             const int cell = (int)(key & kCellMask);
-            const int i = cell % mx + 1, jk = cell / mx, j = jk % my + 1, k = jk / my + 1;
+            int i, j, k;
+        decode_cell(g, cell, i, j, k);
             lo0 = min(lo0, i); hi0 = max(hi0, i);
             lo1 = min(lo1, j); hi1 = max(hi1, j);
             lo2 = min(lo2, k); hi2 = max(hi2, k);
@@ -285,7 +287,8 @@ __global__ void __launch_bounds__(kTileThreads, 2)
         const int flv = (int)(key >> kFlvShift);
         if (flv == 0) continue;
         const int cell = (int)(key & kCellMask);
-        const int i = cell % mx + 1, jk = cell / mx, j = jk % my + 1, k = jk / my + 1;
+        int i, j, k;
+        decode_cell(g, cell, i, j, k);
         const float dx = p.dx[n], dy = p.dy[n], dz = DIMS == 3 ? p.dz[n] : 0.f;
         float wt[8];
         weights<float, DIMS>(dx, dy, dz, wt);

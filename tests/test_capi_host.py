@@ -81,3 +81,19 @@ def test_invalid_configs_rejected_before_device_use():
         with pytest.raises(PicError) as e:
             Simulation(bad)
         assert e.value.code == -1
+
+
+def test_cell_decode_division_is_exact():
+    """The device decodes cell indices with n/d = (n * ceil(2^40/d)) >> 40,
+    exact for n < 2^28 and d <= 4096 (checked at every quotient boundary)."""
+    import numpy as np
+
+    rng = np.random.default_rng(0)
+    for d in (6, 21, 37, 261, 517, 1029, 4096):
+        m = ((1 << 40) + d - 1) // d
+        qmax = (1 << 28) // d
+        q = np.unique(np.concatenate([rng.integers(0, qmax + 1, 20000), np.arange(max(0, qmax - 2000), qmax + 1)]))
+        for r in (0, d - 1):
+            for n in (int(x) * d + r for x in q):
+                if n < (1 << 28):
+                    assert ((n << 24) * m) >> 64 == n // d, (n, d)
