@@ -157,6 +157,24 @@ int pic_phase_times(pic_handle *h, double *ms, int64_t *launches, int32_t n, int
 /* Kernels launched by pic_step since the last call (graph or eager). */
 int pic_launch_count(pic_handle *h, int64_t *launches);
 
+/* Field energy without any device allocation (no counterpart in the
+   reference).  For callers that cannot call cudaMalloc at this point: hosts
+   whose memory pool owns all of the GPU's memory, or that must not let a
+   library allocate/free (cudaFree synchronizes the device) between their own
+   steps.  Inputs are caller-owned DEVICE arrays in the reference layout
+   ((nx+5, ny+5, nz+5 or 1) column-major FP64); out2 is a DEVICE pointer that
+   receives sum|B|^2 and sum|E|^2 over the interior (CalcFldEnergy,
+   savedata_routines.F90:310-326).  Work is enqueued on `stream` (a
+   cudaStream_t, NULL for the default stream); synchronize before reading
+   out2.  The reduction's partial sums use one fixed array of 148*8 pairs in
+   the library's device memory, shared by every call: calls that overlap on
+   the GPU race.  The first call on a device looks up that array's device
+   address.  Returns PIC_ERR_INVALID for bad sizes. */
+int pic_field_energy_noalloc(const double *Ex, const double *Ey, const double *Ez,
+                             const double *Bx, const double *By, const double *Bz,
+                             int32_t nx, int32_t ny, int32_t nz, int32_t dims,
+                             double *out2, void *stream);
+
 /* Text for an error code. */
 const char *pic_error_string(int code);
 

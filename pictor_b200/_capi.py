@@ -107,6 +107,7 @@ SIGNATURES = {
     "pic_profile": (C.c_int, [H, C.c_int32]),
     "pic_phase_times": (C.c_int, [H, PD, PI64, C.c_int32, PI64]),
     "pic_launch_count": (C.c_int, [H, PI64]),
+    "pic_field_energy_noalloc": (C.c_int, [C.c_void_p] * 6 + [C.c_int32] * 4 + [C.c_void_p, C.c_void_p]),
     "pic_error_string": (C.c_char_p, [C.c_int]),
     "pic_stream": (C.c_void_p, [H]),
 }
