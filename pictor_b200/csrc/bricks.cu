@@ -1,0 +1,173 @@
+// bricks.cu -- the reorder of the FP32 form: particles grouped by brick.
+//
+// The reference reorders its particle array every prtl_reorder_period steps
+// by cell (ReorderPrtlArr, src/mem/mem_prtl.F90:166-301) so that the mover
+// walks memory in cell order; holes are dropped.  The FP32 form keeps that
+// role and cadence but groups by brick, a block of TX x TY x TZ interior
+// cells, which is the unit the tiled mover (mover_f32.cu) gives one CTA:
+//
+//   1. brick id per particle; per-brick counts (warp-aggregated atomics),
+//   2. exclusive scan of the counts -> tile_start (first particle of every
+//      brick; the last entry is the live count),
+//   3. scatter: each particle takes the next slot of its brick from an atomic
+//      cursor (one atomic per run of equal bricks within a warp),
+//   4. the per-brick boxes the mover starts from (the bricks themselves).
+//
+// Holes are dropped, as in the reference.  Within a brick the particles keep
+// their relative order in runs of one warp; the order of the runs follows the
+// atomics.  The FP32 step does not depend on the order beyond the rounding of
+// its FP32 current sums, which is order-dependent in any case.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace pic {
+
+__device__ __forceinline__ uint32_t lanemask_lt_b()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Brick of an interior cell (1-based indices 3..n+2), x fastest.
+__device__ __forceinline__ uint32_t brick_of(const Bricks &bk, int i, int j, int k)
+{
+    const int bx = (i - 3) / bk.t[0], by = (j - 3) / bk.t[1], bz = (k - 3) / bk.t[2];
+    return (uint32_t)bx + (uint32_t)bk.nb[0] * ((uint32_t)by + (uint32_t)bk.nb[1] * (uint32_t)bz);
+}
+
+constexpr uint32_t kNoBrick = 0xffffffffu;
+
+// 1. brick id of every slot (kNoBrick for holes) and per-brick counts.
+__global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, PartF32 p, const Counters *__restrict__ cnt,
+                                                          uint32_t *bid, int *err)
+{
+    const long long used = cnt->used;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < used; base += stride) {
+        const long long n = base + lane;
+        uint32_t b = kNoBrick;
+        if (n < used) {
+            const uint32_t key = p.key[n];
+            if ((key >> kFlvShift) != 0) {
+                int i, j, k;
+                decode_cell(g, (int)(key & kCellMask), i, j, k);
+                if (i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 ||
+                    (g.dims == 3 ? (k < 3 || k > g.mz - 3) : k != 1)) {
+                    raise_error(err, PIC_DEVERR_RANGE);  // dropped like a hole
+                } else {
+                    b = brick_of(bk, i, j, g.dims == 3 ? k : 3);
+                }
+            }
+            bid[n] = b;
+        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, b);
+        if (b != kNoBrick && (peers & lanemask_lt_b()) == 0) atomicAdd(&bk.count[b], (uint32_t)__popc(peers));
+    }
+}
+
+// 3. scatter every live particle to the next free slot of its brick.
+__global__ void __launch_bounds__(kThreads) k_brick_scatter(Bricks bk, PartF32 in, PartF32 out, const uint32_t *__restrict__ bid,
+                                                            const Counters *__restrict__ cnt, int has_dz)
+{
+    const long long used = cnt->used;
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < used; base += stride) {
+        const long long n = base + lane;
+        const uint32_t b = n < used ? bid[n] : kNoBrick;
+        const uint32_t peers = __match_any_sync(0xffffffffu, b);
+        const int leader = __ffs(peers) - 1;
+        uint32_t slot = 0;
+        if (b != kNoBrick && lane == leader) slot = atomicAdd(&bk.cursor[b], (uint32_t)__popc(peers));
+        slot = __shfl_sync(0xffffffffu, slot, leader) + (uint32_t)__popc(peers & lanemask_lt_b());
+        if (b == kNoBrick) continue;
+        out.key[slot] = in.key[n];
+        out.dx[slot] = in.dx[n];
+        out.dy[slot] = in.dy[n];
+        if (has_dz) out.dz[slot] = in.dz[n];
+        out.ux[slot] = in.ux[n];
+        out.uy[slot] = in.uy[n];
+        out.uz[slot] = in.uz[n];
+        out.w[slot] = in.w[n];
+    }
+}
+
+// 4. cursors at the brick starts, boxes = the bricks (relative to the centre).
+__global__ void k_brick_prepare(GridP g, Bricks bk)
+{
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= bk.ntiles) return;
+    bk.cursor[b] = bk.tile_start[b];
+    const int bi[3] = {b % bk.nb[0], (b / bk.nb[0]) % bk.nb[1], b / (bk.nb[0] * bk.nb[1])};
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    int *box = bk.box + 8 * (size_t)b;
+    for (int d = 0; d < 3; d++) {
+        if (d >= g.dims) {
+            box[d] = box[d + 3] = 0;
+            continue;
+        }
+        const int lo = 3 + bi[d] * bk.t[d];
+        const int hi = min(lo + bk.t[d] - 1, n3[d] + 2);
+        const int hc = lo + (bk.t[d] >> 1);
+        box[d] = lo - hc;
+        box[d + 3] = hi - hc;
+    }
+    box[6] = box[7] = 0;
+}
+
+__global__ void k_brick_finish(Bricks bk, Counters *cnt)
+{
+    const long long live = bk.tile_start[bk.ntiles];
+    cnt->used = live;
+    cnt->np = live;
+}
+
+static unsigned grid_for(long long n)
+{
+    long long b = (n + kThreads - 1) / kThreads;
+    if (b > (long long)kSMs * 32) b = (long long)kSMs * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
+void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, long long capacity,
+                        const Bricks &bk, int *err, cudaStream_t s)
+{
+    cudaMemsetAsync(bk.count, 0, (size_t)(bk.ntiles + 1) * sizeof(uint32_t), s);
+    k_brick_count<<<grid_for(capacity), kThreads, 0, s>>>(g, bk, p, cnt, bk.bid, err);
+    scan_exclusive_u32(bk.count, bk.tile_start, (size_t)bk.ntiles + 1, bk.scan_tmp, nullptr, s);
+    k_brick_prepare<<<(bk.ntiles + 255) / 256, 256, 0, s>>>(g, bk);
+    k_brick_scatter<<<grid_for(capacity), kThreads, 0, s>>>(bk, p, out, bk.bid, cnt, g.dims == 3);
+    k_brick_finish<<<1, 1, 0, s>>>(bk, cnt);
+    count_launches(5);
+}
+
+// Brick shape for a fill of ppc particles per cell: about 4096 particles per
+// brick, x first, up to 8x8x8 (3D) / 32x32 (2D) so that the brick plus one
+// cell of margin always fits the mover's shared memory.
+void choose_bricks(const GridP &g, double ppc, Bricks &bk)
+{
+    static const int s3[][3] = {{4, 4, 4}, {8, 4, 4}, {8, 8, 4}, {8, 8, 8}};
+    static const int s2[][3] = {{8, 8, 1}, {16, 8, 1}, {16, 16, 1}, {32, 16, 1}, {32, 32, 1}};
+    const double target = 4096.0 / (ppc > 0.5 ? ppc : 0.5);
+    const int ns = g.dims == 3 ? 4 : 5;
+    int pick = ns - 1;
+    for (int q = 0; q < ns; q++) {
+        const int *t = g.dims == 3 ? s3[q] : s2[q];
+        if ((double)t[0] * t[1] * t[2] >= target) {
+            pick = q;
+            break;
+        }
+    }
+    const int *t = g.dims == 3 ? s3[pick] : s2[pick];
+    const int n3[3] = {g.nx, g.ny, g.nz};
+    for (int d = 0; d < 3; d++) {
+        bk.t[d] = d < g.dims ? (t[d] < n3[d] ? t[d] : n3[d]) : 1;
+        bk.nb[d] = d < g.dims ? (n3[d] + bk.t[d] - 1) / bk.t[d] : 1;
+    }
+    bk.ntiles = bk.nb[0] * bk.nb[1] * bk.nb[2];
+    bk.smem_floats = kBrickSmemBytes / 4;
+}
+
+}  // namespace pic

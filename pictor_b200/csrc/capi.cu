@@ -40,8 +40,8 @@ struct pic_handle {
     long long phase_launches[PIC_PHASE_COUNT] = {};
     long long prof_steps = 0;
     long long launches = 0;   // kernels launched by pic_step since the last pic_launch_count
-    // FP32 spatial tiles (valid while `sorted`: set by a reorder, cleared by loads)
-    Tiling tiles = {};
+    // FP32 bricks (tile ranges valid while `sorted`: set by a reorder, cleared by loads)
+    Bricks bricks = {};
     bool sorted = false;
     std::vector<void *> allocs;
 };
@@ -244,8 +244,7 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 break;
             case PIC_PHASE_MOVE:
                 if (h->sorted)
-                    launch_move_deposit_f32_tiled(g, h->p32[cur], h->tiles.tile_start, h->tiles.ntiles, E, B, J, h->err,
-                                                  h->s);
+                    launch_move_deposit_f32_tiled(g, h->p32[cur], h->bricks, E, B, J, h->err, h->s);
                 else
                     launch_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
                 break;
@@ -263,7 +262,7 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 break;
             case PIC_PHASE_REORDER:
                 if (reorder)
-                    launch_reorder_f32(g, h->p32[cur], h->p32[cur ^ 1], h->cnt, h->sc, h->capacity, &h->tiles, h->s);
+                    launch_reorder_f32(g, h->p32[cur], h->p32[cur ^ 1], h->cnt, h->capacity, h->bricks, h->err, h->s);
                 break;
         }
     }
@@ -507,14 +506,14 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (!r && c.curr_filter > 0) r = dalloc(h, (char **)&h->Jtmp, fb);
     if (!r) r = alloc_particles(h);
     if (!r && h->fp32) {
-        // tile width: about 2048 particles per tile at the configured fill
-        const double ppc = (double)h->capacity / ((double)g.nx * g.ny * g.nz);
-        int w = 8;
-        while (w < g.nx && w * 2 * ppc <= 2048.0) w *= 2;
-        h->tiles.width = w < g.nx ? w : g.nx;
-        h->tiles.per_row = (g.nx + h->tiles.width - 1) / h->tiles.width;
-        h->tiles.ntiles = h->tiles.per_row * g.ny * g.nz;
-        r = dalloc(h, &h->tiles.tile_start, (size_t)h->tiles.ntiles + 1);
+        // bricks sized for the configured fill (capacity / interior cells)
+        Bricks &bk = h->bricks;
+        choose_bricks(g, (double)h->capacity / ((double)g.nx * g.ny * g.nz), bk);
+        const size_t nt = (size_t)bk.ntiles;
+        if ((r = dalloc(h, &bk.tile_start, nt + 1)) || (r = dalloc(h, &bk.box, 8 * nt)) ||
+            (r = dalloc(h, &bk.count, nt + 1)) || (r = dalloc(h, &bk.cursor, nt)) ||
+            (r = dalloc(h, &bk.bid, (size_t)h->capacity)) || (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1)))) {
+        }
     }
     if (!r) r = dalloc(h, &h->cnt, 1);
     if (!r) r = dalloc(h, &h->err, 1);
@@ -522,9 +521,11 @@ int pic_create(const pic_config *cfg, pic_handle **out)
         SortScratch &sc = h->sc;
         sc.ntiles = sort_tiles(h->capacity);
         sc.scan_tmp_len = scan_tmp_len(256 * sc.ntiles);
-        if ((r = dalloc(h, &sc.key[0], (size_t)h->capacity)) || (r = dalloc(h, &sc.key[1], (size_t)h->capacity)) ||
-            (r = dalloc(h, &sc.idx[0], (size_t)h->capacity)) || (r = dalloc(h, &sc.idx[1], (size_t)h->capacity)) ||
-            (r = dalloc(h, &sc.hist, 256 * sc.ntiles)) || (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
+        // radix-sort keys and indices: the FP64 reorder only
+        const size_t nk = h->fp32 ? 1 : (size_t)h->capacity;
+        if ((r = dalloc(h, &sc.key[0], nk)) || (r = dalloc(h, &sc.key[1], nk)) || (r = dalloc(h, &sc.idx[0], nk)) ||
+            (r = dalloc(h, &sc.idx[1], nk)) || (r = dalloc(h, &sc.hist, 256 * sc.ntiles)) ||
+            (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
         }
     }
     if (!r) {
@@ -773,8 +774,7 @@ int pic_move_deposit(pic_handle *h)
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         if (h->sorted)
-            launch_move_deposit_f32_tiled(h->g, h->p32[h->cur], h->tiles.tile_start, h->tiles.ntiles, E, B, J, h->err,
-                                          h->s);
+            launch_move_deposit_f32_tiled(h->g, h->p32[h->cur], h->bricks, E, B, J, h->err, h->s);
         else
             launch_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
     } else {
@@ -873,7 +873,7 @@ int pic_add_current(pic_handle *h)
 int pic_reorder(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->fp32) launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->sc, h->capacity, &h->tiles, h->s);
+    if (h->fp32) launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->capacity, h->bricks, h->err, h->s);
     else launch_reorder_f64(h->g, h->p64[h->cur], h->p64[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
     h->cur ^= 1;
     set_sorted(h, h->fp32);

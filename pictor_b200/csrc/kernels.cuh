@@ -1,5 +1,6 @@
 // kernels.cuh -- host launchers of the device kernels (one declaration per
-// kernel family; definitions in fields.cu, mover.cu, particles.cu, diag.cu).
+// kernel family; definitions in fields.cu, mover.cu, mover_f32.cu, bricks.cu,
+// particles.cu, cyl.cu, diag.cu).
 #pragma once
 
 #include "common.cuh"
@@ -39,11 +40,29 @@ void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *c
 // mover.cu
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
                              double *const B[3], double *const J[3], int *err, cudaStream_t s);
+// mover_f32.cu: per-particle FP32 mover (any particle order)
 void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
                              float *const B[3], float *const J[3], int *err, cudaStream_t s);
-// Tiled FP32 mover: one CTA per spatial tile (tile_start[ntiles+1] particle ranges).
-void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const uint32_t *tile_start, int ntiles,
-                                   float *const E[3], float *const B[3], float *const J[3], int *err, cudaStream_t s);
+// Bricks of the FP32 form: blocks of t[0] x t[1] x t[2] interior cells, nb[d]
+// per axis, x fastest.  After a reorder the particles of brick b occupy slots
+// [tile_start[b], tile_start[b+1]); box[8b..8b+5] holds the lower and upper
+// cell bounds (relative to the brick centre 3 + nb*t + t/2, unwrapped) of
+// where the brick's particles are, which the tiled mover reads and rewrites.
+constexpr int kBrickSmemBytes = 64 * 1024;   // dynamic shared memory of the tiled mover
+struct Bricks {
+    uint32_t *tile_start;   // ntiles + 1
+    int *box;               // 8 per brick
+    uint32_t *count;        // ntiles + 1 (scan input)
+    uint32_t *cursor;       // ntiles
+    uint32_t *bid;          // brick id per particle slot (capacity)
+    uint32_t *scan_tmp;
+    int t[3], nb[3], ntiles;
+    int smem_floats;
+};
+void choose_bricks(const GridP &g, double ppc, Bricks &bk);
+// Tiled FP32 mover: one CTA per brick.
+void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
+                                   float *const B[3], float *const J[3], int *err, cudaStream_t s);
 
 // particles.cu
 struct SortScratch {
@@ -63,14 +82,10 @@ void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch 
 // `out`, after which the caller swaps `p` and `out`.
 void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Counters *cnt, SortScratch &sc,
                         long long capacity, int *err, cudaStream_t s);
-// Tiles: row segments of `width` interior cells, S = ceil(nx/width) per (j,k)
-// row; tile_start (ntiles + 1 entries) receives each tile's first particle.
-struct Tiling {
-    uint32_t *tile_start;
-    int width, per_row, ntiles;
-};
-void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, SortScratch &sc,
-                        long long capacity, const Tiling *tiles, cudaStream_t s);
+// Reorder of the FP32 form (bricks.cu): live particles grouped by brick into
+// `out`, after which the caller swaps `p` and `out`.
+void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, long long capacity,
+                        const Bricks &bk, int *err, cudaStream_t s);
 // Reference layout <-> FP32 cell-relative conversion.
 void launch_f64_to_f32(const GridP &g, const PartF64 &in, const PartF32 &out, long long n, int *err, cudaStream_t s);
 void launch_f32_to_f64(const GridP &g, const PartF32 &in, const PartF64 &out, long long n, cudaStream_t s);

@@ -100,6 +100,7 @@ void scan_exclusive_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *t
     const size_t nb = (n + kScanTile - 1) / kScanTile;
     if (nb <= 1) {
         k_scan_block<<<1, kScanBlock, 0, s>>>(in, out, n, nullptr, total);
+        count_launches(1);
         return;
     }
     uint32_t *sums = tmp;
@@ -251,30 +252,6 @@ __global__ void k_keys_f64(GridP g, PartF64 p, const long long *__restrict__ use
     }
 }
 
-__global__ void k_keys_f32(GridP g, PartF32 p, const long long *__restrict__ used, uint32_t *keys, long long *np)
-{
-    const long long n = *used;
-    long long live = 0;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t k = p.key[i];
-        uint32_t key = (uint32_t)g.ncell;
-        if ((k >> kFlvShift) != 0) {
-            key = k & kCellMask;
-            live++;
-        }
-        keys[i] = key;
-    }
-    __shared__ long long red[kThreads / 32];
-    for (int o = 16; o > 0; o >>= 1) live += __shfl_down_sync(0xffffffffu, live, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = live;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        long long t = 0;
-        for (int w = 0; w < kThreads / 32; w++) t += red[w];
-        atomicAdd((unsigned long long *)np, (unsigned long long)t);
-    }
-}
-
 __global__ void k_gather_f64(PartF64 in, PartF64 out, const uint32_t *__restrict__ idx, const long long *__restrict__ used)
 {
     const long long n = *used;
@@ -288,23 +265,6 @@ __global__ void k_gather_f64(PartF64 in, PartF64 out, const uint32_t *__restrict
         out.v[i] = in.v[s];
         out.w[i] = in.w[s];
         out.flv[i] = in.flv[s];
-    }
-}
-
-__global__ void k_gather_f32(PartF32 in, PartF32 out, const uint32_t *__restrict__ idx, const long long *__restrict__ used,
-                             int has_dz)
-{
-    const long long n = *used;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const uint32_t s = idx[i];
-        out.key[i] = in.key[s];
-        out.dx[i] = in.dx[s];
-        out.dy[i] = in.dy[s];
-        if (has_dz) out.dz[i] = in.dz[s];
-        out.ux[i] = in.ux[s];
-        out.uy[i] = in.uy[s];
-        out.uz[i] = in.uz[s];
-        out.w[i] = in.w[s];
     }
 }
 
@@ -329,47 +289,6 @@ void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Co
     count_launches(1);
     k_set_used_np<<<1, 1, 0, s>>>(cnt);
     count_launches(1);
-}
-
-// First particle of every tile in the sorted keys (lower bound of the tile's
-// first cell); tile ntiles ends at the live count.
-__global__ void k_tile_starts(GridP g, const uint32_t *__restrict__ keys, const Counters *__restrict__ cnt, Tiling t)
-{
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q > t.ntiles) return;
-    const long long n = cnt->np;
-    if (q == t.ntiles) {
-        t.tile_start[q] = (uint32_t)n;
-        return;
-    }
-    const int row = q / t.per_row, seg = q % t.per_row;
-    const int j = 3 + row % g.ny, k = g.dims == 3 ? 3 + row / g.ny : 1;
-    const uint32_t first = (uint32_t)cidx(g, 3 + seg * t.width, j, k);
-    long long lo = 0, hi = n;
-    while (lo < hi) {
-        const long long mid = (lo + hi) >> 1;
-        if (keys[mid] < first) lo = mid + 1;
-        else hi = mid;
-    }
-    t.tile_start[q] = (uint32_t)lo;
-}
-
-void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, SortScratch &sc,
-                        long long capacity, const Tiling *tiles, cudaStream_t s)
-{
-    cudaMemsetAsync(&cnt->np, 0, sizeof(long long), s);
-    k_keys_f32<<<stream_grid(capacity), kThreads, 0, s>>>(g, p, &cnt->used, sc.key[0], &cnt->np);
-    count_launches(1);
-    const size_t ntiles = sort_tiles(capacity);
-    const int r = radix_sort(sc, &cnt->used, key_bits(g.ncell), ntiles, s);
-    k_gather_f32<<<stream_grid(capacity), kThreads, 0, s>>>(p, out, sc.idx[r], &cnt->used, g.dims == 3);
-    count_launches(1);
-    k_set_used_np<<<1, 1, 0, s>>>(cnt);
-    count_launches(1);
-    if (tiles) {
-        k_tile_starts<<<(tiles->ntiles + 1 + 255) / 256, 256, 0, s>>>(g, sc.key[r], cnt, *tiles);
-        count_launches(1);
-    }
 }
 
 // ---------------------------------------------------------------------------

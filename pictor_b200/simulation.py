@@ -220,7 +220,8 @@ class Simulation:
         check(self.L.pic_reset_current(self.h), "pic_reset_current")
 
     def ReorderPrtlGPU(self):
-        """ReorderPrtlArr (mem_prtl.F90:166-301): stable cell-key sort."""
+        """ReorderPrtlArr (mem_prtl.F90:166-301): stable cell-key sort (FP64
+        form); the FP32 form groups the particles by brick instead."""
         check(self.L.pic_reorder(self.h), "pic_reorder")
 
     update_b_half = UpdateBfieldHalfGPU

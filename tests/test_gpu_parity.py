@@ -214,28 +214,92 @@ def test_filtered_step_matches_oracle():
 
 @pytest.mark.parametrize("dims", [2, 3])
 def test_fp32_tiled_mover_matches_global_mover(dims):
-    """The tiled FP32 mover (shared-memory fields and current per tile) and the
-    per-particle FP32 mover give the same particles and the same current up to
-    the FP32 rounding of the summation order."""
+    """The tiled FP32 mover (shared-memory fields and current per brick) and
+    the per-particle FP32 mover give bit-identical particles and, once the
+    ghost current is folded, the same current up to the FP32 rounding of the
+    summation order."""
     nx, ny, nz = (48, 40, 1) if dims == 2 else (24, 16, 12)
     g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, precision="fp32", qi=0.00158203125, capacity=1 << 18)
     f = random_fields(g, seed=41, scale=0.02)
     with _sim(cfg) as s:
         s.init_weibel(8, 0.5, 0.4, 0.005, 0.005, 9)
-        s.reorder()                       # tiles valid -> tiled mover
+        s.reorder()                       # bricks valid -> tiled mover
         sorted_p = s.fetch_particles()
         s.load_fields(to_gpu_fields(f))
         s.move_deposit()
+        s.fold_current()
         a_p, a_f = s.fetch_particles(), s.fetch_fields()
-        s.load_particles(sorted_p)        # same state, tiles invalid -> per-particle mover
+        s.load_particles(sorted_p)        # same state, bricks invalid -> per-particle mover
         s.load_fields(to_gpu_fields(f))
         s.move_deposit()
+        s.fold_current()
         b_p, b_f = s.fetch_particles(), s.fetch_fields()
     for k in ("x", "y", "z", "u", "v", "w"):
         np.testing.assert_array_equal(getattr(a_p, k), getattr(b_p, k), err_msg=k)
     for n in ("Jx", "Jy", "Jz"):
-        a, b = getattr(a_f, n), getattr(b_f, n)
+        a, b = interior(getattr(a_f, n), g), interior(getattr(b_f, n), g)
         np.testing.assert_allclose(a, b, rtol=0, atol=2e-6 * np.abs(b).max(), err_msg=n)
+
+
+def _brick_shape(dims, nx, ny, nz, capacity):
+    """Brick shape the library picks: about 4096 particles per brick at
+    capacity / cells, from a fixed ladder of shapes, clipped to the grid."""
+    ladder = [(4, 4, 4), (8, 4, 4), (8, 8, 4), (8, 8, 8)] if dims == 3 else \
+        [(8, 8, 1), (16, 8, 1), (16, 16, 1), (32, 16, 1), (32, 32, 1)]
+    cells = nx * ny * (nz if dims == 3 else 1)
+    target = 4096.0 / max(capacity / cells, 0.5)
+    t = next((s for s in ladder if s[0] * s[1] * s[2] >= target), ladder[-1])
+    n = (nx, ny, nz)
+    return tuple(min(t[d], n[d]) if d < dims else 1 for d in range(3))
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_fp32_reorder_groups_by_brick(dims):
+    """The FP32 reorder keeps every live particle once, drops holes, and
+    groups the particles by brick in increasing brick order."""
+    nx, ny, nz = (40, 36, 1) if dims == 2 else (20, 16, 12)
+    cap = 1 << 16
+    g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, precision="fp32", qi=0.00158203125, capacity=cap)
+    with _sim(cfg) as s:
+        n0 = s.init_weibel(8, 0.5, 0.4, 0.005, 0.005, 5)
+        before = s.fetch_particles()
+        s.reorder()
+        after = s.fetch_particles()
+    assert len(after.x) == n0 and np.all(after.flv > 0)
+    t = _brick_shape(dims, nx, ny, nz, cap)
+    nb = [-(-n // t[d]) for d, n in enumerate((nx, ny, nz))]
+    i = np.floor(after.x).astype(int) - 3
+    j = np.floor(after.y).astype(int) - 3
+    k = np.floor(after.z).astype(int) - 3 if dims == 3 else np.zeros_like(i)
+    bid = i // t[0] + nb[0] * (j // t[1] + nb[1] * (k // t[2]))
+    assert np.all(np.diff(bid) >= 0)
+    key = lambda p: np.lexsort((p.w, p.v, p.u, p.z, p.y, p.x))
+    ka, kb = key(after), key(before)
+    for f in ("x", "y", "z", "u", "v", "w", "q", "flv"):
+        np.testing.assert_array_equal(getattr(after, f)[ka], getattr(before, f)[kb], err_msg=f)
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_fp32_tiled_steps_track_per_particle_steps(dims):
+    """40 steps without a reorder after the first one: the bricks' particles
+    drift well past their bricks (boxes grow, some fall back to the brick plus
+    one cell with the rest of the particles through global memory, some cross
+    the periodic boundary) and the run stays on the per-particle run up to
+    FP32 summation-order noise."""
+    nx, ny, nz = (48, 40, 1) if dims == 2 else (24, 16, 16)
+    res = {}
+    for tiled in (True, False):
+        g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, precision="fp32", qi=0.00158203125,
+                                 capacity=1 << 18, reorder_period=0)
+        with _sim(cfg) as s:
+            s.init_weibel(8, 0.5, 0.8, 0.01, 0.01, 77)
+            if tiled:
+                s.reorder()
+            s.step(40)
+            res[tiled] = s.diagnostics(0.00158203125)
+    a, b = res[True], res[False]
+    np.testing.assert_allclose(a["kinetic"], b["kinetic"], rtol=1e-5)
+    assert abs((a["B2"] + a["E2"]) - (b["B2"] + b["E2"])) <= 1e-3 * (b["B2"] + b["E2"])
 
 
 @pytest.mark.parametrize("dims", [2, 3])
