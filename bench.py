@@ -57,6 +57,21 @@ def bytes_per_cell_mover(precision: str) -> int:
     return 9 * (4 if precision == "fp32" else 8)
 
 
+# DRAM bytes (read + written) per particle of one k_move_f32_tiled<3> launch,
+# from ncu (dram__bytes_read.sum + dram__bytes_write.sum) on the
+# weibel3d_fp32_small workload (8.39 M particles, 270 MB of particle state,
+# larger than L2); scaled to a full launch by the particles it moves.
+TRAFFIC_BYTES_PER_PARTICLE = 57.1
+TRAFFIC_SOURCE = ("ncu on weibel3d_fp32_small scaled by particle count "
+                  "(profiles/k_move_f32_tiled_weibel3d.md)")
+
+
+def traffic_per_launch(wl: dict, n_p: int):
+    if wl["precision"] != "fp32" or wl["dims"] != 3:
+        return None
+    return TRAFFIC_BYTES_PER_PARTICLE * n_p
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -262,7 +277,7 @@ def run_reference(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="weibel3d_fp32")
@@ -391,7 +406,8 @@ def main():
                        "c_ompe": wl["c_ompe"], "reorder_period": 20, "seed": SEED, "parallelism": f"replicas{ws}",
                        "l2": "inputs larger than L2 (particle state >> 126 MB)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "kernel": "k_move_f32" if prec == "fp32" else "k_move_f64",
+                         "traffic": traffic_per_launch(wl, n_p), "traffic_source": TRAFFIC_SOURCE,
+                         "kernel": "k_move_f32_tiled" if prec == "fp32" else "k_move_f64",
                          "algorithmic_bytes_per_launch": bytes_move, "launch_ms": move_ms,
                          "peak_kind": peak_kind, "step_algorithmic_GBs": step_bytes / (ms_max / args.steps * 1e-3) / 1e9},
             "phases_ms_per_step": {k: v / max(phases["steps"], 1) for k, v in phases["ms"].items()},

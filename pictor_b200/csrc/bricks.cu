@@ -11,7 +11,8 @@
 //      brick; the last entry is the live count),
 //   3. scatter: each particle takes the next slot of its brick from an atomic
 //      cursor (one atomic per run of equal bricks within a warp),
-//   4. the per-brick boxes the mover starts from (the bricks themselves).
+//   4. the per-brick boxes the mover starts from (the bricks themselves),
+//      and max |w| over the live particles (the mover's fixed-point scale).
 //
 // Holes are dropped, as in the reference.  Within a brick the particles keep
 // their relative order in runs of one warp; the order of the runs follows the
@@ -47,10 +48,11 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, Pa
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < used; base += stride) {
         const long long n = base + lane;
-        uint32_t b = kNoBrick;
+        uint32_t b = kNoBrick, wbits = 0;
         if (n < used) {
             const uint32_t key = p.key[n];
             if ((key >> kFlvShift) != 0) {
+                wbits = __float_as_uint(fabsf(p.w[n]));
                 int i, j, k;
                 decode_cell(g, (int)(key & kCellMask), i, j, k);
                 if (i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 ||
@@ -64,6 +66,8 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, Pa
         }
         const uint32_t peers = __match_any_sync(0xffffffffu, b);
         if (b != kNoBrick && (peers & lanemask_lt_b()) == 0) atomicAdd(&bk.count[b], (uint32_t)__popc(peers));
+        wbits = __reduce_max_sync(0xffffffffu, wbits);   // |w| bit patterns order as integers
+        if (lane == 0 && wbits) atomicMax(bk.wmax_bits, wbits);
     }
 }
 
@@ -135,6 +139,7 @@ void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Co
                         const Bricks &bk, int *err, cudaStream_t s)
 {
     cudaMemsetAsync(bk.count, 0, (size_t)(bk.ntiles + 1) * sizeof(uint32_t), s);
+    cudaMemsetAsync(bk.wmax_bits, 0, sizeof(uint32_t), s);
     k_brick_count<<<grid_for(capacity), kThreads, 0, s>>>(g, bk, p, cnt, bk.bid, err);
     scan_exclusive_u32(bk.count, bk.tile_start, (size_t)bk.ntiles + 1, bk.scan_tmp, nullptr, s);
     k_brick_prepare<<<(bk.ntiles + 255) / 256, 256, 0, s>>>(g, bk);
@@ -144,8 +149,8 @@ void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Co
 }
 
 // Brick shape for a fill of ppc particles per cell: about 4096 particles per
-// brick, x first, up to 8x8x8 (3D) / 32x32 (2D) so that the brick plus one
-// cell of margin always fits the mover's shared memory.
+// brick, x first, up to 8x8x8 (3D) / 32x32 (2D) so that the boxes of the
+// brick plus one cell of margin always fit the mover's shared memory.
 void choose_bricks(const GridP &g, double ppc, Bricks &bk)
 {
     static const int s3[][3] = {{4, 4, 4}, {8, 4, 4}, {8, 8, 4}, {8, 8, 8}};

@@ -483,6 +483,12 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     g.closed_x = c.geom == PIC_GEOM_CYLINDRICAL;
     g.qm[0] = 0.0;
     for (int f = 1; f <= PIC_MAX_FLVR; f++) g.qm[f] = f <= c.nflvr ? c.qm[f] : 0.0;
+    g.c_f = (float)g.c;
+    g.sqc_f = (float)g.sqc;
+    g.cinv_f = (float)g.cinv;
+    g.qi_f = (float)g.qi;
+    for (int d = 0; d < 3; d++) g.bext_f[d] = (float)g.bext[d];
+    for (int f = 0; f <= PIC_MAX_FLVR; f++) g.qm_half_f[f] = (float)g.qm[f] * 0.5f;
     // subdomains.F90:52-67
     g.xmin = 3.0;
     g.xmax = (double)(g.mx - 2);
@@ -512,7 +518,8 @@ int pic_create(const pic_config *cfg, pic_handle **out)
         const size_t nt = (size_t)bk.ntiles;
         if ((r = dalloc(h, &bk.tile_start, nt + 1)) || (r = dalloc(h, &bk.box, 8 * nt)) ||
             (r = dalloc(h, &bk.count, nt + 1)) || (r = dalloc(h, &bk.cursor, nt)) ||
-            (r = dalloc(h, &bk.bid, (size_t)h->capacity)) || (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1)))) {
+            (r = dalloc(h, &bk.bid, (size_t)h->capacity)) || (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1))) ||
+            (r = dalloc(h, &bk.wmax_bits, 1))) {
         }
     }
     if (!r) r = dalloc(h, &h->cnt, 1);

@@ -32,6 +32,9 @@ struct GridP {
     int geom;                         // PIC_GEOM_*
     int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
     unsigned long long mx_magic, my_magic;  // ceil(2^40 / m): exact n/m for n < 2^28, m <= 4096
+    // FP32 copies for the FP32 form: c, c^2, 1/c, qi, external B, q/m * 0.5
+    float c_f, sqc_f, cinv_f, qi_f, bext_f[3];
+    float qm_half_f[PIC_MAX_FLVR + 1];
 };
 
 // n / d by multiply-shift (the magic of GridP); exact for n < 2^28, d <= 4096.

@@ -187,21 +187,15 @@ __device__ __forceinline__ void e_curl(const GridP &g, T fc, const T *Ex, const 
 
 // Fold partner along one axis of an interior index a (0 = none), see image_of.
 // J1 = J + J(x-partner); J2 = J1 + J1(y-partner); J3 = J2 + J2(z-partner):
-// the order of comm_fld.F90:15-33 (x faces, then y, then z).
-template <typename T, int DIMS, bool ZERO>
-__device__ __forceinline__ T fold_cell(const GridP &g, T *J, int i, int j, int k)
+// the order of comm_fld.F90:15-33 (x faces, then y, then z).  Loads only.
+template <typename T, int DIMS>
+__device__ __forceinline__ T fold_cell(const GridP &g, const T *__restrict__ J, int i, int j, int k)
 {
     const int pi = image_of(i, g.mx), pj = image_of(j, g.my);
     const int pk = DIMS == 3 ? image_of(k, g.mz) : 0;
     auto J1 = [&](int b, int c) -> T {
-        const long long a0 = cidx(g, i, b, c);
-        T v = J[a0];
-        if (ZERO) J[a0] = (T)0;
-        if (pi) {
-            const long long a1 = cidx(g, pi, b, c);
-            v = v + J[a1];
-            if (ZERO) J[a1] = (T)0;
-        }
+        T v = J[cidx(g, i, b, c)];
+        if (pi) v = v + J[cidx(g, pi, b, c)];
         return v;
     };
     auto J2 = [&](int c) -> T {
@@ -214,21 +208,46 @@ __device__ __forceinline__ T fold_cell(const GridP &g, T *J, int i, int j, int k
     return v;
 }
 
+// Zero the J cells fold_cell read (ResetCurrent of the consumed current).
+template <typename T, int DIMS>
+__device__ __forceinline__ void zero_fold_cells(const GridP &g, T *__restrict__ J, int i, int j, int k)
+{
+    const int ii[2] = {i, image_of(i, g.mx)};
+    const int jj[2] = {j, image_of(j, g.my)};
+    const int kk[2] = {k, DIMS == 3 ? image_of(k, g.mz) : 0};
+#pragma unroll
+    for (int c = 0; c < (DIMS == 3 ? 2 : 1); c++) {
+        if (kk[c] == 0) continue;
+#pragma unroll
+        for (int b = 0; b < 2; b++) {
+            if (jj[b] == 0) continue;
+#pragma unroll
+            for (int a = 0; a < 2; a++) {
+                if (ii[a] == 0) continue;
+                J[cidx(g, ii[a], jj[b], kk[c])] = (T)0;
+            }
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // E <- E + c curl B (UpdateEfield) [- fold(J) (AddCurrent)] + halo.
 // MODE 0: curl only; 1: curl + fold + AddCurrent, zeroing J; 2: AddCurrent of
 // an already folded J alone (phase API); 3: curl + AddCurrent of an already
-// folded (and filtered) J.
+// folded (and filtered) J.  Every load of a thread precedes its stores, so
+// the loads of a thread are in flight together (an interleaved load, zero,
+// load sequence on J serialised the memory latency).
 // ---------------------------------------------------------------------------
 template <typename T, int DIMS, int MODE>
-__global__ void __launch_bounds__(256) k_efield(GridP g, T *Ex, T *Ey, T *Ez, const T *__restrict__ Bx,
-                                                const T *__restrict__ By, const T *__restrict__ Bz, T *Jx, T *Jy,
-                                                T *Jz)
+__global__ void __launch_bounds__(256) k_efield(GridP g, T *__restrict__ Ex, T *__restrict__ Ey, T *__restrict__ Ez,
+                                                const T *__restrict__ Bx, const T *__restrict__ By,
+                                                const T *__restrict__ Bz, T *__restrict__ Jx, T *__restrict__ Jy,
+                                                T *__restrict__ Jz)
 {
     const CellIter it = interior_cell<DIMS>(g);
     if (!it.ok) return;
     const long long c0 = cidx(g, it.i, it.j, it.k);
-    T ex, ey, ez;
+    T ex, ey, ez, jx = (T)0, jy = (T)0, jz = (T)0;
     if (MODE == 2) {
         ex = Ex[c0];
         ey = Ey[c0];
@@ -236,18 +255,28 @@ __global__ void __launch_bounds__(256) k_efield(GridP g, T *Ex, T *Ey, T *Ez, co
     } else {
         e_curl<T, DIMS>(g, (T)g.fc, Ex, Ey, Ez, Bx, By, Bz, c0, ex, ey, ez);
     }
-    if (MODE == 1) {  // em_update.F90:96-98 with grid_inv_d = 1
-        ex = ex - (fold_cell<T, DIMS, true>(g, Jx, it.i, it.j, it.k) * (T)1) * (T)1;
-        ey = ey - (fold_cell<T, DIMS, true>(g, Jy, it.i, it.j, it.k) * (T)1) * (T)1;
-        ez = ez - (fold_cell<T, DIMS, true>(g, Jz, it.i, it.j, it.k) * (T)1) * (T)1;
+    if (MODE == 1) {
+        jx = fold_cell<T, DIMS>(g, Jx, it.i, it.j, it.k);
+        jy = fold_cell<T, DIMS>(g, Jy, it.i, it.j, it.k);
+        jz = fold_cell<T, DIMS>(g, Jz, it.i, it.j, it.k);
     } else if (MODE == 2 || MODE == 3) {
-        ex = ex - (Jx[c0] * (T)1) * (T)1;
-        ey = ey - (Jy[c0] * (T)1) * (T)1;
-        ez = ez - (Jz[c0] * (T)1) * (T)1;
+        jx = Jx[c0];
+        jy = Jy[c0];
+        jz = Jz[c0];
+    }
+    if (MODE != 0) {  // em_update.F90:96-98 with grid_inv_d = 1
+        ex = ex - (jx * (T)1) * (T)1;
+        ey = ey - (jy * (T)1) * (T)1;
+        ez = ez - (jz * (T)1) * (T)1;
     }
     store_with_images<T, DIMS>(g, Ex, it.i, it.j, it.k, ex);
     store_with_images<T, DIMS>(g, Ey, it.i, it.j, it.k, ey);
     store_with_images<T, DIMS>(g, Ez, it.i, it.j, it.k, ez);
+    if (MODE == 1) {
+        zero_fold_cells<T, DIMS>(g, Jx, it.i, it.j, it.k);
+        zero_fold_cells<T, DIMS>(g, Jy, it.i, it.j, it.k);
+        zero_fold_cells<T, DIMS>(g, Jz, it.i, it.j, it.k);
+    }
 }
 
 // UpdateCurrentAllFaces as a separate phase: J(interior) <- fold(J).  Each J
@@ -258,9 +287,9 @@ __global__ void __launch_bounds__(256) k_fold(GridP g, T *Jx, T *Jy, T *Jz)
     const CellIter it = interior_cell<DIMS>(g);
     if (!it.ok) return;
     const long long c0 = cidx(g, it.i, it.j, it.k);
-    const T fx = fold_cell<T, DIMS, false>(g, Jx, it.i, it.j, it.k);
-    const T fy = fold_cell<T, DIMS, false>(g, Jy, it.i, it.j, it.k);
-    const T fz = fold_cell<T, DIMS, false>(g, Jz, it.i, it.j, it.k);
+    const T fx = fold_cell<T, DIMS>(g, Jx, it.i, it.j, it.k);
+    const T fy = fold_cell<T, DIMS>(g, Jy, it.i, it.j, it.k);
+    const T fz = fold_cell<T, DIMS>(g, Jz, it.i, it.j, it.k);
     Jx[c0] = fx;
     Jy[c0] = fy;
     Jz[c0] = fz;

@@ -48,7 +48,7 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // [tile_start[b], tile_start[b+1]); box[8b..8b+5] holds the lower and upper
 // cell bounds (relative to the brick centre 3 + nb*t + t/2, unwrapped) of
 // where the brick's particles are, which the tiled mover reads and rewrites.
-constexpr int kBrickSmemBytes = 64 * 1024;   // dynamic shared memory of the tiled mover
+constexpr int kBrickSmemBytes = 64 * 1024;   // dynamic shared memory of the tiled mover (node + current box)
 struct Bricks {
     uint32_t *tile_start;   // ntiles + 1
     int *box;               // 8 per brick
@@ -56,6 +56,7 @@ struct Bricks {
     uint32_t *cursor;       // ntiles
     uint32_t *bid;          // brick id per particle slot (capacity)
     uint32_t *scan_tmp;
+    uint32_t *wmax_bits;    // max |w| of the live particles (FP32 bits), set by the reorder
     int t[3], nb[3], ntiles;
     int smem_floats;
 };

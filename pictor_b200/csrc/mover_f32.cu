@@ -13,21 +13,31 @@
 // Tiled form (after a reorder): particles are grouped by brick (a block of
 // TX x TY x TZ interior cells, see bricks.cu) and one CTA moves one brick's
 // particles.  The CTA stages the node-averaged E and B of its box in shared
-// memory (each node value computed once per brick rather than 8 times per
-// particle), accumulates the current of the box in shared memory, and adds
-// the box to J once.  The box is the bounding box, in cells, of where the
-// brick's particles were after the previous step (particles drift away from
-// their brick between reorders); it is stored per brick relative to the
-// brick's centre, unwrapped across the periodic boundary, and this kernel
-// writes the box for the next step.  A box too large for shared memory falls
-// back to the brick itself plus one cell; particles outside the box gather
-// and deposit through global memory with the same arithmetic.  Box currents
-// go straight to the periodic interior image of each cell.
+// memory, so each node value is computed once per brick rather than 8 times
+// per particle.  The box is the bounding box, in cells, of where the brick's
+// particles were after the previous step (particles drift away from their
+// brick between reorders); it is stored per brick relative to the brick's
+// centre, unwrapped across the periodic boundary, and this kernel writes the
+// box for the next step.  A box too large for shared memory falls back to the
+// brick itself plus one cell; particles outside the box gather and deposit
+// through global memory with the same arithmetic.
+//
+// The current of the brick is summed in a shared-memory box as 32-bit fixed
+// point with native integer atomics (FP32 atomic adds on shared memory are
+// slow here, and per-particle FP32 reductions into L2, as the reference GPU
+// kernel does, movdep_gpu.F90:193-318, saturate the L2 tag lookups).  The
+// scale is set per brick from N * max|w| * qi * c, an upper bound of any sum,
+// so nothing overflows.  The box is added to J once, as FP32 reductions onto
+// the periodic interior image of each cell.
+//
+// Each thread streams particles n, n+256, ... and loads particle n+256 before
+// it moves particle n, so the DRAM latency of the next particle overlaps the
+// arithmetic of this one.
 //
 // The node averages and interpolation sums are computed identically on both
 // paths (same expressions, same order, explicit fmaf), so the tiled and the
-// per-particle kernels move particles bit-identically; currents differ only
-// in the order of the FP32 atomic sums.
+// per-particle kernels move particles bit-identically; currents differ by the
+// order of the FP32 sums and the fixed-point rounding of the box.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -39,9 +49,8 @@ namespace pic {
 template <int DIMS>
 __device__ __forceinline__ void node_avg(const float *__restrict__ Ex, const float *__restrict__ Ey,
                                          const float *__restrict__ Ez, const float *__restrict__ Bx,
-                                         const float *__restrict__ By, const float *__restrict__ Bz, long long nd,
-                                         long long sy, long long sz, float b0, float b1, float b2, float4 &A,
-                                         float2 &Bv)
+                                         const float *__restrict__ By, const float *__restrict__ Bz, int nd, int sy,
+                                         int sz, float b0, float b1, float b2, float4 &A, float2 &Bv)
 {
     A.x = (__ldg(Ex + nd - 1) + __ldg(Ex + nd)) * 0.5f;
     A.y = (__ldg(Ey + nd - sy) + __ldg(Ey + nd)) * 0.5f;
@@ -108,69 +117,146 @@ __device__ __forceinline__ void boris_f32(float c, float sqc, float cinv, const 
     gout = sqc * rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
 }
 
-// VecJ entries of one zigzag segment (movdep.F90:209,233 with the tables of
-// vars.F90:328-355): flux F, segment midpoint W within its cell.
+// Shared-memory accesses with explicit .shared addressing (32-bit shared
+// addresses), so no generic-address resolution is left to run time.
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ float4 lds4(uint32_t a)
+{
+    float4 v;
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ float2 lds2(uint32_t a)
+{
+    float2 v;
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    return v;
+}
+__device__ __forceinline__ void red_shared(uint32_t a, int v)
+{
+    asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(a), "r"(v));
+}
+
+// round(v * S) for |v * S| <= 2^22 with one FMA: adding 1.5 * 2^23 leaves the
+// rounded integer in the low mantissa bits.
+__device__ __forceinline__ int fixed_of(float v, float S)
+{
+    return __float_as_int(fmaf(v, S, 12582912.f)) - 0x4B400000;
+}
+
+// Cell step of a position x in (-1, 2) relative to its cell: floor(x) as
+// -1, 0 or 1, and the same as float.
+__device__ __forceinline__ int cell_step(float x, float &fs)
+{
+    fs = x >= 1.f ? 1.f : (x < 0.f ? -1.f : 0.f);
+    return x >= 1.f ? 1 : (x < 0.f ? -1 : 0);
+}
+
+// One zigzag segment: flux F (charge x displacement) and the segment's
+// midpoint W within its cell (movdep.F90:187-233).
+struct Seg {
+    float Fx, Fy, Fz, Wx, Wy, Wz;
+};
+
+// VecJ entry e of a segment (movdep.F90:209,233 with the tables of
+// vars.F90:328-355): 3D e = 0..3 Jx, 4..7 Jy, 8..11 Jz; 2D e = 0..1 Jx,
+// 2..3 Jy, 4..7 Jz.
 template <int DIMS>
-__device__ __forceinline__ void segment_f32(float Fx, float Fy, float Fz, float Wx, float Wy, float Wz, float *o)
+__device__ __forceinline__ float seg_entry(const Seg &s, int e)
 {
     if (DIMS == 2) {
-        o[0] = Fx * (1.f - Wy);
-        o[1] = Fx * Wy;
-        o[2] = Fy * (1.f - Wx);
-        o[3] = Fy * Wx;
-        const float a = Fz * (1.f - Wx), b = Fz * Wx;
-        o[4] = a * (1.f - Wy);
-        o[5] = b * (1.f - Wy);
-        o[6] = a * Wy;
-        o[7] = b * Wy;
-    } else {
-        const float xa = Fx * (1.f - Wy), xb = Fx * Wy;
-        o[0] = xa * (1.f - Wz);
-        o[1] = xb * (1.f - Wz);
-        o[2] = xa * Wz;
-        o[3] = xb * Wz;
-        const float ya = Fy * (1.f - Wx), yb = Fy * Wx;
-        o[4] = ya * (1.f - Wz);
-        o[5] = yb * (1.f - Wz);
-        o[6] = ya * Wz;
-        o[7] = yb * Wz;
-        const float za = Fz * (1.f - Wx), zb = Fz * Wx;
-        o[8] = za * (1.f - Wy);
-        o[9] = zb * (1.f - Wy);
-        o[10] = za * Wy;
-        o[11] = zb * Wy;
+        switch (e) {
+            case 0: return s.Fx * (1.f - s.Wy);
+            case 1: return s.Fx * s.Wy;
+            case 2: return s.Fy * (1.f - s.Wx);
+            case 3: return s.Fy * s.Wx;
+            case 4: return (s.Fz * (1.f - s.Wx)) * (1.f - s.Wy);
+            case 5: return (s.Fz * s.Wx) * (1.f - s.Wy);
+            case 6: return (s.Fz * (1.f - s.Wx)) * s.Wy;
+            default: return (s.Fz * s.Wx) * s.Wy;
+        }
+    }
+    switch (e) {
+        case 0: return (s.Fx * (1.f - s.Wy)) * (1.f - s.Wz);
+        case 1: return (s.Fx * s.Wy) * (1.f - s.Wz);
+        case 2: return (s.Fx * (1.f - s.Wy)) * s.Wz;
+        case 3: return (s.Fx * s.Wy) * s.Wz;
+        case 4: return (s.Fy * (1.f - s.Wx)) * (1.f - s.Wz);
+        case 5: return (s.Fy * s.Wx) * (1.f - s.Wz);
+        case 6: return (s.Fy * (1.f - s.Wx)) * s.Wz;
+        case 7: return (s.Fy * s.Wx) * s.Wz;
+        case 8: return (s.Fz * (1.f - s.Wx)) * (1.f - s.Wy);
+        case 9: return (s.Fz * s.Wx) * (1.f - s.Wy);
+        case 10: return (s.Fz * (1.f - s.Wx)) * s.Wy;
+        default: return (s.Fz * s.Wx) * s.Wy;
     }
 }
 
-// Scatter of one segment's entries at base offset c0 of an array with row
-// stride sy and plane stride sz (movdep_routines.F90:276-303); A = atomics on
-// global or shared memory alike.
+// Offset of VecJ entry e from the cell's base offset and its component
+// (movdep_routines.F90:276-303): 0 = Jx, 1 = Jy, 2 = Jz.
 template <int DIMS>
-__device__ __forceinline__ void scatter_f32(float *Jx, float *Jy, float *Jz, long long c0, long long sy, long long sz,
-                                            const float *o)
+__device__ __forceinline__ int entry_offset(int e, int sy, int sz, int &comp)
 {
     if (DIMS == 2) {
-        atomicAdd(Jx + c0, o[0]);
-        atomicAdd(Jx + c0 + sy, o[1]);
-        atomicAdd(Jy + c0, o[2]);
-        atomicAdd(Jy + c0 + 1, o[3]);
-        atomicAdd(Jz + c0, o[4]);
-        atomicAdd(Jz + c0 + 1, o[5]);
-        atomicAdd(Jz + c0 + sy, o[6]);
-        atomicAdd(Jz + c0 + 1 + sy, o[7]);
-    } else {
-        atomicAdd(Jx + c0, o[0]);
-        atomicAdd(Jx + c0 + sy, o[1]);
-        atomicAdd(Jx + c0 + sz, o[2]);
-        atomicAdd(Jx + c0 + sy + sz, o[3]);
-        atomicAdd(Jy + c0, o[4]);
-        atomicAdd(Jy + c0 + 1, o[5]);
-        atomicAdd(Jy + c0 + sz, o[6]);
-        atomicAdd(Jy + c0 + 1 + sz, o[7]);
-        atomicAdd(Jz + c0, o[8]);
-        atomicAdd(Jz + c0 + 1, o[9]);
-        atomicAdd(Jz + c0 + sy, o[10]);
-        atomicAdd(Jz + c0 + 1 + sy, o[11]);
+        const int o[8] = {0, sy, 0, 1, 0, 1, sy, 1 + sy};
+        comp = e < 2 ? 0 : e < 4 ? 1 : 2;
+        return o[e];
+    }
+    const int o[12] = {0, sy, sz, sy + sz, 0, 1, sz, 1 + sz, 0, 1, sy, 1 + sy};
+    comp = e >> 2;
+    return o[e];
+}
+
+// Deposit of the two segments of one move into global J: segment 1 into the
+// cell c0 it starts in, segment 2 into the cell c1 the particle ends in; when
+// the move stays in its cell both are summed first and added once.
+template <int DIMS>
+__device__ __forceinline__ void deposit_f32(float *Jx, float *Jy, float *Jz, int c0, int c1, int sy, int sz,
+                                            const Seg &s1, const Seg &s2)
+{
+    constexpr int NE = DIMS == 3 ? 12 : 8;
+    float *J3[3] = {Jx, Jy, Jz};
+    const bool same = c0 == c1;
+#pragma unroll
+    for (int e = 0; e < NE; e++) {
+        int comp;
+        const int o = entry_offset<DIMS>(e, sy, sz, comp);
+        atomicAdd(J3[comp] + c0 + o, seg_entry<DIMS>(s1, e) + (same ? seg_entry<DIMS>(s2, e) : 0.f));
+    }
+    if (!same) {
+#pragma unroll
+        for (int e = 0; e < NE; e++) {
+            int comp;
+            const int o = entry_offset<DIMS>(e, sy, sz, comp);
+            atomicAdd(J3[comp] + c1 + o, seg_entry<DIMS>(s2, e));
+        }
+    }
+}
+
+// The same deposit into the shared current box of a brick (shared address
+// sJ0 of component 0; components njc words apart), as fixed-point integers
+// (v * S rounded to nearest) added with native shared-memory integer atomics;
+// S is chosen per brick so that no entry and no sum can overflow.
+template <int DIMS>
+__device__ __forceinline__ void deposit_box(uint32_t sJ0, int njc, int JX, int JXY, float S, int j0, int j1,
+                                            const Seg &s1, const Seg &s2)
+{
+    constexpr int NE = DIMS == 3 ? 12 : 8;
+    const bool same = j0 == j1;
+#pragma unroll
+    for (int e = 0; e < NE; e++) {
+        int comp;
+        const int o = entry_offset<DIMS>(e, JX, JXY, comp);
+        red_shared(sJ0 + 4u * (uint32_t)(comp * njc + j0 + o),
+                   fixed_of(seg_entry<DIMS>(s1, e) + (same ? seg_entry<DIMS>(s2, e) : 0.f), S));
+    }
+    if (!same) {
+#pragma unroll
+        for (int e = 0; e < NE; e++) {
+            int comp;
+            const int o = entry_offset<DIMS>(e, JX, JXY, comp);
+            red_shared(sJ0 + 4u * (uint32_t)(comp * njc + j1 + o), fixed_of(seg_entry<DIMS>(s2, e), S));
+        }
     }
 }
 
@@ -193,16 +279,16 @@ __device__ __forceinline__ int unwrap_offset(int i, int hc, int n)
     return u;
 }
 
-// Shared-memory view of a tile's box (unused by the per-particle kernel).
+// Shared-memory boxes of a brick (unused by the per-particle kernel).
 struct TileBox {
-    const float4 *nA;   // node E x,y,z, B x
-    const float2 *nB;   // node B y,z
-    float *sJ;          // current box, 3 planar components
+    uint32_t nA, nB;    // shared addresses: node E x,y,z, B x (16 B) / node B y,z (8 B)
+    uint32_t sJ;        // shared address of the current box (3 planar components, fixed point)
     int hc[3];          // brick centre (1-based interior indices)
     int lo[3];          // box lower corner, cells relative to hc
     int C[3];           // box extent in cells (1 on the unused z axis of 2D)
     int NX, NXY;        // node box strides
     int JX, JXY, njc;   // current box strides and size
+    float S;            // fixed-point scale of the current box
 };
 
 // Running bounds of the particles' new cells (relative to the brick centre).
@@ -217,20 +303,43 @@ struct Bounds {
     }
 };
 
-// Move one particle.  TILED: gather/deposit through the tile box when the
-// particle's cell is inside it; otherwise (and always when !TILED) through the
-// global arrays at the particle's wrapped cell.
-template <int DIMS, bool TILED>
-__device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint32_t n, const float *__restrict__ Ex,
-                                         const float *__restrict__ Ey, const float *__restrict__ Ez,
-                                         const float *__restrict__ Bx, const float *__restrict__ By,
-                                         const float *__restrict__ Bz, float *Jx, float *Jy, float *Jz, int *err,
-                                         const TileBox &tb, Bounds &bd)
+// One particle's state in registers.
+struct PState {
+    uint32_t key;
+    float dx, dy, dz, ux, uy, uz, w;
+};
+
+template <int DIMS>
+__device__ __forceinline__ PState load_state(const PartF32 &p, uint32_t n)
 {
-    const uint32_t key = p.key[n];
-    const int flv = (int)(key >> kFlvShift);
+    PState s;
+    s.key = p.key[n];
+    s.dx = p.dx[n];
+    s.dy = p.dy[n];
+    s.dz = DIMS == 3 ? p.dz[n] : 0.f;
+    s.ux = p.ux[n];
+    s.uy = p.uy[n];
+    s.uz = p.uz[n];
+    s.w = p.w[n];
+    return s;
+}
+
+// Move one particle (state s, slot n).  TILED: gather through the node box
+// when the particle's cell is inside it, else (and always when !TILED)
+// through the global arrays at the particle's wrapped cell.  The current of
+// a particle inside the box goes to the box; otherwise to the global J at the
+// wrapped cell (ghost layers included; the fold adds them to their periodic
+// images).
+template <int DIMS, bool TILED>
+__device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint32_t n, const PState &s,
+                                         const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                         const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                         const float *__restrict__ By, const float *__restrict__ Bz, float *Jx,
+                                         float *Jy, float *Jz, int *err, const TileBox &tb, Bounds &bd)
+{
+    const int flv = (int)(s.key >> kFlvShift);
     if (flv == 0) return;
-    const int cell = (int)(key & kCellMask);
+    const int cell = (int)(s.key & kCellMask);
     int i, j, k;
     decode_cell(g, cell, i, j, k);
     if (i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 || (DIMS == 3 && (k < 3 || k > g.mz - 3)) ||
@@ -238,10 +347,10 @@ __device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint3
         raise_error(err, PIC_DEVERR_RANGE);
         return;
     }
-    const float dx = p.dx[n], dy = p.dy[n], dz = DIMS == 3 ? p.dz[n] : 0.f;
+    const float dx = s.dx, dy = s.dy, dz = s.dz;
     float wt[8];
     weights_f32<DIMS>(dx, dy, dz, wt);
-    const long long sy = g.sy, sz = g.sz;
+    const int sy = (int)g.sy, sz = (int)g.sz;
     int uo[3] = {0, 0, 0};   // unwrapped offsets from the brick centre
     bool inside = false;
     int nb = 0;
@@ -259,75 +368,58 @@ __device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint3
 #pragma unroll
         for (int c8 = 0; c8 < (DIMS == 3 ? 8 : 4); c8++) {
             const int q = nb + (c8 & 1) + ((c8 >> 1) & 1) * tb.NX + ((c8 >> 2) & 1) * tb.NXY;
-            accum(wt[c8], tb.nA[q], tb.nB[q], pE, pB);
+            accum(wt[c8], lds4(tb.nA + 16u * (uint32_t)q), lds2(tb.nB + 8u * (uint32_t)q), pE, pB);
         }
     } else {
-        const float b0 = (float)g.bext[0], b1 = (float)g.bext[1], b2 = (float)g.bext[2];
 #pragma unroll
         for (int c8 = 0; c8 < (DIMS == 3 ? 8 : 4); c8++) {
-            const long long nd = (long long)cell + (c8 & 1) + ((c8 >> 1) & 1) * sy + ((c8 >> 2) & 1) * sz;
+            const int nd = cell + (c8 & 1) + ((c8 >> 1) & 1) * sy + ((c8 >> 2) & 1) * sz;
             float4 A;
             float2 Bv;
-            node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, b0, b1, b2, A, Bv);
+            node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
             accum(wt[c8], A, Bv, pE, pB);
         }
     }
-    const float qm = (float)g.qm[flv] * 0.5f;
+    const float qm = g.qm_half_f[flv];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
         pE[d] *= qm;
         pB[d] *= qm;
     }
-    float u = p.ux[n], v = p.uy[n], w = p.uz[n], gg;
-    boris_f32((float)g.c, (float)g.sqc, (float)g.cinv, pE, pB, u, v, w, gg);
+    float u = s.ux, v = s.uy, w = s.uz, gg;
+    boris_f32(g.c_f, g.sqc_f, g.cinv_f, pE, pB, u, v, w, gg);
     // displacement in cell units, positions relative to this cell's corner
     const float x1 = fmaf(u, gg, dx), y1 = fmaf(v, gg, dy), z1 = DIMS == 3 ? fmaf(w, gg, dz) : 0.f;
-    const int sxx = (int)floorf(x1), syy = (int)floorf(y1), szz = DIMS == 3 ? (int)floorf(z1) : 0;
+    // |displacement| < c < 1, so x1 lies in (-1, 2): the cell step is -1, 0 or 1
+    float fsx, fsy, fsz = 0.f;
+    const int sxx = cell_step(x1, fsx), syy = cell_step(y1, fsy), szz = DIMS == 3 ? cell_step(z1, fsz) : 0;
     // zigzag relay point with ip0 = 0, ip = s (movdep.F90:183-185)
-    const float xr = fminf((float)(min(0, sxx) + 1), fmaxf((float)max(0, sxx), 0.5f * (dx + x1)));
-    const float yr = fminf((float)(min(0, syy) + 1), fmaxf((float)max(0, syy), 0.5f * (dy + y1)));
-    const float qthis = p.w[n] * (float)g.qi;
+    const float xr = fminf(fminf(fsx, 0.f) + 1.f, fmaxf(fmaxf(fsx, 0.f), 0.5f * (dx + x1)));
+    const float yr = fminf(fminf(fsy, 0.f) + 1.f, fmaxf(fmaxf(fsy, 0.f), 0.5f * (dy + y1)));
+    const float qthis = s.w * g.qi_f;
     float Fz1, Fz2, Wz1 = 0.f, Wz2 = 0.f;
     if (DIMS == 3) {
-        const float zr = fminf((float)(min(0, szz) + 1), fmaxf((float)max(0, szz), 0.5f * (dz + z1)));
+        const float zr = fminf(fminf(fsz, 0.f) + 1.f, fmaxf(fmaxf(fsz, 0.f), 0.5f * (dz + z1)));
         Fz1 = qthis * (zr - dz);
         Fz2 = qthis * (z1 - zr);
         Wz1 = 0.5f * (dz + zr);
-        Wz2 = 0.5f * (z1 + zr) - (float)szz;
+        Wz2 = 0.5f * (z1 + zr) - fsz;
     } else {
         // out-of-plane motion: no cell crossing, the relay point is the midpoint
         Fz1 = qthis * (0.5f * (w * gg));
         Fz2 = Fz1;
     }
-    float o1[12], o2[12];
-    segment_f32<DIMS>(qthis * (xr - dx), qthis * (yr - dy), Fz1, 0.5f * (dx + xr), 0.5f * (dy + yr), Wz1, o1);
-    segment_f32<DIMS>(qthis * (x1 - xr), qthis * (y1 - yr), Fz2, 0.5f * (x1 + xr) - (float)sxx,
-                      0.5f * (y1 + yr) - (float)syy, Wz2, o2);
-    const bool same = (sxx | syy | szz) == 0;
+    const Seg s1 = {qthis * (xr - dx), qthis * (yr - dy), Fz1, 0.5f * (dx + xr), 0.5f * (dy + yr), Wz1};
+    const Seg s2 = {qthis * (x1 - xr), qthis * (y1 - yr), Fz2, 0.5f * (x1 + xr) - fsx, 0.5f * (y1 + yr) - fsy, Wz2};
     if (inside) {
         const int lx = uo[0] - tb.lo[0], ly = uo[1] - tb.lo[1], lz = DIMS == 3 ? uo[2] - tb.lo[2] : 0;
         const int jb = (lx + 1) + tb.JX * (ly + 1) + (DIMS == 3 ? tb.JXY * (lz + 1) : 0);
-        float *sJx = tb.sJ, *sJy = tb.sJ + tb.njc, *sJz = tb.sJ + 2 * tb.njc;
-        if (same) {
-#pragma unroll
-            for (int e = 0; e < (DIMS == 3 ? 12 : 8); e++) o1[e] += o2[e];
-            scatter_f32<DIMS>(sJx, sJy, sJz, jb, tb.JX, tb.JXY, o1);
-        } else {
-            scatter_f32<DIMS>(sJx, sJy, sJz, jb, tb.JX, tb.JXY, o1);
-            scatter_f32<DIMS>(sJx, sJy, sJz, jb + sxx + syy * tb.JX + szz * tb.JXY, tb.JX, tb.JXY, o2);
-        }
+        deposit_box<DIMS>(tb.sJ, tb.njc, tb.JX, tb.JXY, tb.S, jb, jb + sxx + syy * tb.JX + szz * tb.JXY, s1, s2);
     } else {
-        if (same) {
-#pragma unroll
-            for (int e = 0; e < (DIMS == 3 ? 12 : 8); e++) o1[e] += o2[e];
-            scatter_f32<DIMS>(Jx, Jy, Jz, cell, sy, sz, o1);
-        } else {
-            scatter_f32<DIMS>(Jx, Jy, Jz, cell, sy, sz, o1);
-            scatter_f32<DIMS>(Jx, Jy, Jz, (long long)cell + sxx + syy * sy + szz * sz, sy, sz, o2);
-        }
+        deposit_f32<DIMS>(Jx, Jy, Jz, cell, cell + sxx + syy * sy + szz * sz, sy, sz, s1, s2);
     }
     // new offsets and periodic cell index
-    float nx = x1 - (float)sxx, ny = y1 - (float)syy, nz = z1 - (float)szz;
+    float nx = x1 - fsx, ny = y1 - fsy, nz = z1 - fsz;
     int ax = sxx, ay = syy, az = szz;
     if (nx >= 1.f) { nx -= 1.f; ax += 1; }
     if (ny >= 1.f) { ny -= 1.f; ay += 1; }
@@ -348,6 +440,24 @@ __device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint3
     p.uz[n] = w;
 }
 
+// Particles [n0, n1) with stride `step`, the next particle prefetched.
+template <int DIMS, bool TILED>
+__device__ __forceinline__ void push_range(const GridP &g, const PartF32 &p, uint32_t n0, uint32_t n1, uint32_t step,
+                                           const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                           const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                           const float *__restrict__ By, const float *__restrict__ Bz, float *Jx,
+                                           float *Jy, float *Jz, int *err, const TileBox &tb, Bounds &bd)
+{
+    if (n0 >= n1) return;
+    PState cur = load_state<DIMS>(p, n0);
+    for (uint32_t n = n0; n < n1; n += step) {
+        PState nxt = cur;
+        if (n1 - n > step) nxt = load_state<DIMS>(p, n + step);
+        push_one<DIMS, TILED>(g, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+        cur = nxt;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Per-particle form (before the first reorder): grid-stride over the array.
 // ---------------------------------------------------------------------------
@@ -358,11 +468,11 @@ __global__ void __launch_bounds__(kThreads) k_move_f32(GridP g, PartF32 p, const
                                                        const float *__restrict__ By, const float *__restrict__ Bz,
                                                        float *Jx, float *Jy, float *Jz, int *err)
 {
-    const long long used = cnt->used;
     TileBox tb = {};
     Bounds bd;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x)
-        push_one<DIMS, false>(g, p, (uint32_t)n, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+    const uint32_t step = gridDim.x * blockDim.x;
+    push_range<DIMS, false>(g, p, blockIdx.x * blockDim.x + threadIdx.x, (uint32_t)cnt->used, step, Ex, Ey, Ez, Bx,
+                            By, Bz, Jx, Jy, Jz, err, tb, bd);
 }
 
 void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
@@ -381,13 +491,25 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // ---------------------------------------------------------------------------
 constexpr int kTileThreads = 256;
 constexpr int kTileWarps = kTileThreads / 32;
+constexpr int kBoxAxisMax = 64;   // cells per axis of a box (bricks are at most 32 + 2)
 
-// Shared floats a box of C cells needs: nodes (C+1) x 6 + current (C+3) x 3.
+// Shared words of a box of C cells: (C+1) nodes per axis x 6 field
+// components and (C+3) current cells per axis x 3 components.
 __host__ __device__ inline long long box_floats(int dims, int cx, int cy, int cz)
 {
     const long long nn = (long long)(cx + 1) * (cy + 1) * (dims == 3 ? cz + 1 : 1);
     const long long nj = (long long)(cx + 3) * (cy + 3) * (dims == 3 ? cz + 3 : 1);
     return 6 * nn + 3 * nj;
+}
+
+// Interior index of the unwrapped 1-based index a (no division when a is
+// already interior or one period away).
+__device__ __forceinline__ int interior_of(int a, int n)
+{
+    if (a < 3) a += n;
+    else if (a > n + 2) a -= n;
+    if (a < 3 || a > n + 2) a = wrap_interior(a, n);
+    return a;
 }
 
 template <int DIMS>
@@ -398,6 +520,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 {
     extern __shared__ __align__(16) float sm[];
     __shared__ int red[kTileWarps][6];
+    __shared__ int s_off[3][kBoxAxisMax + 3];
     const int b = blockIdx.x;
     const uint32_t p0 = bk.tile_start[b], p1 = bk.tile_start[b + 1];
     if (p0 >= p1) return;
@@ -423,7 +546,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     // box of this step: the stored bounds, or the brick +- 1 cell if too large
     const int *sb = bk.box + 8 * (size_t)b;
     int lo[3] = {sb[0], sb[1], DIMS == 3 ? sb[2] : 0}, hi[3] = {sb[3], sb[4], DIMS == 3 ? sb[5] : 0};
-    if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2] ||
+    if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2] || hi[0] - lo[0] >= kBoxAxisMax ||
+        hi[1] - lo[1] >= kBoxAxisMax || hi[2] - lo[2] >= kBoxAxisMax ||
         box_floats(DIMS, hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1) > bk.smem_floats) {
 #pragma unroll
         for (int d = 0; d < DIMS; d++) {
@@ -446,55 +570,70 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     tb.njc = JX * JY * JZ;
     float4 *nA = reinterpret_cast<float4 *>(sm);
     float2 *nB = reinterpret_cast<float2 *>(sm + 4 * nnode);
-    float *sJ = sm + 6 * nnode;
-    tb.nA = nA;
-    tb.nB = nB;
-    tb.sJ = sJ;
-    // stage node-averaged fields, one box row (fixed y,z) per warp pass
+    int *sJ = reinterpret_cast<int *>(sm + 6 * nnode);
+    tb.nA = smem_addr(nA);
+    tb.nB = smem_addr(nB);
+    tb.sJ = smem_addr(sJ);
+    // fixed-point scale: a particle adds at most b = |w| qi c to any entry
+    // (its displacement per axis is below c), so with S = 2^30 / (N b) no sum
+    // of the N particles exceeds 2^30; S <= 2^22 / b keeps each contribution
+    // below 2^22 (the range of fixed_of)
     {
-        const long long sy = g.sy, sz = g.sz;
-        const float b0 = (float)g.bext[0], b1 = (float)g.bext[1], b2 = (float)g.bext[2];
-        for (int r = warp; r < NY * NZ; r += kTileWarps) {
-            const int yy = r % NY, zz = r / NY;
-            const int bj = wrap_interior(tb.hc[1] + lo[1] + yy, g.ny);
-            const int ck = DIMS == 3 ? wrap_interior(tb.hc[2] + lo[2] + zz, g.nz) : 1;
-            const long long row = cidx(g, 1, bj, ck);
-            for (int xx = lane; xx < NX; xx += 32) {
-                const int ai = wrap_interior(tb.hc[0] + lo[0] + xx, g.nx);
-                float4 A;
-                float2 Bv;
-                node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, row + (ai - 1), sy, sz, b0, b1, b2, A, Bv);
-                nA[r * NX + xx] = A;
-                nB[r * NX + xx] = Bv;
-            }
+        const float b1 = g.c_f * g.qi_f * __uint_as_float(*bk.wmax_bits);
+        const float n = fmaxf((float)(p1 - p0), 256.f);
+        tb.S = b1 > 0.f ? 1073741824.f / (b1 * n) : 1.f;
+    }
+    // periodic offsets of the box cells lo-1 .. lo+C+1 along each axis
+    // (memory offset of the interior image, times the axis stride)
+    {
+        const int ext[3] = {JX, JY, JZ};
+        const int str[3] = {1, (int)g.sy, (int)g.sz};
+#pragma unroll
+        for (int d = 0; d < DIMS; d++)
+            for (int t = tid; t < ext[d]; t += kTileThreads)
+                s_off[d][t] = (interior_of(tb.hc[d] + lo[d] - 1 + t, n3[d]) - 1) * str[d];
+        if (DIMS == 2 && tid == 0) s_off[2][0] = 0;
+    }
+    for (int q = tid; q < 3 * tb.njc; q += kTileThreads) sJ[q] = 0;
+    __syncthreads();
+    // stage node-averaged fields: node q = xx + NX*(yy + NY*zz); q/NX and
+    // r/NY by multiply-high (exact for q < 2^16, NX, NY < 2^16)
+    {
+        const int sy = (int)g.sy, sz = (int)g.sz;
+        const uint32_t mX = 0xffffffffu / (uint32_t)NX + 1u, mY = 0xffffffffu / (uint32_t)NY + 1u;
+        for (int q = tid; q < nnode; q += kTileThreads) {
+            const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * NX;
+            const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * NY;
+            const int nd = s_off[0][xx + 1] + s_off[1][yy + 1] + (DIMS == 3 ? s_off[2][zz + 1] : 0);
+            float4 A;
+            float2 Bv;
+            node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
+            nA[q] = A;
+            nB[q] = Bv;
         }
     }
-    for (int q = tid; q < 3 * tb.njc; q += kTileThreads) sJ[q] = 0.f;
     __syncthreads();
 
     Bounds bd;
     bd.init();
-    for (uint32_t n = p0 + tid; n < p1; n += kTileThreads)
-        push_one<DIMS, true>(g, p, n, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+    push_range<DIMS, true>(g, p, p0 + tid, p1, kTileThreads, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
     __syncthreads();
 
     // add the box current to the periodic interior image of each cell
     {
-        const int rows = JY * JZ;
-        for (int r = warp; r < 3 * rows; r += kTileWarps) {
-            const int comp = r / rows, rr = r - comp * rows;
-            const int yy = rr % JY, zz = rr / JY;
-            const int bj = wrap_interior(tb.hc[1] + lo[1] - 1 + yy, g.ny);
-            const int ck = DIMS == 3 ? wrap_interior(tb.hc[2] + lo[2] - 1 + zz, g.nz) : 1;
-            float *J = comp == 0 ? Jx : comp == 1 ? Jy : Jz;
-            const long long row = cidx(g, 1, bj, ck);
-            const float *src = sJ + (size_t)comp * tb.njc + (size_t)rr * JX;
-            for (int xx = lane; xx < JX; xx += 32) {
-                const float val = src[xx];
-                if (val != 0.f) atomicAdd(J + row + (wrap_interior(tb.hc[0] + lo[0] - 1 + xx, g.nx) - 1), val);
-            }
+        const float inv = 1.f / tb.S;
+        const uint32_t mX = 0xffffffffu / (uint32_t)JX + 1u, mY = 0xffffffffu / (uint32_t)JY + 1u;
+        for (int q = tid; q < tb.njc; q += kTileThreads) {
+            const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * JX;
+            const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * JY;
+            const int off = s_off[0][xx] + s_off[1][yy] + (DIMS == 3 ? s_off[2][zz] : 0);
+            const int vx = sJ[q], vy = sJ[tb.njc + q], vz = sJ[2 * tb.njc + q];
+            if (vx != 0) atomicAdd(Jx + off, (float)vx * inv);
+            if (vy != 0) atomicAdd(Jy + off, (float)vy * inv);
+            if (vz != 0) atomicAdd(Jz + off, (float)vz * inv);
         }
     }
+
     // bounds of the new cells -> box of the next step (the brick itself if empty)
     int v[6] = {bd.lo[0], bd.lo[1], bd.lo[2], -bd.hi[0], -bd.hi[1], -bd.hi[2]};
 #pragma unroll
@@ -503,19 +642,26 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 #pragma unroll
         for (int e = 0; e < 6; e++) red[warp][e] = v[e];
     __syncthreads();
-    if (tid < 6) {
-        int m = red[0][tid];
-        for (int w = 1; w < kTileWarps; w++) m = min(m, red[w][tid]);
+    if (tid == 0) {
+        int m[6];
+        for (int e = 0; e < 6; e++) {
+            m[e] = red[0][e];
+            for (int w2 = 1; w2 < kTileWarps; w2++) m[e] = min(m[e], red[w2][e]);
+        }
         int *ob = bk.box + 8 * (size_t)b;
-        const int d = tid % 3;
-        const bool empty = red[0][0] == 0x3fffffff && [&] {
-            for (int w = 1; w < kTileWarps; w++)
-                if (red[w][0] != 0x3fffffff) return false;
-            return true;
-        }();
-        if (d >= DIMS) ob[tid] = 0;
-        else if (empty) ob[tid] = tid < 3 ? home_lo[d] : home_hi[d];
-        else ob[tid] = tid < 3 ? m : -m;
+        const bool empty = m[0] == 0x3fffffff;
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            if (d >= DIMS) {
+                ob[d] = ob[d + 3] = 0;
+            } else if (empty) {
+                ob[d] = home_lo[d];
+                ob[d + 3] = home_hi[d];
+            } else {
+                ob[d] = m[d];
+                ob[d + 3] = -m[d + 3];
+            }
+        }
     }
 }
 
