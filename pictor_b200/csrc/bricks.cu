@@ -46,6 +46,7 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, Pa
     const long long used = cnt->used;
     const int lane = threadIdx.x & 31;
     const long long stride = (long long)gridDim.x * blockDim.x;
+    uint32_t wmax = 0;   // max |w| bits seen by this thread
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < used; base += stride) {
         const long long n = base + lane;
         uint32_t b = kNoBrick, wbits = 0;
@@ -66,8 +67,17 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, Pa
         }
         const uint32_t peers = __match_any_sync(0xffffffffu, b);
         if (b != kNoBrick && (peers & lanemask_lt_b()) == 0) atomicAdd(&bk.count[b], (uint32_t)__popc(peers));
-        wbits = __reduce_max_sync(0xffffffffu, wbits);   // |w| bit patterns order as integers
-        if (lane == 0 && wbits) atomicMax(bk.wmax_bits, wbits);
+        wmax = max(wmax, wbits);   // |w| bit patterns order as integers
+    }
+    // one atomic per block
+    __shared__ uint32_t s_w[kThreads / 32];
+    wmax = __reduce_max_sync(0xffffffffu, wmax);
+    if (lane == 0) s_w[threadIdx.x >> 5] = wmax;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t m = 0;
+        for (int w = 0; w < kThreads / 32; w++) m = max(m, s_w[w]);
+        if (m) atomicMax(bk.wmax_bits, m);
     }
 }
 
