@@ -39,6 +39,10 @@ WORKLOADS = {
     # a small case of the headline physics for profiler captures (particles 270 MB > L2)
     "weibel3d_fp32_small": dict(dims=3, nx=128, ny=64, nz=64, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
                                 precision="fp32"),
+    # the batched ensemble: 64 independent 2D Weibel runs, grid 64^2..512^2, 4..32 particles per cell per
+    # species, drift U(0.1, 0.9) c, spread U(0.01, 0.1) c, seed 2930 + run (pictor_b200.ensemble)
+    "ensemble64": dict(dims=2, runs=64, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0, precision="fp32",
+                       nx=256, ny=256, nz=1),
 }
 SEED = 2930
 
@@ -251,6 +255,110 @@ def cpu_sample(wl: dict, target_s: float = 12.0, threads: int | None = None):
                       f"(same physics and seed), FP64, C restatement of the reference CPU path with OpenMP"}
 
 
+def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
+    """--workload ensemble64: this rank's share of the 64 runs (largest-first
+    plan), stepped together with pic_step_many after the per-size-class
+    autotuner, against the same runs in the plain FP64 form one at a time."""
+    import torch
+
+    from pictor_b200.ensemble import ensemble_runs, partition, run_batched, tune_classes
+
+    wl = WORKLOADS[args.workload]
+    runs = ensemble_runs(wl["runs"], steps=args.steps)
+    mine = [runs[i] for i in partition(runs, ws)[rank]]
+    t0 = time.perf_counter()
+    tunings = tune_classes(mine)
+    tune_s = time.perf_counter() - t0
+    run_batched(mine, args.warmup, "fp32", tunings)                      # warm-up (graph capture, clocks)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    res32, t32 = run_batched(mine, args.steps, "fp32", tunings)
+    barrier(ws)
+    clk = clocks.stop()
+    secs = max_over_ranks(ws, t32["seconds"])
+    ps = sum_over_ranks(ws, t32["particle_steps"])
+    value = ps / secs
+    fp64 = None
+    if not args.no_fp64:
+        res64, t64 = run_batched(mine, args.steps, "fp64", None, batched=False)
+        secs64 = max_over_ranks(ws, t64["seconds"])
+        v64 = sum_over_ranks(ws, t64["particle_steps"]) / secs64
+        err_f = max(abs((a["B2"] + a["E2"]) - (b["B2"] + b["E2"])) / max(b["B2"] + b["E2"], 1e-300)
+                    for a, b in zip(res32, res64))
+        err_t = max(abs((0.5 * (a["B2"] + a["E2"]) + sum(a["kinetic"])) - (0.5 * (b["B2"] + b["E2"]) + sum(b["kinetic"])))
+                    / abs(0.5 * (b["B2"] + b["E2"]) + sum(b["kinetic"])) for a, b in zip(res32, res64))
+        fp64 = {"value": v64, "seconds": secs64, "speedup_fp32_batched_over_fp64": value / v64,
+                "max_field_energy_rel_err": err_f, "max_total_energy_rel_err": err_t,
+                "form": "plain FP64 reference layout, runs stepped one after the other"}
+    # end to end: particles from pinned FP64 host arrays for every run, the steps, the diagnostics
+    from pictor_b200.ensemble import make_run, size_class
+    from pictor_b200.simulation import step_many
+
+    sims, hosts = [], []
+    for spec in mine:
+        sim, sc = make_run(spec, "fp32", tunings.get(size_class(spec)))
+        p = sim.fetch_particles()
+        hosts.append(type(p)(*(torch.from_numpy(getattr(p, k)).pin_memory().numpy()
+                               for k in ("q", "x", "y", "z", "u", "v", "w", "flv"))))
+        sims.append((sim, sc))
+    h2d = sum(len(h.x) for h in hosts) * (7 * 8 + 4)
+    barrier(ws)
+    torch.cuda.synchronize()
+    te = time.perf_counter()
+    for (sim, _), hp in zip(sims, hosts):
+        sim.load_particles(hp)
+        sim.reorder()
+    step_many([s for s, _ in sims], args.steps)
+    for sim, sc in sims:
+        sim.diagnostics(sc["masse"])
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(ws, time.perf_counter() - te)
+    for sim, _ in sims:
+        sim.close()
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        from oracle import oracle as O
+
+        O.build()
+        cpu = cpu_sample(wl)
+    n_bytes = sum(2 * r.ppc * r.nx * r.ny * bytes_per_particle(2, "fp32") + r.nx * r.ny * bytes_per_cell_mover("fp32")
+                  for r in mine)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": secs / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "ensemble64", "runs": wl["runs"], "runs_this_rank": len(mine),
+                       "grids": "64^2..512^2", "ppc_per_species": "4..32", "seed": "2930 + run",
+                       "parallelism": f"ensemble shards over {ws} rank(s)", "autotune_seconds": tune_s,
+                       "tunings": {f"{k[0]}x{k[1]}/ppc{k[2]}": {"brick": list(v.brick[:2]),
+                                                                 "reorder_period": v.reorder_period}
+                                   for k, v in tunings.items()},
+                       "l2": "run state of the rank (GBs) larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": n_bytes * args.steps / t32["seconds"] / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": n_bytes * args.steps / t32["seconds"] / 1e9 / peak,
+                         "traffic": None, "kernel": "batched step (k_move_f32_tiled<2> dominant), aggregate",
+                         "peak_kind": peak_kind},
+            "gpu_launches": t32["launches"],
+            "clocks": clk,
+            "e2e": {"value": ps / e2e_s, "unit": "particle-steps/s", "h2d_bytes_per_step": h2d / args.steps,
+                    "d2h_bytes_per_step": 8 * 6 * len(mine) / args.steps, "seconds": e2e_s,
+                    "includes": "pic_load_particles of every run from pinned FP64 host arrays + reorder + "
+                                "pic_step_many + pic_diagnostics"},
+        }
+        if fp64:
+            line["fp64"] = fp64
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU algorithm (C restatement of the
     Fortran CPU path; the Fortran build is not available here) on the host."""
@@ -296,6 +404,9 @@ def main():
 
     build.build()
     ws, rank, local = dist_setup(args.gpus)
+    if args.workload == "ensemble64":
+        peak, peak_kind = measured_peaks()
+        return run_ensemble_bench(args, ws, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]
     prec = wl["precision"]
     seed = SEED + rank

@@ -70,7 +70,11 @@ typedef struct {
        in the domain (parameters.F90:65). */
     double rmin;
     int32_t inc_axis;
-    int32_t reserved[7];
+    /* FP32 form: brick shape in interior cells (the unit of the reorder and
+       of one CTA of the mover); 0 = chosen from the fill (capacity / cells).
+       No counterpart in the reference, whose reorder is per cell. */
+    int32_t brick[3];
+    int32_t reserved[4];
 } pic_config;
 
 typedef struct pic_handle pic_handle;
@@ -125,6 +129,15 @@ int pic_filter_current(pic_handle *h);
    counted from the handle's step counter), captured once as a CUDA graph. */
 int pic_step(pic_handle *h, int32_t nsteps);
 int pic_set_step(pic_handle *h, int64_t t);
+
+/* The batched form of pic_step for an ensemble of independent runs (no
+   counterpart in the reference, which runs one simulation per job): nsteps
+   steps of each of the n handles, enqueued step by step across the handles,
+   each on its own stream, so that the step graphs of small runs execute
+   concurrently on the GPU.  All handles must belong to the current device.
+   Returns the first error of any handle; handles in profiling mode are
+   stepped one after the other. */
+int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps);
 
 /* Diagnostics (savedata_routines.F90:265-348), FP64 accumulation on device:
    out[0] = sum |B|^2, out[1] = sum |E|^2 over the interior (CalcFldEnergy),

@@ -43,7 +43,7 @@ class Config(C.Structure):
         ("qm", C.c_double * (MAX_FLVR + 1)),
         ("reorder_period", C.c_int32), ("curr_filter", C.c_int32),
         ("capacity", C.c_int64),
-        ("rmin", C.c_double), ("inc_axis", C.c_int32), ("reserved", C.c_int32 * 7),
+        ("rmin", C.c_double), ("inc_axis", C.c_int32), ("brick", C.c_int32 * 3), ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -101,6 +101,7 @@ SIGNATURES = {
     "pic_reorder": (C.c_int, [H]),
     "pic_filter_current": (C.c_int, [H]),
     "pic_step": (C.c_int, [H, C.c_int32]),
+    "pic_step_many": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),
     "pic_set_step": (C.c_int, [H, C.c_int64]),
     "pic_diagnostics": (C.c_int, [H, C.c_double, PD, C.c_int32]),
     "pic_device_errors": (C.c_int, [H, PI32]),

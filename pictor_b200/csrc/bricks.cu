@@ -160,22 +160,31 @@ void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Co
 
 // Brick shape for a fill of ppc particles per cell: about 4096 particles per
 // brick, x first, up to 8x8x8 (3D) / 32x32 (2D) so that the boxes of the
-// brick plus one cell of margin always fit the mover's shared memory.
-void choose_bricks(const GridP &g, double ppc, Bricks &bk)
+// brick plus one cell of margin always fit the mover's shared memory; or the
+// requested shape, checked against the same limit.
+bool choose_bricks(const GridP &g, double ppc, const int req[3], Bricks &bk)
 {
     static const int s3[][3] = {{4, 4, 4}, {8, 4, 4}, {8, 8, 4}, {8, 8, 8}};
     static const int s2[][3] = {{8, 8, 1}, {16, 8, 1}, {16, 16, 1}, {32, 16, 1}, {32, 32, 1}};
-    const double target = 4096.0 / (ppc > 0.5 ? ppc : 0.5);
-    const int ns = g.dims == 3 ? 4 : 5;
-    int pick = ns - 1;
-    for (int q = 0; q < ns; q++) {
-        const int *t = g.dims == 3 ? s3[q] : s2[q];
-        if ((double)t[0] * t[1] * t[2] >= target) {
-            pick = q;
-            break;
+    int t[3];
+    if (req && req[0] > 0) {
+        for (int d = 0; d < 3; d++) t[d] = d < g.dims ? req[d] : 1;
+        for (int d = 0; d < g.dims; d++)
+            if (t[d] < 1) return false;
+    } else {
+        const double target = 4096.0 / (ppc > 0.5 ? ppc : 0.5);
+        const int ns = g.dims == 3 ? 4 : 5;
+        int pick = ns - 1;
+        for (int q = 0; q < ns; q++) {
+            const int *c = g.dims == 3 ? s3[q] : s2[q];
+            if ((double)c[0] * c[1] * c[2] >= target) {
+                pick = q;
+                break;
+            }
         }
+        const int *c = g.dims == 3 ? s3[pick] : s2[pick];
+        for (int d = 0; d < 3; d++) t[d] = c[d];
     }
-    const int *t = g.dims == 3 ? s3[pick] : s2[pick];
     const int n3[3] = {g.nx, g.ny, g.nz};
     for (int d = 0; d < 3; d++) {
         bk.t[d] = d < g.dims ? (t[d] < n3[d] ? t[d] : n3[d]) : 1;
@@ -183,6 +192,10 @@ void choose_bricks(const GridP &g, double ppc, Bricks &bk)
     }
     bk.ntiles = bk.nb[0] * bk.nb[1] * bk.nb[2];
     bk.smem_floats = kBrickSmemBytes / 4;
+    // the fallback box (brick + 1 cell per side) must fit
+    for (int d = 0; d < g.dims; d++)
+        if (bk.t[d] + 2 > kBoxAxisMax) return false;
+    return box_floats(g.dims, bk.t[0] + 2, bk.t[1] + 2, g.dims == 3 ? bk.t[2] + 2 : 1) <= bk.smem_floats;
 }
 
 }  // namespace pic

@@ -42,6 +42,13 @@ struct pic_handle {
     long long launches = 0;   // kernels launched by pic_step since the last pic_launch_count
     // FP32 bricks (tile ranges valid while `sorted`: set by a reorder, cleared by loads)
     Bricks bricks = {};
+    // host <-> device staging of the FP32 form (allocated at the first load or
+    // fetch): two device buffers so that the copies of one chunk, on the copy
+    // stream, overlap the conversion kernel of the other, on h->s
+    cudaStream_t cs = nullptr;
+    char *stage[2] = {nullptr, nullptr};
+    size_t stage_bytes = 0;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
     bool sorted = false;
     std::vector<void *> allocs;
 };
@@ -344,6 +351,26 @@ void set_sorted(pic_handle *h, bool sorted)
             }
 }
 
+// One step of pic_step as a graph launch on h->s (graphs captured on first use).
+int enqueue_graph_step(pic_handle *h)
+{
+    h->t += 1;
+    const bool reorder = h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0;
+    cudaGraphExec_t ge = nullptr;
+    int r = get_graph(h, h->cur, reorder, &ge);
+    if (r) return r;
+    CK(cudaGraphLaunch(ge, h->s));
+    h->launches += h->graph_kernels[reorder ? 1 : 0][h->cur];
+    if (reorder) {
+        h->cur ^= 1;
+        if (h->fp32 && !h->sorted) {  // tile ranges are valid from now on
+            CK(cudaStreamSynchronize(h->s));
+            set_sorted(h, true);
+        }
+    }
+    return PIC_OK;
+}
+
 size_t field_bytes(const pic_handle *h) { return (size_t)h->g.ncell * (h->fp32 ? sizeof(float) : sizeof(double)); }
 
 int alloc_particles(pic_handle *h)
@@ -369,27 +396,85 @@ int alloc_particles(pic_handle *h)
     return PIC_OK;
 }
 
-// Temporary FP64 particle buffers for converting FP32 state in chunks.
-constexpr long long kConvChunk = 1ll << 24;
+// Staging of the FP32 form: chunks of at most kConvChunk particles (60 B each
+// in the reference layout) or kFieldChunk field values.
+constexpr long long kConvChunk = 1ll << 23;
+constexpr long long kFieldChunk = 1ll << 24;
+constexpr size_t kPartBytes = 7 * sizeof(double) + sizeof(int32_t);
 
-struct TmpF64 {
-    PartF64 p = {};
-    void *base = nullptr;
-    int alloc(long long n)
-    {
-        const size_t sz = (size_t)n * (7 * sizeof(double) + sizeof(int32_t));
-        cudaError_t e = cudaMalloc(&base, sz);
-        if (e != cudaSuccess) return cuda_status(e);
-        double *d = (double *)base;
-        p.q = d; p.x = d + n; p.y = d + 2 * n; p.z = d + 3 * n; p.u = d + 4 * n; p.v = d + 5 * n; p.w = d + 6 * n;
-        p.flv = (int32_t *)(d + 7 * n);
-        return PIC_OK;
+int ensure_stage(pic_handle *h)
+{
+    if (h->stage[0]) return PIC_OK;
+    const long long np = h->capacity < kConvChunk ? (h->capacity > 0 ? h->capacity : 1) : kConvChunk;
+    const long long nf = h->g.ncell < kFieldChunk ? h->g.ncell : kFieldChunk;
+    size_t bytes = (size_t)np * kPartBytes;
+    if ((size_t)nf * sizeof(double) > bytes) bytes = (size_t)nf * sizeof(double);
+    for (int b = 0; b < 2; b++) {
+        int r = dalloc(h, &h->stage[b], bytes);
+        if (r) return r;
+        CK(cudaEventCreateWithFlags(&h->ev_copied[b], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&h->ev_done[b], cudaEventDisableTiming));
     }
-    ~TmpF64()
-    {
-        if (base) cudaFree(base);
+    CK(cudaStreamCreateWithFlags(&h->cs, cudaStreamNonBlocking));
+    h->stage_bytes = bytes;
+    return PIC_OK;
+}
+
+// Particles of chunk size m in staging buffer b, reference layout.
+PartF64 stage_particles(pic_handle *h, int b, long long m)
+{
+    PartF64 p;
+    double *d = (double *)h->stage[b];
+    p.q = d; p.x = d + m; p.y = d + 2 * m; p.z = d + 3 * m; p.u = d + 4 * m; p.v = d + 5 * m; p.w = d + 6 * m;
+    p.flv = (int32_t *)(d + 7 * m);
+    return p;
+}
+
+long long stage_particle_chunk(const pic_handle *h) { return (long long)(h->stage_bytes / kPartBytes); }
+long long stage_field_chunk(const pic_handle *h) { return (long long)(h->stage_bytes / sizeof(double)); }
+
+// Host FP64 array -> device FP32 array through the staging buffers.
+int load_array_f32(pic_handle *h, const double *src, float *dst, long long n, int &k)
+{
+    const long long chunk = stage_field_chunk(h);
+    for (long long o = 0; o < n; o += chunk, k++) {
+        const int b = k & 1;
+        const long long m = (n - o) < chunk ? (n - o) : chunk;
+        double *t = (double *)h->stage[b];
+        CK(cudaStreamWaitEvent(h->cs, h->ev_done[b], 0));
+        CK(cudaMemcpyAsync(t, src + o, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, h->cs));
+        CK(cudaEventRecord(h->ev_copied[b], h->cs));
+        CK(cudaStreamWaitEvent(h->s, h->ev_copied[b], 0));
+        launch_array_f64_to_f32(t, dst + o, m, h->s);
+        CK(cudaEventRecord(h->ev_done[b], h->s));
     }
-};
+    return PIC_OK;
+}
+
+// Device FP32 array -> host FP64 array through the staging buffers.
+int fetch_array_f32(pic_handle *h, const float *src, double *dst, long long n, int &k)
+{
+    const long long chunk = stage_field_chunk(h);
+    for (long long o = 0; o < n; o += chunk, k++) {
+        const int b = k & 1;
+        const long long m = (n - o) < chunk ? (n - o) : chunk;
+        double *t = (double *)h->stage[b];
+        CK(cudaStreamWaitEvent(h->s, h->ev_copied[b], 0));
+        launch_array_f32_to_f64(src + o, t, m, h->s);
+        CK(cudaEventRecord(h->ev_done[b], h->s));
+        CK(cudaStreamWaitEvent(h->cs, h->ev_done[b], 0));
+        CK(cudaMemcpyAsync(dst + o, t, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, h->cs));
+        CK(cudaEventRecord(h->ev_copied[b], h->cs));
+    }
+    return PIC_OK;
+}
+
+int sync_both(pic_handle *h)
+{
+    CK(cudaStreamSynchronize(h->s));
+    if (h->cs) CK(cudaStreamSynchronize(h->cs));
+    return PIC_OK;
+}
 
 }  // namespace
 
@@ -417,10 +502,16 @@ void pic_destroy(pic_handle *h)
 {
     if (!h) return;
     if (h->s) cudaStreamSynchronize(h->s);
+    if (h->cs) cudaStreamSynchronize(h->cs);
     for (auto &row : h->graph)
         for (auto &ge : row)
             if (ge) cudaGraphExecDestroy(ge);
+    for (int b = 0; b < 2; b++) {
+        if (h->ev_copied[b]) cudaEventDestroy(h->ev_copied[b]);
+        if (h->ev_done[b]) cudaEventDestroy(h->ev_done[b]);
+    }
     for (void *p : h->allocs) cudaFree(p);
+    if (h->cs) cudaStreamDestroy(h->cs);
     if (h->s) cudaStreamDestroy(h->s);
     delete h;
 }
@@ -514,9 +605,9 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (!r && h->fp32) {
         // bricks sized for the configured fill (capacity / interior cells)
         Bricks &bk = h->bricks;
-        choose_bricks(g, (double)h->capacity / ((double)g.nx * g.ny * g.nz), bk);
+        if (!choose_bricks(g, (double)h->capacity / ((double)g.nx * g.ny * g.nz), c.brick, bk)) r = PIC_ERR_INVALID;
         const size_t nt = (size_t)bk.ntiles;
-        if ((r = dalloc(h, &bk.tile_start, nt + 1)) || (r = dalloc(h, &bk.box, 8 * nt)) ||
+        if (r || (r = dalloc(h, &bk.tile_start, nt + 1)) || (r = dalloc(h, &bk.box, 8 * nt)) ||
             (r = dalloc(h, &bk.count, nt + 1)) || (r = dalloc(h, &bk.cursor, nt)) ||
             (r = dalloc(h, &bk.bid, (size_t)h->capacity)) || (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1))) ||
             (r = dalloc(h, &bk.wmax_bits, 1))) {
@@ -574,19 +665,22 @@ int pic_load_fields(pic_handle *h, const double *Ex, const double *Ey, const dou
     const double *src[6] = {Ex, Ey, Ez, Bx, By, Bz};
     void *dst[6] = {h->E[0], h->E[1], h->E[2], h->B[0], h->B[1], h->B[2]};
     const size_t n = (size_t)h->g.ncell;
-    std::vector<float> tmp;
+    if (h->fp32) {
+        int r = ensure_stage(h);
+        if (r) return r;
+    }
+    int seq = 0;   // running chunk number: staging buffer seq % 2
     for (int k = 0; k < 6; k++) {
         if (!src[k]) continue;
         if (!h->fp32) {
             CK(cudaMemcpyAsync(dst[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice, h->s));
-            CK(cudaStreamSynchronize(h->s));
         } else {
-            tmp.resize(n);
-            for (size_t i = 0; i < n; i++) tmp[i] = (float)src[k][i];
-            CK(cudaMemcpyAsync(dst[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->s));
-            CK(cudaStreamSynchronize(h->s));
+            int r = load_array_f32(h, src[k], (float *)dst[k], (long long)n, seq);
+            if (r) return r;
         }
     }
+    int r = sync_both(h);
+    if (r) return r;
     return finish(h);
 }
 
@@ -595,18 +689,22 @@ int pic_load_current(pic_handle *h, const double *Jx, const double *Jy, const do
     if (!h) return PIC_ERR_INVALID;
     const double *src[3] = {Jx, Jy, Jz};
     const size_t n = (size_t)h->g.ncell;
-    std::vector<float> tmp;
+    if (h->fp32) {
+        int r = ensure_stage(h);
+        if (r) return r;
+    }
+    int seq = 0;   // running chunk number: staging buffer seq % 2
     for (int k = 0; k < 3; k++) {
         if (!src[k]) continue;
         if (!h->fp32) {
             CK(cudaMemcpyAsync(h->J[k], src[k], n * sizeof(double), cudaMemcpyHostToDevice, h->s));
         } else {
-            tmp.resize(n);
-            for (size_t i = 0; i < n; i++) tmp[i] = (float)src[k][i];
-            CK(cudaMemcpyAsync(h->J[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice, h->s));
+            int r = load_array_f32(h, src[k], (float *)h->J[k], (long long)n, seq);
+            if (r) return r;
         }
-        CK(cudaStreamSynchronize(h->s));
     }
+    int r = sync_both(h);
+    if (r) return r;
     return finish(h);
 }
 
@@ -617,19 +715,22 @@ int pic_fetch_fields(pic_handle *h, double *Ex, double *Ey, double *Ez, double *
     double *dst[9] = {Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz};
     void *src[9] = {h->E[0], h->E[1], h->E[2], h->B[0], h->B[1], h->B[2], h->J[0], h->J[1], h->J[2]};
     const size_t n = (size_t)h->g.ncell;
-    std::vector<float> tmp;
-    CK(cudaStreamSynchronize(h->s));
+    if (h->fp32) {
+        int r = ensure_stage(h);
+        if (r) return r;
+    }
+    int seq = 0;   // running chunk number: staging buffer seq % 2
     for (int k = 0; k < 9; k++) {
         if (!dst[k]) continue;
         if (!h->fp32) {
             CK(cudaMemcpyAsync(dst[k], src[k], n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
         } else {
-            tmp.resize(n);
-            CK(cudaMemcpyAsync(tmp.data(), src[k], n * sizeof(float), cudaMemcpyDeviceToHost, h->s));
-            CK(cudaStreamSynchronize(h->s));
-            for (size_t i = 0; i < n; i++) dst[k][i] = (double)tmp[i];
+            int r = fetch_array_f32(h, (const float *)src[k], dst[k], (long long)n, seq);
+            if (r) return r;
         }
     }
+    int r = sync_both(h);
+    if (r) return r;
     return finish(h);
 }
 
@@ -655,23 +756,32 @@ int pic_load_particles(pic_handle *h, int64_t n, const double *q, const double *
         for (int k = 0; k < 7; k++)
             if (n) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)n * sizeof(double), cudaMemcpyHostToDevice, h->s));
         if (n) CK(cudaMemcpyAsync(p.flv, flv, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, h->s));
-    } else {
-        TmpF64 tmp;
-        const long long chunk = n < kConvChunk ? (n > 0 ? n : 1) : kConvChunk;
-        int r = tmp.alloc(chunk);
+    } else if (n > 0) {
+        // chunk k: copies on the copy stream into staging buffer k%2 while
+        // chunk k-1 converts on h->s
+        int r = ensure_stage(h);
         if (r) return r;
-        for (long long o = 0; o < n; o += chunk) {
+        const long long chunk = stage_particle_chunk(h);
+        int k = 0;
+        for (long long o = 0; o < n; o += chunk, k++) {
+            const int b = k & 1;
             const long long m = (n - o) < chunk ? (n - o) : chunk;
-            double *dst[7] = {tmp.p.q, tmp.p.x, tmp.p.y, tmp.p.z, tmp.p.u, tmp.p.v, tmp.p.w};
-            for (int k = 0; k < 7; k++)
-                CK(cudaMemcpyAsync(dst[k], src[k] + o, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, h->s));
-            CK(cudaMemcpyAsync(tmp.p.flv, flv + o, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, h->s));
+            const PartF64 t = stage_particles(h, b, chunk);
+            double *dst[7] = {t.q, t.x, t.y, t.z, t.u, t.v, t.w};
+            CK(cudaStreamWaitEvent(h->cs, h->ev_done[b], 0));
+            for (int a = 0; a < 7; a++)
+                CK(cudaMemcpyAsync(dst[a], src[a] + o, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, h->cs));
+            CK(cudaMemcpyAsync(t.flv, flv + o, (size_t)m * sizeof(int32_t), cudaMemcpyHostToDevice, h->cs));
+            CK(cudaEventRecord(h->ev_copied[b], h->cs));
+            CK(cudaStreamWaitEvent(h->s, h->ev_copied[b], 0));
             PartF32 d = h->p32[h->cur];
             d.key += o; d.dx += o; d.dy += o; if (d.dz) d.dz += o;
             d.ux += o; d.uy += o; d.uz += o; d.w += o;
-            launch_f64_to_f32(h->g, tmp.p, d, m, h->err, h->s);
-            CK(cudaStreamSynchronize(h->s));
+            launch_f64_to_f32(h->g, t, d, m, h->err, h->s);
+            CK(cudaEventRecord(h->ev_done[b], h->s));
         }
+        r = sync_both(h);
+        if (r) return r;
     }
     Counters c0 = {};
     c0.used = n;
@@ -696,23 +806,32 @@ int pic_fetch_particles(pic_handle *h, int64_t *nout, double *q, double *x, doub
         for (int k = 0; k < 7; k++)
             if (dst[k] && n) CK(cudaMemcpyAsync(dst[k], src[k], (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, h->s));
         if (flv && n) CK(cudaMemcpyAsync(flv, p.flv, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
-    } else {
-        TmpF64 tmp;
-        const long long chunk = n < kConvChunk ? (n > 0 ? n : 1) : kConvChunk;
-        r = tmp.alloc(chunk);
+    } else if (n > 0) {
+        // chunk k: converts on h->s into staging buffer k%2 while chunk k-1
+        // copies out on the copy stream
+        r = ensure_stage(h);
         if (r) return r;
-        for (long long o = 0; o < n; o += chunk) {
+        const long long chunk = stage_particle_chunk(h);
+        int k = 0;
+        for (long long o = 0; o < n; o += chunk, k++) {
+            const int b = k & 1;
             const long long m = (n - o) < chunk ? (n - o) : chunk;
+            const PartF64 t = stage_particles(h, b, chunk);
             PartF32 sp = h->p32[h->cur];
             sp.key += o; sp.dx += o; sp.dy += o; if (sp.dz) sp.dz += o;
             sp.ux += o; sp.uy += o; sp.uz += o; sp.w += o;
-            launch_f32_to_f64(h->g, sp, tmp.p, m, h->s);
-            const double *src[7] = {tmp.p.q, tmp.p.x, tmp.p.y, tmp.p.z, tmp.p.u, tmp.p.v, tmp.p.w};
-            for (int k = 0; k < 7; k++)
-                if (dst[k]) CK(cudaMemcpyAsync(dst[k] + o, src[k], (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, h->s));
-            if (flv) CK(cudaMemcpyAsync(flv + o, tmp.p.flv, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, h->s));
-            CK(cudaStreamSynchronize(h->s));
+            CK(cudaStreamWaitEvent(h->s, h->ev_copied[b], 0));
+            launch_f32_to_f64(h->g, sp, t, m, h->s);
+            CK(cudaEventRecord(h->ev_done[b], h->s));
+            CK(cudaStreamWaitEvent(h->cs, h->ev_done[b], 0));
+            const double *src[7] = {t.q, t.x, t.y, t.z, t.u, t.v, t.w};
+            for (int a = 0; a < 7; a++)
+                if (dst[a]) CK(cudaMemcpyAsync(dst[a] + o, src[a], (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, h->cs));
+            if (flv) CK(cudaMemcpyAsync(flv + o, t.flv, (size_t)m * sizeof(int32_t), cudaMemcpyDeviceToHost, h->cs));
+            CK(cudaEventRecord(h->ev_copied[b], h->cs));
         }
+        r = sync_both(h);
+        if (r) return r;
     }
     return finish(h);
 }
@@ -910,22 +1029,40 @@ int pic_step(pic_handle *h, int32_t nsteps)
         return finish(h);
     }
     for (int32_t i = 0; i < nsteps; i++) {
-        h->t += 1;
-        const bool reorder = h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0;
-        cudaGraphExec_t ge = nullptr;
-        int r = get_graph(h, h->cur, reorder, &ge);
+        int r = enqueue_graph_step(h);
         if (r) return r;
-        CK(cudaGraphLaunch(ge, h->s));
-        h->launches += h->graph_kernels[reorder ? 1 : 0][h->cur];
-        if (reorder) {
-            h->cur ^= 1;
-            if (h->fp32 && !h->sorted) {  // tile ranges are valid from now on
-                CK(cudaStreamSynchronize(h->s));
-                set_sorted(h, true);
-            }
-        }
     }
     return finish(h);
+}
+
+int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps)
+{
+    if (!hs || n < 0 || nsteps < 0) return PIC_ERR_INVALID;
+    bool eager = false;
+    for (int32_t a = 0; a < n; a++) {
+        if (!hs[a]) return PIC_ERR_INVALID;
+        eager = eager || hs[a]->profiling;
+    }
+    if (eager) {
+        for (int32_t a = 0; a < n; a++) {
+            int r = pic_step(hs[a], nsteps);
+            if (r) return r;
+        }
+        return PIC_OK;
+    }
+    for (int32_t a = 0; a < n; a++)
+        for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(hs[a]->J[k], 0, field_bytes(hs[a]), hs[a]->s));
+    for (int32_t i = 0; i < nsteps; i++)
+        for (int32_t a = 0; a < n; a++) {
+            int r = enqueue_graph_step(hs[a]);
+            if (r) return r;
+        }
+    int first = PIC_OK;
+    for (int32_t a = 0; a < n; a++) {
+        int r = finish(hs[a]);
+        if (r && !first) first = r;
+    }
+    return first;
 }
 
 int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout)

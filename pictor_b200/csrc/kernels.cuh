@@ -60,7 +60,19 @@ struct Bricks {
     int t[3], nb[3], ntiles;
     int smem_floats;
 };
-void choose_bricks(const GridP &g, double ppc, Bricks &bk);
+// Shared words of a mover box of C cells: (C+1) nodes per axis x 6 field
+// components and (C+3) current cells per axis x 3 components.
+__host__ __device__ inline long long box_floats(int dims, int cx, int cy, int cz)
+{
+    const long long nn = (long long)(cx + 1) * (cy + 1) * (dims == 3 ? cz + 1 : 1);
+    const long long nj = (long long)(cx + 3) * (cy + 3) * (dims == 3 ? cz + 3 : 1);
+    return 6 * nn + 3 * nj;
+}
+constexpr int kBoxAxisMax = 64;   // cells per axis of a mover box
+// Brick shape: `req` (all > 0) if given, else about 4096 particles per brick
+// at ppc particles per cell.  Returns false if the brick plus one cell on
+// each side would not fit the mover's shared memory.
+bool choose_bricks(const GridP &g, double ppc, const int req[3], Bricks &bk);
 // Tiled FP32 mover: one CTA per brick.
 void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
                                    float *const B[3], float *const J[3], int *err, cudaStream_t s);
@@ -90,6 +102,8 @@ void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Co
 // Reference layout <-> FP32 cell-relative conversion.
 void launch_f64_to_f32(const GridP &g, const PartF64 &in, const PartF32 &out, long long n, int *err, cudaStream_t s);
 void launch_f32_to_f64(const GridP &g, const PartF32 &in, const PartF64 &out, long long n, cudaStream_t s);
+void launch_array_f64_to_f32(const double *in, float *out, long long n, cudaStream_t s);
+void launch_array_f32_to_f64(const float *in, double *out, long long n, cudaStream_t s);
 // Device Weibel loader.
 struct WeibelParams {
     double epc, density, drift, temp[2];

@@ -491,16 +491,6 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // ---------------------------------------------------------------------------
 constexpr int kTileThreads = 256;
 constexpr int kTileWarps = kTileThreads / 32;
-constexpr int kBoxAxisMax = 64;   // cells per axis of a box (bricks are at most 32 + 2)
-
-// Shared words of a box of C cells: (C+1) nodes per axis x 6 field
-// components and (C+3) current cells per axis x 3 components.
-__host__ __device__ inline long long box_floats(int dims, int cx, int cy, int cz)
-{
-    const long long nn = (long long)(cx + 1) * (cy + 1) * (dims == 3 ? cz + 1 : 1);
-    const long long nj = (long long)(cx + 3) * (cy + 3) * (dims == 3 ? cz + 3 : 1);
-    return 6 * nn + 3 * nj;
-}
 
 // Interior index of the unwrapped 1-based index a (no division when a is
 // already interior or one period away).

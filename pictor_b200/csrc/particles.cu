@@ -532,6 +532,31 @@ void launch_f32_to_f64(const GridP &g, const PartF32 &in, const PartF64 &out, lo
     count_launches(n > 0 ? 1 : 0);
 }
 
+// Field arrays between the FP64 host layout and the FP32 device form.
+__global__ void k_array_f64_to_f32(const double *__restrict__ in, float *__restrict__ out, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (float)in[i];
+}
+
+__global__ void k_array_f32_to_f64(const float *__restrict__ in, double *__restrict__ out, long long n)
+{
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = (double)in[i];
+}
+
+void launch_array_f64_to_f32(const double *in, float *out, long long n, cudaStream_t s)
+{
+    if (n > 0) k_array_f64_to_f32<<<stream_grid(n), kThreads, 0, s>>>(in, out, n);
+    count_launches(n > 0 ? 1 : 0);
+}
+
+void launch_array_f32_to_f64(const float *in, double *out, long long n, cudaStream_t s)
+{
+    if (n > 0) k_array_f32_to_f64<<<stream_grid(n), kThreads, 0, s>>>(in, out, n);
+    count_launches(n > 0 ? 1 : 0);
+}
+
 // ---------------------------------------------------------------------------
 // Weibel loader (setup_weibel.F90:17-61 via InitPrtl, init_prtl.F90:177-221)
 // ---------------------------------------------------------------------------

@@ -52,6 +52,7 @@ class PicConfig:
     capacity: int = 1 << 20
     rmin: float = 0.0
     inc_axis: int = 1
+    brick: tuple = (0, 0, 0)   # FP32 form: brick shape in cells, (0, 0, 0) = from the fill
 
     def to_struct(self) -> _capi.Config:
         s = _capi.Config()
@@ -71,6 +72,8 @@ class PicConfig:
         s.capacity = int(self.capacity)
         s.rmin = self.rmin
         s.inc_axis = self.inc_axis
+        for d in range(3):
+            s.brick[d] = int(self.brick[d])
         return s
 
     @property
@@ -275,3 +278,15 @@ class Simulation:
     @property
     def stream(self) -> int:
         return self.L.pic_stream(self.h)
+
+
+def step_many(sims, nsteps: int = 1) -> None:
+    """pic_step_many: nsteps steps of every simulation of an ensemble, their
+    step graphs interleaved on their own streams so that small runs overlap
+    on the GPU (all on the current device)."""
+    sims = list(sims)
+    if not sims:
+        return
+    L = sims[0].L
+    arr = (C.c_void_p * len(sims))(*[s.h.value for s in sims])
+    check(L.pic_step_many(arr, len(sims), int(nsteps)), "pic_step_many")
