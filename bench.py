@@ -43,6 +43,10 @@ WORKLOADS = {
     # species, drift U(0.1, 0.9) c, spread U(0.01, 0.1) c, seed 2930 + run (pictor_b200.ensemble)
     "ensemble64": dict(dims=2, runs=64, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0, precision="fp32",
                        nx=256, ny=256, nz=1),
+    # the differentiable 2D Weibel run: 128^2 cells, 8 particles per cell per species, drift +-0.4c, spread
+    # 0.05c, 400 steps, checkpoints every 50, objective sum_t 1/2 sum |B_t|^2 (pictor_b200.adjoint)
+    "adjoint128": dict(dims=2, nx=128, ny=128, nz=1, epc=8, drift=0.4, temp=0.005, c=0.45, c_ompe=2.0,
+                       precision="fp32", nsteps=400, checkpoint=50),
 }
 SEED = 2930
 
@@ -359,6 +363,143 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
     return 0
 
 
+def run_adjoint_bench(args, rank, local, peak, peak_kind):
+    """--workload adjoint128: the gradient of the time-integrated magnetic
+    energy (forward with checkpoints + reverse sweep) in the FP32 form, the
+    FP64 reference adjoint on the same run, and central finite differences of
+    the FP64 forward (h = 1e-4 of each parameter / a unit momentum direction)."""
+    import numpy as np
+    import torch
+
+    from pictor_b200 import PicConfig, init_scale
+    from pictor_b200.adjoint import Adjoint
+
+    wl = WORKLOADS[args.workload]
+    steps, K = wl["nsteps"], wl["checkpoint"]
+    sc = init_scale(wl["c"], wl["c_ompe"], wl["epc"])
+    n_cells = wl["nx"] * wl["ny"]
+    cap = int(2 * wl["epc"] * n_cells * 1.2) + 4096
+    load = (wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], SEED)
+
+    def make(prec):
+        return Adjoint(PicConfig(nx=wl["nx"], ny=wl["ny"], dims=2, c=wl["c"], qi=sc["qi"], precision=prec,
+                                 capacity=cap, reorder_period=0))
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = fn()
+        torch.cuda.synchronize()
+        return r, time.perf_counter() - t0
+
+    out = {}
+    for prec in ("fp32", "fp64"):
+        with make(prec) as a:
+            n = a.init_weibel(*load)
+            for _ in range(max(1, args.warmup // 3)):        # warm-up: allocations, clocks
+                a.forward(min(steps, K), K)
+                a.gradient()
+            clocks = ClockSampler(local)
+            clocks.start()
+            J, tf = timed(lambda: a.forward(steps, K))
+            g, tg = timed(lambda: a.gradient())
+            clk = clocks.stop()
+            out[prec] = {"n": n, "J": J, "t_forward": tf, "t_gradient": tg, "g": g, "clocks": clk}
+    g32, g64 = out["fp32"]["g"], out["fp64"]["g"]
+    v32 = np.concatenate([g32[k] for k in ("u", "v", "w")])
+    v64 = np.concatenate([g64[k] for k in ("u", "v", "w")])
+    # agreement with central differences of the FP64 forward (h = 1e-4 of each
+    # parameter, unit momentum direction), and of the FP32 with the FP64
+    # gradient, as a function of the horizon: the Weibel run is unstable, so
+    # gradients grow exponentially with the horizon and the zigzag current's
+    # jumps make long-horizon finite differences meaningless
+    sweep = []
+    with make("fp64") as a64, make("fp32") as a32:
+        a64.init_weibel(*load)
+        a32.init_weibel(*load)
+        p0, sgn = a64.fetch_particles()
+        rng = np.random.default_rng(SEED)
+        d = rng.normal(size=(3, len(p0.x)))
+        d /= np.sqrt((d * d).sum())
+
+        def fd(fn, h):
+            return (fn(h) - fn(-h)) / (2 * h)
+
+        for H in (10, 25, 50, 100, 200, 400):
+            if H > steps:
+                break
+            KH = min(K, H)
+            a64.init_weibel(*load)
+            a64.forward(H, KH)
+            g = a64.gradient()
+            a32.forward(H, KH)
+            gs = a32.gradient()
+
+            def j_load(dd, dti):
+                a64.init_weibel(wl["epc"], 0.5, wl["drift"] + dd, wl["temp"] + dti, wl["temp"], SEED)
+                return a64.forward(H, KH)
+
+            def j_dir(h):
+                p = type(p0)(*(getattr(p0, f).copy() for f in p0.NAMES))
+                p.u += h * d[0]
+                p.v += h * d[1]
+                p.w += h * d[2]
+                a64.load_particles(p, sgn)
+                return a64.forward(H, KH)
+
+            checks = [("drift", g["drift"], fd(lambda h: j_load(h, 0), 1e-4 * wl["drift"])),
+                      ("temp_ion", g["temp_ion"], fd(lambda h: j_load(0, h), 1e-4 * wl["temp"])),
+                      ("momenta_dir", float((g["u"] * d[0] + g["v"] * d[1] + g["w"] * d[2]).sum()), fd(j_dir, 1e-4))]
+            v64h = np.concatenate([g[k] for k in ("u", "v", "w")])
+            v32h = np.concatenate([gs[k] for k in ("u", "v", "w")])
+            sweep.append({"steps": H, "grad_norm_momenta": float(np.linalg.norm(v64h)),
+                          "fp32_vs_fp64_rel_l2": float(np.linalg.norm(v32h - v64h) / np.linalg.norm(v64h)),
+                          "fd": [{"param": nme, "adjoint": ad, "fd": f, "rel_err": abs(ad - f) / max(abs(f), 1e-300)}
+                                 for nme, ad, f in checks]})
+    agree = [r["steps"] for r in sweep if all(c["rel_err"] <= 1e-2 for c in r["fd"])]
+    fdc = sweep[-1]["fd"] if sweep else []
+    n = out["fp32"]["n"]
+    t32 = out["fp32"]["t_forward"] + out["fp32"]["t_gradient"]
+    t64 = out["fp64"]["t_forward"] + out["fp64"]["t_gradient"]
+    value = n * steps / t32
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": t32 / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "adjoint128", "cells": [wl["nx"], wl["ny"]], "particles": n,
+                       "particles_per_cell_per_species": wl["epc"], "drift_c": wl["drift"],
+                       "thermal_c": math.sqrt(wl["temp"] / 2), "courant": wl["c"], "steps": steps,
+                       "checkpoint_every": K, "objective": "sum_t 1/2 sum_cells |B_t|^2",
+                       "counted": "particle-steps of the run per second of forward + reverse sweep",
+                       "l2": "tape of one segment (GBs at this size) larger than L2"},
+            "objective": {"fp32": out["fp32"]["J"], "fp64": out["fp64"]["J"]},
+            "timing_s": {"fp32_forward": out["fp32"]["t_forward"], "fp32_gradient": out["fp32"]["t_gradient"],
+                         "fp64_forward": out["fp64"]["t_forward"], "fp64_gradient": out["fp64"]["t_gradient"]},
+            "fp64": {"value": n * steps / t64, "speedup_fp32_over_fp64": t64 / t32,
+                     "momentum_gradient_rel_l2_fp32_vs_fp64": float(np.linalg.norm(v32 - v64) / np.linalg.norm(v64)),
+                     "drift_gradient": {"fp32": g32["drift"], "fp64": g64["drift"]},
+                     "temp_gradient": {"fp32": [g32["temp_ion"], g32["temp_elc"]],
+                                       "fp64": [g64["temp_ion"], g64["temp_elc"]]}},
+            "fd_checks_fp64_full_horizon": fdc,
+            "fd_mismatch_fraction_full_horizon": (sum(1 for c in fdc if c["rel_err"] > 1e-2) / len(fdc)) if fdc else None,
+            "horizon_sweep": sweep,
+            "fd_agreement_1e-2_up_to_steps": max(agree) if agree else 0,
+            "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
+                         "traffic": None, "kernel": "k_move_T (mover adjoint), latency/atomic bound at this size",
+                         "peak_kind": peak_kind},
+            # forward: 2 B half steps, mover, E update, energy per step; gradient: the 4 kernels of each
+            # recomputed step, the 7 of each reverse step, the parameter reduction and 5 conversions
+            "gpu_launches": 5 * steps + 11 * steps + 6,
+            "clocks": out["fp32"]["clocks"],
+            "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 3 * 8 * n / steps,
+                    "includes": "device loader, forward, reverse sweep, gradient copied to host"},
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU algorithm (C restatement of the
     Fortran CPU path; the Fortran build is not available here) on the host."""
@@ -407,6 +548,9 @@ def main():
     if args.workload == "ensemble64":
         peak, peak_kind = measured_peaks()
         return run_ensemble_bench(args, ws, rank, local, peak, peak_kind)
+    if args.workload == "adjoint128":
+        peak, peak_kind = measured_peaks()
+        return run_adjoint_bench(args, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]
     prec = wl["precision"]
     seed = SEED + rank

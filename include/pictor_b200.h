@@ -188,6 +188,41 @@ int pic_field_energy_noalloc(const double *Ex, const double *Ey, const double *E
                              int32_t nx, int32_t ny, int32_t nz, int32_t dims,
                              double *out2, void *stream);
 
+/* ---------------------------------------------------------------------------
+   The differentiable form (no counterpart in the reference): a 2D Cartesian
+   periodic Yee run whose objective is the time-integrated magnetic energy
+   J = sum over steps t of 1/2 sum over cells |B_t|^2, with hand-written
+   adjoint kernels for the field updates, the push and the deposit.  The
+   forward step is the step of this library (FP64 or FP32 per
+   cfg->precision; dims 2, geom Cartesian, fdtd Yee, no current filter) on
+   interior arrays with periodic indices and particles in fixed slots.
+   --------------------------------------------------------------------------- */
+typedef struct pic_adjoint pic_adjoint;
+int pic_adj_create(const pic_config *cfg, pic_adjoint **out);
+void pic_adj_destroy(pic_adjoint *a);
+/* Initial particles from the Weibel loader of pic_init_weibel (same seed, same
+   particles), recording each particle's beam-drift sign for the parameter
+   gradients.  Fields start at zero. */
+int pic_adj_init_weibel(pic_adjoint *a, double epc, double density, double drift, double temp_ion, double temp_elc,
+                        uint32_t seed, int64_t *n);
+/* Initial particles from host arrays in the reference layout (x, y in ghosted
+   1-based cell units, z in [1,2)); drift_sign may be NULL (parameter
+   gradients are then zero). */
+int pic_adj_load_particles(pic_adjoint *a, int64_t n, const double *q, const double *x, const double *y,
+                           const double *z, const double *u, const double *v, const double *w, const int32_t *flv,
+                           const double *drift_sign);
+int pic_adj_fetch_particles(pic_adjoint *a, int64_t *n, double *q, double *x, double *y, double *z, double *u,
+                            double *v, double *w, int32_t *flv, double *drift_sign);
+/* nsteps steps from the initial state, keeping the state every
+   checkpoint_every steps; *objective = J. */
+int pic_adj_forward(pic_adjoint *a, int32_t nsteps, int32_t checkpoint_every, double *objective);
+/* Reverse sweep of the last forward run (each segment between checkpoints is
+   recomputed): dJ/d(initial u, v, w, x, y) per particle (host arrays of n, any
+   may be NULL) and dparam[0] = dJ/d drift, dparam[1..2] = dJ/d temperature of
+   flavours 1 and 2 (the loader's Maxwell temperatures temp[0..1]). */
+int pic_adj_gradient(pic_adjoint *a, double drift, const double *temp, double *du, double *dv, double *dw, double *dx,
+                     double *dy, double *dparam);
+
 /* Text for an error code. */
 const char *pic_error_string(int code);
 

@@ -109,6 +109,14 @@ SIGNATURES = {
     "pic_phase_times": (C.c_int, [H, PD, PI64, C.c_int32, PI64]),
     "pic_launch_count": (C.c_int, [H, PI64]),
     "pic_field_energy_noalloc": (C.c_int, [C.c_void_p] * 6 + [C.c_int32] * 4 + [C.c_void_p, C.c_void_p]),
+    "pic_adj_create": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_void_p)]),
+    "pic_adj_destroy": (None, [C.c_void_p]),
+    "pic_adj_init_weibel": (C.c_int, [C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                      C.c_uint32, PI64]),
+    "pic_adj_load_particles": (C.c_int, [C.c_void_p, C.c_int64] + [PD] * 7 + [PI32, PD]),
+    "pic_adj_fetch_particles": (C.c_int, [C.c_void_p, PI64] + [PD] * 7 + [PI32, PD]),
+    "pic_adj_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, PD]),
+    "pic_adj_gradient": (C.c_int, [C.c_void_p, C.c_double, PD, PD, PD, PD, PD, PD, PD]),
     "pic_error_string": (C.c_char_p, [C.c_int]),
     "pic_stream": (C.c_void_p, [H]),
 }

@@ -847,6 +847,7 @@ int pic_init_weibel(pic_handle *h, double epc, double density, double drift, dou
     w.temp[0] = temp_ion;
     w.temp[1] = temp_elc;
     w.seed = seed;
+    w.sgn_out = nullptr;
     // init_prtl.F90:190: Nprtl = epc * (x2-x1)*(y2-y1)*(z2-z1), truncated
     const double vol = (double)h->g.nx * (double)h->g.ny * (h->g.dims == 3 ? (double)h->g.nz : 1.0);
     w.ntrial = (long long)(epc * vol);
@@ -1135,3 +1136,33 @@ int pic_device_errors(pic_handle *h, int32_t *bits)
 }
 
 }  // extern "C"
+
+namespace pic {
+int weibel_with_signs(pic_handle *h, double epc, double density, double drift, double temp_ion, double temp_elc,
+                      uint32_t seed, double *sgn, PartF64 *view, long long *n)
+{
+    if (!h || h->fp32 || !sgn || !view || !n || !(epc > 0) || h->cfg.nflvr < 2) return PIC_ERR_INVALID;
+    WeibelParams w;
+    w.epc = epc;
+    w.density = density;
+    w.drift = drift;
+    w.temp[0] = temp_ion;
+    w.temp[1] = temp_elc;
+    w.seed = seed;
+    w.sgn_out = sgn;
+    const double vol = (double)h->g.nx * (double)h->g.ny * (h->g.dims == 3 ? (double)h->g.nz : 1.0);
+    w.ntrial = (long long)(epc * vol);
+    if (w.ntrial <= 0 || 2 * w.ntrial >= (1ll << 32)) return PIC_ERR_INVALID;
+    CK(cudaMemsetAsync(h->cnt, 0, sizeof(Counters), h->s));
+    set_sorted(h, false);
+    int r = launch_weibel(h->g, w, h->tab_x, h->tab_p, h->ntab, &h->p64[h->cur], nullptr, h->cnt, h->sc, h->capacity,
+                          h->err, h->s);
+    if (r) return r;
+    if ((r = finish(h))) return r;
+    int64_t used = 0;
+    if ((r = pic_particle_count(h, &used))) return r;
+    *view = h->p64[h->cur];
+    *n = used;
+    return PIC_OK;
+}
+}  // namespace pic

@@ -109,7 +109,13 @@ struct WeibelParams {
     double epc, density, drift, temp[2];
     uint32_t seed;
     long long ntrial;
+    double *sgn_out;   // optional (FP64 layout): +-1, the sign of each particle's beam drift
 };
+// Weibel loader into the FP64 buffers of handle h with the beam-drift sign of
+// every particle in sgn (device, capacity entries); returns the particles'
+// device view and count (used by the adjoint engine, adjoint.cu).
+int weibel_with_signs(pic_handle *h, double epc, double density, double drift, double temp_ion, double temp_elc,
+                      uint32_t seed, double *sgn, PartF64 *view, long long *n);
 int launch_weibel(const GridP &g, const WeibelParams &w, const double *table_x, const double *table_p, int ntable,
                   const PartF64 *p64, const PartF32 *p32, Counters *cnt, SortScratch &sc, long long capacity,
                   int *err, cudaStream_t s);

@@ -750,6 +750,7 @@ __global__ void __launch_bounds__(256) k_weibel_fill(GridP g, WeibelParams w, co
                 const long long o = slot + sp;
                 const double q = (1.0 * (sp == 0 ? 1.0 : -1.0)) * 1.0;
                 if (!use32) {
+                    if (w.sgn_out) w.sgn_out[o] = sgn;
                     p64.x[o] = xl;
                     p64.y[o] = yl;
                     p64.z[o] = zl;
