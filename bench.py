@@ -47,6 +47,12 @@ WORKLOADS = {
     # 0.05c, 400 steps, checkpoints every 50, objective sum_t 1/2 sum |B_t|^2 (pictor_b200.adjoint)
     "adjoint128": dict(dims=2, nx=128, ny=128, nz=1, epc=8, drift=0.4, temp=0.005, c=0.45, c_ompe=2.0,
                        precision="fp32", nsteps=400, checkpoint=50),
+    # the cylindrical wakefield configuration in the reference's theta-gridded form (FP64, Lehe along z):
+    # Nr = 256, Nz = 2048, 8 theta cells, dr = dz = 0.1 c/wp, 2x2x2 electrons per cell weighted by r with
+    # 0.01c spread, neutralising ions, Gaussian bunch sigma_r = 2, sigma_z = 4 c/wp, gamma 50, 0.1 x n0;
+    # Courant 0.3 (stable next to the axis with 8 theta cells)
+    "cyl_wake": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
+                     bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0),
 }
 SEED = 2930
 
@@ -500,6 +506,101 @@ def run_adjoint_bench(args, rank, local, peak, peak_kind):
     return 0
 
 
+def cpu_sample_cyl(wl: dict, target_s: float = 12.0):
+    """The cylindrical CPU step (C restatement of cyl_movdep_strang.F90 +
+    cyl_em_update*.F90) on a 64 x 8 x 128 sub-box with the same plasma."""
+    from oracle import oracle as O
+
+    qi = O.init_scale(wl["c"], wl["c_ompe"], wl["epc"])[0]
+    g = O.make_grid(3, 64, wl["ny"], 128, c=wl["c"], qi=qi, fdtd="lehe", qm=(1.0, -1.0))
+    # the loader's per-component spread is sqrt(temp / 2)
+    temp = 2.0 * (wl["thermal"] * wl["c"]) ** 2
+    p = O.cyl_load_uniform(g, 2, 2, 2, 1.0, temp, -1.0, 2, SEED, 64 * wl["ny"] * 128 * 8 * 2)
+    o = O.CylOracle(g, p)
+    o.step(1)
+    n_steps, t0, t = 0, time.perf_counter(), 1
+    while True:
+        t += 1
+        o.step(t)
+        n_steps += 1
+        el = time.perf_counter() - t0
+        if el >= target_s or n_steps >= 200:
+            break
+    return {"value": p.used * n_steps / el, "unit": "particle-steps/s", "cores": 1, "kind": "port",
+            "sample": f"64x{wl['ny']}x128 cells, {p.used} particles, {n_steps} steps (same plasma, no bunch), FP64, "
+                      "C restatement of the reference cylindrical CPU path, serial"}
+
+
+def run_cyl_bench(args, rank, local, peak, peak_kind):
+    """--workload cyl_wake: the cylindrical wakefield run in the reference's
+    theta-gridded FP64 form (the form this library has for cylindrical
+    geometry), particles from pictor_b200.setups.cyl_wakefield."""
+    import torch
+
+    from pictor_b200 import Particles, PicConfig, Simulation, init_scale
+    from pictor_b200.setups import cyl_wakefield
+
+    wl = WORKLOADS[args.workload]
+    sc = init_scale(wl["c"], wl["c_ompe"], wl["epc"])
+    p, info = cyl_wakefield(wl["nx"], wl["nz"], wl["ny"], wl["c"], thermal=wl["thermal"], bunch_gamma=wl["bunch_gamma"],
+                            bunch_peak=wl["bunch_peak"], bunch_sigma_r=wl["bunch_sigma_r"],
+                            bunch_sigma_z=wl["bunch_sigma_z"], seed=SEED)
+    n_p = len(p.x)
+    cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=wl["nz"], dims=3, c=wl["c"], qi=sc["qi"], qm=(1.0, -1.0),
+                    fdtd="lehe", geom="cylindrical", precision="fp64", capacity=2 * n_p + 4096,
+                    reorder_period=20, rmin=-0.5, inc_axis=1)
+    pinned = Particles(*(torch.from_numpy(getattr(p, k)).pin_memory().numpy() for k in Particles.NAMES))
+    with Simulation(cfg) as sim:
+        sim.load_particles(pinned)
+        sim.reorder()
+        sim.step(args.warmup)
+        clocks = ClockSampler(local)
+        clocks.start()
+        ms, phases, launches = timed_steps(sim, args.steps, 1, profile=True)
+        clk = clocks.stop()
+        d = sim.diagnostics(sc["masse"])
+        # end to end: the particles from pinned host memory, the steps, diagnostics, the fields back
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.load_particles(pinned)
+        sim.reorder()
+        sim.step(args.steps)
+        sim.diagnostics(sc["masse"])
+        f = sim.fetch_fields(with_current=False)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+    value = n_p * args.steps / (ms * 1e-3)
+    move_ms = phases["ms"]["move"] / max(phases["steps"], 1)
+    n_cells = wl["nx"] * wl["ny"] * wl["nz"]
+    bytes_move = n_p * bytes_per_particle(3, "fp64") + n_cells * bytes_per_cell_mover("fp64")
+    cpu = None if args.no_cpu else cpu_sample_cyl(wl)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "cyl_wake", "form": "theta-gridded FP64 (the reference's representation); "
+                                                       "the modal m=0,1 FP32 form is not built",
+                       "cells_r_theta_z": [wl["nx"], wl["ny"], wl["nz"]], "particles": n_p, **info,
+                       "courant": wl["c"], "c_ompe": wl["c_ompe"], "fdtd": "lehe (z)", "reorder_period": 20,
+                       "l2": "particle state (GBs) larger than L2"},
+            "roofline": {"bound": "hbm", "achieved": bytes_move / (move_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                         "frac": bytes_move / (move_ms * 1e-3) / 1e9 / peak, "traffic": None, "kernel": "k_cyl_move",
+                         "launch_ms": move_ms, "peak_kind": peak_kind},
+            "phases_ms_per_step": {k: v / max(phases["steps"], 1) for k, v in phases["ms"].items()},
+            "gpu_launches": launches, "clocks": clk,
+            "energy": {"field": 0.5 * (d["B2"] + d["E2"]), "kinetic": float(sum(d["kinetic"]))},
+            "e2e": {"value": n_p * args.steps / e2e_s, "unit": "particle-steps/s",
+                    "h2d_bytes_per_step": n_p * 60 / args.steps,
+                    "d2h_bytes_per_step": 6 * 8 * (wl["nx"] + 5) * (wl["ny"] + 5) * (wl["nz"] + 5) / args.steps,
+                    "seconds": e2e_s},
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU algorithm (C restatement of the
     Fortran CPU path; the Fortran build is not available here) on the host."""
@@ -510,7 +611,8 @@ def run_reference(args):
     from oracle import oracle as O
 
     O.build()
-    base = cpu_sample(wl, target_s=max(5.0, min(60.0, 3.0 * args.steps)))
+    target = max(5.0, min(60.0, 3.0 * args.steps))
+    base = cpu_sample_cyl(wl, target_s=target) if args.workload == "cyl_wake" else cpu_sample(wl, target_s=target)
     line = {
         "metric": METRIC, "value": base["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -551,6 +653,9 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
+    if args.workload == "cyl_wake":
+        peak, peak_kind = measured_peaks()
+        return run_cyl_bench(args, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]
     prec = wl["precision"]
     seed = SEED + rank

@@ -452,6 +452,38 @@ def test_cyl_full_steps_lockstep(fdtd):
             np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * max(np.abs(b).max(), 1e-30), err_msg=n)
 
 
+def test_cyl_wakefield_lockstep():
+    """A relativistic (gamma 50) electron bunch crossing the axis of an
+    r-weighted plasma, Lehe along z, Courant 0.3: 6 steps of the CUDA path
+    against the oracle's cylindrical step."""
+    from pictor_b200 import PicConfig, init_scale
+    from pictor_b200.setups import cyl_wakefield
+
+    nr, nt, nz, c = 20, 8, 48, 0.3
+    qi = init_scale(c, 10.0, 8)["qi"]
+    gp, _ = cyl_wakefield(nr, nz, nt, c, bunch_sigma_r=3.0, bunch_sigma_z=5.0, bunch_particles=4096, seed=11)
+    n = len(gp.x)
+    g = O.make_grid(3, nr, nt, nz, c=c, qi=qi, fdtd="lehe", qm=(1.0, -1.0))
+    cfg = PicConfig(nx=nr, ny=nt, nz=nz, dims=3, c=c, qi=qi, qm=(1.0, -1.0), fdtd="lehe", geom="cylindrical",
+                    capacity=3 * n, reorder_period=4, rmin=-0.5, inc_axis=1)
+    o = O.CylOracle(g, O.Particles.from_arrays(3 * n, **{k: getattr(gp, k) for k in gp.NAMES}))
+    with _sim(cfg) as s:
+        s.load_particles(gp)
+        for t in range(1, 7):
+            o.step(t, 4)
+            s.step(1)
+        assert s.particle_count() == o.p.used
+        sp, v = s.fetch_particles(), o.p.view()
+        assert np.array_equal(sp.flv, v["flv"])
+        for k in ("x", "y", "z", "u", "v", "w"):
+            np.testing.assert_allclose(getattr(sp, k), v[k], rtol=1e-9, atol=1e-9, err_msg=k)
+        gf = s.fetch_fields(with_current=False)
+        for name in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+            a, b = getattr(gf, name), getattr(o.f, name)
+            np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * max(np.abs(b).max(), 1e-30), err_msg=name)
+        assert np.abs(gf.Ez).max() > 0
+
+
 def test_cyl_field_energy_matches_oracle():
     g, cfg = _cyl()
     f = random_fields(g, seed=53, consistent_ghosts=False)
