@@ -9,15 +9,24 @@
 //   1. brick id per particle; per-brick counts (warp-aggregated atomics),
 //   2. exclusive scan of the counts -> tile_start (first particle of every
 //      brick; the last entry is the live count),
-//   3. scatter: each particle takes the next slot of its brick from an atomic
-//      cursor (one atomic per run of equal bricks within a warp),
+//   3. each particle takes the next slot of its brick from an atomic cursor
+//      (one atomic per run of equal bricks within a warp); the slot records
+//      where the particle came from and its key,
 //   4. the per-brick boxes the mover starts from (the bricks themselves),
-//      and max |w| over the live particles (the mover's fixed-point scale).
+//      and max |w| over the live particles (the mover's fixed-point scale),
+//   5. one CTA per brick orders the brick's particles by cell (a counting
+//      sort in shared memory) and lays them out transposed: the sorted list
+//      is cut into R = cells-per-brick rows of about ppc particles and stored
+//      column by column, so consecutive slots hold particles of consecutive
+//      cells.  The mover gives consecutive slots to the lanes of a warp, so
+//      its node gathers and current atomics in shared memory hit neighbouring
+//      words (few bank conflicts) instead of random cells of the brick.  The
+//      payload moves once, from the old slot straight to the final one.
 //
-// Holes are dropped, as in the reference.  Within a brick the particles keep
-// their relative order in runs of one warp; the order of the runs follows the
-// atomics.  The FP32 step does not depend on the order beyond the rounding of
-// its FP32 current sums, which is order-dependent in any case.
+// Holes are dropped, as in the reference.  The order of particles within a
+// cell follows shared-memory atomics.  The FP32 step does not depend on the
+// order beyond the rounding of its FP32 current sums, which is
+// order-dependent in any case.
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -81,9 +90,11 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, Pa
     }
 }
 
-// 3. scatter every live particle to the next free slot of its brick.
-__global__ void __launch_bounds__(kThreads) k_brick_scatter(Bricks bk, PartF32 in, PartF32 out, const uint32_t *__restrict__ bid,
-                                                            const Counters *__restrict__ cnt, int has_dz)
+// 3. the next free slot of its brick for every live particle: the slot gets
+//    the particle's source index (src) and key (out.key, read by step 5).
+__global__ void __launch_bounds__(kThreads) k_brick_slots(Bricks bk, PartF32 in, PartF32 out,
+                                                          const uint32_t *__restrict__ bid,
+                                                          const Counters *__restrict__ cnt)
 {
     const long long used = cnt->used;
     const int lane = threadIdx.x & 31;
@@ -98,13 +109,147 @@ __global__ void __launch_bounds__(kThreads) k_brick_scatter(Bricks bk, PartF32 i
         slot = __shfl_sync(0xffffffffu, slot, leader) + (uint32_t)__popc(peers & lanemask_lt_b());
         if (b == kNoBrick) continue;
         out.key[slot] = in.key[n];
-        out.dx[slot] = in.dx[n];
-        out.dy[slot] = in.dy[n];
-        if (has_dz) out.dz[slot] = in.dz[n];
-        out.ux[slot] = in.ux[n];
-        out.uy[slot] = in.uy[n];
-        out.uz[slot] = in.uz[n];
-        out.w[slot] = in.w[n];
+        bk.src[slot] = (uint32_t)n;
+    }
+}
+
+// Slot of sorted position s in the transposed layout of N particles over R
+// rows: row r holds sorted positions [r (C-1) + min(r, L), ...) with C =
+// ceil(N / R) columns and L = N - R (C - 1) rows of length C (the rest have
+// C - 1); slots run down the rows of column 0, then column 1, ...
+__host__ __device__ inline uint32_t transposed_slot(uint32_t s, uint32_t N, uint32_t R)
+{
+    const uint32_t C = (N + R - 1) / R;
+    const uint32_t L = N - R * (C - 1);
+    uint32_t row, col;
+    if (s < L * C) {
+        row = s / C;
+        col = s - row * C;
+    } else {
+        const uint32_t t = s - L * C;
+        row = L + t / (C - 1);
+        col = t - (row - L) * (C - 1);
+    }
+    return col * R + row;
+}
+
+constexpr int kOrderThreads = 256;
+// Particles of a brick whose payload the order pass stages through shared
+// memory (a 16-bit final slot and a staging word each); a larger brick
+// writes its slots directly.
+constexpr uint32_t kOrderStage = 8192;
+
+// 5. order brick b by cell and transpose (see the file comment).  Dynamic
+//    shared memory: one counter per cell of the brick, then a staging word
+//    and a 16-bit final slot per particle.  A brick of at most kOrderStage
+//    particles moves each payload array through shared memory: read in the
+//    brick-grouped order (which follows the old order, so reads stay close
+//    to coalesced), placed by final slot, written out contiguously.  A larger
+//    brick keeps its final slots in bk.bid and writes them directly.
+__global__ void __launch_bounds__(kOrderThreads) k_brick_order(GridP g, Bricks bk, PartF32 in, PartF32 out, int has_dz)
+{
+    extern __shared__ uint32_t s_dyn[];
+    __shared__ uint32_t s_warp[kOrderThreads / 32];
+    const int b = blockIdx.x;
+    const uint32_t p0 = bk.tile_start[b], N = bk.tile_start[b + 1] - p0;
+    if (N == 0) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int R = bk.t[0] * bk.t[1] * bk.t[2];
+    uint32_t *s_cnt = s_dyn, *s_st = s_dyn + R;
+    uint16_t *s_m = reinterpret_cast<uint16_t *>(s_st + kOrderStage);
+    const int bx = b % bk.nb[0], byz = b / bk.nb[0], by = byz % bk.nb[1], bz = byz / bk.nb[1];
+    const int lo0 = 3 + bx * bk.t[0], lo1 = 3 + by * bk.t[1], lo2 = 3 + bz * bk.t[2];
+    for (int c = tid; c < R; c += kOrderThreads) s_cnt[c] = 0;
+    __syncthreads();
+    auto local_cell = [&](uint32_t key) {
+        int i, j, k;
+        decode_cell(g, (int)(key & kCellMask), i, j, k);
+        const int kk = g.dims == 3 ? k - lo2 : 0;
+        return (i - lo0) + bk.t[0] * ((j - lo1) + bk.t[1] * kk);
+    };
+    const bool staged = N <= kOrderStage;
+    const uint32_t *__restrict__ gkey = out.key + p0;   // keys of the brick-grouped slots
+    const uint32_t *__restrict__ src = bk.src + p0;
+    uint32_t *__restrict__ tmp = bk.bid + p0;
+    // rank within the cell (and the cell, when staged)
+    if (staged) {
+#pragma unroll 4
+        for (uint32_t q = tid; q < N; q += kOrderThreads) {
+            const int c = local_cell(gkey[q]);
+            s_m[q] = (uint16_t)atomicAdd(&s_cnt[c], 1u);
+            s_st[q] = (uint32_t)c;
+        }
+    } else {
+        for (uint32_t q = tid; q < N; q += kOrderThreads) tmp[q] = atomicAdd(&s_cnt[local_cell(gkey[q])], 1u);
+    }
+    __syncthreads();
+    // exclusive scan of the cell counts: contiguous chunks per thread, then
+    // the chunk totals across the block
+    {
+        const int per = (R + kOrderThreads - 1) / kOrderThreads;
+        const int c0 = min(tid * per, R), c1 = min(c0 + per, R);
+        uint32_t tot = 0;
+        for (int c = c0; c < c1; c++) tot += s_cnt[c];
+        uint32_t incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        uint32_t base = incl - tot;
+        for (int w2 = 0; w2 < warp; w2++) base += s_warp[w2];
+        for (int c = c0; c < c1; c++) {
+            const uint32_t v = s_cnt[c];
+            s_cnt[c] = base;
+            base += v;
+        }
+    }
+    __syncthreads();
+    const uint32_t *srcs[8] = {in.key,
+                               reinterpret_cast<const uint32_t *>(in.dx),
+                               reinterpret_cast<const uint32_t *>(in.dy),
+                               reinterpret_cast<const uint32_t *>(in.dz),
+                               reinterpret_cast<const uint32_t *>(in.ux),
+                               reinterpret_cast<const uint32_t *>(in.uy),
+                               reinterpret_cast<const uint32_t *>(in.uz),
+                               reinterpret_cast<const uint32_t *>(in.w)};
+    uint32_t *dsts[8] = {out.key,
+                         reinterpret_cast<uint32_t *>(out.dx),
+                         reinterpret_cast<uint32_t *>(out.dy),
+                         reinterpret_cast<uint32_t *>(out.dz),
+                         reinterpret_cast<uint32_t *>(out.ux),
+                         reinterpret_cast<uint32_t *>(out.uy),
+                         reinterpret_cast<uint32_t *>(out.uz),
+                         reinterpret_cast<uint32_t *>(out.w)};
+    if (staged) {
+        for (uint32_t q = tid; q < N; q += kOrderThreads)
+            s_m[q] = (uint16_t)transposed_slot(s_cnt[s_st[q]] + s_m[q], N, (uint32_t)R);
+        __syncthreads();   // every key of the brick read before the key array is rewritten
+#pragma unroll 1
+        for (int a = 0; a < 8; a++) {
+            if (a == 3 && !has_dz) continue;
+            const uint32_t *__restrict__ sa = srcs[a];
+#pragma unroll 4
+            for (uint32_t q = tid; q < N; q += kOrderThreads) s_st[s_m[q]] = sa[src[q]];
+            __syncthreads();
+            uint32_t *__restrict__ da = dsts[a] + p0;
+#pragma unroll 4
+            for (uint32_t t = tid; t < N; t += kOrderThreads) da[t] = s_st[t];
+            __syncthreads();
+        }
+    } else {
+        for (uint32_t q = tid; q < N; q += kOrderThreads)
+            tmp[q] = transposed_slot(s_cnt[local_cell(gkey[q])] + tmp[q], N, (uint32_t)R);
+        __syncthreads();   // every key of the brick read before any slot is overwritten
+#pragma unroll 1
+        for (int a = 0; a < 8; a++) {
+            if (a == 3 && !has_dz) continue;
+            const uint32_t *__restrict__ sa = srcs[a];
+            uint32_t *__restrict__ da = dsts[a] + p0;
+            for (uint32_t q = tid; q < N; q += kOrderThreads) da[tmp[q]] = sa[src[q]];
+        }
     }
 }
 
@@ -153,9 +298,17 @@ void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Co
     k_brick_count<<<grid_for(capacity), kThreads, 0, s>>>(g, bk, p, cnt, bk.bid, err);
     scan_exclusive_u32(bk.count, bk.tile_start, (size_t)bk.ntiles + 1, bk.scan_tmp, nullptr, s);
     k_brick_prepare<<<(bk.ntiles + 255) / 256, 256, 0, s>>>(g, bk);
-    k_brick_scatter<<<grid_for(capacity), kThreads, 0, s>>>(bk, p, out, bk.bid, cnt, g.dims == 3);
+    k_brick_slots<<<grid_for(capacity), kThreads, 0, s>>>(bk, p, out, bk.bid, cnt);
+    const int R = bk.t[0] * bk.t[1] * bk.t[2];
+    const size_t smem = ((size_t)R + kOrderStage) * sizeof(uint32_t) + kOrderStage * sizeof(uint16_t);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_brick_order, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        attr_set = true;
+    }
+    k_brick_order<<<bk.ntiles, kOrderThreads, smem, s>>>(g, bk, p, out, g.dims == 3);
     k_brick_finish<<<1, 1, 0, s>>>(bk, cnt);
-    count_launches(5);
+    count_launches(6);
 }
 
 // Brick shape for a fill of ppc particles per cell: about 4096 particles per
@@ -192,9 +345,11 @@ bool choose_bricks(const GridP &g, double ppc, const int req[3], Bricks &bk)
     }
     bk.ntiles = bk.nb[0] * bk.nb[1] * bk.nb[2];
     bk.smem_floats = kBrickSmemBytes / 4;
-    // the fallback box (brick + 1 cell per side) must fit
+    // the fallback box (brick + 1 cell per side) must fit, and the per-cell
+    // counters of the in-brick order must fit beside its staging words
     for (int d = 0; d < g.dims; d++)
         if (bk.t[d] + 2 > kBoxAxisMax) return false;
+    if ((long long)bk.t[0] * bk.t[1] * bk.t[2] * 4 > 32 * 1024) return false;
     return box_floats(g.dims, bk.t[0] + 2, bk.t[1] + 2, g.dims == 3 ? bk.t[2] + 2 : 1) <= bk.smem_floats;
 }
 

@@ -555,8 +555,8 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     g.sy = g.mx;
     g.sz = (long long)g.mx * g.my;
     g.ncell = g.sz * g.mz;
-    g.mx_magic = div_magic((unsigned)g.mx);
-    g.my_magic = div_magic((unsigned)g.my);
+    div_magic((unsigned)g.mx, g.mx_magic, g.mx_shift);
+    div_magic((unsigned)g.my, g.my_magic, g.my_shift);
     if (g.ncell >= (1ll << kFlvShift) - 1 || g.mx > 4096 || g.my > 4096) {
         delete h;
         return PIC_ERR_INVALID;
@@ -609,7 +609,8 @@ int pic_create(const pic_config *cfg, pic_handle **out)
         const size_t nt = (size_t)bk.ntiles;
         if (r || (r = dalloc(h, &bk.tile_start, nt + 1)) || (r = dalloc(h, &bk.box, 8 * nt)) ||
             (r = dalloc(h, &bk.count, nt + 1)) || (r = dalloc(h, &bk.cursor, nt)) ||
-            (r = dalloc(h, &bk.bid, (size_t)h->capacity)) || (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1))) ||
+            (r = dalloc(h, &bk.bid, (size_t)h->capacity)) || (r = dalloc(h, &bk.src, (size_t)h->capacity)) ||
+            (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1))) ||
             (r = dalloc(h, &bk.wmax_bits, 1))) {
         }
     }

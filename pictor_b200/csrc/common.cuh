@@ -31,27 +31,35 @@ struct GridP {
     double xmin, xmax, ymin, ymax, zmin, zmax, xlen, ylen, zlen;
     int geom;                         // PIC_GEOM_*
     int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
-    unsigned long long mx_magic, my_magic;  // ceil(2^40 / m): exact n/m for n < 2^28, m <= 4096
+    unsigned int mx_magic, my_magic;  // n / m = umulhi(n, magic) >> shift, exact for n < 2^28 (div_magic)
+    int mx_shift, my_shift;
     // FP32 copies for the FP32 form: c, c^2, 1/c, qi, external B, q/m * 0.5
     float c_f, sqc_f, cinv_f, qi_f, bext_f[3];
     float qm_half_f[PIC_MAX_FLVR + 1];
 };
 
 // n / d by multiply-shift (the magic of GridP); exact for n < 2^28, d <= 4096.
-__host__ __device__ inline unsigned long long div_magic(unsigned int d)
+__host__ __device__ inline void div_magic(unsigned int d, unsigned int &magic, int &shift)
 {
-    return ((1ull << 40) + d - 1) / d;
+    // k = max(32, 28 + ceil(log2 d)), magic = ceil(2^k / d) < 2^32 for d >= 2;
+    // floor(n * magic / 2^k) = floor(n / d) when n * (magic d - 2^k) < 2^k,
+    // which holds for n < 2^28 since magic d - 2^k < d <= 2^(k - 28)
+    int l = 0;
+    while ((1u << l) < d) l++;
+    const int k = 28 + l > 32 ? 28 + l : 32;
+    magic = (unsigned int)(((1ull << k) + d - 1) / d);
+    shift = k - 32;
 }
-__device__ __forceinline__ int fast_div(unsigned int n, unsigned long long magic)
+__device__ __forceinline__ int fast_div(unsigned int n, unsigned int magic, int shift)
 {
-    return (int)__umul64hi((unsigned long long)n << 24, magic);  // (n * magic) >> 40 without overflow
+    return (int)(__umulhi(n, magic) >> shift);
 }
 // (i,j,k), 1-based, of a linear ghosted cell index.
 __device__ __forceinline__ void decode_cell(const GridP &g, int cell, int &i, int &j, int &k)
 {
-    const int jk = fast_div((unsigned)cell, g.mx_magic);
+    const int jk = fast_div((unsigned)cell, g.mx_magic, g.mx_shift);
     i = cell - jk * g.mx + 1;
-    k = fast_div((unsigned)jk, g.my_magic);
+    k = fast_div((unsigned)jk, g.my_magic, g.my_shift);
     j = jk - k * g.my + 1;
     k += 1;
 }

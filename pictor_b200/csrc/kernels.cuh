@@ -54,7 +54,8 @@ struct Bricks {
     int *box;               // 8 per brick
     uint32_t *count;        // ntiles + 1 (scan input)
     uint32_t *cursor;       // ntiles
-    uint32_t *bid;          // brick id per particle slot (capacity)
+    uint32_t *bid;          // brick id per particle slot (capacity); slot scratch of the in-brick order
+    uint32_t *src;          // source slot of every brick-grouped slot (capacity)
     uint32_t *scan_tmp;
     uint32_t *wmax_bits;    // max |w| of the live particles (FP32 bits), set by the reorder
     int t[3], nb[3], ntiles;

@@ -120,28 +120,30 @@ __device__ __forceinline__ void boris_f32(float c, float sqc, float cinv, const 
 // Shared-memory accesses with explicit .shared addressing (32-bit shared
 // addresses), so no generic-address resolution is left to run time.
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ float4 lds4(uint32_t a)
+template <int OFF>
+__device__ __forceinline__ float4 lds4i(uint32_t a)
 {
     float4 v;
-    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(a));
+    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4+%5];"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "r"(a), "n"(OFF));
     return v;
 }
-__device__ __forceinline__ float2 lds2(uint32_t a)
+template <int OFF>
+__device__ __forceinline__ float2 lds2i(uint32_t a)
 {
     float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(a));
+    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(a), "n"(OFF));
     return v;
 }
 __device__ __forceinline__ void red_shared(uint32_t a, int v)
 {
     asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(a), "r"(v));
 }
-
-// round(v * S) for |v * S| <= 2^22 with one FMA: adding 1.5 * 2^23 leaves the
-// rounded integer in the low mantissa bits.
-__device__ __forceinline__ int fixed_of(float v, float S)
+template <int OFF>
+__device__ __forceinline__ void red_shared_i(uint32_t a, int v)
 {
-    return __float_as_int(fmaf(v, S, 12582912.f)) - 0x4B400000;
+    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a), "n"(OFF), "r"(v));
 }
 
 // Cell step of a position x in (-1, 2) relative to its cell: floor(x) as
@@ -152,43 +154,95 @@ __device__ __forceinline__ int cell_step(float x, float &fs)
     return x >= 1.f ? 1 : (x < 0.f ? -1 : 0);
 }
 
-// One zigzag segment: flux F (charge x displacement) and the segment's
-// midpoint W within its cell (movdep.F90:187-233).
-struct Seg {
-    float Fx, Fy, Fz, Wx, Wy, Wz;
+// One part of a move's zigzag current (movdep.F90:177-237 with the weight
+// tables of vars.F90:322-356): flux F (charge x displacement) per axis,
+// midpoint weights W within the cell, and the cross terms D = (yz, xz, xy).
+//
+// A move is deposited as part A into the cell it starts in and part B into
+// the cell it ends in.  When the particle stays in its cell the relay point
+// is the midpoint and the two zigzag segments land in the same cell; their
+// sum is written in closed form as one part: with the whole move's F and
+// midpoint W, the entry F (1-Wy)(1-Wz) of the pair of segments equals
+// F ((1-Wy)(1-Wz) + dy dz / 16) (the segment midpoints sit dy/4 and dz/4 on
+// either side), and likewise for every entry with the sign of the cross term
+// + for (1-W)(1-W) and W W, - for the mixed products.  When the particle
+// crosses a face, A is the first segment and B the second, with D = 0.
+struct Part {
+    float F[3], W[3], D[3];
 };
 
-// VecJ entry e of a segment (movdep.F90:209,233 with the tables of
-// vars.F90:328-355): 3D e = 0..3 Jx, 4..7 Jy, 8..11 Jz; 2D e = 0..1 Jx,
-// 2..3 Jy, 4..7 Jz.
-template <int DIMS>
-__device__ __forceinline__ float seg_entry(const Seg &s, int e)
+// The VecJ entries of a part (3D: 0..3 Jx at (y,z) corners, 4..7 Jy at
+// (x,z), 8..11 Jz at (x,y); 2D: 0..1 Jx, 2..3 Jy, 4..7 Jz), scaled by the F
+// the part carries.
+template <int DIMS, bool CROSS = true>
+__device__ __forceinline__ void part_entries(const Part &d, float v[12])
 {
-    if (DIMS == 2) {
-        switch (e) {
-            case 0: return s.Fx * (1.f - s.Wy);
-            case 1: return s.Fx * s.Wy;
-            case 2: return s.Fy * (1.f - s.Wx);
-            case 3: return s.Fy * s.Wx;
-            case 4: return (s.Fz * (1.f - s.Wx)) * (1.f - s.Wy);
-            case 5: return (s.Fz * s.Wx) * (1.f - s.Wy);
-            case 6: return (s.Fz * (1.f - s.Wx)) * s.Wy;
-            default: return (s.Fz * s.Wx) * s.Wy;
+    const float ax = 1.f - d.W[0], ay = 1.f - d.W[1];
+    if (!CROSS) {
+        // D = 0: plain products
+        if (DIMS == 3) {
+            const float az = 1.f - d.W[2];
+            const float Fa = d.F[0] * ay, Fw = d.F[0] * d.W[1];
+            v[0] = Fa * az;
+            v[1] = Fw * az;
+            v[2] = Fa * d.W[2];
+            v[3] = Fw * d.W[2];
+            const float Ga = d.F[1] * ax, Gw = d.F[1] * d.W[0];
+            v[4] = Ga * az;
+            v[5] = Gw * az;
+            v[6] = Ga * d.W[2];
+            v[7] = Gw * d.W[2];
+            const float Ha = d.F[2] * ax, Hw = d.F[2] * d.W[0];
+            v[8] = Ha * ay;
+            v[9] = Hw * ay;
+            v[10] = Ha * d.W[1];
+            v[11] = Hw * d.W[1];
+        } else {
+            v[0] = d.F[0] * ay;
+            v[1] = d.F[0] * d.W[1];
+            v[2] = d.F[1] * ax;
+            v[3] = d.F[1] * d.W[0];
+            const float Ha = d.F[2] * ax, Hw = d.F[2] * d.W[0];
+            v[4] = Ha * ay;
+            v[5] = Hw * ay;
+            v[6] = Ha * d.W[1];
+            v[7] = Hw * d.W[1];
         }
+        return;
     }
-    switch (e) {
-        case 0: return (s.Fx * (1.f - s.Wy)) * (1.f - s.Wz);
-        case 1: return (s.Fx * s.Wy) * (1.f - s.Wz);
-        case 2: return (s.Fx * (1.f - s.Wy)) * s.Wz;
-        case 3: return (s.Fx * s.Wy) * s.Wz;
-        case 4: return (s.Fy * (1.f - s.Wx)) * (1.f - s.Wz);
-        case 5: return (s.Fy * s.Wx) * (1.f - s.Wz);
-        case 6: return (s.Fy * (1.f - s.Wx)) * s.Wz;
-        case 7: return (s.Fy * s.Wx) * s.Wz;
-        case 8: return (s.Fz * (1.f - s.Wx)) * (1.f - s.Wy);
-        case 9: return (s.Fz * s.Wx) * (1.f - s.Wy);
-        case 10: return (s.Fz * (1.f - s.Wx)) * s.Wy;
-        default: return (s.Fz * s.Wx) * s.Wy;
+    if (DIMS == 3) {
+        const float az = 1.f - d.W[2];
+        {
+            const float Fa = d.F[0] * ay, Fw = d.F[0] * d.W[1], Fd = d.F[0] * d.D[0];
+            v[0] = fmaf(Fa, az, Fd);
+            v[1] = fmaf(Fw, az, -Fd);
+            v[2] = fmaf(Fa, d.W[2], -Fd);
+            v[3] = fmaf(Fw, d.W[2], Fd);
+        }
+        {
+            const float Fa = d.F[1] * ax, Fw = d.F[1] * d.W[0], Fd = d.F[1] * d.D[1];
+            v[4] = fmaf(Fa, az, Fd);
+            v[5] = fmaf(Fw, az, -Fd);
+            v[6] = fmaf(Fa, d.W[2], -Fd);
+            v[7] = fmaf(Fw, d.W[2], Fd);
+        }
+        {
+            const float Fa = d.F[2] * ax, Fw = d.F[2] * d.W[0], Fd = d.F[2] * d.D[2];
+            v[8] = fmaf(Fa, ay, Fd);
+            v[9] = fmaf(Fw, ay, -Fd);
+            v[10] = fmaf(Fa, d.W[1], -Fd);
+            v[11] = fmaf(Fw, d.W[1], Fd);
+        }
+    } else {
+        v[0] = d.F[0] * ay;
+        v[1] = d.F[0] * d.W[1];
+        v[2] = d.F[1] * ax;
+        v[3] = d.F[1] * d.W[0];
+        const float Fa = d.F[2] * ax, Fw = d.F[2] * d.W[0], Fd = d.F[2] * d.D[2];
+        v[4] = fmaf(Fa, ay, Fd);
+        v[5] = fmaf(Fw, ay, -Fd);
+        v[6] = fmaf(Fa, d.W[1], -Fd);
+        v[7] = fmaf(Fw, d.W[1], Fd);
     }
 }
 
@@ -207,56 +261,73 @@ __device__ __forceinline__ int entry_offset(int e, int sy, int sz, int &comp)
     return o[e];
 }
 
-// Deposit of the two segments of one move into global J: segment 1 into the
-// cell c0 it starts in, segment 2 into the cell c1 the particle ends in; when
-// the move stays in its cell both are summed first and added once.
-template <int DIMS>
-__device__ __forceinline__ void deposit_f32(float *Jx, float *Jy, float *Jz, int c0, int c1, int sy, int sz,
-                                            const Seg &s1, const Seg &s2)
+// A part into global J at cell offset c (FP32 atomics).
+template <int DIMS, bool CROSS = true>
+__device__ __forceinline__ void deposit_part_global(float *Jx, float *Jy, float *Jz, int c, int sy, int sz,
+                                                    const Part &d)
 {
     constexpr int NE = DIMS == 3 ? 12 : 8;
     float *J3[3] = {Jx, Jy, Jz};
-    const bool same = c0 == c1;
+    float v[12];
+    part_entries<DIMS, CROSS>(d, v);
 #pragma unroll
     for (int e = 0; e < NE; e++) {
         int comp;
         const int o = entry_offset<DIMS>(e, sy, sz, comp);
-        atomicAdd(J3[comp] + c0 + o, seg_entry<DIMS>(s1, e) + (same ? seg_entry<DIMS>(s2, e) : 0.f));
-    }
-    if (!same) {
-#pragma unroll
-        for (int e = 0; e < NE; e++) {
-            int comp;
-            const int o = entry_offset<DIMS>(e, sy, sz, comp);
-            atomicAdd(J3[comp] + c1 + o, seg_entry<DIMS>(s2, e));
-        }
+        atomicAdd(J3[comp] + c + o, v[e]);
     }
 }
 
-// The same deposit into the shared current box of a brick (shared address
-// sJ0 of component 0; components njc words apart), as fixed-point integers
-// (v * S rounded to nearest) added with native shared-memory integer atomics;
-// S is chosen per brick so that no entry and no sum can overflow.
-template <int DIMS>
-__device__ __forceinline__ void deposit_box(uint32_t sJ0, int njc, int JX, int JXY, float S, int j0, int j1,
-                                            const Seg &s1, const Seg &s2)
+// Shared byte offsets of the current box: component planes and the y / z
+// strides (the x stride is 4 bytes, an immediate).
+struct JOff {
+    uint32_t cy, cz;      // Jy, Jz plane - Jx plane
+    uint32_t y, z, yz;    // 4 JX, 4 JXY, 4 (JX + JXY)
+};
+
+// round(v) for |v| <= 2^22, v already scaled by the box's fixed-point scale:
+// adding 1.5 * 2^23 leaves the rounded integer in the low mantissa bits.
+__device__ __forceinline__ int fixed_round(float v)
 {
-    constexpr int NE = DIMS == 3 ? 12 : 8;
-    const bool same = j0 == j1;
-#pragma unroll
-    for (int e = 0; e < NE; e++) {
-        int comp;
-        const int o = entry_offset<DIMS>(e, JX, JXY, comp);
-        red_shared(sJ0 + 4u * (uint32_t)(comp * njc + j0 + o),
-                   fixed_of(seg_entry<DIMS>(s1, e) + (same ? seg_entry<DIMS>(s2, e) : 0.f), S));
-    }
-    if (!same) {
-#pragma unroll
-        for (int e = 0; e < NE; e++) {
-            int comp;
-            const int o = entry_offset<DIMS>(e, JX, JXY, comp);
-            red_shared(sJ0 + 4u * (uint32_t)(comp * njc + j1 + o), fixed_of(seg_entry<DIMS>(s2, e), S));
-        }
+    return __float_as_int(v + 12582912.f) - 0x4B400000;
+}
+
+// A part into the shared current box at byte address a (cell j's Jx word),
+// F already scaled by the fixed-point scale S.
+template <int DIMS, bool CROSS = true>
+__device__ __forceinline__ void deposit_part_box(uint32_t a, const JOff &o, const Part &d)
+{
+    float v[12];
+    part_entries<DIMS, CROSS>(d, v);
+    if (DIMS == 3) {
+        red_shared_i<0>(a, fixed_round(v[0]));
+        red_shared_i<0>(a + o.y, fixed_round(v[1]));
+        red_shared_i<0>(a + o.z, fixed_round(v[2]));
+        red_shared_i<0>(a + o.yz, fixed_round(v[3]));
+        const uint32_t b = a + o.cy;
+        red_shared_i<0>(b, fixed_round(v[4]));
+        red_shared_i<4>(b, fixed_round(v[5]));
+        const uint32_t bz = b + o.z;
+        red_shared_i<0>(bz, fixed_round(v[6]));
+        red_shared_i<4>(bz, fixed_round(v[7]));
+        const uint32_t c = a + o.cz;
+        red_shared_i<0>(c, fixed_round(v[8]));
+        red_shared_i<4>(c, fixed_round(v[9]));
+        const uint32_t cy = c + o.y;
+        red_shared_i<0>(cy, fixed_round(v[10]));
+        red_shared_i<4>(cy, fixed_round(v[11]));
+    } else {
+        red_shared_i<0>(a, fixed_round(v[0]));
+        red_shared_i<0>(a + o.y, fixed_round(v[1]));
+        const uint32_t b = a + o.cy;
+        red_shared_i<0>(b, fixed_round(v[2]));
+        red_shared_i<4>(b, fixed_round(v[3]));
+        const uint32_t c = a + o.cz;
+        red_shared_i<0>(c, fixed_round(v[4]));
+        red_shared_i<4>(c, fixed_round(v[5]));
+        const uint32_t cy = c + o.y;
+        red_shared_i<0>(cy, fixed_round(v[6]));
+        red_shared_i<4>(cy, fixed_round(v[7]));
     }
 }
 
@@ -288,6 +359,8 @@ struct TileBox {
     int C[3];           // box extent in cells (1 on the unused z axis of 2D)
     int NX, NXY;        // node box strides
     int JX, JXY, njc;   // current box strides and size
+    uint32_t oY4, oZ4;  // node-box byte strides of the 16-byte nodes (8-byte nodes: half)
+    JOff jo;            // current-box byte offsets
     float S;            // fixed-point scale of the current box
 };
 
@@ -329,24 +402,23 @@ __device__ __forceinline__ PState load_state(const PartF32 &p, uint32_t n)
 // through the global arrays at the particle's wrapped cell.  The current of
 // a particle inside the box goes to the box; otherwise to the global J at the
 // wrapped cell (ghost layers included; the fold adds them to their periodic
-// images).
+// images).  Returns true when the particle crossed a face inside the box: its
+// second zigzag segment is then left to the caller (Bq, at box address qa),
+// which deposits those of a warp together.  The cell range is checked where
+// it guards a global access; a cell decoded inside the box is in range.
 template <int DIMS, bool TILED>
-__device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint32_t n, const PState &s,
+__device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint32_t n, const PState &s,
                                          const float *__restrict__ Ex, const float *__restrict__ Ey,
                                          const float *__restrict__ Ez, const float *__restrict__ Bx,
                                          const float *__restrict__ By, const float *__restrict__ Bz, float *Jx,
-                                         float *Jy, float *Jz, int *err, const TileBox &tb, Bounds &bd)
+                                         float *Jy, float *Jz, int *err, const TileBox &tb, Bounds &bd, Part &Bq,
+                                         uint32_t &qa)
 {
     const int flv = (int)(s.key >> kFlvShift);
-    if (flv == 0) return;
+    if (flv == 0) return false;
     const int cell = (int)(s.key & kCellMask);
     int i, j, k;
     decode_cell(g, cell, i, j, k);
-    if (i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 || (DIMS == 3 && (k < 3 || k > g.mz - 3)) ||
-        (DIMS == 2 && k != 1)) {
-        raise_error(err, PIC_DEVERR_RANGE);
-        return;
-    }
     const float dx = s.dx, dy = s.dy, dz = s.dz;
     float wt[8];
     weights_f32<DIMS>(dx, dy, dz, wt);
@@ -363,12 +435,27 @@ __device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint3
                  (DIMS == 2 || (unsigned)lz < (unsigned)tb.C[2]);
         nb = lx + tb.NX * ly + tb.NXY * lz;
     }
+    if (!inside && (i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 ||
+                    (DIMS == 3 && (k < 3 || k > g.mz - 3)) || (DIMS == 2 && k != 1))) {
+        raise_error(err, PIC_DEVERR_RANGE);
+        return false;
+    }
     float pE[3] = {0.f, 0.f, 0.f}, pB[3] = {0.f, 0.f, 0.f};
     if (inside) {
-#pragma unroll
-        for (int c8 = 0; c8 < (DIMS == 3 ? 8 : 4); c8++) {
-            const int q = nb + (c8 & 1) + ((c8 >> 1) & 1) * tb.NX + ((c8 >> 2) & 1) * tb.NXY;
-            accum(wt[c8], lds4(tb.nA + 16u * (uint32_t)q), lds2(tb.nB + 8u * (uint32_t)q), pE, pB);
+        // corner rows (y, z) by register offsets, the x neighbour by an immediate
+        const uint32_t a0 = tb.nA + 16u * (uint32_t)nb, b0 = tb.nB + 8u * (uint32_t)nb;
+        const uint32_t a1 = a0 + tb.oY4, b1 = b0 + (tb.oY4 >> 1);
+        accum(wt[0], lds4i<0>(a0), lds2i<0>(b0), pE, pB);
+        accum(wt[1], lds4i<16>(a0), lds2i<8>(b0), pE, pB);
+        accum(wt[2], lds4i<0>(a1), lds2i<0>(b1), pE, pB);
+        accum(wt[3], lds4i<16>(a1), lds2i<8>(b1), pE, pB);
+        if (DIMS == 3) {
+            const uint32_t a2 = a0 + tb.oZ4, b2 = b0 + (tb.oZ4 >> 1);
+            const uint32_t a3 = a1 + tb.oZ4, b3 = b1 + (tb.oZ4 >> 1);
+            accum(wt[4], lds4i<0>(a2), lds2i<0>(b2), pE, pB);
+            accum(wt[5], lds4i<16>(a2), lds2i<8>(b2), pE, pB);
+            accum(wt[6], lds4i<0>(a3), lds2i<0>(b3), pE, pB);
+            accum(wt[7], lds4i<16>(a3), lds2i<8>(b3), pE, pB);
         }
     } else {
 #pragma unroll
@@ -396,27 +483,52 @@ __device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint3
     // zigzag relay point with ip0 = 0, ip = s (movdep.F90:183-185)
     const float xr = fminf(fminf(fsx, 0.f) + 1.f, fmaxf(fmaxf(fsx, 0.f), 0.5f * (dx + x1)));
     const float yr = fminf(fminf(fsy, 0.f) + 1.f, fmaxf(fmaxf(fsy, 0.f), 0.5f * (dy + y1)));
-    const float qthis = s.w * g.qi_f;
-    float Fz1, Fz2, Wz1 = 0.f, Wz2 = 0.f;
+    const float zr = DIMS == 3 ? fminf(fminf(fsz, 0.f) + 1.f, fmaxf(fmaxf(fsz, 0.f), 0.5f * (dz + z1))) : 0.f;
+    const bool stays = (sxx | syy | szz) == 0;
+    // charge, times the box's fixed-point scale for a particle inside the box
+    const float qthis = s.w * g.qi_f * (inside ? tb.S : 1.f);
+    // part A: the whole move (stays) or the first segment, ending at e
+    const float ex = stays ? x1 : xr, ey = stays ? y1 : yr, ez = stays ? z1 : zr;
+    const float mx = ex - dx, my = ey - dy, mz = ez - dz;
+    Part A, B;
+    A.F[0] = qthis * mx;
+    A.F[1] = qthis * my;
+    A.W[0] = 0.5f * (dx + ex);
+    A.W[1] = 0.5f * (dy + ey);
+    A.D[2] = stays ? 0.0625f * (mx * my) : 0.f;
+    B.F[0] = qthis * (x1 - xr);
+    B.F[1] = qthis * (y1 - yr);
+    B.W[0] = 0.5f * (x1 + xr) - fsx;
+    B.W[1] = 0.5f * (y1 + yr) - fsy;
+    B.D[0] = B.D[1] = B.D[2] = 0.f;
     if (DIMS == 3) {
-        const float zr = fminf(fminf(fsz, 0.f) + 1.f, fmaxf(fmaxf(fsz, 0.f), 0.5f * (dz + z1)));
-        Fz1 = qthis * (zr - dz);
-        Fz2 = qthis * (z1 - zr);
-        Wz1 = 0.5f * (dz + zr);
-        Wz2 = 0.5f * (z1 + zr) - fsz;
+        A.F[2] = qthis * mz;
+        A.W[2] = 0.5f * (dz + ez);
+        A.D[0] = stays ? 0.0625f * (my * mz) : 0.f;
+        A.D[1] = stays ? 0.0625f * (mx * mz) : 0.f;
+        B.F[2] = qthis * (z1 - zr);
+        B.W[2] = 0.5f * (z1 + zr) - fsz;
     } else {
-        // out-of-plane motion: no cell crossing, the relay point is the midpoint
-        Fz1 = qthis * (0.5f * (w * gg));
-        Fz2 = Fz1;
+        // out-of-plane motion: no cell crossing, each segment carries half
+        const float fz = qthis * (0.5f * (w * gg));
+        A.F[2] = stays ? 2.f * fz : fz;
+        B.F[2] = fz;
+        A.W[2] = B.W[2] = 0.f;
+        A.D[0] = A.D[1] = 0.f;
     }
-    const Seg s1 = {qthis * (xr - dx), qthis * (yr - dy), Fz1, 0.5f * (dx + xr), 0.5f * (dy + yr), Wz1};
-    const Seg s2 = {qthis * (x1 - xr), qthis * (y1 - yr), Fz2, 0.5f * (x1 + xr) - fsx, 0.5f * (y1 + yr) - fsy, Wz2};
+    bool queued = false;
     if (inside) {
         const int lx = uo[0] - tb.lo[0], ly = uo[1] - tb.lo[1], lz = DIMS == 3 ? uo[2] - tb.lo[2] : 0;
         const int jb = (lx + 1) + tb.JX * (ly + 1) + (DIMS == 3 ? tb.JXY * (lz + 1) : 0);
-        deposit_box<DIMS>(tb.sJ, tb.njc, tb.JX, tb.JXY, tb.S, jb, jb + sxx + syy * tb.JX + szz * tb.JXY, s1, s2);
+        deposit_part_box<DIMS>(tb.sJ + 4u * (uint32_t)jb, tb.jo, A);
+        if (!stays) {
+            Bq = B;
+            qa = tb.sJ + 4u * (uint32_t)(jb + sxx + syy * tb.JX + szz * tb.JXY);
+            queued = true;
+        }
     } else {
-        deposit_f32<DIMS>(Jx, Jy, Jz, cell, cell + sxx + syy * sy + szz * sz, sy, sz, s1, s2);
+        deposit_part_global<DIMS>(Jx, Jy, Jz, cell, sy, sz, A);
+        if (!stays) deposit_part_global<DIMS, false>(Jx, Jy, Jz, cell + sxx + syy * sy + szz * sz, sy, sz, B);
     }
     // new offsets and periodic cell index
     float nx = x1 - fsx, ny = y1 - fsy, nz = z1 - fsz;
@@ -438,10 +550,12 @@ __device__ __forceinline__ void push_one(const GridP &g, const PartF32 &p, uint3
     p.ux[n] = u;
     p.uy[n] = v;
     p.uz[n] = w;
+    return queued;
 }
 
-// Particles [n0, n1) with stride `step`, the next particle prefetched.
-template <int DIMS, bool TILED>
+// Particles [n0, n1) with stride `step`, the next particle prefetched (per-
+// particle form: second segments deposited at once).
+template <int DIMS>
 __device__ __forceinline__ void push_range(const GridP &g, const PartF32 &p, uint32_t n0, uint32_t n1, uint32_t step,
                                            const float *__restrict__ Ex, const float *__restrict__ Ey,
                                            const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -450,12 +564,104 @@ __device__ __forceinline__ void push_range(const GridP &g, const PartF32 &p, uin
 {
     if (n0 >= n1) return;
     PState cur = load_state<DIMS>(p, n0);
+    Part Bq;
+    uint32_t qa;
     for (uint32_t n = n0; n < n1; n += step) {
         PState nxt = cur;
         if (n1 - n > step) nxt = load_state<DIMS>(p, n + step);
-        push_one<DIMS, TILED>(g, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+        push_one<DIMS, false>(g, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, Bq, qa);
         cur = nxt;
     }
+}
+
+constexpr int kTileThreads = 256;
+constexpr int kTileWarps = kTileThreads / 32;
+
+// Second zigzag segments queued by the lanes of one warp (structure of
+// arrays: F x, y, z, W x, y, z, box address; 32 entries each).
+constexpr int kQueueRows = 7;
+
+__device__ __forceinline__ uint32_t lanemask_lt()
+{
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Deposit the first k queued segments, one per lane, into the box.
+template <int DIMS>
+__device__ __forceinline__ void drain_queue(float (*q)[32], int k, const JOff &jo)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    if (lane < k) {
+        Part B;
+        B.F[0] = q[0][lane];
+        B.F[1] = q[1][lane];
+        B.F[2] = q[2][lane];
+        B.W[0] = q[3][lane];
+        B.W[1] = q[4][lane];
+        B.W[2] = q[5][lane];
+        deposit_part_box<DIMS, false>(__float_as_uint(q[6][lane]), jo, B);
+    }
+    __syncwarp();
+}
+
+// Tiled form: warp w of the CTA moves slots p0 + 32 w + 256 t + lane, all
+// lanes of a warp stepping together (lanes past p1 idle), so that the second
+// segments of the lanes that crossed a face can be gathered into the warp's
+// queue and deposited 32 at a time instead of in a branch that nearly every
+// warp would take for a few of its lanes.  The next particle loads while
+// this one moves.
+template <int DIMS>
+__device__ __forceinline__ void push_range_tiled(const GridP &g, const PartF32 &p, uint32_t p0, uint32_t p1,
+                                                 const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                                 const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                                 const float *__restrict__ By, const float *__restrict__ Bz,
+                                                 float *Jx, float *Jy, float *Jz, int *err, const TileBox &tb,
+                                                 Bounds &bd, float (*q)[32])
+{
+    constexpr uint32_t step = kTileThreads;
+    const int lane = threadIdx.x & 31;
+    uint32_t base = p0 + 32u * (threadIdx.x >> 5);
+    if (base >= p1) return;   // uniform across the warp
+    int qn = 0;
+    auto move = [&](const PState &st, uint32_t b) {
+        Part Bq;
+        uint32_t qa = 0;
+        const bool cross = push_one<DIMS, true>(g, p, b + lane, st, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd,
+                                                Bq, qa);
+        const uint32_t m = __ballot_sync(0xffffffffu, cross);
+        if (m) {
+            const int c = __popc(m);
+            if (qn + c > 32) {
+                drain_queue<DIMS>(q, qn, tb.jo);
+                qn = 0;
+            }
+            if (cross) {
+                const int e = qn + __popc(m & lanemask_lt());
+                q[0][e] = Bq.F[0];
+                q[1][e] = Bq.F[1];
+                q[2][e] = Bq.F[2];
+                q[3][e] = Bq.W[0];
+                q[4][e] = Bq.W[1];
+                q[5][e] = Bq.W[2];
+                q[6][e] = __uint_as_float(qa);
+            }
+            qn += c;
+        }
+    };
+    PState cur;
+    cur.key = 0;
+    if (base + lane < p1) cur = load_state<DIMS>(p, base + lane);
+    for (; base < p1; base += step) {
+        PState nxt = cur;
+        nxt.key = 0;
+        if (base + step + lane < p1) nxt = load_state<DIMS>(p, base + step + lane);
+        move(cur, base);
+        cur = nxt;
+    }
+    if (qn) drain_queue<DIMS>(q, qn, tb.jo);
 }
 
 // ---------------------------------------------------------------------------
@@ -471,7 +677,7 @@ __global__ void __launch_bounds__(kThreads) k_move_f32(GridP g, PartF32 p, const
     TileBox tb = {};
     Bounds bd;
     const uint32_t step = gridDim.x * blockDim.x;
-    push_range<DIMS, false>(g, p, blockIdx.x * blockDim.x + threadIdx.x, (uint32_t)cnt->used, step, Ex, Ey, Ez, Bx,
+    push_range<DIMS>(g, p, blockIdx.x * blockDim.x + threadIdx.x, (uint32_t)cnt->used, step, Ex, Ey, Ez, Bx,
                             By, Bz, Jx, Jy, Jz, err, tb, bd);
 }
 
@@ -489,8 +695,6 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // ---------------------------------------------------------------------------
 // Tiled form: one CTA per brick.
 // ---------------------------------------------------------------------------
-constexpr int kTileThreads = 256;
-constexpr int kTileWarps = kTileThreads / 32;
 
 // Interior index of the unwrapped 1-based index a (no division when a is
 // already interior or one period away).
@@ -511,6 +715,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     extern __shared__ __align__(16) float sm[];
     __shared__ int red[kTileWarps][6];
     __shared__ int s_off[3][kBoxAxisMax + 3];
+    __shared__ float s_q[kTileWarps][kQueueRows][32];
     const int b = blockIdx.x;
     const uint32_t p0 = bk.tile_start[b], p1 = bk.tile_start[b + 1];
     if (p0 >= p1) return;
@@ -558,6 +763,13 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     tb.JX = JX;
     tb.JXY = JX * JY;
     tb.njc = JX * JY * JZ;
+    tb.oY4 = 16u * (uint32_t)NX;
+    tb.oZ4 = 16u * (uint32_t)(NX * NY);
+    tb.jo.cy = 4u * (uint32_t)tb.njc;
+    tb.jo.cz = 8u * (uint32_t)tb.njc;
+    tb.jo.y = 4u * (uint32_t)JX;
+    tb.jo.z = 4u * (uint32_t)tb.JXY;
+    tb.jo.yz = tb.jo.y + tb.jo.z;
     float4 *nA = reinterpret_cast<float4 *>(sm);
     float2 *nB = reinterpret_cast<float2 *>(sm + 4 * nnode);
     int *sJ = reinterpret_cast<int *>(sm + 6 * nnode);
@@ -567,7 +779,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     // fixed-point scale: a particle adds at most b = |w| qi c to any entry
     // (its displacement per axis is below c), so with S = 2^30 / (N b) no sum
     // of the N particles exceeds 2^30; S <= 2^22 / b keeps each contribution
-    // below 2^22 (the range of fixed_of)
+    // below 2^22 (the range of fixed_round)
     {
         const float b1 = g.c_f * g.qi_f * __uint_as_float(*bk.wmax_bits);
         const float n = fmaxf((float)(p1 - p0), 256.f);
@@ -606,7 +818,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 
     Bounds bd;
     bd.init();
-    push_range<DIMS, true>(g, p, p0 + tid, p1, kTileThreads, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+    push_range_tiled<DIMS>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, s_q[warp]);
     __syncthreads();
 
     // add the box current to the periodic interior image of each cell
