@@ -305,6 +305,15 @@ __device__ __forceinline__ T wrap_pos(T x, int n)
     return x;
 }
 
+// Particle of work item L in the mover adjoint: the lanes of a warp take
+// particles np/32 apart.  The loader writes particles cell by cell, so
+// consecutive slots share cells and their 24 cotangent atomics would hit the
+// same words; spread this way the lanes of a warp land in different cells.
+// The particle state of this form is small enough to stay in L2, where the
+// scattered loads hit.  (The forward mover, with fewer atomics per particle,
+// is faster with coalesced loads.)
+__device__ __forceinline__ long long spread_slot(long long L, long long q) { return (L & 31) * q + (L >> 5); }
+
 template <typename T>
 __global__ void k_move(AG g, PS<T> p, const T *__restrict__ qw, const int *__restrict__ flv, long long np, F3<T> E,
                        F3<T> B, F3<T> J)
@@ -330,14 +339,19 @@ __global__ void k_move(AG g, PS<T> p, const T *__restrict__ qw, const int *__res
 
 // The mover's adjoint.  P is the tape's state at the start of the step, pb
 // the cotangents of the particle after the step (replaced by those before),
-// Ebt the cotangent of E after the step (J-bar = -Ebt), Eb / Bb receive the
-// gather's cotangents of E and of the B the gather used.
+// Ebt the cotangent of E after the step (J-bar = -Ebt); Nb (6 arrays: E x,
+// y, z, B x, y, z) receives the gather's cotangents of the node-averaged
+// fields, which k_node_T then takes back to the staggered E and B.
 template <typename T>
 __global__ void k_move_T(AG g, PS<T> P, const T *__restrict__ qw, const int *__restrict__ flv, long long np, F3<T> E,
-                         F3<T> B, F3<T> Ebt, PS<T> pb, F3<T> Eb, F3<T> Bb)
+                         F3<T> B, F3<T> Ebt, PS<T> pb, T *Nb)
 {
+    const size_t nc = (size_t)g.nx * g.ny;
     const T c = (T)g.c, cinv = (T)g.cinv;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
+    const long long q = (np + 31) >> 5;
+    for (long long L = (long long)blockIdx.x * blockDim.x + threadIdx.x; L < 32 * q; L += (long long)gridDim.x * blockDim.x) {
+        const long long n = spread_slot(L, q);
+        if (n >= np) continue;
         Mv<T> M;
         const T x0 = P.x[n], y0 = P.y[n], z0 = P.z[n];
         move_fwd<T>(g, x0, y0, z0, P.u[n], P.v[n], P.w[n], qw[n] * (T)g.qi, (T)g.qm_half[flv[n]], E, B, M);
@@ -426,30 +440,40 @@ __global__ void k_move_T(AG g, PS<T> P, const T *__restrict__ qw, const int *__r
             for (int k = 0; k < 3; k++) wtb += M.V[nn][k] * Epb[k] + M.V[nn][3 + k] * Bpb[k];
             wxb[ax] += wtb * M.wy[ay];
             wyb[ay] += wtb * M.wx[ax];
-            // node-averaging adjoint into the staggered cotangents
-            const int a = M.ip0 + ax, b = M.jp0 + ay;
-            const int cc = at(g, a, b), cxm = at(g, a - 1, b), cym = at(g, a, b - 1), cxym = at(g, a - 1, b - 1);
-            const T ve = wt * Epb[0] * (T)0.5, vy = wt * Epb[1] * (T)0.5, vz = wt * Epb[2];
-            const T bx = wt * Bpb[0] * (T)0.5, by = wt * Bpb[1] * (T)0.5, bz = wt * Bpb[2] * (T)0.25;
-            atomicAdd(Eb.x + cxm, ve);
-            atomicAdd(Eb.x + cc, ve);
-            atomicAdd(Eb.y + cym, vy);
-            atomicAdd(Eb.y + cc, vy);
-            atomicAdd(Eb.z + cc, vz);
-            atomicAdd(Bb.x + cym, bx);
-            atomicAdd(Bb.x + cc, bx);
-            atomicAdd(Bb.y + cxm, by);
-            atomicAdd(Bb.y + cc, by);
-            atomicAdd(Bb.z + cxym, bz);
-            atomicAdd(Bb.z + cxm, bz);
-            atomicAdd(Bb.z + cym, bz);
-            atomicAdd(Bb.z + cc, bz);
+            // cotangents of the node values (node averaging undone by k_node_T)
+            const size_t cc = (size_t)at(g, M.ip0 + ax, M.jp0 + ay);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                atomicAdd(Nb + k * nc + cc, wt * Epb[k]);
+                atomicAdd(Nb + (3 + k) * nc + cc, wt * Bpb[k]);
+            }
         }
         x0b += wxb[1] - wxb[0];
         y0b += wyb[1] - wyb[0];
         pb.x[n] = x0b;
         pb.y[n] = y0b;
         pb.z[n] = z0b;
+    }
+}
+
+// Adjoint of the node averaging (movdep_routines.F90:6-223 in 2D: E x and B y
+// averaged over the cells at x-1 and x, E y and B x over y-1 and y, B z over
+// the four cells around the node): Eb, Bb += the node cotangents Nb taken
+// back to the staggered components.
+template <typename T>
+__global__ void k_node_T(AG g, const T *__restrict__ Nb, F3<T> Eb, F3<T> Bb)
+{
+    const int n = g.nx * g.ny;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const int i = c % g.nx, j = c / g.nx;
+        const int cx = at(g, i + 1, j), cy = at(g, i, j + 1), cxy = at(g, i + 1, j + 1);
+        const T *N0 = Nb, *N1 = Nb + n, *N2 = Nb + 2 * n, *N3 = Nb + 3 * n, *N4 = Nb + 4 * n, *N5 = Nb + 5 * n;
+        Eb.x[c] += (T)0.5 * (N0[c] + N0[cx]);
+        Eb.y[c] += (T)0.5 * (N1[c] + N1[cy]);
+        Eb.z[c] += N2[c];
+        Bb.x[c] += (T)0.5 * (N3[c] + N3[cy]);
+        Bb.y[c] += (T)0.5 * (N4[c] + N4[cx]);
+        Bb.z[c] += (T)0.25 * (((N5[c] + N5[cx]) + N5[cy]) + N5[cxy]);
     }
 }
 
@@ -551,6 +575,11 @@ struct pic_adjoint {
     // fields: E, B, J, scratch B_a, B_t, cotangents Ebar (2), Bbar; initial E, B
     void *E[3] = {}, *B[3] = {}, *J[3] = {}, *Ba[3] = {}, *Bt[3] = {}, *Ebar[2][3] = {}, *Bbar[3] = {};
     void *E0[3] = {}, *B0[3] = {};
+    void *Nb = nullptr;               // node cotangents of the gather (6 planes)
+    // the forward run and the reverse sweep captured as CUDA graphs, rebuilt
+    // when the step count, the checkpoint interval or the particle count change
+    cudaGraphExec_t gf = nullptr, gb = nullptr;
+    long long gf_key[3] = {-1, -1, -1}, gb_key[3] = {-1, -1, -1};
     // checkpoints (every K steps) and the tape of one segment
     int K = 0, T = 0, tapeK = 0;
     std::vector<void *> ck_p, ck_f;   // per checkpoint: 6 particle arrays / 6 field arrays
@@ -676,14 +705,47 @@ void step_rev(pic_adjoint *a, PS<T> P, F3<T> E, F3<T> B, int &cur)
     k_curlB_T<T><<<gc, 256, 0, a->s>>>(g, Ebt, Bb, (T)g.fc);                        // E_t = E + c curlB(B_t) - J
     for (int k = 0; k < 3; k++) cudaMemcpyAsync(a->Ebar[cur ^ 1][k], a->Ebar[cur][k], fn, cudaMemcpyDeviceToDevice, a->s);
     k_curlE_T<T><<<gc, 256, 0, a->s>>>(g, Bb, Ebp, (T)-g.h);                        // second half step
-    k_move_T<T><<<gp, 256, 0, a->s>>>(g, P, (const T *)a->qw, a->flv, a->np, E, Ba, Ebt, ps<T>(a->pb), Ebp, Bb);
+    cudaMemsetAsync(a->Nb, 0, 6 * fn, a->s);
+    k_move_T<T><<<gp, 256, 0, a->s>>>(g, P, (const T *)a->qw, a->flv, a->np, E, Ba, Ebt, ps<T>(a->pb), (T *)a->Nb);
+    k_node_T<T><<<gc, 256, 0, a->s>>>(g, (const T *)a->Nb, Ebp, Bb);
     k_curlE_T<T><<<gc, 256, 0, a->s>>>(g, Bb, Ebp, (T)-g.h);                        // first half step
-    count_launches(7);
+    count_launches(8);
     cur ^= 1;
 }
 
+// Launch the graph cached in *ge for key, or capture enqueue() on a->s into
+// a new one first.
+template <typename F>
+int launch_cached(pic_adjoint *a, cudaGraphExec_t *ge, long long *cached, const long long key[3], F enqueue)
+{
+    if (!*ge || cached[0] != key[0] || cached[1] != key[1] || cached[2] != key[2]) {
+        if (*ge) {
+            cudaGraphExecDestroy(*ge);
+            *ge = nullptr;
+        }
+        ACK(cudaStreamBeginCapture(a->s, cudaStreamCaptureModeThreadLocal));
+        const int r = enqueue();
+        cudaGraph_t gr = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(a->s, &gr);
+        if (r || e != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            cudaGetLastError();
+            return r ? r : cstat(e);
+        }
+        const cudaError_t ei = cudaGraphInstantiate(ge, gr, 0);
+        cudaGraphDestroy(gr);
+        if (ei != cudaSuccess) {
+            *ge = nullptr;
+            return cstat(ei);
+        }
+        for (int k = 0; k < 3; k++) cached[k] = key[k];
+    }
+    ACK(cudaGraphLaunch(*ge, a->s));
+    return PIC_OK;
+}
+
 template <typename T>
-int run_forward(pic_adjoint *a, int nsteps, int K, double *objective)
+int enqueue_forward(pic_adjoint *a, int nsteps, int K)
 {
     // fresh state from the initial particles and fields
     const size_t pn = (size_t)a->np * sizeof(T), fn = cells(a) * sizeof(T);
@@ -694,6 +756,20 @@ int run_forward(pic_adjoint *a, int nsteps, int K, double *objective)
         ACK(cudaMemsetAsync(a->J[k], 0, fn, a->s));
     }
     ACK(cudaMemsetAsync(a->acc, 0, 4 * sizeof(double), a->s));
+    for (int t = 0; t < nsteps; t++) {
+        if (t % K == 0) {
+            int r = save_state<T>(a, a->ck_p[t / K], a->ck_f[t / K]);
+            if (r) return r;
+        }
+        step_fwd<T>(a, true);
+    }
+    ACK(cudaGetLastError());
+    return PIC_OK;
+}
+
+template <typename T>
+int run_forward(pic_adjoint *a, int nsteps, int K, double *objective)
+{
     const int nck = (nsteps + K - 1) / K;
     // checkpoint storage (kept between calls)
     for (int c = (int)a->ck_p.size(); c < nck; c++) {
@@ -704,14 +780,9 @@ int run_forward(pic_adjoint *a, int nsteps, int K, double *objective)
         a->ck_p.push_back(pp);
         a->ck_f.push_back(ff);
     }
-    for (int t = 0; t < nsteps; t++) {
-        if (t % K == 0) {
-            int r = save_state<T>(a, a->ck_p[t / K], a->ck_f[t / K]);
-            if (r) return r;
-        }
-        step_fwd<T>(a, true);
-    }
-    ACK(cudaGetLastError());
+    const long long key[3] = {nsteps, K, a->np};
+    int r = launch_cached(a, &a->gf, a->gf_key, key, [&] { return enqueue_forward<T>(a, nsteps, K); });
+    if (r) return r;
     ACK(cudaMemcpyAsync(objective, a->acc, sizeof(double), cudaMemcpyDeviceToHost, a->s));
     ACK(cudaStreamSynchronize(a->s));
     a->K = K;
@@ -719,24 +790,35 @@ int run_forward(pic_adjoint *a, int nsteps, int K, double *objective)
     return PIC_OK;
 }
 
+// The tape holds one segment of K steps (allocated outside any capture).
 template <typename T>
-int run_backward(pic_adjoint *a)
+int ensure_tape(pic_adjoint *a)
+{
+    const int K = a->K;
+    if (K <= a->tapeK) return PIC_OK;
+    for (void *t : {a->tape_p, a->tape_f}) {
+        if (!t) continue;
+        cudaFree(t);
+        a->allocs.erase(std::find(a->allocs.begin(), a->allocs.end(), t));
+    }
+    a->tape_p = a->tape_f = nullptr;
+    if (a->gb) {   // the cached sweep refers to the old tape
+        cudaGraphExecDestroy(a->gb);
+        a->gb = nullptr;
+    }
+    int r;
+    if ((r = aalloc(a, &a->tape_p, (size_t)K * 6 * (size_t)a->cap * sizeof(T))) ||
+        (r = aalloc(a, &a->tape_f, (size_t)K * 6 * cells(a) * sizeof(T))))
+        return r;
+    a->tapeK = K;
+    return PIC_OK;
+}
+
+template <typename T>
+int enqueue_backward(pic_adjoint *a)
 {
     const size_t pn = (size_t)a->np * sizeof(T), fn = cells(a) * sizeof(T);
     const int K = a->K, nsteps = a->T;
-    if (K > a->tapeK) {   // the tape holds one segment of K steps
-        for (void *t : {a->tape_p, a->tape_f}) {
-            if (!t) continue;
-            cudaFree(t);
-            a->allocs.erase(std::find(a->allocs.begin(), a->allocs.end(), t));
-        }
-        a->tape_p = a->tape_f = nullptr;
-        int r;
-        if ((r = aalloc(a, &a->tape_p, (size_t)K * 6 * (size_t)a->cap * sizeof(T))) ||
-            (r = aalloc(a, &a->tape_f, (size_t)K * 6 * cells(a) * sizeof(T))))
-            return r;
-        a->tapeK = K;
-    }
     for (int k = 0; k < 6; k++) ACK(cudaMemsetAsync(a->pb[k], 0, pn, a->s));
     for (int k = 0; k < 3; k++) {
         ACK(cudaMemsetAsync(a->Ebar[0][k], 0, fn, a->s));
@@ -764,8 +846,19 @@ int run_backward(pic_adjoint *a)
                         cur);
         }
     }
-    // the cotangents are of the initial state now; keep Ebar[cur] for reading
     ACK(cudaGetLastError());
+    return PIC_OK;
+}
+
+// The reverse sweep of the last forward run; the particle cotangents are of
+// the initial state afterwards.
+template <typename T>
+int run_backward(pic_adjoint *a)
+{
+    int r = ensure_tape<T>(a);
+    if (r) return r;
+    const long long key[3] = {a->T, a->K, a->np};
+    if ((r = launch_cached(a, &a->gb, a->gb_key, key, [&] { return enqueue_backward<T>(a); }))) return r;
     ACK(cudaStreamSynchronize(a->s));
     return PIC_OK;
 }
@@ -820,6 +913,8 @@ int pic_adj_create(const pic_config *cfg, pic_adjoint **out)
             if ((r = aalloc(a, &f[k], fn))) break;
             if (cudaMemset(f[k], 0, fn) != cudaSuccess) r = PIC_ERR_CUDA;
         }
+    if (!r) r = aalloc(a, &a->Nb, 6 * fn);
+    if (!r && cudaMemset(a->Nb, 0, 6 * fn) != cudaSuccess) r = PIC_ERR_CUDA;
     if (!r) r = aalloc(a, (void **)&a->acc, 4 * sizeof(double));
     if (r) {
         pic_adj_destroy(a);
@@ -833,6 +928,8 @@ void pic_adj_destroy(pic_adjoint *a)
 {
     if (!a) return;
     if (a->s) cudaStreamSynchronize(a->s);
+    if (a->gf) cudaGraphExecDestroy(a->gf);
+    if (a->gb) cudaGraphExecDestroy(a->gb);
     for (void *p : a->allocs) cudaFree(p);
     if (a->loader) pic_destroy(a->loader);
     if (a->s) cudaStreamDestroy(a->s);
