@@ -53,6 +53,9 @@ WORKLOADS = {
     # Courant 0.3 (stable next to the axis with 8 theta cells)
     "cyl_wake": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                      bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0),
+    # a small case of the same physics for profiler captures (4.2 M particles, 250 MB > L2)
+    "cyl_wake_small": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
+                           bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0, bunch_sigma_z=10.0),
 }
 SEED = 2930
 
@@ -420,48 +423,49 @@ def run_adjoint_bench(args, rank, local, peak, peak_kind):
     # gradients grow exponentially with the horizon and the zigzag current's
     # jumps make long-horizon finite differences meaningless
     sweep = []
-    with make("fp64") as a64, make("fp32") as a32:
-        a64.init_weibel(*load)
-        a32.init_weibel(*load)
-        p0, sgn = a64.fetch_particles()
-        rng = np.random.default_rng(SEED)
-        d = rng.normal(size=(3, len(p0.x)))
-        d /= np.sqrt((d * d).sum())
-
-        def fd(fn, h):
-            return (fn(h) - fn(-h)) / (2 * h)
-
-        for H in (10, 25, 50, 100, 200, 400):
-            if H > steps:
-                break
-            KH = min(K, H)
+    if not args.no_sweep:
+        with make("fp64") as a64, make("fp32") as a32:
             a64.init_weibel(*load)
-            a64.forward(H, KH)
-            g = a64.gradient()
-            a32.forward(H, KH)
-            gs = a32.gradient()
+            a32.init_weibel(*load)
+            p0, sgn = a64.fetch_particles()
+            rng = np.random.default_rng(SEED)
+            d = rng.normal(size=(3, len(p0.x)))
+            d /= np.sqrt((d * d).sum())
 
-            def j_load(dd, dti):
-                a64.init_weibel(wl["epc"], 0.5, wl["drift"] + dd, wl["temp"] + dti, wl["temp"], SEED)
-                return a64.forward(H, KH)
+            def fd(fn, h):
+                return (fn(h) - fn(-h)) / (2 * h)
 
-            def j_dir(h):
-                p = type(p0)(*(getattr(p0, f).copy() for f in p0.NAMES))
-                p.u += h * d[0]
-                p.v += h * d[1]
-                p.w += h * d[2]
-                a64.load_particles(p, sgn)
-                return a64.forward(H, KH)
+            for H in (10, 25, 50, 100, 200, 400):
+                if H > steps:
+                    break
+                KH = min(K, H)
+                a64.init_weibel(*load)
+                a64.forward(H, KH)
+                g = a64.gradient()
+                a32.forward(H, KH)
+                gs = a32.gradient()
 
-            checks = [("drift", g["drift"], fd(lambda h: j_load(h, 0), 1e-4 * wl["drift"])),
-                      ("temp_ion", g["temp_ion"], fd(lambda h: j_load(0, h), 1e-4 * wl["temp"])),
-                      ("momenta_dir", float((g["u"] * d[0] + g["v"] * d[1] + g["w"] * d[2]).sum()), fd(j_dir, 1e-4))]
-            v64h = np.concatenate([g[k] for k in ("u", "v", "w")])
-            v32h = np.concatenate([gs[k] for k in ("u", "v", "w")])
-            sweep.append({"steps": H, "grad_norm_momenta": float(np.linalg.norm(v64h)),
-                          "fp32_vs_fp64_rel_l2": float(np.linalg.norm(v32h - v64h) / np.linalg.norm(v64h)),
-                          "fd": [{"param": nme, "adjoint": ad, "fd": f, "rel_err": abs(ad - f) / max(abs(f), 1e-300)}
-                                 for nme, ad, f in checks]})
+                def j_load(dd, dti):
+                    a64.init_weibel(wl["epc"], 0.5, wl["drift"] + dd, wl["temp"] + dti, wl["temp"], SEED)
+                    return a64.forward(H, KH)
+
+                def j_dir(h):
+                    p = type(p0)(*(getattr(p0, f).copy() for f in p0.NAMES))
+                    p.u += h * d[0]
+                    p.v += h * d[1]
+                    p.w += h * d[2]
+                    a64.load_particles(p, sgn)
+                    return a64.forward(H, KH)
+
+                checks = [("drift", g["drift"], fd(lambda h: j_load(h, 0), 1e-4 * wl["drift"])),
+                          ("temp_ion", g["temp_ion"], fd(lambda h: j_load(0, h), 1e-4 * wl["temp"])),
+                          ("momenta_dir", float((g["u"] * d[0] + g["v"] * d[1] + g["w"] * d[2]).sum()), fd(j_dir, 1e-4))]
+                v64h = np.concatenate([g[k] for k in ("u", "v", "w")])
+                v32h = np.concatenate([gs[k] for k in ("u", "v", "w")])
+                sweep.append({"steps": H, "grad_norm_momenta": float(np.linalg.norm(v64h)),
+                              "fp32_vs_fp64_rel_l2": float(np.linalg.norm(v32h - v64h) / np.linalg.norm(v64h)),
+                              "fd": [{"param": nme, "adjoint": ad, "fd": f, "rel_err": abs(ad - f) / max(abs(f), 1e-300)}
+                                     for nme, ad, f in checks]})
     agree = [r["steps"] for r in sweep if all(c["rel_err"] <= 1e-2 for c in r["fd"])]
     fdc = sweep[-1]["fd"] if sweep else []
     n = out["fp32"]["n"]
@@ -579,7 +583,7 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "cyl_wake", "form": "theta-gridded FP64 (the reference's representation); "
+            "config": {"workload": args.workload, "form": "theta-gridded FP64 (the reference's representation); "
                                                        "the modal m=0,1 FP32 form is not built",
                        "cells_r_theta_z": [wl["nx"], wl["ny"], wl["nz"]], "particles": n_p, **info,
                        "courant": wl["c"], "c_ompe": wl["c_ompe"], "fdtd": "lehe (z)", "reorder_period": 20,
@@ -612,7 +616,7 @@ def run_reference(args):
 
     O.build()
     target = max(5.0, min(60.0, 3.0 * args.steps))
-    base = cpu_sample_cyl(wl, target_s=target) if args.workload == "cyl_wake" else cpu_sample(wl, target_s=target)
+    base = cpu_sample_cyl(wl, target_s=target) if args.workload.startswith("cyl") else cpu_sample(wl, target_s=target)
     line = {
         "metric": METRIC, "value": base["value"], "unit": "particle-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -635,6 +639,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-sweep", action="store_true", help="adjoint128: skip the finite-difference horizon sweep")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -653,7 +658,7 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
-    if args.workload == "cyl_wake":
+    if args.workload in ("cyl_wake", "cyl_wake_small"):
         peak, peak_kind = measured_peaks()
         return run_cyl_bench(args, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]
