@@ -53,6 +53,10 @@ WORKLOADS = {
     # Courant 0.3 (stable next to the axis with 8 theta cells)
     "cyl_wake": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                      bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0),
+    # the same run with the field solve on azimuthal modes m = 0, 1 (the theta-gridded scheme projected
+    # onto them; particles gather from / deposit onto the 8 theta cells)
+    "cyl_wake_modal": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
+                           bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0, cyl_modes=2),
     # a small case of the same physics for profiler captures (4.2 M particles, 250 MB > L2)
     "cyl_wake_small": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                            bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0, bunch_sigma_z=10.0),
@@ -552,7 +556,7 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
     n_p = len(p.x)
     cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=wl["nz"], dims=3, c=wl["c"], qi=sc["qi"], qm=(1.0, -1.0),
                     fdtd="lehe", geom="cylindrical", precision="fp64", capacity=2 * n_p + 4096,
-                    reorder_period=20, rmin=-0.5, inc_axis=1)
+                    reorder_period=20, rmin=-0.5, inc_axis=1, cyl_modes=wl.get("cyl_modes", 0))
     pinned = Particles(*(torch.from_numpy(getattr(p, k)).pin_memory().numpy() for k in Particles.NAMES))
     with Simulation(cfg) as sim:
         sim.load_particles(pinned)
@@ -583,8 +587,9 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "form": "theta-gridded FP64 (the reference's representation); "
-                                                       "the modal m=0,1 FP32 form is not built",
+            "config": {"workload": args.workload,
+                       "form": ("field solve on azimuthal modes m=0,1 (FP64), particles on the theta grid"
+                                if wl.get("cyl_modes", 0) else "theta-gridded FP64 (the reference's representation)"),
                        "cells_r_theta_z": [wl["nx"], wl["ny"], wl["nz"]], "particles": n_p, **info,
                        "courant": wl["c"], "c_ompe": wl["c_ompe"], "fdtd": "lehe (z)", "reorder_period": 20,
                        "l2": "particle state (GBs) larger than L2"},
@@ -658,7 +663,7 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
-    if args.workload in ("cyl_wake", "cyl_wake_small"):
+    if args.workload in ("cyl_wake", "cyl_wake_small", "cyl_wake_modal"):
         peak, peak_kind = measured_peaks()
         return run_cyl_bench(args, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]

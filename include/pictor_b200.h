@@ -74,7 +74,12 @@ typedef struct {
        of one CTA of the mover); 0 = chosen from the fill (capacity / cells).
        No counterpart in the reference, whose reorder is per cell. */
     int32_t brick[3];
-    int32_t reserved[4];
+    /* cylindrical: 0 = the reference's theta-gridded field solve; 2 = the
+       field solve on azimuthal modes m = 0, 1 (the theta-gridded scheme
+       projected onto them; particles still gather from and deposit onto the
+       ny theta cells).  No counterpart in the reference. */
+    int32_t cyl_modes;
+    int32_t reserved[3];
 } pic_config;
 
 typedef struct pic_handle pic_handle;

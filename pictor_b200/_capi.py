@@ -43,7 +43,8 @@ class Config(C.Structure):
         ("qm", C.c_double * (MAX_FLVR + 1)),
         ("reorder_period", C.c_int32), ("curr_filter", C.c_int32),
         ("capacity", C.c_int64),
-        ("rmin", C.c_double), ("inc_axis", C.c_int32), ("brick", C.c_int32 * 3), ("reserved", C.c_int32 * 4),
+        ("rmin", C.c_double), ("inc_axis", C.c_int32), ("brick", C.c_int32 * 3), ("cyl_modes", C.c_int32),
+        ("reserved", C.c_int32 * 3),
     ]
 
 

@@ -19,6 +19,10 @@ struct pic_handle {
     bool fp32 = false;
     void *E[3] = {}, *B[3] = {}, *J[3] = {};
     void *Jtmp = nullptr;
+    // cylindrical modal form: the fields on modes m = 0, 1, (mx, 3, mz) each;
+    // E and B above are kept equal to their theta-gridded synthesis
+    bool modal = false;
+    double *Em[3] = {}, *Bm[3] = {}, *Jm[3] = {};
     PartF64 p64[2] = {};
     PartF32 p32[2] = {};
     int cur = 0;
@@ -191,7 +195,12 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
         switch (phase) {
             case PIC_PHASE_BHALF1:  // cyl_em_update.F90:49-110 + halo
             case PIC_PHASE_BHALF2:
-                launch_cyl_bhalf(g, E, B, h->s);
+                if (h->modal) {
+                    launch_modal_bhalf(g, h->Em, h->Bm, h->s);
+                    launch_modal_synth(g, h->Bm, B, h->s);
+                } else {
+                    launch_cyl_bhalf(g, E, B, h->s);
+                }
                 break;
             case PIC_PHASE_MOVE:  // cyl_movdep_strang.F90:14-378
                 launch_cyl_move_deposit(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);
@@ -200,9 +209,17 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s);
                 break;
             case PIC_PHASE_EFIELD:  // UpdateEfield, halo, fold, AddCurrent, halo, ResetCurrent
-                launch_cyl_efield(g, 0, E, B, J, h->s);
-                launch_cyl_fold(g, J, h->s);
-                launch_cyl_efield(g, 2, E, B, J, h->s);
+                if (h->modal) {
+                    launch_modal_efield(g, 0, h->Em, h->Bm, h->Jm, h->s);
+                    launch_cyl_fold(g, J, h->s);
+                    launch_modal_project(g, J, h->Jm, h->s);
+                    launch_modal_efield(g, 2, h->Em, h->Bm, h->Jm, h->s);
+                    launch_modal_synth(g, h->Em, E, h->s);
+                } else {
+                    launch_cyl_efield(g, 0, E, B, J, h->s);
+                    launch_cyl_fold(g, J, h->s);
+                    launch_cyl_efield(g, 2, E, B, J, h->s);
+                }
                 for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(double), h->s);
                 break;
             case PIC_PHASE_REORDER:
@@ -528,6 +545,7 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (c.geom == PIC_GEOM_CYLINDRICAL &&
         (c.dims != 3 || c.precision != PIC_PREC_FP64 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
         return PIC_ERR_INVALID;
+    if (c.cyl_modes != 0 && (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4)) return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
@@ -601,6 +619,17 @@ int pic_create(const pic_config *cfg, pic_handle **out)
         if ((r = dalloc(h, (char **)&h->J[k], fb))) break;
     }
     if (!r && c.curr_filter > 0) r = dalloc(h, (char **)&h->Jtmp, fb);
+    if (!r && c.cyl_modes == 2) {
+        h->modal = true;
+        const size_t nm = (size_t)g.mx * 3 * (size_t)g.mz;
+        for (int k = 0; k < 3 && !r; k++)
+            if ((r = dalloc(h, &h->Em[k], nm)) || (r = dalloc(h, &h->Bm[k], nm)) || (r = dalloc(h, &h->Jm[k], nm))) break;
+        for (int k = 0; k < 3 && !r; k++) {
+            cudaMemsetAsync(h->Em[k], 0, nm * sizeof(double), h->s);
+            cudaMemsetAsync(h->Bm[k], 0, nm * sizeof(double), h->s);
+            cudaMemsetAsync(h->Jm[k], 0, nm * sizeof(double), h->s);
+        }
+    }
     if (!r) r = alloc_particles(h);
     if (!r && h->fp32) {
         // bricks sized for the configured fill (capacity / interior cells)
@@ -679,6 +708,14 @@ int pic_load_fields(pic_handle *h, const double *Ex, const double *Ey, const dou
             int r = load_array_f32(h, src[k], (float *)dst[k], (long long)n, seq);
             if (r) return r;
         }
+    }
+    if (h->modal) {   // the modes m = 0, 1 of the loaded fields; E, B become their synthesis
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_modal_project(h->g, E, h->Em, h->s);
+        launch_modal_project(h->g, B, h->Bm, h->s);
+        launch_modal_synth(h->g, h->Em, E, h->s);
+        launch_modal_synth(h->g, h->Bm, B, h->s);
     }
     int r = sync_both(h);
     if (r) return r;
@@ -867,7 +904,12 @@ int pic_init_weibel(pic_handle *h, double epc, double density, double drift, dou
 int pic_update_b_half(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+    if (h->modal) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_modal_bhalf(h->g, h->Em, h->Bm, h->s);
+        launch_modal_synth(h->g, h->Bm, B, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_cyl_bhalf(h->g, E, B, h->s);
@@ -923,7 +965,12 @@ int pic_exchange_particles(pic_handle *h)
 int pic_update_e(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+    if (h->modal) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_modal_efield(h->g, 0, h->Em, h->Bm, h->Jm, h->s);
+        launch_modal_synth(h->g, h->Em, E, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_cyl_efield(h->g, 0, E, B, J, h->s);
@@ -982,7 +1029,13 @@ int pic_filter_current(pic_handle *h)
 int pic_add_current(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+    if (h->modal) {
+        double *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_modal_project(h->g, J, h->Jm, h->s);
+        launch_modal_efield(h->g, 2, h->Em, h->Bm, h->Jm, h->s);
+        launch_modal_synth(h->g, h->Em, E, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_cyl_efield(h->g, 2, E, B, J, h->s);

@@ -53,6 +53,7 @@ class PicConfig:
     rmin: float = 0.0
     inc_axis: int = 1
     brick: tuple = (0, 0, 0)   # FP32 form: brick shape in cells, (0, 0, 0) = from the fill
+    cyl_modes: int = 0         # cylindrical: 0 = theta-gridded field solve, 2 = modes m = 0, 1
 
     def to_struct(self) -> _capi.Config:
         s = _capi.Config()
@@ -74,6 +75,7 @@ class PicConfig:
         s.inc_axis = self.inc_axis
         for d in range(3):
             s.brick[d] = int(self.brick[d])
+        s.cyl_modes = int(self.cyl_modes)
         return s
 
     @property
