@@ -296,6 +296,17 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
     secs = max_over_ranks(ws, t32["seconds"])
     ps = sum_over_ranks(ws, t32["particle_steps"])
     value = ps / secs
+    # the same runs with one launch per phase for each group of runs (pic_step_batched)
+    run_batched(mine, args.warmup, "fp32", tunings, per_phase=True)          # warm-up
+    barrier(ws)
+    resp, tp = run_batched(mine, args.steps, "fp32", tunings, per_phase=True)
+    secs_p = max_over_ranks(ws, tp["seconds"])
+    per_phase = {"value": sum_over_ranks(ws, tp["particle_steps"]) / secs_p, "seconds": secs_p,
+                 "gpu_launches": tp["launches"],
+                 "max_kinetic_rel_diff_vs_streams": max(abs(sum(a["kinetic"]) - sum(b["kinetic"])) / abs(sum(b["kinetic"]))
+                                                        for a, b in zip(resp, res32)),
+                 "form": "pic_step_batched: the runs in 4 groups, each phase of a group one launch over all "
+                         "its runs, one CUDA graph per group and step"}
     fp64 = None
     if not args.no_fp64:
         res64, t64 = run_batched(mine, args.steps, "fp64", None, batched=False)
@@ -364,6 +375,7 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
                     "includes": "pic_load_particles of every run from pinned FP64 host arrays + reorder + "
                                 "pic_step_many + pic_diagnostics"},
         }
+        line["one_launch_per_phase"] = per_phase
         if fp64:
             line["fp64"] = fp64
         if cpu:

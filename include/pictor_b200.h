@@ -144,6 +144,16 @@ int pic_set_step(pic_handle *h, int64_t t);
    stepped one after the other. */
 int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps);
 
+/* The same ensemble step with one launch per phase for a group of runs:
+   the runs are split into up to four groups of about equal particle count;
+   each group's B half step, mover, B half step and E update are single
+   launches over all of its runs (work items: (32, 8) blocks of every run's
+   interior, and every run's bricks), captured as one CUDA graph per group on
+   the group's stream.  Requires FP32 runs of one dimensionality and FDTD,
+   all reordered at least once (their bricks valid), without the current
+   filter; returns PIC_ERR_INVALID otherwise. */
+int pic_step_batched(pic_handle *const *hs, int32_t n, int32_t nsteps);
+
 /* Diagnostics (savedata_routines.F90:265-348), FP64 accumulation on device:
    out[0] = sum |B|^2, out[1] = sum |E|^2 over the interior (CalcFldEnergy),
    out[2] = max |divE - rho| over interior nodes, out[3] = max |rho_+|,

@@ -103,6 +103,7 @@ SIGNATURES = {
     "pic_filter_current": (C.c_int, [H]),
     "pic_step": (C.c_int, [H, C.c_int32]),
     "pic_step_many": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),
+    "pic_step_batched": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),
     "pic_set_step": (C.c_int, [H, C.c_int64]),
     "pic_diagnostics": (C.c_int, [H, C.c_double, PD, C.c_int32]),
     "pic_device_errors": (C.c_int, [H, PI32]),

@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI of include/pictor_b200.h: handle lifetime, host <->
 // device copies, the phase entry points that replace the reference's
 // `#ifdef gpu` subroutines, and the CUDA-graph step loop.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -58,6 +59,7 @@ struct pic_handle {
 };
 
 static thread_local long long g_launches = 0;
+static void batch_forget(pic_handle *h);
 
 namespace pic {
 void count_launches(int n) { g_launches += n; }
@@ -495,6 +497,204 @@ int sync_both(pic_handle *h)
 
 }  // namespace
 
+// The batched form of pic_step_many: FP32 runs of one dimensionality, all
+// reordered once (bricks valid), no current filter.  Every phase of a group
+// of runs is one launch (k_field_batch, k_move_f32_batch; the four launches
+// of a step captured in one CUDA graph on the group's stream); a run whose
+// reorder period comes up is reordered right after the step, on the same
+// stream, and its current buffer is flipped on the device.
+static bool batchable(pic_handle *const *hs, int32_t n)
+{
+    if (n < 1) return false;
+    for (int32_t a = 0; a < n; a++) {
+        const pic_handle *h = hs[a];
+        if (!h->fp32 || !h->sorted || h->g.geom != PIC_GEOM_CARTESIAN || h->cfg.curr_filter != 0 || h->profiling ||
+            h->g.dims != hs[0]->g.dims || h->g.fdtd != hs[0]->g.fdtd)
+            return false;
+    }
+    return true;
+}
+
+// The device descriptors, work lists and the captured step graph of one
+// group of runs, kept for the next call with the same runs (the descriptors
+// are uploaded again at every call: a run's current buffer may have changed).
+struct BatchGroup {
+    std::vector<pic_handle *> runs;
+    cudaStream_t s = nullptr;
+    int nf = 0, nm = 0;
+    BatchRun *druns = nullptr;
+    int *dstart = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    long long step_kernels = 0;
+    void release()
+    {
+        if (ge) cudaGraphExecDestroy(ge);
+        if (druns) cudaFree(druns);
+        if (dstart) cudaFree(dstart);
+        ge = nullptr;
+        druns = nullptr;
+        dstart = nullptr;
+        runs.clear();
+    }
+};
+struct BatchCache {
+    std::vector<pic_handle *> key;
+    std::vector<BatchGroup> groups;
+    void release()
+    {
+        for (BatchGroup &g : groups) g.release();
+        groups.clear();
+        key.clear();
+    }
+};
+static BatchCache g_batch;
+static std::mutex g_batch_mu;
+
+// A handle that goes away takes the cached batch with it.
+static void batch_forget(pic_handle *h)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    for (pic_handle *k : g_batch.key)
+        if (k == h) {
+            g_batch.release();
+            return;
+        }
+}
+
+// Runs per group: the batch is split into kBatchGroups groups of about equal
+// particle count, each stepped by its own four launches on its own stream, so
+// that the phases of different groups overlap (one group's field phase with
+// another's mover) as separate runs' step graphs do.
+constexpr int kBatchGroups = 4;
+
+static BatchRun batch_run_of(pic_handle *h)
+{
+    BatchRun R;
+    std::memset(&R, 0, sizeof(R));
+    R.g = h->g;
+    R.p[0] = h->p32[0];
+    R.p[1] = h->p32[1];
+    R.bk = h->bricks;
+    for (int k = 0; k < 3; k++) {
+        R.E[k] = (float *)h->E[k];
+        R.B[k] = (float *)h->B[k];
+        R.J[k] = (float *)h->J[k];
+    }
+    R.err = h->err;
+    R.cur = h->cur;
+    R.fb[0] = (h->g.nx + 31) / 32;
+    R.fb[1] = (h->g.ny + 7) / 8;
+    R.fb[2] = h->g.dims == 3 ? h->g.nz : 1;
+    return R;
+}
+
+// Upload the group's descriptors and work lists; capture its step graph the
+// first time.
+static int batch_group_prepare(BatchGroup &G, bool fresh)
+{
+    const int n = (int)G.runs.size();
+    pic_handle *h0 = G.runs[0];
+    std::vector<BatchRun> runs((size_t)n);
+    std::vector<int> starts(2 * ((size_t)n + 1), 0);
+    int *fstart = starts.data(), *mstart = starts.data() + n + 1;
+    for (int a = 0; a < n; a++) {
+        runs[(size_t)a] = batch_run_of(G.runs[(size_t)a]);
+        const BatchRun &R = runs[(size_t)a];
+        fstart[a + 1] = fstart[a] + R.fb[0] * R.fb[1] * R.fb[2];
+        mstart[a + 1] = mstart[a] + R.bk.ntiles;
+    }
+    if (fresh) {
+        G.s = h0->s;
+        G.nf = fstart[n];
+        G.nm = mstart[n];
+        if (cudaMalloc(&G.druns, sizeof(BatchRun) * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&G.dstart, sizeof(int) * starts.size()) != cudaSuccess)
+            return PIC_ERR_OOM;
+    }
+    CK(cudaMemcpyAsync(G.druns, runs.data(), sizeof(BatchRun) * (size_t)n, cudaMemcpyHostToDevice, G.s));
+    CK(cudaMemcpyAsync(G.dstart, starts.data(), sizeof(int) * starts.size(), cudaMemcpyHostToDevice, G.s));
+    CK(cudaStreamSynchronize(G.s));
+    if (!fresh) return PIC_OK;
+    // one step of every run: B half, move + deposit, B half, E + fold + AddCurrent
+    const int dims = h0->g.dims, fdtd = h0->g.fdtd;
+    g_launches = 0;
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(G.s, cudaStreamCaptureModeThreadLocal));
+    launch_batch_bhalf(dims, fdtd, G.druns, G.dstart, n, G.nf, G.s);
+    launch_batch_move(dims, G.druns, G.dstart + n + 1, n, G.nm, G.s);
+    launch_batch_bhalf(dims, fdtd, G.druns, G.dstart, n, G.nf, G.s);
+    launch_batch_efield(dims, G.druns, G.dstart, n, G.nf, G.s);
+    G.step_kernels = g_launches;
+    const cudaError_t e = cudaStreamEndCapture(G.s, &gr);
+    const cudaError_t ei = e == cudaSuccess ? cudaGraphInstantiate(&G.ge, gr, 0) : e;
+    if (gr) cudaGraphDestroy(gr);
+    if (ei != cudaSuccess) {
+        G.ge = nullptr;
+        return cuda_status(ei);
+    }
+    return PIC_OK;
+}
+
+static int step_many_batched(pic_handle *const *hs, int32_t n, int32_t nsteps)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    for (int32_t a = 0; a < n; a++) CK(cudaStreamSynchronize(hs[a]->s));
+    BatchCache &C = g_batch;
+    const bool same = !C.groups.empty() && C.key.size() == (size_t)n && std::equal(C.key.begin(), C.key.end(), hs);
+    if (!same) {
+        C.release();
+        // largest first, dealt to the lightest group
+        std::vector<int32_t> order((size_t)n);
+        for (int32_t a = 0; a < n; a++) order[(size_t)a] = a;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t x, int32_t y) { return hs[x]->capacity > hs[y]->capacity; });
+        const int ng = n < kBatchGroups ? (int)n : kBatchGroups;
+        C.groups.resize((size_t)ng);
+        std::vector<long long> load((size_t)ng, 0);
+        for (int32_t a : order) {
+            size_t gi = 0;
+            for (size_t q = 1; q < load.size(); q++)
+                if (load[q] < load[gi]) gi = q;
+            C.groups[gi].runs.push_back(hs[a]);
+            load[gi] += hs[a]->capacity;
+        }
+        C.key.assign(hs, hs + n);
+    }
+    for (BatchGroup &G : C.groups) {
+        for (pic_handle *h : G.runs)
+            for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), G.runs[0]->s));
+        const int r = batch_group_prepare(G, !same);
+        if (r) {
+            C.release();
+            return r;
+        }
+    }
+    for (int32_t i = 0; i < nsteps; i++)
+        for (BatchGroup &G : C.groups) {
+            CK(cudaGraphLaunch(G.ge, G.s));
+            G.runs[0]->launches += G.step_kernels;
+            for (size_t a = 0; a < G.runs.size(); a++) {
+                pic_handle *h = G.runs[a];
+                h->t += 1;
+                if (h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0) {
+                    g_launches = 0;
+                    launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->capacity, h->bricks,
+                                       h->err, G.s);
+                    launch_batch_flip(G.druns, (int)a, G.s);
+                    h->launches += g_launches;
+                    h->cur ^= 1;
+                }
+            }
+        }
+    for (BatchGroup &G : C.groups) CK(cudaStreamSynchronize(G.s));
+    int first = PIC_OK;
+    for (int32_t a = 0; a < n; a++) {
+        const int q = finish(hs[a]);
+        if (q && !first) first = q;
+    }
+    return first;
+}
+
 extern "C" {
 
 int pic_version(void) { return 10000; }
@@ -517,6 +717,7 @@ const char *pic_error_string(int code)
 
 void pic_destroy(pic_handle *h)
 {
+    if (h) batch_forget(h);
     if (!h) return;
     if (h->s) cudaStreamSynchronize(h->s);
     if (h->cs) cudaStreamSynchronize(h->cs);
@@ -1088,6 +1289,16 @@ int pic_step(pic_handle *h, int32_t nsteps)
         if (r) return r;
     }
     return finish(h);
+}
+
+int pic_step_batched(pic_handle *const *hs, int32_t n, int32_t nsteps)
+{
+    if (!hs || n < 1 || nsteps < 0) return PIC_ERR_INVALID;
+    for (int32_t a = 0; a < n; a++)
+        if (!hs[a]) return PIC_ERR_INVALID;
+    if (!batchable(hs, n)) return PIC_ERR_INVALID;
+    if (nsteps == 0) return PIC_OK;
+    return step_many_batched(hs, n, nsteps);
 }
 
 int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps)

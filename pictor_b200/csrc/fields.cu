@@ -117,25 +117,31 @@ struct CellIter {
     bool ok;
 };
 
+// Interior cell of thread (threadIdx.x, threadIdx.y) in block (bx, by, bz)
+// of the (32, 8) tiling of the interior.
+template <int DIMS>
+__device__ __forceinline__ CellIter interior_cell_at(const GridP &g, int bx, int by, int bz)
+{
+    CellIter it;
+    it.i = 3 + bx * blockDim.x + threadIdx.x;
+    it.j = 3 + by * blockDim.y + threadIdx.y;
+    it.k = DIMS == 3 ? 3 + bz : 1;
+    it.ok = it.i <= g.mx - 3 && it.j <= g.my - 3;
+    return it;
+}
 template <int DIMS>
 __device__ __forceinline__ CellIter interior_cell(const GridP &g)
 {
-    CellIter it;
-    it.i = 3 + blockIdx.x * blockDim.x + threadIdx.x;
-    it.j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
-    it.k = DIMS == 3 ? 3 + (int)blockIdx.z : 1;
-    it.ok = it.i <= g.mx - 3 && it.j <= g.my - 3;
-    return it;
+    return interior_cell_at<DIMS>(g, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
 // ---------------------------------------------------------------------------
 // B <- B - (c/2) curl E (UpdateBfieldHalf) + halo (SendRecvFlds(B)).
 // ---------------------------------------------------------------------------
 template <typename T, int DIMS, int FDTD>
-__global__ void __launch_bounds__(256) k_bhalf(GridP g, const T *__restrict__ Ex, const T *__restrict__ Ey,
-                                               const T *__restrict__ Ez, T *Bx, T *By, T *Bz)
+__device__ __forceinline__ void bhalf_at(const GridP &g, const CellIter &it, const T *__restrict__ Ex,
+                                         const T *__restrict__ Ey, const T *__restrict__ Ez, T *Bx, T *By, T *Bz)
 {
-    const CellIter it = interior_cell<DIMS>(g);
     if (!it.ok) return;
     const Coef<T> C(g);
     const T h = C.h;
@@ -166,6 +172,13 @@ __global__ void __launch_bounds__(256) k_bhalf(GridP g, const T *__restrict__ Ex
     store_with_images<T, DIMS>(g, Bx, it.i, it.j, it.k, bx);
     store_with_images<T, DIMS>(g, By, it.i, it.j, it.k, by);
     store_with_images<T, DIMS>(g, Bz, it.i, it.j, it.k, bz);
+}
+
+template <typename T, int DIMS, int FDTD>
+__global__ void __launch_bounds__(256) k_bhalf(GridP g, const T *__restrict__ Ex, const T *__restrict__ Ey,
+                                               const T *__restrict__ Ez, T *Bx, T *By, T *Bz)
+{
+    bhalf_at<T, DIMS, FDTD>(g, interior_cell<DIMS>(g), Ex, Ey, Ez, Bx, By, Bz);
 }
 
 // Yee E update of one cell (em_update.F90:27-34; Lehe keeps it, em_update_lehe.F90:174-181).
@@ -239,12 +252,11 @@ __device__ __forceinline__ void zero_fold_cells(const GridP &g, T *__restrict__ 
 // load sequence on J serialised the memory latency).
 // ---------------------------------------------------------------------------
 template <typename T, int DIMS, int MODE>
-__global__ void __launch_bounds__(256) k_efield(GridP g, T *__restrict__ Ex, T *__restrict__ Ey, T *__restrict__ Ez,
-                                                const T *__restrict__ Bx, const T *__restrict__ By,
-                                                const T *__restrict__ Bz, T *__restrict__ Jx, T *__restrict__ Jy,
-                                                T *__restrict__ Jz)
+__device__ __forceinline__ void efield_at(const GridP &g, const CellIter &it, T *__restrict__ Ex, T *__restrict__ Ey,
+                                          T *__restrict__ Ez, const T *__restrict__ Bx, const T *__restrict__ By,
+                                          const T *__restrict__ Bz, T *__restrict__ Jx, T *__restrict__ Jy,
+                                          T *__restrict__ Jz)
 {
-    const CellIter it = interior_cell<DIMS>(g);
     if (!it.ok) return;
     const long long c0 = cidx(g, it.i, it.j, it.k);
     T ex, ey, ez, jx = (T)0, jy = (T)0, jz = (T)0;
@@ -277,6 +289,15 @@ __global__ void __launch_bounds__(256) k_efield(GridP g, T *__restrict__ Ex, T *
         zero_fold_cells<T, DIMS>(g, Jy, it.i, it.j, it.k);
         zero_fold_cells<T, DIMS>(g, Jz, it.i, it.j, it.k);
     }
+}
+
+template <typename T, int DIMS, int MODE>
+__global__ void __launch_bounds__(256) k_efield(GridP g, T *__restrict__ Ex, T *__restrict__ Ey, T *__restrict__ Ez,
+                                                const T *__restrict__ Bx, const T *__restrict__ By,
+                                                const T *__restrict__ Bz, T *__restrict__ Jx, T *__restrict__ Jy,
+                                                T *__restrict__ Jz)
+{
+    efield_at<T, DIMS, MODE>(g, interior_cell<DIMS>(g), Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz);
 }
 
 // UpdateCurrentAllFaces as a separate phase: J(interior) <- fold(J).  Each J
@@ -319,6 +340,91 @@ __global__ void __launch_bounds__(256) k_filter_axis(GridP g, int axis, const T 
 static dim3 interior_grid(const GridP &g)
 {
     return dim3((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 7) / 8), (unsigned)(g.dims == 3 ? g.nz : 1));
+}
+
+// ---------------------------------------------------------------------------
+// Batched field phases: one persistent launch for all runs of a batch.  A
+// CTA takes work items (a (32, 8) block of one run's interior) in turn; the
+// run's grid description is copied into shared memory for the item.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int batch_run_of(const int *__restrict__ start, int n, int item)
+{
+    int lo = 0, hi = n;   // start[lo] <= item < start[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (start[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// Copy the words of *src into *dst with the threads of the block.
+template <typename S>
+__device__ __forceinline__ void block_copy(S *dst, const S *src)
+{
+    static_assert(sizeof(S) % 4 == 0, "word copy");
+    const int *a = reinterpret_cast<const int *>(src);
+    int *b = reinterpret_cast<int *>(dst);
+    const int nt = blockDim.x * blockDim.y;
+    for (int w = threadIdx.y * blockDim.x + threadIdx.x; w < (int)(sizeof(S) / 4); w += nt) b[w] = a[w];
+}
+
+template <int DIMS, int FDTD, int PHASE>   // PHASE 0: B half step, 1: E update + fold + AddCurrent + zero J
+__global__ void __launch_bounds__(256) k_field_batch(const BatchRun *__restrict__ runs, const int *__restrict__ start,
+                                                     int n, int total)
+{
+    __shared__ BatchRun sr;
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+        const int r = batch_run_of(start, n, item);
+        __syncthreads();   // the previous item is done with sr
+        block_copy(&sr, &runs[r]);
+        __syncthreads();
+        const int local = item - start[r];
+        const int bx = local % sr.fb[0], byz = local / sr.fb[0], by = byz % sr.fb[1], bz = byz / sr.fb[1];
+        const CellIter it = interior_cell_at<DIMS>(sr.g, bx, by, bz);
+        if (PHASE == 0)
+            bhalf_at<float, DIMS, FDTD>(sr.g, it, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1], sr.B[2]);
+        else
+            efield_at<float, DIMS, 1>(sr.g, it, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1], sr.B[2], sr.J[0], sr.J[1],
+                                      sr.J[2]);
+    }
+}
+
+static unsigned batch_grid(int total)
+{
+    const int cap = kSMs * 8;
+    return (unsigned)(total < cap ? (total > 0 ? total : 1) : cap);
+}
+
+void launch_batch_bhalf(int dims, int fdtd, const BatchRun *runs, const int *fstart, int n, int total, cudaStream_t s)
+{
+    const dim3 block(32, 8, 1);
+    const unsigned grid = batch_grid(total);
+    if (dims == 3) {
+        if (fdtd == PIC_FDTD_YEE) k_field_batch<3, PIC_FDTD_YEE, 0><<<grid, block, 0, s>>>(runs, fstart, n, total);
+        else k_field_batch<3, PIC_FDTD_LEHE, 0><<<grid, block, 0, s>>>(runs, fstart, n, total);
+    } else {
+        if (fdtd == PIC_FDTD_YEE) k_field_batch<2, PIC_FDTD_YEE, 0><<<grid, block, 0, s>>>(runs, fstart, n, total);
+        else k_field_batch<2, PIC_FDTD_LEHE, 0><<<grid, block, 0, s>>>(runs, fstart, n, total);
+    }
+    count_launches(1);
+}
+
+void launch_batch_efield(int dims, const BatchRun *runs, const int *fstart, int n, int total, cudaStream_t s)
+{
+    const dim3 block(32, 8, 1);
+    const unsigned grid = batch_grid(total);
+    if (dims == 3) k_field_batch<3, PIC_FDTD_YEE, 1><<<grid, block, 0, s>>>(runs, fstart, n, total);
+    else k_field_batch<2, PIC_FDTD_YEE, 1><<<grid, block, 0, s>>>(runs, fstart, n, total);
+    count_launches(1);
+}
+
+__global__ void k_batch_flip(BatchRun *runs, int r) { runs[r].cur ^= 1; }
+
+void launch_batch_flip(BatchRun *runs, int r, cudaStream_t s)
+{
+    k_batch_flip<<<1, 1, 0, s>>>(runs, r);
+    count_launches(1);
 }
 
 template <typename T>

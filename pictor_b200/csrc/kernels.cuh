@@ -81,6 +81,24 @@ constexpr int kBoxAxisMax = 64;   // cells per axis of a mover box
 // each side would not fit the mover's shared memory.
 bool choose_bricks(const GridP &g, double ppc, const int req[3], Bricks &bk);
 // Tiled FP32 mover: one CTA per brick.
+// One run of a batch of FP32 runs stepped by shared kernels (one launch per
+// phase for all runs).  `cur` is the run's current particle buffer; a
+// reorder of the run flips it on the device (launch_batch_flip).
+struct BatchRun {
+    GridP g;
+    PartF32 p[2];
+    Bricks bk;
+    float *E[3], *B[3], *J[3];
+    int *err;
+    int cur;
+    int fb[3];   // blocks of the (32, 8) interior tiling of the field kernels
+};
+// Work lists: run r owns field items [fstart[r], fstart[r+1]) and bricks
+// [mstart[r], mstart[r+1]).
+void launch_batch_bhalf(int dims, int fdtd, const BatchRun *runs, const int *fstart, int n, int total, cudaStream_t s);
+void launch_batch_efield(int dims, const BatchRun *runs, const int *fstart, int n, int total, cudaStream_t s);
+void launch_batch_move(int dims, const BatchRun *runs, const int *mstart, int n, int total, cudaStream_t s);
+void launch_batch_flip(BatchRun *runs, int r, cudaStream_t s);
 void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
                                    float *const B[3], float *const J[3], int *err, cudaStream_t s);
 

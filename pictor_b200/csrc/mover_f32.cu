@@ -706,17 +706,22 @@ __device__ __forceinline__ int interior_of(int a, int n)
     return a;
 }
 
+// Static shared memory of one brick's move (the node and current boxes are
+// the dynamic part, sm).
+struct TileShared {
+    int red[kTileWarps][6];
+    int s_off[3][kBoxAxisMax + 3];
+    float s_q[kTileWarps][kQueueRows][32];
+};
+
+// Move the particles of brick b (one CTA).
 template <int DIMS>
-__global__ void __launch_bounds__(kTileThreads, 3)
-    k_move_f32_tiled(GridP g, PartF32 p, Bricks bk, const float *__restrict__ Ex, const float *__restrict__ Ey,
-                     const float *__restrict__ Ez, const float *__restrict__ Bx, const float *__restrict__ By,
-                     const float *__restrict__ Bz, float *Jx, float *Jy, float *Jz, int *err)
+__device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, const Bricks &bk, int b, float *sm,
+                                           TileShared &ts, const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                           const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                           const float *__restrict__ By, const float *__restrict__ Bz, float *Jx,
+                                           float *Jy, float *Jz, int *err)
 {
-    extern __shared__ __align__(16) float sm[];
-    __shared__ int red[kTileWarps][6];
-    __shared__ int s_off[3][kBoxAxisMax + 3];
-    __shared__ float s_q[kTileWarps][kQueueRows][32];
-    const int b = blockIdx.x;
     const uint32_t p0 = bk.tile_start[b], p1 = bk.tile_start[b + 1];
     if (p0 >= p1) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -793,8 +798,8 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 #pragma unroll
         for (int d = 0; d < DIMS; d++)
             for (int t = tid; t < ext[d]; t += kTileThreads)
-                s_off[d][t] = (interior_of(tb.hc[d] + lo[d] - 1 + t, n3[d]) - 1) * str[d];
-        if (DIMS == 2 && tid == 0) s_off[2][0] = 0;
+                ts.s_off[d][t] = (interior_of(tb.hc[d] + lo[d] - 1 + t, n3[d]) - 1) * str[d];
+        if (DIMS == 2 && tid == 0) ts.s_off[2][0] = 0;
     }
     for (int q = tid; q < 3 * tb.njc; q += kTileThreads) sJ[q] = 0;
     __syncthreads();
@@ -806,7 +811,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
         for (int q = tid; q < nnode; q += kTileThreads) {
             const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * NX;
             const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * NY;
-            const int nd = s_off[0][xx + 1] + s_off[1][yy + 1] + (DIMS == 3 ? s_off[2][zz + 1] : 0);
+            const int nd = ts.s_off[0][xx + 1] + ts.s_off[1][yy + 1] + (DIMS == 3 ? ts.s_off[2][zz + 1] : 0);
             float4 A;
             float2 Bv;
             node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
@@ -818,7 +823,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 
     Bounds bd;
     bd.init();
-    push_range_tiled<DIMS>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, s_q[warp]);
+    push_range_tiled<DIMS>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, ts.s_q[warp]);
     __syncthreads();
 
     // add the box current to the periodic interior image of each cell
@@ -828,7 +833,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
         for (int q = tid; q < tb.njc; q += kTileThreads) {
             const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * JX;
             const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * JY;
-            const int off = s_off[0][xx] + s_off[1][yy] + (DIMS == 3 ? s_off[2][zz] : 0);
+            const int off = ts.s_off[0][xx] + ts.s_off[1][yy] + (DIMS == 3 ? ts.s_off[2][zz] : 0);
             const int vx = sJ[q], vy = sJ[tb.njc + q], vz = sJ[2 * tb.njc + q];
             if (vx != 0) atomicAdd(Jx + off, (float)vx * inv);
             if (vy != 0) atomicAdd(Jy + off, (float)vy * inv);
@@ -842,13 +847,13 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     for (int e = 0; e < 6; e++) v[e] = __reduce_min_sync(0xffffffffu, v[e]);
     if (lane == 0)
 #pragma unroll
-        for (int e = 0; e < 6; e++) red[warp][e] = v[e];
+        for (int e = 0; e < 6; e++) ts.red[warp][e] = v[e];
     __syncthreads();
     if (tid == 0) {
         int m[6];
         for (int e = 0; e < 6; e++) {
-            m[e] = red[0][e];
-            for (int w2 = 1; w2 < kTileWarps; w2++) m[e] = min(m[e], red[w2][e]);
+            m[e] = ts.red[0][e];
+            for (int w2 = 1; w2 < kTileWarps; w2++) m[e] = min(m[e], ts.red[w2][e]);
         }
         int *ob = bk.box + 8 * (size_t)b;
         const bool empty = m[0] == 0x3fffffff;
@@ -865,6 +870,64 @@ __global__ void __launch_bounds__(kTileThreads, 3)
             }
         }
     }
+}
+
+template <int DIMS>
+__global__ void __launch_bounds__(kTileThreads, 3)
+    k_move_f32_tiled(GridP g, PartF32 p, Bricks bk, const float *__restrict__ Ex, const float *__restrict__ Ey,
+                     const float *__restrict__ Ez, const float *__restrict__ Bx, const float *__restrict__ By,
+                     const float *__restrict__ Bz, float *Jx, float *Jy, float *Jz, int *err)
+{
+    extern __shared__ __align__(16) float sm[];
+    __shared__ TileShared ts;
+    move_brick<DIMS>(g, p, bk, blockIdx.x, sm, ts, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err);
+}
+
+// The tiled mover for all runs of a batch in one launch: CTA b takes brick b
+// of the concatenated brick list (the run's description copied into shared
+// memory).
+__device__ __forceinline__ int batch_run_of_m(const int *__restrict__ start, int n, int item)
+{
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (start[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <int DIMS>
+__global__ void __launch_bounds__(kTileThreads, 3)
+    k_move_f32_batch(const BatchRun *__restrict__ runs, const int *__restrict__ start, int n)
+{
+    extern __shared__ __align__(16) float sm[];
+    __shared__ TileShared ts;
+    __shared__ BatchRun sr;
+    const int item = blockIdx.x;
+    const int r = batch_run_of_m(start, n, item);
+    {
+        const int *a = reinterpret_cast<const int *>(&runs[r]);
+        int *d = reinterpret_cast<int *>(&sr);
+        for (int w = threadIdx.x; w < (int)(sizeof(BatchRun) / 4); w += kTileThreads) d[w] = a[w];
+    }
+    __syncthreads();
+    move_brick<DIMS>(sr.g, sr.p[sr.cur], sr.bk, item - start[r], sm, ts, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1],
+                     sr.B[2], sr.J[0], sr.J[1], sr.J[2], sr.err);
+}
+
+void launch_batch_move(int dims, const BatchRun *runs, const int *mstart, int n, int total, cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_move_f32_batch<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_batch<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        attr_set = true;
+    }
+    if (total <= 0) return;
+    if (dims == 3) k_move_f32_batch<3><<<total, kTileThreads, kBrickSmemBytes, s>>>(runs, mstart, n);
+    else k_move_f32_batch<2><<<total, kTileThreads, kBrickSmemBytes, s>>>(runs, mstart, n);
+    count_launches(1);
 }
 
 void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],

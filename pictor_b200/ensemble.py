@@ -206,10 +206,11 @@ def tune_classes(runs: list[RunSpec], **kw) -> dict:
 
 
 def run_batched(runs: list[RunSpec], steps: int, precision: str = "fp32", tunings: dict | None = None,
-                batched: bool = True) -> tuple[list[dict], dict]:
+                batched: bool = True, per_phase: bool = False) -> tuple[list[dict], dict]:
     """Step every run of the list `steps` times on the current GPU, together
-    (pic_step_many) or one after the other; returns the per-run diagnostics
-    and the timing {seconds, particle_steps, value, launches}."""
+    (pic_step_many, or with per_phase pic_step_batched: one launch per phase
+    for each group of runs) or one after the other; returns the per-run
+    diagnostics and the timing {seconds, particle_steps, value, launches}."""
     import torch
 
     from .simulation import step_many
@@ -226,7 +227,7 @@ def run_batched(runs: list[RunSpec], steps: int, precision: str = "fp32", tuning
             s.launch_count()   # reset the per-handle kernel counters
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        step_many([s for s, _ in sims], steps)
+        step_many([s for s, _ in sims], steps, per_phase=per_phase)
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
         launches = sum(s.launch_count() for s, _ in sims)

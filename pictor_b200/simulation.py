@@ -282,13 +282,17 @@ class Simulation:
         return self.L.pic_stream(self.h)
 
 
-def step_many(sims, nsteps: int = 1) -> None:
+def step_many(sims, nsteps: int = 1, per_phase: bool = False) -> None:
     """pic_step_many: nsteps steps of every simulation of an ensemble, their
     step graphs interleaved on their own streams so that small runs overlap
-    on the GPU (all on the current device)."""
+    on the GPU (all on the current device).  per_phase: pic_step_batched,
+    one launch per phase for each group of runs (FP32, all reordered)."""
     sims = list(sims)
     if not sims:
         return
     L = sims[0].L
     arr = (C.c_void_p * len(sims))(*[s.h.value for s in sims])
-    check(L.pic_step_many(arr, len(sims), int(nsteps)), "pic_step_many")
+    if per_phase:
+        check(L.pic_step_batched(arr, len(sims), int(nsteps)), "pic_step_batched")
+    else:
+        check(L.pic_step_many(arr, len(sims), int(nsteps)), "pic_step_many")

@@ -32,6 +32,21 @@ def test_step_many_matches_separate_steps(precision):
     assert t1["particle_steps"] == t2["particle_steps"]
 
 
+def test_one_launch_per_phase_matches_separate_steps():
+    """pic_step_batched (every phase of a group of runs in one launch, the
+    runs' reorders in between) against the runs stepped one after the other:
+    the same particles per run and energies to FP32 summation-order noise."""
+    runs = _runs()
+    together, t1 = run_batched(runs, 12, "fp32", batched=True, per_phase=True)
+    alone, t2 = run_batched(runs, 12, "fp32", batched=False)
+    for a, b in zip(together, alone):
+        assert a["particles"] == b["particles"]
+        np.testing.assert_allclose(a["kinetic"], b["kinetic"], rtol=1e-5)
+        np.testing.assert_allclose(a["B2"] + a["E2"], b["B2"] + b["E2"], rtol=1e-3)
+    # four launches per group (at most four groups) and step; no reorder is due in 12 steps
+    assert t1["launches"] == 4 * min(len(runs), 4) * 12
+
+
 def test_brick_override_keeps_the_physics():
     """A requested brick shape changes how particles are grouped, not the
     step: energies after 10 steps match the automatic shape."""
