@@ -456,6 +456,7 @@ def run_adjoint_bench(args, rank, local, peak, peak_kind):
                     break
                 KH = min(K, H)
                 a64.init_weibel(*load)
+                a64.branches("record")
                 a64.forward(H, KH)
                 g = a64.gradient()
                 a32.forward(H, KH)
@@ -473,16 +474,29 @@ def run_adjoint_bench(args, rank, local, peak, peak_kind):
                     a64.load_particles(p, sgn)
                     return a64.forward(H, KH)
 
-                checks = [("drift", g["drift"], fd(lambda h: j_load(h, 0), 1e-4 * wl["drift"])),
-                          ("temp_ion", g["temp_ion"], fd(lambda h: j_load(0, h), 1e-4 * wl["temp"])),
-                          ("momenta_dir", float((g["u"] * d[0] + g["v"] * d[1] + g["w"] * d[2]).sum()), fd(j_dir, 1e-4))]
+                def fd_checks():
+                    return [("drift", g["drift"], fd(lambda h: j_load(h, 0), 1e-4 * wl["drift"])),
+                            ("temp_ion", g["temp_ion"], fd(lambda h: j_load(0, h), 1e-4 * wl["temp"])),
+                            ("momenta_dir", float((g["u"] * d[0] + g["v"] * d[1] + g["w"] * d[2]).sum()),
+                             fd(j_dir, 1e-4))]
+
+                # perturbed runs replaying the base run's discrete decisions (smooth in the inputs),
+                # then free ones (straddling the zigzag current's jumps)
+                a64.branches("replay")
+                frozen = fd_checks()
+                a64.branches("free")
+                checks = fd_checks()
                 v64h = np.concatenate([g[k] for k in ("u", "v", "w")])
                 v32h = np.concatenate([gs[k] for k in ("u", "v", "w")])
                 sweep.append({"steps": H, "grad_norm_momenta": float(np.linalg.norm(v64h)),
                               "fp32_vs_fp64_rel_l2": float(np.linalg.norm(v32h - v64h) / np.linalg.norm(v64h)),
                               "fd": [{"param": nme, "adjoint": ad, "fd": f, "rel_err": abs(ad - f) / max(abs(f), 1e-300)}
-                                     for nme, ad, f in checks]})
+                                     for nme, ad, f in checks],
+                              "fd_frozen_branches": [{"param": nme, "adjoint": ad, "fd": f,
+                                                      "rel_err": abs(ad - f) / max(abs(f), 1e-300)}
+                                                     for nme, ad, f in frozen]})
     agree = [r["steps"] for r in sweep if all(c["rel_err"] <= 1e-2 for c in r["fd"])]
+    agree_frozen = [r["steps"] for r in sweep if all(c["rel_err"] <= 1e-3 for c in r["fd_frozen_branches"])]
     fdc = sweep[-1]["fd"] if sweep else []
     n = out["fp32"]["n"]
     t32 = out["fp32"]["t_forward"] + out["fp32"]["t_gradient"]
@@ -511,6 +525,7 @@ def run_adjoint_bench(args, rank, local, peak, peak_kind):
             "fd_mismatch_fraction_full_horizon": (sum(1 for c in fdc if c["rel_err"] > 1e-2) / len(fdc)) if fdc else None,
             "horizon_sweep": sweep,
             "fd_agreement_1e-2_up_to_steps": max(agree) if agree else 0,
+            "fd_frozen_branches_agreement_1e-3_up_to_steps": max(agree_frozen) if agree_frozen else 0,
             "roofline": {"bound": "hbm", "achieved": None, "peak": peak, "unit": "GB/s", "frac": None,
                          "traffic": None, "kernel": "k_move_T (mover adjoint), latency/atomic bound at this size",
                          "peak_kind": peak_kind},

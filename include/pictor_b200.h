@@ -231,6 +231,15 @@ int pic_adj_fetch_particles(pic_adjoint *a, int64_t *n, double *q, double *x, do
 /* nsteps steps from the initial state, keeping the state every
    checkpoint_every steps; *objective = J. */
 int pic_adj_forward(pic_adjoint *a, int32_t nsteps, int32_t checkpoint_every, double *objective);
+/* Branches of the forward mover for the following pic_adj_forward calls:
+   0 free (default); 1 record the discrete decisions of every particle and
+   step (start and end cells, the side of the relay point's clamp, the
+   periodic wrap); 2 replay the recorded ones (same particle count, at most
+   the recorded step count), which makes the run a smooth function of the
+   initial state whose derivative at the recorded run is the adjoint's:
+   central differences of replayed runs check the gradient without the jumps
+   of the zigzag current.  The reverse sweep always recomputes freely. */
+int pic_adj_branches(pic_adjoint *a, int32_t mode);
 /* Reverse sweep of the last forward run (each segment between checkpoints is
    recomputed): dJ/d(initial u, v, w, x, y) per particle (host arrays of n, any
    may be NULL) and dparam[0] = dJ/d drift, dparam[1..2] = dJ/d temperature of

@@ -118,6 +118,7 @@ SIGNATURES = {
     "pic_adj_load_particles": (C.c_int, [C.c_void_p, C.c_int64] + [PD] * 7 + [PI32, PD]),
     "pic_adj_fetch_particles": (C.c_int, [C.c_void_p, PI64] + [PD] * 7 + [PI32, PD]),
     "pic_adj_forward": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, PD]),
+    "pic_adj_branches": (C.c_int, [C.c_void_p, C.c_int32]),
     "pic_adj_gradient": (C.c_int, [C.c_void_p, C.c_double, PD, PD, PD, PD, PD, PD, PD]),
     "pic_error_string": (C.c_char_p, [C.c_int]),
     "pic_stream": (C.c_void_p, [H]),

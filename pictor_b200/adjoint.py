@@ -76,6 +76,11 @@ class Adjoint:
               "pic_adj_fetch_particles")
         return p, sgn
 
+    def branches(self, mode: str) -> None:
+        """'free' (default), 'record' the mover's discrete decisions in the
+        next forward runs, or 'replay' them (pic_adj_branches)."""
+        check(self.L.pic_adj_branches(self.h, {"free": 0, "record": 1, "replay": 2}[mode]), "pic_adj_branches")
+
     def forward(self, nsteps: int, checkpoint_every: int = 50) -> float:
         """J of nsteps steps from the initial state (state kept every
         checkpoint_every steps for the reverse sweep)."""

@@ -196,12 +196,63 @@ __device__ __forceinline__ T relay(int i0, int i1, T mid, bool &active)
     return fmin(hi, fmax(lo, mid));
 }
 
-template <typename T>
-__device__ void move_fwd(const AG &g, T x0, T y0, T z0, T u, T v, T w, T qthis, T qm, const F3<T> &E, const F3<T> &B,
-                         Mv<T> &M)
+// Frozen branches.  The step is piecewise smooth in the state: floor() of
+// the start and end positions, the side the relay point's clamp takes and
+// the periodic wrap are discrete decisions.  A forward run can record them
+// per particle and step (one word each) and a later run replay them, which
+// makes the replayed run a smooth function of its inputs whose derivative
+// at the recorded state is the adjoint's (the derivative of the active
+// branch): central differences of replayed runs check the adjoint without
+// the jumps of the zigzag current.  Word: start cell x, y (20 bits each),
+// end-cell offsets + 1, relay sides (0 lower bound, 1 midpoint, 2 upper
+// bound), wrap shifts + 1 (2 bits each).
+enum { kBranchFree = 0, kBranchRecord = 1, kBranchReplay = 2 };
+
+struct Branch {
+    int ip0, jp0, dip, djp, rx, ry, wx, wy;
+};
+
+__device__ __forceinline__ unsigned long long pack_branch(const Branch &b)
 {
-    M.ip0 = (int)floor(x0);
-    M.jp0 = (int)floor(y0);
+    return (unsigned long long)(unsigned)b.ip0 | ((unsigned long long)(unsigned)b.jp0 << 20) |
+           ((unsigned long long)(b.dip + 1) << 40) | ((unsigned long long)(b.djp + 1) << 42) |
+           ((unsigned long long)b.rx << 44) | ((unsigned long long)b.ry << 46) |
+           ((unsigned long long)(b.wx + 1) << 48) | ((unsigned long long)(b.wy + 1) << 50);
+}
+
+__device__ __forceinline__ Branch unpack_branch(unsigned long long w)
+{
+    Branch b;
+    b.ip0 = (int)(w & 0xfffffu);
+    b.jp0 = (int)((w >> 20) & 0xfffffu);
+    b.dip = (int)((w >> 40) & 3u) - 1;
+    b.djp = (int)((w >> 42) & 3u) - 1;
+    b.rx = (int)((w >> 44) & 3u);
+    b.ry = (int)((w >> 46) & 3u);
+    b.wx = (int)((w >> 48) & 3u) - 1;
+    b.wy = (int)((w >> 50) & 3u) - 1;
+    return b;
+}
+
+// The relay point on a given side of the clamp.
+template <typename T>
+__device__ __forceinline__ T relay_side(int i0, int i1, T mid, int side)
+{
+    return side == 0 ? (T)max(i0, i1) : (side == 2 ? (T)(min(i0, i1) + 1) : mid);
+}
+template <typename T>
+__device__ __forceinline__ int relay_side_of(int i0, int i1, T mid)
+{
+    const T lo = (T)max(i0, i1), hi = (T)(min(i0, i1) + 1);
+    return mid > lo ? (mid < hi ? 1 : 2) : 0;
+}
+
+template <typename T, int BR = kBranchFree>
+__device__ void move_fwd(const AG &g, T x0, T y0, T z0, T u, T v, T w, T qthis, T qm, const F3<T> &E, const F3<T> &B,
+                         Mv<T> &M, Branch *br = nullptr)
+{
+    M.ip0 = BR == kBranchReplay ? br->ip0 : (int)floor(x0);
+    M.jp0 = BR == kBranchReplay ? br->jp0 : (int)floor(y0);
     M.kp0 = (int)floor(z0);
     M.dx = x0 - (T)M.ip0;
     M.dy = y0 - (T)M.jp0;
@@ -243,11 +294,26 @@ __device__ void move_fwd(const AG &g, T x0, T y0, T z0, T u, T v, T w, T qthis, 
     M.x1 = x0 + (M.U[0] * cinv) * g2;
     M.y1 = y0 + (M.U[1] * cinv) * g2;
     M.z1 = z0 + (M.U[2] * cinv) * g2;
-    M.ip = (int)floor(M.x1);
-    M.jp = (int)floor(M.y1);
+    M.ip = BR == kBranchReplay ? M.ip0 + br->dip : (int)floor(M.x1);
+    M.jp = BR == kBranchReplay ? M.jp0 + br->djp : (int)floor(M.y1);
     M.kp = (int)floor(M.z1);
-    M.xr = relay<T>(M.ip0, M.ip, (T)0.5 * (x0 + M.x1), M.xa);
-    M.yr = relay<T>(M.jp0, M.jp, (T)0.5 * (y0 + M.y1), M.ya);
+    if (BR == kBranchReplay) {
+        M.xr = relay_side<T>(M.ip0, M.ip, (T)0.5 * (x0 + M.x1), br->rx);
+        M.yr = relay_side<T>(M.jp0, M.jp, (T)0.5 * (y0 + M.y1), br->ry);
+        M.xa = br->rx == 1;
+        M.ya = br->ry == 1;
+    } else {
+        M.xr = relay<T>(M.ip0, M.ip, (T)0.5 * (x0 + M.x1), M.xa);
+        M.yr = relay<T>(M.jp0, M.jp, (T)0.5 * (y0 + M.y1), M.ya);
+        if (BR == kBranchRecord) {
+            br->ip0 = M.ip0;
+            br->jp0 = M.jp0;
+            br->dip = M.ip - M.ip0;
+            br->djp = M.jp - M.jp0;
+            br->rx = relay_side_of<T>(M.ip0, M.ip, (T)0.5 * (x0 + M.x1));
+            br->ry = relay_side_of<T>(M.jp0, M.jp, (T)0.5 * (y0 + M.y1));
+        }
+    }
     // out-of-plane current: both segments carry half of the z displacement
     // (the midpoint relay of the FP32 form; continuous in z, unlike the z
     // relay of movdep.F90:185, which jumps when z crosses 1 or 2)
@@ -314,22 +380,43 @@ __device__ __forceinline__ T wrap_pos(T x, int n)
 // is faster with coalesced loads.)
 __device__ __forceinline__ long long spread_slot(long long L, long long q) { return (L & 31) * q + (L >> 5); }
 
+// Shift of the periodic wrap of x in [-1, n + 1): -1 (x -= n), +1 or 0.
 template <typename T>
+__device__ __forceinline__ int wrap_shift(T x, int n)
+{
+    return x >= (T)n ? -1 : (x < (T)0 ? 1 : 0);
+}
+
+// Forward mover; BR: free, record the branches into tape[n] or replay them.
+template <typename T, int BR>
 __global__ void k_move(AG g, PS<T> p, const T *__restrict__ qw, const int *__restrict__ flv, long long np, F3<T> E,
-                       F3<T> B, F3<T> J)
+                       F3<T> B, F3<T> J, unsigned long long *tape)
 {
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < np; n += (long long)gridDim.x * blockDim.x) {
         Mv<T> M;
+        Branch br;
+        if (BR == kBranchReplay) br = unpack_branch(tape[n]);
         const T z0 = p.z[n];
-        move_fwd<T>(g, p.x[n], p.y[n], z0, p.u[n], p.v[n], p.w[n], qw[n] * (T)g.qi, (T)g.qm_half[flv[n]], E, B, M);
+        move_fwd<T, BR>(g, p.x[n], p.y[n], z0, p.u[n], p.v[n], p.w[n], qw[n] * (T)g.qi, (T)g.qm_half[flv[n]], E, B, M,
+                        &br);
         scatter_seg<T>(g, J, M.ip0, M.jp0, M.F1, M.W1);
         scatter_seg<T>(g, J, M.ip, M.jp, M.F2, M.W2);
         const T cinv = (T)g.cinv;
         p.u[n] = M.U[0] * cinv;
         p.v[n] = M.U[1] * cinv;
         p.w[n] = M.U[2] * cinv;
-        p.x[n] = wrap_pos<T>(M.x1, g.nx);
-        p.y[n] = wrap_pos<T>(M.y1, g.ny);
+        if (BR == kBranchFree) {
+            p.x[n] = wrap_pos<T>(M.x1, g.nx);
+            p.y[n] = wrap_pos<T>(M.y1, g.ny);
+        } else {
+            if (BR == kBranchRecord) {
+                br.wx = wrap_shift<T>(M.x1, g.nx);
+                br.wy = wrap_shift<T>(M.y1, g.ny);
+                tape[n] = pack_branch(br);
+            }
+            p.x[n] = M.x1 + (T)(br.wx * g.nx);
+            p.y[n] = M.y1 + (T)(br.wy * g.ny);
+        }
         T zn = M.z1;   // movdep.F90:241-249 (zmin = 1, zmax = 2)
         if (zn > (T)2) zn = zn - (T)1;
         else if (zn < (T)1) zn = (T)1 + zn;
@@ -579,7 +666,12 @@ struct pic_adjoint {
     // the forward run and the reverse sweep captured as CUDA graphs, rebuilt
     // when the step count, the checkpoint interval or the particle count change
     cudaGraphExec_t gf = nullptr, gb = nullptr;
-    long long gf_key[3] = {-1, -1, -1}, gb_key[3] = {-1, -1, -1};
+    long long gf_key[4] = {-1, -1, -1, -1}, gb_key[4] = {-1, -1, -1, -1};
+    // frozen branches of the forward mover (record / replay), one word per
+    // particle and step of the recorded run
+    int br_mode = 0;
+    unsigned long long *br_tape = nullptr;
+    long long br_words = 0, br_np = 0, br_steps = 0;
     // checkpoints (every K steps) and the tape of one segment
     int K = 0, T = 0, tapeK = 0;
     std::vector<void *> ck_p, ck_f;   // per checkpoint: 6 particle arrays / 6 field arrays
@@ -677,13 +769,19 @@ int restore_state(pic_adjoint *a, void *pbase, void *fbase)
 
 // One forward step on the current state; obj accumulates 1/2 |B_t|^2.
 template <typename T>
-void step_fwd(pic_adjoint *a, bool obj)
+void step_fwd(pic_adjoint *a, bool obj, int t)
 {
     const AG &g = a->g;
     const unsigned gc = grid_of((long long)cells(a)), gp = grid_of(a->np);
     F3<T> E = f3<T>(a->E), B = f3<T>(a->B), J = f3<T>(a->J);
     k_bhalf<T><<<gc, 256, 0, a->s>>>(g, E, B, B);
-    k_move<T><<<gp, 256, 0, a->s>>>(g, ps<T>(a->p), (const T *)a->qw, a->flv, a->np, E, B, J);
+    unsigned long long *tape = t >= 0 && a->br_mode != kBranchFree ? a->br_tape + (size_t)t * (size_t)a->np : nullptr;
+    if (tape && a->br_mode == kBranchRecord)
+        k_move<T, kBranchRecord><<<gp, 256, 0, a->s>>>(g, ps<T>(a->p), (const T *)a->qw, a->flv, a->np, E, B, J, tape);
+    else if (tape)
+        k_move<T, kBranchReplay><<<gp, 256, 0, a->s>>>(g, ps<T>(a->p), (const T *)a->qw, a->flv, a->np, E, B, J, tape);
+    else
+        k_move<T, kBranchFree><<<gp, 256, 0, a->s>>>(g, ps<T>(a->p), (const T *)a->qw, a->flv, a->np, E, B, J, nullptr);
     k_bhalf<T><<<gc, 256, 0, a->s>>>(g, E, B, B);
     k_efield<T><<<gc, 256, 0, a->s>>>(g, E, B, J);
     if (obj) k_benergy<T><<<gc, 256, 0, a->s>>>(g, B, a->acc);
@@ -716,9 +814,9 @@ void step_rev(pic_adjoint *a, PS<T> P, F3<T> E, F3<T> B, int &cur)
 // Launch the graph cached in *ge for key, or capture enqueue() on a->s into
 // a new one first.
 template <typename F>
-int launch_cached(pic_adjoint *a, cudaGraphExec_t *ge, long long *cached, const long long key[3], F enqueue)
+int launch_cached(pic_adjoint *a, cudaGraphExec_t *ge, long long *cached, const long long key[4], F enqueue)
 {
-    if (!*ge || cached[0] != key[0] || cached[1] != key[1] || cached[2] != key[2]) {
+    if (!*ge || cached[0] != key[0] || cached[1] != key[1] || cached[2] != key[2] || cached[3] != key[3]) {
         if (*ge) {
             cudaGraphExecDestroy(*ge);
             *ge = nullptr;
@@ -738,7 +836,7 @@ int launch_cached(pic_adjoint *a, cudaGraphExec_t *ge, long long *cached, const 
             *ge = nullptr;
             return cstat(ei);
         }
-        for (int k = 0; k < 3; k++) cached[k] = key[k];
+        for (int k = 0; k < 4; k++) cached[k] = key[k];
     }
     ACK(cudaGraphLaunch(*ge, a->s));
     return PIC_OK;
@@ -761,7 +859,7 @@ int enqueue_forward(pic_adjoint *a, int nsteps, int K)
             int r = save_state<T>(a, a->ck_p[t / K], a->ck_f[t / K]);
             if (r) return r;
         }
-        step_fwd<T>(a, true);
+        step_fwd<T>(a, true, t);
     }
     ACK(cudaGetLastError());
     return PIC_OK;
@@ -780,13 +878,33 @@ int run_forward(pic_adjoint *a, int nsteps, int K, double *objective)
         a->ck_p.push_back(pp);
         a->ck_f.push_back(ff);
     }
-    const long long key[3] = {nsteps, K, a->np};
+    if (a->br_mode == kBranchReplay && (a->br_np != a->np || a->br_steps < nsteps)) return PIC_ERR_INVALID;
+    if (a->br_mode == kBranchRecord && a->br_words < (long long)nsteps * a->np) {
+        if (a->br_tape) {
+            cudaFree(a->br_tape);
+            a->allocs.erase(std::find(a->allocs.begin(), a->allocs.end(), (void *)a->br_tape));
+            a->br_tape = nullptr;
+        }
+        a->br_words = 0;
+        int q = aalloc(a, (void **)&a->br_tape, (size_t)nsteps * (size_t)a->np * sizeof(unsigned long long));
+        if (q) return q;
+        a->br_words = (long long)nsteps * a->np;
+        if (a->gf) {   // captured with the old tape
+            cudaGraphExecDestroy(a->gf);
+            a->gf = nullptr;
+        }
+    }
+    const long long key[4] = {nsteps, K, a->np, a->br_mode};
     int r = launch_cached(a, &a->gf, a->gf_key, key, [&] { return enqueue_forward<T>(a, nsteps, K); });
     if (r) return r;
     ACK(cudaMemcpyAsync(objective, a->acc, sizeof(double), cudaMemcpyDeviceToHost, a->s));
     ACK(cudaStreamSynchronize(a->s));
     a->K = K;
     a->T = nsteps;
+    if (a->br_mode == kBranchRecord) {
+        a->br_np = a->np;
+        a->br_steps = nsteps;
+    }
     return PIC_OK;
 }
 
@@ -836,7 +954,7 @@ int enqueue_backward(pic_adjoint *a)
             if ((r = save_state<T>(a, (char *)a->tape_p + (size_t)s * 6 * a->cap * sizeof(T),
                                    (char *)a->tape_f + (size_t)s * 6 * cells(a) * sizeof(T))))
                 return r;
-            step_fwd<T>(a, false);
+            step_fwd<T>(a, false, -1);
         }
         for (int t = t1 - 1; t >= t0; t--) {
             const int s = t - t0;
@@ -857,7 +975,7 @@ int run_backward(pic_adjoint *a)
 {
     int r = ensure_tape<T>(a);
     if (r) return r;
-    const long long key[3] = {a->T, a->K, a->np};
+    const long long key[4] = {a->T, a->K, a->np, 0};
     if ((r = launch_cached(a, &a->gb, a->gb_key, key, [&] { return enqueue_backward<T>(a); }))) return r;
     ACK(cudaStreamSynchronize(a->s));
     return PIC_OK;
@@ -1038,6 +1156,14 @@ int pic_adj_fetch_particles(pic_adjoint *a, int64_t *nout, double *q, double *x,
     if (!r && drift_sign && cudaMemcpy(drift_sign, a->sgn, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
         r = PIC_ERR_CUDA;
     return r;
+}
+
+int pic_adj_branches(pic_adjoint *a, int32_t mode)
+{
+    if (!a || mode < kBranchFree || mode > kBranchReplay) return PIC_ERR_INVALID;
+    if (mode == kBranchReplay && a->br_steps == 0) return PIC_ERR_INVALID;
+    a->br_mode = mode;
+    return PIC_OK;
 }
 
 int pic_adj_forward(pic_adjoint *a, int32_t nsteps, int32_t checkpoint_every, double *objective)
