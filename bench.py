@@ -57,6 +57,9 @@ WORKLOADS = {
     # onto them; particles gather from / deposit onto the 8 theta cells)
     "cyl_wake_modal": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                            bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0, cyl_modes=2),
+    # the same run in the FP32 cell-relative form (theta-gridded FP32 fields)
+    "cyl_wake_fp32": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp32", thermal=0.01,
+                          bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0),
     # a small case of the same physics for profiler captures (4.2 M particles, 250 MB > L2)
     "cyl_wake_small": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                            bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0, bunch_sigma_z=10.0),
@@ -582,7 +585,7 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
                             bunch_sigma_z=wl["bunch_sigma_z"], seed=SEED)
     n_p = len(p.x)
     cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=wl["nz"], dims=3, c=wl["c"], qi=sc["qi"], qm=(1.0, -1.0),
-                    fdtd="lehe", geom="cylindrical", precision="fp64", capacity=2 * n_p + 4096,
+                    fdtd="lehe", geom="cylindrical", precision=wl["precision"], capacity=2 * n_p + 4096,
                     reorder_period=20, rmin=-0.5, inc_axis=1, cyl_modes=wl.get("cyl_modes", 0))
     pinned = Particles(*(torch.from_numpy(getattr(p, k)).pin_memory().numpy() for k in Particles.NAMES))
     with Simulation(cfg) as sim:
@@ -607,21 +610,24 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
     value = n_p * args.steps / (ms * 1e-3)
     move_ms = phases["ms"]["move"] / max(phases["steps"], 1)
     n_cells = wl["nx"] * wl["ny"] * wl["nz"]
-    bytes_move = n_p * bytes_per_particle(3, "fp64") + n_cells * bytes_per_cell_mover("fp64")
+    bytes_move = n_p * bytes_per_particle(3, wl["precision"]) + n_cells * bytes_per_cell_mover(wl["precision"])
     cpu = None if args.no_cpu else cpu_sample_cyl(wl)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32" if wl["precision"] == "fp32" else "f64", "data": "synthetic",
             "config": {"workload": args.workload,
                        "form": ("field solve on azimuthal modes m=0,1 (FP64), particles on the theta grid"
-                                if wl.get("cyl_modes", 0) else "theta-gridded FP64 (the reference's representation)"),
+                                if wl.get("cyl_modes", 0) else
+                                "FP32 cell-relative particles, theta-gridded FP32 fields" if wl["precision"] == "fp32"
+                                else "theta-gridded FP64 (the reference's representation)"),
                        "cells_r_theta_z": [wl["nx"], wl["ny"], wl["nz"]], "particles": n_p, **info,
                        "courant": wl["c"], "c_ompe": wl["c_ompe"], "fdtd": "lehe (z)", "reorder_period": 20,
                        "l2": "particle state (GBs) larger than L2"},
             "roofline": {"bound": "hbm", "achieved": bytes_move / (move_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
-                         "frac": bytes_move / (move_ms * 1e-3) / 1e9 / peak, "traffic": None, "kernel": "k_cyl_move",
+                         "frac": bytes_move / (move_ms * 1e-3) / 1e9 / peak, "traffic": None,
+                         "kernel": "k_cyl_move_f32" if wl["precision"] == "fp32" else "k_cyl_move",
                          "launch_ms": move_ms, "peak_kind": peak_kind},
             "phases_ms_per_step": {k: v / max(phases["steps"], 1) for k, v in phases["ms"].items()},
             "gpu_launches": launches, "clocks": clk,
@@ -690,7 +696,7 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
-    if args.workload in ("cyl_wake", "cyl_wake_small", "cyl_wake_modal"):
+    if args.workload in ("cyl_wake", "cyl_wake_small", "cyl_wake_modal", "cyl_wake_fp32"):
         peak, peak_kind = measured_peaks()
         return run_cyl_bench(args, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]

@@ -191,6 +191,32 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
     const GridP &g = h->g;
     const bool filt = h->cfg.curr_filter > 0;
     g_launches = 0;
+    if (g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {  // the FP32 cell-relative form
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        switch (phase) {
+            case PIC_PHASE_BHALF1:
+            case PIC_PHASE_BHALF2:
+                launch_cyl_bhalf<float>(g, E, B, h->s);
+                break;
+            case PIC_PHASE_MOVE:  // push, deposit and the wrap / outer-radius drop
+                launch_cyl_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
+                break;
+            case PIC_PHASE_EXCHANGE:
+                break;
+            case PIC_PHASE_EFIELD:
+                launch_cyl_efield<float>(g, 0, E, B, J, h->s);
+                launch_cyl_fold<float>(g, J, h->s);
+                launch_cyl_efield<float>(g, 2, E, B, J, h->s);
+                for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(float), h->s);
+                break;
+            case PIC_PHASE_REORDER:
+                if (reorder)
+                    launch_reorder_f32(g, h->p32[cur], h->p32[cur ^ 1], h->cnt, h->capacity, h->bricks, h->err, h->s);
+                break;
+        }
+        return (int)g_launches;
+    }
     if (g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -741,12 +767,14 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     const pic_config &c = *cfg;
     if (c.dims != 2 && c.dims != 3) return PIC_ERR_INVALID;
     if (c.geom != PIC_GEOM_CARTESIAN && c.geom != PIC_GEOM_CYLINDRICAL) return PIC_ERR_INVALID;
-    // the cylindrical step exists in the reference's FP64 form, 3D, with the
-    // axis on this rank and no current filter
-    if (c.geom == PIC_GEOM_CYLINDRICAL &&
-        (c.dims != 3 || c.precision != PIC_PREC_FP64 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
+    // the cylindrical step: 3D, with the axis on this rank, no current filter;
+    // the reference's FP64 form or the FP32 cell-relative one (theta-gridded
+    // fields); the modal field solve in FP64
+    if (c.geom == PIC_GEOM_CYLINDRICAL && (c.dims != 3 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
         return PIC_ERR_INVALID;
-    if (c.cyl_modes != 0 && (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4)) return PIC_ERR_INVALID;
+    if (c.cyl_modes != 0 &&
+        (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4 || c.precision != PIC_PREC_FP64))
+        return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
@@ -1110,6 +1138,10 @@ int pic_update_b_half(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_modal_bhalf(h->g, h->Em, h->Bm, h->s);
         launch_modal_synth(h->g, h->Bm, B, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_bhalf<float>(h->g, E, B, h->s);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -1137,7 +1169,11 @@ int pic_move_deposit(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
-    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_cyl_move_deposit(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s);
@@ -1171,6 +1207,10 @@ int pic_update_e(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_modal_efield(h->g, 0, h->Em, h->Bm, h->Jm, h->s);
         launch_modal_synth(h->g, h->Em, E, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_efield<float>(h->g, 0, E, B, J, h->s);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -1190,7 +1230,11 @@ int pic_update_e(pic_handle *h)
 int pic_fold_current(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
-    if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
+    if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_fold<float>(h->g, J, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         launch_cyl_fold(h->g, J, h->s);
@@ -1236,6 +1280,10 @@ int pic_add_current(pic_handle *h)
         launch_modal_project(h->g, J, h->Jm, h->s);
         launch_modal_efield(h->g, 2, h->Em, h->Bm, h->Jm, h->s);
         launch_modal_synth(h->g, h->Em, E, h->s);
+    } else if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
+        float *E[3], *B[3], *J[3];
+        field_ptrs(h, E, B, J);
+        launch_cyl_efield<float>(h->g, 2, E, B, J, h->s);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);

@@ -24,82 +24,89 @@ struct CylP {
     double dtheta, ax_perm_area, inv_dtheta, rmin;
 };
 
-__device__ __forceinline__ double ldd(const double *p) { return __ldg(p); }
+template <typename T>
+__device__ __forceinline__ T ldd(const T *p) { return __ldg(p); }
 
 // ---------------------------------------------------------------------------
 // Fields
 // ---------------------------------------------------------------------------
 
 // Lehe directional differences of cyl_em_update_lehe.F90:255-289.
-__device__ __forceinline__ double lgx(const GridP &g, const double *F, long long c0)
+template <typename T>
+__device__ __forceinline__ T lgx(const GridP &g, const T *F, long long c0)
 {
-    double r = g.lehe[0] * (ldd(F + c0 + 1) - ldd(F + c0));
-    r = r + g.lehe[4] * (ldd(F + c0 + 1 + g.sz) - ldd(F + c0 + g.sz));
-    r = r + g.lehe[4] * (ldd(F + c0 + 1 - g.sz) - ldd(F + c0 - g.sz));
+    T r = (T)g.lehe[0] * (ldd(F + c0 + 1) - ldd(F + c0));
+    r = r + (T)g.lehe[4] * (ldd(F + c0 + 1 + g.sz) - ldd(F + c0 + g.sz));
+    r = r + (T)g.lehe[4] * (ldd(F + c0 + 1 - g.sz) - ldd(F + c0 - g.sz));
     return r;
 }
-__device__ __forceinline__ double lgx1(const GridP &g, const double *F, long long c0, double rp, double rr)
+template <typename T>
+__device__ __forceinline__ T lgx1(const GridP &g, const T *F, long long c0, T rp, T rr)
 {
-    double r = g.lehe[0] * (rp * ldd(F + c0 + 1) - rr * ldd(F + c0));
-    r = r + g.lehe[4] * (rp * ldd(F + c0 + 1 + g.sz) - rr * ldd(F + c0 + g.sz));
-    r = r + g.lehe[4] * (rp * ldd(F + c0 + 1 - g.sz) - rr * ldd(F + c0 - g.sz));
+    T r = (T)g.lehe[0] * (rp * ldd(F + c0 + 1) - rr * ldd(F + c0));
+    r = r + (T)g.lehe[4] * (rp * ldd(F + c0 + 1 + g.sz) - rr * ldd(F + c0 + g.sz));
+    r = r + (T)g.lehe[4] * (rp * ldd(F + c0 + 1 - g.sz) - rr * ldd(F + c0 - g.sz));
     return r;
 }
-__device__ __forceinline__ double lgy(const GridP &g, const double *F, long long c0)
+template <typename T>
+__device__ __forceinline__ T lgy(const GridP &g, const T *F, long long c0)
 {
-    double r = (g.lehe[1] * 1.0) * (ldd(F + c0 + g.sy) - ldd(F + c0));
-    r = r + (g.lehe[6] * 1.0) * (ldd(F + c0 + g.sy + g.sz) - ldd(F + c0 + g.sz));
-    r = r + (g.lehe[6] * 1.0) * (ldd(F + c0 + g.sy - g.sz) - ldd(F + c0 - g.sz));
+    T r = (T)(g.lehe[1] * 1.0) * (ldd(F + c0 + g.sy) - ldd(F + c0));
+    r = r + (T)(g.lehe[6] * 1.0) * (ldd(F + c0 + g.sy + g.sz) - ldd(F + c0 + g.sz));
+    r = r + (T)(g.lehe[6] * 1.0) * (ldd(F + c0 + g.sy - g.sz) - ldd(F + c0 - g.sz));
     return r;
 }
-__device__ __forceinline__ double lgz(const GridP &g, const double *F, long long c0)
+template <typename T>
+__device__ __forceinline__ T lgz(const GridP &g, const T *F, long long c0)
 {
     const long long sy = g.sy, sz = g.sz;
-    double r = g.lehe[2] * (ldd(F + c0 + sz) - ldd(F + c0));
-    r = r + g.lehe[7] * (ldd(F + c0 + 1 + sz) - ldd(F + c0 + 1));
-    r = r + g.lehe[7] * (ldd(F + c0 - 1 + sz) - ldd(F + c0 - 1));
-    r = r + g.lehe[8] * (ldd(F + c0 + sy + sz) - ldd(F + c0 + sy));
-    r = r + g.lehe[8] * (ldd(F + c0 - sy + sz) - ldd(F + c0 - sy));
-    r = r + g.lehe[11] * (ldd(F + c0 + 2 * sz) - ldd(F + c0 - sz));
+    T r = (T)g.lehe[2] * (ldd(F + c0 + sz) - ldd(F + c0));
+    r = r + (T)g.lehe[7] * (ldd(F + c0 + 1 + sz) - ldd(F + c0 + 1));
+    r = r + (T)g.lehe[7] * (ldd(F + c0 - 1 + sz) - ldd(F + c0 - 1));
+    r = r + (T)g.lehe[8] * (ldd(F + c0 + sy + sz) - ldd(F + c0 + sy));
+    r = r + (T)g.lehe[8] * (ldd(F + c0 - sy + sz) - ldd(F + c0 - sy));
+    r = r + (T)g.lehe[11] * (ldd(F + c0 + 2 * sz) - ldd(F + c0 - sz));
     return r;
 }
 
 // UpdateBfieldHalf main loop (cyl_em_update.F90:66-83): i 4..mx-1, j 1..my-1,
-// k 1..mz-1 (Lehe: k 2..mz-2, see the oracle for why).
-template <int FDTD>
-__global__ void k_cyl_bhalf(GridP g, CylP cp, const double *__restrict__ Ex, const double *__restrict__ Ey,
-                            const double *__restrict__ Ez, double *Bx, double *By, double *Bz)
+// k 1..mz-1 (Lehe: k 2..mz-2, see the oracle for why).  T = double is the
+// reference form; T = float the FP32 form (same expressions).
+template <typename T, int FDTD>
+__global__ void k_cyl_bhalf(GridP g, CylP cp, const T *__restrict__ Ex, const T *__restrict__ Ey,
+                            const T *__restrict__ Ez, T *Bx, T *By, T *Bz)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     const int k = (FDTD == PIC_FDTD_LEHE ? 2 : 1) + blockIdx.z;
     if (i > g.mx - 1 || j > g.my - 1) return;
-    const double h = g.h, dtheta = cp.dtheta;
-    const double r = (((double)i - 3.0) + cp.rmin) * 1.0;
-    const double rp_half = r + 0.5 * 1.0, rp = r + 1.0;
+    const T h = (T)g.h, dtheta = (T)cp.dtheta;
+    const T r = (((T)i - (T)3.0) + (T)cp.rmin) * (T)1.0;
+    const T rp_half = r + (T)0.5 * (T)1.0, rp = r + (T)1.0;
     const long long c0 = cidx(g, i, j, k);
     const long long sy = g.sy, sz = g.sz;
     if (FDTD == PIC_FDTD_YEE) {
-        Bx[c0] = (Bx[c0] - (h * (ldd(Ez + c0 + sy) - ldd(Ez + c0))) / (r * dtheta)) + (h * 1.0) * (ldd(Ey + c0 + sz) - ldd(Ey + c0));
-        By[c0] = (By[c0] - (h * 1.0) * (ldd(Ex + c0 + sz) - ldd(Ex + c0))) + (h * 1.0) * (ldd(Ez + c0 + 1) - ldd(Ez + c0));
-        Bz[c0] = Bz[c0] - (h * ((1.0 * (rp * ldd(Ey + c0 + 1) - r * ldd(Ey + c0))) - (ldd(Ex + c0 + sy) - ldd(Ex + c0)) / dtheta)) / rp_half;
+        Bx[c0] = (Bx[c0] - (h * (ldd(Ez + c0 + sy) - ldd(Ez + c0))) / (r * dtheta)) + (h * (T)1.0) * (ldd(Ey + c0 + sz) - ldd(Ey + c0));
+        By[c0] = (By[c0] - (h * (T)1.0) * (ldd(Ex + c0 + sz) - ldd(Ex + c0))) + (h * (T)1.0) * (ldd(Ez + c0 + 1) - ldd(Ez + c0));
+        Bz[c0] = Bz[c0] - (h * (((T)1.0 * (rp * ldd(Ey + c0 + 1) - r * ldd(Ey + c0))) - (ldd(Ex + c0 + sy) - ldd(Ex + c0)) / dtheta)) / rp_half;
     } else {
-        Bx[c0] = (Bx[c0] - (h * lgy(g, Ez, c0)) / (r * dtheta)) + (h * 1.0) * lgz(g, Ey, c0);
-        By[c0] = (By[c0] - (h * 1.0) * lgz(g, Ex, c0)) + (h * 1.0) * lgx(g, Ez, c0);
-        Bz[c0] = Bz[c0] - (h * ((1.0 * lgx1(g, Ey, c0, rp, r)) - lgy(g, Ex, c0) / dtheta)) / rp_half;
+        Bx[c0] = (Bx[c0] - (h * lgy(g, Ez, c0)) / (r * dtheta)) + (h * (T)1.0) * lgz(g, Ey, c0);
+        By[c0] = (By[c0] - (h * (T)1.0) * lgz(g, Ex, c0)) + (h * (T)1.0) * lgx(g, Ez, c0);
+        Bz[c0] = Bz[c0] - (h * (((T)1.0 * lgx1(g, Ey, c0, rp, r)) - lgy(g, Ex, c0) / dtheta)) / rp_half;
     }
 }
 
 // UpdateBzAxis (cyl_em_update.F90:231-246) + Bz(3,j,k) = Bz_ax(k): one
 // thread per k sums Ey(4,j,k) over j in the reference's order.
-__global__ void k_cyl_bz_axis(GridP g, CylP cp, const double *__restrict__ Ey, double *Bz)
+template <typename T>
+__global__ void k_cyl_bz_axis(GridP g, CylP cp, const T *__restrict__ Ey, T *Bz)
 {
     const int k = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     if (k > g.mz - 1) return;
-    const double hax = g.h * cp.ax_perm_area;
-    double s = 0.0;
+    const T hax = (T)(g.h * cp.ax_perm_area);
+    T s = (T)0.0;
     for (int j = 3; j <= g.my - 3; j++) s = s - hax * Ey[cidx(g, 4, j, k)];
-    const double v = Bz[cidx(g, 3, 3, k)] + s;
+    const T v = Bz[cidx(g, 3, 3, k)] + s;
     for (int j = 1; j <= g.my - 1; j++) Bz[cidx(g, 3, j, k)] = v;
 }
 
@@ -111,26 +118,28 @@ __device__ __forceinline__ int axis_partner(const GridP &g, int j)
 }
 
 // UpdateBFldAxis (cyl_em_update.F90:187-227), all j, k.
-__global__ void k_cyl_b_axis(GridP g, double *Bx, double *By, double *Bz)
+template <typename T>
+__global__ void k_cyl_b_axis(GridP g, T *Bx, T *By, T *Bz)
 {
     const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 1 + blockIdx.y;
     if (j > g.my) return;
     const int jpp = axis_partner(g, j);
-    By[cidx(g, 3, j, k)] = 0.5 * (By[cidx(g, 4, j, k)] - By[cidx(g, 4, jpp, k)]);
+    By[cidx(g, 3, j, k)] = (T)0.5 * (By[cidx(g, 4, j, k)] - By[cidx(g, 4, jpp, k)]);
     By[cidx(g, 2, j, k)] = -By[cidx(g, 4, jpp, k)];
     Bx[cidx(g, 3, j, k)] = -Bx[cidx(g, 4, jpp, k)];
     Bz[cidx(g, 2, j, k)] = Bz[cidx(g, 4, jpp, k)];
 }
 
 // UpdateEFldAxis (cyl_em_update.F90:143-185), all j, k.
-__global__ void k_cyl_e_axis(GridP g, double *Ex, double *Ey, double *Ez)
+template <typename T>
+__global__ void k_cyl_e_axis(GridP g, T *Ex, T *Ey, T *Ez)
 {
     const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 1 + blockIdx.y;
     if (j > g.my) return;
     const int jpp = axis_partner(g, j);
-    Ex[cidx(g, 3, j, k)] = 0.5 * (Ex[cidx(g, 4, j, k)] - Ex[cidx(g, 4, jpp, k)]);
+    Ex[cidx(g, 3, j, k)] = (T)0.5 * (Ex[cidx(g, 4, j, k)] - Ex[cidx(g, 4, jpp, k)]);
     Ex[cidx(g, 2, j, k)] = -Ex[cidx(g, 4, jpp, k)];
     Ey[cidx(g, 3, j, k)] = -Ey[cidx(g, 4, jpp, k)];
     Ez[cidx(g, 3, j, k)] = Ez[cidx(g, 4, jpp, k)];
@@ -138,33 +147,34 @@ __global__ void k_cyl_e_axis(GridP g, double *Ex, double *Ey, double *Ez)
 
 // UpdateEfield (MODE 0, cyl_em_update.F90:24-41) or AddCurrent (MODE 2,
 // :128-137): i 4..mx-3, j, k 3..m-3.
-template <int MODE>
-__global__ void k_cyl_e(GridP g, CylP cp, double *Ex, double *Ey, double *Ez, const double *__restrict__ Bx,
-                        const double *__restrict__ By, const double *__restrict__ Bz, const double *__restrict__ Jx,
-                        const double *__restrict__ Jy, const double *__restrict__ Jz)
+template <typename T, int MODE>
+__global__ void k_cyl_e(GridP g, CylP cp, T *Ex, T *Ey, T *Ez, const T *__restrict__ Bx, const T *__restrict__ By,
+                        const T *__restrict__ Bz, const T *__restrict__ Jx, const T *__restrict__ Jy,
+                        const T *__restrict__ Jz)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
     const int k = 3 + blockIdx.z;
     if (i > g.mx - 3 || j > g.my - 3) return;
-    const double dtheta = cp.dtheta;
-    const double r = (((double)i - 3.0) + cp.rmin) * 1.0;
-    const double rp_half = r + 0.5 * 1.0, rm_half = r - 0.5 * 1.0;
+    const T dtheta = (T)cp.dtheta;
+    const T r = (((T)i - (T)3.0) + (T)cp.rmin) * (T)1.0;
+    const T rp_half = r + (T)0.5 * (T)1.0, rm_half = r - (T)0.5 * (T)1.0;
     const long long c0 = cidx(g, i, j, k);
     if (MODE == 0) {
-        const double fc = g.fc;
-        Ex[c0] = (Ex[c0] + (fc * (ldd(Bz + c0) - ldd(Bz + c0 - g.sy))) / (rp_half * dtheta)) - (fc * 1.0) * (ldd(By + c0) - ldd(By + c0 - g.sz));
-        Ey[c0] = (Ey[c0] + (fc * 1.0) * (ldd(Bx + c0) - ldd(Bx + c0 - g.sz))) - (fc * 1.0) * (ldd(Bz + c0) - ldd(Bz + c0 - 1));
-        Ez[c0] = (Ez[c0] + ((fc * 1.0) * (rp_half * ldd(By + c0) - rm_half * ldd(By + c0 - 1))) / r) - (fc * (ldd(Bx + c0) - ldd(Bx + c0 - g.sy))) / (r * dtheta);
+        const T fc = (T)g.fc;
+        Ex[c0] = (Ex[c0] + (fc * (ldd(Bz + c0) - ldd(Bz + c0 - g.sy))) / (rp_half * dtheta)) - (fc * (T)1.0) * (ldd(By + c0) - ldd(By + c0 - g.sz));
+        Ey[c0] = (Ey[c0] + (fc * (T)1.0) * (ldd(Bx + c0) - ldd(Bx + c0 - g.sz))) - (fc * (T)1.0) * (ldd(Bz + c0) - ldd(Bz + c0 - 1));
+        Ez[c0] = (Ez[c0] + ((fc * (T)1.0) * (rp_half * ldd(By + c0) - rm_half * ldd(By + c0 - 1))) / r) - (fc * (ldd(Bx + c0) - ldd(Bx + c0 - g.sy))) / (r * dtheta);
     } else {
-        Ex[c0] = Ex[c0] - (ldd(Jx + c0) * 1.0) / (rp_half * dtheta);
-        Ey[c0] = Ey[c0] - (ldd(Jy + c0) * 1.0) * 1.0;
-        Ez[c0] = Ez[c0] - (ldd(Jz + c0) * 1.0) / (r * dtheta);
+        Ex[c0] = Ex[c0] - (ldd(Jx + c0) * (T)1.0) / (rp_half * dtheta);
+        Ey[c0] = Ey[c0] - (ldd(Jy + c0) * (T)1.0) * (T)1.0;
+        Ez[c0] = Ez[c0] - (ldd(Jz + c0) * (T)1.0) / (r * dtheta);
     }
 }
 
 // Halo along y over x 1..mx and z 3..mz-3, then along z over all x, y.
-__global__ void k_cyl_halo_y(GridP g, double *F)
+template <typename T>
+__global__ void k_cyl_halo_y(GridP g, T *F)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 3 + blockIdx.y;
@@ -173,7 +183,8 @@ __global__ void k_cyl_halo_y(GridP g, double *F)
     for (int l = 0; l < 3; l++) F[cidx(g, i, m - 2 + l, k)] = F[cidx(g, i, 3 + l, k)];
     for (int l = 0; l < 2; l++) F[cidx(g, i, 1 + l, k)] = F[cidx(g, i, m - 4 + l, k)];
 }
-__global__ void k_cyl_halo_z(GridP g, double *F)
+template <typename T>
+__global__ void k_cyl_halo_z(GridP g, T *F)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
@@ -184,25 +195,27 @@ __global__ void k_cyl_halo_z(GridP g, double *F)
 }
 
 // Current fold: z faces over all x, y, then y faces over x 1..mx, z 3..mz-3.
-__global__ void k_cyl_fold_z(GridP g, double *F)
+template <typename T>
+__global__ void k_cyl_fold_z(GridP g, T *F)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y;
     if (i > g.mx) return;
     const int m = g.mz;
-    double hi3[3], lo2[2];
+    T hi3[3], lo2[2];
     for (int l = 0; l < 3; l++) hi3[l] = F[cidx(g, i, j, m - 2 + l)];
     for (int l = 0; l < 2; l++) lo2[l] = F[cidx(g, i, j, 1 + l)];
     for (int l = 0; l < 3; l++) F[cidx(g, i, j, 3 + l)] = F[cidx(g, i, j, 3 + l)] + hi3[l];
     for (int l = 0; l < 2; l++) F[cidx(g, i, j, m - 4 + l)] = F[cidx(g, i, j, m - 4 + l)] + lo2[l];
 }
-__global__ void k_cyl_fold_y(GridP g, double *F)
+template <typename T>
+__global__ void k_cyl_fold_y(GridP g, T *F)
 {
     const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 3 + blockIdx.y;
     if (i > g.mx) return;
     const int m = g.my;
-    double hi3[3], lo2[2];
+    T hi3[3], lo2[2];
     for (int l = 0; l < 3; l++) hi3[l] = F[cidx(g, i, m - 2 + l, k)];
     for (int l = 0; l < 2; l++) lo2[l] = F[cidx(g, i, 1 + l, k)];
     for (int l = 0; l < 3; l++) F[cidx(g, i, 3 + l, k)] = F[cidx(g, i, 3 + l, k)] + hi3[l];
@@ -220,45 +233,60 @@ static CylP cyl_params(const GridP &g)
     return c;
 }
 
-static void halo(const GridP &g, double *const F[3], cudaStream_t s)
+template <typename T>
+static void halo(const GridP &g, T *const F[3], cudaStream_t s)
 {
     for (int c = 0; c < 3; c++) {
-        k_cyl_halo_y<<<dim3((g.mx + 127) / 128, g.mz - 5), 128, 0, s>>>(g, F[c]);
-        k_cyl_halo_z<<<dim3((g.mx + 127) / 128, g.my), 128, 0, s>>>(g, F[c]);
+        k_cyl_halo_y<T><<<dim3((g.mx + 127) / 128, g.mz - 5), 128, 0, s>>>(g, F[c]);
+        k_cyl_halo_z<T><<<dim3((g.mx + 127) / 128, g.my), 128, 0, s>>>(g, F[c]);
     }
     count_launches(6);
 }
 
-void launch_cyl_bhalf(const GridP &g, double *const E[3], double *const B[3], cudaStream_t s)
+template <typename T>
+void launch_cyl_bhalf(const GridP &g, T *const E[3], T *const B[3], cudaStream_t s)
 {
     const CylP cp = cyl_params(g);
     const int nk = g.fdtd == PIC_FDTD_LEHE ? g.mz - 3 : g.mz - 1;
     const dim3 grid((g.mx - 4 + 31) / 32, (g.my - 1 + 7) / 8, nk), block(32, 8, 1);
-    if (g.fdtd == PIC_FDTD_LEHE) k_cyl_bhalf<PIC_FDTD_LEHE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
-    else k_cyl_bhalf<PIC_FDTD_YEE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
-    k_cyl_bz_axis<<<(g.mz + 127) / 128, 128, 0, s>>>(g, cp, E[1], B[2]);
-    k_cyl_b_axis<<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, B[0], B[1], B[2]);
+    if (g.fdtd == PIC_FDTD_LEHE)
+        k_cyl_bhalf<T, PIC_FDTD_LEHE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
+    else
+        k_cyl_bhalf<T, PIC_FDTD_YEE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
+    k_cyl_bz_axis<T><<<(g.mz + 127) / 128, 128, 0, s>>>(g, cp, E[1], B[2]);
+    k_cyl_b_axis<T><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, B[0], B[1], B[2]);
     count_launches(3);
-    halo(g, B, s);
+    halo<T>(g, B, s);
 }
 
-void launch_cyl_efield(const GridP &g, int mode, double *const E[3], double *const B[3], double *const J[3], cudaStream_t s)
+template <typename T>
+void launch_cyl_efield(const GridP &g, int mode, T *const E[3], T *const B[3], T *const J[3], cudaStream_t s)
 {
     const CylP cp = cyl_params(g);
     const dim3 grid((g.mx - 6 + 31) / 32, (g.my - 5 + 7) / 8, g.mz - 5), block(32, 8, 1);
-    if (mode == 0) k_cyl_e<0><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
-    else k_cyl_e<2><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
-    k_cyl_e_axis<<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, E[0], E[1], E[2]);
+    if (mode == 0) k_cyl_e<T, 0><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
+    else k_cyl_e<T, 2><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
+    k_cyl_e_axis<T><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, E[0], E[1], E[2]);
     count_launches(2);
-    halo(g, E, s);
+    halo<T>(g, E, s);
 }
 
-void launch_cyl_fold(const GridP &g, double *const J[3], cudaStream_t s)
+template <typename T>
+void launch_cyl_fold(const GridP &g, T *const J[3], cudaStream_t s)
 {
-    for (int c = 0; c < 3; c++) k_cyl_fold_z<<<dim3((g.mx + 127) / 128, g.my), 128, 0, s>>>(g, J[c]);
-    for (int c = 0; c < 3; c++) k_cyl_fold_y<<<dim3((g.mx + 127) / 128, g.mz - 5), 128, 0, s>>>(g, J[c]);
+    for (int c = 0; c < 3; c++) k_cyl_fold_z<T><<<dim3((g.mx + 127) / 128, g.my), 128, 0, s>>>(g, J[c]);
+    for (int c = 0; c < 3; c++) k_cyl_fold_y<T><<<dim3((g.mx + 127) / 128, g.mz - 5), 128, 0, s>>>(g, J[c]);
     count_launches(6);
 }
+
+template void launch_cyl_bhalf<double>(const GridP &, double *const[3], double *const[3], cudaStream_t);
+template void launch_cyl_bhalf<float>(const GridP &, float *const[3], float *const[3], cudaStream_t);
+template void launch_cyl_efield<double>(const GridP &, int, double *const[3], double *const[3], double *const[3],
+                                        cudaStream_t);
+template void launch_cyl_efield<float>(const GridP &, int, float *const[3], float *const[3], float *const[3],
+                                       cudaStream_t);
+template void launch_cyl_fold<double>(const GridP &, double *const[3], cudaStream_t);
+template void launch_cyl_fold<float>(const GridP &, float *const[3], cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Mover
@@ -513,16 +541,17 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64
 }
 
 // AxisCurrentBC (cyl_movdep_strang.F90:570-584), all j, k.
-__global__ void k_cyl_axis_current(GridP g, double *Jx, double *Jy, double *Jz)
+template <typename T>
+__global__ void k_cyl_axis_current(GridP g, T *Jx, T *Jy, T *Jz)
 {
     const int j = 1 + blockIdx.x * blockDim.x + threadIdx.x;
     const int k = 1 + blockIdx.y;
     if (j > g.my) return;
     Jy[cidx(g, 4, j, k)] = Jy[cidx(g, 4, j, k)] - Jy[cidx(g, 3, j, k)];
     Jz[cidx(g, 4, j, k)] = Jz[cidx(g, 4, j, k)] - Jz[cidx(g, 3, j, k)];
-    Jx[cidx(g, 3, j, k)] = 0.0;
-    Jy[cidx(g, 2, j, k)] = 0.0;
-    Jz[cidx(g, 2, j, k)] = 0.0;
+    Jx[cidx(g, 3, j, k)] = (T)0.0;
+    Jy[cidx(g, 2, j, k)] = (T)0.0;
+    Jz[cidx(g, 2, j, k)] = (T)0.0;
 }
 
 void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
@@ -530,7 +559,317 @@ void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *c
 {
     const CylP cp = cyl_params(g);
     k_cyl_move<0><<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
-    k_cyl_axis_current<<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
+    k_cyl_axis_current<double><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
+    count_launches(2);
+}
+
+// ---------------------------------------------------------------------------
+// FP32 cell-relative form of the cylindrical mover.  The algorithm is the
+// one of k_cyl_move (cyl_movdep_strang.F90:14-378 with the near-axis
+// sub-stepper :404-566); positions are (cell, offset) as in the Cartesian
+// FP32 form, and the radial, azimuthal and axial displacements are added to
+// the offsets, never to absolute coordinates: the new radius is r0 + dr with
+// dr = (dx (2 r0 + dx) + dy^2) / (r1 + r0) (= r1 - r0 without cancellation),
+// so FP32 keeps sub-cell resolution far from the axis and along a long z.
+// Near the axis (x < 4.5) the sub-stepper runs on absolute x and theta
+// (small numbers there) and on z relative to the start cell.  The periodic
+// wrap in theta and z and the drop of particles leaving the outer radius are
+// integer updates of the cell, inside the mover.
+// ---------------------------------------------------------------------------
+
+// Interp_VecEM_GridPoints at cell (ip, jp, kp) + offsets (dx, dy, dz).
+__device__ __forceinline__ void interp3f(const GridP &g, const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                         const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                         const float *__restrict__ By, const float *__restrict__ Bz, int ip, int jp,
+                                         int kp, float dx, float dy, float dz, float pE[3], float pB[3])
+{
+    float wt[8];
+#pragma unroll
+    for (int nn = 0; nn < 8; nn++) {
+        const float wx = (nn & 1) ? dx : 1.f - dx;
+        const float wy = (nn & 2) ? dy : 1.f - dy;
+        const float wz = (nn & 4) ? dz : 1.f - dz;
+        wt[nn] = (wx * wy) * wz;
+    }
+    const long long sy = g.sy, sz = g.sz;
+    const long long c0 = cidx(g, ip, jp, kp);
+    pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.f;
+#pragma unroll
+    for (int nn = 0; nn < 8; nn++) {
+        const long long nd = c0 + (nn & 1) + ((nn >> 1) & 1) * sy + ((nn >> 2) & 1) * sz;
+        const float vex = (ldd(Ex + nd - 1) + ldd(Ex + nd)) * 0.5f;
+        const float vey = (ldd(Ey + nd - sy) + ldd(Ey + nd)) * 0.5f;
+        const float vez = (ldd(Ez + nd - sz) + ldd(Ez + nd)) * 0.5f;
+        const float vbx = (((ldd(Bx + nd - sy - sz) + ldd(Bx + nd - sz)) + ldd(Bx + nd - sy)) + ldd(Bx + nd)) * 0.25f + g.bext_f[0];
+        const float vby = (((ldd(By + nd - 1 - sz) + ldd(By + nd - 1)) + ldd(By + nd - sz)) + ldd(By + nd)) * 0.25f + g.bext_f[1];
+        const float vbz = (((ldd(Bz + nd - 1 - sy) + ldd(Bz + nd - 1)) + ldd(Bz + nd - sy)) + ldd(Bz + nd)) * 0.25f + g.bext_f[2];
+        pE[0] = fmaf(wt[nn], vex, pE[0]);
+        pE[1] = fmaf(wt[nn], vey, pE[1]);
+        pE[2] = fmaf(wt[nn], vez, pE[2]);
+        pB[0] = fmaf(wt[nn], vbx, pB[0]);
+        pB[1] = fmaf(wt[nn], vby, pB[1]);
+        pB[2] = fmaf(wt[nn], vbz, pB[2]);
+    }
+}
+
+// Absolute (cell + offset) coordinate x split into cell and offset.
+__device__ __forceinline__ int split_coord(float x, float &off)
+{
+    const float f = floorf(x);
+    off = x - f;
+    return (int)f;
+}
+
+__device__ __forceinline__ void half_boris_f(float sqc, const float pE[3], const float pB[3], float &u0, float &v0,
+                                             float &w0)
+{
+    const float gg = rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
+    const float bx = gg * pB[0], by = gg * pB[1], bz = gg * pB[2];
+    const float ff = __fdividef(2.f, fmaf(bz, bz, fmaf(by, by, fmaf(bx, bx, 1.f))));
+    const float u1 = fmaf(-w0, by, fmaf(v0, bz, u0)) * ff;
+    const float v1 = fmaf(-u0, bz, fmaf(w0, bx, v0)) * ff;
+    const float w1 = fmaf(-v0, bx, fmaf(u0, by, w0)) * ff;
+    u0 = fmaf(-w1, by, fmaf(v1, bz, u0)) + pE[0];
+    v0 = fmaf(-u1, bz, fmaf(w1, bx, v0)) + pE[1];
+    w0 = fmaf(-v1, bx, fmaf(u1, by, w0)) + pE[2];
+}
+
+// DepositCurrentPIC (deposit.F90:11-103) for the sub-stepper: x, y absolute,
+// z relative to cell kb.
+__device__ void deposit_pic_f(const GridP &g, float *Jx, float *Jy, float *Jz, float x0, float y0, float z0, float x,
+                              float y, float z, int kb, float qthis)
+{
+    const int i1 = (int)floorf(x0), i2 = (int)floorf(x), j1 = (int)floorf(y0), j2 = (int)floorf(y);
+    const int kk1 = (int)floorf(z0), kk2 = (int)floorf(z);
+    const float xr = fminf((float)(min(i1, i2) + 1), fmaxf((float)max(i1, i2), 0.5f * (x0 + x)));
+    const float yr = fminf((float)(min(j1, j2) + 1), fmaxf((float)max(j1, j2), 0.5f * (y0 + y)));
+    const float zr = fminf((float)(min(kk1, kk2) + 1), fmaxf((float)max(kk1, kk2), 0.5f * (z0 + z)));
+    const float Fx1 = qthis * (xr - x0), Fy1 = qthis * (yr - y0), Fz1 = qthis * (zr - z0);
+    const float Wx1 = 0.5f * (x0 + xr) - i1, Wy1 = 0.5f * (y0 + yr) - j1;
+    const float Wx2 = 0.5f * (x + xr) - i2, Wy2 = 0.5f * (y + yr) - j2;
+    const float Wz1 = 0.5f * (z0 + zr) - kk1, Wz2 = 0.5f * (z + zr) - kk2;
+    const float Fx2 = qthis * (x - xr), Fy2 = qthis * (y - yr), Fz2 = qthis * (z - zr);
+    const int k1 = kb + kk1, k2 = kb + kk2;
+    atomicAdd(Jx + cidx(g, i1, j1, k1), (Fx1 * (1.f - Wy1)) * (1.f - Wz1));
+    atomicAdd(Jx + cidx(g, i1, j1 + 1, k1), (Fx1 * Wy1) * (1.f - Wz1));
+    atomicAdd(Jx + cidx(g, i1, j1, k1 + 1), (Fx1 * (1.f - Wy1)) * Wz1);
+    atomicAdd(Jx + cidx(g, i1, j1 + 1, k1 + 1), (Fx1 * Wy1) * Wz1);
+    atomicAdd(Jx + cidx(g, i2, j2, k2), (Fx2 * (1.f - Wy2)) * (1.f - Wz2));
+    atomicAdd(Jx + cidx(g, i2, j2 + 1, k2), (Fx2 * Wy2) * (1.f - Wz2));
+    atomicAdd(Jx + cidx(g, i2, j2, k2 + 1), (Fx2 * (1.f - Wy2)) * Wz2);
+    atomicAdd(Jx + cidx(g, i2, j2 + 1, k2 + 1), (Fx2 * Wy2) * Wz2);
+    atomicAdd(Jy + cidx(g, i1, j1, k1), (Fy1 * (1.f - Wx1)) * (1.f - Wz1));
+    atomicAdd(Jy + cidx(g, i1 + 1, j1, k1), (Fy1 * Wx1) * (1.f - Wz1));
+    atomicAdd(Jy + cidx(g, i1, j1, k1 + 1), (Fy1 * (1.f - Wx1)) * Wz1);
+    atomicAdd(Jy + cidx(g, i1 + 1, j1, k1 + 1), (Fy1 * Wx1) * Wz1);
+    atomicAdd(Jy + cidx(g, i2, j2, k2), (Fy2 * (1.f - Wx2)) * (1.f - Wz2));
+    atomicAdd(Jy + cidx(g, i2 + 1, j2, k2), (Fy2 * Wx2) * (1.f - Wz2));
+    atomicAdd(Jy + cidx(g, i2, j2, k2 + 1), (Fy2 * (1.f - Wx2)) * Wz2);
+    atomicAdd(Jy + cidx(g, i2 + 1, j2, k2 + 1), (Fy2 * Wx2) * Wz2);
+    atomicAdd(Jz + cidx(g, i1, j1, k1), (Fz1 * (1.f - Wx1)) * (1.f - Wy1));
+    atomicAdd(Jz + cidx(g, i1 + 1, j1, k1), (Fz1 * Wx1) * (1.f - Wy1));
+    atomicAdd(Jz + cidx(g, i1, j1 + 1, k1), (Fz1 * (1.f - Wx1)) * Wy1);
+    atomicAdd(Jz + cidx(g, i1 + 1, j1 + 1, k1), (Fz1 * Wx1) * Wy1);
+    atomicAdd(Jz + cidx(g, i2, j2, k2), (Fz2 * (1.f - Wx2)) * (1.f - Wy2));
+    atomicAdd(Jz + cidx(g, i2 + 1, j2, k2), (Fz2 * Wx2) * (1.f - Wy2));
+    atomicAdd(Jz + cidx(g, i2, j2 + 1, k2), (Fz2 * (1.f - Wx2)) * Wy2);
+    atomicAdd(Jz + cidx(g, i2 + 1, j2 + 1, k2), (Fz2 * Wx2) * Wy2);
+}
+
+__global__ void __launch_bounds__(kThreads) k_cyl_move_f32(GridP g, CylP cp, PartF32 p, const Counters *__restrict__ cnt,
+                                                           const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                                           const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                                           const float *__restrict__ By, const float *__restrict__ Bz,
+                                                           float *Jx, float *Jy, float *Jz, int *err)
+{
+    const long long used = cnt->used;
+    const float c = g.c_f, sqc = g.sqc_f, cinv = g.cinv_f, qi = g.qi_f;
+    const float inv_dtheta = (float)cp.inv_dtheta;
+    const float ymin = (float)g.ymin, ymax = (float)g.ymax, ylen = (float)g.ylen;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
+        const uint32_t key = p.key[n];
+        const int flv = (int)(key >> kFlvShift);
+        if (flv == 0) continue;  // a hole moves nowhere and deposits zero
+        int i, j, k;
+        decode_cell(g, (int)(key & kCellMask), i, j, k);
+        if (flv > PIC_MAX_FLVR || i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 || k < 3 || k > g.mz - 3) {
+            raise_error(err, PIC_DEVERR_RANGE);
+            continue;
+        }
+        const float dx = p.dx[n], dy = p.dy[n], dz = p.dz[n];
+        const float ui = p.ux[n], vi = p.uy[n], wi = p.uz[n], w8 = p.w[n];
+        const float qm = (float)(g.qm[flv] * 0.25);  // cyl_movdep_strang.F90:100
+        int ni, nj, nk;            // new cell
+        float ox, oy, oz;          // new offsets
+        float un, vn, wn;
+        if (i > 4 || (i == 4 && dx >= 0.5f)) {
+            // Strang step away from the axis (:104-341)
+            float pE[3], pB[3];
+            interp3f(g, Ex, Ey, Ez, Bx, By, Bz, i, j, k, dx, dy, dz, pE, pB);
+            for (int d = 0; d < 3; d++) {
+                pE[d] *= qm;
+                pB[d] *= qm;
+            }
+            float u0 = fmaf(c, ui, pE[0]), v0 = fmaf(c, vi, pE[1]), w0 = fmaf(c, wi, pE[2]);
+            half_boris_f(sqc, pE, pB, u0, v0, w0);
+            float u1 = u0 * cinv, v1 = v0 * cinv;
+            const float gg = sqc * rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
+            const float r0 = ((float)i - 3.5f) + dx;          // x - 3 + rmin, rmin = -0.5
+            const float ddx = u1 * gg, ddy = v1 * gg;
+            const float xx1 = r0 + ddx;
+            const float r1 = sqrtf(fmaf(xx1, xx1, ddy * ddy));
+            const float dr = __fdividef(fmaf(ddx, 2.f * r0 + ddx, ddy * ddy), r1 + r0);
+            const float dth = atanf(__fdividef(ddy, xx1)) * inv_dtheta;
+            const float dzz = wi * gg;                          // z moves with this step's initial w (:202)
+            const float rinv = 1.f / r1;
+            u1 = fmaf(r0, u0, fmaf(u0 * u1, gg, v0 * ddy)) * rinv;
+            v1 = (v0 * r0) * rinv;
+            // new cell and offsets (each displacement is below one cell here)
+            const float Xn = dx + dr, Yn = dy + dth, Zn = dz + dzz;
+            const int sx = Xn >= 1.f ? 1 : (Xn < 0.f ? -1 : 0);
+            const int sy = Yn >= 1.f ? 1 : (Yn < 0.f ? -1 : 0);
+            const int sz = Zn >= 1.f ? 1 : (Zn < 0.f ? -1 : 0);
+            ni = i + sx;
+            nj = j + sy;
+            nk = k + sz;
+            ox = Xn - (float)sx;
+            oy = Yn - (float)sy;
+            oz = Zn - (float)sz;
+            interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ni, nj, nk, ox, oy, oz, pE, pB);
+            for (int d = 0; d < 3; d++) {
+                pE[d] *= qm;
+                pB[d] *= qm;
+            }
+            u0 = u1 + pE[0];
+            v0 = v1 + pE[1];
+            w0 = w0 + pE[2];
+            half_boris_f(sqc, pE, pB, u0, v0, w0);
+            un = u0 * cinv;
+            vn = v0 * cinv;
+            wn = w0 * cinv;
+            // zigzag deposit; both segments use the start cell (:341)
+            const float qthis = w8 * qi;
+            const float xr = fminf((float)(min(0, sx) + 1), fmaxf((float)max(0, sx), 0.5f * (dx + Xn)));
+            const float yr = fminf((float)(min(0, sy) + 1), fmaxf((float)max(0, sy), 0.5f * (dy + Yn)));
+            const float zr = fminf((float)(min(0, sz) + 1), fmaxf((float)max(0, sz), 0.5f * (dz + Zn)));
+            float o[12], o2[12];
+            segment<float, 3>(qthis * (xr - dx), qthis * (yr - dy), qthis * (zr - dz), 0.5f * (dx + xr),
+                              0.5f * (dy + yr), 0.5f * (dz + zr), o);
+            segment<float, 3>(qthis * (Xn - xr), qthis * (Yn - yr), qthis * (Zn - zr), 0.5f * (Xn + xr) - (float)sx,
+                              0.5f * (Yn + yr) - (float)sy, 0.5f * (Zn + zr) - (float)sz, o2);
+            for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
+            scatter<float, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o);
+        } else {
+            // SubStepMovDep (:404-438) from the step's initial state: x and
+            // theta absolute (small here), z relative to the start cell
+            float pE[3], pB[3];
+            float xn = (float)i + dx, yn = (float)j + dy, zn = dz;
+            un = ui;
+            vn = vi;
+            wn = wi;
+            float t = 0.f, dt = 1.f, sx0 = xn, sy0 = yn, sz0 = zn;
+            int tries = 0;
+            while (t < 1.f) {
+                if (++tries > kMaxSubsteps) {
+                    raise_error(err, PIC_DEVERR_SUBSTEP);
+                    break;
+                }
+                const float delt = (t + dt > 1.f) ? 1.f - t : dt;
+                // MovePrtlAxis (:462-566)
+                {
+                    float fx, fy, fz;
+                    const int ci = split_coord(sx0, fx), cj = split_coord(sy0, fy), ck = k + split_coord(sz0, fz);
+                    interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ci, cj, ck, fx, fy, fz, pE, pB);
+                }
+                for (int d = 0; d < 3; d++) {
+                    pE[d] = (pE[d] * qm) * delt;
+                    pB[d] = (pB[d] * qm) * delt;
+                }
+                float a0 = fmaf(c, un, pE[0]), b0 = fmaf(c, vn, pE[1]), c0 = fmaf(c, wn, pE[2]);
+                half_boris_f(sqc, pE, pB, a0, b0, c0);
+                float a1 = a0 * cinv, b1 = b0 * cinv;
+                const float c1 = c0 * cinv;
+                const float g2 = sqc * rsqrtf(fmaf(c0, c0, fmaf(b0, b0, fmaf(a0, a0, sqc))));
+                const float rr0 = sx0 - 3.5f;
+                const float X1 = rr0 + (a1 * g2) * delt;
+                const float Y1 = (b1 * g2) * delt;
+                const float R1 = sqrtf(fmaf(X1, X1, Y1 * Y1));
+                const float ddy = X1 > 0.f ? atanf(__fdividef(Y1, X1)) * inv_dtheta : 0.f;
+                if (fabsf(ddy) > 0.45f) {
+                    dt = dt * 0.5f;
+                    continue;
+                }
+                float nx;
+                if (X1 > 0.f) {
+                    nx = R1 + 3.5f;
+                    a1 = fmaf(rr0, a0, fmaf((a0 * a1) * g2, delt, b0 * Y1)) / R1;
+                    b1 = (b0 * rr0) / R1;
+                } else {
+                    nx = X1 + 3.5f;
+                }
+                const float ny = yn + ddy;
+                const float nz = zn + (c1 * g2) * delt;
+                {
+                    float fx, fy, fz;
+                    const int ci = split_coord(nx, fx), cj = split_coord(ny, fy), ck = k + split_coord(nz, fz);
+                    interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ci, cj, ck, fx, fy, fz, pE, pB);
+                }
+                for (int d = 0; d < 3; d++) {
+                    pE[d] = (pE[d] * qm) * delt;
+                    pB[d] = (pB[d] * qm) * delt;
+                }
+                a0 = a1 + pE[0];
+                b0 = b1 + pE[1];
+                c0 = c0 + pE[2];
+                half_boris_f(sqc, pE, pB, a0, b0, c0);
+                xn = nx;
+                yn = ny;
+                zn = nz;
+                un = a0 * cinv;
+                vn = b0 * cinv;
+                wn = c0 * cinv;
+                t = t + delt;
+                deposit_pic_f(g, Jx, Jy, Jz, sx0, sy0, sz0, xn, yn, zn, k, w8 * qi);
+                // PrtlAxisBC (:450-460)
+                if (xn < 3.5f) {
+                    xn = 3.5f + (3.5f - xn);
+                    yn = yn + 0.5f * (float)g.ny;
+                    un = -un;
+                    vn = -vn;
+                }
+                if (yn > ymax) yn = yn - ylen;
+                if (yn < ymin) yn = yn + ylen;
+                dt = dt * 1.7f;
+                sx0 = xn;
+                sy0 = yn;
+                sz0 = zn;
+            }
+            ni = split_coord(xn, ox);
+            nj = split_coord(yn, oy);
+            nk = k + split_coord(zn, oz);
+        }
+        // periodic theta and z, particles past the outer radius leave
+        nj = wrap_index(nj, g.my);
+        nk = wrap_index(nk, g.mz);
+        uint32_t nkey = 0;
+        if (ni >= 3 && ni <= g.mx - 3) nkey = ((uint32_t)flv << kFlvShift) | (uint32_t)cidx(g, ni, nj, nk);
+        p.key[n] = nkey;
+        p.dx[n] = ox;
+        p.dy[n] = oy;
+        p.dz[n] = oz;
+        p.ux[n] = un;
+        p.uy[n] = vn;
+        p.uz[n] = wn;
+    }
+}
+
+void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
+                                 float *const B[3], float *const J[3], int *err, cudaStream_t s)
+{
+    const CylP cp = cyl_params(g);
+    k_cyl_move_f32<<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
+                                                 err);
+    k_cyl_axis_current<float><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
     count_launches(2);
 }
 

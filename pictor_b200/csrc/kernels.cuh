@@ -31,9 +31,12 @@ template <typename T> void launch_fold(const GridP &g, T *const J[3], cudaStream
 template <typename T> void launch_filter(const GridP &g, T *const J[3], T *tmp, cudaStream_t s);
 
 // cyl.cu (cylindrical FP64 form)
-void launch_cyl_bhalf(const GridP &g, double *const E[3], double *const B[3], cudaStream_t s);
-void launch_cyl_efield(const GridP &g, int mode, double *const E[3], double *const B[3], double *const J[3], cudaStream_t s);
-void launch_cyl_fold(const GridP &g, double *const J[3], cudaStream_t s);
+template <typename T>
+void launch_cyl_bhalf(const GridP &g, T *const E[3], T *const B[3], cudaStream_t s);
+template <typename T>
+void launch_cyl_efield(const GridP &g, int mode, T *const E[3], T *const B[3], T *const J[3], cudaStream_t s);
+template <typename T>
+void launch_cyl_fold(const GridP &g, T *const J[3], cudaStream_t s);
 // modal.cu: the cylindrical field solve on azimuthal modes m = 0, 1 (arrays (mx, 3, mz))
 void launch_modal_bhalf(const GridP &g, double *const Em[3], double *const Bm[3], cudaStream_t s);
 void launch_modal_efield(const GridP &g, int mode, double *const Em[3], double *const Bm[3], double *const Jm[3],
@@ -42,6 +45,8 @@ void launch_modal_synth(const GridP &g, double *const Fm[3], double *const F[3],
 void launch_modal_project(const GridP &g, double *const F[3], double *const Fm[3], cudaStream_t s);
 void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
                              double *const B[3], double *const J[3], int *err, cudaStream_t s);
+void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
+                                 float *const B[3], float *const J[3], int *err, cudaStream_t s);
 
 // mover.cu
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],

@@ -561,6 +561,104 @@ def test_cyl_wakefield_lockstep():
         assert np.abs(gf.Ez).max() > 0
 
 
+@pytest.mark.parametrize("fdtd", ["yee", "lehe"])
+def test_cyl_fp32_field_phases_track_fp64(fdtd):
+    """The FP32 cylindrical form's field phases (B half step with the axis
+    updates, E update, fold, AddCurrent) equal the FP64 ones to FP32
+    rounding (1e-6 of the field scale)."""
+    g, cfg64 = _cyl(fdtd)
+    _, cfg32 = _cyl(fdtd)
+    cfg32.precision = "fp32"
+    f = random_fields(g, seed=51, consistent_ghosts=False)
+    rng = np.random.default_rng(6)
+    J = [np.asfortranarray(rng.normal(scale=1e-3, size=O.grid_shape(g))) for _ in range(3)]
+    out = {}
+    for name, cfg in (("fp64", cfg64), ("fp32", cfg32)):
+        with _sim(cfg) as s:
+            s.load_fields(to_gpu_fields(f))
+            s.update_b_half()
+            s.update_e()
+            s.load_current(*J)
+            s.fold_current()
+            s.add_current()
+            out[name] = s.fetch_fields()
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Jy", "Jz"):
+        a, b = getattr(out["fp32"], n), getattr(out["fp64"], n)
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-6 * np.abs(b).max(), err_msg=n)
+
+
+def test_cyl_fp32_mover_tracks_fp64():
+    """One push + deposit of the FP32 cell-relative cylindrical mover against
+    the FP64 one on the same particles (including near-axis particles, which
+    take the sub-stepper) and fields: positions to 1e-5 of a cell (the FP64
+    ones wrapped in theta and z as the FP32 mover does), momenta to 1e-5
+    relative, and the folded current to 1e-4 of its scale."""
+    g, cfg64 = _cyl("lehe", capacity=1 << 15)
+    _, cfg32 = _cyl("lehe", capacity=1 << 15)
+    cfg32.precision = "fp32"
+    f = random_fields(g, seed=57, scale=0.02)
+    p = _cyl_particles(g, seed=8)
+    # keep clear of the outer radius (the FP32 mover drops leavers at once)
+    keep = p.x[:p.used] < g.mx - 4.0
+    n = int(keep.sum())
+    gp = to_gpu_particles(p)
+    from pictor_b200 import Particles
+
+    gp = Particles(*(getattr(gp, k)[:p.used][keep].copy() for k in gp.NAMES))
+    out = {}
+    for name, cfg in (("fp64", cfg64), ("fp32", cfg32)):
+        with _sim(cfg) as s:
+            s.load_particles(gp)
+            s.load_fields(to_gpu_fields(f))
+            s.move_deposit()
+            s.fold_current()
+            assert s.device_errors() == 0
+            out[name] = (s.fetch_particles(), s.fetch_fields())
+    (p64, f64), (p32, f32) = out["fp64"], out["fp32"]
+    assert len(p32.x) == len(p64.x) == n
+    ylo, ylen = 3.0, g.my - 5.0
+    zlo, zlen = 3.0, g.mz - 5.0
+    y64 = (p64.y - ylo) % ylen + ylo
+    z64 = (p64.z - zlo) % zlen + zlo
+    np.testing.assert_allclose(p32.x, p64.x, rtol=0, atol=1e-5)
+    dy = np.abs(p32.y - y64)
+    assert np.minimum(dy, ylen - dy).max() < 1e-5
+    dz = np.abs(p32.z - z64)
+    assert np.minimum(dz, zlen - dz).max() < 1e-5
+    for k in ("u", "v", "w"):
+        a, b = getattr(p32, k), getattr(p64, k)
+        np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * np.abs(b).max(), err_msg=k)
+    for nme in ("Jx", "Jy", "Jz"):
+        a, b = interior(getattr(f32, nme), g), interior(getattr(f64, nme), g)
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-4 * np.abs(b).max(), err_msg=nme)
+
+
+def test_cyl_fp32_steps_track_fp64():
+    """The wakefield case of test_cyl_wakefield_lockstep, 20 steps in the
+    FP32 form against the FP64 form: particle count equal, field energy
+    within 1e-3 and kinetic energy within 1e-5."""
+    from pictor_b200 import PicConfig, Simulation, init_scale
+    from pictor_b200.setups import cyl_wakefield
+
+    nr, nt, nz, c = 20, 8, 48, 0.3
+    qi = init_scale(c, 10.0, 8)["qi"]
+    gp, _ = cyl_wakefield(nr, nz, nt, c, bunch_sigma_r=3.0, bunch_sigma_z=5.0, bunch_particles=4096, seed=11)
+    res = {}
+    for prec in ("fp64", "fp32"):
+        cfg = PicConfig(nx=nr, ny=nt, nz=nz, dims=3, c=c, qi=qi, qm=(1.0, -1.0), fdtd="lehe", geom="cylindrical",
+                        precision=prec, capacity=3 * len(gp.x), reorder_period=10, rmin=-0.5, inc_axis=1)
+        with Simulation(cfg) as s:
+            s.load_particles(gp)
+            s.step(20)
+            assert s.device_errors() == 0
+            res[prec] = (s.particle_count(), s.diagnostics())
+    (n64, d64), (n32, d32) = res["fp64"], res["fp32"]
+    assert n32 == n64
+    fe64, fe32 = d64["B2"] + d64["E2"], d32["B2"] + d32["E2"]
+    assert abs(fe32 - fe64) <= 1e-3 * fe64
+    np.testing.assert_allclose(d32["kinetic"].sum(), d64["kinetic"].sum(), rtol=1e-5)
+
+
 def test_cyl_field_energy_matches_oracle():
     g, cfg = _cyl()
     f = random_fields(g, seed=53, consistent_ghosts=False)
