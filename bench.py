@@ -60,6 +60,10 @@ WORKLOADS = {
     # the same run in the FP32 cell-relative form (theta-gridded FP32 fields)
     "cyl_wake_fp32": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp32", thermal=0.01,
                           bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0),
+    # the C3 configuration as stated: modes m = 0, 1, FP32 fields and particles
+    "cyl_wake_modal_fp32": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp32",
+                                thermal=0.01, bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0,
+                                cyl_modes=2),
     # a small case of the same physics for profiler captures (4.2 M particles, 250 MB > L2)
     "cyl_wake_small": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                            bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0, bunch_sigma_z=10.0),
@@ -618,7 +622,8 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if wl["precision"] == "fp32" else "f64", "data": "synthetic",
             "config": {"workload": args.workload,
-                       "form": ("field solve on azimuthal modes m=0,1 (FP64), particles on the theta grid"
+                       "form": (("field solve on azimuthal modes m=0,1, particles on the theta grid, "
+                                 + ("FP32 (cell-relative particles)" if wl["precision"] == "fp32" else "FP64"))
                                 if wl.get("cyl_modes", 0) else
                                 "FP32 cell-relative particles, theta-gridded FP32 fields" if wl["precision"] == "fp32"
                                 else "theta-gridded FP64 (the reference's representation)"),
@@ -696,7 +701,7 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
-    if args.workload in ("cyl_wake", "cyl_wake_small", "cyl_wake_modal", "cyl_wake_fp32"):
+    if args.workload.startswith("cyl_wake"):
         peak, peak_kind = measured_peaks()
         return run_cyl_bench(args, rank, local, peak, peak_kind)
     wl = WORKLOADS[args.workload]

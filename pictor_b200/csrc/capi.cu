@@ -23,7 +23,7 @@ struct pic_handle {
     // cylindrical modal form: the fields on modes m = 0, 1, (mx, 3, mz) each;
     // E and B above are kept equal to their theta-gridded synthesis
     bool modal = false;
-    double *Em[3] = {}, *Bm[3] = {}, *Jm[3] = {};
+    void *Em[3] = {}, *Bm[3] = {}, *Jm[3] = {};   // the handle's precision
     PartF64 p64[2] = {};
     PartF32 p32[2] = {};
     int cur = 0;
@@ -183,6 +183,72 @@ void field_ptrs(pic_handle *h, T *E[3], T *B[3], T *J[3])
     }
 }
 
+// The modal field phases (cyl_modes = 2) in the handle's precision T: each
+// leaves the theta-gridded E / B equal to the synthesis of the modes.
+template <typename T>
+void modal_ptrs(pic_handle *h, T *Em[3], T *Bm[3], T *Jm[3])
+{
+    for (int k = 0; k < 3; k++) {
+        Em[k] = (T *)h->Em[k];
+        Bm[k] = (T *)h->Bm[k];
+        Jm[k] = (T *)h->Jm[k];
+    }
+}
+template <typename T>
+void modal_bhalf(pic_handle *h)
+{
+    T *E[3], *B[3], *J[3], *Em[3], *Bm[3], *Jm[3];
+    field_ptrs(h, E, B, J);
+    modal_ptrs(h, Em, Bm, Jm);
+    launch_modal_bhalf<T>(h->g, Em, Bm, h->s);
+    launch_modal_synth<T>(h->g, Bm, B, h->s);
+}
+template <typename T>
+void modal_update_e(pic_handle *h)
+{
+    T *E[3], *B[3], *J[3], *Em[3], *Bm[3], *Jm[3];
+    field_ptrs(h, E, B, J);
+    modal_ptrs(h, Em, Bm, Jm);
+    launch_modal_efield<T>(h->g, 0, Em, Bm, Jm, h->s);
+    launch_modal_synth<T>(h->g, Em, E, h->s);
+}
+// AddCurrent of the (folded) theta-gridded J, projected onto the modes.
+template <typename T>
+void modal_add_current(pic_handle *h)
+{
+    T *E[3], *B[3], *J[3], *Em[3], *Bm[3], *Jm[3];
+    field_ptrs(h, E, B, J);
+    modal_ptrs(h, Em, Bm, Jm);
+    launch_modal_project<T>(h->g, J, Jm, h->s);
+    launch_modal_efield<T>(h->g, 2, Em, Bm, Jm, h->s);
+    launch_modal_synth<T>(h->g, Em, E, h->s);
+}
+// The E phase of a step: E update, fold, projection, AddCurrent, synthesis.
+template <typename T>
+void modal_efield_phase(pic_handle *h)
+{
+    T *E[3], *B[3], *J[3], *Em[3], *Bm[3], *Jm[3];
+    field_ptrs(h, E, B, J);
+    modal_ptrs(h, Em, Bm, Jm);
+    launch_modal_efield<T>(h->g, 0, Em, Bm, Jm, h->s);
+    launch_cyl_fold<T>(h->g, J, h->s);
+    launch_modal_project<T>(h->g, J, Jm, h->s);
+    launch_modal_efield<T>(h->g, 2, Em, Bm, Jm, h->s);
+    launch_modal_synth<T>(h->g, Em, E, h->s);
+}
+// Loaded theta-gridded fields -> their modes m = 0, 1; E, B become the synthesis.
+template <typename T>
+void modal_load(pic_handle *h)
+{
+    T *E[3], *B[3], *J[3], *Em[3], *Bm[3], *Jm[3];
+    field_ptrs(h, E, B, J);
+    modal_ptrs(h, Em, Bm, Jm);
+    launch_modal_project<T>(h->g, E, Em, h->s);
+    launch_modal_project<T>(h->g, B, Bm, h->s);
+    launch_modal_synth<T>(h->g, Em, E, h->s);
+    launch_modal_synth<T>(h->g, Bm, B, h->s);
+}
+
 // One phase of a full step (MAIN.F90:42-284), enqueued on h->s; reads
 // buffer `cur` and, for the reorder phase, leaves the particles in cur^1.
 // Returns the number of kernels it launched.
@@ -197,7 +263,8 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
         switch (phase) {
             case PIC_PHASE_BHALF1:
             case PIC_PHASE_BHALF2:
-                launch_cyl_bhalf<float>(g, E, B, h->s);
+                if (h->modal) modal_bhalf<float>(h);
+                else launch_cyl_bhalf<float>(g, E, B, h->s);
                 break;
             case PIC_PHASE_MOVE:  // push, deposit and the wrap / outer-radius drop
                 launch_cyl_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
@@ -205,9 +272,13 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
             case PIC_PHASE_EXCHANGE:
                 break;
             case PIC_PHASE_EFIELD:
-                launch_cyl_efield<float>(g, 0, E, B, J, h->s);
-                launch_cyl_fold<float>(g, J, h->s);
-                launch_cyl_efield<float>(g, 2, E, B, J, h->s);
+                if (h->modal) {
+                    modal_efield_phase<float>(h);
+                } else {
+                    launch_cyl_efield<float>(g, 0, E, B, J, h->s);
+                    launch_cyl_fold<float>(g, J, h->s);
+                    launch_cyl_efield<float>(g, 2, E, B, J, h->s);
+                }
                 for (int c = 0; c < 3; c++) cudaMemsetAsync(J[c], 0, (size_t)g.ncell * sizeof(float), h->s);
                 break;
             case PIC_PHASE_REORDER:
@@ -223,12 +294,8 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
         switch (phase) {
             case PIC_PHASE_BHALF1:  // cyl_em_update.F90:49-110 + halo
             case PIC_PHASE_BHALF2:
-                if (h->modal) {
-                    launch_modal_bhalf(g, h->Em, h->Bm, h->s);
-                    launch_modal_synth(g, h->Bm, B, h->s);
-                } else {
-                    launch_cyl_bhalf(g, E, B, h->s);
-                }
+                if (h->modal) modal_bhalf<double>(h);
+                else launch_cyl_bhalf(g, E, B, h->s);
                 break;
             case PIC_PHASE_MOVE:  // cyl_movdep_strang.F90:14-378
                 launch_cyl_move_deposit(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);
@@ -238,11 +305,7 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 break;
             case PIC_PHASE_EFIELD:  // UpdateEfield, halo, fold, AddCurrent, halo, ResetCurrent
                 if (h->modal) {
-                    launch_modal_efield(g, 0, h->Em, h->Bm, h->Jm, h->s);
-                    launch_cyl_fold(g, J, h->s);
-                    launch_modal_project(g, J, h->Jm, h->s);
-                    launch_modal_efield(g, 2, h->Em, h->Bm, h->Jm, h->s);
-                    launch_modal_synth(g, h->Em, E, h->s);
+                    modal_efield_phase<double>(h);
                 } else {
                     launch_cyl_efield(g, 0, E, B, J, h->s);
                     launch_cyl_fold(g, J, h->s);
@@ -768,13 +831,11 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (c.dims != 2 && c.dims != 3) return PIC_ERR_INVALID;
     if (c.geom != PIC_GEOM_CARTESIAN && c.geom != PIC_GEOM_CYLINDRICAL) return PIC_ERR_INVALID;
     // the cylindrical step: 3D, with the axis on this rank, no current filter;
-    // the reference's FP64 form or the FP32 cell-relative one (theta-gridded
-    // fields); the modal field solve in FP64
+    // the reference's FP64 form or the FP32 cell-relative one, each with the
+    // theta-gridded or the modal (m = 0, 1) field solve
     if (c.geom == PIC_GEOM_CYLINDRICAL && (c.dims != 3 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
         return PIC_ERR_INVALID;
-    if (c.cyl_modes != 0 &&
-        (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4 || c.precision != PIC_PREC_FP64))
-        return PIC_ERR_INVALID;
+    if (c.cyl_modes != 0 && (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4)) return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
@@ -850,13 +911,15 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (!r && c.curr_filter > 0) r = dalloc(h, (char **)&h->Jtmp, fb);
     if (!r && c.cyl_modes == 2) {
         h->modal = true;
-        const size_t nm = (size_t)g.mx * 3 * (size_t)g.mz;
+        const size_t nm = (size_t)g.mx * 3 * (size_t)g.mz, esz = h->fp32 ? sizeof(float) : sizeof(double);
         for (int k = 0; k < 3 && !r; k++)
-            if ((r = dalloc(h, &h->Em[k], nm)) || (r = dalloc(h, &h->Bm[k], nm)) || (r = dalloc(h, &h->Jm[k], nm))) break;
+            if ((r = dalloc(h, (char **)&h->Em[k], nm * esz)) || (r = dalloc(h, (char **)&h->Bm[k], nm * esz)) ||
+                (r = dalloc(h, (char **)&h->Jm[k], nm * esz)))
+                break;
         for (int k = 0; k < 3 && !r; k++) {
-            cudaMemsetAsync(h->Em[k], 0, nm * sizeof(double), h->s);
-            cudaMemsetAsync(h->Bm[k], 0, nm * sizeof(double), h->s);
-            cudaMemsetAsync(h->Jm[k], 0, nm * sizeof(double), h->s);
+            cudaMemsetAsync(h->Em[k], 0, nm * esz, h->s);
+            cudaMemsetAsync(h->Bm[k], 0, nm * esz, h->s);
+            cudaMemsetAsync(h->Jm[k], 0, nm * esz, h->s);
         }
     }
     if (!r) r = alloc_particles(h);
@@ -939,12 +1002,8 @@ int pic_load_fields(pic_handle *h, const double *Ex, const double *Ey, const dou
         }
     }
     if (h->modal) {   // the modes m = 0, 1 of the loaded fields; E, B become their synthesis
-        double *E[3], *B[3], *J[3];
-        field_ptrs(h, E, B, J);
-        launch_modal_project(h->g, E, h->Em, h->s);
-        launch_modal_project(h->g, B, h->Bm, h->s);
-        launch_modal_synth(h->g, h->Em, E, h->s);
-        launch_modal_synth(h->g, h->Bm, B, h->s);
+        if (h->fp32) modal_load<float>(h);
+        else modal_load<double>(h);
     }
     int r = sync_both(h);
     if (r) return r;
@@ -1134,10 +1193,8 @@ int pic_update_b_half(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     if (h->modal) {
-        double *E[3], *B[3], *J[3];
-        field_ptrs(h, E, B, J);
-        launch_modal_bhalf(h->g, h->Em, h->Bm, h->s);
-        launch_modal_synth(h->g, h->Bm, B, h->s);
+        if (h->fp32) modal_bhalf<float>(h);
+        else modal_bhalf<double>(h);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -1203,10 +1260,8 @@ int pic_update_e(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     if (h->modal) {
-        double *E[3], *B[3], *J[3];
-        field_ptrs(h, E, B, J);
-        launch_modal_efield(h->g, 0, h->Em, h->Bm, h->Jm, h->s);
-        launch_modal_synth(h->g, h->Em, E, h->s);
+        if (h->fp32) modal_update_e<float>(h);
+        else modal_update_e<double>(h);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
@@ -1275,11 +1330,8 @@ int pic_add_current(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     if (h->modal) {
-        double *E[3], *B[3], *J[3];
-        field_ptrs(h, E, B, J);
-        launch_modal_project(h->g, J, h->Jm, h->s);
-        launch_modal_efield(h->g, 2, h->Em, h->Bm, h->Jm, h->s);
-        launch_modal_synth(h->g, h->Em, E, h->s);
+        if (h->fp32) modal_add_current<float>(h);
+        else modal_add_current<double>(h);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);

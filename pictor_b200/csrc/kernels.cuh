@@ -38,11 +38,14 @@ void launch_cyl_efield(const GridP &g, int mode, T *const E[3], T *const B[3], T
 template <typename T>
 void launch_cyl_fold(const GridP &g, T *const J[3], cudaStream_t s);
 // modal.cu: the cylindrical field solve on azimuthal modes m = 0, 1 (arrays (mx, 3, mz))
-void launch_modal_bhalf(const GridP &g, double *const Em[3], double *const Bm[3], cudaStream_t s);
-void launch_modal_efield(const GridP &g, int mode, double *const Em[3], double *const Bm[3], double *const Jm[3],
-                         cudaStream_t s);
-void launch_modal_synth(const GridP &g, double *const Fm[3], double *const F[3], cudaStream_t s);
-void launch_modal_project(const GridP &g, double *const F[3], double *const Fm[3], cudaStream_t s);
+template <typename T>
+void launch_modal_bhalf(const GridP &g, T *const Em[3], T *const Bm[3], cudaStream_t s);
+template <typename T>
+void launch_modal_efield(const GridP &g, int mode, T *const Em[3], T *const Bm[3], T *const Jm[3], cudaStream_t s);
+template <typename T>
+void launch_modal_synth(const GridP &g, T *const Fm[3], T *const F[3], cudaStream_t s);
+template <typename T>
+void launch_modal_project(const GridP &g, T *const F[3], T *const Fm[3], cudaStream_t s);
 void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
                              double *const B[3], double *const J[3], int *err, cudaStream_t s);
 void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],

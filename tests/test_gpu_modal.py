@@ -97,6 +97,36 @@ def test_modal_field_phases_equal_theta_gridded(fdtd):
                                        err_msg=f"stage {stage} {n}")
 
 
+@pytest.mark.parametrize("fdtd", ["yee", "lehe"])
+def test_modal_fp32_tracks_modal_fp64(fdtd):
+    """The modal solve in FP32 (modes, theta-gridded synthesis and the FP32
+    cell-relative mover) against the FP64 modal form on the m = 1 cold-plasma
+    case: fields projected onto m = 0, 1 within 1e-4 of their scale after 8
+    steps."""
+    from pictor_b200 import Simulation
+
+    g, o = _cold_plasma_case(fdtd, 1, 1e-4)
+    got = {}
+    for prec in ("fp64", "fp32"):
+        cfg = _cfg(2, fdtd, nx=16, ny=8, nz=12)
+        cfg.precision = prec
+        with Simulation(cfg) as s:
+            s.load_particles(to_gpu_particles(o.p))
+            s.load_fields(to_gpu_fields(o.f))
+            s.step(8)
+            assert s.device_errors() == 0
+            got[prec] = s.fetch_fields(with_current=False)
+    for kind in ("E", "B"):
+        names = [kind + c for c in "xyz"]
+        ref = {n: project(getattr(got["fp64"], n), 8) for n in names}
+        f32 = {n: project(getattr(got["fp32"], n), 8) for n in names}
+        scale = max(max(np.abs(x).max() for x in ref[n]) for n in names)
+        assert scale > 0
+        for n in names:
+            for plane, (x, y) in enumerate(zip(ref[n], f32[n])):
+                np.testing.assert_allclose(y, x, rtol=0, atol=1e-4 * scale, err_msg=f"{n} plane {plane}")
+
+
 def _cold_plasma_case(fdtd, mode, amp):
     g = O.make_grid(3, 16, 8, 12, c=0.3, qi=0.01, fdtd=fdtd, qm=(1.0, -1.0))
     p = O.cyl_load_uniform(g, 1, 1, 1, 1.0, 0.0, -1.0, 2, 5, 1 << 15)
