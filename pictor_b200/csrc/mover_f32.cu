@@ -32,7 +32,12 @@
 //
 // Each thread streams particles n, n+256, ... and loads particle n+256 before
 // it moves particle n, so the DRAM latency of the next particle overlaps the
-// arithmetic of this one.
+// arithmetic of this one.  The reorder lays a brick's particles out so that
+// the lanes of a warp hold particles of neighbouring cells (bricks.cu), which
+// keeps their shared-memory accesses on distinct banks.  A particle that
+// stays in its cell deposits its two zigzag segments in closed form in one
+// pass; the second segments of the lanes that cross a face are queued per
+// warp and deposited 32 at a time.
 //
 // The node averages and interpolation sums are computed identically on both
 // paths (same expressions, same order, explicit fmaf), so the tiled and the
@@ -135,10 +140,6 @@ __device__ __forceinline__ float2 lds2i(uint32_t a)
     float2 v;
     asm volatile("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(a), "n"(OFF));
     return v;
-}
-__device__ __forceinline__ void red_shared(uint32_t a, int v)
-{
-    asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(a), "r"(v));
 }
 template <int OFF>
 __device__ __forceinline__ void red_shared_i(uint32_t a, int v)
