@@ -133,7 +133,7 @@ __host__ __device__ inline uint32_t transposed_slot(uint32_t s, uint32_t N, uint
     return col * R + row;
 }
 
-constexpr int kOrderThreads = 256;
+constexpr int kOrderThreads = 512;
 // Particles of a brick whose payload the order pass stages through shared
 // memory (a 16-bit final slot and a staging word each); a larger brick
 // writes its slots directly.
