@@ -635,7 +635,7 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
                        "l2": "particle state (GBs) larger than L2"},
             "roofline": {"bound": "hbm", "achieved": bytes_move / (move_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                          "frac": bytes_move / (move_ms * 1e-3) / 1e9 / peak, "traffic": None,
-                         "kernel": "k_cyl_move_f32" if wl["precision"] == "fp32" else "k_cyl_move",
+                         "kernel": "k_cyl_move_f32_tiled" if wl["precision"] == "fp32" else "k_cyl_move",
                          "launch_ms": move_ms, "peak_kind": peak_kind},
             "phases_ms_per_step": {k: v / max(phases["steps"], 1) for k, v in phases["ms"].items()},
             "gpu_launches": launches, "clocks": clk,

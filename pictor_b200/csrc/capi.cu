@@ -267,7 +267,10 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 else launch_cyl_bhalf<float>(g, E, B, h->s);
                 break;
             case PIC_PHASE_MOVE:  // push, deposit and the wrap / outer-radius drop
-                launch_cyl_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
+                if (h->sorted)
+                    launch_cyl_move_deposit_f32_tiled(g, h->p32[cur], h->bricks, E, B, J, h->err, h->s);
+                else
+                    launch_cyl_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
                 break;
             case PIC_PHASE_EXCHANGE:
                 break;
@@ -1229,7 +1232,10 @@ int pic_move_deposit(pic_handle *h)
     if (h->g.geom == PIC_GEOM_CYLINDRICAL && h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_cyl_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
+        if (h->sorted)
+            launch_cyl_move_deposit_f32_tiled(h->g, h->p32[h->cur], h->bricks, E, B, J, h->err, h->s);
+        else
+            launch_cyl_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);

@@ -17,6 +17,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "particle_math.cuh"
+#include "tile.cuh"
 
 namespace pic {
 
@@ -676,6 +677,237 @@ __device__ void deposit_pic_f(const GridP &g, float *Jx, float *Jy, float *Jz, f
     atomicAdd(Jz + cidx(g, i2 + 1, j2 + 1, k2), (Fz2 * Wx2) * Wy2);
 }
 
+// One particle of the FP32 cylindrical mover: slot n, loaded state st.
+// TILED (one CTA per brick, tile.cuh): the two gathers of the Strang step
+// read the node box when their cell is in it, and the step's current (both
+// segments in the start cell, :341) goes to the current box when the start
+// cell is in it; otherwise, and always for the near-axis sub-stepper, global
+// memory with the same arithmetic, so both forms move particles bit for
+// bit alike.  The new cell, unwrapped from the brick centre, widens bd.
+template <bool TILED>
+__device__ __forceinline__ void cyl_push_f32(const GridP &g, const CylP &cp, const PartF32 &p, uint32_t n,
+                                             const PState &st, const float *__restrict__ Ex,
+                                             const float *__restrict__ Ey, const float *__restrict__ Ez,
+                                             const float *__restrict__ Bx, const float *__restrict__ By,
+                                             const float *__restrict__ Bz, float *Jx, float *Jy, float *Jz, int *err,
+                                             const TileBox &tb, Bounds &bd)
+{
+    const float c = g.c_f, sqc = g.sqc_f, cinv = g.cinv_f, qi = g.qi_f;
+    const float inv_dtheta = (float)cp.inv_dtheta;
+    const float ymin = (float)g.ymin, ymax = (float)g.ymax, ylen = (float)g.ylen;
+    const uint32_t key = st.key;
+    const int flv = (int)(key >> kFlvShift);
+    if (flv == 0) return;  // a hole moves nowhere and deposits zero
+    int i, j, k;
+    decode_cell(g, (int)(key & kCellMask), i, j, k);
+    if (flv > PIC_MAX_FLVR || i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 || k < 3 || k > g.mz - 3) {
+        raise_error(err, PIC_DEVERR_RANGE);
+        return;
+    }
+    const float dx = st.dx, dy = st.dy, dz = st.dz;
+    const float ui = st.ux, vi = st.uy, wi = st.uz, w8 = st.w;
+    const float qm = (float)(g.qm[flv] * 0.25);  // cyl_movdep_strang.F90:100
+    int ni, nj, nk;            // new cell
+    float ox, oy, oz;          // new offsets
+    float un, vn, wn;
+    if (i > 4 || (i == 4 && dx >= 0.5f)) {
+        // Strang step away from the axis (:104-341)
+        int l0 = 0, l1 = 0, l2 = 0;   // box cell of the start cell
+        bool in1 = false;
+        if (TILED) {
+            l0 = i - tb.hc[0] - tb.lo[0];
+            l1 = unwrap_offset(j, tb.hc[1], g.ny) - tb.lo[1];
+            l2 = unwrap_offset(k, tb.hc[2], g.nz) - tb.lo[2];
+            in1 = (unsigned)l0 < (unsigned)tb.C[0] && (unsigned)l1 < (unsigned)tb.C[1] &&
+                  (unsigned)l2 < (unsigned)tb.C[2];
+        }
+        float pE[3], pB[3];
+        if (TILED && in1) {
+            float wt[8];
+            weights_f32<3>(dx, dy, dz, wt);
+            pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.f;
+            gather_box<3>(tb, l0 + tb.NX * l1 + tb.NXY * l2, wt, pE, pB);
+        } else {
+            interp3f(g, Ex, Ey, Ez, Bx, By, Bz, i, j, k, dx, dy, dz, pE, pB);
+        }
+        for (int d = 0; d < 3; d++) {
+            pE[d] *= qm;
+            pB[d] *= qm;
+        }
+        float u0 = fmaf(c, ui, pE[0]), v0 = fmaf(c, vi, pE[1]), w0 = fmaf(c, wi, pE[2]);
+        half_boris_f(sqc, pE, pB, u0, v0, w0);
+        float u1 = u0 * cinv, v1 = v0 * cinv;
+        const float gg = sqc * rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
+        const float r0 = ((float)i - 3.5f) + dx;          // x - 3 + rmin, rmin = -0.5
+        const float ddx = u1 * gg, ddy = v1 * gg;
+        const float xx1 = r0 + ddx;
+        const float r1 = sqrtf(fmaf(xx1, xx1, ddy * ddy));
+        const float dr = __fdividef(fmaf(ddx, 2.f * r0 + ddx, ddy * ddy), r1 + r0);
+        const float dth = atanf(__fdividef(ddy, xx1)) * inv_dtheta;
+        const float dzz = wi * gg;                          // z moves with this step's initial w (:202)
+        const float rinv = 1.f / r1;
+        u1 = fmaf(r0, u0, fmaf(u0 * u1, gg, v0 * ddy)) * rinv;
+        v1 = (v0 * r0) * rinv;
+        // new cell and offsets (each displacement is below one cell here)
+        const float Xn = dx + dr, Yn = dy + dth, Zn = dz + dzz;
+        const int sx = Xn >= 1.f ? 1 : (Xn < 0.f ? -1 : 0);
+        const int sy = Yn >= 1.f ? 1 : (Yn < 0.f ? -1 : 0);
+        const int sz = Zn >= 1.f ? 1 : (Zn < 0.f ? -1 : 0);
+        ni = i + sx;
+        nj = j + sy;
+        nk = k + sz;
+        ox = Xn - (float)sx;
+        oy = Yn - (float)sy;
+        oz = Zn - (float)sz;
+        bool in2 = false;
+        if (TILED)
+            in2 = (unsigned)(l0 + sx) < (unsigned)tb.C[0] && (unsigned)(l1 + sy) < (unsigned)tb.C[1] &&
+                  (unsigned)(l2 + sz) < (unsigned)tb.C[2];
+        if (TILED && in2) {
+            float wt[8];
+            weights_f32<3>(ox, oy, oz, wt);
+            pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.f;
+            gather_box<3>(tb, (l0 + sx) + tb.NX * (l1 + sy) + tb.NXY * (l2 + sz), wt, pE, pB);
+        } else {
+            interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ni, nj, nk, ox, oy, oz, pE, pB);
+        }
+        for (int d = 0; d < 3; d++) {
+            pE[d] *= qm;
+            pB[d] *= qm;
+        }
+        u0 = u1 + pE[0];
+        v0 = v1 + pE[1];
+        w0 = w0 + pE[2];
+        half_boris_f(sqc, pE, pB, u0, v0, w0);
+        un = u0 * cinv;
+        vn = v0 * cinv;
+        wn = w0 * cinv;
+        // zigzag deposit; both segments use the start cell (:341)
+        const float qthis = w8 * qi * (TILED && in1 ? tb.S : 1.f);
+        const float xr = fminf((float)(min(0, sx) + 1), fmaxf((float)max(0, sx), 0.5f * (dx + Xn)));
+        const float yr = fminf((float)(min(0, sy) + 1), fmaxf((float)max(0, sy), 0.5f * (dy + Yn)));
+        const float zr = fminf((float)(min(0, sz) + 1), fmaxf((float)max(0, sz), 0.5f * (dz + Zn)));
+        float o[12], o2[12];
+        segment<float, 3>(qthis * (xr - dx), qthis * (yr - dy), qthis * (zr - dz), 0.5f * (dx + xr),
+                          0.5f * (dy + yr), 0.5f * (dz + zr), o);
+        segment<float, 3>(qthis * (Xn - xr), qthis * (Yn - yr), qthis * (Zn - zr), 0.5f * (Xn + xr) - (float)sx,
+                          0.5f * (Yn + yr) - (float)sy, 0.5f * (Zn + zr) - (float)sz, o2);
+        for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
+        if (TILED && in1)
+            red_entries_box<3>(tb.sJ + 4u * (uint32_t)((l0 + 1) + tb.JX * (l1 + 1) + tb.JXY * (l2 + 1)), tb.jo, o);
+        else
+            scatter<float, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o);
+    } else {
+        // SubStepMovDep (:404-438) from the step's initial state: x and
+        // theta absolute (small here), z relative to the start cell
+        float pE[3], pB[3];
+        float xn = (float)i + dx, yn = (float)j + dy, zn = dz;
+        un = ui;
+        vn = vi;
+        wn = wi;
+        float t = 0.f, dt = 1.f, sx0 = xn, sy0 = yn, sz0 = zn;
+        int tries = 0;
+        while (t < 1.f) {
+            if (++tries > kMaxSubsteps) {
+                raise_error(err, PIC_DEVERR_SUBSTEP);
+                break;
+            }
+            const float delt = (t + dt > 1.f) ? 1.f - t : dt;
+            // MovePrtlAxis (:462-566)
+            {
+                float fx, fy, fz;
+                const int ci = split_coord(sx0, fx), cj = split_coord(sy0, fy), ck = k + split_coord(sz0, fz);
+                interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ci, cj, ck, fx, fy, fz, pE, pB);
+            }
+            for (int d = 0; d < 3; d++) {
+                pE[d] = (pE[d] * qm) * delt;
+                pB[d] = (pB[d] * qm) * delt;
+            }
+            float a0 = fmaf(c, un, pE[0]), b0 = fmaf(c, vn, pE[1]), c0 = fmaf(c, wn, pE[2]);
+            half_boris_f(sqc, pE, pB, a0, b0, c0);
+            float a1 = a0 * cinv, b1 = b0 * cinv;
+            const float c1 = c0 * cinv;
+            const float g2 = sqc * rsqrtf(fmaf(c0, c0, fmaf(b0, b0, fmaf(a0, a0, sqc))));
+            const float rr0 = sx0 - 3.5f;
+            const float X1 = rr0 + (a1 * g2) * delt;
+            const float Y1 = (b1 * g2) * delt;
+            const float R1 = sqrtf(fmaf(X1, X1, Y1 * Y1));
+            const float ddy = X1 > 0.f ? atanf(__fdividef(Y1, X1)) * inv_dtheta : 0.f;
+            if (fabsf(ddy) > 0.45f) {
+                dt = dt * 0.5f;
+                continue;
+            }
+            float nx;
+            if (X1 > 0.f) {
+                nx = R1 + 3.5f;
+                a1 = fmaf(rr0, a0, fmaf((a0 * a1) * g2, delt, b0 * Y1)) / R1;
+                b1 = (b0 * rr0) / R1;
+            } else {
+                nx = X1 + 3.5f;
+            }
+            const float ny = yn + ddy;
+            const float nz = zn + (c1 * g2) * delt;
+            {
+                float fx, fy, fz;
+                const int ci = split_coord(nx, fx), cj = split_coord(ny, fy), ck = k + split_coord(nz, fz);
+                interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ci, cj, ck, fx, fy, fz, pE, pB);
+            }
+            for (int d = 0; d < 3; d++) {
+                pE[d] = (pE[d] * qm) * delt;
+                pB[d] = (pB[d] * qm) * delt;
+            }
+            a0 = a1 + pE[0];
+            b0 = b1 + pE[1];
+            c0 = c0 + pE[2];
+            half_boris_f(sqc, pE, pB, a0, b0, c0);
+            xn = nx;
+            yn = ny;
+            zn = nz;
+            un = a0 * cinv;
+            vn = b0 * cinv;
+            wn = c0 * cinv;
+            t = t + delt;
+            deposit_pic_f(g, Jx, Jy, Jz, sx0, sy0, sz0, xn, yn, zn, k, w8 * qi);
+            // PrtlAxisBC (:450-460)
+            if (xn < 3.5f) {
+                xn = 3.5f + (3.5f - xn);
+                yn = yn + 0.5f * (float)g.ny;
+                un = -un;
+                vn = -vn;
+            }
+            if (yn > ymax) yn = yn - ylen;
+            if (yn < ymin) yn = yn + ylen;
+            dt = dt * 1.7f;
+            sx0 = xn;
+            sy0 = yn;
+            sz0 = zn;
+        }
+        ni = split_coord(xn, ox);
+        nj = split_coord(yn, oy);
+        nk = k + split_coord(zn, oz);
+    }
+    // periodic theta and z, particles past the outer radius leave
+    nj = wrap_index(nj, g.my);
+    nk = wrap_index(nk, g.mz);
+    uint32_t nkey = 0;
+    if (ni >= 3 && ni <= g.mx - 3) {
+        nkey = ((uint32_t)flv << kFlvShift) | (uint32_t)cidx(g, ni, nj, nk);
+        if (TILED) {
+            const int u0 = ni - tb.hc[0], u1 = unwrap_offset(nj, tb.hc[1], g.ny), u2 = unwrap_offset(nk, tb.hc[2], g.nz);
+            bd.lo[0] = min(bd.lo[0], u0); bd.hi[0] = max(bd.hi[0], u0);
+            bd.lo[1] = min(bd.lo[1], u1); bd.hi[1] = max(bd.hi[1], u1);
+            bd.lo[2] = min(bd.lo[2], u2); bd.hi[2] = max(bd.hi[2], u2);
+        }
+    }
+    p.key[n] = nkey;
+    p.dx[n] = ox;
+    p.dy[n] = oy;
+    p.dz[n] = oz;
+    p.ux[n] = un;
+    p.uy[n] = vn;
+    p.uz[n] = wn;
+}
+
 __global__ void __launch_bounds__(kThreads) k_cyl_move_f32(GridP g, CylP cp, PartF32 p, const Counters *__restrict__ cnt,
                                                            const float *__restrict__ Ex, const float *__restrict__ Ey,
                                                            const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -683,184 +915,47 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move_f32(GridP g, CylP cp, Par
                                                            float *Jx, float *Jy, float *Jz, int *err)
 {
     const long long used = cnt->used;
-    const float c = g.c_f, sqc = g.sqc_f, cinv = g.cinv_f, qi = g.qi_f;
-    const float inv_dtheta = (float)cp.inv_dtheta;
-    const float ymin = (float)g.ymin, ymax = (float)g.ymax, ylen = (float)g.ylen;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
-        const uint32_t key = p.key[n];
-        const int flv = (int)(key >> kFlvShift);
-        if (flv == 0) continue;  // a hole moves nowhere and deposits zero
-        int i, j, k;
-        decode_cell(g, (int)(key & kCellMask), i, j, k);
-        if (flv > PIC_MAX_FLVR || i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 || k < 3 || k > g.mz - 3) {
-            raise_error(err, PIC_DEVERR_RANGE);
-            continue;
+    const TileBox tb = {};
+    Bounds bd;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x)
+        cyl_push_f32<false>(g, cp, p, (uint32_t)n, load_state<3>(p, (uint32_t)n), Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz,
+                            err, tb, bd);
+}
+
+// Tiled form: one CTA per brick (after a reorder).  The box is the stored
+// bounds of the brick's particles widened by one cell (the second gather is
+// at the cell a particle moves to); the radius is not periodic.  Each thread
+// loads its next particle while it moves this one.
+__global__ void __launch_bounds__(kTileThreads, 2)
+    k_cyl_move_f32_tiled(GridP g, CylP cp, PartF32 p, Bricks bk, const float *__restrict__ Ex,
+                         const float *__restrict__ Ey, const float *__restrict__ Ez, const float *__restrict__ Bx,
+                         const float *__restrict__ By, const float *__restrict__ Bz, float *Jx, float *Jy, float *Jz,
+                         int *err)
+{
+    extern __shared__ __align__(16) float sm[];
+    __shared__ TileShared ts;
+    const int b = blockIdx.x;
+    const uint32_t p0 = bk.tile_start[b], p1 = bk.tile_start[b + 1];
+    if (p0 >= p1) return;
+    TileBox tb;
+    int home_lo[3], home_hi[3];
+    brick_home<3>(g, bk, b, tb, home_lo, home_hi);
+    // a Strang move is below one cell per axis, a sub-stepped one below two
+    tile_setup<3, false>(g, bk, b, p1 - p0, 1, 2.f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By, Bz);
+    Bounds bd;
+    bd.init();
+    const uint32_t n0 = p0 + threadIdx.x;
+    if (n0 < p1) {
+        PState cur = load_state<3>(p, n0);
+        for (uint32_t n = n0; n < p1; n += kTileThreads) {
+            PState nxt = cur;
+            if (p1 - n > kTileThreads) nxt = load_state<3>(p, n + kTileThreads);
+            cyl_push_f32<true>(g, cp, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+            cur = nxt;
         }
-        const float dx = p.dx[n], dy = p.dy[n], dz = p.dz[n];
-        const float ui = p.ux[n], vi = p.uy[n], wi = p.uz[n], w8 = p.w[n];
-        const float qm = (float)(g.qm[flv] * 0.25);  // cyl_movdep_strang.F90:100
-        int ni, nj, nk;            // new cell
-        float ox, oy, oz;          // new offsets
-        float un, vn, wn;
-        if (i > 4 || (i == 4 && dx >= 0.5f)) {
-            // Strang step away from the axis (:104-341)
-            float pE[3], pB[3];
-            interp3f(g, Ex, Ey, Ez, Bx, By, Bz, i, j, k, dx, dy, dz, pE, pB);
-            for (int d = 0; d < 3; d++) {
-                pE[d] *= qm;
-                pB[d] *= qm;
-            }
-            float u0 = fmaf(c, ui, pE[0]), v0 = fmaf(c, vi, pE[1]), w0 = fmaf(c, wi, pE[2]);
-            half_boris_f(sqc, pE, pB, u0, v0, w0);
-            float u1 = u0 * cinv, v1 = v0 * cinv;
-            const float gg = sqc * rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
-            const float r0 = ((float)i - 3.5f) + dx;          // x - 3 + rmin, rmin = -0.5
-            const float ddx = u1 * gg, ddy = v1 * gg;
-            const float xx1 = r0 + ddx;
-            const float r1 = sqrtf(fmaf(xx1, xx1, ddy * ddy));
-            const float dr = __fdividef(fmaf(ddx, 2.f * r0 + ddx, ddy * ddy), r1 + r0);
-            const float dth = atanf(__fdividef(ddy, xx1)) * inv_dtheta;
-            const float dzz = wi * gg;                          // z moves with this step's initial w (:202)
-            const float rinv = 1.f / r1;
-            u1 = fmaf(r0, u0, fmaf(u0 * u1, gg, v0 * ddy)) * rinv;
-            v1 = (v0 * r0) * rinv;
-            // new cell and offsets (each displacement is below one cell here)
-            const float Xn = dx + dr, Yn = dy + dth, Zn = dz + dzz;
-            const int sx = Xn >= 1.f ? 1 : (Xn < 0.f ? -1 : 0);
-            const int sy = Yn >= 1.f ? 1 : (Yn < 0.f ? -1 : 0);
-            const int sz = Zn >= 1.f ? 1 : (Zn < 0.f ? -1 : 0);
-            ni = i + sx;
-            nj = j + sy;
-            nk = k + sz;
-            ox = Xn - (float)sx;
-            oy = Yn - (float)sy;
-            oz = Zn - (float)sz;
-            interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ni, nj, nk, ox, oy, oz, pE, pB);
-            for (int d = 0; d < 3; d++) {
-                pE[d] *= qm;
-                pB[d] *= qm;
-            }
-            u0 = u1 + pE[0];
-            v0 = v1 + pE[1];
-            w0 = w0 + pE[2];
-            half_boris_f(sqc, pE, pB, u0, v0, w0);
-            un = u0 * cinv;
-            vn = v0 * cinv;
-            wn = w0 * cinv;
-            // zigzag deposit; both segments use the start cell (:341)
-            const float qthis = w8 * qi;
-            const float xr = fminf((float)(min(0, sx) + 1), fmaxf((float)max(0, sx), 0.5f * (dx + Xn)));
-            const float yr = fminf((float)(min(0, sy) + 1), fmaxf((float)max(0, sy), 0.5f * (dy + Yn)));
-            const float zr = fminf((float)(min(0, sz) + 1), fmaxf((float)max(0, sz), 0.5f * (dz + Zn)));
-            float o[12], o2[12];
-            segment<float, 3>(qthis * (xr - dx), qthis * (yr - dy), qthis * (zr - dz), 0.5f * (dx + xr),
-                              0.5f * (dy + yr), 0.5f * (dz + zr), o);
-            segment<float, 3>(qthis * (Xn - xr), qthis * (Yn - yr), qthis * (Zn - zr), 0.5f * (Xn + xr) - (float)sx,
-                              0.5f * (Yn + yr) - (float)sy, 0.5f * (Zn + zr) - (float)sz, o2);
-            for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
-            scatter<float, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o);
-        } else {
-            // SubStepMovDep (:404-438) from the step's initial state: x and
-            // theta absolute (small here), z relative to the start cell
-            float pE[3], pB[3];
-            float xn = (float)i + dx, yn = (float)j + dy, zn = dz;
-            un = ui;
-            vn = vi;
-            wn = wi;
-            float t = 0.f, dt = 1.f, sx0 = xn, sy0 = yn, sz0 = zn;
-            int tries = 0;
-            while (t < 1.f) {
-                if (++tries > kMaxSubsteps) {
-                    raise_error(err, PIC_DEVERR_SUBSTEP);
-                    break;
-                }
-                const float delt = (t + dt > 1.f) ? 1.f - t : dt;
-                // MovePrtlAxis (:462-566)
-                {
-                    float fx, fy, fz;
-                    const int ci = split_coord(sx0, fx), cj = split_coord(sy0, fy), ck = k + split_coord(sz0, fz);
-                    interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ci, cj, ck, fx, fy, fz, pE, pB);
-                }
-                for (int d = 0; d < 3; d++) {
-                    pE[d] = (pE[d] * qm) * delt;
-                    pB[d] = (pB[d] * qm) * delt;
-                }
-                float a0 = fmaf(c, un, pE[0]), b0 = fmaf(c, vn, pE[1]), c0 = fmaf(c, wn, pE[2]);
-                half_boris_f(sqc, pE, pB, a0, b0, c0);
-                float a1 = a0 * cinv, b1 = b0 * cinv;
-                const float c1 = c0 * cinv;
-                const float g2 = sqc * rsqrtf(fmaf(c0, c0, fmaf(b0, b0, fmaf(a0, a0, sqc))));
-                const float rr0 = sx0 - 3.5f;
-                const float X1 = rr0 + (a1 * g2) * delt;
-                const float Y1 = (b1 * g2) * delt;
-                const float R1 = sqrtf(fmaf(X1, X1, Y1 * Y1));
-                const float ddy = X1 > 0.f ? atanf(__fdividef(Y1, X1)) * inv_dtheta : 0.f;
-                if (fabsf(ddy) > 0.45f) {
-                    dt = dt * 0.5f;
-                    continue;
-                }
-                float nx;
-                if (X1 > 0.f) {
-                    nx = R1 + 3.5f;
-                    a1 = fmaf(rr0, a0, fmaf((a0 * a1) * g2, delt, b0 * Y1)) / R1;
-                    b1 = (b0 * rr0) / R1;
-                } else {
-                    nx = X1 + 3.5f;
-                }
-                const float ny = yn + ddy;
-                const float nz = zn + (c1 * g2) * delt;
-                {
-                    float fx, fy, fz;
-                    const int ci = split_coord(nx, fx), cj = split_coord(ny, fy), ck = k + split_coord(nz, fz);
-                    interp3f(g, Ex, Ey, Ez, Bx, By, Bz, ci, cj, ck, fx, fy, fz, pE, pB);
-                }
-                for (int d = 0; d < 3; d++) {
-                    pE[d] = (pE[d] * qm) * delt;
-                    pB[d] = (pB[d] * qm) * delt;
-                }
-                a0 = a1 + pE[0];
-                b0 = b1 + pE[1];
-                c0 = c0 + pE[2];
-                half_boris_f(sqc, pE, pB, a0, b0, c0);
-                xn = nx;
-                yn = ny;
-                zn = nz;
-                un = a0 * cinv;
-                vn = b0 * cinv;
-                wn = c0 * cinv;
-                t = t + delt;
-                deposit_pic_f(g, Jx, Jy, Jz, sx0, sy0, sz0, xn, yn, zn, k, w8 * qi);
-                // PrtlAxisBC (:450-460)
-                if (xn < 3.5f) {
-                    xn = 3.5f + (3.5f - xn);
-                    yn = yn + 0.5f * (float)g.ny;
-                    un = -un;
-                    vn = -vn;
-                }
-                if (yn > ymax) yn = yn - ylen;
-                if (yn < ymin) yn = yn + ylen;
-                dt = dt * 1.7f;
-                sx0 = xn;
-                sy0 = yn;
-                sz0 = zn;
-            }
-            ni = split_coord(xn, ox);
-            nj = split_coord(yn, oy);
-            nk = k + split_coord(zn, oz);
-        }
-        // periodic theta and z, particles past the outer radius leave
-        nj = wrap_index(nj, g.my);
-        nk = wrap_index(nk, g.mz);
-        uint32_t nkey = 0;
-        if (ni >= 3 && ni <= g.mx - 3) nkey = ((uint32_t)flv << kFlvShift) | (uint32_t)cidx(g, ni, nj, nk);
-        p.key[n] = nkey;
-        p.dx[n] = ox;
-        p.dy[n] = oy;
-        p.dz[n] = oz;
-        p.ux[n] = un;
-        p.uy[n] = vn;
-        p.uz[n] = wn;
     }
+    __syncthreads();
+    tile_finish<3, false>(g, bk, b, tb, sm, ts, bd, home_lo, home_hi, Jx, Jy, Jz);
 }
 
 void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
@@ -869,6 +964,21 @@ void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counter
     const CylP cp = cyl_params(g);
     k_cyl_move_f32<<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
                                                  err);
+    k_cyl_axis_current<float><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
+    count_launches(2);
+}
+
+void launch_cyl_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
+                                       float *const B[3], float *const J[3], int *err, cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_cyl_move_f32_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        attr_set = true;
+    }
+    const CylP cp = cyl_params(g);
+    k_cyl_move_f32_tiled<<<bk.ntiles, kTileThreads, bk.smem_floats * 4, s>>>(g, cp, p, bk, E[0], E[1], E[2], B[0],
+                                                                            B[1], B[2], J[0], J[1], J[2], err);
     k_cyl_axis_current<float><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
     count_launches(2);
 }

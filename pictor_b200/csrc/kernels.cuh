@@ -109,6 +109,9 @@ void launch_batch_move(int dims, const BatchRun *runs, const int *mstart, int n,
 void launch_batch_flip(BatchRun *runs, int r, cudaStream_t s);
 void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
                                    float *const B[3], float *const J[3], int *err, cudaStream_t s);
+// cyl.cu: tiled FP32 cylindrical mover, one CTA per brick (+ the axis current)
+void launch_cyl_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
+                                       float *const B[3], float *const J[3], int *err, cudaStream_t s);
 
 // particles.cu
 struct SortScratch {

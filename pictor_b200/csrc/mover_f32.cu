@@ -45,58 +45,9 @@
 // order of the FP32 sums and the fixed-point rounding of the box.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tile.cuh"
 
 namespace pic {
-
-// Node-averaged fields at node offset nd (GatherVecEfld / GatherVecBfld,
-// movdep_routines.F90:6-223): E averaged over the 2 edges, B over the 4 faces
-// meeting at the node (2 in 2D), plus the external field.
-template <int DIMS>
-__device__ __forceinline__ void node_avg(const float *__restrict__ Ex, const float *__restrict__ Ey,
-                                         const float *__restrict__ Ez, const float *__restrict__ Bx,
-                                         const float *__restrict__ By, const float *__restrict__ Bz, int nd, int sy,
-                                         int sz, float b0, float b1, float b2, float4 &A, float2 &Bv)
-{
-    A.x = (__ldg(Ex + nd - 1) + __ldg(Ex + nd)) * 0.5f;
-    A.y = (__ldg(Ey + nd - sy) + __ldg(Ey + nd)) * 0.5f;
-    if (DIMS == 3) {
-        A.z = (__ldg(Ez + nd - sz) + __ldg(Ez + nd)) * 0.5f;
-        A.w = (((__ldg(Bx + nd - sy - sz) + __ldg(Bx + nd - sz)) + __ldg(Bx + nd - sy)) + __ldg(Bx + nd)) * 0.25f + b0;
-        Bv.x = (((__ldg(By + nd - 1 - sz) + __ldg(By + nd - 1)) + __ldg(By + nd - sz)) + __ldg(By + nd)) * 0.25f + b1;
-    } else {
-        A.z = __ldg(Ez + nd);
-        A.w = (__ldg(Bx + nd - sy) + __ldg(Bx + nd)) * 0.5f + b0;
-        Bv.x = (__ldg(By + nd - 1) + __ldg(By + nd)) * 0.5f + b1;
-    }
-    Bv.y = (((__ldg(Bz + nd - 1 - sy) + __ldg(Bz + nd - 1)) + __ldg(Bz + nd - sy)) + __ldg(Bz + nd)) * 0.25f + b2;
-}
-
-__device__ __forceinline__ void accum(float w, const float4 &A, const float2 &Bv, float pE[3], float pB[3])
-{
-    pE[0] = fmaf(w, A.x, pE[0]);
-    pE[1] = fmaf(w, A.y, pE[1]);
-    pE[2] = fmaf(w, A.z, pE[2]);
-    pB[0] = fmaf(w, A.w, pB[0]);
-    pB[1] = fmaf(w, Bv.x, pB[1]);
-    pB[2] = fmaf(w, Bv.y, pB[2]);
-}
-
-// Interpolation weights of the 4 / 8 corners (corner bit 0 = x, 1 = y, 2 = z).
-template <int DIMS>
-__device__ __forceinline__ void weights_f32(float dx, float dy, float dz, float wt[8])
-{
-    const float wx[2] = {1.f - dx, dx}, wy[2] = {1.f - dy, dy};
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-        const float xy = wx[c & 1] * wy[c >> 1];
-        if (DIMS == 3) {
-            wt[c] = xy * (1.f - dz);
-            wt[c + 4] = xy * dz;
-        } else {
-            wt[c] = xy;
-        }
-    }
-}
 
 // Relativistic Boris rotation (movdep.F90:143-167) in FP32 with hardware
 // reciprocal square root.  On entry u,v,w = gamma v / c and pE, pB are
@@ -120,31 +71,6 @@ __device__ __forceinline__ void boris_f32(float c, float sqc, float cinv, const 
     v = v0 * cinv;
     w = w0 * cinv;
     gout = sqc * rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
-}
-
-// Shared-memory accesses with explicit .shared addressing (32-bit shared
-// addresses), so no generic-address resolution is left to run time.
-__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-template <int OFF>
-__device__ __forceinline__ float4 lds4i(uint32_t a)
-{
-    float4 v;
-    asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4+%5];"
-                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
-                 : "r"(a), "n"(OFF));
-    return v;
-}
-template <int OFF>
-__device__ __forceinline__ float2 lds2i(uint32_t a)
-{
-    float2 v;
-    asm volatile("ld.shared.v2.f32 {%0, %1}, [%2+%3];" : "=f"(v.x), "=f"(v.y) : "r"(a), "n"(OFF));
-    return v;
-}
-template <int OFF>
-__device__ __forceinline__ void red_shared_i(uint32_t a, int v)
-{
-    asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a), "n"(OFF), "r"(v));
 }
 
 // Cell step of a position x in (-1, 2) relative to its cell: floor(x) as
@@ -279,20 +205,6 @@ __device__ __forceinline__ void deposit_part_global(float *Jx, float *Jy, float 
     }
 }
 
-// Shared byte offsets of the current box: component planes and the y / z
-// strides (the x stride is 4 bytes, an immediate).
-struct JOff {
-    uint32_t cy, cz;      // Jy, Jz plane - Jx plane
-    uint32_t y, z, yz;    // 4 JX, 4 JXY, 4 (JX + JXY)
-};
-
-// round(v) for |v| <= 2^22, v already scaled by the box's fixed-point scale:
-// adding 1.5 * 2^23 leaves the rounded integer in the low mantissa bits.
-__device__ __forceinline__ int fixed_round(float v)
-{
-    return __float_as_int(v + 12582912.f) - 0x4B400000;
-}
-
 // A part into the shared current box at byte address a (cell j's Jx word),
 // F already scaled by the fixed-point scale S.
 template <int DIMS, bool CROSS = true>
@@ -300,102 +212,7 @@ __device__ __forceinline__ void deposit_part_box(uint32_t a, const JOff &o, cons
 {
     float v[12];
     part_entries<DIMS, CROSS>(d, v);
-    if (DIMS == 3) {
-        red_shared_i<0>(a, fixed_round(v[0]));
-        red_shared_i<0>(a + o.y, fixed_round(v[1]));
-        red_shared_i<0>(a + o.z, fixed_round(v[2]));
-        red_shared_i<0>(a + o.yz, fixed_round(v[3]));
-        const uint32_t b = a + o.cy;
-        red_shared_i<0>(b, fixed_round(v[4]));
-        red_shared_i<4>(b, fixed_round(v[5]));
-        const uint32_t bz = b + o.z;
-        red_shared_i<0>(bz, fixed_round(v[6]));
-        red_shared_i<4>(bz, fixed_round(v[7]));
-        const uint32_t c = a + o.cz;
-        red_shared_i<0>(c, fixed_round(v[8]));
-        red_shared_i<4>(c, fixed_round(v[9]));
-        const uint32_t cy = c + o.y;
-        red_shared_i<0>(cy, fixed_round(v[10]));
-        red_shared_i<4>(cy, fixed_round(v[11]));
-    } else {
-        red_shared_i<0>(a, fixed_round(v[0]));
-        red_shared_i<0>(a + o.y, fixed_round(v[1]));
-        const uint32_t b = a + o.cy;
-        red_shared_i<0>(b, fixed_round(v[2]));
-        red_shared_i<4>(b, fixed_round(v[3]));
-        const uint32_t c = a + o.cz;
-        red_shared_i<0>(c, fixed_round(v[4]));
-        red_shared_i<4>(c, fixed_round(v[5]));
-        const uint32_t cy = c + o.y;
-        red_shared_i<0>(cy, fixed_round(v[6]));
-        red_shared_i<4>(cy, fixed_round(v[7]));
-    }
-}
-
-// Interior index 3..n+2 of a periodic (unwrapped) 1-based index a.
-__device__ __forceinline__ int wrap_interior(int a, int n)
-{
-    int t = (a - 3) % n;
-    if (t < 0) t += n;
-    return 3 + t;
-}
-
-// Unwrapped offset of interior index i from centre hc on a periodic axis of
-// n cells: the representative of (i - hc) mod n in [-n/2, n - n/2).
-__device__ __forceinline__ int unwrap_offset(int i, int hc, int n)
-{
-    int u = i - hc;
-    const int half = n >> 1;
-    if (u >= n - half) u -= n;
-    else if (u < -half) u += n;
-    return u;
-}
-
-// Shared-memory boxes of a brick (unused by the per-particle kernel).
-struct TileBox {
-    uint32_t nA, nB;    // shared addresses: node E x,y,z, B x (16 B) / node B y,z (8 B)
-    uint32_t sJ;        // shared address of the current box (3 planar components, fixed point)
-    int hc[3];          // brick centre (1-based interior indices)
-    int lo[3];          // box lower corner, cells relative to hc
-    int C[3];           // box extent in cells (1 on the unused z axis of 2D)
-    int NX, NXY;        // node box strides
-    int JX, JXY, njc;   // current box strides and size
-    uint32_t oY4, oZ4;  // node-box byte strides of the 16-byte nodes (8-byte nodes: half)
-    JOff jo;            // current-box byte offsets
-    float S;            // fixed-point scale of the current box
-};
-
-// Running bounds of the particles' new cells (relative to the brick centre).
-struct Bounds {
-    int lo[3], hi[3];
-    __device__ void init()
-    {
-        for (int d = 0; d < 3; d++) {
-            lo[d] = 0x3fffffff;
-            hi[d] = -0x3fffffff;
-        }
-    }
-};
-
-// One particle's state in registers.
-struct PState {
-    uint32_t key;
-    float dx, dy, dz, ux, uy, uz, w;
-};
-
-template <int DIMS>
-__device__ __forceinline__ PState load_state(const PartF32 &p, uint32_t n)
-{
-    PState s;
-    s.key = p.key[n];
-    s.dx = p.dx[n];
-    s.dy = p.dy[n];
-    s.dz = DIMS == 3 ? p.dz[n] : 0.f;
-    s.ux = p.ux[n];
-    s.uy = p.uy[n];
-    s.uz = p.uz[n];
-    s.w = p.w[n];
-    return s;
+    red_entries_box<DIMS>(a, o, v);
 }
 
 // Move one particle (state s, slot n).  TILED: gather through the node box
@@ -443,21 +260,7 @@ __device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint3
     }
     float pE[3] = {0.f, 0.f, 0.f}, pB[3] = {0.f, 0.f, 0.f};
     if (inside) {
-        // corner rows (y, z) by register offsets, the x neighbour by an immediate
-        const uint32_t a0 = tb.nA + 16u * (uint32_t)nb, b0 = tb.nB + 8u * (uint32_t)nb;
-        const uint32_t a1 = a0 + tb.oY4, b1 = b0 + (tb.oY4 >> 1);
-        accum(wt[0], lds4i<0>(a0), lds2i<0>(b0), pE, pB);
-        accum(wt[1], lds4i<16>(a0), lds2i<8>(b0), pE, pB);
-        accum(wt[2], lds4i<0>(a1), lds2i<0>(b1), pE, pB);
-        accum(wt[3], lds4i<16>(a1), lds2i<8>(b1), pE, pB);
-        if (DIMS == 3) {
-            const uint32_t a2 = a0 + tb.oZ4, b2 = b0 + (tb.oZ4 >> 1);
-            const uint32_t a3 = a1 + tb.oZ4, b3 = b1 + (tb.oZ4 >> 1);
-            accum(wt[4], lds4i<0>(a2), lds2i<0>(b2), pE, pB);
-            accum(wt[5], lds4i<16>(a2), lds2i<8>(b2), pE, pB);
-            accum(wt[6], lds4i<0>(a3), lds2i<0>(b3), pE, pB);
-            accum(wt[7], lds4i<16>(a3), lds2i<8>(b3), pE, pB);
-        }
+        gather_box<DIMS>(tb, nb, wt, pE, pB);
     } else {
 #pragma unroll
         for (int c8 = 0; c8 < (DIMS == 3 ? 8 : 4); c8++) {
@@ -575,13 +378,6 @@ __device__ __forceinline__ void push_range(const GridP &g, const PartF32 &p, uin
     }
 }
 
-constexpr int kTileThreads = 256;
-constexpr int kTileWarps = kTileThreads / 32;
-
-// Second zigzag segments queued by the lanes of one warp (structure of
-// arrays: F x, y, z, W x, y, z, box address; 32 entries each).
-constexpr int kQueueRows = 7;
-
 __device__ __forceinline__ uint32_t lanemask_lt()
 {
     uint32_t m;
@@ -697,24 +493,6 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // Tiled form: one CTA per brick.
 // ---------------------------------------------------------------------------
 
-// Interior index of the unwrapped 1-based index a (no division when a is
-// already interior or one period away).
-__device__ __forceinline__ int interior_of(int a, int n)
-{
-    if (a < 3) a += n;
-    else if (a > n + 2) a -= n;
-    if (a < 3 || a > n + 2) a = wrap_interior(a, n);
-    return a;
-}
-
-// Static shared memory of one brick's move (the node and current boxes are
-// the dynamic part, sm).
-struct TileShared {
-    int red[kTileWarps][6];
-    int s_off[3][kBoxAxisMax + 3];
-    float s_q[kTileWarps][kQueueRows][32];
-};
-
 // Move the particles of brick b (one CTA).
 template <int DIMS>
 __device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, const Bricks &bk, int b, float *sm,
@@ -725,152 +503,16 @@ __device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, con
 {
     const uint32_t p0 = bk.tile_start[b], p1 = bk.tile_start[b + 1];
     if (p0 >= p1) return;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // brick centre and home extent
-    const int bx = b % bk.nb[0], byz = b / bk.nb[0], by = byz % bk.nb[1], bz = byz / bk.nb[1];
-    const int n3[3] = {g.nx, g.ny, g.nz};
-    const int bi[3] = {bx, by, bz};
     TileBox tb;
     int home_lo[3], home_hi[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        const int lo = 3 + bi[d] * bk.t[d];
-        const int hi = min(lo + bk.t[d] - 1, n3[d] + 2);
-        tb.hc[d] = lo + (bk.t[d] >> 1);
-        home_lo[d] = lo - tb.hc[d];
-        home_hi[d] = hi - tb.hc[d];
-    }
-    if (DIMS == 2) {
-        tb.hc[2] = 1;
-        home_lo[2] = home_hi[2] = 0;
-    }
-    // box of this step: the stored bounds, or the brick +- 1 cell if too large
-    const int *sb = bk.box + 8 * (size_t)b;
-    int lo[3] = {sb[0], sb[1], DIMS == 3 ? sb[2] : 0}, hi[3] = {sb[3], sb[4], DIMS == 3 ? sb[5] : 0};
-    if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2] || hi[0] - lo[0] >= kBoxAxisMax ||
-        hi[1] - lo[1] >= kBoxAxisMax || hi[2] - lo[2] >= kBoxAxisMax ||
-        box_floats(DIMS, hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1) > bk.smem_floats) {
-#pragma unroll
-        for (int d = 0; d < DIMS; d++) {
-            lo[d] = home_lo[d] - 1;
-            hi[d] = home_hi[d] + 1;
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        tb.lo[d] = lo[d];
-        tb.C[d] = hi[d] - lo[d] + 1;
-    }
-    const int NX = tb.C[0] + 1, NY = tb.C[1] + 1, NZ = DIMS == 3 ? tb.C[2] + 1 : 1;
-    const int JX = tb.C[0] + 3, JY = tb.C[1] + 3, JZ = DIMS == 3 ? tb.C[2] + 3 : 1;
-    const int nnode = NX * NY * NZ;
-    tb.NX = NX;
-    tb.NXY = NX * NY;
-    tb.JX = JX;
-    tb.JXY = JX * JY;
-    tb.njc = JX * JY * JZ;
-    tb.oY4 = 16u * (uint32_t)NX;
-    tb.oZ4 = 16u * (uint32_t)(NX * NY);
-    tb.jo.cy = 4u * (uint32_t)tb.njc;
-    tb.jo.cz = 8u * (uint32_t)tb.njc;
-    tb.jo.y = 4u * (uint32_t)JX;
-    tb.jo.z = 4u * (uint32_t)tb.JXY;
-    tb.jo.yz = tb.jo.y + tb.jo.z;
-    float4 *nA = reinterpret_cast<float4 *>(sm);
-    float2 *nB = reinterpret_cast<float2 *>(sm + 4 * nnode);
-    int *sJ = reinterpret_cast<int *>(sm + 6 * nnode);
-    tb.nA = smem_addr(nA);
-    tb.nB = smem_addr(nB);
-    tb.sJ = smem_addr(sJ);
-    // fixed-point scale: a particle adds at most b = |w| qi c to any entry
-    // (its displacement per axis is below c), so with S = 2^30 / (N b) no sum
-    // of the N particles exceeds 2^30; S <= 2^22 / b keeps each contribution
-    // below 2^22 (the range of fixed_round)
-    {
-        const float b1 = g.c_f * g.qi_f * __uint_as_float(*bk.wmax_bits);
-        const float n = fmaxf((float)(p1 - p0), 256.f);
-        tb.S = b1 > 0.f ? 1073741824.f / (b1 * n) : 1.f;
-    }
-    // periodic offsets of the box cells lo-1 .. lo+C+1 along each axis
-    // (memory offset of the interior image, times the axis stride)
-    {
-        const int ext[3] = {JX, JY, JZ};
-        const int str[3] = {1, (int)g.sy, (int)g.sz};
-#pragma unroll
-        for (int d = 0; d < DIMS; d++)
-            for (int t = tid; t < ext[d]; t += kTileThreads)
-                ts.s_off[d][t] = (interior_of(tb.hc[d] + lo[d] - 1 + t, n3[d]) - 1) * str[d];
-        if (DIMS == 2 && tid == 0) ts.s_off[2][0] = 0;
-    }
-    for (int q = tid; q < 3 * tb.njc; q += kTileThreads) sJ[q] = 0;
-    __syncthreads();
-    // stage node-averaged fields: node q = xx + NX*(yy + NY*zz); q/NX and
-    // r/NY by multiply-high (exact for q < 2^16, NX, NY < 2^16)
-    {
-        const int sy = (int)g.sy, sz = (int)g.sz;
-        const uint32_t mX = 0xffffffffu / (uint32_t)NX + 1u, mY = 0xffffffffu / (uint32_t)NY + 1u;
-        for (int q = tid; q < nnode; q += kTileThreads) {
-            const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * NX;
-            const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * NY;
-            const int nd = ts.s_off[0][xx + 1] + ts.s_off[1][yy + 1] + (DIMS == 3 ? ts.s_off[2][zz + 1] : 0);
-            float4 A;
-            float2 Bv;
-            node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
-            nA[q] = A;
-            nB[q] = Bv;
-        }
-    }
-    __syncthreads();
-
+    brick_home<DIMS>(g, bk, b, tb, home_lo, home_hi);
+    // a move is below c per axis; the box is the stored bounds (no margin)
+    tile_setup<DIMS, true>(g, bk, b, p1 - p0, 0, g.c_f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By, Bz);
     Bounds bd;
     bd.init();
-    push_range_tiled<DIMS>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, ts.s_q[warp]);
+    push_range_tiled<DIMS>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, ts.s_q[threadIdx.x >> 5]);
     __syncthreads();
-
-    // add the box current to the periodic interior image of each cell
-    {
-        const float inv = 1.f / tb.S;
-        const uint32_t mX = 0xffffffffu / (uint32_t)JX + 1u, mY = 0xffffffffu / (uint32_t)JY + 1u;
-        for (int q = tid; q < tb.njc; q += kTileThreads) {
-            const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * JX;
-            const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * JY;
-            const int off = ts.s_off[0][xx] + ts.s_off[1][yy] + (DIMS == 3 ? ts.s_off[2][zz] : 0);
-            const int vx = sJ[q], vy = sJ[tb.njc + q], vz = sJ[2 * tb.njc + q];
-            if (vx != 0) atomicAdd(Jx + off, (float)vx * inv);
-            if (vy != 0) atomicAdd(Jy + off, (float)vy * inv);
-            if (vz != 0) atomicAdd(Jz + off, (float)vz * inv);
-        }
-    }
-
-    // bounds of the new cells -> box of the next step (the brick itself if empty)
-    int v[6] = {bd.lo[0], bd.lo[1], bd.lo[2], -bd.hi[0], -bd.hi[1], -bd.hi[2]};
-#pragma unroll
-    for (int e = 0; e < 6; e++) v[e] = __reduce_min_sync(0xffffffffu, v[e]);
-    if (lane == 0)
-#pragma unroll
-        for (int e = 0; e < 6; e++) ts.red[warp][e] = v[e];
-    __syncthreads();
-    if (tid == 0) {
-        int m[6];
-        for (int e = 0; e < 6; e++) {
-            m[e] = ts.red[0][e];
-            for (int w2 = 1; w2 < kTileWarps; w2++) m[e] = min(m[e], ts.red[w2][e]);
-        }
-        int *ob = bk.box + 8 * (size_t)b;
-        const bool empty = m[0] == 0x3fffffff;
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            if (d >= DIMS) {
-                ob[d] = ob[d + 3] = 0;
-            } else if (empty) {
-                ob[d] = home_lo[d];
-                ob[d + 3] = home_hi[d];
-            } else {
-                ob[d] = m[d];
-                ob[d + 3] = -m[d + 3];
-            }
-        }
-    }
+    tile_finish<DIMS, true>(g, bk, b, tb, sm, ts, bd, home_lo, home_hi, Jx, Jy, Jz);
 }
 
 template <int DIMS>
