@@ -68,6 +68,8 @@ WORKLOADS = {
     "cyl_wake_small_modal_fp32": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp32",
                                       thermal=0.01, bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0,
                                       bunch_sigma_z=10.0, cyl_modes=2),
+    "cyl_wake_small_fp32": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp32",
+                                thermal=0.01, bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0, bunch_sigma_z=10.0),
     "cyl_wake_small": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp64", thermal=0.01,
                            bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0, bunch_sigma_z=10.0),
 }

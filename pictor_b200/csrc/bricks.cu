@@ -350,7 +350,8 @@ bool choose_bricks(const GridP &g, double ppc, const int req[3], Bricks &bk)
     for (int d = 0; d < g.dims; d++)
         if (bk.t[d] + 2 > kBoxAxisMax) return false;
     if ((long long)bk.t[0] * bk.t[1] * bk.t[2] * 4 > 32 * 1024) return false;
-    return box_floats(g.dims, bk.t[0] + 2, bk.t[1] + 2, g.dims == 3 ? bk.t[2] + 2 : 1) <= bk.smem_floats;
+    return box_floats(g.dims, bk.t[0] + 2, bk.t[1] + 2, g.dims == 3 ? bk.t[2] + 2 : 1, box_current_words(g)) <=
+           bk.smem_floats;
 }
 
 }  // namespace pic

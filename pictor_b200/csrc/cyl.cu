@@ -677,20 +677,32 @@ __device__ void deposit_pic_f(const GridP &g, float *Jx, float *Jy, float *Jz, f
     atomicAdd(Jz + cidx(g, i2 + 1, j2 + 1, k2), (Fz2 * Wx2) * Wy2);
 }
 
+// The box current of a thread's consecutive particles that start in the same
+// cell, summed in registers (FP32, in the box's fixed-point units) and added
+// to the 64-bit box when the cell changes: a thread of the tiled mover walks
+// one row of its brick, which the reorder fills with the particles of one or
+// two cells.
+constexpr uint32_t kNoCell = 0xffffffffu;
+struct JAcc {
+    float v[12];
+    uint32_t a;   // box byte address of the cell's Jx word, or kNoCell
+};
+
 // One particle of the FP32 cylindrical mover: slot n, loaded state st.
 // TILED (one CTA per brick, tile.cuh): the two gathers of the Strang step
 // read the node box when their cell is in it, and the step's current (both
-// segments in the start cell, :341) goes to the current box when the start
-// cell is in it; otherwise, and always for the near-axis sub-stepper, global
-// memory with the same arithmetic, so both forms move particles bit for
-// bit alike.  The new cell, unwrapped from the brick centre, widens bd.
+// segments in the start cell, :341) goes to the box (through acc) when the
+// start cell is in it; otherwise, and always for the near-axis sub-stepper,
+// global memory with the same arithmetic, so both forms move particles bit
+// for bit alike.  The new cell, unwrapped from the brick centre, widens bd.
 template <bool TILED>
 __device__ __forceinline__ void cyl_push_f32(const GridP &g, const CylP &cp, const PartF32 &p, uint32_t n,
                                              const PState &st, const float *__restrict__ Ex,
                                              const float *__restrict__ Ey, const float *__restrict__ Ez,
                                              const float *__restrict__ Bx, const float *__restrict__ By,
                                              const float *__restrict__ Bz, float *Jx, float *Jy, float *Jz, int *err,
-                                             const TileBox &tb, Bounds &bd)
+                                             const TileBox &tb, Bounds &bd, JAcc &acc, uint32_t *subq,
+                                             uint32_t *subq_n)
 {
     const float c = g.c_f, sqc = g.sqc_f, cinv = g.cinv_f, qi = g.qi_f;
     const float inv_dtheta = (float)cp.inv_dtheta;
@@ -710,7 +722,25 @@ __device__ __forceinline__ void cyl_push_f32(const GridP &g, const CylP &cp, con
     int ni, nj, nk;            // new cell
     float ox, oy, oz;          // new offsets
     float un, vn, wn;
-    if (i > 4 || (i == 4 && dx >= 0.5f)) {
+    const bool strang = i > 4 || (i == 4 && dx >= 0.5f);
+    if (TILED) {
+        // near-axis particles are left to k_cyl_substep_f32 (their slots
+        // queued); the box of the next step covers their cell +- 1
+        const uint32_t m = __ballot_sync(__activemask(), !strang);
+        if (!strang) {
+            const int lane = threadIdx.x & 31, leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(subq_n, (uint32_t)__popc(m));
+            base = __shfl_sync(m, base, leader);
+            subq[base + __popc(m & ((1u << lane) - 1u))] = n;
+            const int u0 = i - tb.hc[0], u1 = unwrap_offset(j, tb.hc[1], g.ny), u2 = unwrap_offset(k, tb.hc[2], g.nz);
+            bd.lo[0] = min(bd.lo[0], u0 - 1); bd.hi[0] = max(bd.hi[0], u0 + 1);
+            bd.lo[1] = min(bd.lo[1], u1 - 1); bd.hi[1] = max(bd.hi[1], u1 + 1);
+            bd.lo[2] = min(bd.lo[2], u2 - 1); bd.hi[2] = max(bd.hi[2], u2 + 1);
+            return;
+        }
+    }
+    if (strang) {
         // Strang step away from the axis (:104-341)
         int l0 = 0, l1 = 0, l2 = 0;   // box cell of the start cell
         bool in1 = false;
@@ -793,10 +823,20 @@ __device__ __forceinline__ void cyl_push_f32(const GridP &g, const CylP &cp, con
         segment<float, 3>(qthis * (Xn - xr), qthis * (Yn - yr), qthis * (Zn - zr), 0.5f * (Xn + xr) - (float)sx,
                           0.5f * (Yn + yr) - (float)sy, 0.5f * (Zn + zr) - (float)sz, o2);
         for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
-        if (TILED && in1)
-            red_entries_box<3>(tb.sJ + 4u * (uint32_t)((l0 + 1) + tb.JX * (l1 + 1) + tb.JXY * (l2 + 1)), tb.jo, o);
-        else
+        if (TILED && in1) {
+            const uint32_t a = tb.sJ + 8u * (uint32_t)((l0 + 1) + tb.JX * (l1 + 1) + tb.JXY * (l2 + 1));
+            if (a == acc.a) {
+#pragma unroll
+                for (int e = 0; e < 12; e++) acc.v[e] += o[e];
+            } else {
+                if (acc.a != kNoCell) red_entries_box_wide(acc.a, tb.jo, acc.v);
+                acc.a = a;
+#pragma unroll
+                for (int e = 0; e < 12; e++) acc.v[e] = o[e];
+            }
+        } else {
             scatter<float, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o);
+        }
     } else {
         // SubStepMovDep (:404-438) from the step's initial state: x and
         // theta absolute (small here), z relative to the start cell
@@ -917,9 +957,32 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move_f32(GridP g, CylP cp, Par
     const long long used = cnt->used;
     const TileBox tb = {};
     Bounds bd;
+    JAcc acc;
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x)
         cyl_push_f32<false>(g, cp, p, (uint32_t)n, load_state<3>(p, (uint32_t)n), Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz,
-                            err, tb, bd);
+                            err, tb, bd, acc, nullptr, nullptr);
+}
+
+// The near-axis particles the tiled mover queued (slots q[0 .. *qn)): the
+// sub-stepper, spread over every SM (a brick next to the axis would
+// otherwise hold its CTA for many times a brick's Strang steps, with the
+// lanes of its warps waiting on the few that sub-step).
+__global__ void __launch_bounds__(kThreads) k_cyl_substep_f32(GridP g, CylP cp, PartF32 p, const uint32_t *__restrict__ q,
+                                                              const uint32_t *__restrict__ qn,
+                                                              const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                                              const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                                              const float *__restrict__ By, const float *__restrict__ Bz,
+                                                              float *Jx, float *Jy, float *Jz, int *err)
+{
+    const uint32_t nq = *qn;
+    const TileBox tb = {};
+    Bounds bd;
+    JAcc acc;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nq; t += gridDim.x * blockDim.x) {
+        const uint32_t n = q[t];
+        cyl_push_f32<false>(g, cp, p, n, load_state<3>(p, n), Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, acc,
+                            nullptr, nullptr);
+    }
 }
 
 // Tiled form: one CTA per brick (after a reorder).  The box is the stored
@@ -941,21 +1004,25 @@ __global__ void __launch_bounds__(kTileThreads, 2)
     int home_lo[3], home_hi[3];
     brick_home<3>(g, bk, b, tb, home_lo, home_hi);
     // a Strang move is below one cell per axis, a sub-stepped one below two
-    tile_setup<3, false>(g, bk, b, p1 - p0, 1, 2.f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By, Bz);
+    tile_setup<3, false, true>(g, bk, b, p1 - p0, 1, 2.f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By, Bz);
     Bounds bd;
     bd.init();
+    JAcc acc;
+    acc.a = kNoCell;
     const uint32_t n0 = p0 + threadIdx.x;
     if (n0 < p1) {
         PState cur = load_state<3>(p, n0);
         for (uint32_t n = n0; n < p1; n += kTileThreads) {
             PState nxt = cur;
             if (p1 - n > kTileThreads) nxt = load_state<3>(p, n + kTileThreads);
-            cyl_push_f32<true>(g, cp, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
+            cyl_push_f32<true>(g, cp, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, acc, bk.bid,
+                               bk.count);
             cur = nxt;
         }
     }
+    if (acc.a != kNoCell) red_entries_box_wide(acc.a, tb.jo, acc.v);
     __syncthreads();
-    tile_finish<3, false>(g, bk, b, tb, sm, ts, bd, home_lo, home_hi, Jx, Jy, Jz);
+    tile_finish<3, false, true>(g, bk, b, tb, sm, ts, bd, home_lo, home_hi, Jx, Jy, Jz);
 }
 
 void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
@@ -977,10 +1044,15 @@ void launch_cyl_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const B
         attr_set = true;
     }
     const CylP cp = cyl_params(g);
+    // the queue of near-axis slots: the brick-id scratch of the reorder, its
+    // length in the scan scratch (both free between reorders)
+    cudaMemsetAsync(bk.count, 0, sizeof(uint32_t), s);
     k_cyl_move_f32_tiled<<<bk.ntiles, kTileThreads, bk.smem_floats * 4, s>>>(g, cp, p, bk, E[0], E[1], E[2], B[0],
                                                                             B[1], B[2], J[0], J[1], J[2], err);
+    k_cyl_substep_f32<<<kSMs * 4, kThreads, 0, s>>>(g, cp, p, bk.bid, bk.count, E[0], E[1], E[2], B[0], B[1], B[2],
+                                                   J[0], J[1], J[2], err);
     k_cyl_axis_current<float><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
-    count_launches(2);
+    count_launches(3);
 }
 
 }  // namespace pic

@@ -76,13 +76,18 @@ struct Bricks {
     int smem_floats;
 };
 // Shared words of a mover box of C cells: (C+1) nodes per axis x 6 field
-// components and (C+3) current cells per axis x 3 components.
-__host__ __device__ inline long long box_floats(int dims, int cx, int cy, int cz)
+// components and (C+3) current cells per axis x 3 components of jw words
+// (1: 32-bit fixed point, 2: 64-bit).
+__host__ __device__ inline long long box_floats(int dims, int cx, int cy, int cz, int jw = 1)
 {
     const long long nn = (long long)(cx + 1) * (cy + 1) * (dims == 3 ? cz + 1 : 1);
     const long long nj = (long long)(cx + 3) * (cy + 3) * (dims == 3 ? cz + 3 : 1);
-    return 6 * nn + 3 * nj;
+    return 6 * nn + 3 * jw * nj;
 }
+// Words per current entry of a mover box: 64-bit fixed point for the
+// cylindrical form, whose weights grow with the radius (a 32-bit scale set by
+// the largest weight leaves too few bits for the currents near the axis).
+__host__ __device__ inline int box_current_words(const GridP &g) { return g.geom == PIC_GEOM_CYLINDRICAL ? 2 : 1; }
 constexpr int kBoxAxisMax = 64;   // cells per axis of a mover box
 // Brick shape: `req` (all > 0) if given, else about 4096 particles per brick
 // at ppc particles per cell.  Returns false if the brick plus one cell on

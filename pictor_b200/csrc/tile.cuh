@@ -91,6 +91,11 @@ __device__ __forceinline__ void red_shared_i(uint32_t a, int v)
 {
     asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a), "n"(OFF), "r"(v));
 }
+template <int OFF>
+__device__ __forceinline__ void red_shared_l(uint32_t a, long long v)
+{
+    asm volatile("red.shared.add.u64 [%0+%1], %2;" ::"r"(a), "n"(OFF), "l"(v));
+}
 
 // Shared byte offsets of the current box: component planes and the y / z
 // strides (the x stride is 4 bytes, an immediate).
@@ -224,12 +229,13 @@ __device__ __forceinline__ void brick_home(const GridP &g, const Bricks &bk, int
 // stored bounds widened by `margin` cells on each side (movers that gather a
 // second time at the cell they move to), or the brick +- 1 cell when that is
 // too large; strides and byte offsets; the fixed-point scale for the n
-// particles of the brick, whose moves are below dmax cells per axis; the
+// particles of the brick, whose moves are below dmax cells per axis (current
+// words of 32 bits, or 64 with WIDE); the
 // memory offsets of the box cells along each axis (the periodic interior
 // image, or along a non-periodic x axis (XPER false: the radius of the
 // cylindrical form) the index itself); the current box zeroed and the
 // node-averaged fields staged.
-template <int DIMS, bool XPER>
+template <int DIMS, bool XPER, bool WIDE = false>
 __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int b, uint32_t n, int margin, float dmax,
                                            float *sm, TileShared &ts, TileBox &tb, const int home_lo[3],
                                            const int home_hi[3], const float *__restrict__ Ex,
@@ -244,7 +250,7 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     int hi[3] = {sb[3] + margin, sb[4] + margin, DIMS == 3 ? sb[5] + margin : 0};
     if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2] || hi[0] - lo[0] >= kBoxAxisMax ||
         hi[1] - lo[1] >= kBoxAxisMax || hi[2] - lo[2] >= kBoxAxisMax ||
-        box_floats(DIMS, hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1) > bk.smem_floats) {
+        box_floats(DIMS, hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1, WIDE ? 2 : 1) > bk.smem_floats) {
 #pragma unroll
         for (int d = 0; d < DIMS; d++) {
             lo[d] = home_lo[d] - 1;
@@ -266,10 +272,11 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     tb.njc = JX * JY * JZ;
     tb.oY4 = 16u * (uint32_t)NX;
     tb.oZ4 = 16u * (uint32_t)(NX * NY);
-    tb.jo.cy = 4u * (uint32_t)tb.njc;
-    tb.jo.cz = 8u * (uint32_t)tb.njc;
-    tb.jo.y = 4u * (uint32_t)JX;
-    tb.jo.z = 4u * (uint32_t)tb.JXY;
+    constexpr uint32_t wb = WIDE ? 8u : 4u;   // bytes per current word
+    tb.jo.cy = wb * (uint32_t)tb.njc;
+    tb.jo.cz = 2u * wb * (uint32_t)tb.njc;
+    tb.jo.y = wb * (uint32_t)JX;
+    tb.jo.z = wb * (uint32_t)tb.JXY;
     tb.jo.yz = tb.jo.y + tb.jo.z;
     float4 *nA = reinterpret_cast<float4 *>(sm);
     float2 *nB = reinterpret_cast<float2 *>(sm + 4 * nnode);
@@ -280,11 +287,12 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     // fixed-point scale: a particle adds at most b = |w| qi dmax to any entry,
     // so with S = 2^30 / (N b) no sum of the N particles exceeds 2^30;
     // S <= 2^22 / b keeps each contribution below 2^22 (the range of
-    // fixed_round)
+    // fixed_round).  64-bit words: S = 2^62 / (N b), each contribution an
+    // FP32 value rounded to an integer of up to 2^54, the sums exact.
     {
         const float b1 = dmax * g.qi_f * __uint_as_float(*bk.wmax_bits);
         const float nf = fmaxf((float)n, 256.f);
-        tb.S = b1 > 0.f ? 1073741824.f / (b1 * nf) : 1.f;
+        tb.S = b1 > 0.f ? (WIDE ? 4.611686018427388e18f : 1073741824.f) / (b1 * nf) : 1.f;
     }
     // offsets of the box cells lo-1 .. lo+C+1 along each axis (memory offset
     // of the interior image, times the axis stride)
@@ -299,7 +307,7 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
             }
         if (DIMS == 2 && tid == 0) ts.s_off[2][0] = 0;
     }
-    for (int q = tid; q < 3 * tb.njc; q += kTileThreads) sJ[q] = 0;
+    for (int q = tid; q < (WIDE ? 6 : 3) * tb.njc; q += kTileThreads) sJ[q] = 0;
     __syncthreads();
     // stage node-averaged fields: node q = xx + NX*(yy + NY*zz); q/NX and
     // r/NY by multiply-high (exact for q < 2^16, NX, NY < 2^16)
@@ -324,26 +332,35 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
 // to global J at the offsets of tile_setup (FP32 reductions), and the bounds
 // of the particles' new cells stored as the box of the next step (the brick
 // itself if no particle is left).
-template <int DIMS, bool XPER>
+template <int DIMS, bool XPER, bool WIDE = false>
 __device__ __forceinline__ void tile_finish(const GridP &g, const Bricks &bk, int b, const TileBox &tb, float *sm,
                                             TileShared &ts, const Bounds &bd, const int home_lo[3],
                                             const int home_hi[3], float *Jx, float *Jy, float *Jz)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nnode = tb.NXY * (DIMS == 3 ? tb.C[2] + 1 : 1);
-    const int *sJ = reinterpret_cast<const int *>(sm + 6 * nnode);
     {
         const int JX = tb.JX, JY = tb.C[1] + 3;
-        const float inv = 1.f / tb.S;
         const uint32_t mX = 0xffffffffu / (uint32_t)JX + 1u, mY = 0xffffffffu / (uint32_t)JY + 1u;
+        const int *sJ = reinterpret_cast<const int *>(sm + 6 * nnode);
+        const long long *sJ8 = reinterpret_cast<const long long *>(sm + 6 * nnode);
+        const float inv = 1.f / tb.S;
+        const double inv8 = 1.0 / (double)tb.S;
         for (int q = tid; q < tb.njc; q += kTileThreads) {
             const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * JX;
             const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * JY;
             const int off = ts.s_off[0][xx] + ts.s_off[1][yy] + (DIMS == 3 ? ts.s_off[2][zz] : 0);
-            const int vx = sJ[q], vy = sJ[tb.njc + q], vz = sJ[2 * tb.njc + q];
-            if (vx != 0) atomicAdd(Jx + off, (float)vx * inv);
-            if (vy != 0) atomicAdd(Jy + off, (float)vy * inv);
-            if (vz != 0) atomicAdd(Jz + off, (float)vz * inv);
+            if (WIDE) {
+                const long long vx = sJ8[q], vy = sJ8[tb.njc + q], vz = sJ8[2 * tb.njc + q];
+                if (vx != 0) atomicAdd(Jx + off, (float)((double)vx * inv8));
+                if (vy != 0) atomicAdd(Jy + off, (float)((double)vy * inv8));
+                if (vz != 0) atomicAdd(Jz + off, (float)((double)vz * inv8));
+            } else {
+                const int vx = sJ[q], vy = sJ[tb.njc + q], vz = sJ[2 * tb.njc + q];
+                if (vx != 0) atomicAdd(Jx + off, (float)vx * inv);
+                if (vy != 0) atomicAdd(Jy + off, (float)vy * inv);
+                if (vz != 0) atomicAdd(Jz + off, (float)vz * inv);
+            }
         }
     }
     int v[6] = {bd.lo[0], bd.lo[1], bd.lo[2], -bd.hi[0], -bd.hi[1], -bd.hi[2]};
@@ -396,6 +413,29 @@ __device__ __forceinline__ void gather_box(const TileBox &tb, int nb, const floa
         accum(wt[6], lds4i<0>(a3), lds2i<0>(b3), pE, pB);
         accum(wt[7], lds4i<16>(a3), lds2i<8>(b3), pE, pB);
     }
+}
+
+// The 12 VecJ entries v of a 3D cell (in fixed-point units, FP32) into a
+// current box of 64-bit words at byte address a, each rounded to the nearest
+// integer (the layout of red_entries_box).
+__device__ __forceinline__ void red_entries_box_wide(uint32_t a, const JOff &o, const float v[12])
+{
+    red_shared_l<0>(a, __float2ll_rn(v[0]));
+    red_shared_l<0>(a + o.y, __float2ll_rn(v[1]));
+    red_shared_l<0>(a + o.z, __float2ll_rn(v[2]));
+    red_shared_l<0>(a + o.yz, __float2ll_rn(v[3]));
+    const uint32_t b = a + o.cy;
+    red_shared_l<0>(b, __float2ll_rn(v[4]));
+    red_shared_l<8>(b, __float2ll_rn(v[5]));
+    const uint32_t bz = b + o.z;
+    red_shared_l<0>(bz, __float2ll_rn(v[6]));
+    red_shared_l<8>(bz, __float2ll_rn(v[7]));
+    const uint32_t c = a + o.cz;
+    red_shared_l<0>(c, __float2ll_rn(v[8]));
+    red_shared_l<8>(c, __float2ll_rn(v[9]));
+    const uint32_t cy = c + o.y;
+    red_shared_l<0>(cy, __float2ll_rn(v[10]));
+    red_shared_l<8>(cy, __float2ll_rn(v[11]));
 }
 
 // VecJ entries v (already in fixed-point units, FP32) into the current box

@@ -1,7 +1,7 @@
 """The tiled FP32 cylindrical mover (one CTA per brick, node-averaged fields
-and a fixed-point current box in shared memory, the radius not periodic)
-against the per-particle FP32 cylindrical mover: particles bit for bit,
-currents up to FP32 summation order and the fixed-point rounding."""
+and a 64-bit fixed-point current box in shared memory, the radius not
+periodic) against the per-particle FP32 cylindrical mover: particles bit for
+bit, currents up to FP32 rounding and summation order."""
 import numpy as np
 import pytest
 
@@ -60,9 +60,11 @@ def test_cyl_tiled_mover_matches_per_particle_mover():
     """One push + deposit after a reorder (tiled) and of the same particles
     reloaded (per-particle): every position and momentum equal, the same
     particles dropped at the outer radius, and the folded current equal up to
-    FP32 summation order plus the fixed-point bound (S = 2^30 / (2 qi max|w|
-    max(N, 256)) per brick; each of the 8 cells around an entry adds one
-    rounded value per particle)."""
+    FP32 rounding and summation order: the box adds each contribution as an
+    FP32 value scaled by S = 2^62 / (2 qi max|w| max(N, 256)) and rounded to
+    a 64-bit integer, so the integer rounding (the slack below) is far
+    below the FP32 rounding of the contribution itself, weights near the
+    axis 20 times below the largest included."""
     from pictor_b200 import Simulation
 
     nx, ny, nz = 24, 8, 16
@@ -89,21 +91,22 @@ def test_cyl_tiled_mover_matches_per_particle_mover():
     for k in ("x", "y", "z", "u", "v", "w", "q", "flv"):
         np.testing.assert_array_equal(getattr(a_p, k), getattr(b_p, k), err_msg=k)
     nmax, per_cell = _brick_max(sorted_p, _brick_shape(3, nx, ny, nz, 1 << 16), nx, ny, nz)
-    s_min = 2.0 ** 30 / (2.0 * QI * np.abs(sorted_p.q).max() * nmax)
+    s_min = 2.0 ** 62 / (2.0 * QI * np.abs(sorted_p.q).max() * nmax)
     slack = 8 * per_cell * 0.5 / s_min
     for n in ("Jx", "Jy", "Jz"):
         a, b = interior(getattr(a_f, n), g), interior(getattr(b_f, n), g)
         np.testing.assert_allclose(a, b, rtol=0, atol=2e-6 * np.abs(b).max() + slack, err_msg=n)
-        assert slack < 1e-2 * np.abs(b).max()     # the bound itself is small
+        assert slack < 1e-10 * np.abs(b).max()     # the bound itself is negligible
 
 
 @pytest.mark.parametrize("modes", [0, 2])
 def test_cyl_tiled_steps_track_per_particle_steps(modes):
-    """The wakefield case, 30 steps without a reorder after the first one
-    (the bunch drifts 9 cells in z, past its bricks' boxes), theta-gridded
-    and modal field solves: the tiled run stays on the per-particle run up
-    to FP32 summation-order noise (same particle count, kinetic energy 1e-5,
-    field energy 1e-3)."""
+    """The wakefield case (weights by radius, a cold background whose
+    currents are small next to the bunch's), 30 steps without a reorder
+    after the first one (the bunch drifts 9 cells in z, past its bricks'
+    boxes), theta-gridded and modal field solves: the tiled run stays on the
+    per-particle run up to FP32 summation-order noise (same particle count,
+    kinetic energy 1e-6, field energy 1e-5)."""
     from pictor_b200 import PicConfig, Simulation, init_scale
     from pictor_b200.setups import cyl_wakefield
 
@@ -124,6 +127,6 @@ def test_cyl_tiled_steps_track_per_particle_steps(modes):
             res[tiled] = (s.particle_count(), s.diagnostics())
     (na, da), (nb, db) = res[True], res[False]
     assert na == nb
-    np.testing.assert_allclose(da["kinetic"].sum(), db["kinetic"].sum(), rtol=1e-5)
+    np.testing.assert_allclose(da["kinetic"].sum(), db["kinetic"].sum(), rtol=1e-6)
     fa, fb = da["B2"] + da["E2"], db["B2"] + db["E2"]
-    assert abs(fa - fb) <= 1e-3 * fb
+    assert abs(fa - fb) <= 1e-5 * fb, (fa, fb)
