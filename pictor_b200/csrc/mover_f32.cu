@@ -106,24 +106,18 @@ __device__ __forceinline__ void part_entries(const Part &d, float v[12])
 {
     const float ax = 1.f - d.W[0], ay = 1.f - d.W[1];
     if (!CROSS) {
-        // D = 0: plain products
+        // D = 0: plain products (pairs of entries by packed multiplies)
         if (DIMS == 3) {
             const float az = 1.f - d.W[2];
-            const float Fa = d.F[0] * ay, Fw = d.F[0] * d.W[1];
-            v[0] = Fa * az;
-            v[1] = Fw * az;
-            v[2] = Fa * d.W[2];
-            v[3] = Fw * d.W[2];
-            const float Ga = d.F[1] * ax, Gw = d.F[1] * d.W[0];
-            v[4] = Ga * az;
-            v[5] = Gw * az;
-            v[6] = Ga * d.W[2];
-            v[7] = Gw * d.W[2];
-            const float Ha = d.F[2] * ax, Hw = d.F[2] * d.W[0];
-            v[8] = Ha * ay;
-            v[9] = Hw * ay;
-            v[10] = Ha * d.W[1];
-            v[11] = Hw * d.W[1];
+            const float2 Fx = fmul2(make_float2(d.F[0], d.F[0]), make_float2(ay, d.W[1]));
+            const float2 v01 = fmul2(Fx, make_float2(az, az)), v23 = fmul2(Fx, make_float2(d.W[2], d.W[2]));
+            const float2 Fy = fmul2(make_float2(d.F[1], d.F[1]), make_float2(ax, d.W[0]));
+            const float2 v45 = fmul2(Fy, make_float2(az, az)), v67 = fmul2(Fy, make_float2(d.W[2], d.W[2]));
+            const float2 Fz = fmul2(make_float2(d.F[2], d.F[2]), make_float2(ax, d.W[0]));
+            const float2 v89 = fmul2(Fz, make_float2(ay, ay)), vab = fmul2(Fz, make_float2(d.W[1], d.W[1]));
+            v[0] = v01.x; v[1] = v01.y; v[2] = v23.x; v[3] = v23.y;
+            v[4] = v45.x; v[5] = v45.y; v[6] = v67.x; v[7] = v67.y;
+            v[8] = v89.x; v[9] = v89.y; v[10] = vab.x; v[11] = vab.y;
         } else {
             v[0] = d.F[0] * ay;
             v[1] = d.F[0] * d.W[1];
@@ -138,27 +132,29 @@ __device__ __forceinline__ void part_entries(const Part &d, float v[12])
         return;
     }
     if (DIMS == 3) {
+        // (Fa, Fw) = F (1-W, W) along the entry's first transverse axis, then
+        // each pair of entries by one packed FMA with the cross term +-Fd
         const float az = 1.f - d.W[2];
         {
-            const float Fa = d.F[0] * ay, Fw = d.F[0] * d.W[1], Fd = d.F[0] * d.D[0];
-            v[0] = fmaf(Fa, az, Fd);
-            v[1] = fmaf(Fw, az, -Fd);
-            v[2] = fmaf(Fa, d.W[2], -Fd);
-            v[3] = fmaf(Fw, d.W[2], Fd);
+            const float2 Fp = fmul2(make_float2(d.F[0], d.F[0]), make_float2(ay, d.W[1]));
+            const float Fd = d.F[0] * d.D[0];
+            const float2 v01 = ffma2(Fp, make_float2(az, az), make_float2(Fd, -Fd));
+            const float2 v23 = ffma2(Fp, make_float2(d.W[2], d.W[2]), make_float2(-Fd, Fd));
+            v[0] = v01.x; v[1] = v01.y; v[2] = v23.x; v[3] = v23.y;
         }
         {
-            const float Fa = d.F[1] * ax, Fw = d.F[1] * d.W[0], Fd = d.F[1] * d.D[1];
-            v[4] = fmaf(Fa, az, Fd);
-            v[5] = fmaf(Fw, az, -Fd);
-            v[6] = fmaf(Fa, d.W[2], -Fd);
-            v[7] = fmaf(Fw, d.W[2], Fd);
+            const float2 Fp = fmul2(make_float2(d.F[1], d.F[1]), make_float2(ax, d.W[0]));
+            const float Fd = d.F[1] * d.D[1];
+            const float2 v45 = ffma2(Fp, make_float2(az, az), make_float2(Fd, -Fd));
+            const float2 v67 = ffma2(Fp, make_float2(d.W[2], d.W[2]), make_float2(-Fd, Fd));
+            v[4] = v45.x; v[5] = v45.y; v[6] = v67.x; v[7] = v67.y;
         }
         {
-            const float Fa = d.F[2] * ax, Fw = d.F[2] * d.W[0], Fd = d.F[2] * d.D[2];
-            v[8] = fmaf(Fa, ay, Fd);
-            v[9] = fmaf(Fw, ay, -Fd);
-            v[10] = fmaf(Fa, d.W[1], -Fd);
-            v[11] = fmaf(Fw, d.W[1], Fd);
+            const float2 Fp = fmul2(make_float2(d.F[2], d.F[2]), make_float2(ax, d.W[0]));
+            const float Fd = d.F[2] * d.D[2];
+            const float2 v89 = ffma2(Fp, make_float2(ay, ay), make_float2(Fd, -Fd));
+            const float2 vab = ffma2(Fp, make_float2(d.W[1], d.W[1]), make_float2(-Fd, Fd));
+            v[8] = v89.x; v[9] = v89.y; v[10] = vab.x; v[11] = vab.y;
         }
     } else {
         v[0] = d.F[0] * ay;

@@ -40,14 +40,61 @@ __device__ __forceinline__ void node_avg(const float *__restrict__ Ex, const flo
     Bv.y = (((__ldg(Bz + nd - 1 - sy) + __ldg(Bz + nd - 1)) + __ldg(Bz + nd - sy)) + __ldg(Bz + nd)) * 0.25f + b2;
 }
 
+// Packed FP32 pair arithmetic of sm_100 (one instruction for two lanes of
+// IEEE single precision, each rounded as the scalar operation would be).
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c)
+{
+    float2 d;
+    asm("{.reg .b64 ra, rb, rc, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mov.b64 rc, {%6, %7};\n\t"
+        "fma.rn.f32x2 rd, ra, rb, rc;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
+    return d;
+}
+
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "mul.rn.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b)
+{
+    float2 d;
+    asm("{.reg .b64 ra, rb, rd;\n\t"
+        "mov.b64 ra, {%2, %3};\n\t"
+        "mov.b64 rb, {%4, %5};\n\t"
+        "add.rn.f32x2 rd, ra, rb;\n\t"
+        "mov.b64 {%0, %1}, rd;}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+
+// pE += w * (E at a node), pB += w * (B at a node): the interpolation sums
+// of movdep.F90:116-129, three packed FMAs (the same roundings as six fmaf).
 __device__ __forceinline__ void accum(float w, const float4 &A, const float2 &Bv, float pE[3], float pB[3])
 {
-    pE[0] = fmaf(w, A.x, pE[0]);
-    pE[1] = fmaf(w, A.y, pE[1]);
-    pE[2] = fmaf(w, A.z, pE[2]);
-    pB[0] = fmaf(w, A.w, pB[0]);
-    pB[1] = fmaf(w, Bv.x, pB[1]);
-    pB[2] = fmaf(w, Bv.y, pB[2]);
+    const float2 ww = make_float2(w, w);
+    const float2 a = ffma2(make_float2(A.x, A.y), ww, make_float2(pE[0], pE[1]));
+    const float2 b = ffma2(make_float2(A.z, A.w), ww, make_float2(pE[2], pB[0]));
+    const float2 c = ffma2(Bv, ww, make_float2(pB[1], pB[2]));
+    pE[0] = a.x;
+    pE[1] = a.y;
+    pE[2] = b.x;
+    pB[0] = b.y;
+    pB[1] = c.x;
+    pB[2] = c.y;
 }
 
 // Interpolation weights of the 4 / 8 corners (corner bit 0 = x, 1 = y, 2 = z).
@@ -109,6 +156,12 @@ struct JOff {
 __device__ __forceinline__ int fixed_round(float v)
 {
     return __float_as_int(v + 12582912.f) - 0x4B400000;
+}
+// The same for a pair, with one packed add.
+__device__ __forceinline__ int2 fixed_round2(float a, float b)
+{
+    const float2 t = fadd2(make_float2(a, b), make_float2(12582912.f, 12582912.f));
+    return make_int2(__float_as_int(t.x) - 0x4B400000, __float_as_int(t.y) - 0x4B400000);
 }
 
 // Interior index 3..n+2 of a periodic (unwrapped) 1-based index a.
@@ -445,22 +498,25 @@ template <int DIMS>
 __device__ __forceinline__ void red_entries_box(uint32_t a, const JOff &o, const float v[12])
 {
     if (DIMS == 3) {
-        red_shared_i<0>(a, fixed_round(v[0]));
-        red_shared_i<0>(a + o.y, fixed_round(v[1]));
-        red_shared_i<0>(a + o.z, fixed_round(v[2]));
-        red_shared_i<0>(a + o.yz, fixed_round(v[3]));
+        const int2 r01 = fixed_round2(v[0], v[1]), r23 = fixed_round2(v[2], v[3]);
+        const int2 r45 = fixed_round2(v[4], v[5]), r67 = fixed_round2(v[6], v[7]);
+        const int2 r89 = fixed_round2(v[8], v[9]), rab = fixed_round2(v[10], v[11]);
+        red_shared_i<0>(a, r01.x);
+        red_shared_i<0>(a + o.y, r01.y);
+        red_shared_i<0>(a + o.z, r23.x);
+        red_shared_i<0>(a + o.yz, r23.y);
         const uint32_t b = a + o.cy;
-        red_shared_i<0>(b, fixed_round(v[4]));
-        red_shared_i<4>(b, fixed_round(v[5]));
+        red_shared_i<0>(b, r45.x);
+        red_shared_i<4>(b, r45.y);
         const uint32_t bz = b + o.z;
-        red_shared_i<0>(bz, fixed_round(v[6]));
-        red_shared_i<4>(bz, fixed_round(v[7]));
+        red_shared_i<0>(bz, r67.x);
+        red_shared_i<4>(bz, r67.y);
         const uint32_t c = a + o.cz;
-        red_shared_i<0>(c, fixed_round(v[8]));
-        red_shared_i<4>(c, fixed_round(v[9]));
+        red_shared_i<0>(c, r89.x);
+        red_shared_i<4>(c, r89.y);
         const uint32_t cy = c + o.y;
-        red_shared_i<0>(cy, fixed_round(v[10]));
-        red_shared_i<4>(cy, fixed_round(v[11]));
+        red_shared_i<0>(cy, rab.x);
+        red_shared_i<4>(cy, rab.y);
     } else {
         red_shared_i<0>(a, fixed_round(v[0]));
         red_shared_i<0>(a + o.y, fixed_round(v[1]));
