@@ -79,7 +79,14 @@ typedef struct {
        projected onto them; particles still gather from and deposit onto the
        ny theta cells).  No counterpart in the reference. */
     int32_t cyl_modes;
-    int32_t reserved[3];
+    /* 1 = this handle is one slab of a domain split along x (the reference's
+       MPI decomposition with the x neighbours on other ranks): the kernels
+       leave the x ghost layers to the pic_slab_* exchanges and particles
+       leaving through the x faces to pic_slab_pack_particles; y and z stay
+       periodic on the slab.  FP64 Cartesian, no current filter.  0 = one
+       periodic domain. */
+    int32_t slab_x;
+    int32_t reserved[2];
 } pic_config;
 
 typedef struct pic_handle pic_handle;
@@ -129,6 +136,32 @@ int pic_reset_current(pic_handle *h);      /* ResetCurrentGPU (fields_gpu.F90:61
 int pic_reorder(pic_handle *h);            /* ReorderPrtlGPU / ReorderPrtlArr (mem_prtl.F90:166-301)        */
 /* Current filter passes (smoothen_current, current.F90:19-163). */
 int pic_filter_current(pic_handle *h);
+
+/* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
+   with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:
+   13-106, comm_prtl.F90:11-66 across ranks); the caller moves the buffers
+   (device pointers) between neighbouring slabs, the left neighbour of the
+   first slab being the last one:
+     pic_update_b_half; B faces | pic_move_deposit; pic_slab_pack_particles,
+     particles, pic_slab_unpack_particles (from the left, then from the
+     right) | pic_update_b_half; B faces | pic_update_e | J faces;
+     pic_fold_current; pic_add_current; E faces | pic_reorder every period.
+   Face buffers hold pic_slab_face_len doubles each: component-major layers
+   of my * mz values.  pack_fields(which: 0 E, 1 B, 2 J) fills to_left and
+   to_right (J: the ghost current, which it zeroes); unpack_fields takes what
+   the left neighbour packed to its right (from_left) and what the right one
+   packed to its left (from_right), copied into the ghosts (E, B) or added to
+   the interior layers (J).  pack_particles removes the particles that left
+   through the x faces and writes them to `out` (8 doubles each: q, x, y, z,
+   u, v, w, flv, positions in the receiver's coordinates): n_right bound
+   right first, then n_left bound left; y and z leavers wrap on the slab.
+   PIC_ERR_OVERFLOW if more than `cap` leave.  pic_step, pic_step_many and
+   pic_exchange_particles refuse a slab. */
+int pic_slab_face_len(pic_handle *h, int64_t *n);
+int pic_slab_pack_fields(pic_handle *h, int32_t which, double *to_left, double *to_right);
+int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left, const double *from_right);
+int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_right, int64_t *n_left);
+int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n);
 
 /* nsteps full steps of MAIN.F90:42-284 (reorder every reorder_period steps,
    counted from the handle's step counter), captured once as a CUDA graph. */

@@ -44,7 +44,7 @@ class Config(C.Structure):
         ("reorder_period", C.c_int32), ("curr_filter", C.c_int32),
         ("capacity", C.c_int64),
         ("rmin", C.c_double), ("inc_axis", C.c_int32), ("brick", C.c_int32 * 3), ("cyl_modes", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("slab_x", C.c_int32), ("reserved", C.c_int32 * 2),
     ]
 
 
@@ -101,6 +101,11 @@ SIGNATURES = {
     "pic_reset_current": (C.c_int, [H]),
     "pic_reorder": (C.c_int, [H]),
     "pic_filter_current": (C.c_int, [H]),
+    "pic_slab_face_len": (C.c_int, [H, PI64]),
+    "pic_slab_pack_fields": (C.c_int, [H, C.c_int32, C.c_void_p, C.c_void_p]),
+    "pic_slab_unpack_fields": (C.c_int, [H, C.c_int32, C.c_void_p, C.c_void_p]),
+    "pic_slab_pack_particles": (C.c_int, [H, C.c_void_p, C.c_int64, PI64, PI64]),
+    "pic_slab_unpack_particles": (C.c_int, [H, C.c_void_p, C.c_int64]),
     "pic_step": (C.c_int, [H, C.c_int32]),
     "pic_step_many": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),
     "pic_step_batched": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),

@@ -55,6 +55,8 @@ struct pic_handle {
     size_t stage_bytes = 0;
     cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
     bool sorted = false;
+    // slab form: device counts of the particles sent through the x faces
+    uint32_t *slab_sent = nullptr;
     std::vector<void *> allocs;
 };
 
@@ -839,6 +841,12 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (c.geom == PIC_GEOM_CYLINDRICAL && (c.dims != 3 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
         return PIC_ERR_INVALID;
     if (c.cyl_modes != 0 && (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4)) return PIC_ERR_INVALID;
+    // the slab form: the reference's FP64 Cartesian step with its x faces on
+    // neighbouring ranks (no current filter: its passes would need a halo
+    // exchange per pass)
+    if (c.slab_x != 0 && (c.slab_x != 1 || c.geom != PIC_GEOM_CARTESIAN || c.precision != PIC_PREC_FP64 ||
+                          c.curr_filter != 0))
+        return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
@@ -883,6 +891,7 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     else lehe_coefficients(c.dims, c.c, g.lehe);
     g.geom = c.geom;
     g.closed_x = c.geom == PIC_GEOM_CYLINDRICAL;
+    g.x_external = c.slab_x;
     g.qm[0] = 0.0;
     for (int f = 1; f <= PIC_MAX_FLVR; f++) g.qm[f] = f <= c.nflvr ? c.qm[f] : 0.0;
     g.c_f = (float)g.c;
@@ -940,6 +949,7 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     }
     if (!r) r = dalloc(h, &h->cnt, 1);
     if (!r) r = dalloc(h, &h->err, 1);
+    if (!r && c.slab_x) r = dalloc(h, &h->slab_sent, 2);
     if (!r) {
         SortScratch &sc = h->sc;
         sc.ntiles = sort_tiles(h->capacity);
@@ -1257,7 +1267,7 @@ int pic_move_deposit(pic_handle *h)
 
 int pic_exchange_particles(pic_handle *h)
 {
-    if (!h) return PIC_ERR_INVALID;
+    if (!h || h->g.x_external) return PIC_ERR_INVALID;   // a slab exchanges through pic_slab_pack_particles
     if (!h->fp32) launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s);
     return finish(h);
 }
@@ -1358,6 +1368,50 @@ int pic_add_current(pic_handle *h)
     return finish(h);
 }
 
+int pic_slab_face_len(pic_handle *h, int64_t *n)
+{
+    if (!h || !n || !h->g.x_external) return PIC_ERR_INVALID;
+    *n = 9ll * h->g.my * h->g.mz;
+    return PIC_OK;
+}
+
+int pic_slab_pack_fields(pic_handle *h, int32_t which, double *to_left, double *to_right)
+{
+    if (!h || !h->g.x_external || which < 0 || which > 2 || !to_left || !to_right) return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_slab_pack_fields(h->g, which, which == 0 ? E : which == 1 ? B : J, to_left, to_right, h->s);
+    return finish(h);
+}
+
+int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left, const double *from_right)
+{
+    if (!h || !h->g.x_external || which < 0 || which > 2 || !from_left || !from_right) return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_slab_unpack_fields(h->g, which, which == 0 ? E : which == 1 ? B : J, from_left, from_right, h->s);
+    return finish(h);
+}
+
+int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_right, int64_t *n_left)
+{
+    if (!h || !h->g.x_external || !out || cap < 0 || !n_right || !n_left) return PIC_ERR_INVALID;
+    launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s, out, cap, h->slab_sent);
+    uint32_t sent[2] = {0, 0};
+    CK(cudaMemcpyAsync(sent, h->slab_sent, sizeof(sent), cudaMemcpyDeviceToHost, h->s));
+    const int r = finish(h);
+    *n_right = sent[0];
+    *n_left = (int64_t)sent[1] - (int64_t)sent[0];
+    return r;
+}
+
+int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n)
+{
+    if (!h || !h->g.x_external || n < 0 || (n > 0 && !in)) return PIC_ERR_INVALID;
+    launch_slab_append(h->g, h->p64[h->cur], h->cnt, in, n, h->capacity, h->err, h->s);
+    return finish(h);
+}
+
 int pic_reorder(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
@@ -1377,7 +1431,8 @@ int pic_set_step(pic_handle *h, int64_t t)
 
 int pic_step(pic_handle *h, int32_t nsteps)
 {
-    if (!h || nsteps < 0) return PIC_ERR_INVALID;
+    // a slab's step has exchanges with its neighbours between the phases
+    if (!h || nsteps < 0 || h->g.x_external) return PIC_ERR_INVALID;
     // J must be zero when a deposit starts; inside the loop the E update
     // consumes and clears it.
     for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
@@ -1401,7 +1456,7 @@ int pic_step_batched(pic_handle *const *hs, int32_t n, int32_t nsteps)
 {
     if (!hs || n < 1 || nsteps < 0) return PIC_ERR_INVALID;
     for (int32_t a = 0; a < n; a++)
-        if (!hs[a]) return PIC_ERR_INVALID;
+        if (!hs[a] || hs[a]->g.x_external) return PIC_ERR_INVALID;
     if (!batchable(hs, n)) return PIC_ERR_INVALID;
     if (nsteps == 0) return PIC_OK;
     return step_many_batched(hs, n, nsteps);
@@ -1412,7 +1467,7 @@ int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps)
     if (!hs || n < 0 || nsteps < 0) return PIC_ERR_INVALID;
     bool eager = false;
     for (int32_t a = 0; a < n; a++) {
-        if (!hs[a]) return PIC_ERR_INVALID;
+        if (!hs[a] || hs[a]->g.x_external) return PIC_ERR_INVALID;
         eager = eager || hs[a]->profiling;
     }
     if (eager) {

@@ -31,6 +31,7 @@ struct GridP {
     double xmin, xmax, ymin, ymax, zmin, zmax, xlen, ylen, zlen;
     int geom;                         // PIC_GEOM_*
     int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
+    int x_external;                   // slab form: x faces exchanged with neighbouring slabs (no x images)
     unsigned int mx_magic, my_magic;  // n / m = umulhi(n, magic) >> shift, exact for n < 2^28 (div_magic)
     int mx_shift, my_shift;
     // FP32 copies for the FP32 form: c, c^2, 1/c, qi, external B, q/m * 0.5

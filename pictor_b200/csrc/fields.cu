@@ -41,11 +41,15 @@ __device__ __forceinline__ int image_of(int a, int m)
     return 0;
 }
 
+// Image along x: none in the slab form, whose x ghosts the neighbouring
+// slabs fill (SendRecvFlds / UpdateCurrentAllFaces across ranks).
+__device__ __forceinline__ int image_x(const GridP &g, int i) { return g.x_external ? 0 : image_of(i, g.mx); }
+
 // Write v to interior cell (i,j,k) and all of its periodic ghost images.
 template <typename T, int DIMS>
 __device__ __forceinline__ void store_with_images(const GridP &g, T *F, int i, int j, int k, T v)
 {
-    const int ii[2] = {i, image_of(i, g.mx)};
+    const int ii[2] = {i, image_x(g, i)};
     const int jj[2] = {j, image_of(j, g.my)};
     const int kk[2] = {k, DIMS == 3 ? image_of(k, g.mz) : 0};
 #pragma unroll
@@ -204,7 +208,7 @@ __device__ __forceinline__ void e_curl(const GridP &g, T fc, const T *Ex, const 
 template <typename T, int DIMS>
 __device__ __forceinline__ T fold_cell(const GridP &g, const T *__restrict__ J, int i, int j, int k)
 {
-    const int pi = image_of(i, g.mx), pj = image_of(j, g.my);
+    const int pi = image_x(g, i), pj = image_of(j, g.my);
     const int pk = DIMS == 3 ? image_of(k, g.mz) : 0;
     auto J1 = [&](int b, int c) -> T {
         T v = J[cidx(g, i, b, c)];
@@ -225,7 +229,7 @@ __device__ __forceinline__ T fold_cell(const GridP &g, const T *__restrict__ J, 
 template <typename T, int DIMS>
 __device__ __forceinline__ void zero_fold_cells(const GridP &g, T *__restrict__ J, int i, int j, int k)
 {
-    const int ii[2] = {i, image_of(i, g.mx)};
+    const int ii[2] = {i, image_x(g, i)};
     const int jj[2] = {j, image_of(j, g.my)};
     const int kk[2] = {k, DIMS == 3 ? image_of(k, g.mz) : 0};
 #pragma unroll

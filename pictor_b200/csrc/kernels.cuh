@@ -130,8 +130,17 @@ struct SortScratch {
 size_t sort_tiles(long long capacity);
 size_t scan_tmp_len(size_t n);
 // Exchange (wrap) of the reference layout: holes + append in AppendParticles order.
+// Slab form (g.x_external): the x leavers go to `out` (out_cap particles of 8
+// doubles) and sent_counts (device) receives {right-bound, right + left-bound}.
 void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch &sc, long long capacity, int *err,
-                         cudaStream_t s);
+                         cudaStream_t s, double *out = nullptr, long long out_cap = 0, uint32_t *sent_counts = nullptr);
+// slab.cu: x faces of a slab (fields and particles), see pic_slab_* in the C ABI
+void launch_slab_pack_fields(const GridP &g, int which, double *const F[3], double *to_left, double *to_right,
+                             cudaStream_t s);
+void launch_slab_unpack_fields(const GridP &g, int which, double *const F[3], const double *from_left,
+                               const double *from_right, cudaStream_t s);
+void launch_slab_append(const GridP &g, PartF64 &p, Counters *cnt, const double *in, long long n, long long capacity,
+                        int *err, cudaStream_t s);
 // Stable cell-key reorder (ReorderPrtlArr).  The payload is gathered into
 // `out`, after which the caller swaps `p` and `out`.
 void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Counters *cnt, SortScratch &sc,

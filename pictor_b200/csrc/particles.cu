@@ -357,14 +357,21 @@ __global__ void __launch_bounds__(256) k_exch_count(GridP g, PartF64 p, const lo
     if (threadIdx.x < 6) counts[(size_t)threadIdx.x * ntiles + blockIdx.x] = c[threadIdx.x];
 }
 
+// Slab form (g.x_external): what leaves through the x faces goes to the
+// neighbouring slabs instead: slots 0 and 1 (faces 2 and 1) fill the front of
+// the scan order, so their particles go to `out` at their scan position
+// (right-bound first, then left-bound; 8 doubles each: q, x, y, z, u, v, w,
+// flv, x already in the receiver's coordinates), and the y / z leavers are
+// appended after the local particles from scan position offs[2 ntiles] on.
 template <int DIMS>
 __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counters *cnt, const uint32_t *__restrict__ offs,
                                                       const uint32_t *__restrict__ total, size_t ntiles,
-                                                      long long capacity, int *err)
+                                                      long long capacity, int *err, double *out, long long out_cap)
 {
     __shared__ uint32_t wh[kTileWarps][6];
     const long long n = cnt->used;
-    if ((long long)*total + n > capacity) {
+    const uint32_t sent = g.x_external ? offs[2 * ntiles] : 0u;   // particles leaving through the x faces
+    if ((long long)(*total - sent) + n > capacity || (long long)sent > out_cap) {
         if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
         return;
     }
@@ -408,21 +415,33 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
             __syncwarp();
         }
         if (s >= 0) {
-            const long long d = n + pos;
             double pos3[3] = {p.x[i], p.y[i], p.z[i]};
             const int axis = (face - 1) >> 1;
             // CopyTransferPrtl subtracts the send list's shift, InsertPrtls adds
             // the receiving list's (subdomains.F90:720-740): low faces +len, high -len.
             if (face & 1) pos3[axis] = (pos3[axis] - 0.0) + len[axis];
             else pos3[axis] = (pos3[axis] - len[axis]) + 0.0;
-            p.q[d] = p.q[i];
-            p.x[d] = pos3[0];
-            p.y[d] = pos3[1];
-            p.z[d] = pos3[2];
-            p.u[d] = p.u[i];
-            p.v[d] = p.v[i];
-            p.w[d] = p.w[i];
-            p.flv[d] = p.flv[i];
+            if (g.x_external && s <= 1) {
+                double *o = out + 8 * (size_t)pos;
+                o[0] = p.q[i];
+                o[1] = pos3[0];
+                o[2] = pos3[1];
+                o[3] = pos3[2];
+                o[4] = p.u[i];
+                o[5] = p.v[i];
+                o[6] = p.w[i];
+                o[7] = (double)p.flv[i];
+            } else {
+                const long long d = n + (pos - sent);
+                p.q[d] = p.q[i];
+                p.x[d] = pos3[0];
+                p.y[d] = pos3[1];
+                p.z[d] = pos3[2];
+                p.u[d] = p.u[i];
+                p.v[d] = p.v[i];
+                p.w[d] = p.w[i];
+                p.flv[d] = p.flv[i];
+            }
             // RemovePrtl, loadprtlout.F90:164-181
             p.q[i] = 0.0;
             p.flv[i] = 0;
@@ -446,15 +465,16 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
     }
 }
 
-__global__ void k_exch_finish(Counters *cnt, const uint32_t *__restrict__ total, long long capacity)
+__global__ void k_exch_finish(Counters *cnt, const uint32_t *__restrict__ total, const uint32_t *__restrict__ sent,
+                              long long capacity)
 {
-    const long long t = (long long)*total;
+    const long long t = (long long)*total - (sent ? (long long)*sent : 0);
     cnt->append = t;
     if (cnt->used + t <= capacity) cnt->used += t;
 }
 
 void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch &sc, long long capacity, int *err,
-                         cudaStream_t s)
+                         cudaStream_t s, double *out, long long out_cap, uint32_t *sent_counts)
 {
     const size_t ntiles = sort_tiles(capacity);
     uint32_t *counts = sc.hist;  // 6 * ntiles <= 256 * ntiles
@@ -462,9 +482,16 @@ void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch 
     if (g.dims == 3) k_exch_count<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, &cnt->used, counts, ntiles);
     else k_exch_count<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, &cnt->used, counts, ntiles);
     scan_exclusive_u32(counts, counts, 6 * ntiles, sc.scan_tmp, total, s);
-    if (g.dims == 3) k_exch_scatter<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err);
-    else k_exch_scatter<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err);
-    k_exch_finish<<<1, 1, 0, s>>>(cnt, total, capacity);
+    if (g.dims == 3)
+        k_exch_scatter<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err, out, out_cap);
+    else
+        k_exch_scatter<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err, out, out_cap);
+    k_exch_finish<<<1, 1, 0, s>>>(cnt, total, g.x_external ? counts + 2 * ntiles : nullptr, capacity);
+    if (g.x_external && sent_counts) {
+        // right-bound (face 2, slot 0) and right + left-bound particle counts
+        cudaMemcpyAsync(sent_counts, counts + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(sent_counts + 1, counts + 2 * ntiles, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+    }
     count_launches(1);
     count_launches(2);
 }

@@ -54,6 +54,7 @@ class PicConfig:
     inc_axis: int = 1
     brick: tuple = (0, 0, 0)   # FP32 form: brick shape in cells, (0, 0, 0) = from the fill
     cyl_modes: int = 0         # cylindrical: 0 = theta-gridded field solve, 2 = modes m = 0, 1
+    slab_x: int = 0            # 1 = one slab of a domain split along x (pictor_b200.slab)
 
     def to_struct(self) -> _capi.Config:
         s = _capi.Config()
@@ -76,6 +77,7 @@ class PicConfig:
         for d in range(3):
             s.brick[d] = int(self.brick[d])
         s.cyl_modes = int(self.cyl_modes)
+        s.slab_x = int(self.slab_x)
         return s
 
     @property

@@ -1,0 +1,100 @@
+"""The slab decomposition along x on one GPU: S slab handles stepped with
+the x exchanges between them (device copies) against the single periodic
+domain on the same state.  Fields and particles agree to round-off: a slab
+holds positions in its own coordinates (x shifted by an integer, as each
+rank of the reference does), so positions round differently from the
+single domain's by a few ulps a step; currents sum in atomic order."""
+import numpy as np
+import pytest
+
+from ._util import grid_and_config, random_fields, random_particles, to_gpu_fields, to_gpu_particles
+
+pytestmark = pytest.mark.gpu
+
+
+def _sorted(p, lens):
+    """Live particles in a canonical order; a position within 1e-6 of the
+    upper periodic edge is taken at the lower one (a particle on the edge may
+    have wrapped in one run and not in the other)."""
+    m = np.asarray(p.flv) != 0
+    out = {k: np.asarray(getattr(p, k))[m].copy() for k in ("q", "x", "y", "z", "u", "v", "w", "flv")}
+    for k, L in zip(("x", "y", "z"), lens):
+        if L:
+            out[k][out[k] > 3.0 + L - 1e-6] -= L
+    o = np.lexsort((np.round(out["z"], 9), np.round(out["y"], 9), np.round(out["x"], 9), out["flv"]))
+    return {k: v[o] for k, v in out.items()}
+
+
+@pytest.mark.parametrize("dims,fdtd,nslabs", [(3, "yee", 2), (3, "lehe", 3), (2, "yee", 3), (2, "lehe", 2)])
+def test_slabs_track_single_domain(dims, fdtd, nslabs):
+    """6 steps (a reorder at step 3) of a 24-cell-wide domain as one
+    periodic domain and as 2 or 3 slabs, particles up to 0.8 per momentum
+    component, a fifth of them next to a face: the same live particles
+    (positions and momenta to 1e-11), E and B to 1e-11 of their scale."""
+    import torch
+
+    from pictor_b200 import Simulation
+    from pictor_b200.slab import join_interior, join_particles, local_domain, split_fields, split_particles
+
+    nx, ny, nz = 24, 8, 8
+    g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, fdtd=fdtd, capacity=1 << 15, reorder_period=3)
+    f = to_gpu_fields(random_fields(g, seed=71, scale=0.05))
+    p = to_gpu_particles(random_particles(g, n=6000, seed=72, umax=0.8))
+    with Simulation(cfg) as s:
+        s.load_particles(p)
+        s.load_fields(f)
+        s.step(6)
+        assert s.device_errors() == 0
+        ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096)
+    try:
+        for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
+            sl.sim.load_particles(ps)
+            sl.sim.load_fields(fs)
+        dom.step(6)
+        for sl in dom.slabs:
+            assert sl.sim.device_errors() == 0
+        got_p = join_particles([sl.sim.fetch_particles() for sl in dom.slabs], nx)
+        got_f = [sl.sim.fetch_fields(with_current=False) for sl in dom.slabs]
+    finally:
+        dom.close()
+    lens = (nx, ny, nz if dims == 3 else 0)
+    a, b = _sorted(got_p, lens), _sorted(ref_p, lens)
+    assert len(a["x"]) == len(b["x"])
+    np.testing.assert_array_equal(a["flv"], b["flv"])
+    np.testing.assert_array_equal(a["q"], b["q"])
+    for k, L in zip(("x", "y", "z"), lens):
+        d = a[k] - b[k]
+        if L:
+            d -= L * np.round(d / L)     # the same point on the periodic axis
+        assert np.abs(d).max() <= 1e-11, k
+    for k in ("u", "v", "w"):
+        np.testing.assert_allclose(a[k], b[k], rtol=0, atol=1e-11, err_msg=k)
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        ref = getattr(ref_f, n)[2:-3]
+        got = join_interior(got_f, n)
+        if dims == 3:
+            ref, got = ref[:, 2:-3, 2:-3], got[:, 2:-3, 2:-3]
+        else:
+            ref, got = ref[:, 2:-3, :], got[:, 2:-3, :]
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-11 * max(np.abs(ref).max(), 1e-30), err_msg=n)
+
+
+def test_slab_refuses_the_periodic_entry_points():
+    """A slab's step has exchanges between its phases: pic_step and the
+    single-domain particle exchange refuse it; the slab form is FP64
+    Cartesian without a current filter."""
+    from pictor_b200 import PicError, Simulation
+
+    g, cfg = grid_and_config(dims=2, nx=12, ny=8)
+    cfg.slab_x = 1
+    with Simulation(cfg) as s:
+        with pytest.raises(PicError):
+            s.step(1)
+        with pytest.raises(PicError):
+            s.exchange_particles()
+    for bad in (dict(precision="fp32"), dict(curr_filter=1)):
+        g, cfg = grid_and_config(dims=2, nx=12, ny=8, **bad)
+        cfg.slab_x = 1
+        with pytest.raises(PicError):
+            Simulation(cfg)
