@@ -73,27 +73,35 @@ __device__ __forceinline__ T lgz(const GridP &g, const T *F, long long c0)
 // UpdateBfieldHalf main loop (cyl_em_update.F90:66-83): i 4..mx-1, j 1..my-1,
 // k 1..mz-1 (Lehe: k 2..mz-2, see the oracle for why).  T = double is the
 // reference form; T = float the FP32 form (same expressions).
+// Each thread walks kCylZChunk consecutive k of its (i, j) column, so the
+// planes its stencil reads above and below were loaded by its CTA one step
+// earlier and come from L1 rather than L2.
+constexpr int kCylZChunk = 16;
+
 template <typename T, int FDTD>
 __global__ void k_cyl_bhalf(GridP g, CylP cp, const T *__restrict__ Ex, const T *__restrict__ Ey,
                             const T *__restrict__ Ez, T *Bx, T *By, T *Bz)
 {
     const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int k = (FDTD == PIC_FDTD_LEHE ? 2 : 1) + blockIdx.z;
     if (i > g.mx - 1 || j > g.my - 1) return;
+    const int k0 = (FDTD == PIC_FDTD_LEHE ? 2 : 1) + blockIdx.z * kCylZChunk;
+    const int k1 = min(k0 + kCylZChunk - 1, FDTD == PIC_FDTD_LEHE ? g.mz - 2 : g.mz - 1);
     const T h = (T)g.h, dtheta = (T)cp.dtheta;
     const T r = (((T)i - (T)3.0) + (T)cp.rmin) * (T)1.0;
     const T rp_half = r + (T)0.5 * (T)1.0, rp = r + (T)1.0;
-    const long long c0 = cidx(g, i, j, k);
     const long long sy = g.sy, sz = g.sz;
-    if (FDTD == PIC_FDTD_YEE) {
-        Bx[c0] = (Bx[c0] - (h * (ldd(Ez + c0 + sy) - ldd(Ez + c0))) / (r * dtheta)) + (h * (T)1.0) * (ldd(Ey + c0 + sz) - ldd(Ey + c0));
-        By[c0] = (By[c0] - (h * (T)1.0) * (ldd(Ex + c0 + sz) - ldd(Ex + c0))) + (h * (T)1.0) * (ldd(Ez + c0 + 1) - ldd(Ez + c0));
-        Bz[c0] = Bz[c0] - (h * (((T)1.0 * (rp * ldd(Ey + c0 + 1) - r * ldd(Ey + c0))) - (ldd(Ex + c0 + sy) - ldd(Ex + c0)) / dtheta)) / rp_half;
-    } else {
-        Bx[c0] = (Bx[c0] - (h * lgy(g, Ez, c0)) / (r * dtheta)) + (h * (T)1.0) * lgz(g, Ey, c0);
-        By[c0] = (By[c0] - (h * (T)1.0) * lgz(g, Ex, c0)) + (h * (T)1.0) * lgx(g, Ez, c0);
-        Bz[c0] = Bz[c0] - (h * (((T)1.0 * lgx1(g, Ey, c0, rp, r)) - lgy(g, Ex, c0) / dtheta)) / rp_half;
+    for (int k = k0; k <= k1; k++) {
+        const long long c0 = cidx(g, i, j, k);
+        if (FDTD == PIC_FDTD_YEE) {
+            Bx[c0] = (Bx[c0] - (h * (ldd(Ez + c0 + sy) - ldd(Ez + c0))) / (r * dtheta)) + (h * (T)1.0) * (ldd(Ey + c0 + sz) - ldd(Ey + c0));
+            By[c0] = (By[c0] - (h * (T)1.0) * (ldd(Ex + c0 + sz) - ldd(Ex + c0))) + (h * (T)1.0) * (ldd(Ez + c0 + 1) - ldd(Ez + c0));
+            Bz[c0] = Bz[c0] - (h * (((T)1.0 * (rp * ldd(Ey + c0 + 1) - r * ldd(Ey + c0))) - (ldd(Ex + c0 + sy) - ldd(Ex + c0)) / dtheta)) / rp_half;
+        } else {
+            Bx[c0] = (Bx[c0] - (h * lgy(g, Ez, c0)) / (r * dtheta)) + (h * (T)1.0) * lgz(g, Ey, c0);
+            By[c0] = (By[c0] - (h * (T)1.0) * lgz(g, Ex, c0)) + (h * (T)1.0) * lgx(g, Ez, c0);
+            Bz[c0] = Bz[c0] - (h * (((T)1.0 * lgx1(g, Ey, c0, rp, r)) - lgy(g, Ex, c0) / dtheta)) / rp_half;
+        }
     }
 }
 
@@ -249,7 +257,7 @@ void launch_cyl_bhalf(const GridP &g, T *const E[3], T *const B[3], cudaStream_t
 {
     const CylP cp = cyl_params(g);
     const int nk = g.fdtd == PIC_FDTD_LEHE ? g.mz - 3 : g.mz - 1;
-    const dim3 grid((g.mx - 4 + 31) / 32, (g.my - 1 + 7) / 8, nk), block(32, 8, 1);
+    const dim3 grid((g.mx - 4 + 31) / 32, (g.my - 1 + 3) / 4, (nk + kCylZChunk - 1) / kCylZChunk), block(32, 4, 1);
     if (g.fdtd == PIC_FDTD_LEHE)
         k_cyl_bhalf<T, PIC_FDTD_LEHE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
     else
