@@ -106,6 +106,40 @@ module pictor_b200_capi
       end function
    end interface
 
+   ! Slab form (cfg%reserved(5) = slab_x = 1): x faces exchanged by the host
+   ! between ranks; buffers are device addresses (a CUDA-aware MPI_Sendrecv
+   ! takes them as they are), see include/pictor_b200.h.
+   interface
+      integer(c_int) function pic_slab_face_len(h, n) bind(C, name="pic_slab_face_len")
+         import :: c_int, c_ptr, c_int64_t
+         type(c_ptr), value :: h
+         integer(c_int64_t), intent(out) :: n
+      end function
+      integer(c_int) function pic_slab_pack_fields(h, which, to_left, to_right) bind(C, name="pic_slab_pack_fields")
+         import :: c_int, c_ptr, c_int32_t
+         type(c_ptr), value :: h, to_left, to_right
+         integer(c_int32_t), value :: which
+      end function
+      integer(c_int) function pic_slab_unpack_fields(h, which, from_left, from_right) &
+            bind(C, name="pic_slab_unpack_fields")
+         import :: c_int, c_ptr, c_int32_t
+         type(c_ptr), value :: h, from_left, from_right
+         integer(c_int32_t), value :: which
+      end function
+      integer(c_int) function pic_slab_pack_particles(h, out, cap, n_right, n_left) &
+            bind(C, name="pic_slab_pack_particles")
+         import :: c_int, c_ptr, c_int64_t
+         type(c_ptr), value :: h, out
+         integer(c_int64_t), value :: cap
+         integer(c_int64_t), intent(out) :: n_right, n_left
+      end function
+      integer(c_int) function pic_slab_unpack_particles(h, in, n) bind(C, name="pic_slab_unpack_particles")
+         import :: c_int, c_ptr, c_int64_t
+         type(c_ptr), value :: h, in
+         integer(c_int64_t), value :: n
+      end function
+   end interface
+
    type(c_ptr), save :: pic_h = c_null_ptr
 
 contains
