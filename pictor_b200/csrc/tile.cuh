@@ -315,8 +315,17 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
         tb.lo[d] = lo[d];
         tb.C[d] = hi[d] - lo[d] + 1;
     }
-    const int NX = tb.C[0] + 1, NY = tb.C[1] + 1, NZ = DIMS == 3 ? tb.C[2] + 1 : 1;
+    const int NXn = tb.C[0] + 1, NY = tb.C[1] + 1, NZ = DIMS == 3 ? tb.C[2] + 1 : 1;
     const int JX = tb.C[0] + 3, JY = tb.C[1] + 3, JZ = DIMS == 3 ? tb.C[2] + 3 : 1;
+    // node rows padded to 8 mod 16 words of 16 / 8 bytes when the box still
+    // fits: the quarter-warps of the 16-byte gathers and the half-warps of
+    // the 8-byte ones then see the lanes of two y rows on disjoint banks (the
+    // lanes of a warp hold neighbouring cells of 4 rows of an 8-wide brick)
+    int NX = NXn;
+    if (DIMS == 3) {
+        const int NXp = NXn + ((8 - NXn) & 15);
+        if (6ll * NXp * NY * NZ + (WIDE ? 6ll : 3ll) * JX * JY * JZ <= (long long)bk.smem_floats) NX = NXp;
+    }
     const int nnode = NX * NY * NZ;
     tb.NX = NX;
     tb.NXY = NX * NY;
@@ -362,13 +371,18 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     }
     for (int q = tid; q < (WIDE ? 6 : 3) * tb.njc; q += kTileThreads) sJ[q] = 0;
     __syncthreads();
-    // stage node-averaged fields: node q = xx + NX*(yy + NY*zz); q/NX and
-    // r/NY by multiply-high (exact for q < 2^16, NX, NY < 2^16)
+    // stage node-averaged fields: node q = xx + NX*(yy + NY*zz) over the
+    // padded rows, the padding skipped (the threads of a warp then load one
+    // or two rows of the box; walking the real nodes densely spread a warp
+    // over three rows and its loads missed L1 four times as often: 27 % more
+    // time); q/NX and r/NY by multiply-high (exact for q < 2^16, NX, NY <
+    // 2^16)
     {
         const int sy = (int)g.sy, sz = (int)g.sz;
         const uint32_t mX = 0xffffffffu / (uint32_t)NX + 1u, mY = 0xffffffffu / (uint32_t)NY + 1u;
         for (int q = tid; q < nnode; q += kTileThreads) {
             const int r = (int)__umulhi((uint32_t)q, mX), xx = q - r * NX;
+            if (xx >= NXn) continue;   // row padding
             const int zz = (int)__umulhi((uint32_t)r, mY), yy = r - zz * NY;
             const int nd = ts.s_off[0][xx + 1] + ts.s_off[1][yy + 1] + (DIMS == 3 ? ts.s_off[2][zz + 1] : 0);
             float4 A;
