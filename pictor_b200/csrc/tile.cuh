@@ -374,9 +374,9 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     // stage node-averaged fields: node q = xx + NX*(yy + NY*zz) over the
     // padded rows, the padding skipped (the threads of a warp then load one
     // or two rows of the box; walking the real nodes densely spread a warp
-    // over three rows and its loads missed L1 four times as often: 27 % more
-    // time); q/NX and r/NY by multiply-high (exact for q < 2^16, NX, NY <
-    // 2^16)
+    // over three rows, its loads read 42 % more from L2 and the mover took
+    // 23 % longer); q/NX and r/NY by multiply-high (exact for q < 2^16, NX,
+    // NY < 2^16)
     {
         const int sy = (int)g.sy, sz = (int)g.sz;
         const uint32_t mX = 0xffffffffu / (uint32_t)NX + 1u, mY = 0xffffffffu / (uint32_t)NY + 1u;
