@@ -43,6 +43,10 @@ WORKLOADS = {
     # species, drift U(0.1, 0.9) c, spread U(0.01, 0.1) c, seed 2930 + run (pictor_b200.ensemble)
     "ensemble64": dict(dims=2, runs=64, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0, precision="fp32",
                        nx=256, ny=256, nz=1),
+    # the 2D FP64 Weibel configuration split along x into one slab per rank (strong scaling: the
+    # global grid fixed), the slabs exchanging their x faces over NCCL between the phases
+    "slab_weibel2d_fp64": dict(dims=2, nx=256, ny=256, nz=1, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0,
+                               precision="fp64"),
     # the differentiable 2D Weibel run: 128^2 cells, 8 particles per cell per species, drift +-0.4c, spread
     # 0.05c, 400 steps, checkpoints every 50, objective sum_t 1/2 sum |B_t|^2 (pictor_b200.adjoint)
     "adjoint128": dict(dims=2, nx=128, ny=128, nz=1, epc=8, drift=0.4, temp=0.005, c=0.45, c_ompe=2.0,
@@ -282,6 +286,70 @@ def cpu_sample(wl: dict, target_s: float = 12.0, threads: int | None = None):
     return {"value": p.used * n_steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "port",
             "sample": f"{'x'.join(map(str, (nx, ny, nz)[:dims]))} cells, {p.used} particles, {n_steps} steps "
                       f"(same physics and seed), FP64, C restatement of the reference CPU path with OpenMP"}
+
+
+def run_slab_bench(args, ws, rank, local, peak, peak_kind):
+    """--workload slab_weibel2d_fp64: the 2D FP64 Weibel grid split along x
+    into one slab per rank (pictor_b200.slab; x faces over NCCL, or copied
+    in place on one rank), each slab loaded by the device loader (seed +
+    rank); the whole step timed with CUDA events, max over ranks."""
+    import torch
+
+    from pictor_b200 import init_scale
+    from pictor_b200.slab import DistTransport, LocalTransport, Slab, SlabDomain
+
+    wl = WORKLOADS[args.workload]
+    sc = init_scale(wl["c"], wl["c_ompe"], wl["epc"])
+    cap = int(2 * wl["epc"] * wl["nx"] * wl["ny"] * 1.04 / ws) + (1 << 16)
+    from pictor_b200 import PicConfig
+
+    cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=1, dims=2, c=wl["c"], qi=sc["qi"], precision="fp64", capacity=cap,
+                    reorder_period=20)
+    dev = torch.device("cuda", local)
+    transport = DistTransport() if ws > 1 else LocalTransport()
+    dom = SlabDomain([Slab(cfg, rank, ws, dev)], transport)
+    sim = dom.slabs[0].sim
+    n_p = sim.init_weibel(wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], SEED + rank)
+    sim.reorder()
+    dom.step(args.warmup)
+    stream = torch.cuda.ExternalStream(sim.stream)
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    dom.step(args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    clk = clocks.stop()
+    ms = max_over_ranks(ws, e0.elapsed_time(e1))
+    n_tot = sum_over_ranks(ws, float(n_p))
+    d = sim.diagnostics(sc["masse"])
+    field = sum_over_ranks(ws, 0.5 * (d["B2"] + d["E2"]))
+    dom.close()
+    value = n_tot * args.steps / (ms * 1e-3)
+    step_bytes = n_tot * bytes_per_particle(2, "fp64") + wl["nx"] * wl["ny"] * 24 * 8
+    achieved = step_bytes / (ms / args.steps * 1e-3) / 1e9
+    cpu = None if (args.no_cpu or rank != 0) else cpu_sample(WORKLOADS["weibel2d_fp64"])
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "global_cells": [wl["nx"], wl["ny"]], "slabs": ws,
+                       "slab_cells_x": wl["nx"] // ws, "particles": int(n_tot), "parallelism": f"slab{ws}",
+                       "exchange": "NCCL point-to-point between ranks" if ws > 1 else "x faces copied on the rank",
+                       "l2": "particles and fields smaller than L2 at this size"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "traffic": None, "kernel": "whole slab step (phases and host-driven exchanges)",
+                         "peak_kind": peak_kind},
+            "cpu_baseline": cpu, "e2e": None, "gpu_launches": None, "clocks": clk,
+            "energy": {"field": field},
+        }
+        print(json.dumps(line))
+    return 0
 
 
 def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
@@ -706,6 +774,9 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
+    if args.workload == "slab_weibel2d_fp64":
+        peak, peak_kind = measured_peaks()
+        return run_slab_bench(args, ws, rank, local, peak, peak_kind)
     if args.workload.startswith("cyl_wake"):
         peak, peak_kind = measured_peaks()
         return run_cyl_bench(args, rank, local, peak, peak_kind)
