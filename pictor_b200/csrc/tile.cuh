@@ -4,8 +4,9 @@
 // A CTA moves the particles of one brick (bricks.cu groups them).  It stages
 // the node-averaged E and B of a box of cells around the brick in shared
 // memory (node_avg: each node once per brick instead of 8 times per
-// particle) and sums the brick's current in a shared box of 32-bit fixed
-// point words, added to the global J once at the end.  The box is the
+// particle) and sums the brick's current in a shared box of fixed-point
+// words (32-bit; 64-bit for the cylindrical form, whose weights span the
+// radius), added to the global J once at the end.  The box is the
 // bounding box, in cells relative to the brick centre and unwrapped across
 // periodic boundaries, of where the brick's particles were after the
 // previous step (Bricks::box, rewritten by the mover for the next step); a
