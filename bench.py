@@ -307,7 +307,7 @@ def run_slab_bench(args, ws, rank, local, peak, peak_kind):
                     reorder_period=20)
     dev = torch.device("cuda", local)
     transport = DistTransport() if ws > 1 else LocalTransport()
-    dom = SlabDomain([Slab(cfg, rank, ws, dev)], transport)
+    dom = SlabDomain([Slab(cfg, rank, ws, dev)], transport, queued=True)
     sim = dom.slabs[0].sim
     n_p = sim.init_weibel(wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], SEED + rank)
     sim.reorder()
@@ -340,7 +340,8 @@ def run_slab_bench(args, ws, rank, local, peak, peak_kind):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "global_cells": [wl["nx"], wl["ny"]], "slabs": ws,
                        "slab_cells_x": wl["nx"] // ws, "particles": int(n_tot), "parallelism": f"slab{ws}",
-                       "exchange": "NCCL point-to-point between ranks" if ws > 1 else "x faces copied on the rank",
+                       "exchange": ("NCCL point-to-point between ranks" if ws > 1 else "x faces copied on the rank")
+                       + ", ordered on the library's stream (one host wait per step, for the particle counts)",
                        "l2": "particles and fields smaller than L2 at this size"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": "whole slab step (phases and host-driven exchanges)",

@@ -158,6 +158,13 @@ int pic_filter_current(pic_handle *h);
    PIC_ERR_OVERFLOW if more than `cap` leave.  pic_step, pic_step_many and
    pic_exchange_particles refuse a slab. */
 int pic_slab_face_len(pic_handle *h, int64_t *n);
+/* sync = 0: the phase entry points (pic_update_b_half ... pic_reorder and
+   the pic_slab_* calls) only enqueue their work on the handle's stream
+   (pic_stream) and report launch errors; device errors surface at the next
+   synchronous call or pic_device_errors.  For a host that orders its own
+   transfers on that stream (the slab exchanges).  sync = 1 (the default)
+   waits for the queued work and returns its device errors. */
+int pic_set_sync(pic_handle *h, int32_t sync);
 int pic_slab_pack_fields(pic_handle *h, int32_t which, double *to_left, double *to_right);
 int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left, const double *from_right);
 int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_right, int64_t *n_left);

@@ -57,6 +57,8 @@ struct pic_handle {
     bool sorted = false;
     // slab form: device counts of the particles sent through the x faces
     uint32_t *slab_sent = nullptr;
+    // phase entry points wait for their work (pic_set_sync)
+    bool sync = true;
     std::vector<void *> allocs;
 };
 
@@ -173,6 +175,15 @@ int finish(pic_handle *h)
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(h->s));
     return check_device_errors(h);
+}
+
+// Finish a phase entry point: as finish, or, with pic_set_sync(h, 0), launch
+// errors only (the work stays queued on the handle's stream).
+int finish_phase(pic_handle *h)
+{
+    if (h->sync) return finish(h);
+    CK(cudaGetLastError());
+    return PIC_OK;
 }
 
 template <typename T>
@@ -1225,14 +1236,14 @@ int pic_update_b_half(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_bhalf<double>(h->g, E, B, h->s);
     }
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_reset_current(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     for (int k = 0; k < 3; k++) CK(cudaMemsetAsync(h->J[k], 0, field_bytes(h), h->s));
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_move_deposit(pic_handle *h)
@@ -1262,14 +1273,14 @@ int pic_move_deposit(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_move_deposit_f64(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s);
     }
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_exchange_particles(pic_handle *h)
 {
     if (!h || h->g.x_external) return PIC_ERR_INVALID;   // a slab exchanges through pic_slab_pack_particles
     if (!h->fp32) launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s);
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_update_e(pic_handle *h)
@@ -1295,7 +1306,7 @@ int pic_update_e(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_efield<double>(h->g, 0, E, B, J, h->s);
     }
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_fold_current(pic_handle *h)
@@ -1318,7 +1329,7 @@ int pic_fold_current(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_fold<double>(h->g, J, h->s);
     }
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_filter_current(pic_handle *h)
@@ -1339,7 +1350,7 @@ int pic_filter_current(pic_handle *h)
             launch_filter<double>(h->g, J, (double *)h->Jtmp, h->s);
         }
     }
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_add_current(pic_handle *h)
@@ -1365,7 +1376,14 @@ int pic_add_current(pic_handle *h)
         field_ptrs(h, E, B, J);
         launch_efield<double>(h->g, 2, E, B, J, h->s);
     }
-    return finish(h);
+    return finish_phase(h);
+}
+
+int pic_set_sync(pic_handle *h, int32_t sync)
+{
+    if (!h) return PIC_ERR_INVALID;
+    h->sync = sync != 0;
+    return h->sync ? finish(h) : PIC_OK;
 }
 
 int pic_slab_face_len(pic_handle *h, int64_t *n)
@@ -1381,7 +1399,7 @@ int pic_slab_pack_fields(pic_handle *h, int32_t which, double *to_left, double *
     double *E[3], *B[3], *J[3];
     field_ptrs(h, E, B, J);
     launch_slab_pack_fields(h->g, which, which == 0 ? E : which == 1 ? B : J, to_left, to_right, h->s);
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left, const double *from_right)
@@ -1390,7 +1408,7 @@ int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left
     double *E[3], *B[3], *J[3];
     field_ptrs(h, E, B, J);
     launch_slab_unpack_fields(h->g, which, which == 0 ? E : which == 1 ? B : J, from_left, from_right, h->s);
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_right, int64_t *n_left)
@@ -1399,7 +1417,8 @@ int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_
     launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s, out, cap, h->slab_sent);
     uint32_t sent[2] = {0, 0};
     CK(cudaMemcpyAsync(sent, h->slab_sent, sizeof(sent), cudaMemcpyDeviceToHost, h->s));
-    const int r = finish(h);
+    CK(cudaStreamSynchronize(h->s));   // the counts size the transfers, in either mode
+    const int r = finish_phase(h);
     *n_right = sent[0];
     *n_left = (int64_t)sent[1] - (int64_t)sent[0];
     return r;
@@ -1409,7 +1428,7 @@ int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n)
 {
     if (!h || !h->g.x_external || n < 0 || (n > 0 && !in)) return PIC_ERR_INVALID;
     launch_slab_append(h->g, h->p64[h->cur], h->cnt, in, n, h->capacity, h->err, h->s);
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_reorder(pic_handle *h)
@@ -1419,7 +1438,7 @@ int pic_reorder(pic_handle *h)
     else launch_reorder_f64(h->g, h->p64[h->cur], h->p64[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
     h->cur ^= 1;
     set_sorted(h, h->fp32);
-    return finish(h);
+    return finish_phase(h);
 }
 
 int pic_set_step(pic_handle *h, int64_t t)

@@ -241,6 +241,11 @@ class Simulation:
     reset_current = ResetCurrentGPU
     reorder = ReorderPrtlGPU
 
+    def set_sync(self, sync: bool = True) -> None:
+        """False: the phase calls only enqueue their work on the handle's
+        stream (``stream``); True (the default) waits and checks device errors."""
+        check(self.L.pic_set_sync(self.h, 1 if sync else 0), "pic_set_sync")
+
     def step(self, nsteps: int = 1) -> None:
         """nsteps full steps of MAIN.F90:42-284 as one CUDA graph per step."""
         check(self.L.pic_step(self.h, int(nsteps)), "pic_step")

@@ -249,27 +249,56 @@ class Slab:
 class SlabDomain:
     """The slabs of this process and the transport between them: MAIN.F90's
     step with the x exchanges (all slabs of the ring in one process with a
-    LocalTransport, or one slab per rank with a DistTransport)."""
+    LocalTransport, or one slab per rank with a DistTransport).
+
+    queued=True: the library's phase calls only enqueue their work; a single
+    slab's transfers run on its handle's stream (NCCL ordered after the pack
+    kernels, the unpack kernels after the transfers), so a step waits on the
+    host only for the particle counts; several slabs in one process
+    synchronise the device around each exchange instead of after every
+    call."""
 
     E, B, J = 0, 1, 2
 
-    def __init__(self, slabs: list[Slab], transport):
+    def __init__(self, slabs: list[Slab], transport, queued: bool = False):
+        import torch
+
         self.slabs = slabs
         self.transport = transport
         self.t = 0
+        self.queued = queued
+        self._stream = None
+        if queued:
+            for s in slabs:
+                s.sim.set_sync(False)
+            if len(slabs) == 1 and slabs[0].device.type == "cuda":
+                self._stream = torch.cuda.ExternalStream(slabs[0].sim.stream, device=slabs[0].device)
 
-    def _sync(self):
+    def _device_sync(self):
         import torch
 
         if self.slabs and self.slabs[0].device.type == "cuda":
             torch.cuda.synchronize(self.slabs[0].device)
 
+    def _transfer(self, fn):
+        """Run a transfer: on the slab's stream when queued with one slab,
+        else between device synchronisations."""
+        import torch
+
+        if self._stream is not None:
+            with torch.cuda.stream(self._stream):
+                return fn()
+        if self.queued:
+            self._device_sync()
+        r = fn()
+        self._device_sync()
+        return r
+
     def exchange_fields(self, which: int):
         for s in self.slabs:
             s.pack_fields(which)
-        self.transport.exchange([(s.to_left, s.to_right) for s in self.slabs],
-                                [(s.from_left, s.from_right) for s in self.slabs])
-        self._sync()
+        self._transfer(lambda: self.transport.exchange([(s.to_left, s.to_right) for s in self.slabs],
+                                                       [(s.from_left, s.from_right) for s in self.slabs]))
         for s in self.slabs:
             s.unpack_fields(which)
 
@@ -280,9 +309,8 @@ class SlabDomain:
         outs = [(tl, tr) for (tl, _), (tr, _) in packed]
         counts = [(nl, nr) for (_, nl), (_, nr) in packed]
         dev = self.slabs[0].device
-        got = exchange_particle_buffers(self.transport, outs, counts,
-                                        lambda n: torch.empty(P_WORDS * n, dtype=torch.float64, device=dev))
-        self._sync()
+        got = self._transfer(lambda: exchange_particle_buffers(
+            self.transport, outs, counts, lambda n: torch.empty(P_WORDS * n, dtype=torch.float64, device=dev)))
         # AppendParticles order: what came from the left, then from the right
         for s, ((fl, nl), (fr, nr)) in zip(self.slabs, got):
             s.unpack_particles(fl, nl)
@@ -317,13 +345,14 @@ class SlabDomain:
             s.close()
 
 
-def local_domain(cfg: PicConfig, nslabs: int, device=None, out_capacity: int | None = None) -> SlabDomain:
+def local_domain(cfg: PicConfig, nslabs: int, device=None, out_capacity: int | None = None,
+                 queued: bool = False) -> SlabDomain:
     """All slabs of a domain split along x in this process (one GPU)."""
-    return SlabDomain([Slab(cfg, s, nslabs, device, out_capacity) for s in range(nslabs)], LocalTransport())
+    return SlabDomain([Slab(cfg, s, nslabs, device, out_capacity) for s in range(nslabs)], LocalTransport(), queued)
 
 
-def distributed_slab(cfg: PicConfig, group=None, out_capacity: int | None = None) -> SlabDomain:
+def distributed_slab(cfg: PicConfig, group=None, out_capacity: int | None = None, queued: bool = True) -> SlabDomain:
     """This rank's slab of a domain split along x over the ranks of the
     process group (one GPU per rank, the current CUDA device)."""
     t = DistTransport(group)
-    return SlabDomain([Slab(cfg, t.rank, t.world, None, out_capacity)], t)
+    return SlabDomain([Slab(cfg, t.rank, t.world, None, out_capacity)], t, queued)

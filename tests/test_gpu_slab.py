@@ -25,12 +25,15 @@ def _sorted(p, lens):
     return {k: v[o] for k, v in out.items()}
 
 
-@pytest.mark.parametrize("dims,fdtd,nslabs", [(3, "yee", 2), (3, "lehe", 3), (2, "yee", 3), (2, "lehe", 2)])
-def test_slabs_track_single_domain(dims, fdtd, nslabs):
+@pytest.mark.parametrize("dims,fdtd,nslabs,queued", [(3, "yee", 2, False), (3, "lehe", 3, True), (2, "yee", 3, False),
+                                                      (2, "lehe", 2, True), (3, "yee", 1, True)])
+def test_slabs_track_single_domain(dims, fdtd, nslabs, queued):
     """6 steps (a reorder at step 3) of a 24-cell-wide domain as one
-    periodic domain and as 2 or 3 slabs, particles up to 0.8 per momentum
-    component, a fifth of them next to a face: the same live particles
-    (positions and momenta to 1e-11), E and B to 1e-11 of their scale."""
+    periodic domain and as 1, 2 or 3 slabs (the library's phase calls
+    waiting for their work, or queued with the exchanges ordered on the
+    streams), particles up to 0.8 per momentum component, a fifth of them
+    next to a face: the same live particles (positions and momenta to
+    1e-11), E and B to 1e-11 of their scale."""
     import torch
 
     from pictor_b200 import Simulation
@@ -46,7 +49,7 @@ def test_slabs_track_single_domain(dims, fdtd, nslabs):
         s.step(6)
         assert s.device_errors() == 0
         ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
-    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096, queued=queued)
     try:
         for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
             sl.sim.load_particles(ps)
