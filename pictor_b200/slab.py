@@ -214,8 +214,10 @@ class Slab:
         check(self.sim.L.pic_slab_face_len(self.sim.h, C.byref(n)), "pic_slab_face_len")
         mk = lambda: torch.zeros(n.value, dtype=torch.float64, device=self.device)   # noqa: E731
         self.to_left, self.to_right, self.from_left, self.from_right = mk(), mk(), mk(), mk()
-        # particles leaving through the x faces in one step, at most
-        self.out_capacity = int(out_capacity or max(4096, self.cfg.capacity // 8))
+        # particles leaving through the x faces in one step, at most: those of
+        # the two edge layers (a move is below one cell), capacity / w per
+        # layer at the configured fill, with a factor 2 for the fluctuations
+        self.out_capacity = int(out_capacity or 4 * (self.cfg.capacity // self.w) + 4096)
         self.out = torch.zeros(P_WORDS * self.out_capacity, dtype=torch.float64, device=self.device)
 
     def close(self):
