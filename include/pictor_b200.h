@@ -137,6 +137,18 @@ int pic_reorder(pic_handle *h);            /* ReorderPrtlGPU / ReorderPrtlArr (m
 /* Current filter passes (smoothen_current, current.F90:19-163). */
 int pic_filter_current(pic_handle *h);
 
+/* Walls along x (src/bc/bc_reflect.F90 on one rank), for setups whose
+   bc_face(1) (side 0, left) or bc_face(2) (side 1, right) is a wall at
+   `pos` cells from the first interior cell.  pic_bc_reflect_x:
+   RefBC_Prtl_Left/Right — particles beyond the wall mirrored with u
+   reversed, the current beyond it folded back (EnforceBC_PostMovDep,
+   MAIN.F90:77: after pic_move_deposit, before pic_exchange_particles).
+   pic_bc_conducting_x: CondBC_Fld_Left/Right — Ey, Ez zeroed beyond the
+   wall (EnforceBC_Final, MAIN.F90:209: after pic_add_current).  The FP64
+   Cartesian single domain; the phase API, not pic_step. */
+int pic_bc_reflect_x(pic_handle *h, int32_t side, double pos);
+int pic_bc_conducting_x(pic_handle *h, int32_t side, double pos);
+
 /* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
    with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:
    13-106, comm_prtl.F90:11-66 across ranks); the caller moves the buffers

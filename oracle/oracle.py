@@ -91,6 +91,10 @@ def _declare(L: C.CDLL) -> None:
     L.orc_exchange_particles.argtypes = [P(Grid), P(_Particles)]
     L.orc_exchange_particles.restype = C.c_int
     L.orc_reorder.argtypes = [P(Grid), P(_Particles), P(C.c_int64)]
+    for fn in ("orc_refl_prtl_left", "orc_refl_prtl_right"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_double]
+    for fn in ("orc_cond_fld_left", "orc_cond_fld_right"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -256,6 +260,18 @@ class Oracle:
 
     def exchange_particles(self) -> int:
         return self._call_p(self.L.orc_exchange_particles)
+
+    def reflect_particles_x(self, side: int, pos: float):
+        """RefBC_Prtl_Left (side 0) / RefBC_Prtl_Right (side 1) at wall pos."""
+        fs = self.f.struct()
+        fn = self.L.orc_refl_prtl_left if side == 0 else self.L.orc_refl_prtl_right
+        self._call_p(fn, C.byref(fs), float(pos))
+
+    def conducting_x(self, side: int, pos: float):
+        """CondBC_Fld_Left (side 0) / CondBC_Fld_Right (side 1) at wall pos."""
+        fs = self.f.struct()
+        fn = self.L.orc_cond_fld_left if side == 0 else self.L.orc_cond_fld_right
+        fn(C.byref(self.g), C.byref(fs), float(pos))
 
     def reorder(self) -> np.ndarray:
         perm = np.zeros(max(self.p.used, 1), dtype=np.int64)

@@ -723,6 +723,90 @@ void orc_reorder(const orc_grid *g, orc_particles *p, int64_t *perm)
 }
 
 /* ------------------------------------------------------------------------- */
+/* Walls along x on one rank (xborders(procxind) = 0): src/bc/bc_reflect.F90  */
+/* ------------------------------------------------------------------------- */
+/* Add (sign +1) or subtract (-1) the x layer `from` onto the layer `to` of F
+   over every (j, k), then zero `from` (whole planes, ghosts included). */
+static void fold_x_layer(const orc_grid *g, double *F, int to, int from, double sign)
+{
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= g->my; j++) {
+            if (sign > 0) F[ID(g, to, j, k)] = F[ID(g, to, j, k)] + F[ID(g, from, j, k)];
+            else F[ID(g, to, j, k)] = F[ID(g, to, j, k)] - F[ID(g, from, j, k)];
+        }
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= g->my; j++) F[ID(g, from, j, k)] = 0.0;
+}
+
+/* RefBC_Prtl_Left (bc_reflect.F90:146-155), RefPrtlLeft (:164-176),
+   ReflCurrentLeft (:195-213). */
+void orc_refl_prtl_left(const orc_grid *g, orc_particles *p, orc_fields *f, double pos)
+{
+    const double xmin = pos - 0.0 + 3;
+    if (xmin > 1)
+        for (int64_t n = 0; n < p->used; n++)
+            if (p->flv[n] != 0 && p->x[n] < xmin) {
+                p->u[n] = -p->u[n];
+                p->x[n] = 2.0 * xmin - p->x[n];
+            }
+    int ind = (int)ceil(pos - 0.0 + 3);
+    if (ind >= 2 && ind <= g->mx) {
+        fold_x_layer(g, f->Jy, ind, ind - 1, 1.0);
+        fold_x_layer(g, f->Jz, ind, ind - 1, 1.0);
+    }
+    ind = (int)ceil(pos - 0.5 - 0.0 + 3);
+    if (ind >= 2 && ind <= g->mx) fold_x_layer(g, f->Jx, ind, ind - 1, -1.0);
+}
+
+/* RefBC_Prtl_Right (bc_reflect.F90:135-144), RefPrtlRight (:178-190),
+   ReflCurrentRight (:215-237); the wall of bc_face(2) is `pos` itself. */
+void orc_refl_prtl_right(const orc_grid *g, orc_particles *p, orc_fields *f, double pos)
+{
+    const double xmax = pos - 0.0 + 3;
+    if (xmax < g->mx - 1)
+        for (int64_t n = 0; n < p->used; n++)
+            if (p->flv[n] != 0 && p->x[n] > xmax) {
+                p->u[n] = -p->u[n];
+                p->x[n] = 2.0 * xmax - p->x[n];
+            }
+    int ind = (int)floor(pos - 0.0 + 3);
+    if (ind >= 1 && ind <= g->mx - 1) {
+        fold_x_layer(g, f->Jy, ind, ind + 1, 1.0);
+        fold_x_layer(g, f->Jz, ind, ind + 1, 1.0);
+    }
+    ind = (int)floor(pos - 0.5 - 0.0 + 3);
+    if (ind >= 1 && ind <= g->mx - 1) fold_x_layer(g, f->Jx, ind, ind + 1, -1.0);
+}
+
+/* CondBC_Fld_Left (bc_reflect.F90:58-72): Ey, Ez = 0 on x layers 1..floor(pos+3). */
+void orc_cond_fld_left(const orc_grid *g, orc_fields *f, double pos)
+{
+    int xl = (int)floor(pos - 0.0 + 3);
+    if (xl < 1) return;
+    if (xl > g->mx) xl = g->mx;
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= g->my; j++)
+            for (int i = 1; i <= xl; i++) {
+                f->Ey[ID(g, i, j, k)] = 0.0;
+                f->Ez[ID(g, i, j, k)] = 0.0;
+            }
+}
+
+/* CondBC_Fld_Right (bc_reflect.F90:43-56): Ey, Ez = 0 on x layers ceiling(pos+3)..mx. */
+void orc_cond_fld_right(const orc_grid *g, orc_fields *f, double pos)
+{
+    int xr = (int)ceil(pos - 0.0 + 3);
+    if (xr > g->mx) return;
+    if (xr < 1) xr = 1;
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= g->my; j++)
+            for (int i = xr; i <= g->mx; i++) {
+                f->Ey[ID(g, i, j, k)] = 0.0;
+                f->Ez[ID(g, i, j, k)] = 0.0;
+            }
+}
+
+/* ------------------------------------------------------------------------- */
 /* One time step, src/MAIN.F90:42-284                                        */
 /* ------------------------------------------------------------------------- */
 int orc_step_filtered(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period, int curr_filter)

@@ -83,6 +83,15 @@ void orc_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f);
 /* loadprtlout.F90 LoadPrtlOutliers + comm_prtl.F90 AppendParticles on a single
    periodic rank.  Returns 0, or -1 when the particle capacity is exceeded. */
 int orc_exchange_particles(const orc_grid *g, orc_particles *p);
+/* Walls along x on one rank (xborders = 0), src/bc/bc_reflect.F90: pos in
+   cells from the first interior cell (bc_face%pos_prtl / pos_fld).
+   RefBC_Prtl_Left/Right (:135-155): specular reflection of the particles
+   beyond the wall and ReflCurrentLeft/Right (:195-237) of the current;
+   CondBC_Fld_Left/Right (:43-72): tangential E zeroed beyond the wall. */
+void orc_refl_prtl_left(const orc_grid *g, orc_particles *p, orc_fields *f, double pos);
+void orc_refl_prtl_right(const orc_grid *g, orc_particles *p, orc_fields *f, double pos);
+void orc_cond_fld_left(const orc_grid *g, orc_fields *f, double pos);
+void orc_cond_fld_right(const orc_grid *g, orc_fields *f, double pos);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

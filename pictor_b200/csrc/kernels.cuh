@@ -134,6 +134,10 @@ size_t scan_tmp_len(size_t n);
 // doubles) and sent_counts (device) receives {right-bound, right + left-bound}.
 void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch &sc, long long capacity, int *err,
                          cudaStream_t s, double *out = nullptr, long long out_cap = 0, uint32_t *sent_counts = nullptr);
+// bc.cu: walls along x (src/bc/bc_reflect.F90 on one rank), FP64 reference layout
+void launch_wall_reflect(const GridP &g, PartF64 &p, const Counters *cnt, double *const J[3], int side, double pos,
+                         long long capacity, cudaStream_t s);
+void launch_wall_conducting(const GridP &g, double *const E[3], int side, double pos, cudaStream_t s);
 // slab.cu: x faces of a slab (fields and particles), see pic_slab_* in the C ABI
 void launch_slab_pack_fields(const GridP &g, int which, double *const F[3], double *to_left, double *to_right,
                              cudaStream_t s);

@@ -106,6 +106,23 @@ module pictor_b200_capi
       end function
    end interface
 
+   ! Walls along x: EnforceBC_PostMovDep / EnforceBC_Final (bc.F90) call
+   ! these for bc_face(1:2) of type 'refl' / 'cond'; side 0 = left.
+   interface
+      integer(c_int) function pic_bc_reflect_x(h, side, pos) bind(C, name="pic_bc_reflect_x")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+      integer(c_int) function pic_bc_conducting_x(h, side, pos) bind(C, name="pic_bc_conducting_x")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+   end interface
+
    ! Slab form (cfg%reserved(5) = slab_x = 1): x faces exchanged by the host
    ! between ranks; buffers are device addresses (a CUDA-aware MPI_Sendrecv
    ! takes them as they are), see include/pictor_b200.h.

@@ -231,6 +231,15 @@ class Simulation:
         form); the FP32 form groups the particles by brick instead."""
         check(self.L.pic_reorder(self.h), "pic_reorder")
 
+    def RefBC_Prtl_x(self, side: int, pos: float):
+        """RefBC_Prtl_Left (side 0) / RefBC_Prtl_Right (side 1), bc_reflect.F90:135-237:
+        particles beyond the wall at pos mirrored, the current beyond it folded back."""
+        check(self.L.pic_bc_reflect_x(self.h, int(side), float(pos)), "pic_bc_reflect_x")
+
+    def CondBC_Fld_x(self, side: int, pos: float):
+        """CondBC_Fld_Left (side 0) / CondBC_Fld_Right (side 1), bc_reflect.F90:43-72."""
+        check(self.L.pic_bc_conducting_x(self.h, int(side), float(pos)), "pic_bc_conducting_x")
+
     update_b_half = UpdateBfieldHalfGPU
     move_deposit = MoveDepositPrtlGPU
     exchange_particles = ExchangePrtlGPU
