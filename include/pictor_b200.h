@@ -148,6 +148,11 @@ int pic_filter_current(pic_handle *h);
    Cartesian single domain; the phase API, not pic_step. */
 int pic_bc_reflect_x(pic_handle *h, int32_t side, double pos);
 int pic_bc_conducting_x(pic_handle *h, int32_t side, double pos);
+/* The y faces (bc_face(3) side 0 bottom, bc_face(4) side 1 top):
+   RefBC_Prtl_Bottom/Top with their current fold (bc_reflect.F90:79-128) and
+   CondBC_Fld_Bottom/Top (Ex, Ez zeroed, :11-41); also on a slab. */
+int pic_bc_reflect_y(pic_handle *h, int32_t side, double pos);
+int pic_bc_conducting_y(pic_handle *h, int32_t side, double pos);
 
 /* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
    with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:

@@ -95,6 +95,10 @@ def _declare(L: C.CDLL) -> None:
         getattr(L, fn).argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_double]
     for fn in ("orc_cond_fld_left", "orc_cond_fld_right"):
         getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
+    for fn in ("orc_refl_prtl_bottom", "orc_refl_prtl_top"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_double]
+    for fn in ("orc_cond_fld_bottom", "orc_cond_fld_top"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -271,6 +275,18 @@ class Oracle:
         """CondBC_Fld_Left (side 0) / CondBC_Fld_Right (side 1) at wall pos."""
         fs = self.f.struct()
         fn = self.L.orc_cond_fld_left if side == 0 else self.L.orc_cond_fld_right
+        fn(C.byref(self.g), C.byref(fs), float(pos))
+
+    def reflect_particles_y(self, side: int, pos: float):
+        """RefBC_Prtl_Bottom (side 0) / RefBC_Prtl_Top (side 1) at wall pos."""
+        fs = self.f.struct()
+        fn = self.L.orc_refl_prtl_bottom if side == 0 else self.L.orc_refl_prtl_top
+        self._call_p(fn, C.byref(fs), float(pos))
+
+    def conducting_y(self, side: int, pos: float):
+        """CondBC_Fld_Bottom (side 0) / CondBC_Fld_Top (side 1) at wall pos."""
+        fs = self.f.struct()
+        fn = self.L.orc_cond_fld_bottom if side == 0 else self.L.orc_cond_fld_top
         fn(C.byref(self.g), C.byref(fs), float(pos))
 
     def reorder(self) -> np.ndarray:

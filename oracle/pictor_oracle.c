@@ -806,6 +806,93 @@ void orc_cond_fld_right(const orc_grid *g, orc_fields *f, double pos)
             }
 }
 
+/* y layer version of fold_x_layer: F(:,to,:) +-= F(:,from,:); F(:,from,:) = 0. */
+static void fold_y_layer(const orc_grid *g, double *F, int to, int from, double sign)
+{
+    for (int k = 1; k <= g->mz; k++)
+        for (int i = 1; i <= g->mx; i++) {
+            if (sign > 0) F[ID(g, i, to, k)] = F[ID(g, i, to, k)] + F[ID(g, i, from, k)];
+            else F[ID(g, i, to, k)] = F[ID(g, i, to, k)] - F[ID(g, i, from, k)];
+        }
+    for (int k = 1; k <= g->mz; k++)
+        for (int i = 1; i <= g->mx; i++) F[ID(g, i, from, k)] = 0.0;
+}
+
+/* RefBC_Prtl_Bottom (bc_reflect.F90:106-128): y mirrored below ymin = pos + 3,
+   the current of layer W - 1 (W = int(ymin)) folded onto W. */
+void orc_refl_prtl_bottom(const orc_grid *g, orc_particles *p, orc_fields *f, double pos)
+{
+    const double ymin = pos - 0.0 + 3;
+    const int W = (int)ymin;
+    if (ymin > 1)
+        for (int64_t n = 0; n < p->used; n++)
+            if (p->flv[n] != 0 && p->y[n] < ymin) {
+                p->v[n] = -p->v[n];
+                p->y[n] = 2.0 * ymin - p->y[n];
+            }
+    if (W >= 3 && W <= g->my - 2) {
+        fold_y_layer(g, f->Jx, W, W - 1, 1.0);
+        fold_y_layer(g, f->Jy, W, W - 1, -1.0);
+        fold_y_layer(g, f->Jz, W, W - 1, 1.0);
+    }
+}
+
+/* RefBC_Prtl_Top (bc_reflect.F90:79-104): y mirrored above ymax = pos + 3,
+   Jx, Jz of layer W + 1 folded onto W and Jy of W onto W - 1 (W = int(ymax)). */
+void orc_refl_prtl_top(const orc_grid *g, orc_particles *p, orc_fields *f, double pos)
+{
+    const double ymax = pos - 0.0 + 3;
+    const int W = (int)ymax;
+    if (ymax < g->my - 1)
+        for (int64_t n = 0; n < p->used; n++)
+            if (p->flv[n] != 0 && p->y[n] > ymax) {
+                p->v[n] = -p->v[n];
+                p->y[n] = 2.0 * ymax - p->y[n];
+            }
+    if (W >= 2 && W <= g->my - 2) {
+        for (int k = 1; k <= g->mz; k++)
+            for (int i = 1; i <= g->mx; i++) {
+                f->Jx[ID(g, i, W, k)] = f->Jx[ID(g, i, W, k)] + f->Jx[ID(g, i, W + 1, k)];
+                f->Jy[ID(g, i, W - 1, k)] = f->Jy[ID(g, i, W - 1, k)] - f->Jy[ID(g, i, W, k)];
+                f->Jz[ID(g, i, W, k)] = f->Jz[ID(g, i, W, k)] + f->Jz[ID(g, i, W + 1, k)];
+            }
+        for (int k = 1; k <= g->mz; k++)
+            for (int i = 1; i <= g->mx; i++) {
+                f->Jx[ID(g, i, W + 1, k)] = 0.0;
+                f->Jy[ID(g, i, W, k)] = 0.0;
+                f->Jz[ID(g, i, W + 1, k)] = 0.0;
+            }
+    }
+}
+
+/* CondBC_Fld_Bottom (bc_reflect.F90:27-41): Ex, Ez = 0 on y layers 1..floor(pos+3). */
+void orc_cond_fld_bottom(const orc_grid *g, orc_fields *f, double pos)
+{
+    int yl = (int)floor(pos - 0.0 + 3);
+    if (yl < 1) return;
+    if (yl > g->my) yl = g->my;
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= yl; j++)
+            for (int i = 1; i <= g->mx; i++) {
+                f->Ex[ID(g, i, j, k)] = 0.0;
+                f->Ez[ID(g, i, j, k)] = 0.0;
+            }
+}
+
+/* CondBC_Fld_Top (bc_reflect.F90:11-25): Ex, Ez = 0 on y layers ceiling(pos+3)..my. */
+void orc_cond_fld_top(const orc_grid *g, orc_fields *f, double pos)
+{
+    int yl = (int)ceil(pos - 0.0 + 3);
+    if (yl > g->my) return;
+    if (yl < 1) yl = 1;
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = yl; j <= g->my; j++)
+            for (int i = 1; i <= g->mx; i++) {
+                f->Ex[ID(g, i, j, k)] = 0.0;
+                f->Ez[ID(g, i, j, k)] = 0.0;
+            }
+}
+
 /* ------------------------------------------------------------------------- */
 /* One time step, src/MAIN.F90:42-284                                        */
 /* ------------------------------------------------------------------------- */

@@ -92,6 +92,12 @@ void orc_refl_prtl_left(const orc_grid *g, orc_particles *p, orc_fields *f, doub
 void orc_refl_prtl_right(const orc_grid *g, orc_particles *p, orc_fields *f, double pos);
 void orc_cond_fld_left(const orc_grid *g, orc_fields *f, double pos);
 void orc_cond_fld_right(const orc_grid *g, orc_fields *f, double pos);
+/* The y faces (bc_reflect.F90:11-41 CondBC_Fld_Top/Bottom, :79-128
+   RefBC_Prtl_Top/Bottom with their own current fold). */
+void orc_refl_prtl_bottom(const orc_grid *g, orc_particles *p, orc_fields *f, double pos);
+void orc_refl_prtl_top(const orc_grid *g, orc_particles *p, orc_fields *f, double pos);
+void orc_cond_fld_bottom(const orc_grid *g, orc_fields *f, double pos);
+void orc_cond_fld_top(const orc_grid *g, orc_fields *f, double pos);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

@@ -1399,6 +1399,24 @@ int pic_bc_conducting_x(pic_handle *h, int32_t side, double pos)
     return finish_phase(h);
 }
 
+int pic_bc_reflect_y(pic_handle *h, int32_t side, double pos)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || (side != 0 && side != 1)) return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_wall_reflect_y(h->g, h->p64[h->cur], h->cnt, J, side, pos, h->capacity, h->s);
+    return finish_phase(h);
+}
+
+int pic_bc_conducting_y(pic_handle *h, int32_t side, double pos)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || (side != 0 && side != 1)) return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_wall_conducting_y(h->g, E, side, pos, h->s);
+    return finish_phase(h);
+}
+
 int pic_set_sync(pic_handle *h, int32_t sync)
 {
     if (!h) return PIC_ERR_INVALID;

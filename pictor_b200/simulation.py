@@ -240,6 +240,14 @@ class Simulation:
         """CondBC_Fld_Left (side 0) / CondBC_Fld_Right (side 1), bc_reflect.F90:43-72."""
         check(self.L.pic_bc_conducting_x(self.h, int(side), float(pos)), "pic_bc_conducting_x")
 
+    def RefBC_Prtl_y(self, side: int, pos: float):
+        """RefBC_Prtl_Bottom (side 0) / RefBC_Prtl_Top (side 1), bc_reflect.F90:79-128."""
+        check(self.L.pic_bc_reflect_y(self.h, int(side), float(pos)), "pic_bc_reflect_y")
+
+    def CondBC_Fld_y(self, side: int, pos: float):
+        """CondBC_Fld_Bottom (side 0) / CondBC_Fld_Top (side 1), bc_reflect.F90:11-41."""
+        check(self.L.pic_bc_conducting_y(self.h, int(side), float(pos)), "pic_bc_conducting_y")
+
     update_b_half = UpdateBfieldHalfGPU
     move_deposit = MoveDepositPrtlGPU
     exchange_particles = ExchangePrtlGPU

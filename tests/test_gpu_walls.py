@@ -1,7 +1,7 @@
-"""Walls along x (src/bc/bc_reflect.F90 on one rank) on the GPU against the
-oracle, phase by phase as MAIN.F90 calls them: reflecting particle walls
-after the move (EnforceBC_PostMovDep) and conducting field walls after
-AddCurrent (EnforceBC_Final), 10 steps with a reorder every 5."""
+"""Walls along x and y (src/bc/bc_reflect.F90 on one rank) on the GPU
+against the oracle, phase by phase as MAIN.F90 calls them: reflecting
+particle walls after the move (EnforceBC_PostMovDep) and conducting field
+walls after AddCurrent (EnforceBC_Final), 10 steps with a reorder every 5."""
 import numpy as np
 import pytest
 
@@ -12,12 +12,13 @@ from ._util import assert_particles_equal, grid_and_config, to_gpu_particles
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("dims,fdtd", [(2, "yee"), (3, "lehe")])
-def test_walls_lockstep(dims, fdtd):
+@pytest.mark.parametrize("dims,fdtd,axis", [(2, "yee", "x"), (3, "lehe", "x"), (2, "lehe", "y"), (3, "yee", "y")])
+def test_walls_lockstep(dims, fdtd, axis):
     from pictor_b200 import Simulation
 
     nx, ny, nz = (24, 16, 1) if dims == 2 else (12, 10, 8)
-    pl, pr = 1.5, nx - 2.5                      # walls at local x = 4.5 and nx + 0.5
+    n_ax = nx if axis == "x" else ny
+    pl, pr = 1.5, n_ax - 2.5                    # walls at local 4.5 and n + 0.5 along the axis
     g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, fdtd=fdtd, reorder_period=5, qi=0.00158203125,
                              capacity=1 << 17)
     p = O.load_weibel(dims, nx, ny, nz, epc=4 if dims == 3 else 8, drift=0.6, temp=0.01, seed=17)
@@ -28,8 +29,8 @@ def test_walls_lockstep(dims, fdtd):
             o.update_b_half(); o.send_recv_flds("B"); s.update_b_half()
             o.move_deposit(); s.move_deposit()
             for side, pos in ((0, pl), (1, pr)):
-                o.reflect_particles_x(side, pos)
-                s.RefBC_Prtl_x(side, pos)
+                getattr(o, "reflect_particles_" + axis)(side, pos)
+                getattr(s, "RefBC_Prtl_" + axis)(side, pos)
             o.exchange_particles(); s.exchange_particles()
             if t == 1:
                 assert_particles_equal(s.fetch_particles(), o.p, exact=True)
@@ -39,8 +40,8 @@ def test_walls_lockstep(dims, fdtd):
             o.fold_current(); s.fold_current()
             o.add_current(); o.send_recv_flds("E"); s.add_current()
             for side, pos in ((0, pl), (1, pr)):
-                o.conducting_x(side, pos)
-                s.CondBC_Fld_x(side, pos)
+                getattr(o, "conducting_" + axis)(side, pos)
+                getattr(s, "CondBC_Fld_" + axis)(side, pos)
             if t % 5 == 0:
                 o.reorder(); s.reorder()
         assert s.device_errors() == 0
@@ -49,11 +50,15 @@ def test_walls_lockstep(dims, fdtd):
     v = o.p.view()
     assert len(gp.x) == o.p.used
     live = v["flv"] != 0
-    assert ((v["x"][live] >= 4.5) & (v["x"][live] <= nx + 0.5)).all()     # every particle between the walls
+    c = v[axis][live]
+    assert ((c >= 4.5) & (c <= n_ax + 0.5)).all()                           # every particle between the walls
     assert np.array_equal(gp.flv, v["flv"])
     for k in ("x", "y", "z", "u", "v", "w"):
         np.testing.assert_allclose(getattr(gp, k), v[k], rtol=1e-9, atol=1e-9, err_msg=k)
     for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
         a, b = getattr(gf, n), getattr(o.f, n)
         np.testing.assert_allclose(a, b, rtol=0, atol=1e-9 * max(np.abs(b).max(), 1e-30), err_msg=n)
-    assert not gf.Ey[:4].any() and not gf.Ez[:4].any()                    # conducting: Ey, Ez beyond the left wall
+    if axis == "x":                                                          # tangential E beyond the low wall
+        assert not gf.Ey[:4].any() and not gf.Ez[:4].any()
+    else:
+        assert not gf.Ex[:, :4].any() and not gf.Ez[:, :4].any()

@@ -61,3 +61,39 @@ def test_conducting_walls():
         assert not a[:4].any() and not a[11:].any()
         np.testing.assert_array_equal(a[4:11], E0[n][4:11])
     np.testing.assert_array_equal(o.f.Ex, E0["Ex"])
+
+
+def test_y_walls():
+    """Bottom wall at y = 4.5 (pos 1.5), top wall at y = 8.5 (pos 5.5) on
+    a 12 x 8 grid (my = 13): W = int(4.5) = 4 and int(8.5) = 8."""
+    g, p, f = _state()
+    for n, y in enumerate([4.2, 5.0, 3.8, 8.7, 8.4, 6.0]):
+        p.y[n], p.v[n] = y, [-0.3, 0.1, 0.0, 0.2, 0.25, -0.1][n]
+    J0 = {n: getattr(f, n).copy() for n in ("Jx", "Jy", "Jz")}
+    E0 = {n: getattr(f, n).copy() for n in ("Ex", "Ey", "Ez")}
+    o = O.Oracle(g, p, f)
+    o.reflect_particles_y(0, 1.5)
+    o.reflect_particles_y(1, 5.5)
+    v = o.p.view()
+    np.testing.assert_array_equal(v["y"], [2.0 * 4.5 - 4.2, 5.0, 3.8, 2.0 * 8.5 - 8.7, 8.4, 6.0])
+    np.testing.assert_array_equal(v["v"], [0.3, 0.1, 0.0, -0.2, 0.25, -0.1])
+    ex = {n: a.copy() for n, a in J0.items()}
+    # bottom (W = 4, 0-based 3): Jx, Jz += layer 3; Jy -= layer 3; layer 3 zeroed
+    for n, sgn in (("Jx", 1), ("Jy", -1), ("Jz", 1)):
+        ex[n][:, 3] = J0[n][:, 3] + sgn * J0[n][:, 2]
+        ex[n][:, 2] = 0.0
+    # top (W = 8, 0-based 7): Jx, Jz(8) += (9); Jy(7) -= Jy(8); Jx, Jz(9) and Jy(8) zeroed
+    for n in ("Jx", "Jz"):
+        ex[n][:, 7] = ex[n][:, 7] + ex[n][:, 8]
+        ex[n][:, 8] = 0.0
+    ex["Jy"][:, 6] = ex["Jy"][:, 6] - ex["Jy"][:, 7]
+    ex["Jy"][:, 7] = 0.0
+    for n in ("Jx", "Jy", "Jz"):
+        np.testing.assert_array_equal(getattr(o.f, n), ex[n], err_msg=n)
+    o.conducting_y(0, 1.5)            # y layers 1..4
+    o.conducting_y(1, 5.5)            # y layers 9..13
+    for n in ("Ex", "Ez"):
+        a = getattr(o.f, n)
+        assert not a[:, :4].any() and not a[:, 8:].any()
+        np.testing.assert_array_equal(a[:, 4:8], E0[n][:, 4:8])
+    np.testing.assert_array_equal(o.f.Ey, E0["Ey"])
