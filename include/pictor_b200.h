@@ -153,6 +153,11 @@ int pic_bc_conducting_x(pic_handle *h, int32_t side, double pos);
    CondBC_Fld_Bottom/Top (Ex, Ez zeroed, :11-41); also on a slab. */
 int pic_bc_reflect_y(pic_handle *h, int32_t side, double pos);
 int pic_bc_conducting_y(pic_handle *h, int32_t side, double pos);
+/* A face of type 'remv' (bc.F90:258-283, RemovePrtl_Left/Right of
+   bc_open.F90:8-62): the particles beyond the wall at `pos` on face 1..6
+   (x, y, z; low, high) become holes; called where EnforceBC_PostMovDep
+   calls it.  FP64 Cartesian. */
+int pic_bc_remove(pic_handle *h, int32_t face, double pos);
 
 /* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
    with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:

@@ -99,6 +99,7 @@ def _declare(L: C.CDLL) -> None:
         getattr(L, fn).argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_double]
     for fn in ("orc_cond_fld_bottom", "orc_cond_fld_top"):
         getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
+    L.orc_remove_prtl.argtypes = [P(Grid), P(_Particles), C.c_int, C.c_double]
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -276,6 +277,10 @@ class Oracle:
         fs = self.f.struct()
         fn = self.L.orc_cond_fld_left if side == 0 else self.L.orc_cond_fld_right
         fn(C.byref(self.g), C.byref(fs), float(pos))
+
+    def remove_particles(self, face: int, pos: float):
+        """RemovePrtl_Left / Right for face 1..6 (x, y, z; low, high) at wall pos."""
+        self._call_p(self.L.orc_remove_prtl, int(face), float(pos))
 
     def reflect_particles_y(self, side: int, pos: float):
         """RefBC_Prtl_Bottom (side 0) / RefBC_Prtl_Top (side 1) at wall pos."""

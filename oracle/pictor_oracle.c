@@ -893,6 +893,30 @@ void orc_cond_fld_top(const orc_grid *g, orc_fields *f, double pos)
             }
 }
 
+/* RemovePrtl_Left / Right (bc_open.F90:8-62): the coordinate of the face's
+   axis compared with the wall, the removed particle holed as RemovePrtl
+   does (x = y = 3.8, z = 3.8 in 3D, 1.5 in 2D; the y and z faces pass
+   their axis as the routine's x, which changes nothing in those values). */
+void orc_remove_prtl(const orc_grid *g, orc_particles *p, int face, double pos)
+{
+    const double wall = pos - 0.0 + 3;   /* bc_pos_local with the borders at 0 */
+    const int axis = (face - 1) / 2, low = (face % 2) == 1;
+    for (int64_t n = 0; n < p->used; n++) {
+        if (p->flv[n] == 0) continue;
+        const double c = axis == 0 ? p->x[n] : axis == 1 ? p->y[n] : p->z[n];
+        if (low ? c < wall : c > wall) {
+            p->q[n] = 0;
+            p->flv[n] = 0;
+            p->u[n] = 0;
+            p->v[n] = 0;
+            p->w[n] = 0;
+            p->x[n] = 3.8;
+            p->y[n] = 3.8;
+            p->z[n] = g->dims == 3 ? 3.8 : 1.5;
+        }
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* One time step, src/MAIN.F90:42-284                                        */
 /* ------------------------------------------------------------------------- */

@@ -98,6 +98,10 @@ void orc_refl_prtl_bottom(const orc_grid *g, orc_particles *p, orc_fields *f, do
 void orc_refl_prtl_top(const orc_grid *g, orc_particles *p, orc_fields *f, double pos);
 void orc_cond_fld_bottom(const orc_grid *g, orc_fields *f, double pos);
 void orc_cond_fld_top(const orc_grid *g, orc_fields *f, double pos);
+/* RemovePrtl_Left / RemovePrtl_Right (bc_open.F90:8-62) for face 1..6 (x, y,
+   z; low, high): the particles beyond bc_pos_local(face, pos) = pos + 3
+   (bc.F90:350-363) become holes. */
+void orc_remove_prtl(const orc_grid *g, orc_particles *p, int face, double pos);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

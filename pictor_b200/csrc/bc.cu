@@ -80,6 +80,28 @@ __global__ void k_zero_x_layers(GridP g, double *Ey, double *Ez, int x0, int x1)
     }
 }
 
+// RemovePrtl_Left / Right (bc_open.F90:8-62): a particle beyond the wall on
+// the face's axis becomes a hole with RemovePrtl's values.
+__global__ void k_remove_prtl(PartF64 p, const Counters *__restrict__ cnt, int axis, int low, double wall, double zhole)
+{
+    const long long used = cnt->used;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used;
+         n += (long long)gridDim.x * blockDim.x) {
+        if (p.flv[n] == 0) continue;
+        const double c = axis == 0 ? p.x[n] : axis == 1 ? p.y[n] : p.z[n];
+        if (low ? c < wall : c > wall) {
+            p.q[n] = 0.0;
+            p.flv[n] = 0;
+            p.u[n] = 0.0;
+            p.v[n] = 0.0;
+            p.w[n] = 0.0;
+            p.x[n] = 3.8;
+            p.y[n] = 3.8;
+            p.z[n] = zhole;
+        }
+    }
+}
+
 int grid_for(long long n)
 {
     const long long b = (n + kThreads - 1) / kThreads;
@@ -165,6 +187,15 @@ void launch_wall_conducting_y(const GridP &g, double *const E[3], int side, doub
         y1 = g.my;
     }
     k_zero_y_layers<<<grid_for((long long)g.mx * (y1 - y0 + 1) * g.mz), kThreads, 0, s>>>(g, E[0], E[2], y0, y1);
+    count_launches(1);
+}
+
+// RemovePrtl at face 1..6 (x, y, z; low, high), wall at bc_pos_local = pos + 3.
+void launch_wall_remove(const GridP &g, PartF64 &p, const Counters *cnt, int face, double pos, long long capacity,
+                        cudaStream_t s)
+{
+    k_remove_prtl<<<grid_for(capacity), kThreads, 0, s>>>(p, cnt, (face - 1) / 2, face % 2, pos - 0.0 + 3,
+                                                          g.dims == 3 ? 3.8 : 1.5);
     count_launches(1);
 }
 

@@ -1417,6 +1417,15 @@ int pic_bc_conducting_y(pic_handle *h, int32_t side, double pos)
     return finish_phase(h);
 }
 
+int pic_bc_remove(pic_handle *h, int32_t face, double pos)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || face < 1 || face > 6 || (h->g.dims == 2 && face > 4) ||
+        (h->g.x_external && face <= 2))
+        return PIC_ERR_INVALID;
+    launch_wall_remove(h->g, h->p64[h->cur], h->cnt, face, pos, h->capacity, h->s);
+    return finish_phase(h);
+}
+
 int pic_set_sync(pic_handle *h, int32_t sync)
 {
     if (!h) return PIC_ERR_INVALID;

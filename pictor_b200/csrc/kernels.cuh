@@ -141,6 +141,8 @@ void launch_wall_conducting(const GridP &g, double *const E[3], int side, double
 void launch_wall_reflect_y(const GridP &g, PartF64 &p, const Counters *cnt, double *const J[3], int side, double pos,
                            long long capacity, cudaStream_t s);
 void launch_wall_conducting_y(const GridP &g, double *const E[3], int side, double pos, cudaStream_t s);
+void launch_wall_remove(const GridP &g, PartF64 &p, const Counters *cnt, int face, double pos, long long capacity,
+                        cudaStream_t s);
 // slab.cu: x faces of a slab (fields and particles), see pic_slab_* in the C ABI
 void launch_slab_pack_fields(const GridP &g, int which, double *const F[3], double *to_left, double *to_right,
                              cudaStream_t s);

@@ -248,6 +248,10 @@ class Simulation:
         """CondBC_Fld_Bottom (side 0) / CondBC_Fld_Top (side 1), bc_reflect.F90:11-41."""
         check(self.L.pic_bc_conducting_y(self.h, int(side), float(pos)), "pic_bc_conducting_y")
 
+    def RemovePrtl(self, face: int, pos: float):
+        """RemovePrtl_Left / Right (bc_open.F90:8-62) at face 1..6 (x, y, z; low, high)."""
+        check(self.L.pic_bc_remove(self.h, int(face), float(pos)), "pic_bc_remove")
+
     update_b_half = UpdateBfieldHalfGPU
     move_deposit = MoveDepositPrtlGPU
     exchange_particles = ExchangePrtlGPU

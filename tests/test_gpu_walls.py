@@ -62,3 +62,41 @@ def test_walls_lockstep(dims, fdtd, axis):
         assert not gf.Ey[:4].any() and not gf.Ez[:4].any()
     else:
         assert not gf.Ex[:, :4].any() and not gf.Ez[:, :4].any()
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_remove_faces_lockstep(dims):
+    """Particles removed beyond walls on the low x face and the high y face
+    (and the low z face in 3D) every step, after the move: the same holes
+    and the same survivors as the oracle, 8 steps with a reorder every 4."""
+    from pictor_b200 import Simulation
+
+    nx, ny, nz = (24, 16, 1) if dims == 2 else (12, 10, 8)
+    faces = [(1, 2.5), (4, ny - 3.5)] + ([(5, 2.0)] if dims == 3 else [])
+    g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, reorder_period=4, qi=0.00158203125, capacity=1 << 17)
+    p = O.load_weibel(dims, nx, ny, nz, epc=4 if dims == 3 else 8, drift=0.6, temp=0.01, seed=23)
+    o = O.Oracle(g, p.copy())
+    with Simulation(cfg) as s:
+        s.load_particles(to_gpu_particles(p))
+        for t in range(1, 9):
+            o.update_b_half(); o.send_recv_flds("B"); s.update_b_half()
+            o.move_deposit(); s.move_deposit()
+            for face, pos in faces:
+                o.remove_particles(face, pos)
+                s.RemovePrtl(face, pos)
+            o.exchange_particles(); s.exchange_particles()
+            if t == 1:
+                assert_particles_equal(s.fetch_particles(), o.p, exact=True)
+            o.update_b_half(); o.send_recv_flds("B"); s.update_b_half()
+            o.update_e(); o.send_recv_flds("E"); s.update_e()
+            o.fold_current(); s.fold_current()
+            o.add_current(); o.send_recv_flds("E"); s.add_current()
+            if t % 4 == 0:
+                o.reorder(); s.reorder()
+        assert s.device_errors() == 0
+        gp = s.fetch_particles()
+    v = o.p.view()
+    assert len(gp.x) == o.p.used < len(p.view()["x"])                      # holes dropped by the reorders
+    assert np.array_equal(gp.flv, v["flv"])
+    for k in ("x", "y", "z", "u", "v", "w", "q"):
+        np.testing.assert_allclose(getattr(gp, k), v[k], rtol=1e-9, atol=1e-9, err_msg=k)

@@ -97,3 +97,20 @@ def test_y_walls():
         assert not a[:, :4].any() and not a[:, 8:].any()
         np.testing.assert_array_equal(a[:, 4:8], E0[n][:, 4:8])
     np.testing.assert_array_equal(o.f.Ey, E0["Ey"])
+
+
+def test_remove_beyond_walls():
+    """RemovePrtl at the low x face (x < 4.5) and the high y face (y > 6.5):
+    those particles become holes with RemovePrtl's values, the rest stay."""
+    g, p, f = _state()
+    for n, y in enumerate([5.0, 5.0, 3.8, 7.0, 5.5, 6.0]):
+        p.y[n] = y
+    o = O.Oracle(g, p, f)
+    o.remove_particles(1, 1.5)
+    o.remove_particles(4, 3.5)
+    v = o.p.view()
+    # particle 0 (x 4.2) and 3 (y 7.0) removed; 2 was a hole already
+    np.testing.assert_array_equal(v["flv"], [0, 2, 0, 0, 1, 1])
+    for n in (0, 3):
+        assert (v["q"][n], v["u"][n], v["x"][n], v["y"][n], v["z"][n]) == (0.0, 0.0, 3.8, 3.8, 1.5)
+    np.testing.assert_array_equal(v["x"][[1, 4, 5]], [5.0, 11.4, 7.0])
