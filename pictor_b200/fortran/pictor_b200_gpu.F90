@@ -106,8 +106,8 @@ module pictor_b200_capi
       end function
    end interface
 
-   ! Walls along x: EnforceBC_PostMovDep / EnforceBC_Final (bc.F90) call
-   ! these for bc_face(1:2) of type 'refl' / 'cond'; side 0 = left.
+   ! Walls: EnforceBC_PostMovDep / EnforceBC_Final (bc.F90) call these for
+   ! bc_face(1:4) of type 'refl' / 'cond' (side 0 = low face) and 'remv'.
    interface
       integer(c_int) function pic_bc_reflect_x(h, side, pos) bind(C, name="pic_bc_reflect_x")
          import :: c_int, c_ptr, c_int32_t, c_double
@@ -119,6 +119,24 @@ module pictor_b200_capi
          import :: c_int, c_ptr, c_int32_t, c_double
          type(c_ptr), value :: h
          integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+      integer(c_int) function pic_bc_reflect_y(h, side, pos) bind(C, name="pic_bc_reflect_y")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+      integer(c_int) function pic_bc_conducting_y(h, side, pos) bind(C, name="pic_bc_conducting_y")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+      integer(c_int) function pic_bc_remove(h, face, pos) bind(C, name="pic_bc_remove")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: face
          real(c_double), value :: pos
       end function
    end interface
