@@ -1,6 +1,7 @@
 // capi.cu -- the C ABI of include/pictor_b200.h: handle lifetime, host <->
 // device copies, the phase entry points that replace the reference's
-// `#ifdef gpu` subroutines, and the CUDA-graph step loop.
+// `#ifdef gpu` subroutines (walls of src/bc and the x faces of a slab
+// included), the CUDA-graph step loop and the ensemble steps.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
