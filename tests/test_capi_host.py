@@ -97,3 +97,29 @@ def test_cell_decode_division_is_exact():
             for n in (int(x) * d + r for x in q):
                 if n < (1 << 28):
                     assert ((n << 24) * m) >> 64 == n // d, (n, d)
+
+
+def test_slab_and_wall_entry_points_validate_without_gpu():
+    """The slab form is refused outside the FP64 Cartesian step without a
+    current filter (before any device use), and the slab, wall and sync
+    entry points reject a null handle and bad arguments."""
+    from pictor_b200 import PicConfig, PicError, Simulation, _capi
+
+    for bad in (PicConfig(nx=12, ny=8, slab_x=1, precision="fp32"), PicConfig(nx=12, ny=8, slab_x=2),
+                PicConfig(nx=12, ny=8, slab_x=1, curr_filter=1),
+                PicConfig(nx=12, ny=8, nz=8, dims=3, slab_x=1, geom="cylindrical")):
+        with pytest.raises(PicError) as e:
+            Simulation(bad)
+        assert e.value.code == -1
+    L = _capi.lib()
+    n = C.c_int64()
+    a, b = C.c_int64(), C.c_int64()
+    assert L.pic_slab_face_len(None, C.byref(n)) == -1
+    assert L.pic_slab_pack_fields(None, 0, None, None) == -1
+    assert L.pic_slab_unpack_fields(None, 0, None, None) == -1
+    assert L.pic_slab_pack_particles(None, None, 0, C.byref(a), C.byref(b)) == -1
+    assert L.pic_slab_unpack_particles(None, None, 0) == -1
+    assert L.pic_set_sync(None, 0) == -1
+    for fn in (L.pic_bc_reflect_x, L.pic_bc_conducting_x, L.pic_bc_reflect_y, L.pic_bc_conducting_y):
+        assert fn(None, 0, 1.5) == -1
+    assert L.pic_bc_remove(None, 1, 1.5) == -1
