@@ -99,8 +99,8 @@ def bytes_per_cell_mover(precision: str) -> int:
 # weibel3d_fp32_small workload (8.39 M particles, 270 MB of particle state,
 # larger than L2); scaled to a full launch by the particles it moves.
 TRAFFIC_BYTES_PER_PARTICLE = 57.1
-TRAFFIC_SOURCE = ("ncu on weibel3d_fp32_small scaled by particle count "
-                  "(profiles/k_move_f32_tiled_weibel3d.md)")
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of k_move_f32_tiled on weibel3d_fp32_small, "
+                  "per particle, scaled by the particles of the launch")
 
 
 def traffic_per_launch(wl: dict, n_p: int):

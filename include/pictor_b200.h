@@ -6,7 +6,8 @@
  * 113-116, 128-130, 161-163, 173-175, 189-191, 223-233, 250-252, 263-265)
  * that work on module globals (vars.F90, src/var_gpu.F90).  Each entry point
  * below replaces one of those subroutines; a Fortran module binds them with
- * ISO_C_BINDING.  Plain pointers and sizes only.
+ * ISO_C_BINDING (pictor_b200/fortran/pictor_b200_gpu.F90).  Plain pointers
+ * and sizes only.
  *
  * Layout on the host side is the reference's: fields are column-major
  * (mx,my,mz) double arrays with 2 low and 3 high ghost layers (mx = nx+5,
