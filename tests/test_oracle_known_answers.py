@@ -246,3 +246,31 @@ def test_cyl_vacuum_fields_stay_bounded():
         o.step(t)
     e = sum(o.field_energy())
     assert np.isfinite(e) and e < 10 * e0
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_empty_and_all_hole_particle_sets(dims):
+    """Edge cases of the particle side: a step with no particles leaves J
+    zero and evolves the fields as in vacuum; an array of holes moves
+    nothing, deposits nothing, appends nothing and reorders to empty."""
+    nx, ny, nz = (12, 10, 1) if dims == 2 else (8, 8, 8)
+    g = O.make_grid(dims, nx, ny, nz, c=0.45, qi=0.01)
+    rng = np.random.default_rng(4)
+    f = O.Fields(g)
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        getattr(f, n)[...] = rng.normal(size=O.grid_shape(g))
+    o_vac = O.Oracle(g, O.Particles(4), f.copy())
+    o_vac.send_recv_flds("E"); o_vac.send_recv_flds("B")
+    assert o_vac.step(1, 20) == 0
+    assert not o_vac.f.Jx.any() and not o_vac.f.Jy.any() and not o_vac.f.Jz.any()
+    assert o_vac.p.used == 0
+    holes = 64
+    p = O.Particles.from_arrays(holes + 8, q=np.zeros(holes), x=np.full(holes, 3.8), y=np.full(holes, 3.8),
+                                z=np.full(holes, 3.8 if dims == 3 else 1.5), u=np.zeros(holes), v=np.zeros(holes),
+                                w=np.zeros(holes), flv=np.zeros(holes, dtype=np.int32))
+    o = O.Oracle(g, p, f.copy())
+    o.send_recv_flds("E"); o.send_recv_flds("B")
+    assert o.step(1, 1) == 0                     # reorder every step: the holes are dropped
+    assert o.p.used == 0
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        np.testing.assert_array_equal(getattr(o.f, n), getattr(o_vac.f, n), err_msg=n)
