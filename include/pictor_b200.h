@@ -87,7 +87,15 @@ typedef struct {
        periodic on the slab.  FP64 Cartesian, no current filter.  0 = one
        periodic domain. */
     int32_t slab_x;
-    int32_t reserved[2];
+    /* FP64 Cartesian form: 1 = sum the current in the reference's serial
+       order (each cell's VecJ entries in particle order, then the cells onto
+       the edges in the loop order of ReduceCurrentMatrix,
+       movdep_routines.F90:243-311), so that J and every later phase equal
+       the serial CPU build bit for bit and a run is reproducible; costs a
+       sort of two records per particle each step.  0 = FP64 atomics into J
+       (the sums differ from the serial build's in the last bits). */
+    int32_t exact_current;
+    int32_t reserved[1];
 } pic_config;
 
 typedef struct pic_handle pic_handle;
@@ -178,8 +186,11 @@ int pic_bc_remove(pic_handle *h, int32_t face, double pos);
    through the x faces and writes them to `out` (8 doubles each: q, x, y, z,
    u, v, w, flv, positions in the receiver's coordinates): n_right bound
    right first, then n_left bound left; y and z leavers wrap on the slab.
-   PIC_ERR_OVERFLOW if more than `cap` leave.  pic_step, pic_step_many and
-   pic_exchange_particles refuse a slab. */
+   pack_particles waits for its work in either sync mode (the counts size the
+   transfers) and returns the device errors like a synchronous call:
+   PIC_ERR_OVERFLOW, with both counts 0 and no particle moved, if more than
+   `cap` leave or the appended particles would pass the capacity.  pic_step,
+   pic_step_many and pic_exchange_particles refuse a slab. */
 int pic_slab_face_len(pic_handle *h, int64_t *n);
 /* sync = 0: the phase entry points (pic_update_b_half ... pic_reorder and
    the pic_slab_* calls) only enqueue their work on the handle's stream
@@ -254,13 +265,13 @@ int pic_launch_count(pic_handle *h, int64_t *launches);
    library allocate/free (cudaFree synchronizes the device) between their own
    steps.  Inputs are caller-owned DEVICE arrays in the reference layout
    ((nx+5, ny+5, nz+5 or 1) column-major FP64); out2 is a DEVICE pointer that
-   receives sum|B|^2 and sum|E|^2 over the interior (CalcFldEnergy,
-   savedata_routines.F90:310-326).  Work is enqueued on `stream` (a
-   cudaStream_t, NULL for the default stream); synchronize before reading
+   receives the sum of Bx^2 + By^2 + Bz^2 and the sum of Ex^2 + Ey^2 + Ez^2
+   over the interior cells 3..m-3 of each axis.  Work is enqueued on `stream`
+   (a cudaStream_t, NULL for the default stream); synchronize before reading
    out2.  The reduction's partial sums use one fixed array of 148*8 pairs in
    the library's device memory, shared by every call: calls that overlap on
-   the GPU race.  The first call on a device looks up that array's device
-   address.  Returns PIC_ERR_INVALID for bad sizes. */
+   the GPU race.  Each call looks up that array's device address in the
+   current context.  Returns PIC_ERR_INVALID for bad sizes. */
 int pic_field_energy_noalloc(const double *Ex, const double *Ey, const double *Ez,
                              const double *Bx, const double *By, const double *Bz,
                              int32_t nx, int32_t ny, int32_t nz, int32_t dims,

@@ -309,6 +309,14 @@ class Oracle:
         self.L.orc_field_energy(C.byref(self.g), C.byref(fs), out)
         return out[0], out[1]
 
+    def particle_energy(self, masse: float, massi: float = 0.0) -> np.ndarray:
+        """CalcPrtlEnergy per species (orc_particle_energy)."""
+        out = np.zeros(self.g.nflvr)
+        ps = self.p.struct()
+        self.L.orc_particle_energy(C.byref(self.g), C.byref(ps), float(masse), float(massi),
+                                   out.ctypes.data_as(C.POINTER(C.c_double)))
+        return out
+
     def gauss_residual(self):
         rm = C.c_double(0)
         fs = self.f.struct()

@@ -44,7 +44,7 @@ class Config(C.Structure):
         ("reorder_period", C.c_int32), ("curr_filter", C.c_int32),
         ("capacity", C.c_int64),
         ("rmin", C.c_double), ("inc_axis", C.c_int32), ("brick", C.c_int32 * 3), ("cyl_modes", C.c_int32),
-        ("slab_x", C.c_int32), ("reserved", C.c_int32 * 2),
+        ("slab_x", C.c_int32), ("exact_current", C.c_int32), ("reserved", C.c_int32 * 1),
     ]
 
 

@@ -60,6 +60,9 @@ struct pic_handle {
     uint32_t *slab_sent = nullptr;
     // phase entry points wait for their work (pic_set_sync)
     bool sync = true;
+    // FP64 current summed in the serial order (pic_config.exact_current)
+    bool exact = false;
+    SegRecords rec = {};
     std::vector<void *> allocs;
 };
 
@@ -346,7 +349,7 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 launch_bhalf<double>(g, E, B, h->s);
                 break;
             case PIC_PHASE_MOVE:  // MAIN.F90:63-71
-                launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);
+                launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s, h->exact ? &h->rec : nullptr);
                 break;
             case PIC_PHASE_EXCHANGE:  // MAIN.F90:86-94 + 145-150
                 launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s);
@@ -859,6 +862,10 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (c.slab_x != 0 && (c.slab_x != 1 || c.geom != PIC_GEOM_CARTESIAN || c.precision != PIC_PREC_FP64 ||
                           c.curr_filter != 0))
         return PIC_ERR_INVALID;
+    // the exact-order current: FP64 Cartesian, two sorted records per slot
+    if (c.exact_current != 0 && (c.exact_current != 1 || c.geom != PIC_GEOM_CARTESIAN ||
+                                 c.precision != PIC_PREC_FP64 || c.capacity >= (1ll << 31)))
+        return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
@@ -971,6 +978,20 @@ int pic_create(const pic_config *cfg, pic_handle **out)
         if ((r = dalloc(h, &sc.key[0], nk)) || (r = dalloc(h, &sc.key[1], nk)) || (r = dalloc(h, &sc.idx[0], nk)) ||
             (r = dalloc(h, &sc.idx[1], nk)) || (r = dalloc(h, &sc.hist, 256 * sc.ntiles)) ||
             (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
+        }
+    }
+    if (!r && c.exact_current) {
+        SegRecords &R = h->rec;
+        h->exact = true;
+        R.n2 = 2 * h->capacity;
+        R.sc.ntiles = sort_tiles(R.n2);
+        R.sc.scan_tmp_len = scan_tmp_len(256 * R.sc.ntiles);
+        const size_t ne = g.dims == 3 ? 12 : 8;
+        if ((r = dalloc(h, &R.sc.key[0], (size_t)R.n2)) || (r = dalloc(h, &R.sc.key[1], (size_t)R.n2)) ||
+            (r = dalloc(h, &R.sc.idx[0], (size_t)R.n2)) || (r = dalloc(h, &R.sc.idx[1], (size_t)R.n2)) ||
+            (r = dalloc(h, &R.sc.hist, 256 * R.sc.ntiles)) || (r = dalloc(h, &R.sc.scan_tmp, R.sc.scan_tmp_len)) ||
+            (r = dalloc(h, &R.val, ne * (size_t)R.n2)) || (r = dalloc(h, &R.vecj, ne * (size_t)g.ncell)) ||
+            (r = dalloc(h, &R.count, 1))) {
         }
     }
     if (!r) {
@@ -1272,7 +1293,7 @@ int pic_move_deposit(pic_handle *h)
     } else {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_move_deposit_f64(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s);
+        launch_move_deposit_f64(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s, h->exact ? &h->rec : nullptr);
     }
     return finish_phase(h);
 }
@@ -1464,12 +1485,19 @@ int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_
     if (!h || !h->g.x_external || !out || cap < 0 || !n_right || !n_left) return PIC_ERR_INVALID;
     launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s, out, cap, h->slab_sent);
     uint32_t sent[2] = {0, 0};
+    *n_right = 0;
+    *n_left = 0;
     CK(cudaMemcpyAsync(sent, h->slab_sent, sizeof(sent), cudaMemcpyDeviceToHost, h->s));
-    CK(cudaStreamSynchronize(h->s));   // the counts size the transfers, in either mode
-    const int r = finish_phase(h);
+    // the counts size the transfers, so this call waits in either sync mode
+    // and checks the device error word like a synchronous call: an outbox or
+    // capacity overflow (nothing moved, the count unchanged) returns
+    // PIC_ERR_OVERFLOW with zero counts instead of counts no buffer holds
+    const int r = finish(h);
+    if (r != PIC_OK) return r;
+    if ((int64_t)sent[1] > cap) return PIC_ERR_OVERFLOW;
     *n_right = sent[0];
     *n_left = (int64_t)sent[1] - (int64_t)sent[0];
-    return r;
+    return PIC_OK;
 }
 
 int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n)

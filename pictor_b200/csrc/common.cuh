@@ -88,6 +88,19 @@ void count_launches(int n);
 // Error bits written by kernels (never __trap): see PIC_DEVERR_*.
 __device__ inline void raise_error(int *err, int bit) { atomicOr(err, bit); }
 
+// A momentum triple is finite (false for NaN or +-Inf in any component).
+// The movers test the pushed momentum before any index is formed from the
+// new position: a non-finite displacement would truncate to an arbitrary
+// cell, so the particle is left as it was and PIC_DEVERR_NAN is raised.
+__device__ __forceinline__ bool finite3(float a, float b, float c)
+{
+    return fabsf(a) + fabsf(b) + fabsf(c) <= 3.402823466e38f;
+}
+__device__ __forceinline__ bool finite3(double a, double b, double c)
+{
+    return fabs(a) + fabs(b) + fabs(c) <= 1.7976931348623157e308;
+}
+
 // Device-side particle counters shared by the step kernels.
 struct Counters {
     long long used;        // used_prtl_arr_size

@@ -427,6 +427,10 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64
         }
         double u0 = c * ui + pE[0], v0 = c * vi + pE[1], w0 = c * wi + pE[2];
         half_boris_d(sqc, pE, pB, u0, v0, w0);
+        if (!finite3(u0, v0, w0)) {   // the particle keeps its state (see finite3)
+            raise_error(err, PIC_DEVERR_NAN);
+            continue;
+        }
         double u1 = u0 * cinv, v1 = v0 * cinv;
         const double gg = sqc / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
         const double r0 = (x0 + r_proc) * 1.0;
@@ -464,6 +468,7 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64
             xn = x0; yn = y0; zn = z0; un = ui; vn = vi; wn = wi;
             double t = 0.0, dt = 1.0, sx0 = x0, sy0 = y0, sz0 = z0;
             int tries = 0;
+            bool bad = false;
             while (t < 1.0) {
                 if (++tries > kMaxSubsteps) {
                     raise_error(err, PIC_DEVERR_SUBSTEP);
@@ -478,6 +483,11 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64
                 }
                 double a0 = c * un + pE[0], b0 = c * vn + pE[1], c0 = c * wn + pE[2];
                 half_boris_d(sqc, pE, pB, a0, b0, c0);
+                if (!finite3(a0, b0, c0)) {
+                    raise_error(err, PIC_DEVERR_NAN);
+                    bad = true;
+                    break;
+                }
                 double a1 = a0 * cinv, b1 = b0 * cinv;
                 const double c1 = c0 * cinv;
                 const double g2 = sqc / sqrt(((sqc + a0 * a0) + b0 * b0) + c0 * c0);
@@ -525,6 +535,7 @@ __global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64
                 dt = dt * 1.7;
                 sx0 = xn; sy0 = yn; sz0 = zn;
             }
+            if (bad) continue;   // the particle keeps its state
         }
         // zigzag deposit; both segments use the start cell (:341)
         const double xr = fmin((double)(min(ip0, ip) + 1), fmax((double)max(ip0, ip), 0.5 * (x0 + xn)));
@@ -774,6 +785,10 @@ __device__ __forceinline__ void cyl_push_f32(const GridP &g, const CylP &cp, con
         }
         float u0 = fmaf(c, ui, pE[0]), v0 = fmaf(c, vi, pE[1]), w0 = fmaf(c, wi, pE[2]);
         half_boris_f(sqc, pE, pB, u0, v0, w0);
+        if (!finite3(u0, v0, w0)) {   // the particle keeps its state (see finite3)
+            raise_error(err, PIC_DEVERR_NAN);
+            return;
+        }
         float u1 = u0 * cinv, v1 = v0 * cinv;
         const float gg = sqc * rsqrtf(fmaf(w0, w0, fmaf(v0, v0, fmaf(u0, u0, sqc))));
         const float r0 = ((float)i - 3.5f) + dx;          // x - 3 + rmin, rmin = -0.5
@@ -873,6 +888,10 @@ __device__ __forceinline__ void cyl_push_f32(const GridP &g, const CylP &cp, con
             }
             float a0 = fmaf(c, un, pE[0]), b0 = fmaf(c, vn, pE[1]), c0 = fmaf(c, wn, pE[2]);
             half_boris_f(sqc, pE, pB, a0, b0, c0);
+            if (!finite3(a0, b0, c0)) {   // the particle keeps its state (see finite3)
+                raise_error(err, PIC_DEVERR_NAN);
+                return;
+            }
             float a1 = a0 * cinv, b1 = b0 * cinv;
             const float c1 = c0 * cinv;
             const float g2 = sqc * rsqrtf(fmaf(c0, c0, fmaf(b0, b0, fmaf(a0, a0, sqc))));

@@ -52,8 +52,12 @@ void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counter
                                  float *const B[3], float *const J[3], int *err, cudaStream_t s);
 
 // mover.cu
+struct SegRecords;
+// rec == nullptr: the current goes to J by FP64 atomics; otherwise it is
+// summed in the reference's order (pic_config.exact_current, see mover.cu).
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
-                             double *const B[3], double *const J[3], int *err, cudaStream_t s);
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s,
+                             SegRecords *rec = nullptr);
 // mover_f32.cu: per-particle FP32 mover (any particle order)
 void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
                              float *const B[3], float *const J[3], int *err, cudaStream_t s);
@@ -129,6 +133,24 @@ struct SortScratch {
 };
 size_t sort_tiles(long long capacity);
 size_t scan_tmp_len(size_t n);
+// Stable LSD radix sort of sc.key[0] (with the slot index as payload) over
+// the first *used keys, each < 2^nbits; returns r with the result in
+// sc.key[r] / sc.idx[r].
+int radix_sort_keys(SortScratch &sc, const long long *used, int nbits, cudaStream_t s);
+int sort_key_bits(long long ncell);
+// Exact-order deposit of the FP64 form: the two zigzag segments of particle n
+// are records 2n and 2n+1 (key = the cell of the segment, ncell for none;
+// NE values each, structure of arrays: val[e * n2 + r]); sorted by cell
+// (stable, so a cell's records stay in particle order), summed per cell into
+// vecj[e * ncell + cell] in that order, and assembled into J in the loop
+// order of ReduceCurrentMatrix.
+struct SegRecords {
+    SortScratch sc;       // sized for n2 keys; sc.key[0] receives the record keys
+    double *val;          // NE * n2
+    double *vecj;         // NE * ncell
+    long long *count;     // device: 2 * used
+    long long n2;         // 2 * capacity
+};
 // Exchange (wrap) of the reference layout: holes + append in AppendParticles order.
 // Slab form (g.x_external): the x leavers go to `out` (out_cap particles of 8
 // doubles) and sent_counts (device) receives {right-bound, right + left-bound}.

@@ -10,7 +10,12 @@
 // reference stages in VecE*/VecB* are recomputed per particle from the field
 // arrays with the same expressions, so interpolated fields, momenta and
 // positions equal the serial CPU build bit for bit.  Currents go to J with
-// FP64 atomics (order-dependent in the last bits only).
+// FP64 atomics (order-dependent in the last bits only), or, with
+// pic_config.exact_current, are summed in the serial build's order: each
+// cell's VecJ entries in particle order (segment 1 before segment 2), then
+// the VecJ entries onto the edges in the loop order of ReduceCurrentMatrix
+// (movdep_routines.F90:262-308), which makes J, and with it the whole step,
+// equal to the serial CPU build bit for bit and independent of the launch.
 //
 // The FP32 cell-relative movers are in mover_f32.cu.
 #include "common.cuh"
@@ -22,16 +27,38 @@ namespace pic {
 // ---------------------------------------------------------------------------
 // FP64, reference layout
 // ---------------------------------------------------------------------------
+// Records of the exact-order deposit (see SegRecords): key and values of
+// record r, or key ncell for a record that carries nothing.
+struct RecOut {
+    uint32_t *key;
+    double *val;
+    long long n2;
+};
+
 template <int DIMS>
+__device__ __forceinline__ void put_record(const GridP &g, const RecOut &ro, long long r, long long cell,
+                                           const double *o)
+{
+    constexpr int NE = DIMS == 3 ? 12 : 8;
+    ro.key[r] = (uint32_t)cell;
+#pragma unroll
+    for (int e = 0; e < NE; e++) ro.val[e * ro.n2 + r] = o[e];
+}
+
+template <int DIMS, bool RECORD>
 __global__ void __launch_bounds__(kThreads) k_move_f64(GridP g, PartF64 p, const Counters *__restrict__ cnt,
                                                        const double *__restrict__ Ex, const double *__restrict__ Ey,
                                                        const double *__restrict__ Ez, const double *__restrict__ Bx,
                                                        const double *__restrict__ By, const double *__restrict__ Bz,
-                                                       double *Jx, double *Jy, double *Jz, int *err)
+                                                       double *Jx, double *Jy, double *Jz, int *err, RecOut ro)
 {
     const long long used = cnt->used;
     const double c = g.c, sqc = g.sqc, cinv = g.cinv, qi = g.qi;
     for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
+        if (RECORD) {   // nothing recorded unless the particle deposits below
+            ro.key[2 * n] = (uint32_t)g.ncell;
+            ro.key[2 * n + 1] = (uint32_t)g.ncell;
+        }
         const int flv = p.flv[n];
         if (flv == 0) continue;  // hole: moves nothing, deposits zero
         const double x0 = p.x[n], y0 = p.y[n], z0 = p.z[n];
@@ -52,6 +79,10 @@ __global__ void __launch_bounds__(kThreads) k_move_f64(GridP g, PartF64 p, const
         }
         double u = p.u[n], v = p.v[n], w = p.w[n], gg;
         boris<double>(c, sqc, cinv, pE, pB, u, v, w, gg);
+        if (!finite3(u, v, w)) {
+            raise_error(err, PIC_DEVERR_NAN);
+            continue;
+        }
         const double x1 = x0 + (u * gg) * 1.0, y1 = y0 + (v * gg) * 1.0, z1 = z0 + (w * gg) * 1.0; // :169-171
         // zigzag deposit, movdep.F90:177-237
         const int ip = (int)x1, jp = (int)y1, kp = (int)z1;
@@ -62,10 +93,12 @@ __global__ void __launch_bounds__(kThreads) k_move_f64(GridP g, PartF64 p, const
         double o[12];
         segment<double, DIMS>(qthis * (xr - x0), qthis * (yr - y0), qthis * (zr - z0), 0.5 * (x0 + xr) - ip0,
                               0.5 * (y0 + yr) - jp0, DIMS == 3 ? 0.5 * (z0 + zr) - kp0 : 0.0, o);
-        scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip0, jp0, DIMS == 3 ? kp0 : 1), o);
+        if (RECORD) put_record<DIMS>(g, ro, 2 * n, cidx(g, ip0, jp0, DIMS == 3 ? kp0 : 1), o);
+        else scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip0, jp0, DIMS == 3 ? kp0 : 1), o);
         segment<double, DIMS>(qthis * (x1 - xr), qthis * (y1 - yr), qthis * (z1 - zr), 0.5 * (x1 + xr) - ip,
                               0.5 * (y1 + yr) - jp, DIMS == 3 ? 0.5 * (z1 + zr) - kp : 0.0, o);
-        scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip, jp, DIMS == 3 ? kp : 1), o);
+        if (RECORD) put_record<DIMS>(g, ro, 2 * n + 1, cidx(g, ip, jp, DIMS == 3 ? kp : 1), o);
+        else scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip, jp, DIMS == 3 ? kp : 1), o);
         p.u[n] = u;
         p.v[n] = v;
         p.w[n] = w;
@@ -80,15 +113,112 @@ __global__ void __launch_bounds__(kThreads) k_move_f64(GridP g, PartF64 p, const
     }
 }
 
+// The records' count: two per particle slot.
+__global__ void k_record_count(const Counters *__restrict__ cnt, long long *count) { *count = 2 * cnt->used; }
+
+// VecJ of every cell that has records: the thread at the first sorted record
+// of a cell sums the cell's records in sorted order (particle order, segment
+// 1 before 2) from +0, as the serial build adds to its zeroed VecJ
+// (movdep.F90:209,233).  Cells without records keep the zeros of the memset.
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_vecj_sum(GridP g, const uint32_t *__restrict__ key,
+                                                       const uint32_t *__restrict__ idx, const long long *__restrict__ count,
+                                                       const double *__restrict__ val, long long n2, double *vecj)
+{
+    constexpr int NE = DIMS == 3 ? 12 : 8;
+    const long long n = *count;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const uint32_t k = key[q];
+        if (k >= (uint32_t)g.ncell || (q > 0 && key[q - 1] == k)) continue;
+        double acc[NE];
+#pragma unroll
+        for (int e = 0; e < NE; e++) acc[e] = 0.0;
+        for (long long t = q; t < n && key[t] == k; t++) {
+            const long long r = idx[t];
+#pragma unroll
+            for (int e = 0; e < NE; e++) acc[e] = acc[e] + val[e * n2 + r];
+        }
+#pragma unroll
+        for (int e = 0; e < NE; e++) vecj[e * g.ncell + k] = acc[e];
+    }
+}
+
+// J from VecJ in the loop order of ReduceCurrentMatrix (movdep_routines.F90:
+// 262-308: cells i = 1..mx-1, j = 1..my-1, k = 1..mz-1 in column-major order,
+// entries 0..NE-1 within a cell, added onto J zeroed by ResetCurrent).  An
+// edge receives the entries of up to 4 cells; they are added in the order
+// the loop visits those cells (increasing linear index).
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_assemble_j(GridP g, const double *__restrict__ vecj, double *Jx,
+                                                         double *Jy, double *Jz)
+{
+    const long long N = g.ncell;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode_cell(g, (int)c, i, j, k);
+        // source cell (a, b, d) = (i - da, j - db, k - dd) takes part if inside the loop range
+        auto V = [&](int e, int da, int db, int dd) -> double {
+            const int a = i - da, b = j - db, d = k - dd;
+            if (a < 1 || a > g.mx - 1 || b < 1 || b > g.my - 1) return 0.0;
+            if (DIMS == 3 && (d < 1 || d > g.mz - 1)) return 0.0;
+            return vecj[e * N + (c - da - db * g.sy - dd * g.sz)];
+        };
+        if (DIMS == 3) {
+            Jx[c] = (((0.0 + V(3, 0, 1, 1)) + V(2, 0, 0, 1)) + V(1, 0, 1, 0)) + V(0, 0, 0, 0);
+            Jy[c] = (((0.0 + V(7, 1, 0, 1)) + V(6, 0, 0, 1)) + V(5, 1, 0, 0)) + V(4, 0, 0, 0);
+            Jz[c] = (((0.0 + V(11, 1, 1, 0)) + V(10, 0, 1, 0)) + V(9, 1, 0, 0)) + V(8, 0, 0, 0);
+        } else {
+            Jx[c] = (0.0 + V(1, 0, 1, 0)) + V(0, 0, 0, 0);
+            Jy[c] = (0.0 + V(3, 1, 0, 0)) + V(2, 0, 0, 0);
+            Jz[c] = (((0.0 + V(7, 1, 1, 0)) + V(6, 0, 1, 0)) + V(5, 1, 0, 0)) + V(4, 0, 0, 0);
+        }
+    }
+}
+
+static unsigned grid_for(long long n)
+{
+    long long b = (n + kThreads - 1) / kThreads;
+    if (b > (long long)kSMs * 32) b = (long long)kSMs * 32;
+    return (unsigned)(b < 1 ? 1 : b);
+}
+
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
-                             double *const B[3], double *const J[3], int *err, cudaStream_t s)
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s, SegRecords *rec)
 {
     const int grid = kSMs * 16;
+    if (!rec) {
+        const RecOut ro = {nullptr, nullptr, 0};
+        if (g.dims == 3)
+            k_move_f64<3, false><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1],
+                                                          J[2], err, ro);
+        else
+            k_move_f64<2, false><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1],
+                                                          J[2], err, ro);
+        count_launches(1);
+        return;
+    }
+    const RecOut ro = {rec->sc.key[0], rec->val, rec->n2};
+    const int NE = g.dims == 3 ? 12 : 8;
     if (g.dims == 3)
-        k_move_f64<3><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+        k_move_f64<3, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
+                                                     err, ro);
     else
-        k_move_f64<2><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
-    count_launches(1);
+        k_move_f64<2, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
+                                                     err, ro);
+    k_record_count<<<1, 1, 0, s>>>(cnt, rec->count);
+    count_launches(2);
+    const int r = radix_sort_keys(rec->sc, rec->count, sort_key_bits(g.ncell), s);
+    cudaMemsetAsync(rec->vecj, 0, (size_t)NE * (size_t)g.ncell * sizeof(double), s);
+    const unsigned gq = grid_for(rec->n2);
+    if (g.dims == 3)
+        k_vecj_sum<3><<<gq, kThreads, 0, s>>>(g, rec->sc.key[r], rec->sc.idx[r], rec->count, rec->val, rec->n2,
+                                              rec->vecj);
+    else
+        k_vecj_sum<2><<<gq, kThreads, 0, s>>>(g, rec->sc.key[r], rec->sc.idx[r], rec->count, rec->val, rec->n2,
+                                              rec->vecj);
+    if (g.dims == 3) k_assemble_j<3><<<grid_for(g.ncell), kThreads, 0, s>>>(g, rec->vecj, J[0], J[1], J[2]);
+    else k_assemble_j<2><<<grid_for(g.ncell), kThreads, 0, s>>>(g, rec->vecj, J[0], J[1], J[2]);
+    count_launches(2);
 }
 
 }  // namespace pic

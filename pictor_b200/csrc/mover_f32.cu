@@ -275,6 +275,10 @@ __device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint3
     }
     float u = s.ux, v = s.uy, w = s.uz, gg;
     boris_f32(g.c_f, g.sqc_f, g.cinv_f, pE, pB, u, v, w, gg);
+    if (!finite3(u, v, w)) {   // the particle keeps its state (see finite3)
+        raise_error(err, PIC_DEVERR_NAN);
+        return false;
+    }
     // displacement in cell units, positions relative to this cell's corner
     const float x1 = fmaf(u, gg, dx), y1 = fmaf(v, gg, dy), z1 = DIMS == 3 ? fmaf(w, gg, dz) : 0.f;
     // |displacement| < c < 1, so x1 lies in (-1, 2): the cell step is -1, 0 or 1

@@ -17,8 +17,6 @@
 // overlaps on the GPU (on different streams, or from different host threads)
 // race on it.  Each call overwrites every partial it later reads, so nothing
 // in it has to start at zero, and it keeps the last call's contents.
-#include <mutex>
-
 #include "common.cuh"
 #include "kernels.cuh"
 
@@ -30,22 +28,15 @@ constexpr int kNoAllocMaxBlocks = kSMs * 8;
 
 static __device__ __align__(256) double g_energy_partials[2 * kNoAllocMaxBlocks];
 
-// Device address of g_energy_partials, looked up once per device (with that
-// device current): in host code the symbol is only a host-side stand-in.
-static std::mutex g_noalloc_mutex;
-static double *g_noalloc_ptr[64] = {};
-
+// Device address of g_energy_partials in the current context: in host code
+// the symbol is only a host-side stand-in.  Looked up on every call (no
+// allocation, a table look-up in the runtime), so the address stays right
+// after a cudaDeviceReset or on another device made current.
 static int noalloc_scratch(double **out)
 {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PIC_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        double *p = nullptr;
-        if (cudaGetSymbolAddress((void **)&p, g_energy_partials) != cudaSuccess || !p) return PIC_ERR_CUDA;
-        g_noalloc_ptr[dev] = p;
-    }
-    *out = g_noalloc_ptr[dev];
+    double *p = nullptr;
+    if (cudaGetSymbolAddress((void **)&p, g_energy_partials) != cudaSuccess || !p) return PIC_ERR_CUDA;
+    *out = p;
     return PIC_OK;
 }
 
@@ -74,7 +65,7 @@ extern "C" int pic_field_energy_noalloc(const double *Ex, const double *Ey, cons
     const int nblocks = field_energy_blocks(g);
     if (nblocks < 1 || nblocks > kNoAllocMaxBlocks) return PIC_ERR_INVALID;  // beyond the scratch array
     double *partials = nullptr;
-    const int r = noalloc_scratch(&partials);  // first call on a device: symbol look-up
+    const int r = noalloc_scratch(&partials);
     if (r) return r;
     const void *E[3] = {Ex, Ey, Ez}, *B[3] = {Bx, By, Bz};
     launch_field_energy(g, E, B, false, partials, nblocks, out2, (cudaStream_t)stream);

@@ -211,12 +211,19 @@ static int radix_sort(SortScratch &sc, const long long *used, int nbits, size_t 
     return cur;
 }
 
+int radix_sort_keys(SortScratch &sc, const long long *used, int nbits, cudaStream_t s)
+{
+    return radix_sort(sc, used, nbits, sc.ntiles, s);
+}
+
 static int key_bits(long long ncell)
 {
     int b = 1;
     while ((1ll << b) <= ncell) b++;
     return b;
 }
+
+int sort_key_bits(long long ncell) { return key_bits(ncell); }
 
 // ---------------------------------------------------------------------------
 // ReorderPrtlArr (mem_prtl.F90:166-301)
@@ -465,12 +472,16 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
     }
 }
 
+// The scatter stops before moving anything when the appended particles would
+// pass the capacity or the x leavers the outbox; the count then stays as it
+// was (and the overflow bit is set), so no stale slot becomes live.
 __global__ void k_exch_finish(Counters *cnt, const uint32_t *__restrict__ total, const uint32_t *__restrict__ sent,
-                              long long capacity)
+                              long long capacity, long long out_cap)
 {
-    const long long t = (long long)*total - (sent ? (long long)*sent : 0);
+    const long long s = sent ? (long long)*sent : 0;
+    const long long t = (long long)*total - s;
     cnt->append = t;
-    if (cnt->used + t <= capacity) cnt->used += t;
+    if (cnt->used + t <= capacity && s <= out_cap) cnt->used += t;
 }
 
 void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch &sc, long long capacity, int *err,
@@ -486,7 +497,7 @@ void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch 
         k_exch_scatter<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err, out, out_cap);
     else
         k_exch_scatter<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err, out, out_cap);
-    k_exch_finish<<<1, 1, 0, s>>>(cnt, total, g.x_external ? counts + 2 * ntiles : nullptr, capacity);
+    k_exch_finish<<<1, 1, 0, s>>>(cnt, total, g.x_external ? counts + 2 * ntiles : nullptr, capacity, out_cap);
     if (g.x_external && sent_counts) {
         // right-bound (face 2, slot 0) and right + left-bound particle counts
         cudaMemcpyAsync(sent_counts, counts + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);

@@ -55,6 +55,7 @@ class PicConfig:
     brick: tuple = (0, 0, 0)   # FP32 form: brick shape in cells, (0, 0, 0) = from the fill
     cyl_modes: int = 0         # cylindrical: 0 = theta-gridded field solve, 2 = modes m = 0, 1
     slab_x: int = 0            # 1 = one slab of a domain split along x (pictor_b200.slab)
+    exact_current: int = 0     # FP64: 1 = current summed in the reference's serial order (bit-exact J)
 
     def to_struct(self) -> _capi.Config:
         s = _capi.Config()
@@ -78,6 +79,7 @@ class PicConfig:
             s.brick[d] = int(self.brick[d])
         s.cyl_modes = int(self.cyl_modes)
         s.slab_x = int(self.slab_x)
+        s.exact_current = int(self.exact_current)
         return s
 
     @property

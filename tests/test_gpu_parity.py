@@ -178,6 +178,31 @@ def test_diagnostics_match_oracle():
         assert d["gauss_linf"] <= 1e-12 * rmax and res <= 1e-12 * rmax
 
 
+@pytest.mark.parametrize("dims,prec", [(2, "fp64"), (3, "fp64"), (2, "fp32"), (3, "fp32")])
+def test_kinetic_energy_matches_oracle(dims, prec):
+    """CalcPrtlEnergy (savedata_routines.F90:283-308) per species on the
+    device (FP64 accumulation) against orc_particle_energy, on the loader's
+    particles and after 6 steps.  FP64: the sums differ by their order only
+    (1e-12); FP32: the momenta are FP32 (1e-6 of each species' energy)."""
+    nx, ny, nz = (24, 24, 1) if dims == 2 else (10, 8, 8)
+    sc_qi = 0.00158203125
+    g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, qi=sc_qi, precision=prec, reorder_period=4)
+    p = O.load_weibel(dims, nx, ny, nz, epc=8, drift=0.5, temp=0.005, seed=4)
+    o = O.Oracle(g, p.copy())
+    masse = sc_qi
+    tol = 1e-12 if prec == "fp64" else 1e-6
+    with _sim(cfg) as s:
+        s.load_particles(to_gpu_particles(p))
+        np.testing.assert_allclose(s.diagnostics(masse)["kinetic"], o.particle_energy(masse), rtol=tol)
+        s.step(6)
+        # the oracle's energies of the device's own particles after 6 steps
+        o2 = O.Oracle(g, O.Particles.from_arrays(1 << 15, **{k: getattr(s.fetch_particles(), k)
+                                                              for k in ("q", "x", "y", "z", "u", "v", "w", "flv")}))
+        ke = s.diagnostics(masse)["kinetic"]
+        assert (ke > 0).all()
+        np.testing.assert_allclose(ke, o2.particle_energy(masse), rtol=tol if prec == "fp64" else 1e-9)
+
+
 @pytest.mark.parametrize("dims", [2, 3])
 def test_current_filter_bit_exact(dims):
     """smoothen_current (current.F90:19-163): two passes of the (1/4,1/2,1/4)

@@ -274,3 +274,21 @@ def test_empty_and_all_hole_particle_sets(dims):
     assert o.p.used == 0
     for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
         np.testing.assert_array_equal(getattr(o.f, n), getattr(o_vac.f, n), err_msg=n)
+
+
+def test_particle_energy_known_answer():
+    """CalcPrtlEnergy (savedata_routines.F90:283-308): (gamma - 1) |w| times
+    (q qi / qm) c^2 for a positive charge and masse c^2 for a negative one,
+    summed per species; holes count nothing."""
+    g = O.make_grid(2, 8, 8, c=0.45, qi=0.01, qm=(1.0, -1.0))
+    u = np.array([0.3, 0.0, 1.2, 0.5])
+    v = np.array([0.4, 0.0, 0.0, 0.5])
+    flv = np.array([1, 2, 2, 0], dtype=np.int32)
+    q = np.array([2.0, -1.5, -0.5, 0.0])
+    p = O.Particles.from_arrays(8, q=q, x=np.full(4, 4.5), y=np.full(4, 4.5), z=np.full(4, 1.5), u=u, v=v,
+                                w=np.zeros(4), flv=flv)
+    masse = 0.01
+    gm = np.sqrt(1.0 + u * u + v * v)
+    e1 = (gm[0] - 1.0) * 2.0 * (2.0 * 0.01 / 1.0) * 0.45 ** 2
+    e2 = (gm[1] - 1.0) * 1.5 * masse * 0.45 ** 2 + (gm[2] - 1.0) * 0.5 * masse * 0.45 ** 2
+    np.testing.assert_allclose(O.Oracle(g, p).particle_energy(masse), [e1, e2], rtol=1e-14)

@@ -16,13 +16,15 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("dims", [2, 3])
-def test_noalloc_energy_matches_diagnostics(dims):
+# (2, 40, 24, 1) and (3, 20, 12, 10) launch one block per 2048 interior cells;
+# 160 x 128 x 128 = 2.6 M interior cells reaches the cap of 148 * 8 blocks, so
+# the blocks stride over the grid and every slot of the fixed scratch is used.
+@pytest.mark.parametrize("dims,nx,ny,nz", [(2, 40, 24, 1), (3, 20, 12, 10), (3, 160, 128, 128)])
+def test_noalloc_energy_matches_diagnostics(dims, nx, ny, nz):
     import torch
 
     from pictor_b200 import Fields, PicConfig, Simulation, _capi
 
-    nx, ny, nz = (40, 24, 1) if dims == 2 else (20, 12, 10)
     cfg = PicConfig(nx=nx, ny=ny, nz=nz, dims=dims, capacity=1024)
     rng = np.random.default_rng(3)
     host = Fields.zeros(cfg.shape)
