@@ -16,6 +16,7 @@ region is bracketed by a barrier and the max over ranks is taken.
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -33,16 +34,16 @@ METRIC = "particle-steps/s on 1 B200 (FP32/batched vs plain FP64) at stated ener
 WORKLOADS = {
     # configs: the 3D FP32 Weibel run (headline) and the 2D FP64 Weibel run
     "weibel3d_fp32": dict(dims=3, nx=512, ny=256, nz=256, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
-                          precision="fp32"),
+                          precision="fp32", horizon=200),
     "weibel2d_fp64": dict(dims=2, nx=256, ny=256, nz=1, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0,
-                          precision="fp64"),
+                          precision="fp64", horizon=1000),
     # a small case of the headline physics for profiler captures (particles 270 MB > L2)
     "weibel3d_fp32_small": dict(dims=3, nx=128, ny=64, nz=64, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
-                                precision="fp32"),
+                                precision="fp32", horizon=200),
     # the batched ensemble: 64 independent 2D Weibel runs, grid 64^2..512^2, 4..32 particles per cell per
     # species, drift U(0.1, 0.9) c, spread U(0.01, 0.1) c, seed 2930 + run (pictor_b200.ensemble)
     "ensemble64": dict(dims=2, runs=64, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0, precision="fp32",
-                       nx=256, ny=256, nz=1),
+                       nx=256, ny=256, nz=1, horizon=500),
     # the 2D FP64 Weibel configuration split along x into one slab per rank (strong scaling: the
     # global grid fixed), the slabs exchanging their x faces over NCCL between the phases
     "slab_weibel2d_fp64": dict(dims=2, nx=256, ny=256, nz=1, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0,
@@ -63,11 +64,11 @@ WORKLOADS = {
                            bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0, cyl_modes=2),
     # the same run in the FP32 cell-relative form (theta-gridded FP32 fields)
     "cyl_wake_fp32": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp32", thermal=0.01,
-                          bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0),
+                          bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0, horizon=2000),
     # the C3 configuration as stated: modes m = 0, 1, FP32 fields and particles
     "cyl_wake_modal_fp32": dict(dims=3, nx=256, ny=8, nz=2048, epc=8, c=0.3, c_ompe=10.0, precision="fp32",
                                 thermal=0.01, bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=20.0, bunch_sigma_z=40.0,
-                                cyl_modes=2),
+                                cyl_modes=2, horizon=2000),
     # small cases of the same physics for profiler captures (4.2 M particles, 250 MB > L2)
     "cyl_wake_small_modal_fp32": dict(dims=3, nx=64, ny=8, nz=1024, epc=8, c=0.3, c_ompe=10.0, precision="fp32",
                                       thermal=0.01, bunch_gamma=50.0, bunch_peak=0.1, bunch_sigma_r=5.0,
@@ -250,6 +251,38 @@ def timed_steps(sim, steps: int, ws: int, profile: bool):
     return ms, phases, launches
 
 
+def energy_curve(sim, sc, done: int, horizon: int, every: int = 20) -> dict:
+    """Step a run from step `done` to `horizon`, recording its energies at
+    every multiple of `every` (and at the horizon)."""
+    curve = {}
+    t = done
+    while t < horizon:
+        nxt = min(horizon, (t // every + 1) * every)
+        sim.step(nxt - t)
+        t = nxt
+        curve[t] = energies(sim, sc)
+    return curve
+
+
+def curve_errors(a: dict, b: dict) -> dict:
+    """Max relative differences of curve a from curve b (FP64) over their
+    common steps: field, kinetic and total energy; and the values at the last."""
+    steps = sorted(set(a) & set(b))
+    if not steps:
+        return {}
+    def rel(x, y):
+        return abs(x - y) / max(abs(y), 1e-300)
+    last = steps[-1]
+    return {"steps_compared": [steps[0], last], "points": len(steps),
+            "field_energy_rel_err_max": max(rel(a[t]["field"], b[t]["field"]) for t in steps),
+            "kinetic_energy_rel_err_max": max(rel(a[t]["kinetic"], b[t]["kinetic"]) for t in steps),
+            "total_energy_rel_err_max": max(rel(a[t]["field"] + a[t]["kinetic"], b[t]["field"] + b[t]["kinetic"])
+                                            for t in steps),
+            "field_energy_at_horizon": {"fp32": a[last]["field"], "fp64": b[last]["field"]},
+            "gauss_linf_over_rho_at_horizon": {"fp32": a[last]["gauss_linf"] / max(a[last]["rho_max"], 1e-300),
+                                               "fp64": b[last]["gauss_linf"] / max(b[last]["rho_max"], 1e-300)}}
+
+
 def energies(sim, sc) -> dict:
     d = sim.diagnostics(sc["masse"])
     return {"field": 0.5 * (d["B2"] + d["E2"]), "B": 0.5 * d["B2"], "kinetic": float(sum(d["kinetic"])),
@@ -272,7 +305,7 @@ def cpu_sample(wl: dict, target_s: float = 12.0, threads: int | None = None):
     qi = O.init_scale(wl["c"], wl["c_ompe"], wl["epc"])[0]
     g = O.make_grid(dims, nx, ny, nz, c=wl["c"], qi=qi)
     p = O.load_weibel(dims, nx, ny, nz, epc=wl["epc"], drift=wl["drift"], temp=wl["temp"], seed=SEED)
-    o = O.Oracle(g, p, openmp=True)
+    o = O.Oracle(g, p, openmp=True, exact_order=False)   # the reference's thread slices
     o.step(1)
     n_steps, t0, t = 0, time.perf_counter(), 1
     while True:
@@ -286,6 +319,74 @@ def cpu_sample(wl: dict, target_s: float = 12.0, threads: int | None = None):
     return {"value": p.used * n_steps / el, "unit": "particle-steps/s", "cores": cores, "kind": "port",
             "sample": f"{'x'.join(map(str, (nx, ny, nz)[:dims]))} cells, {p.used} particles, {n_steps} steps "
                       f"(same physics and seed), FP64, C restatement of the reference CPU path with OpenMP"}
+
+
+def parity_weibel2d(wl: dict, horizon: int, every: int = 10) -> dict:
+    """The 2D FP64 Weibel configuration at full size stepped to its horizon on
+    the GPU and in the OpenMP C restatement (exact order: each cell's current
+    in particle order, the serial build's result), from the same particles:
+    the exact-order current (pic_config.exact_current = 1), compared bit for
+    bit at the horizon and in its energies every `every` steps, and the
+    default atomic current, whose rounding differences the instability
+    amplifies, in its energy curves."""
+    import numpy as np
+
+    from oracle import oracle as O
+    from pictor_b200 import Particles, PicConfig, Simulation, init_scale
+
+    sc = init_scale(wl["c"], wl["c_ompe"], wl["epc"])
+    nx, ny = wl["nx"], wl["ny"]
+    g = O.make_grid(2, nx, ny, c=wl["c"], qi=sc["qi"])
+    p = O.load_weibel(2, nx, ny, epc=wl["epc"], drift=wl["drift"], temp=wl["temp"], seed=SEED)
+    v = p.view()
+    host = Particles(*(v[k].copy() for k in ("q", "x", "y", "z", "u", "v", "w")), v["flv"].astype(np.int32))
+    o = O.Oracle(g, p.copy(), openmp=True, exact_order=True)
+    cap = int(p.used * 1.3) + 65536
+    mk = lambda exact: PicConfig(nx=nx, ny=ny, dims=2, c=wl["c"], qi=sc["qi"], precision="fp64",  # noqa: E731
+                                 capacity=cap, reorder_period=20, exact_current=exact)
+    err = {"exact": {"field": 0.0, "kinetic": 0.0}, "atomic": {"field": 0.0, "kinetic": 0.0}}
+    gauss = {"exact": 0.0, "oracle": 0.0}
+    t_oracle = t_gpu = 0.0
+    with Simulation(mk(1)) as se, Simulation(mk(0)) as sf:
+        se.load_particles(host)
+        sf.load_particles(host)
+        for t in range(1, horizon + 1):
+            c0 = time.perf_counter()
+            o.step(t, 20)
+            c1 = time.perf_counter()
+            se.step(1)
+            sf.step(1)
+            t_oracle += c1 - c0
+            t_gpu += time.perf_counter() - c1
+            if t % every == 0 or t == horizon:
+                ob, oe = o.field_energy()
+                of = 0.5 * (ob + oe)
+                ok = float(sum(o.particle_energy(sc["masse"])))
+                for name, sim in (("exact", se), ("atomic", sf)):
+                    d = sim.diagnostics(sc["masse"])
+                    fe, ke = 0.5 * (d["B2"] + d["E2"]), float(sum(d["kinetic"]))
+                    err[name]["field"] = max(err[name]["field"], abs(fe - of) / of)
+                    err[name]["kinetic"] = max(err[name]["kinetic"], abs(ke - ok) / ok)
+                    if name == "exact":
+                        gauss["exact"] = max(gauss["exact"], d["gauss_linf"] / max(d["rho_max"], 1e-300))
+            if t % 100 == 0 or t == horizon:
+                res, rmax = o.gauss_residual()
+                gauss["oracle"] = max(gauss["oracle"], res / max(rmax, 1e-300))
+        gp = se.fetch_particles()
+        gf = se.fetch_fields(with_current=False)
+        ov = o.p.view()
+        same_p = len(gp.x) == o.p.used and all(np.array_equal(getattr(gp, k), ov[k]) for k in ("q", "x", "y", "z", "u", "v", "w", "flv"))
+        same_f = all(np.array_equal(getattr(gf, n), getattr(o.f, n)) for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"))
+    return {"horizon_steps": horizon, "particles": int(p.used), "energies_every": every,
+            "oracle": f"OpenMP C restatement of the reference CPU path, exact order, "
+                      f"{os.environ.get('OMP_NUM_THREADS', os.cpu_count())} threads",
+            "exact_current": {"bit_exact_particles_at_horizon": bool(same_p),
+                              "bit_exact_fields_at_horizon": bool(same_f),
+                              "field_energy_rel_diff_max": err["exact"]["field"],
+                              "kinetic_energy_rel_diff_max": err["exact"]["kinetic"]},
+            "atomic_current": {"field_energy_rel_diff_max": err["atomic"]["field"],
+                               "kinetic_energy_rel_diff_max": err["atomic"]["kinetic"]},
+            "gauss_linf_over_rho_max": gauss, "seconds": {"oracle": t_oracle, "gpu_both_forms": t_gpu}}
 
 
 def run_slab_bench(args, ws, rank, local, peak, peak_kind):
@@ -367,11 +468,14 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
     t0 = time.perf_counter()
     tunings = tune_classes(mine)
     tune_s = time.perf_counter() - t0
+    horizon = args.horizon if args.horizon is not None else wl.get("horizon", 0)
+    if args.no_fp64:
+        horizon = 0
     run_batched(mine, args.warmup, "fp32", tunings)                      # warm-up (graph capture, clocks)
     clocks = ClockSampler(local)
     clocks.start()
     barrier(ws)
-    res32, t32 = run_batched(mine, args.steps, "fp32", tunings)
+    res32, t32 = run_batched(mine, args.steps, "fp32", tunings, horizon=horizon)
     barrier(ws)
     clk = clocks.stop()
     secs = max_over_ranks(ws, t32["seconds"])
@@ -390,16 +494,32 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
                          "its runs, one CUDA graph per group and step"}
     fp64 = None
     if not args.no_fp64:
-        res64, t64 = run_batched(mine, args.steps, "fp64", None, batched=False)
+        def errs(r32, r64):
+            ef = max(abs((a["B2"] + a["E2"]) - (b["B2"] + b["E2"])) / max(b["B2"] + b["E2"], 1e-300)
+                     for a, b in zip(r32, r64))
+            et = max(abs((0.5 * (a["B2"] + a["E2"]) + sum(a["kinetic"])) - (0.5 * (b["B2"] + b["E2"]) + sum(b["kinetic"])))
+                     / abs(0.5 * (b["B2"] + b["E2"]) + sum(b["kinetic"])) for a, b in zip(r32, r64))
+            return ef, et
+        # the same runs in the plain FP64 form, stepped together as the FP32 runs are (pic_step_many)
+        res64, t64 = run_batched(mine, args.steps, "fp64", None, batched=True, horizon=horizon)
         secs64 = max_over_ranks(ws, t64["seconds"])
         v64 = sum_over_ranks(ws, t64["particle_steps"]) / secs64
-        err_f = max(abs((a["B2"] + a["E2"]) - (b["B2"] + b["E2"])) / max(b["B2"] + b["E2"], 1e-300)
-                    for a, b in zip(res32, res64))
-        err_t = max(abs((0.5 * (a["B2"] + a["E2"]) + sum(a["kinetic"])) - (0.5 * (b["B2"] + b["E2"]) + sum(b["kinetic"])))
-                    / abs(0.5 * (b["B2"] + b["E2"]) + sum(b["kinetic"])) for a, b in zip(res32, res64))
+        err_f, err_t = errs(res32, res64)
+        # and one after the other
+        _, t64s = run_batched(mine, args.steps, "fp64", None, batched=False)
+        secs64s = max_over_ranks(ws, t64s["seconds"])
+        v64s = sum_over_ranks(ws, t64s["particle_steps"]) / secs64s
         fp64 = {"value": v64, "seconds": secs64, "speedup_fp32_batched_over_fp64": value / v64,
                 "max_field_energy_rel_err": err_f, "max_total_energy_rel_err": err_t,
-                "form": "plain FP64 reference layout, runs stepped one after the other"}
+                "errors_at": f"step {args.steps}",
+                "form": "plain FP64 reference layout, the runs stepped together on their own streams (pic_step_many)",
+                "one_after_the_other": {"value": v64s, "seconds": secs64s,
+                                        "speedup_fp32_batched_over_fp64": value / v64s}}
+        if horizon and "horizon" in t32 and "horizon" in t64:
+            hf, ht = errs(t32["horizon"], t64["horizon"])
+            fp64["horizon"] = {"steps": horizon, "max_field_energy_rel_err": hf, "max_total_energy_rel_err": ht,
+                               "form": "every run continued to step 500 in both forms; the largest per-run "
+                                       "relative difference"}
     # end to end: particles from pinned FP64 host arrays for every run, the steps, the diagnostics
     from pictor_b200.ensemble import make_run, size_class
     from pictor_b200.simulation import step_many
@@ -689,6 +809,19 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
     move_ms = phases["ms"]["move"] / max(phases["steps"], 1)
     n_cells = wl["nx"] * wl["ny"] * wl["nz"]
     bytes_move = n_p * bytes_per_particle(3, wl["precision"]) + n_cells * bytes_per_cell_mover(wl["precision"])
+    # the FP32 form against the FP64 form of the same run to the configuration's horizon
+    horizon_cmp = None
+    horizon = args.horizon if args.horizon is not None else wl.get("horizon", 0)
+    if wl["precision"] == "fp32" and horizon and not args.no_fp64:
+        curves = {}
+        for prec in ("fp32", "fp64"):
+            with Simulation(dataclasses.replace(cfg, precision=prec)) as sim:
+                sim.load_particles(pinned)
+                sim.reorder()
+                curves[prec] = energy_curve(sim, sc, 0, horizon, every=100)
+        horizon_cmp = {"steps": horizon, "every": 100, **curve_errors(curves["fp32"], curves["fp64"]),
+                       "form": "the FP32 form and the FP64 form of the same run (same field solve), "
+                               "energies compared every 100 steps"}
     cpu = None if args.no_cpu else cpu_sample_cyl(wl)
     if rank == 0:
         line = {
@@ -711,6 +844,7 @@ def run_cyl_bench(args, rank, local, peak, peak_kind):
             "phases_ms_per_step": {k: v / max(phases["steps"], 1) for k, v in phases["ms"].items()},
             "gpu_launches": launches, "clocks": clk,
             "energy": {"field": 0.5 * (d["B2"] + d["E2"]), "kinetic": float(sum(d["kinetic"]))},
+            **({"fp32_vs_fp64": horizon_cmp} if horizon_cmp else {}),
             "e2e": {"value": n_p * args.steps / e2e_s, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": n_p * 60 / args.steps,
                     "d2h_bytes_per_step": 6 * 8 * (wl["nx"] + 5) * (wl["ny"] + 5) * (wl["nz"] + 5) / args.steps,
@@ -757,6 +891,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end (host buffers) run")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-sweep", action="store_true", help="adjoint128: skip the finite-difference horizon sweep")
+    ap.add_argument("--parity", action="store_true",
+                    help="weibel2d_fp64: step the full configuration to its horizon on the GPU and in the "
+                         "OpenMP C restatement and report the differences")
+    ap.add_argument("--horizon", type=int, default=None,
+                    help="steps to which the FP32 and FP64 runs are continued for the energy comparison "
+                         "(default: the configuration's; 0 = none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -796,6 +936,12 @@ def main():
     ms, phases, launches = timed_steps(sim, args.steps, ws, profile=True)
     clk = clocks.stop()
     e32 = energies(sim, sc)
+    # the run continued to the configuration's horizon, energies every 20 steps
+    horizon = args.horizon if args.horizon is not None else wl.get("horizon", 0)
+    done = args.warmup + args.steps
+    curve32 = {done: e32}
+    if not args.no_fp64 and prec == "fp32" and horizon > done:
+        curve32.update(energy_curve(sim, sc, done, horizon))
     ms_max = max_over_ranks(ws, ms)
     n_tot = sum_over_ranks(ws, float(n_p))
     value = n_tot * args.steps / (ms_max * 1e-3)
@@ -817,6 +963,9 @@ def main():
         sim64.step(args.warmup)
         ms64, ph64, _ = timed_steps(sim64, args.steps, ws, profile=True)
         e64 = energies(sim64, sc)
+        curve64 = {done: e64}
+        if horizon > done:
+            curve64.update(energy_curve(sim64, sc, done, horizon))
         ms64 = max_over_ranks(ws, ms64)
         v64 = n_tot * args.steps / (ms64 * 1e-3)
         fp64 = {"value": v64, "ms_per_step": ms64 / args.steps, "speedup_fp32_over_fp64": value / v64,
@@ -825,7 +974,12 @@ def main():
                 / max(abs(e64["field"] + e64["kinetic"]), 1e-300),
                 "field_energy_fp64": e64["field"], "field_energy_fp32": e32["field"],
                 "gauss_linf_over_rho": e64["gauss_linf"] / max(e64["rho_max"], 1e-300),
-                "move_ms": ph64["ms"]["move"] / max(ph64["steps"], 1)}
+                "move_ms": ph64["ms"]["move"] / max(ph64["steps"], 1),
+                "errors_at": f"step {done} (the first three keys above)"}
+        if horizon > done:
+            fp64["horizon"] = {"steps": horizon, "every": 20, **curve_errors(curve32, curve64),
+                               "form": "both runs from the same seed to the configuration's horizon, energies "
+                                       "compared every 20 steps"}
         sim64.close()
         del sim64
 
@@ -906,6 +1060,8 @@ def main():
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if args.parity and args.workload == "weibel2d_fp64" and ws == 1:
+            line["parity"] = parity_weibel2d(wl, args.horizon or wl["horizon"])
         print(json.dumps(line), flush=True)
     if ws > 1:
         import torch.distributed as dist

@@ -103,6 +103,7 @@ def _declare(L: C.CDLL) -> None:
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
+    L.orc_set_exact_order.argtypes = [C.c_int]
     L.orc_particle_energy.argtypes = [P(Grid), P(_Particles), C.c_double, C.c_double, P(C.c_double)]
     L.orc_gauss_residual.argtypes = [P(Grid), P(_Fields), P(_Particles), P(C.c_double)]
     L.orc_gauss_residual.restype = C.c_double
@@ -221,11 +222,18 @@ class Particles:
 class Oracle:
     """Stateful wrapper: one grid, its fields and particles."""
 
-    def __init__(self, g: Grid, particles: Particles, fields: Fields | None = None, openmp: bool = False):
+    def __init__(self, g: Grid, particles: Particles, fields: Fields | None = None, openmp: bool = False,
+                 exact_order: bool = True):
+        """openmp: the OpenMP build; exact_order (OpenMP build only): each
+        cell's current summed in particle order, bit for bit the serial
+        build's result; False: the reference's thread slices.  The setting is
+        global to the OpenMP library and made again by every Oracle."""
         self.g = g
         self.p = particles
         self.f = fields if fields is not None else Fields(g)
         self.L = lib(openmp)
+        if openmp:
+            self.L.orc_set_exact_order(1 if exact_order else 0)
 
     def _call_p(self, fn, *extra):
         ps = self.p.struct()

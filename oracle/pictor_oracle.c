@@ -398,8 +398,10 @@ static void segment_values(int dims, double Fx, double Fy, double Fz, double Wx,
 }
 
 /* Per-particle body of movdep.F90:68-249.  Appends the two deposit segments
-   to VecJ (thread slice vj). */
-static void move_one(const orc_grid *g, orc_particles *p, const orc_fields *f, int64_t n, double *vj)
+   to VecJ (thread slice vj), or, with rec != NULL, stores them as the two
+   records rec[0], rec[1] (cell and values) for a later ordered sum. */
+static void move_one(const orc_grid *g, orc_particles *p, const orc_fields *f, int64_t n, double *vj,
+                     vecj_contrib *rec)
 {
     const int nc = g->dims == 3 ? 8 : 4, nj = g->dims == 3 ? 12 : 8;
     const double c = g->c, sqc = c * c, cinv = 1.0 / c;
@@ -471,7 +473,12 @@ static void move_one(const orc_grid *g, orc_particles *p, const orc_fields *f, i
         const double Wz1 = g->dims == 3 ? 0.5 * (z0 + zr) - kp0 : 0.0;
         const int64_t cell = g->dims == 3 ? ID(g, ip0, jp0, kp0) : ID(g, ip0, jp0, 1);
         segment_values(g->dims, Fx1, Fy1, Fz1, Wx1, Wy1, Wz1, seg);
-        for (int nn = 0; nn < nj; nn++) vj[cell * nj + nn] = vj[cell * nj + nn] + seg[nn];
+        if (rec) {
+            rec[0].cell = cell;
+            memcpy(rec[0].val, seg, sizeof(seg));
+        } else {
+            for (int nn = 0; nn < nj; nn++) vj[cell * nj + nn] = vj[cell * nj + nn] + seg[nn];
+        }
     }
     {
         const double Fx2 = qthis * (x1 - xr), Fy2 = qthis * (y1 - yr), Fz2 = qthis * (z1 - zr);
@@ -479,7 +486,12 @@ static void move_one(const orc_grid *g, orc_particles *p, const orc_fields *f, i
         const double Wz2 = g->dims == 3 ? 0.5 * (z1 + zr) - kp : 0.0;
         const int64_t cell = g->dims == 3 ? ID(g, ip, jp, kp) : ID(g, ip, jp, 1);
         segment_values(g->dims, Fx2, Fy2, Fz2, Wx2, Wy2, Wz2, seg);
-        for (int nn = 0; nn < nj; nn++) vj[cell * nj + nn] = vj[cell * nj + nn] + seg[nn];
+        if (rec) {
+            rec[1].cell = cell;
+            memcpy(rec[1].val, seg, sizeof(seg));
+        } else {
+            for (int nn = 0; nn < nj; nn++) vj[cell * nj + nn] = vj[cell * nj + nn] + seg[nn];
+        }
     }
     /* 2D periodic z, movdep.F90:241-249 (zmin=1, zmax=2, zlen=1) */
     if (g->dims == 2) {
@@ -527,6 +539,16 @@ static void reduce_current_matrix(const orc_grid *g, const double *vj, orc_field
     }
 }
 
+/* With OpenMP: 0 = the reference's OPEN_MP structure (thread-private VecJ
+   slices summed in thread order, movdep.F90:57-66 and
+   movdep_routines.F90:251-255), whose rounding depends on the thread count;
+   1 = each cell's VecJ entries summed in particle order, as the serial build
+   does, so that the result equals the serial build bit for bit at any thread
+   count (the particles are moved in parallel into per-particle records,
+   which a stable counting sort by cell groups for the per-cell sums). */
+static int g_exact_order = 0;
+void orc_set_exact_order(int on) { g_exact_order = on != 0; }
+
 void orc_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f)
 {
     const int nj = g->dims == 3 ? 12 : 8;
@@ -539,7 +561,31 @@ void orc_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f)
     int nthreads = 1;
 #endif
     if (nthreads <= 1 || p->used < 4096) {
-        for (int64_t n = 0; n < p->used; n++) move_one(g, p, f, n, vj);
+        for (int64_t n = 0; n < p->used; n++) move_one(g, p, f, n, vj, NULL);
+    } else if (g_exact_order) {
+#ifdef _OPENMP
+        const int64_t nrec = 2 * p->used;
+        vecj_contrib *rec = (vecj_contrib *)malloc((size_t)nrec * sizeof(vecj_contrib));
+        int64_t *start = (int64_t *)calloc(ncell + 1, sizeof(int64_t));
+        int64_t *order = (int64_t *)malloc((size_t)nrec * sizeof(int64_t));
+#pragma omp parallel for schedule(static)
+        for (int64_t n = 0; n < p->used; n++) move_one(g, p, f, n, NULL, rec + 2 * n);
+        for (int64_t r = 0; r < nrec; r++) start[rec[r].cell + 1]++;
+        for (size_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+        {
+            int64_t *fill = (int64_t *)malloc(ncell * sizeof(int64_t));
+            memcpy(fill, start, ncell * sizeof(int64_t));
+            for (int64_t r = 0; r < nrec; r++) order[fill[rec[r].cell]++] = r;
+            free(fill);
+        }
+#pragma omp parallel for schedule(static)
+        for (int64_t c = 0; c < (int64_t)ncell; c++)
+            for (int64_t t = start[c]; t < start[c + 1]; t++)
+                for (int nn = 0; nn < nj; nn++) vj[c * nj + nn] = vj[c * nj + nn] + rec[order[t]].val[nn];
+        free(order);
+        free(start);
+        free(rec);
+#endif
     } else {
 #ifdef _OPENMP
         /* OPEN_MP path of movdep.F90:57-66: blocks of 32 particles, one private
@@ -552,7 +598,7 @@ void orc_move_deposit(const orc_grid *g, orc_particles *p, orc_fields *f)
 #pragma omp for schedule(static)
             for (int64_t b = 0; b < nblocks; b++) {
                 const int64_t e = (b + 1) * 32 < p->used ? (b + 1) * 32 : p->used;
-                for (int64_t n = b * 32; n < e; n++) move_one(g, p, f, n, mine);
+                for (int64_t n = b * 32; n < e; n++) move_one(g, p, f, n, mine, NULL);
             }
 #pragma omp for schedule(static)
             for (int64_t cidx = 0; cidx < (int64_t)ncell; cidx++)

@@ -116,6 +116,10 @@ int orc_step_filtered(const orc_grid *g, orc_particles *p, orc_fields *f, int t,
 /* savedata_routines.F90 CalcFldEnergy (sums, not halved): out[0]=sum|B|^2,
    out[1]=sum|E|^2 over the interior 3..m-3. */
 void orc_field_energy(const orc_grid *g, const orc_fields *f, double out[2]);
+/* OpenMP build: 1 = sum each cell's current in particle order, bit for bit
+   the serial build's result at any thread count; 0 (default) = thread
+   slices as the reference's OPEN_MP path.  No effect in the serial build. */
+void orc_set_exact_order(int on);
 /* savedata_routines.F90 CalcPrtlEnergy: energy[flv-1] per species. */
 void orc_particle_energy(const orc_grid *g, const orc_particles *p, double masse, double massi, double *energy);
 /* L-infinity norm over interior nodes of divE - rho, with divE as in

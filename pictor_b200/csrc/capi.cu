@@ -63,6 +63,9 @@ struct pic_handle {
     // FP64 current summed in the serial order (pic_config.exact_current)
     bool exact = false;
     SegRecords rec = {};
+    // FP64 Cartesian mover by tiles of cells after a reorder (valid while `sorted`)
+    bool tiled64 = false;
+    Tiles64 t64 = {};
     std::vector<void *> allocs;
 };
 
@@ -349,7 +352,10 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 launch_bhalf<double>(g, E, B, h->s);
                 break;
             case PIC_PHASE_MOVE:  // MAIN.F90:63-71
-                launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s, h->exact ? &h->rec : nullptr);
+                if (h->tiled64 && h->sorted)
+                    launch_move_deposit_f64_tiled(g, h->p64[cur], h->cnt, h->t64, E, B, J, h->err, h->s);
+                else
+                    launch_move_deposit_f64(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s, h->exact ? &h->rec : nullptr);
                 break;
             case PIC_PHASE_EXCHANGE:  // MAIN.F90:86-94 + 145-150
                 launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s);
@@ -366,7 +372,8 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 break;
             case PIC_PHASE_REORDER:  // MAIN.F90:259-265
                 if (reorder)
-                    launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+                    launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s,
+                                       h->tiled64 ? &h->t64 : nullptr);
                 break;
         }
     } else {
@@ -449,7 +456,7 @@ int step_profiled(pic_handle *h, int32_t nsteps)
         }
         if (reorder) {
             h->cur ^= 1;
-            if (h->fp32) h->sorted = true;  // eager launches: no graph to drop
+            if (h->fp32 || h->tiled64) h->sorted = true;  // eager launches: no graph to drop
         }
         h->prof_steps += 1;
         if (cudaGetLastError() != cudaSuccess) rc = PIC_ERR_CUDA;
@@ -491,7 +498,7 @@ int enqueue_graph_step(pic_handle *h)
     h->launches += h->graph_kernels[reorder ? 1 : 0][h->cur];
     if (reorder) {
         h->cur ^= 1;
-        if (h->fp32 && !h->sorted) {  // tile ranges are valid from now on
+        if ((h->fp32 || h->tiled64) && !h->sorted) {  // tile ranges are valid from now on
             CK(cudaStreamSynchronize(h->s));
             set_sorted(h, true);
         }
@@ -980,6 +987,15 @@ int pic_create(const pic_config *cfg, pic_handle **out)
             (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
         }
     }
+    // the tiles of the FP64 Cartesian mover (the exact-order current keeps
+    // the per-particle mover, whose records it sorts anyway)
+    if (!r && c.geom == PIC_GEOM_CARTESIAN && c.precision == PIC_PREC_FP64 && !c.exact_current) {
+        Tiles64 &T = h->t64;
+        choose_tiles64(g, T);
+        if (!(r = dalloc(h, &T.range, 2 * (size_t)T.H * (size_t)T.ntiles)) &&
+            !(r = dalloc(h, &T.box, 8 * (size_t)T.ntiles)) && !(r = dalloc(h, &T.np, 1)))
+            h->tiled64 = true;
+    }
     if (!r && c.exact_current) {
         SegRecords &R = h->rec;
         h->exact = true;
@@ -1293,7 +1309,11 @@ int pic_move_deposit(pic_handle *h)
     } else {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_move_deposit_f64(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s, h->exact ? &h->rec : nullptr);
+        if (h->tiled64 && h->sorted)
+            launch_move_deposit_f64_tiled(h->g, h->p64[h->cur], h->cnt, h->t64, E, B, J, h->err, h->s);
+        else
+            launch_move_deposit_f64(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s,
+                                    h->exact ? &h->rec : nullptr);
     }
     return finish_phase(h);
 }
@@ -1511,9 +1531,11 @@ int pic_reorder(pic_handle *h)
 {
     if (!h) return PIC_ERR_INVALID;
     if (h->fp32) launch_reorder_f32(h->g, h->p32[h->cur], h->p32[h->cur ^ 1], h->cnt, h->capacity, h->bricks, h->err, h->s);
-    else launch_reorder_f64(h->g, h->p64[h->cur], h->p64[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+    else
+        launch_reorder_f64(h->g, h->p64[h->cur], h->p64[h->cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s,
+                           h->tiled64 ? &h->t64 : nullptr);
     h->cur ^= 1;
-    set_sorted(h, h->fp32);
+    set_sorted(h, h->fp32 || h->tiled64);
     return finish_phase(h);
 }
 

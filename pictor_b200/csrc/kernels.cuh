@@ -55,9 +55,30 @@ void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counter
 struct SegRecords;
 // rec == nullptr: the current goes to J by FP64 atomics; otherwise it is
 // summed in the reference's order (pic_config.exact_current, see mover.cu).
+// first (device, may be null): move the slots [*first, used) only.
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
                              double *const B[3], double *const J[3], int *err, cudaStream_t s,
-                             SegRecords *rec = nullptr);
+                             SegRecords *rec = nullptr, const long long *first = nullptr);
+// mover_f64_tiled.cu: the FP64 mover after a reorder, one CTA per tile of H
+// row segments of W consecutive cells (x in [1 + sx W, 1 + (sx+1) W), rows
+// j0 .. j0 + H - 1, plane k; the tiles cover the ghosted grid), whose
+// particles the cell-order reorder leaves in H slot ranges.
+constexpr int kTile64SmemBytes = 100 * 1024;   // node box + FP64 current box of one tile
+constexpr int kTile64MaxRows = 8;
+struct Tiles64 {
+    uint32_t *range;              // 2 H per tile: first and past-the-end slot of each row segment
+    int *box;                     // 8 per tile: lo[3], hi[3] of the cells its particles occupy (1-based)
+    long long *np;                // the live count at the reorder: slots past it were appended since
+    int W, H, nsx, ntiles;        // W cells per row segment, H rows per tile
+    int smem_bytes;
+};
+void choose_tiles64(const GridP &g, Tiles64 &T);
+// After a reorder: the tiles' slot ranges from the sorted keys, the boxes.
+void launch_tiles64_after_reorder(const GridP &g, const uint32_t *keys, const Counters *cnt, Tiles64 &T,
+                                  cudaStream_t s);
+void launch_move_deposit_f64_tiled(const GridP &g, const PartF64 &p, const Counters *cnt, const Tiles64 &T,
+                                   double *const E[3], double *const B[3], double *const J[3], int *err,
+                                   cudaStream_t s);
 // mover_f32.cu: per-particle FP32 mover (any particle order)
 void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
                              float *const B[3], float *const J[3], int *err, cudaStream_t s);
@@ -175,7 +196,7 @@ void launch_slab_append(const GridP &g, PartF64 &p, Counters *cnt, const double 
 // Stable cell-key reorder (ReorderPrtlArr).  The payload is gathered into
 // `out`, after which the caller swaps `p` and `out`.
 void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Counters *cnt, SortScratch &sc,
-                        long long capacity, int *err, cudaStream_t s);
+                        long long capacity, int *err, cudaStream_t s, Tiles64 *tiles = nullptr);
 // Reorder of the FP32 form (bricks.cu): live particles grouped by brick into
 // `out`, after which the caller swaps `p` and `out`.
 void launch_reorder_f32(const GridP &g, const PartF32 &p, const PartF32 &out, Counters *cnt, long long capacity,

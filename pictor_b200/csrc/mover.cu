@@ -50,11 +50,14 @@ __global__ void __launch_bounds__(kThreads) k_move_f64(GridP g, PartF64 p, const
                                                        const double *__restrict__ Ex, const double *__restrict__ Ey,
                                                        const double *__restrict__ Ez, const double *__restrict__ Bx,
                                                        const double *__restrict__ By, const double *__restrict__ Bz,
-                                                       double *Jx, double *Jy, double *Jz, int *err, RecOut ro)
+                                                       double *Jx, double *Jy, double *Jz, int *err, RecOut ro,
+                                                       const long long *__restrict__ first)
 {
     const long long used = cnt->used;
+    const long long n0 = first ? *first : 0;
     const double c = g.c, sqc = g.sqc, cinv = g.cinv, qi = g.qi;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
+    for (long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used;
+         n += (long long)gridDim.x * blockDim.x) {
         if (RECORD) {   // nothing recorded unless the particle deposits below
             ro.key[2 * n] = (uint32_t)g.ncell;
             ro.key[2 * n + 1] = (uint32_t)g.ncell;
@@ -183,17 +186,18 @@ static unsigned grid_for(long long n)
 }
 
 void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
-                             double *const B[3], double *const J[3], int *err, cudaStream_t s, SegRecords *rec)
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s, SegRecords *rec,
+                             const long long *first)
 {
     const int grid = kSMs * 16;
     if (!rec) {
         const RecOut ro = {nullptr, nullptr, 0};
         if (g.dims == 3)
             k_move_f64<3, false><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1],
-                                                          J[2], err, ro);
+                                                          J[2], err, ro, first);
         else
             k_move_f64<2, false><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1],
-                                                          J[2], err, ro);
+                                                          J[2], err, ro, first);
         count_launches(1);
         return;
     }
@@ -201,10 +205,10 @@ void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *c
     const int NE = g.dims == 3 ? 12 : 8;
     if (g.dims == 3)
         k_move_f64<3, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
-                                                     err, ro);
+                                                     err, ro, nullptr);
     else
         k_move_f64<2, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
-                                                     err, ro);
+                                                     err, ro, nullptr);
     k_record_count<<<1, 1, 0, s>>>(cnt, rec->count);
     count_launches(2);
     const int r = radix_sort_keys(rec->sc, rec->count, sort_key_bits(g.ncell), s);

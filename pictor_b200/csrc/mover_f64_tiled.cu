@@ -1,0 +1,436 @@
+// mover_f64_tiled.cu -- the FP64 mover in the reference layout, one CTA per
+// tile of cells, for the steps after a reorder.
+//
+// Reference: src/movdep/movdep.F90:62-249 (the per-particle algorithm),
+// src/movdep/movdep_routines.F90:6-223 (node-averaged fields VecE/VecB, which
+// the reference computes once per cell before the particle loop) and
+// :243-311 (the per-cell current VecJ it scatters onto the edges afterwards).
+//
+// After ReorderPrtlArr the particles are in cell order (mem_prtl.F90:166-301),
+// so the particles of W consecutive cells of one row occupy one contiguous
+// slot range.  A tile is H such row segments (x in [1 + sx W, 1 + (sx+1) W),
+// rows j0 .. j0 + H - 1 of one plane k, over the whole ghosted grid): H slot
+// ranges.  One CTA moves a
+// tile's particles:
+//   * it stages the node-averaged E and B of the box of cells its particles
+//     occupy in shared memory (FP64, the expressions and order of gather(),
+//     so the interpolated fields, and with them positions and momenta, equal
+//     the per-particle mover's and the serial CPU build's bit for bit);
+//   * it sums the tile's current in a shared FP64 box (a particle that stays
+//     in its cell adds its two zigzag segments in registers first, so most
+//     particles make 8 / 12 shared atomics instead of 16 / 24) and adds the
+//     box to J once with FP64 atomics, instead of 16 / 24 global FP64
+//     atomics per particle;
+//   * it records the cells its particles move to, which bound the box of the
+//     next step (the particles drift out of their tile between reorders).
+// The current differs from the per-particle mover's only in the order of
+// its FP64 sums.  A particle that leaves the interior is wrapped by the
+// exchange and appended after the sorted range; those are moved by the
+// per-particle kernel (k_move_f64).  A particle of a tile whose cell lies
+// outside the box, or all particles of a tile whose box does not fit in
+// shared memory, gather and deposit through global memory with the same
+// arithmetic.
+#include "common.cuh"
+#include "kernels.cuh"
+#include "particle_math.cuh"
+
+namespace pic {
+
+namespace {
+
+constexpr int kT64Threads = 256;
+
+// Tile t -> its row segments: cells x0 .. x1 - 1 (1-based) of rows j0 ..
+// j0 + nrow - 1 in plane k.  The tiles cover every cell of the ghosted
+// grid, not only the interior: the exchange sends a particle that left
+// through an edge or a corner through one face per step (the diagonal-face
+// rule of LoadPrtlOutliers), so a reorder can find it in a ghost cell, and
+// it must still belong to a tile (the range check of the move raises
+// PIC_ERR_RANGE for a cell outside the ghost frame, before any access).
+__device__ __forceinline__ void tile_cells(const GridP &g, const Tiles64 &T, int t, int &x0, int &x1, int &j0,
+                                           int &nrow, int &k)
+{
+    const int sx = t % T.nsx, r = t / T.nsx;
+    const int nry = (g.my + T.H - 1) / T.H;   // row groups per plane
+    x0 = 1 + sx * T.W;
+    x1 = min(x0 + T.W, g.mx + 1);
+    const int ry = r % nry;
+    j0 = 1 + ry * T.H;
+    nrow = min(T.H, g.my + 1 - j0);
+    k = g.dims == 3 ? 1 + r / nry : 1;
+}
+
+__device__ __forceinline__ uint32_t lower_bound_key(const uint32_t *__restrict__ keys, long long np, uint32_t c)
+{
+    long long lo = 0, hi = np;
+    while (lo < hi) {
+        const long long mid = (lo + hi) >> 1;
+        if (keys[mid] < c) lo = mid + 1;
+        else hi = mid;
+    }
+    return (uint32_t)lo;
+}
+
+// The slot range of every row segment of every tile (lower bounds of the
+// segment's first and past-the-end cells in the sorted keys) and the boxes of
+// the next move: the tile's own cells.
+__global__ void k_tile_starts(GridP g, Tiles64 T, const uint32_t *__restrict__ keys, const Counters *__restrict__ cnt)
+{
+    const long long np = cnt->np;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T.ntiles; t += gridDim.x * blockDim.x) {
+        if (t == 0) *T.np = np;
+        int x0, x1, j0, nrow, k;
+        tile_cells(g, T, t, x0, x1, j0, nrow, k);
+        uint32_t *rg = T.range + 2 * (size_t)T.H * t;
+        for (int r = 0; r < T.H; r++) {
+            uint32_t b = 0, e = 0;
+            if (r < nrow) {
+                b = lower_bound_key(keys, np, (uint32_t)cidx(g, x0, j0 + r, k));
+                e = lower_bound_key(keys, np, (uint32_t)cidx(g, x1, j0 + r, k));
+            }
+            rg[2 * r] = b;
+            rg[2 * r + 1] = e;
+        }
+        // the box of the first move: the tile's interior cells (a tile of
+        // ghost cells only gets an empty box: its rare particles take the
+        // global path)
+        int *bx = T.box + 8 * (size_t)t;
+        bx[0] = max(x0, 3); bx[1] = max(j0, 3); bx[2] = g.dims == 3 ? max(k, 3) : 1;
+        bx[3] = min(x1 - 1, g.mx - 3); bx[4] = min(j0 + nrow - 1, g.my - 3); bx[5] = g.dims == 3 ? min(k, g.mz - 3) : 1;
+    }
+}
+
+struct Box64 {
+    int lo[3], C[3];      // box cells: lo .. lo + C - 1 per axis (z: 1 cell in 2D)
+    int NX, NXY;          // node strides (C + 1 per axis)
+    int JX, JXY, nj;      // current strides (C + 3 per axis) and words per component
+};
+
+template <int DIMS>
+__device__ __forceinline__ bool in_box(const Box64 &bx, int i, int j, int k, int &nb)
+{
+    const int a = i - bx.lo[0], b = j - bx.lo[1], c = DIMS == 3 ? k - bx.lo[2] : 0;
+    nb = a + bx.NX * b + bx.NXY * c;
+    return (unsigned)a < (unsigned)bx.C[0] && (unsigned)b < (unsigned)bx.C[1] && (DIMS == 2 || (unsigned)c < (unsigned)bx.C[2]);
+}
+
+// gather() on the staged nodes: node q of the box holds the 6 node values of
+// GatherVecEfld / GatherVecBfld; the corner sums run in the same order.
+template <int DIMS>
+__device__ __forceinline__ void gather_box64(const Box64 &bx, const double *sN, int nb, const double *wt, double pE[3],
+                                             double pB[3])
+{
+    pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.0;
+#pragma unroll
+    for (int nn = 0; nn < (DIMS == 3 ? 8 : 4); nn++) {
+        const int q = nb + (nn & 1) + ((nn >> 1) & 1) * bx.NX + ((nn >> 2) & 1) * bx.NXY;
+        const double2 a = *reinterpret_cast<const double2 *>(sN + 6 * q);
+        const double2 b = *reinterpret_cast<const double2 *>(sN + 6 * q + 2);
+        const double2 c = *reinterpret_cast<const double2 *>(sN + 6 * q + 4);
+        pE[0] = pE[0] + wt[nn] * a.x;
+        pE[1] = pE[1] + wt[nn] * a.y;
+        pE[2] = pE[2] + wt[nn] * b.x;
+        pB[0] = pB[0] + wt[nn] * b.y;
+        pB[1] = pB[1] + wt[nn] * c.x;
+        pB[2] = pB[2] + wt[nn] * c.y;
+    }
+}
+
+// The VecJ entries o of a cell whose box current cell is jb, added into the
+// FP64 box (the scatter offsets of movdep_routines.F90:276-303).
+template <int DIMS>
+__device__ __forceinline__ void deposit_box64(const Box64 &bx, double *sJ, int jb, const double *o)
+{
+    double *jx = sJ + jb, *jy = sJ + bx.nj + jb, *jz = sJ + 2 * bx.nj + jb;
+    const int oy = bx.JX, oz = bx.JXY;
+    if (DIMS == 2) {
+        atomicAdd(jx, o[0]);
+        atomicAdd(jx + oy, o[1]);
+        atomicAdd(jy, o[2]);
+        atomicAdd(jy + 1, o[3]);
+        atomicAdd(jz, o[4]);
+        atomicAdd(jz + 1, o[5]);
+        atomicAdd(jz + oy, o[6]);
+        atomicAdd(jz + 1 + oy, o[7]);
+    } else {
+        atomicAdd(jx, o[0]);
+        atomicAdd(jx + oy, o[1]);
+        atomicAdd(jx + oz, o[2]);
+        atomicAdd(jx + oy + oz, o[3]);
+        atomicAdd(jy, o[4]);
+        atomicAdd(jy + 1, o[5]);
+        atomicAdd(jy + oz, o[6]);
+        atomicAdd(jy + 1 + oz, o[7]);
+        atomicAdd(jz, o[8]);
+        atomicAdd(jz + 1, o[9]);
+        atomicAdd(jz + oy, o[10]);
+        atomicAdd(jz + 1 + oy, o[11]);
+    }
+}
+
+// One particle's state in the reference layout.
+struct P64 {
+    double q, x, y, z, u, v, w;
+    int flv;
+};
+__device__ __forceinline__ P64 load_p64(const PartF64 &p, uint32_t n)
+{
+    P64 s;
+    s.flv = p.flv[n];
+    s.q = p.q[n];
+    s.x = p.x[n];
+    s.y = p.y[n];
+    s.z = p.z[n];
+    s.u = p.u[n];
+    s.v = p.v[n];
+    s.w = p.w[n];
+    return s;
+}
+
+template <int DIMS>
+__global__ void __launch_bounds__(kT64Threads, 2) k_move_f64_tiled(GridP g, PartF64 p, Tiles64 T,
+                                                                   const double *__restrict__ Ex,
+                                                                   const double *__restrict__ Ey,
+                                                                   const double *__restrict__ Ez,
+                                                                   const double *__restrict__ Bx,
+                                                                   const double *__restrict__ By,
+                                                                   const double *__restrict__ Bz, double *Jx,
+                                                                   double *Jy, double *Jz, int *err)
+{
+    extern __shared__ __align__(16) double smem64[];
+    __shared__ int s_red[kT64Threads / 32][6];
+    __shared__ uint32_t s_rg[2 * kTile64MaxRows];
+    const int t = blockIdx.x, tid = threadIdx.x;
+    if (tid < 2 * T.H) s_rg[tid] = T.range[2 * (size_t)T.H * t + tid];
+    __syncthreads();
+    // the tile's particles: item i -> slot, over the H ranges in order
+    uint32_t total = 0;
+    for (int r = 0; r < T.H; r++) total += s_rg[2 * r + 1] - s_rg[2 * r];
+    if (total == 0) return;   // uniform across the CTA
+    int *gbox = T.box + 8 * (size_t)t;
+    Box64 bx;
+    const int lo[3] = {gbox[0], gbox[1], DIMS == 3 ? gbox[2] : 1};
+    const int hi[3] = {gbox[3], gbox[4], DIMS == 3 ? gbox[5] : 1};
+    for (int d = 0; d < 3; d++) {
+        bx.lo[d] = lo[d];
+        bx.C[d] = hi[d] - lo[d] + 1;
+    }
+    bx.NX = bx.C[0] + 1;
+    bx.NXY = bx.NX * (bx.C[1] + 1);
+    const int nnode = bx.NXY * (DIMS == 3 ? bx.C[2] + 1 : 1);
+    bx.JX = bx.C[0] + 3;
+    bx.JXY = bx.JX * (bx.C[1] + 3);
+    bx.nj = bx.JXY * (DIMS == 3 ? bx.C[2] + 3 : 1);
+    // the box fits (and lies where the kernel may read and write) or the
+    // tile's particles all take the global path
+    const bool use_box = bx.C[0] >= 1 && bx.C[1] >= 1 && bx.C[2] >= 1 && lo[0] >= 2 && hi[0] <= g.mx - 2 &&
+                         lo[1] >= 2 && hi[1] <= g.my - 2 && (DIMS == 2 || (lo[2] >= 2 && hi[2] <= g.mz - 2)) &&
+                         8ll * (6ll * nnode + 3ll * bx.nj) <= (long long)T.smem_bytes;
+    double *sN = smem64;
+    double *sJ = smem64 + 6 * (use_box ? nnode : 0);
+    if (use_box) {
+        const long long sy = g.sy, sz = g.sz;
+        for (int q = tid; q < 3 * bx.nj; q += kT64Threads) sJ[q] = 0.0;
+        for (int q = tid; q < nnode; q += kT64Threads) {
+            const int a = q % bx.NX, r = q / bx.NX, b = r % (bx.C[1] + 1), c = r / (bx.C[1] + 1);
+            const long long nd = cidx(g, lo[0] + a, lo[1] + b, DIMS == 3 ? lo[2] + c : 1);
+            double *v = sN + 6 * q;
+            // the node values of gather() (GatherVecEfld / GatherVecBfld)
+            v[0] = (__ldg(Ex + nd - 1) + __ldg(Ex + nd)) * 0.5;
+            v[1] = (__ldg(Ey + nd - sy) + __ldg(Ey + nd)) * 0.5;
+            if (DIMS == 3) {
+                v[2] = (__ldg(Ez + nd - sz) + __ldg(Ez + nd)) * 0.5;
+                v[3] = (((__ldg(Bx + nd - sy - sz) + __ldg(Bx + nd - sz)) + __ldg(Bx + nd - sy)) + __ldg(Bx + nd)) * 0.25 + g.bext[0];
+                v[4] = (((__ldg(By + nd - 1 - sz) + __ldg(By + nd - 1)) + __ldg(By + nd - sz)) + __ldg(By + nd)) * 0.25 + g.bext[1];
+            } else {
+                v[2] = __ldg(Ez + nd);
+                v[3] = (__ldg(Bx + nd - sy) + __ldg(Bx + nd)) * 0.5 + g.bext[0];
+                v[4] = (__ldg(By + nd - 1) + __ldg(By + nd)) * 0.5 + g.bext[1];
+            }
+            v[5] = (((__ldg(Bz + nd - 1 - sy) + __ldg(Bz + nd - 1)) + __ldg(Bz + nd - sy)) + __ldg(Bz + nd)) * 0.25 + g.bext[2];
+        }
+    }
+    __syncthreads();
+    const double c = g.c, sqc = g.sqc, cinv = g.cinv, qi = g.qi;
+    int blo[3] = {0x3fffffff, 0x3fffffff, 0x3fffffff}, bhi[3] = {-0x3fffffff, -0x3fffffff, -0x3fffffff};
+    auto slot_of = [&](uint32_t i) {
+        for (int r = 0; r < T.H; r++) {
+            const uint32_t len = s_rg[2 * r + 1] - s_rg[2 * r];
+            if (i < len) return s_rg[2 * r] + i;
+            i -= len;
+        }
+        return 0u;   // not reached for i < total
+    };
+    P64 cur;
+    cur.flv = 0;
+    uint32_t ncur = 0;
+    if ((uint32_t)tid < total) {
+        ncur = slot_of(tid);
+        cur = load_p64(p, ncur);
+    }
+    for (uint32_t i = tid; i < total; i += kT64Threads) {
+        // the next particle loads while this one moves
+        P64 nxt;
+        nxt.flv = 0;
+        uint32_t nn = 0;
+        if (i + kT64Threads < total) {
+            nn = slot_of(i + kT64Threads);
+            nxt = load_p64(p, nn);
+        }
+        const uint32_t n = ncur;
+        const P64 s = cur;
+        cur = nxt;
+        ncur = nn;
+        const int flv = s.flv;
+        if (flv == 0) continue;
+        const double x0 = s.x, y0 = s.y, z0 = s.z;
+        if (flv < 0 || flv > PIC_MAX_FLVR || !(x0 >= 2.0 && x0 < (double)(g.mx - 1)) ||
+            !(y0 >= 2.0 && y0 < (double)(g.my - 1)) || (DIMS == 3 && !(z0 >= 2.0 && z0 < (double)(g.mz - 1)))) {
+            raise_error(err, PIC_DEVERR_RANGE);
+            continue;
+        }
+        const double qm = g.qm[flv] * 0.5;
+        const int ip0 = (int)x0, jp0 = (int)y0, kz0 = (int)z0, kp0 = DIMS == 3 ? kz0 : 1;
+        double wt[8];
+        weights<double, DIMS>(x0 - ip0, y0 - jp0, z0 - kz0, wt);
+        double pE[3], pB[3];
+        int nb = 0;
+        const bool inside = use_box && in_box<DIMS>(bx, ip0, jp0, kp0, nb);
+        if (inside) gather_box64<DIMS>(bx, sN, nb, wt, pE, pB);
+        else gather<double, DIMS>(g, Ex, Ey, Ez, Bx, By, Bz, cidx(g, ip0, jp0, kp0), wt, pE, pB);
+        for (int d = 0; d < 3; d++) {
+            pE[d] = pE[d] * qm;
+            pB[d] = pB[d] * qm;
+        }
+        double u = s.u, v = s.v, w = s.w, gg;
+        boris<double>(c, sqc, cinv, pE, pB, u, v, w, gg);
+        if (!finite3(u, v, w)) {
+            raise_error(err, PIC_DEVERR_NAN);
+            continue;
+        }
+        const double x1 = x0 + (u * gg) * 1.0, y1 = y0 + (v * gg) * 1.0, z1 = z0 + (w * gg) * 1.0;
+        const int ip = (int)x1, jp = (int)y1, kp = (int)z1;
+        const double xr = fmin((double)(min(ip0, ip) + 1), fmax((double)max(ip0, ip), 0.5 * (x0 + x1)));
+        const double yr = fmin((double)(min(jp0, jp) + 1), fmax((double)max(jp0, jp), 0.5 * (y0 + y1)));
+        const double zr = fmin((double)(min(kz0, kp) + 1), fmax((double)max(kz0, kp), 0.5 * (z0 + z1)));
+        const double qthis = s.q * qi;
+        double o[12], o2[12];
+        segment<double, DIMS>(qthis * (xr - x0), qthis * (yr - y0), qthis * (zr - z0), 0.5 * (x0 + xr) - ip0,
+                              0.5 * (y0 + yr) - jp0, DIMS == 3 ? 0.5 * (z0 + zr) - kp0 : 0.0, o);
+        segment<double, DIMS>(qthis * (x1 - xr), qthis * (y1 - yr), qthis * (z1 - zr), 0.5 * (x1 + xr) - ip,
+                              0.5 * (y1 + yr) - jp, DIMS == 3 ? 0.5 * (z1 + zr) - kp : 0.0, o2);
+        const int nk = DIMS == 3 ? kp : 1;
+        const bool same = ip == ip0 && jp == jp0 && nk == kp0;
+        if (inside) {
+            // box current cell of the start cell: (ip0 - lo + 1, ...)
+            const int jb0 = (ip0 - bx.lo[0] + 1) + bx.JX * (jp0 - bx.lo[1] + 1) +
+                            (DIMS == 3 ? bx.JXY * (kp0 - bx.lo[2] + 1) : 0);
+            if (same) {
+#pragma unroll
+                for (int e = 0; e < (DIMS == 3 ? 12 : 8); e++) o[e] = o[e] + o2[e];
+                deposit_box64<DIMS>(bx, sJ, jb0, o);
+            } else {
+                deposit_box64<DIMS>(bx, sJ, jb0, o);
+                deposit_box64<DIMS>(bx, sJ, jb0 + (ip - ip0) + bx.JX * (jp - jp0) + (DIMS == 3 ? bx.JXY * (kp - kp0) : 0),
+                                    o2);
+            }
+        } else {
+            scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip0, jp0, kp0), o);
+            scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip, jp, nk), o2);
+        }
+        p.u[n] = u;
+        p.v[n] = v;
+        p.w[n] = w;
+        p.x[n] = x1;
+        p.y[n] = y1;
+        double zn = z1;
+        if (DIMS == 2) {  // movdep.F90:241-249
+            if (zn > 2.0) zn = zn - 1.0;
+            else if (zn < 1.0) zn = 1.0 + zn;
+        }
+        p.z[n] = zn;
+        // the particles that stay in the interior bound the next box (the
+        // others are wrapped by the exchange and leave the tile's ranges)
+        if (ip >= 3 && ip <= g.mx - 3 && jp >= 3 && jp <= g.my - 3 && (DIMS == 2 || (nk >= 3 && nk <= g.mz - 3))) {
+            blo[0] = min(blo[0], ip); bhi[0] = max(bhi[0], ip);
+            blo[1] = min(blo[1], jp); bhi[1] = max(bhi[1], jp);
+            blo[2] = min(blo[2], nk); bhi[2] = max(bhi[2], nk);
+        }
+    }
+    __syncthreads();
+    if (use_box) {
+        // the box current onto J (one FP64 atomic per nonzero word)
+        const int JY = bx.C[1] + 3;
+        for (int q = tid; q < bx.nj; q += kT64Threads) {
+            const double vx = sJ[q], vy = sJ[bx.nj + q], vz = sJ[2 * bx.nj + q];
+            if (vx == 0.0 && vy == 0.0 && vz == 0.0) continue;
+            const int a = q % bx.JX, r = q / bx.JX, b = r % JY, cc = r / JY;
+            const long long off = cidx(g, bx.lo[0] - 1 + a, bx.lo[1] - 1 + b, DIMS == 3 ? bx.lo[2] - 1 + cc : 1);
+            if (vx != 0.0) atomicAdd(Jx + off, vx);
+            if (vy != 0.0) atomicAdd(Jy + off, vy);
+            if (vz != 0.0) atomicAdd(Jz + off, vz);
+        }
+    }
+    // the bounds of the next box (block reduction)
+    int vred[6] = {blo[0], blo[1], blo[2], -bhi[0], -bhi[1], -bhi[2]};
+#pragma unroll
+    for (int e = 0; e < 6; e++) vred[e] = __reduce_min_sync(0xffffffffu, vred[e]);
+    if ((tid & 31) == 0)
+        for (int e = 0; e < 6; e++) s_red[tid >> 5][e] = vred[e];
+    __syncthreads();
+    if (tid == 0) {
+        int m[6];
+        for (int e = 0; e < 6; e++) {
+            m[e] = s_red[0][e];
+            for (int w2 = 1; w2 < kT64Threads / 32; w2++) m[e] = min(m[e], s_red[w2][e]);
+        }
+        if (m[0] != 0x3fffffff) {   // else keep the box (every particle left or is a hole)
+            gbox[0] = m[0]; gbox[1] = m[1]; gbox[2] = m[2];
+            gbox[3] = -m[3]; gbox[4] = -m[4]; gbox[5] = -m[5];
+        }
+    }
+}
+
+}  // namespace
+
+void choose_tiles64(const GridP &g, Tiles64 &T)
+{
+    T.W = g.dims == 3 ? 32 : 64;
+    if (T.W > g.mx) T.W = g.mx;
+    T.H = g.dims == 3 ? 4 : 2;
+    if (T.H > g.my) T.H = g.my;
+    T.nsx = (g.mx + T.W - 1) / T.W;
+    const int nry = (g.my + T.H - 1) / T.H;
+    T.ntiles = T.nsx * nry * (g.dims == 3 ? g.mz : 1);
+    T.smem_bytes = kTile64SmemBytes;
+}
+
+void launch_tiles64_after_reorder(const GridP &g, const uint32_t *keys, const Counters *cnt, Tiles64 &T,
+                                  cudaStream_t s)
+{
+    const int b = (T.ntiles + kThreads - 1) / kThreads;
+    k_tile_starts<<<b < kSMs * 8 ? (b > 0 ? b : 1) : kSMs * 8, kThreads, 0, s>>>(g, T, keys, cnt);
+    count_launches(1);
+}
+
+void launch_move_deposit_f64_tiled(const GridP &g, const PartF64 &p, const Counters *cnt, const Tiles64 &T,
+                                   double *const E[3], double *const B[3], double *const J[3], int *err, cudaStream_t s)
+{
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_move_f64_tiled<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTile64SmemBytes);
+        cudaFuncSetAttribute(k_move_f64_tiled<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTile64SmemBytes);
+        attr_set = true;
+    }
+    if (g.dims == 3)
+        k_move_f64_tiled<3><<<T.ntiles, kT64Threads, T.smem_bytes, s>>>(g, p, T, E[0], E[1], E[2], B[0], B[1], B[2],
+                                                                       J[0], J[1], J[2], err);
+    else
+        k_move_f64_tiled<2><<<T.ntiles, kT64Threads, T.smem_bytes, s>>>(g, p, T, E[0], E[1], E[2], B[0], B[1], B[2],
+                                                                       J[0], J[1], J[2], err);
+    count_launches(1);
+    // the particles appended by the wraps since the reorder, per particle
+    launch_move_deposit_f64(g, p, cnt, E, B, J, err, s, nullptr, T.np);
+}
+
+}  // namespace pic

@@ -285,7 +285,7 @@ static unsigned stream_grid(long long capacity)
 }
 
 void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Counters *cnt, SortScratch &sc,
-                        long long capacity, int *err, cudaStream_t s)
+                        long long capacity, int *err, cudaStream_t s, Tiles64 *tiles)
 {
     cudaMemsetAsync(&cnt->np, 0, sizeof(long long), s);
     k_keys_f64<<<stream_grid(capacity), kThreads, 0, s>>>(g, p, &cnt->used, sc.key[0], &cnt->np, err);
@@ -296,6 +296,8 @@ void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Co
     count_launches(1);
     k_set_used_np<<<1, 1, 0, s>>>(cnt);
     count_launches(1);
+    // the tiles of the FP64 tiled mover: slot ranges from the sorted keys
+    if (tiles) launch_tiles64_after_reorder(g, sc.key[r], cnt, *tiles, s);
 }
 
 // ---------------------------------------------------------------------------

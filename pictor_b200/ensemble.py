@@ -205,12 +205,21 @@ def tune_classes(runs: list[RunSpec], **kw) -> dict:
     return out
 
 
+def _diag(spec, sim, sc, n) -> dict:
+    d = sim.diagnostics(sc["masse"])
+    return {"run": spec.run, "particles": n, "B2": float(d["B2"]), "E2": float(d["E2"]),
+            "kinetic": [float(x) for x in d["kinetic"]], "gauss_linf": float(d["gauss_linf"])}
+
+
 def run_batched(runs: list[RunSpec], steps: int, precision: str = "fp32", tunings: dict | None = None,
-                batched: bool = True, per_phase: bool = False) -> tuple[list[dict], dict]:
+                batched: bool = True, per_phase: bool = False, horizon: int = 0) -> tuple[list[dict], dict]:
     """Step every run of the list `steps` times on the current GPU, together
     (pic_step_many, or with per_phase pic_step_batched: one launch per phase
     for each group of runs) or one after the other; returns the per-run
-    diagnostics and the timing {seconds, particle_steps, value, launches}."""
+    diagnostics and the timing {seconds, particle_steps, value, launches}.
+    horizon > steps (together only): the runs then continue, untimed, to
+    step `horizon`, and the timing dict carries their diagnostics there
+    ("horizon")."""
     import torch
 
     from .simulation import step_many
@@ -231,16 +240,19 @@ def run_batched(runs: list[RunSpec], steps: int, precision: str = "fp32", tuning
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
         launches = sum(s.launch_count() for s, _ in sims)
-        results = []
-        for spec, (s, sc), n in zip(runs, sims, counts):
-            d = s.diagnostics(sc["masse"])
-            results.append({"run": spec.run, "particles": n, "B2": float(d["B2"]), "E2": float(d["E2"]),
-                            "kinetic": [float(x) for x in d["kinetic"]], "gauss_linf": float(d["gauss_linf"])})
+        results = [_diag(spec, s, sc, n) for spec, (s, sc), n in zip(runs, sims, counts)]
+        at_horizon = None
+        if horizon > steps:
+            step_many([s for s, _ in sims], horizon - steps, per_phase=per_phase)
+            at_horizon = [_diag(spec, s, sc, n) for spec, (s, sc), n in zip(runs, sims, counts)]
     finally:
         for s, _ in sims:
             s.close()
     ps = float(sum(counts)) * steps
-    return results, {"seconds": secs, "particle_steps": ps, "value": ps / secs, "launches": launches}
+    out = {"seconds": secs, "particle_steps": ps, "value": ps / secs, "launches": launches}
+    if at_horizon is not None:
+        out["horizon"] = at_horizon
+    return results, out
 
 
 def _run_one_by_one(runs: list[RunSpec], steps: int, precision: str, tunings: dict | None):

@@ -22,7 +22,7 @@ module pictor_b200_capi
       integer(c_int32_t) :: reorder_period, curr_filter
       integer(c_int64_t) :: capacity
       real(c_double) :: rmin
-      integer(c_int32_t) :: inc_axis, reserved(7)
+      integer(c_int32_t) :: inc_axis, brick(3), cyl_modes, slab_x, exact_current, reserved(1)
    end type pic_config
 
    interface
@@ -141,7 +141,7 @@ module pictor_b200_capi
       end function
    end interface
 
-   ! Slab form (cfg%reserved(5) = slab_x = 1): x faces exchanged by the host
+   ! Slab form (cfg%slab_x = 1): x faces exchanged by the host
    ! between ranks; buffers are device addresses (a CUDA-aware MPI_Sendrecv
    ! takes them as they are), see include/pictor_b200.h.
    interface
@@ -177,7 +177,24 @@ module pictor_b200_capi
 
    type(c_ptr), save :: pic_h = c_null_ptr
 
+   ! Choices with no counterpart in the reference's parameters.F90, read by
+   ! InitAll_gpu from the environment so that no setup file changes:
+   !   PICTOR_PRECISION=fp32   the FP32 cell-relative form (default fp64, the
+   !                           reference layout and arithmetic)
+   !   PICTOR_EXACT_CURRENT=1  FP64: the current summed in the serial CPU
+   !                           build's order (bit-exact, reproducible runs)
+   integer(c_int32_t), save :: pictor_precision = 0, pictor_exact_current = 0
+
 contains
+
+   subroutine pictor_read_env()
+      character(len=16) :: val
+      integer :: ln, st
+      call get_environment_variable("PICTOR_PRECISION", val, ln, st)
+      if (st .eq. 0 .and. (val(1:4) .eq. 'fp32' .or. val(1:4) .eq. 'FP32')) pictor_precision = 1
+      call get_environment_variable("PICTOR_EXACT_CURRENT", val, ln, st)
+      if (st .eq. 0 .and. val(1:1) .eq. '1') pictor_exact_current = 1
+   end subroutine pictor_read_env
 
    subroutine pic_check(code)
       use communication, only: Abort   ! communication.F90:96-102
@@ -214,12 +231,16 @@ contains
 #else
       cfg%geom = 0
 #endif
+      ! FDTD=Lehe in the reference Makefile only swaps sources (Makefile:70-74):
+      ! add -DLehe to the flags of this file in a Lehe build
 #ifdef Lehe
       cfg%fdtd = 1
 #else
       cfg%fdtd = 0
 #endif
-      cfg%precision = 0
+      call pictor_read_env()
+      cfg%precision = pictor_precision
+      cfg%exact_current = pictor_exact_current
       cfg%nflvr = Nflvr
       cfg%c = c; cfg%qi = qi
       cfg%bext = (/ Bx_ext0, By_ext0, Bz_ext0 /)
@@ -230,11 +251,27 @@ contains
       cfg%reorder_period = prtl_reorder_period
       cfg%curr_filter = curr_filter
       cfg%capacity = gpu_prtl_arr_size
-      cfg%rmin = 0; cfg%inc_axis = 1; cfg%reserved = 0
+#ifdef cyl
+      ! r of the first interior x cell and whether the axis is on this rank
+      ! (cyl_common.F90:19-32, cyl_em_update.F90:145)
+      cfg%rmin = xborders(procxind) + rshift
+      cfg%inc_axis = merge(1, 0, inc_axis .and. procxind .eq. 0)
+#else
+      cfg%rmin = 0; cfg%inc_axis = 1
+#endif
+      cfg%brick = 0; cfg%cyl_modes = 0; cfg%slab_x = 0; cfg%reserved = 0
       call pic_check(pic_create(cfg, pic_h))
       call pic_check(pic_load_fields(pic_h, Ex, Ey, Ez, Bx, By, Bz))
       call pic_check(pic_load_particles(pic_h, int(used_prtl_arr_size, c_int64_t), qp, xp, yp, zp, up, vp, wp, flvp))
    end subroutine InitAll_gpu
+
+   ! MAIN.F90:390 calls this after InitAll_gpu in a -Dcyl build.  The
+   ! reference's version (cyl_common.F90:35-39) allocates the device arrays
+   ! of the axis update; pic_create has allocated everything the cylindrical
+   ! step needs, so nothing is left to do.  Compile src/cyl/cyl_common.F90
+   ! without -Dgpu so that this is the only InitAll_cyl_gpu.
+   subroutine InitAll_cyl_gpu
+   end subroutine InitAll_cyl_gpu
 end module initialise_gpu
 
 module em_update_gpu

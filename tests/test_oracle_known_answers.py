@@ -292,3 +292,35 @@ def test_particle_energy_known_answer():
     e1 = (gm[0] - 1.0) * 2.0 * (2.0 * 0.01 / 1.0) * 0.45 ** 2
     e2 = (gm[1] - 1.0) * 1.5 * masse * 0.45 ** 2 + (gm[2] - 1.0) * 0.5 * masse * 0.45 ** 2
     np.testing.assert_allclose(O.Oracle(g, p).particle_energy(masse), [e1, e2], rtol=1e-14)
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_openmp_exact_order_equals_serial(dims):
+    """The OpenMP restatement with each cell's current summed in particle
+    order gives the serial build's fields and particles bit for bit (the
+    parity runs at the configurations' full sizes use it); the reference's
+    thread-slice order differs from it in the last bits only."""
+    nx, ny, nz = (48, 40, 1) if dims == 2 else (16, 12, 12)
+    qi = 0.00158203125
+    g = O.make_grid(dims, nx, ny, nz, c=0.45, qi=qi)
+    p = O.load_weibel(dims, nx, ny, nz, epc=8, drift=0.5, temp=0.005, seed=11)
+    assert p.used > 4096   # the parallel path
+    ser = O.Oracle(g, p.copy())
+    par = O.Oracle(g, p.copy(), openmp=True, exact_order=True)
+    for t in range(1, 7):
+        ser.step(t, 5)
+        par.step(t, 5)
+    assert par.p.used == ser.p.used
+    for k in ("x", "y", "z", "u", "v", "w", "q"):
+        assert np.array_equal(par.p.view()[k], ser.p.view()[k]), k
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        assert np.array_equal(getattr(par.f, n), getattr(ser.f, n)), n
+    sl = O.Oracle(g, p.copy(), openmp=True, exact_order=False)
+    for t in range(1, 3):
+        sl.step(t, 5)
+    ref = O.Oracle(g, p.copy())
+    for t in range(1, 3):
+        ref.step(t, 5)
+    for n in ("Ex", "Ey", "Ez"):
+        a, b = getattr(sl.f, n), getattr(ref.f, n)
+        np.testing.assert_allclose(a, b, rtol=0, atol=1e-12 * np.abs(b).max())
