@@ -492,6 +492,17 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
                                                         for a, b in zip(resp, res32)),
                  "form": "pic_step_batched: the runs in 4 groups, each phase of a group one launch over all "
                          "its runs, one CUDA graph per group and step"}
+    # and as one persistent launch per span between reorders (pic_step_persistent)
+    run_batched(mine, args.warmup, "fp32", tunings, persistent=True)         # warm-up
+    barrier(ws)
+    resq, tq = run_batched(mine, args.steps, "fp32", tunings, persistent=True)
+    secs_q = max_over_ranks(ws, tq["seconds"])
+    persistent = {"value": sum_over_ranks(ws, tq["particle_steps"]) / secs_q, "seconds": secs_q,
+                  "gpu_launches": tq["launches"],
+                  "max_kinetic_rel_diff_vs_streams": max(abs(sum(a["kinetic"]) - sum(b["kinetic"])) / abs(sum(b["kinetic"]))
+                                                         for a, b in zip(resq, res32)),
+                  "form": "pic_step_persistent: every phase of every run in one launch of 3 CTAs per SM per "
+                          "span of steps between reorders, work items ordered by per-run counters"}
     fp64 = None
     if not args.no_fp64:
         def errs(r32, r64):
@@ -577,6 +588,7 @@ def run_ensemble_bench(args, ws, rank, local, peak, peak_kind):
                                 "pic_step_many + pic_diagnostics"},
         }
         line["one_launch_per_phase"] = per_phase
+        line["persistent"] = persistent
         if fp64:
             line["fp64"] = fp64
         if cpu:

@@ -95,7 +95,21 @@ typedef struct {
        sort of two records per particle each step.  0 = FP64 atomics into J
        (the sums differ from the serial build's in the last bits). */
     int32_t exact_current;
-    int32_t reserved[1];
+    /* FP64 Cartesian form after a reorder: 0 = the mover by tiles of cells
+       (node and current boxes in shared memory) when the grid's current
+       arrays are larger than L2, else one thread per particle with global
+       atomics; 1 = always by tiles; -1 = never.  Positions and momenta are
+       the same either way; the current differs in the order of its sums. */
+    int32_t fp64_tiles;
+    /* FP32 Cartesian form, 3D: 1 = each zigzag segment's current is its
+       exact line integral of the bilinear weights (the cross term q dx dy dz
+       / 12 of Villasenor and Buneman), so charge is conserved exactly and the
+       Gauss residual stays at FP32 round-off; 0 = the reference's weights
+       (products of segment-midpoint weights, vars.F90:343-355), which the
+       FP64 form keeps: the FP32 form then differs from it by precision only.
+       No counterpart in the reference. */
+    int32_t exact_charge;
+    int32_t reserved[3];
 } pic_config;
 
 typedef struct pic_handle pic_handle;
@@ -218,6 +232,23 @@ int pic_set_step(pic_handle *h, int64_t t);
    stepped one after the other. */
 int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps);
 
+/* The same ensemble step as one persistent kernel per span of steps: every
+   phase of every run, for the steps up to the next reorder of any run, in a
+   single launch whose CTAs (three per SM) take the work items (the B half
+   step's blocks of 32 x 8 cells, the mover's bricks, the second B half step,
+   the E update) in order from one counter; an item first waits until its
+   run has finished the phase it depends on, so each run steps at its own
+   pace and the phases of different runs overlap.  The reorders due between
+   spans run on the device between the launches; the whole sequence of the
+   call is captured as one CUDA graph (kept for the next call with the same
+   runs, steps and reorder phases).  Requires what pic_step_batched requires.
+   Every wait gives up after spin_limit polls (0: a default of about one
+   second) and the call then returns PIC_ERR_TIMEOUT; force_timeout = 1 makes
+   the first mover item wait for a count that is never reached (a test of
+   that bound: the runs' state is then undefined, the GPU stays usable). */
+int pic_step_persistent(pic_handle *const *hs, int32_t n, int32_t nsteps, uint32_t spin_limit,
+                        int32_t force_timeout);
+
 /* The same ensemble step with one launch per phase for a group of runs:
    the runs are split into up to four groups of about equal particle count;
    each group's B half step, mover, B half step and E update are single
@@ -236,7 +267,8 @@ int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout);
 
 /* Device error word accumulated by the kernels since the last call (bit set of
    PIC_DEVERR_*); cleared by the call. */
-enum { PIC_DEVERR_RANGE = 1, PIC_DEVERR_OVERFLOW = 2, PIC_DEVERR_NAN = 4, PIC_DEVERR_SUBSTEP = 8 };
+enum { PIC_DEVERR_RANGE = 1, PIC_DEVERR_OVERFLOW = 2, PIC_DEVERR_NAN = 4, PIC_DEVERR_SUBSTEP = 8,
+       PIC_DEVERR_TIMEOUT = 16 };
 int pic_device_errors(pic_handle *h, int32_t *bits);
 
 /* Phases of pic_step, in step order. */

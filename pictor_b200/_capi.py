@@ -44,7 +44,8 @@ class Config(C.Structure):
         ("reorder_period", C.c_int32), ("curr_filter", C.c_int32),
         ("capacity", C.c_int64),
         ("rmin", C.c_double), ("inc_axis", C.c_int32), ("brick", C.c_int32 * 3), ("cyl_modes", C.c_int32),
-        ("slab_x", C.c_int32), ("exact_current", C.c_int32), ("reserved", C.c_int32 * 1),
+        ("slab_x", C.c_int32), ("exact_current", C.c_int32), ("fp64_tiles", C.c_int32),
+        ("exact_charge", C.c_int32), ("reserved", C.c_int32 * 3),
     ]
 
 
@@ -115,6 +116,7 @@ SIGNATURES = {
     "pic_step": (C.c_int, [H, C.c_int32]),
     "pic_step_many": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),
     "pic_step_batched": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32]),
+    "pic_step_persistent": (C.c_int, [C.POINTER(C.c_void_p), C.c_int32, C.c_int32, C.c_uint32, C.c_int32]),
     "pic_set_step": (C.c_int, [H, C.c_int64]),
     "pic_diagnostics": (C.c_int, [H, C.c_double, PD, C.c_int32]),
     "pic_device_errors": (C.c_int, [H, PI32]),

@@ -9,10 +9,24 @@
 #include <mutex>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "common.cuh"
 #include "kernels.cuh"
 
 using namespace pic;
+
+namespace {
+// NVTX ranges (header-only NVTX v3): one per step of pic_step and, in the
+// profiling mode, one per phase, named as the reference's timers are
+// (MAIN.F90:440-452), for nsys / ncu range filters.
+const char *const kPhaseNames[PIC_PHASE_COUNT] = {"UpdateBfieldHalf", "MoveDepositPrtl", "ExchangePrtl",
+                                                  "UpdateBfieldHalf2", "UpdateEfield+AddCurrent", "ReorderPrtl"};
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+}  // namespace
 
 struct pic_handle {
     pic_config cfg;
@@ -71,6 +85,7 @@ struct pic_handle {
 
 static thread_local long long g_launches = 0;
 static void batch_forget(pic_handle *h);
+static void persist_forget(pic_handle *h);
 
 namespace pic {
 void count_launches(int n) { g_launches += n; }
@@ -172,7 +187,7 @@ int check_device_errors(pic_handle *h)
     if (bits & PIC_DEVERR_OVERFLOW) return PIC_ERR_OVERFLOW;
     if (bits & PIC_DEVERR_RANGE) return PIC_ERR_RANGE;
     if (bits & PIC_DEVERR_NAN) return PIC_ERR_NAN;
-    if (bits & PIC_DEVERR_SUBSTEP) return PIC_ERR_TIMEOUT;
+    if (bits & (PIC_DEVERR_SUBSTEP | PIC_DEVERR_TIMEOUT)) return PIC_ERR_TIMEOUT;
     return PIC_OK;
 }
 
@@ -451,6 +466,7 @@ int step_profiled(pic_handle *h, int32_t nsteps)
         cudaEvent_t *e = &ev[(size_t)i * NE];
         cudaEventRecord(e[0], h->s);
         for (int ph = 0; ph < PIC_PHASE_COUNT; ph++) {
+            NvtxRange r(kPhaseNames[ph]);
             h->phase_launches[ph] += enqueue_phase(h, h->cur, reorder, ph);
             cudaEventRecord(e[ph + 1], h->s);
         }
@@ -489,6 +505,7 @@ void set_sorted(pic_handle *h, bool sorted)
 // One step of pic_step as a graph launch on h->s (graphs captured on first use).
 int enqueue_graph_step(pic_handle *h)
 {
+    NvtxRange range("pic_step");
     h->t += 1;
     const bool reorder = h->cfg.reorder_period > 0 && (h->t % h->cfg.reorder_period) == 0;
     cudaGraphExec_t ge = nullptr;
@@ -625,7 +642,7 @@ static bool batchable(pic_handle *const *hs, int32_t n)
     for (int32_t a = 0; a < n; a++) {
         const pic_handle *h = hs[a];
         if (!h->fp32 || !h->sorted || h->g.geom != PIC_GEOM_CARTESIAN || h->cfg.curr_filter != 0 || h->profiling ||
-            h->g.dims != hs[0]->g.dims || h->g.fdtd != hs[0]->g.fdtd)
+            h->g.dims != hs[0]->g.dims || h->g.fdtd != hs[0]->g.fdtd || h->g.exact_charge != hs[0]->g.exact_charge)
             return false;
     }
     return true;
@@ -666,6 +683,48 @@ struct BatchCache {
 static BatchCache g_batch;
 static std::mutex g_batch_mu;
 
+// The persistent form of pic_step_batched (ensemble.cu): all runs in one
+// group; the device descriptors and work lists uploaded once per set of
+// runs, the call's launch sequence captured once per (runs, steps, reorder
+// phases and buffers) and replayed.
+struct PersistCache {
+    std::vector<pic_handle *> key;
+    BatchRun *druns = nullptr;
+    int *dstart = nullptr;
+    unsigned *ctl = nullptr;
+    int nf = 0, nm = 0;
+    struct Graph {
+        std::vector<long long> key;
+        cudaGraphExec_t exec;
+        long long launches;
+    };
+    std::vector<Graph> graphs;
+    void release()
+    {
+        for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
+        graphs.clear();
+        if (druns) cudaFree(druns);
+        if (dstart) cudaFree(dstart);
+        if (ctl) cudaFree(ctl);
+        druns = nullptr;
+        dstart = nullptr;
+        ctl = nullptr;
+        key.clear();
+    }
+};
+static PersistCache g_persist;
+
+// A handle that goes away takes the cached persistent sequence with it.
+static void persist_forget(pic_handle *h)
+{
+    for (pic_handle *k : g_persist.key)
+        if (k == h) {
+            g_persist.release();
+            return;
+        }
+}
+
+
 // A handle that goes away takes the cached batch with it.
 static void batch_forget(pic_handle *h)
 {
@@ -673,8 +732,9 @@ static void batch_forget(pic_handle *h)
     for (pic_handle *k : g_batch.key)
         if (k == h) {
             g_batch.release();
-            return;
+            break;
         }
+    persist_forget(h);
 }
 
 // Runs per group: the batch is split into kBatchGroups groups of about equal
@@ -737,7 +797,7 @@ static int batch_group_prepare(BatchGroup &G, bool fresh)
     cudaGraph_t gr = nullptr;
     CK(cudaStreamBeginCapture(G.s, cudaStreamCaptureModeThreadLocal));
     launch_batch_bhalf(dims, fdtd, G.druns, G.dstart, n, G.nf, G.s);
-    launch_batch_move(dims, G.druns, G.dstart + n + 1, n, G.nm, G.s);
+    launch_batch_move(dims, h0->g.exact_charge != 0, G.druns, G.dstart + n + 1, n, G.nm, G.s);
     launch_batch_bhalf(dims, fdtd, G.druns, G.dstart, n, G.nf, G.s);
     launch_batch_efield(dims, G.druns, G.dstart, n, G.nf, G.s);
     G.step_kernels = g_launches;
@@ -874,6 +934,9 @@ int pic_create(const pic_config *cfg, pic_handle **out)
                                  c.precision != PIC_PREC_FP64 || c.capacity >= (1ll << 31)))
         return PIC_ERR_INVALID;
     if (c.fdtd != PIC_FDTD_YEE && c.fdtd != PIC_FDTD_LEHE) return PIC_ERR_INVALID;
+    if (c.fp64_tiles < -1 || c.fp64_tiles > 1) return PIC_ERR_INVALID;
+    if (c.exact_charge != 0 && (c.exact_charge != 1 || c.precision != PIC_PREC_FP32 || c.geom != PIC_GEOM_CARTESIAN))
+        return PIC_ERR_INVALID;
     if (c.precision != PIC_PREC_FP64 && c.precision != PIC_PREC_FP32) return PIC_ERR_INVALID;
     if (c.nx < 5 || c.ny < 5 || (c.dims == 3 && c.nz < 5)) return PIC_ERR_INVALID;
     if (c.nflvr < 1 || c.nflvr > PIC_MAX_FLVR) return PIC_ERR_INVALID;
@@ -918,6 +981,7 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     g.geom = c.geom;
     g.closed_x = c.geom == PIC_GEOM_CYLINDRICAL;
     g.x_external = c.slab_x;
+    g.exact_charge = c.exact_charge != 0;
     g.qm[0] = 0.0;
     for (int f = 1; f <= PIC_MAX_FLVR; f++) g.qm[f] = f <= c.nflvr ? c.qm[f] : 0.0;
     g.c_f = (float)g.c;
@@ -987,9 +1051,13 @@ int pic_create(const pic_config *cfg, pic_handle **out)
             (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
         }
     }
-    // the tiles of the FP64 Cartesian mover (the exact-order current keeps
-    // the per-particle mover, whose records it sorts anyway)
-    if (!r && c.geom == PIC_GEOM_CARTESIAN && c.precision == PIC_PREC_FP64 && !c.exact_current) {
+    // the tiles of the FP64 Cartesian mover, for grids whose current arrays
+    // are larger than L2 (there the per-particle mover's global atomics miss
+    // L2; on smaller grids they hit it and that mover is faster); the
+    // exact-order current keeps the per-particle mover, whose records it
+    // sorts anyway
+    if (!r && c.geom == PIC_GEOM_CARTESIAN && c.precision == PIC_PREC_FP64 && !c.exact_current &&
+        (c.fp64_tiles > 0 || (c.fp64_tiles == 0 && 3.0 * 8.0 * (double)g.ncell > kTile64MinCurrentBytes))) {
         Tiles64 &T = h->t64;
         choose_tiles64(g, T);
         if (!(r = dalloc(h, &T.range, 2 * (size_t)T.H * (size_t)T.ntiles)) &&
@@ -1577,6 +1645,146 @@ int pic_step_batched(pic_handle *const *hs, int32_t n, int32_t nsteps)
     if (!batchable(hs, n)) return PIC_ERR_INVALID;
     if (nsteps == 0) return PIC_OK;
     return step_many_batched(hs, n, nsteps);
+}
+
+static int step_persistent(pic_handle *const *hs, int32_t n, int32_t nsteps, unsigned spin_limit, int force_timeout)
+{
+    std::lock_guard<std::mutex> lk(g_batch_mu);
+    PersistCache &P = g_persist;
+    pic_handle *h0 = hs[0];
+    cudaStream_t s = h0->s;
+    for (int32_t a = 0; a < n; a++) CK(cudaStreamSynchronize(hs[a]->s));
+    if (!(P.key.size() == (size_t)n && std::equal(P.key.begin(), P.key.end(), hs))) {
+        P.release();
+        std::vector<int> starts(2 * ((size_t)n + 1), 0);
+        int *fstart = starts.data(), *mstart = starts.data() + n + 1;
+        for (int32_t a = 0; a < n; a++) {
+            const BatchRun R = batch_run_of(hs[a]);
+            fstart[a + 1] = fstart[a] + R.fb[0] * R.fb[1] * R.fb[2];
+            mstart[a + 1] = mstart[a] + R.bk.ntiles;
+        }
+        if (cudaMalloc(&P.druns, sizeof(BatchRun) * (size_t)n) != cudaSuccess ||
+            cudaMalloc(&P.dstart, sizeof(int) * starts.size()) != cudaSuccess ||
+            cudaMalloc(&P.ctl, sizeof(unsigned) * (3 + 4 * (size_t)n)) != cudaSuccess) {
+            P.release();
+            return PIC_ERR_OOM;
+        }
+        CK(cudaMemcpyAsync(P.dstart, starts.data(), sizeof(int) * starts.size(), cudaMemcpyHostToDevice, s));
+        P.nf = fstart[n];
+        P.nm = mstart[n];
+        P.key.assign(hs, hs + n);
+    }
+    // the descriptors as they are now (each run's current particle buffer)
+    {
+        std::vector<BatchRun> runs((size_t)n);
+        for (int32_t a = 0; a < n; a++) runs[(size_t)a] = batch_run_of(hs[a]);
+        CK(cudaMemcpyAsync(P.druns, runs.data(), sizeof(BatchRun) * (size_t)n, cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    // the graph of this call: keyed by the steps, the test switches and every
+    // run's reorder phase and current buffer
+    std::vector<long long> key = {nsteps, (long long)spin_limit, force_timeout};
+    for (int32_t a = 0; a < n; a++) {
+        const pic_handle *h = hs[a];
+        key.push_back(h->cfg.reorder_period > 0 ? h->t % h->cfg.reorder_period : 0);
+        key.push_back(h->cur);
+    }
+    cudaGraphExec_t ge = nullptr;
+    long long launches = 0;
+    for (auto &g : P.graphs)
+        if (g.key == key) {
+            ge = g.exec;
+            launches = g.launches;
+        }
+    // the host-side step counters and buffers advance as the sequence does
+    std::vector<long long> t((size_t)n);
+    std::vector<int> cur((size_t)n);
+    for (int32_t a = 0; a < n; a++) {
+        t[(size_t)a] = hs[a]->t;
+        cur[(size_t)a] = hs[a]->cur;
+    }
+    auto enqueue = [&]() {
+        long long launches = 0;
+        for (int32_t done = 0; done < nsteps;) {
+            int span = nsteps - done;
+            for (int32_t a = 0; a < n; a++) {
+                const int per = hs[a]->cfg.reorder_period;
+                if (per > 0) span = std::min(span, (int)(per - t[(size_t)a] % per));
+            }
+            for (int32_t a = 0; a < n; a++)
+                for (int k = 0; k < 3 && done == 0; k++) cudaMemsetAsync(hs[a]->J[k], 0, field_bytes(hs[a]), s);
+            g_launches = 0;
+            launch_ensemble_persistent(h0->g.dims, h0->g.fdtd, h0->g.exact_charge != 0, P.druns, P.dstart,
+                                       P.dstart + n + 1, n, span, P.ctl, spin_limit, force_timeout, s);
+            launches += g_launches;
+            for (int32_t a = 0; a < n; a++) {
+                pic_handle *h = hs[a];
+                t[(size_t)a] += span;
+                if (h->cfg.reorder_period > 0 && t[(size_t)a] % h->cfg.reorder_period == 0) {
+                    g_launches = 0;
+                    const int c = cur[(size_t)a];
+                    launch_reorder_f32(h->g, h->p32[c], h->p32[c ^ 1], h->cnt, h->capacity, h->bricks, h->err, s);
+                    launch_batch_flip(P.druns, (int)a, s);
+                    launches += g_launches;
+                    cur[(size_t)a] ^= 1;
+                }
+            }
+            done += span;
+        }
+        return launches;
+    };
+    if (!ge) {
+        cudaGraph_t gr = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        launches = enqueue();
+        const cudaError_t e = cudaStreamEndCapture(s, &gr);
+        const cudaError_t ei = e == cudaSuccess ? cudaGraphInstantiate(&ge, gr, 0) : e;
+        if (gr) cudaGraphDestroy(gr);
+        if (ei != cudaSuccess) return cuda_status(ei);
+        P.graphs.push_back({key, ge, launches});
+    } else {
+        // the host-side counters advance as the captured sequence does
+        for (int32_t done = 0; done < nsteps;) {
+            int span = nsteps - done;
+            for (int32_t a = 0; a < n; a++) {
+                const int per = hs[a]->cfg.reorder_period;
+                if (per > 0) span = std::min(span, (int)(per - t[(size_t)a] % per));
+            }
+            for (int32_t a = 0; a < n; a++) {
+                t[(size_t)a] += span;
+                const int per = hs[a]->cfg.reorder_period;
+                if (per > 0 && t[(size_t)a] % per == 0) cur[(size_t)a] ^= 1;
+            }
+            done += span;
+        }
+    }
+    CK(cudaGraphLaunch(ge, s));
+    for (int32_t a = 0; a < n; a++) {
+        hs[a]->t = t[(size_t)a];
+        hs[a]->cur = cur[(size_t)a];
+    }
+    h0->launches += launches;
+    unsigned status = 0;
+    CK(cudaMemcpyAsync(&status, P.ctl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (status & PIC_DEVERR_TIMEOUT) return PIC_ERR_TIMEOUT;
+    int first = PIC_OK;
+    for (int32_t a = 0; a < n; a++) {
+        const int q = finish(hs[a]);
+        if (q && !first) first = q;
+    }
+    return first;
+}
+
+int pic_step_persistent(pic_handle *const *hs, int32_t n, int32_t nsteps, uint32_t spin_limit, int32_t force_timeout)
+{
+    if (!hs || n < 1 || nsteps < 0) return PIC_ERR_INVALID;
+    for (int32_t a = 0; a < n; a++)
+        if (!hs[a] || hs[a]->g.x_external || hs[a]->s == nullptr) return PIC_ERR_INVALID;
+    if (!batchable(hs, n)) return PIC_ERR_INVALID;
+    if (nsteps == 0) return PIC_OK;
+    // about one second of polls (each sleeps 200 ns) unless the caller sets it
+    return step_persistent(hs, n, nsteps, spin_limit ? spin_limit : 4000000u, force_timeout != 0);
 }
 
 int pic_step_many(pic_handle *const *hs, int32_t n, int32_t nsteps)

@@ -32,6 +32,7 @@ struct GridP {
     int geom;                         // PIC_GEOM_*
     int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
     int x_external;                   // slab form: x faces exchanged with neighbouring slabs (no x images)
+    int exact_charge;                 // FP32 3D: exactly charge-conserving segment currents (pic_config)
     unsigned int mx_magic, my_magic;  // n / m = umulhi(n, magic) >> shift, exact for n < 2^28 (div_magic)
     int mx_shift, my_shift;
     // FP32 copies for the FP32 form: c, c^2, 1/c, qi, external B, q/m * 0.5
@@ -84,6 +85,25 @@ __host__ __device__ inline int wrap_index(int i, int m)
 // Kernel-launch accounting (for the launch count a benchmark reports): every
 // host launcher adds the number of kernels it enqueued.
 void count_launches(int n);
+
+// Loads of data a kernel does not write while it runs (ldro) and of data it
+// may write through other threads (ldco).  The persistent ensemble step
+// (ensemble.cu, compiled with PIC_COHERENT_LOADS) runs every phase of many
+// steps in one launch: a work item reads what earlier items wrote on other
+// SMs, ordered by the items' release / acquire counters, so there both load
+// through L2 only (ld.global.cg) and never see a stale L1 line.  Everywhere
+// else ldro takes the read-only path and ldco is a plain load.
+#ifdef PIC_COHERENT_LOADS
+template <typename T>
+__device__ __forceinline__ T ldro(const T *p) { return __ldcg(p); }
+template <typename T>
+__device__ __forceinline__ T ldco(const T *p) { return __ldcg(p); }
+#else
+template <typename T>
+__device__ __forceinline__ T ldro(const T *p) { return __ldg(p); }
+template <typename T>
+__device__ __forceinline__ T ldco(const T *p) { return *p; }
+#endif
 
 // Error bits written by kernels (never __trap): see PIC_DEVERR_*.
 __device__ inline void raise_error(int *err, int bit) { atomicOr(err, bit); }

@@ -63,8 +63,9 @@ void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *c
 // row segments of W consecutive cells (x in [1 + sx W, 1 + (sx+1) W), rows
 // j0 .. j0 + H - 1, plane k; the tiles cover the ghosted grid), whose
 // particles the cell-order reorder leaves in H slot ranges.
-constexpr int kTile64SmemBytes = 100 * 1024;   // node box + FP64 current box of one tile
+constexpr int kTile64SmemBytes = 110 * 1024;   // node box + FP64 current box of one tile (2 CTAs per SM)
 constexpr int kTile64MaxRows = 8;
+constexpr double kTile64MinCurrentBytes = 48.0 * 1024 * 1024;   // the tiles for J (3 FP64 arrays) above this
 struct Tiles64 {
     uint32_t *range;              // 2 H per tile: first and past-the-end slot of each row segment
     int *box;                     // 8 per tile: lo[3], hi[3] of the cells its particles occupy (1-based)
@@ -135,8 +136,14 @@ struct BatchRun {
 // [mstart[r], mstart[r+1]).
 void launch_batch_bhalf(int dims, int fdtd, const BatchRun *runs, const int *fstart, int n, int total, cudaStream_t s);
 void launch_batch_efield(int dims, const BatchRun *runs, const int *fstart, int n, int total, cudaStream_t s);
-void launch_batch_move(int dims, const BatchRun *runs, const int *mstart, int n, int total, cudaStream_t s);
+void launch_batch_move(int dims, bool exact_charge, const BatchRun *runs, const int *mstart, int n, int total,
+                       cudaStream_t s);
 void launch_batch_flip(BatchRun *runs, int r, cudaStream_t s);
+// ensemble.cu: the persistent ensemble step, nsteps steps of the n runs in one
+// launch; ctl holds 3 + 4 n counters (zeroed by the launcher).
+void launch_ensemble_persistent(int dims, int fdtd, bool exact_charge, const BatchRun *runs, const int *fstart,
+                                const int *mstart, int n, int nsteps, unsigned *ctl, unsigned spin_limit,
+                                int force_timeout, cudaStream_t s);
 void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
                                    float *const B[3], float *const J[3], int *err, cudaStream_t s);
 // cyl.cu: tiled FP32 cylindrical mover, one CTA per brick (+ the axis current)

@@ -209,23 +209,40 @@ __global__ void __launch_bounds__(kT64Threads, 2) k_move_f64_tiled(GridP g, Part
     if (total == 0) return;   // uniform across the CTA
     int *gbox = T.box + 8 * (size_t)t;
     Box64 bx;
-    const int lo[3] = {gbox[0], gbox[1], DIMS == 3 ? gbox[2] : 1};
-    const int hi[3] = {gbox[3], gbox[4], DIMS == 3 ? gbox[5] : 1};
-    for (int d = 0; d < 3; d++) {
-        bx.lo[d] = lo[d];
-        bx.C[d] = hi[d] - lo[d] + 1;
+    int lo[3] = {gbox[0], gbox[1], DIMS == 3 ? gbox[2] : 1};
+    int hi[3] = {gbox[3], gbox[4], DIMS == 3 ? gbox[5] : 1};
+    auto set_box = [&]() {
+        for (int d = 0; d < 3; d++) {
+            bx.lo[d] = lo[d];
+            bx.C[d] = hi[d] - lo[d] + 1;
+        }
+        bx.NX = bx.C[0] + 1;
+        bx.NXY = bx.NX * (bx.C[1] + 1);
+        bx.JX = bx.C[0] + 3;
+        bx.JXY = bx.JX * (bx.C[1] + 3);
+        bx.nj = bx.JXY * (DIMS == 3 ? bx.C[2] + 3 : 1);
+        return bx.NXY * (DIMS == 3 ? bx.C[2] + 1 : 1);
+    };
+    auto fits = [&](int nn) {
+        return bx.C[0] >= 1 && bx.C[1] >= 1 && bx.C[2] >= 1 && lo[0] >= 2 && hi[0] <= g.mx - 2 && lo[1] >= 2 &&
+               hi[1] <= g.my - 2 && (DIMS == 2 || (lo[2] >= 2 && hi[2] <= g.mz - 2)) &&
+               8ll * (6ll * nn + 3ll * bx.nj) <= (long long)T.smem_bytes;
+    };
+    int nnode = set_box();
+    if (!fits(nnode)) {
+        // the particles spread further than shared memory holds: the tile's
+        // own cells plus one on each side (clamped to the ghost frame), the
+        // particles beyond it through global memory
+        int x0, x1, j0, nrow, k;
+        tile_cells(g, T, t, x0, x1, j0, nrow, k);
+        lo[0] = max(x0 - 1, 2); hi[0] = min(x1, g.mx - 2);
+        lo[1] = max(j0 - 1, 2); hi[1] = min(j0 + nrow, g.my - 2);
+        if (DIMS == 3) { lo[2] = max(k - 1, 2); hi[2] = min(k + 1, g.mz - 2); }
+        nnode = set_box();
     }
-    bx.NX = bx.C[0] + 1;
-    bx.NXY = bx.NX * (bx.C[1] + 1);
-    const int nnode = bx.NXY * (DIMS == 3 ? bx.C[2] + 1 : 1);
-    bx.JX = bx.C[0] + 3;
-    bx.JXY = bx.JX * (bx.C[1] + 3);
-    bx.nj = bx.JXY * (DIMS == 3 ? bx.C[2] + 3 : 1);
     // the box fits (and lies where the kernel may read and write) or the
     // tile's particles all take the global path
-    const bool use_box = bx.C[0] >= 1 && bx.C[1] >= 1 && bx.C[2] >= 1 && lo[0] >= 2 && hi[0] <= g.mx - 2 &&
-                         lo[1] >= 2 && hi[1] <= g.my - 2 && (DIMS == 2 || (lo[2] >= 2 && hi[2] <= g.mz - 2)) &&
-                         8ll * (6ll * nnode + 3ll * bx.nj) <= (long long)T.smem_bytes;
+    const bool use_box = fits(nnode);
     double *sN = smem64;
     double *sJ = smem64 + 6 * (use_box ? nnode : 0);
     if (use_box) {

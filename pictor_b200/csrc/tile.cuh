@@ -27,18 +27,18 @@ __device__ __forceinline__ void node_avg(const float *__restrict__ Ex, const flo
                                          const float *__restrict__ By, const float *__restrict__ Bz, int nd, int sy,
                                          int sz, float b0, float b1, float b2, float4 &A, float2 &Bv)
 {
-    A.x = (__ldg(Ex + nd - 1) + __ldg(Ex + nd)) * 0.5f;
-    A.y = (__ldg(Ey + nd - sy) + __ldg(Ey + nd)) * 0.5f;
+    A.x = (ldro(Ex + nd - 1) + ldro(Ex + nd)) * 0.5f;
+    A.y = (ldro(Ey + nd - sy) + ldro(Ey + nd)) * 0.5f;
     if (DIMS == 3) {
-        A.z = (__ldg(Ez + nd - sz) + __ldg(Ez + nd)) * 0.5f;
-        A.w = (((__ldg(Bx + nd - sy - sz) + __ldg(Bx + nd - sz)) + __ldg(Bx + nd - sy)) + __ldg(Bx + nd)) * 0.25f + b0;
-        Bv.x = (((__ldg(By + nd - 1 - sz) + __ldg(By + nd - 1)) + __ldg(By + nd - sz)) + __ldg(By + nd)) * 0.25f + b1;
+        A.z = (ldro(Ez + nd - sz) + ldro(Ez + nd)) * 0.5f;
+        A.w = (((ldro(Bx + nd - sy - sz) + ldro(Bx + nd - sz)) + ldro(Bx + nd - sy)) + ldro(Bx + nd)) * 0.25f + b0;
+        Bv.x = (((ldro(By + nd - 1 - sz) + ldro(By + nd - 1)) + ldro(By + nd - sz)) + ldro(By + nd)) * 0.25f + b1;
     } else {
-        A.z = __ldg(Ez + nd);
-        A.w = (__ldg(Bx + nd - sy) + __ldg(Bx + nd)) * 0.5f + b0;
-        Bv.x = (__ldg(By + nd - 1) + __ldg(By + nd)) * 0.5f + b1;
+        A.z = ldro(Ez + nd);
+        A.w = (ldro(Bx + nd - sy) + ldro(Bx + nd)) * 0.5f + b0;
+        Bv.x = (ldro(By + nd - 1) + ldro(By + nd)) * 0.5f + b1;
     }
-    Bv.y = (((__ldg(Bz + nd - 1 - sy) + __ldg(Bz + nd - 1)) + __ldg(Bz + nd - sy)) + __ldg(Bz + nd)) * 0.25f + b2;
+    Bv.y = (((ldro(Bz + nd - 1 - sy) + ldro(Bz + nd - 1)) + ldro(Bz + nd - sy)) + ldro(Bz + nd)) * 0.25f + b2;
 }
 
 // Packed FP32 pair arithmetic of sm_100 (one instruction for two lanes of
@@ -220,14 +220,14 @@ template <int DIMS>
 __device__ __forceinline__ PState load_state(const PartF32 &p, uint32_t n)
 {
     PState s;
-    s.key = p.key[n];
-    s.dx = p.dx[n];
-    s.dy = p.dy[n];
-    s.dz = DIMS == 3 ? p.dz[n] : 0.f;
-    s.ux = p.ux[n];
-    s.uy = p.uy[n];
-    s.uz = p.uz[n];
-    s.w = p.w[n];
+    s.key = ldco(p.key + n);
+    s.dx = ldco(p.dx + n);
+    s.dy = ldco(p.dy + n);
+    s.dz = DIMS == 3 ? ldco(p.dz + n) : 0.f;
+    s.ux = ldco(p.ux + n);
+    s.uy = ldco(p.uy + n);
+    s.uz = ldco(p.uz + n);
+    s.w = ldco(p.w + n);
     return s;
 }
 
@@ -235,8 +235,8 @@ constexpr int kTileThreads = 256;
 constexpr int kTileWarps = kTileThreads / 32;
 
 // Second zigzag segments queued by the lanes of one warp (structure of
-// arrays: F x, y, z, W x, y, z, box address; 32 entries each).
-constexpr int kQueueRows = 7;
+// arrays: F x, y, z, W x, y, z, box address, cross term; 32 entries each).
+constexpr int kQueueRows = 8;
 
 // Interior index of the unwrapped 1-based index a (no division when a is
 // already interior or one period away).
@@ -300,8 +300,8 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     const int tid = threadIdx.x;
     const int n3[3] = {g.nx, g.ny, g.nz};
     const int *sb = bk.box + 8 * (size_t)b;
-    int lo[3] = {sb[0] - margin, sb[1] - margin, DIMS == 3 ? sb[2] - margin : 0};
-    int hi[3] = {sb[3] + margin, sb[4] + margin, DIMS == 3 ? sb[5] + margin : 0};
+    int lo[3] = {ldco(sb) - margin, ldco(sb + 1) - margin, DIMS == 3 ? ldco(sb + 2) - margin : 0};
+    int hi[3] = {ldco(sb + 3) + margin, ldco(sb + 4) + margin, DIMS == 3 ? ldco(sb + 5) + margin : 0};
     if (hi[0] < lo[0] || hi[1] < lo[1] || hi[2] < lo[2] || hi[0] - lo[0] >= kBoxAxisMax ||
         hi[1] - lo[1] >= kBoxAxisMax || hi[2] - lo[2] >= kBoxAxisMax ||
         box_floats(DIMS, hi[0] - lo[0] + 1, hi[1] - lo[1] + 1, hi[2] - lo[2] + 1, WIDE ? 2 : 1) > bk.smem_floats) {
@@ -353,7 +353,7 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
     // fixed_round).  64-bit words: S = 2^62 / (N b), each contribution an
     // FP32 value rounded to an integer of up to 2^54, the sums exact.
     {
-        const float b1 = dmax * g.qi_f * __uint_as_float(*bk.wmax_bits);
+        const float b1 = dmax * g.qi_f * __uint_as_float(ldco(bk.wmax_bits));
         const float nf = fmaxf((float)n, 256.f);
         tb.S = b1 > 0.f ? (WIDE ? 4.611686018427388e18f : 1073741824.f) / (b1 * nf) : 1.f;
     }

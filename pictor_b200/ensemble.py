@@ -212,10 +212,13 @@ def _diag(spec, sim, sc, n) -> dict:
 
 
 def run_batched(runs: list[RunSpec], steps: int, precision: str = "fp32", tunings: dict | None = None,
-                batched: bool = True, per_phase: bool = False, horizon: int = 0) -> tuple[list[dict], dict]:
+                batched: bool = True, per_phase: bool = False, horizon: int = 0,
+                persistent: bool = False) -> tuple[list[dict], dict]:
     """Step every run of the list `steps` times on the current GPU, together
-    (pic_step_many, or with per_phase pic_step_batched: one launch per phase
-    for each group of runs) or one after the other; returns the per-run
+    (pic_step_many; with per_phase pic_step_batched: one launch per phase
+    for each group of runs; with persistent pic_step_persistent: one
+    persistent launch per span between reorders) or one after the other;
+    returns the per-run
     diagnostics and the timing {seconds, particle_steps, value, launches}.
     horizon > steps (together only): the runs then continue, untimed, to
     step `horizon`, and the timing dict carries their diagnostics there
@@ -236,14 +239,14 @@ def run_batched(runs: list[RunSpec], steps: int, precision: str = "fp32", tuning
             s.launch_count()   # reset the per-handle kernel counters
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        step_many([s for s, _ in sims], steps, per_phase=per_phase)
+        step_many([s for s, _ in sims], steps, per_phase=per_phase, persistent=persistent)
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
         launches = sum(s.launch_count() for s, _ in sims)
         results = [_diag(spec, s, sc, n) for spec, (s, sc), n in zip(runs, sims, counts)]
         at_horizon = None
         if horizon > steps:
-            step_many([s for s, _ in sims], horizon - steps, per_phase=per_phase)
+            step_many([s for s, _ in sims], horizon - steps, per_phase=per_phase, persistent=persistent)
             at_horizon = [_diag(spec, s, sc, n) for spec, (s, sc), n in zip(runs, sims, counts)]
     finally:
         for s, _ in sims:

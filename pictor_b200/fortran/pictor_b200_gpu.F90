@@ -22,7 +22,8 @@ module pictor_b200_capi
       integer(c_int32_t) :: reorder_period, curr_filter
       integer(c_int64_t) :: capacity
       real(c_double) :: rmin
-      integer(c_int32_t) :: inc_axis, brick(3), cyl_modes, slab_x, exact_current, reserved(1)
+      integer(c_int32_t) :: inc_axis, brick(3), cyl_modes, slab_x, exact_current, fp64_tiles, exact_charge, &
+                            reserved(3)
    end type pic_config
 
    interface
@@ -259,7 +260,7 @@ contains
 #else
       cfg%rmin = 0; cfg%inc_axis = 1
 #endif
-      cfg%brick = 0; cfg%cyl_modes = 0; cfg%slab_x = 0; cfg%reserved = 0
+      cfg%brick = 0; cfg%cyl_modes = 0; cfg%slab_x = 0; cfg%fp64_tiles = 0; cfg%exact_charge = 0; cfg%reserved = 0
       call pic_check(pic_create(cfg, pic_h))
       call pic_check(pic_load_fields(pic_h, Ex, Ey, Ez, Bx, By, Bz))
       call pic_check(pic_load_particles(pic_h, int(used_prtl_arr_size, c_int64_t), qp, xp, yp, zp, up, vp, wp, flvp))

@@ -56,6 +56,8 @@ class PicConfig:
     cyl_modes: int = 0         # cylindrical: 0 = theta-gridded field solve, 2 = modes m = 0, 1
     slab_x: int = 0            # 1 = one slab of a domain split along x (pictor_b200.slab)
     exact_current: int = 0     # FP64: 1 = current summed in the reference's serial order (bit-exact J)
+    fp64_tiles: int = 0        # FP64 mover: 0 = tiles when J exceeds L2, 1 = always, -1 = never
+    exact_charge: int = 0      # FP32 3D: 1 = exactly charge-conserving deposit, 0 = the reference's weights
 
     def to_struct(self) -> _capi.Config:
         s = _capi.Config()
@@ -80,6 +82,8 @@ class PicConfig:
         s.cyl_modes = int(self.cyl_modes)
         s.slab_x = int(self.slab_x)
         s.exact_current = int(self.exact_current)
+        s.fp64_tiles = int(self.fp64_tiles)
+        s.exact_charge = int(self.exact_charge)
         return s
 
     @property
@@ -312,17 +316,25 @@ class Simulation:
         return self.L.pic_stream(self.h)
 
 
-def step_many(sims, nsteps: int = 1, per_phase: bool = False) -> None:
+def step_many(sims, nsteps: int = 1, per_phase: bool = False, persistent: bool = False,
+              spin_limit: int = 0, force_timeout: bool = False) -> None:
     """pic_step_many: nsteps steps of every simulation of an ensemble, their
     step graphs interleaved on their own streams so that small runs overlap
     on the GPU (all on the current device).  per_phase: pic_step_batched,
-    one launch per phase for each group of runs (FP32, all reordered)."""
+    one launch per phase for each group of runs (FP32, all reordered).
+    persistent: pic_step_persistent, one persistent launch per span of steps
+    between reorders (same requirements); spin_limit bounds every wait of
+    its work items (0: about a second) and force_timeout makes the first
+    wait run out (a test of that bound)."""
     sims = list(sims)
     if not sims:
         return
     L = sims[0].L
     arr = (C.c_void_p * len(sims))(*[s.h.value for s in sims])
-    if per_phase:
+    if persistent:
+        check(L.pic_step_persistent(arr, len(sims), int(nsteps), int(spin_limit), int(bool(force_timeout))),
+              "pic_step_persistent")
+    elif per_phase:
         check(L.pic_step_batched(arr, len(sims), int(nsteps)), "pic_step_batched")
     else:
         check(L.pic_step_many(arr, len(sims), int(nsteps)), "pic_step_many")

@@ -77,3 +77,83 @@ def test_tuner_picks_a_candidate():
     t = tune(spec, periods=(5, 10), warmup=2)
     assert t.brick in brick_candidates(spec)
     assert t.reorder_period in (5, 10)
+
+
+def test_persistent_step_matches_separate_steps():
+    """pic_step_persistent (every phase of every run in one persistent
+    launch per span, the runs' reorders in between) against the runs stepped
+    one after the other, across reorders at different periods per run: the
+    same particles per run and energies to FP32 summation-order noise."""
+    runs = _runs()
+    tunings = {(r.nx, r.ny, r.ppc): Tuning(reorder_period=p) for r, p in zip(runs, (5, 7, 20))}
+    together, t1 = run_batched(runs, 23, "fp32", tunings, batched=True, persistent=True)
+    alone, t2 = run_batched(runs, 23, "fp32", tunings, batched=False)
+    for a, b in zip(together, alone):
+        assert a["particles"] == b["particles"]
+        np.testing.assert_allclose(a["kinetic"], b["kinetic"], rtol=1e-5)
+        np.testing.assert_allclose(a["B2"] + a["E2"], b["B2"] + b["E2"], rtol=1e-3)
+        assert a["gauss_linf"] < 1e-2
+    assert t1["particle_steps"] == t2["particle_steps"]
+    # one launch per span (spans end at steps 5, 7, 10, 14, 15, 20, 21, 23)
+    # plus the reorders, against at least four per run and step one by one
+    assert t1["launches"] < t2["launches"] // 4
+
+
+def test_persistent_step_3d_matches_step():
+    """Two 3D FP32 runs (Lehe and Yee solvers are separate template cases;
+    here Yee) through the persistent kernel against pic_step of each."""
+    from pictor_b200 import PicConfig, Simulation, init_scale
+    from pictor_b200.simulation import step_many
+
+    sc = init_scale(0.45, 2.0, 4)
+    shapes = [(32, 16, 16), (24, 24, 8)]
+    res = {}
+    for mode in ("alone", "persistent"):
+        sims = []
+        for i, (nx, ny, nz) in enumerate(shapes):
+            cfg = PicConfig(nx=nx, ny=ny, nz=nz, dims=3, c=0.45, qi=sc["qi"], precision="fp32",
+                            capacity=int(2 * 4 * nx * ny * nz * 1.05) + 4096, reorder_period=10)
+            s = Simulation(cfg)
+            s.init_weibel(4, 0.5, 0.3, 0.0008, 0.0008, 2930 + i)
+            s.reorder()
+            sims.append(s)
+        try:
+            if mode == "alone":
+                for s in sims:
+                    s.step(15)
+            else:
+                step_many(sims, 15, persistent=True)
+            res[mode] = [s.diagnostics(sc["masse"]) for s in sims]
+        finally:
+            for s in sims:
+                s.close()
+    for a, b in zip(res["persistent"], res["alone"]):
+        np.testing.assert_allclose(a["kinetic"], b["kinetic"], rtol=1e-5)
+        np.testing.assert_allclose(a["B2"] + a["E2"], b["B2"] + b["E2"], rtol=1e-3)
+
+
+def test_persistent_wait_timeout_returns_error_and_gpu_stays_usable():
+    """The bound on the persistent kernel's waits: with force_timeout the
+    first mover item waits for a count nothing reaches; after spin_limit
+    polls the kernel records the timeout, every CTA stops, and the call
+    returns PIC_ERR_TIMEOUT.  The GPU then still runs a normal step."""
+    import torch
+
+    from pictor_b200 import PicError
+    from pictor_b200.simulation import step_many
+
+    runs = _runs()[:2]
+    sims = [make_run(r, "fp32") for r in runs]
+    try:
+        with pytest.raises(PicError) as e:
+            step_many([s for s, _ in sims], 3, persistent=True, spin_limit=2000, force_timeout=True)
+        assert e.value.code == -5
+        torch.cuda.synchronize()
+    finally:
+        for s, _ in sims:
+            s.close()
+    # a fresh run steps normally afterwards
+    sim, sc = make_run(runs[0], "fp32")
+    with sim:
+        sim.step(3)
+        assert np.isfinite(sim.diagnostics(sc["masse"])["kinetic"]).all()

@@ -111,6 +111,7 @@ def test_tiled_f64_mover_after_reorder(dims):
     the sorted range (moved per particle) in between."""
     g, cfg = grid_and_config(dims=dims, nx=40 if dims == 2 else 20, ny=24 if dims == 2 else 12,
                              nz=10, bext=(0.01, -0.02, 0.03))
+    cfg.fp64_tiles = 1   # tiles on this small grid too
     f = random_fields(g, seed=41)
     p = random_particles(g, n=20000 if dims == 2 else 12000, seed=42, umax=1.5)
     # particles left in ghost cells (an edge leaver that the exchange sent
@@ -135,14 +136,17 @@ def test_tiled_f64_mover_after_reorder(dims):
         assert s.device_errors() == 0
 
 
+@pytest.mark.parametrize("tiles", [-1, 1])
 @pytest.mark.parametrize("dims,fdtd", CASES)
-def test_full_steps_lockstep(dims, fdtd):
+def test_full_steps_lockstep(dims, fdtd, tiles):
     """Whole steps (one CUDA graph per step) against orc_step: identical
     particle state after the first step; thereafter the deposit's summation
-    order enters E at round-off and the comparison uses tolerances."""
+    order enters E at round-off and the comparison uses tolerances.  The FP64
+    mover per particle and by tiles (after the reorders at steps 5, 10)."""
     nx, ny, nz = (24, 20, 1) if dims == 2 else (12, 10, 8)
     g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, fdtd=fdtd, reorder_period=5,
                              qi=0.00158203125, capacity=1 << 17)
+    cfg.fp64_tiles = tiles
     p = O.load_weibel(dims, nx, ny, nz, epc=4 if dims == 3 else 8, drift=0.5, temp=0.005, seed=7)
     o = O.Oracle(g, p.copy())
     with _sim(cfg) as s:
@@ -477,7 +481,34 @@ def test_fp32_form_tracks_fp64(dims):
     assert abs(tot32 - tot64) <= 1e-5 * abs(tot64)
     fe32, fe64 = a["B2"] + a["E2"], b["B2"] + b["E2"]
     assert abs(fe32 - fe64) <= 1e-2 * fe64
+    # both forms keep the reference's weights, which conserve charge exactly
+    # in 2D and not in 3D
     assert a["gauss_linf"] <= (1e-4 if dims == 2 else 2e-2) * a["rho_max"]
+    assert b["gauss_linf"] <= (1e-12 if dims == 2 else 1e-2) * b["rho_max"]
+
+
+def test_fp32_exact_charge_conserves_charge():
+    """The FP32 3D form with pic_config.exact_charge: each zigzag segment
+    deposits its exact line integral (cross term q dx dy dz / 12), so the
+    Gauss residual stays at FP32 round-off (1e-4 of the peak charge density
+    over 60 steps, against 2e-2 with the reference's weights), by tiles and
+    per particle alike, and the energies follow the FP64 form's."""
+    nx, ny, nz = 24, 24, 24
+    res = {}
+    for tiled in (True, False):
+        g, cfg = grid_and_config(dims=3, nx=nx, ny=ny, nz=nz, precision="fp32", qi=0.00158203125,
+                                 capacity=1 << 19, reorder_period=20 if tiled else 0)
+        cfg.exact_charge = 1
+        with _sim(cfg) as s:
+            s.init_weibel(4, 0.5, 0.5, 0.005, 0.005, 2930)
+            if tiled:
+                s.reorder()
+            s.step(60)
+            res[tiled] = s.diagnostics(0.00158203125)
+    for d in res.values():
+        assert d["gauss_linf"] <= 1e-4 * d["rho_max"], d
+    a, b = res[True], res[False]
+    np.testing.assert_allclose(a["kinetic"], b["kinetic"], rtol=1e-5)
 
 
 # ---------------------------------------------------------------------------
