@@ -1660,7 +1660,7 @@ static int step_persistent(pic_handle *const *hs, int32_t n, int32_t nsteps, uns
         int *fstart = starts.data(), *mstart = starts.data() + n + 1;
         for (int32_t a = 0; a < n; a++) {
             const BatchRun R = batch_run_of(hs[a]);
-            fstart[a + 1] = fstart[a] + R.fb[0] * R.fb[1] * R.fb[2];
+            fstart[a + 1] = fstart[a] + R.fb[0] * ((R.fb[1] + kPersistFieldRows - 1) / kPersistFieldRows) * R.fb[2];
             mstart[a + 1] = mstart[a] + R.bk.ntiles;
         }
         if (cudaMalloc(&P.druns, sizeof(BatchRun) * (size_t)n) != cudaSuccess ||

@@ -90,14 +90,16 @@ void count_launches(int n);
 // may write through other threads (ldco).  The persistent ensemble step
 // (ensemble.cu, compiled with PIC_COHERENT_LOADS) runs every phase of many
 // steps in one launch: a work item reads what earlier items wrote on other
-// SMs, ordered by the items' release / acquire counters, so there both load
-// through L2 only (ld.global.cg) and never see a stale L1 line.  Everywhere
-// else ldro takes the read-only path and ldco is a plain load.
+// SMs.  The non-coherent read-only path (ld.global.nc) is only defined for
+// data that no thread writes during the kernel, so there both are weak
+// loads (ld.global.ca): the PTX memory model orders them after the writers'
+// stores through the items' release / acquire counters (one thread
+// acquires, then a CTA barrier), whatever level of cache serves them.
 #ifdef PIC_COHERENT_LOADS
 template <typename T>
-__device__ __forceinline__ T ldro(const T *p) { return __ldcg(p); }
+__device__ __forceinline__ T ldro(const T *p) { return __ldca(p); }
 template <typename T>
-__device__ __forceinline__ T ldco(const T *p) { return __ldcg(p); }
+__device__ __forceinline__ T ldco(const T *p) { return __ldca(p); }
 #else
 template <typename T>
 __device__ __forceinline__ T ldro(const T *p) { return __ldg(p); }

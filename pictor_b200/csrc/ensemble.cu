@@ -3,7 +3,7 @@
 // reference, which runs one simulation per job).
 //
 // The work of a step is a list of items in the order (phase, run, item): the
-// B half step of every run (blocks of 32 x 8 interior cells), the mover of
+// B half step of every run (blocks of 32 x 32 interior cells), the mover of
 // every run (bricks), the second B half step, the E update with the current
 // fold and AddCurrent; the span of S steps is S such lists, one after the
 // other.  A grid of resident CTAs takes the items in that order from one
@@ -13,15 +13,21 @@
 // mover <- B half step, second B half step <- mover, E update <- second B
 // half step).  So each run steps at its own pace while the others fill the
 // SMs, as the runs' step graphs on separate streams do, without a launch per
-// phase and run.  An item only ever waits on items earlier in the order, all
-// taken by running CTAs, so the waits end without any assumption on which
-// CTAs are resident.
+// phase and run.
 //
 // Ordering: a CTA finishes an item with a barrier, then one thread makes a
 // release increment of the run's counter; a waiting CTA's thread spins on an
 // acquire load of it, then a barrier.  The items read fields, currents and
 // particles that other SMs wrote in the same launch, so this file is compiled
-// with PIC_COHERENT_LOADS (all such loads through L2, no stale L1 line).
+// with PIC_COHERENT_LOADS: those reads are weak loads, which the release /
+// acquire pattern orders after the writes (never the non-coherent read-only
+// path, which is only defined for data no thread writes during the kernel).
+//
+// Progress: items are claimed in order and an item waits only on earlier
+// items.  The earliest unfinished item is either being worked on or claimed
+// by a CTA whose current item is finished (a CTA claims one item ahead), so
+// it always proceeds: the waits end without any assumption on which CTAs are
+// resident.
 //
 // Every wait is bounded: after `spin_limit` polls (with a short sleep each)
 // the CTA records PIC_DEVERR_TIMEOUT in the launch's status word, raises the
@@ -83,18 +89,31 @@ template <int DIMS, int FDTD>
 __device__ __noinline__ void persist_field_item(const BatchRun &sr, int phase, int local)
 {
     const int tid = threadIdx.x;
-    // a block of 32 x 8 interior cells (the tiling of the field kernels)
-    const int bx = local % sr.fb[0], byz = local / sr.fb[0], by = byz % sr.fb[1], bz = byz / sr.fb[1];
-    const CellIter it = interior_cell_at<DIMS>(sr.g, bx, by, bz, tid & 31, tid >> 5);
-    if (phase == 3)
-        efield_at<float, DIMS, 1>(sr.g, it, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1], sr.B[2], sr.J[0], sr.J[1],
-                                  sr.J[2]);
-    else
-        bhalf_at<float, DIMS, FDTD>(sr.g, it, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1], sr.B[2]);
+    // kPersistFieldRows blocks of 32 x 8 interior cells (the tiling of the
+    // field kernels) stacked along y
+    const int nby = (sr.fb[1] + kPersistFieldRows - 1) / kPersistFieldRows;
+    const int bx = local % sr.fb[0], byz = local / sr.fb[0], byq = byz % nby, bz = byz / nby;
+    for (int sub = 0; sub < kPersistFieldRows; sub++) {
+        const int by = byq * kPersistFieldRows + sub;
+        if (by >= sr.fb[1]) break;
+        const CellIter it = interior_cell_at<DIMS>(sr.g, bx, by, bz, tid & 31, tid >> 5);
+        if (phase == 3)
+            efield_at<float, DIMS, 1>(sr.g, it, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1], sr.B[2], sr.J[0], sr.J[1],
+                                      sr.J[2]);
+        else
+            bhalf_at<float, DIMS, FDTD>(sr.g, it, sr.E[0], sr.E[1], sr.E[2], sr.B[0], sr.B[1], sr.B[2]);
+    }
 }
 
 // ctl: [0] next item, [1] abort flag, [2] status bits, [3 + 4 r + phase]
 // finished items of run r's phase (cumulative over the span's steps).
+//
+// Thread 0 schedules: it claims the item after the current one while the
+// CTA works on the current one (the claim's latency overlaps the work),
+// waits for the current item's dependency, and publishes it in shared
+// memory; two CTA barriers per item.  A run's descriptor is copied into
+// shared memory only when the run changes (the descriptors do not change
+// during a launch).
 template <int DIMS, int FDTD, bool XC>
 __global__ void __launch_bounds__(kTileThreads, 3)
     k_ensemble_persistent(const BatchRun *__restrict__ runs, const int *__restrict__ fstart,
@@ -106,16 +125,18 @@ __global__ void __launch_bounds__(kTileThreads, 3)
     __shared__ BatchRun sr;
     __shared__ int s_go, s_run, s_phase, s_local;
     const int tid = threadIdx.x;
-    const int F = fstart[n], M = mstart[n];
-    const unsigned W = 3u * (unsigned)F + (unsigned)M;
-    const unsigned total = W * (unsigned)nsteps;
     unsigned *next = ctl, *abort_flag = ctl + 1, *status = ctl + 2, *done = ctl + 3;
+    unsigned claim = 0;
+    if (tid == 0) claim = atomicAdd(next, 1u);
+    int loaded = -1;   // the run whose descriptor sr holds
     for (;;) {
-        __syncthreads();   // the previous item is done with the shared memory
         if (tid == 0) {
-            const unsigned item = atomicAdd(next, 1u);
-            int go = item < total && ld_acquire(abort_flag) == 0;
+            const int F = fstart[n], M = mstart[n];
+            const unsigned W = 3u * (unsigned)F + (unsigned)M;
+            const unsigned item = claim;
+            int go = item < W * (unsigned)nsteps && *(volatile unsigned *)abort_flag == 0;
             if (go) {
+                claim = atomicAdd(next, 1u);   // consumed at the next item
                 const unsigned s = item / W, rem = item - s * W;
                 int phase, local;
                 if (rem < (unsigned)F) { phase = 0; local = (int)rem; }
@@ -136,7 +157,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
                     const unsigned *c = done + 4 * r + dep;
                     unsigned polls = 0;
                     while (ld_acquire(c) < need) {
-                        if (ld_acquire(abort_flag) != 0) { go = 0; break; }
+                        if (*(volatile unsigned *)abort_flag != 0) { go = 0; break; }
                         if (++polls > spin_limit) {
                             atomicOr(status, (unsigned)PIC_DEVERR_TIMEOUT);
                             atomicExch(abort_flag, 1u);
@@ -152,11 +173,14 @@ __global__ void __launch_bounds__(kTileThreads, 3)
             }
             s_go = go;
         }
-        __syncthreads();
+        __syncthreads();   // the item is published; the previous one is finished
         if (!s_go) break;
         const int r = s_run, phase = s_phase, local = s_local;
-        copy_words(&sr, &runs[r]);
-        __syncthreads();
+        if (r != loaded) {
+            copy_words(&sr, &runs[r]);
+            loaded = r;
+            __syncthreads();
+        }
         if (phase == 1) persist_move_item<DIMS, XC>(sr, local, sm, ts);
         else persist_field_item<DIMS, FDTD>(sr, phase, local);
         __syncthreads();   // every thread's writes of the item precede the release

@@ -139,6 +139,9 @@ void launch_batch_efield(int dims, const BatchRun *runs, const int *fstart, int 
 void launch_batch_move(int dims, bool exact_charge, const BatchRun *runs, const int *mstart, int n, int total,
                        cudaStream_t s);
 void launch_batch_flip(BatchRun *runs, int r, cudaStream_t s);
+// Field work items of the persistent ensemble step: 32 x (8 kPersistFieldRows)
+// interior cells (kPersistFieldRows blocks of the field kernels' tiling).
+constexpr int kPersistFieldRows = 4;
 // ensemble.cu: the persistent ensemble step, nsteps steps of the n runs in one
 // launch; ctl holds 3 + 4 n counters (zeroed by the launcher).
 void launch_ensemble_persistent(int dims, int fdtd, bool exact_charge, const BatchRun *runs, const int *fstart,

@@ -346,24 +346,80 @@ __device__ __forceinline__ int append_slot(const GridP &g, int face)
     return (face - 1) ^ 1;
 }
 
+// The exchange in two passes over the particles of blocks of kTile slots.
+// The count pass reads each particle's flavour and position once, with
+// 16-byte loads of four consecutive slots per thread, and writes the face it
+// leaves through (0: stays or a hole, 1..6: outlier_face) as one byte per
+// slot, four to a word; it counts the leavers of each append slot per block.
+// After the scan of those counts, the scatter pass reads only the face words
+// and, for the few particles that leave, their state.  The append order is
+// slot order within each face (LoadPrtlOutliers walks the array in order).
+__device__ __forceinline__ void load_quad_f64(const double *a, long long i, long long n, double v[4])
+{
+    if (i + 4 <= n) {
+        const double2 lo = *reinterpret_cast<const double2 *>(a + i);
+        const double2 hi = *reinterpret_cast<const double2 *>(a + i + 2);
+        v[0] = lo.x; v[1] = lo.y; v[2] = hi.x; v[3] = hi.y;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; k++) v[k] = i + k < n ? a[i + k] : 0.0;
+    }
+}
+
 template <int DIMS>
 __global__ void __launch_bounds__(256) k_exch_count(GridP g, PartF64 p, const long long *__restrict__ used,
-                                                    uint32_t *counts, size_t ntiles)
+                                                    uint32_t *counts, uint32_t *faces, size_t ntiles)
 {
     __shared__ uint32_t c[6];
     if (threadIdx.x < 6) c[threadIdx.x] = 0;
     __syncthreads();
     const long long n = *used;
-    const long long base = (long long)blockIdx.x * kTile;
-    for (int r = 0; r < kTile / 256; r++) {
-        const long long i = base + r * 256 + threadIdx.x;
-        if (i < n && p.flv[i] != 0) {
-            const int s = append_slot(g, outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i]));
-            if (s >= 0) atomicAdd(&c[s], 1u);
+    const long long qbase = (long long)blockIdx.x * (kTile / 4);
+    // a round's loads (flavours as one int4, each coordinate as two double2)
+    // are in flight together; unrolling the rounds makes the compiler spill
+#pragma unroll 1
+    for (int r = 0; r < kTile / 1024; r++) {
+        const long long q = qbase + r * 256 + threadIdx.x;   // four slots 4q .. 4q + 3
+        const long long i = 4 * q;
+        if (i >= n) continue;
+        int f4[4];
+        if (i + 4 <= n) {
+            const int4 fl = *reinterpret_cast<const int4 *>(p.flv + i);
+            f4[0] = fl.x; f4[1] = fl.y; f4[2] = fl.z; f4[3] = fl.w;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; k++) f4[k] = i + k < n ? p.flv[i + k] : 0;
         }
+        double x4[4], y4[4], z4[4] = {0.0, 0.0, 0.0, 0.0};
+        load_quad_f64(p.x, i, n, x4);
+        load_quad_f64(p.y, i, n, y4);
+        if (DIMS == 3) load_quad_f64(p.z, i, n, z4);
+        uint32_t word = 0;
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int face = f4[k] != 0 ? outlier_face<DIMS>(g, x4[k], y4[k], z4[k]) : 0;
+            word |= (uint32_t)face << (8 * k);
+            const int sl = append_slot(g, face);
+            if (sl >= 0) atomicAdd(&c[sl], 1u);
+        }
+        faces[q] = word;
     }
     __syncthreads();
     if (threadIdx.x < 6) counts[(size_t)threadIdx.x * ntiles + blockIdx.x] = c[threadIdx.x];
+}
+
+// RemovePrtl, loadprtlout.F90:164-181
+template <int DIMS>
+__device__ __forceinline__ void remove_prtl(const PartF64 &p, long long i)
+{
+    p.q[i] = 0.0;
+    p.flv[i] = 0;
+    p.u[i] = 0.0;
+    p.v[i] = 0.0;
+    p.w[i] = 0.0;
+    p.x[i] = 3.8;
+    p.y[i] = 3.8;
+    p.z[i] = DIMS == 3 ? 3.8 : 1.5;
 }
 
 // Slab form (g.x_external): what leaves through the x faces goes to the
@@ -374,7 +430,8 @@ __global__ void __launch_bounds__(256) k_exch_count(GridP g, PartF64 p, const lo
 // appended after the local particles from scan position offs[2 ntiles] on.
 template <int DIMS>
 __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counters *cnt, const uint32_t *__restrict__ offs,
-                                                      const uint32_t *__restrict__ total, size_t ntiles,
+                                                      const uint32_t *__restrict__ total,
+                                                      const uint32_t *__restrict__ faces, size_t ntiles,
                                                       long long capacity, int *err, double *out, long long out_cap)
 {
     __shared__ uint32_t wh[kTileWarps][6];
@@ -387,14 +444,31 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
     if (threadIdx.x < kTileWarps * 6) (&wh[0][0])[threadIdx.x] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const long long wbase = (long long)blockIdx.x * kTile + (long long)warp * kWarpItems;
-    const uint32_t lt = lanemask_lt();
-    for (int r = 0; r < kWarpItems / 32; r++) {
-        const long long i = wbase + r * 32 + lane;
-        const int s = (i < n && p.flv[i] != 0) ? append_slot(g, outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i])) : -1;
+    // warp w takes slots [w kWarpItems, (w + 1) kWarpItems) of the block, 128
+    // per round, four consecutive slots per lane
+    const long long wq = (long long)blockIdx.x * (kTile / 4) + (long long)warp * (kWarpItems / 4);
+    constexpr int kRounds = kWarpItems / 128;
+    uint32_t words[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; r++) {
+        const long long q = wq + r * 32 + lane;
+        words[r] = 4 * q < n ? faces[q] : 0u;
+    }
+    // the warp's leavers per append slot
+#pragma unroll
+    for (int r = 0; r < kRounds; r++) {
+        if (__ballot_sync(0xffffffffu, words[r] != 0u) == 0u) continue;   // uniform over the warp
+        uint32_t c6[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int sl = append_slot(g, (int)((words[r] >> (8 * k)) & 0xffu));
+#pragma unroll
+            for (int f = 0; f < 6; f++) c6[f] += sl == f;
+        }
+#pragma unroll
         for (int f = 0; f < 6; f++) {
-            const uint32_t b = __ballot_sync(0xffffffffu, s == f);
-            if (lane == 0) wh[warp][f] += __popc(b);
+            const uint32_t t = __reduce_add_sync(0xffffffffu, c6[f]);
+            if (lane == 0) wh[warp][f] += t;
         }
     }
     __syncthreads();
@@ -409,67 +483,73 @@ __global__ void __launch_bounds__(256) k_exch_scatter(GridP g, PartF64 p, Counte
     }
     __syncthreads();
     const double len[3] = {g.xlen, g.ylen, g.zlen};
-    for (int r = 0; r < kWarpItems / 32; r++) {
-        const long long i = wbase + r * 32 + lane;
-        const bool ok = i < n && p.flv[i] != 0;
-        int face = 0;
-        if (ok) face = outlier_face<DIMS>(g, p.x[i], p.y[i], p.z[i]);
-        const int s = append_slot(g, face);
-        uint32_t pos = 0;
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < kRounds; r++) {
+        const uint32_t word = words[r];
+        if (__ballot_sync(0xffffffffu, word != 0u) == 0u) continue;   // uniform over the warp
+        int sl[4];
+#pragma unroll
+        for (int k = 0; k < 4; k++) sl[k] = append_slot(g, (int)((word >> (8 * k)) & 0xffu));
+        // position of each of the lane's leavers: the warp's base for its
+        // slot, the same slot's leavers of the lower lanes, then those of the
+        // lane's lower slots
+        uint32_t pos[4] = {0, 0, 0, 0};
+#pragma unroll
         for (int f = 0; f < 6; f++) {
-            const uint32_t b = __ballot_sync(0xffffffffu, s == f);
-            if (s == f) pos = wh[warp][f] + __popc(b & lt);
+            uint32_t below = 0, all = 0;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const uint32_t m = __ballot_sync(0xffffffffu, sl[k] == f);
+                below += __popc(m & lt);
+                all += __popc(m);
+            }
+            uint32_t run = wh[warp][f] + below;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (sl[k] == f) pos[k] = run++;
             __syncwarp();
-            if (lane == 0) wh[warp][f] += __popc(b);
+            if (lane == 0) wh[warp][f] += all;
             __syncwarp();
         }
-        if (s >= 0) {
-            double pos3[3] = {p.x[i], p.y[i], p.z[i]};
-            const int axis = (face - 1) >> 1;
-            // CopyTransferPrtl subtracts the send list's shift, InsertPrtls adds
-            // the receiving list's (subdomains.F90:720-740): low faces +len, high -len.
-            if (face & 1) pos3[axis] = (pos3[axis] - 0.0) + len[axis];
-            else pos3[axis] = (pos3[axis] - len[axis]) + 0.0;
-            if (g.x_external && s <= 1) {
-                double *o = out + 8 * (size_t)pos;
-                o[0] = p.q[i];
-                o[1] = pos3[0];
-                o[2] = pos3[1];
-                o[3] = pos3[2];
-                o[4] = p.u[i];
-                o[5] = p.v[i];
-                o[6] = p.w[i];
-                o[7] = (double)p.flv[i];
-            } else {
-                const long long d = n + (pos - sent);
-                p.q[d] = p.q[i];
-                p.x[d] = pos3[0];
-                p.y[d] = pos3[1];
-                p.z[d] = pos3[2];
-                p.u[d] = p.u[i];
-                p.v[d] = p.v[i];
-                p.w[d] = p.w[i];
-                p.flv[d] = p.flv[i];
+        const long long i0 = 4 * (wq + r * 32 + lane);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int face = (int)((word >> (8 * k)) & 0xffu);
+            if (face == 0) continue;
+            const long long i = i0 + k;
+            if (sl[k] >= 0) {
+                double pos3[3] = {p.x[i], p.y[i], p.z[i]};
+                const int axis = (face - 1) >> 1;
+                // CopyTransferPrtl subtracts the send list's shift, InsertPrtls adds
+                // the receiving list's (subdomains.F90:720-740): low faces +len, high -len.
+                if (face & 1) pos3[axis] = (pos3[axis] - 0.0) + len[axis];
+                else pos3[axis] = (pos3[axis] - len[axis]) + 0.0;
+                if (g.x_external && sl[k] <= 1) {
+                    double *o = out + 8 * (size_t)pos[k];
+                    o[0] = p.q[i];
+                    o[1] = pos3[0];
+                    o[2] = pos3[1];
+                    o[3] = pos3[2];
+                    o[4] = p.u[i];
+                    o[5] = p.v[i];
+                    o[6] = p.w[i];
+                    o[7] = (double)p.flv[i];
+                } else {
+                    const long long d = n + (pos[k] - sent);
+                    p.q[d] = p.q[i];
+                    p.x[d] = pos3[0];
+                    p.y[d] = pos3[1];
+                    p.z[d] = pos3[2];
+                    p.u[d] = p.u[i];
+                    p.v[d] = p.v[i];
+                    p.w[d] = p.w[i];
+                    p.flv[d] = p.flv[i];
+                }
             }
-            // RemovePrtl, loadprtlout.F90:164-181
-            p.q[i] = 0.0;
-            p.flv[i] = 0;
-            p.u[i] = 0.0;
-            p.v[i] = 0.0;
-            p.w[i] = 0.0;
-            p.x[i] = 3.8;
-            p.y[i] = 3.8;
-            p.z[i] = DIMS == 3 ? 3.8 : 1.5;
-        } else if (face != 0) {
-            // sent to MPI_PROC_NULL: RemovePrtl without a matching append
-            p.q[i] = 0.0;
-            p.flv[i] = 0;
-            p.u[i] = 0.0;
-            p.v[i] = 0.0;
-            p.w[i] = 0.0;
-            p.x[i] = 3.8;
-            p.y[i] = 3.8;
-            p.z[i] = DIMS == 3 ? 3.8 : 1.5;
+            // a leaver, or sent to MPI_PROC_NULL: RemovePrtl (without a
+            // matching append in the second case)
+            remove_prtl<DIMS>(p, i);
         }
     }
 }
@@ -492,13 +572,19 @@ void launch_exchange_f64(const GridP &g, PartF64 &p, Counters *cnt, SortScratch 
     const size_t ntiles = sort_tiles(capacity);
     uint32_t *counts = sc.hist;  // 6 * ntiles <= 256 * ntiles
     uint32_t *total = sc.scan_tmp + sc.scan_tmp_len - 1;
-    if (g.dims == 3) k_exch_count<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, &cnt->used, counts, ntiles);
-    else k_exch_count<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, &cnt->used, counts, ntiles);
+    // the face words: one per four slots below `used` (<= capacity / 4 + 1
+    // words) in the radix-sort key buffer, which holds capacity words and is
+    // free between reorders
+    uint32_t *faces = sc.key[1];
+    if (g.dims == 3) k_exch_count<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, &cnt->used, counts, faces, ntiles);
+    else k_exch_count<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, &cnt->used, counts, faces, ntiles);
     scan_exclusive_u32(counts, counts, 6 * ntiles, sc.scan_tmp, total, s);
     if (g.dims == 3)
-        k_exch_scatter<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err, out, out_cap);
+        k_exch_scatter<3><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, faces, ntiles, capacity, err, out,
+                                                          out_cap);
     else
-        k_exch_scatter<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, ntiles, capacity, err, out, out_cap);
+        k_exch_scatter<2><<<(unsigned)ntiles, 256, 0, s>>>(g, p, cnt, counts, total, faces, ntiles, capacity, err, out,
+                                                          out_cap);
     k_exch_finish<<<1, 1, 0, s>>>(cnt, total, g.x_external ? counts + 2 * ntiles : nullptr, capacity, out_cap);
     if (g.x_external && sent_counts) {
         // right-bound (face 2, slot 0) and right + left-bound particle counts
