@@ -181,6 +181,36 @@ int pic_bc_conducting_y(pic_handle *h, int32_t side, double pos);
    (x, y, z; low, high) become holes; called where EnforceBC_PostMovDep
    calls it.  FP64 Cartesian. */
 int pic_bc_remove(pic_handle *h, int32_t face, double pos);
+/* Field faces of EnforceBC_Final (bc.F90:292-340) besides 'cond'; FP64
+   Cartesian single domain, called after pic_add_current (MAIN.F90:209).
+   pic_bc_attenuate: the faces of type 'attn' (SetBC_Fld, bc.F90:24-52) —
+   Attenuate_EM_Vacuum with AttenFactorVacuum (bc_attenuate.F90:151-290):
+   bit n-1 of `faces` marks bc_face(n) (1, 2 x; 3, 4 y; 5, 6 z, 3D only),
+   pos[n-1] its pos_fld and scale[n-1] its attn_scale (SetBC_Fld default 4);
+   every field component outside the attenuating faces is scaled by
+   1 - min(1, (d / scale)^3) at its staggered position.
+   pic_bc_attenuate_flow: face 1..4 of type 'iflw' (SetBC_InflowFld,
+   bc.F90:163-205) — Attenuate_EM_Flow (bc_attenuate.F90:16-131) for a
+   uniform flow: MagFld = bflow[3], DriftVelocity = drift[3]; the layer of
+   `thickness` (attn_thickness, default 1) beside pos relaxes E to -v x B and
+   B to bflow with the scale length `scale` (attn_scale, default 4).
+   pic_bc_open_x: an 'open' field face along x (OpenBC_Fld_Left side 0,
+   OpenBC_Fld_Right side 1, bc.F90:411-469). */
+int pic_bc_attenuate(pic_handle *h, int32_t faces, const double *pos, const double *scale);
+int pic_bc_attenuate_flow(pic_handle *h, int32_t face, double pos, double thickness, double scale,
+                          const double *bflow, const double *drift);
+int pic_bc_open_x(pic_handle *h, int32_t side, double pos);
+/* An 'open' particle face along x (OpenBC_Prtl_Left side 0, OpenBC_Prtl_Right
+   side 1, bc.F90:478-621, with dx = 1 as EnforceBC_Final calls them,
+   :333-334): the particles beyond the face at `pos` become holes; every
+   particle within one cell inside it is mirrored across the face and
+   appended in slot order (InsertNewPrtl), its u lowered by gamma v0, v0 the
+   mean x velocity of flavours 1 and 2 in its (j, k) column of that layer
+   (OpenBC_MeanPrtlSpeed), taken <= 0 on the right face and >= 0 on the left.
+   The column sums are FP64 atomics, so v0 (and the copies' u) can differ from
+   the serial sum in the last bit.  PIC_ERR_OVERFLOW (nothing appended) when
+   the copies do not fit in the capacity. */
+int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos);
 
 /* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
    with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:

@@ -100,6 +100,13 @@ def _declare(L: C.CDLL) -> None:
     for fn in ("orc_cond_fld_bottom", "orc_cond_fld_top"):
         getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
     L.orc_remove_prtl.argtypes = [P(Grid), P(_Particles), C.c_int, C.c_double]
+    L.orc_attn_vacuum.argtypes = [P(Grid), P(_Fields), C.c_int, P(C.c_double), P(C.c_double)]
+    L.orc_attn_flow.argtypes = [P(Grid), P(_Fields), C.c_int, C.c_double, C.c_double, C.c_double, P(C.c_double),
+                                P(C.c_double)]
+    for fn in ("orc_open_fld_right", "orc_open_fld_left"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
+    L.orc_open_prtl.argtypes = [P(Grid), P(_Particles), C.c_int, C.c_double, C.c_double]
+    L.orc_open_prtl.restype = C.c_int
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -301,6 +308,35 @@ class Oracle:
         fs = self.f.struct()
         fn = self.L.orc_cond_fld_bottom if side == 0 else self.L.orc_cond_fld_top
         fn(C.byref(self.g), C.byref(fs), float(pos))
+
+    def attenuate_vacuum(self, faces: dict):
+        """Attenuate_EM_Vacuum for the 'attn' faces {n: (pos, scale)}, n = 1..6."""
+        mask = 0
+        pos = (C.c_double * 6)()
+        sc = (C.c_double * 6)(*([1.0] * 6))
+        for n, (p, s) in faces.items():
+            mask |= 1 << (int(n) - 1)
+            pos[int(n) - 1] = float(p)
+            sc[int(n) - 1] = float(s)
+        fs = self.f.struct()
+        self.L.orc_attn_vacuum(C.byref(self.g), C.byref(fs), mask, pos, sc)
+
+    def attenuate_flow(self, face: int, pos: float, thickness: float, scale: float, bflow, drift):
+        """Attenuate_EM_Flow of face 1..4 with a uniform flow."""
+        fs = self.f.struct()
+        b = (C.c_double * 3)(*map(float, bflow))
+        v = (C.c_double * 3)(*map(float, drift))
+        self.L.orc_attn_flow(C.byref(self.g), C.byref(fs), int(face), float(pos), float(thickness), float(scale), b, v)
+
+    def open_fld_x(self, side: int, pos: float):
+        """OpenBC_Fld_Left (side 0) / OpenBC_Fld_Right (side 1) at pos."""
+        fs = self.f.struct()
+        fn = self.L.orc_open_fld_left if side == 0 else self.L.orc_open_fld_right
+        fn(C.byref(self.g), C.byref(fs), float(pos))
+
+    def open_prtl_x(self, side: int, pos: float, dx: float = 1.0) -> int:
+        """OpenBC_Prtl_Left (side 0) / OpenBC_Prtl_Right (side 1) at pos."""
+        return self._call_p(self.L.orc_open_prtl, int(side), float(pos), float(dx))
 
     def reorder(self) -> np.ndarray:
         perm = np.zeros(max(self.p.used, 1), dtype=np.int64)

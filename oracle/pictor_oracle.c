@@ -964,6 +964,239 @@ void orc_remove_prtl(const orc_grid *g, orc_particles *p, int face, double pos)
 }
 
 /* ------------------------------------------------------------------------- */
+/* Field faces of EnforceBC_Final (bc.F90:292-340) on one rank: x0 = y0 =    */
+/* z0 = -3 (z0 = 0 in 2D)                                                    */
+/* ------------------------------------------------------------------------- */
+static double cube(double t) { return t * t * t; }   /* t**3 */
+
+/* AttenFactorVacuum (bc_attenuate.F90:222-290). */
+static double atten_factor_vacuum(const double *p, const double *sc, int three_d, double x, double y, double z)
+{
+    double af = 0.0;
+    if (x < p[0]) {
+        if ((y <= (p[3] + p[0] - x)) && (y >= (p[2] - p[0] + x)))
+            if (z <= (p[5] + p[0] - x) && (z >= (p[4] - p[0] + x))) af = cube(fabs(x - p[0]) / sc[0]);
+    } else if (x > p[1]) {
+        if ((y <= (p[3] - p[1] + x)) && (y >= (p[2] + p[1] - x)))
+            if ((z <= (p[5] - p[1] + x)) && (z >= (p[4] + p[1] - x))) af = cube(fabs(x - p[1]) / sc[1]);
+    }
+    if (y < p[2]) {
+        if ((y < (p[2] - p[0] + x)) && (y < (p[2] + p[1] - x)))
+            if ((z >= (p[4] - p[2] + y)) && (z <= (p[5] + p[2] - y))) af = cube(fabs(y - p[2]) / sc[2]);
+    } else if (y > p[3]) {
+        if ((y > (p[3] + p[0] - x)) && (y > (p[3] - p[1] + x)))
+            if ((z >= (p[4] + p[3] - y)) && (z <= (p[5] - p[3] + y))) af = cube(fabs(y - p[3]) / sc[3]);
+    }
+    if (three_d) {
+        if (z < p[4]) {
+            if ((z < (p[4] - p[0] + x)) && (z < (p[4] + p[1] - x)))
+                if ((z < (p[4] - p[2] + y)) && (z < (p[4] + p[3] - y))) af = cube(fabs(z - p[4]) / sc[4]);
+        } else if (z > p[5]) {
+            if (z > (p[5] + p[0] - x) && (z > (p[5] - p[1] + x)))
+                if ((z > (p[5] + p[2] - y)) && (z > (p[5] - p[3] + y))) af = cube(fabs(z - p[5]) / sc[5]);
+        }
+    }
+    af = af < 1.0 ? af : 1.0;   /* min(1.0, af) */
+    af = af > 0.0 ? af : 0.0;   /* max(0.0, af) */
+    return 1.0 - af;
+}
+
+/* Attenuate_EM_Vacuum (bc_attenuate.F90:151-220): bit n-1 of `faces` marks
+   bc_face(n) as 'attn' at pos[n-1] with attn_scale scale[n-1]; the other
+   faces keep attn_vac_pos = -+huge(1) and attn_vac_pos_ind = -+huge(1). */
+void orc_attn_vacuum(const orc_grid *g, orc_fields *f, int faces, const double *pos, const double *scale)
+{
+    double p[6], sc[6];
+    long long ind[6];
+    for (int n = 0; n < 6; n++) {
+        const int on = (faces >> n) & 1, upper = (n & 1) != 0;
+        p[n] = on ? pos[n] : (upper ? 2147483647.0 : -2147483647.0);
+        sc[n] = on ? scale[n] : 1.0;
+        ind[n] = on ? (upper ? (long long)ceil(p[n]) + 1 : (long long)floor(p[n]) - 1) : (upper ? 2147483647 : -2147483647);
+    }
+    const int three_d = g->dims == 3;
+    int inside = 1 - 3 > ind[0] && g->mx - 3 < ind[1] && 1 - 3 > ind[2] && g->my - 3 < ind[3] &&
+                 (!three_d || (1 - 3 > ind[4] && g->mz - 3 < ind[5]));
+    if (inside) return;
+    const double x0 = -3, y0 = -3, z0 = three_d ? -3 : 0;
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= g->my; j++)
+            for (int i = 1; i <= g->mx; i++) {
+                inside = i - 3 > ind[0] && i - 3 < ind[1] && j - 3 > ind[2] && j - 3 < ind[3] &&
+                         (!three_d || (k - 3 > ind[4] && k - 3 < ind[5]));
+                if (inside) continue;
+                const int64_t c = ID(g, i, j, k);
+                f->Ex[c] = f->Ex[c] * atten_factor_vacuum(p, sc, three_d, i + 0.5 + x0, j + y0, k + z0);
+                f->Ey[c] = f->Ey[c] * atten_factor_vacuum(p, sc, three_d, i + x0, j + 0.5 + y0, k + z0);
+                f->Ez[c] = f->Ez[c] * atten_factor_vacuum(p, sc, three_d, i + x0, j + y0, k + 0.5 + z0);
+                f->Bx[c] = f->Bx[c] * atten_factor_vacuum(p, sc, three_d, i + x0, j + 0.5 + y0, k + 0.5 + z0);
+                f->By[c] = f->By[c] * atten_factor_vacuum(p, sc, three_d, i + 0.5 + x0, j + y0, k + 0.5 + z0);
+                f->Bz[c] = f->Bz[c] * atten_factor_vacuum(p, sc, three_d, i + 0.5 + x0, j + 0.5 + y0, k + z0);
+            }
+}
+
+/* atnn_domain (bc_attenuate.F90:117-131) and AttenFactor (:102-115). */
+static int atnn_domain(double xg, double yg, double pos, int side, double dl)
+{
+    switch (side) {
+        case 1: return xg >= pos && xg <= pos + dl;
+        case 2: return xg <= pos && xg >= pos - dl;
+        case 3: return yg >= pos && yg <= pos + dl;
+        case 4: return yg <= pos && yg >= pos - dl;
+    }
+    return 0;
+}
+static double atten_factor(double x, double y, double pos, int side, double dl)
+{
+    double af = 0.0;
+    if (side == 1 || side == 2) af = cube(fabs(x - pos) / dl);
+    else af = cube(fabs(y - pos) / dl);
+    af = af < 1.0 ? af : 1.0;
+    af = af > 0.0 ? af : 0.0;
+    return 1.0 - af;
+}
+
+/* Attenuate_EM_Flow (bc_attenuate.F90:16-98) on face `side` 1..4 for a flow
+   with the uniform MagFld b[3] and Drift v[3]. */
+void orc_attn_flow(const orc_grid *g, orc_fields *f, int side, double pos, double dl, double scale, const double *b,
+                   const double *v)
+{
+    const double x0 = -3, y0 = -3;
+    if (dl == 0) return;
+    if ((side == 1 || side == 3) && (side == 1 ? (pos + dl) - x0 < 1 : (pos + dl) - y0 < 1)) return;
+    if ((side == 2 || side == 4) && (side == 2 ? (pos - dl) - x0 > g->mx : (pos - dl) - y0 > g->my)) return;
+    for (int k = 1; k <= g->mz; k++)
+        for (int j = 1; j <= g->my; j++)
+            for (int i = 1; i <= g->mx; i++) {
+                const int64_t c = ID(g, i, j, k);
+                double xg, yg, f0;
+                xg = i + 0.5 + x0; yg = j + y0;
+                if (atnn_domain(xg, yg, pos, side, dl)) {
+                    f0 = v[2] * b[1] - v[1] * b[2];
+                    f->Ex[c] = (f->Ex[c] - f0) * atten_factor(xg, yg, pos, side, scale) + f0;
+                }
+                xg = i + x0; yg = j + 0.5 + y0;
+                if (atnn_domain(xg, yg, pos, side, dl)) {
+                    f0 = v[0] * b[2] - v[2] * b[0];
+                    f->Ey[c] = (f->Ey[c] - f0) * atten_factor(xg, yg, pos, side, scale) + f0;
+                }
+                xg = i + x0; yg = j + y0;
+                if (atnn_domain(xg, yg, pos, side, dl)) {
+                    f0 = v[1] * b[0] - v[0] * b[1];
+                    f->Ez[c] = (f->Ez[c] - f0) * atten_factor(xg, yg, pos, side, scale) + f0;
+                }
+                xg = i + x0; yg = j + 0.5 + y0;
+                if (atnn_domain(xg, yg, pos, side, dl))
+                    f->Bx[c] = (f->Bx[c] - b[0]) * atten_factor(xg, yg, pos, side, scale) + b[0];
+                xg = i + 0.5 + x0; yg = j + y0;
+                if (atnn_domain(xg, yg, pos, side, dl))
+                    f->By[c] = (f->By[c] - b[1]) * atten_factor(xg, yg, pos, side, scale) + b[1];
+                xg = i + 0.5 + x0; yg = j + 0.5 + y0;
+                if (atnn_domain(xg, yg, pos, side, dl))
+                    f->Bz[c] = (f->Bz[c] - b[2]) * atten_factor(xg, yg, pos, side, scale) + b[2];
+            }
+}
+
+/* OpenBC_Fld_Right (bc.F90:411-440). */
+void orc_open_fld_right(const orc_grid *g, orc_fields *f, double pos)
+{
+    const int xl = (int)ceil(pos - 0.0 + 3);
+    if (!(xl >= 1 && xl <= g->mx - 1)) return;
+    for (int i = xl + 1; i <= g->mx; i++)
+        for (int k = 1; k <= g->mz; k++)
+            for (int j = 1; j <= g->my; j++) {
+                f->Ey[ID(g, i, j, k)] = 0.5 * f->Ey[ID(g, i, j, k)];
+                f->Ez[ID(g, i, j, k)] = 0.5 * f->Ez[ID(g, i, j, k)];
+                f->Bx[ID(g, i, j, k)] = f->Bx[ID(g, xl, j, k)];
+            }
+    for (int i = xl; i <= g->mx; i++)
+        for (int k = 1; k <= g->mz; k++)
+            for (int j = 1; j <= g->my; j++) {
+                f->Ex[ID(g, i, j, k)] = 0.5 * f->Ex[ID(g, i, j, k)];
+                f->By[ID(g, i, j, k)] = 0.5 * f->By[ID(g, i, j, k)];
+                f->Bz[ID(g, i, j, k)] = 0.5 * f->Bz[ID(g, i, j, k)];
+            }
+}
+
+/* OpenBC_Fld_Left (bc.F90:442-469). */
+void orc_open_fld_left(const orc_grid *g, orc_fields *f, double pos)
+{
+    const int xl = (int)ceil(pos - 0.0 + 3);
+    if (!(xl >= 2 && xl <= g->mx)) return;
+    for (int i = 1; i <= xl - 1; i++)
+        for (int k = 1; k <= g->mz; k++)
+            for (int j = 1; j <= g->my; j++) {
+                f->Ey[ID(g, i, j, k)] = 0.5 * f->Ey[ID(g, i, j, k)];
+                f->Ez[ID(g, i, j, k)] = 0.5 * f->Ez[ID(g, i, j, k)];
+                f->Bx[ID(g, i, j, k)] = f->Bx[ID(g, xl, j, k)];
+                f->Ex[ID(g, i, j, k)] = 0.5 * f->Ex[ID(g, i, j, k)];
+                f->By[ID(g, i, j, k)] = 0.5 * f->By[ID(g, i, j, k)];
+                f->Bz[ID(g, i, j, k)] = 0.5 * f->Bz[ID(g, i, j, k)];
+            }
+}
+
+/* OpenBC_Prtl_Right (bc.F90:478-538) / OpenBC_Prtl_Left (:540-600) with the
+   column means of OpenBC_MeanPrtlSpeed (:603-621), DeletePrtl
+   (mem_prtl.F90:7-22) and InsertNewPrtl (:120-133); side 1 right, 0 left.
+   Returns -1 (nothing appended past the capacity) when the copies do not
+   fit. */
+int orc_open_prtl(const orc_grid *g, orc_particles *p, int side, double pos, double dx)
+{
+    const double wall = pos - 0.0 + 3;
+    if (side == 1 ? !(wall < g->mx - 1) : !(wall > 1)) return 0;
+    for (int64_t n = 0; n < p->used; n++)
+        if (p->q[n] != 0 && (side == 1 ? p->x[n] > wall : p->x[n] < wall)) {
+            p->q[n] = 0.0;
+            p->x[n] = 3.8;
+            p->y[n] = 3.8;
+            p->z[n] = g->dims == 3 ? 3.8 : 1.5;
+            p->u[n] = 0.0;
+            p->v[n] = 0.0;
+            p->w[n] = 0.0;
+            p->flv[n] = 0;
+        }
+    const int ncol = g->my * g->mz;
+    double *den = malloc(sizeof(double) * (size_t)ncol), *vel = malloc(sizeof(double) * (size_t)ncol);
+    for (int c = 0; c < ncol; c++) { den[c] = 1.0; vel[c] = 0.0; }
+#define IN_LAYER(n) (p->q[n] != 0 && (side == 1 ? (p->x[n] > wall - dx && p->x[n] < wall) \
+                                              : (p->x[n] < wall + dx && p->x[n] > wall)))
+    for (int64_t n = 0; n < p->used; n++)
+        if (IN_LAYER(n) && p->flv[n] <= 2) {
+            const int j = (int)p->y[n], k = g->dims == 3 ? (int)p->z[n] : 1;
+            const double invg = 1.0 / sqrt(1.0 + p->u[n] * p->u[n] + p->v[n] * p->v[n] + p->w[n] * p->w[n]);
+            const double vx = p->u[n] * invg;
+            den[(j - 1) + g->my * (k - 1)] = den[(j - 1) + g->my * (k - 1)] + 1.0;
+            vel[(j - 1) + g->my * (k - 1)] = vel[(j - 1) + g->my * (k - 1)] + vx;
+        }
+    for (int c = 0; c < ncol; c++) vel[c] = vel[c] / den[c];
+    const int64_t used0 = p->used;
+    int64_t m = 0;
+    for (int64_t n = 0; n < used0; n++) if (IN_LAYER(n)) m++;
+    if (used0 + m > p->capacity) { free(den); free(vel); return -1; }
+    for (int64_t n = 0; n < used0; n++)
+        if (IN_LAYER(n)) {
+            const int j = (int)p->y[n], k = g->dims == 3 ? (int)p->z[n] : 1;
+            double v0 = vel[(j - 1) + g->my * (k - 1)];
+            if (side == 1 ? v0 > 0 : v0 < 0) v0 = 0.0;
+            const double gamma = sqrt(1.0 + p->u[n] * p->u[n] + p->v[n] * p->v[n] + p->w[n] * p->w[n]);
+            const int64_t d = p->used;
+            p->x[d] = 2 * wall - p->x[n];
+            p->y[d] = p->y[n];
+            p->z[d] = p->z[n];
+            p->u[d] = p->u[n] - gamma * v0;
+            p->v[d] = p->v[n];
+            p->w[d] = p->w[n];
+            p->q[d] = p->q[n];
+            p->flv[d] = p->flv[n];
+            p->used = d + 1;
+        }
+#undef IN_LAYER
+    free(den);
+    free(vel);
+    return 0;
+}
+
+/* ------------------------------------------------------------------------- */
 /* One time step, src/MAIN.F90:42-284                                        */
 /* ------------------------------------------------------------------------- */
 int orc_step_filtered(const orc_grid *g, orc_particles *p, orc_fields *f, int t, int reorder_period, int curr_filter)

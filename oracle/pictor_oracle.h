@@ -102,6 +102,16 @@ void orc_cond_fld_top(const orc_grid *g, orc_fields *f, double pos);
    z; low, high): the particles beyond bc_pos_local(face, pos) = pos + 3
    (bc.F90:350-363) become holes. */
 void orc_remove_prtl(const orc_grid *g, orc_particles *p, int face, double pos);
+/* Field faces of EnforceBC_Final (bc.F90:292-340): Attenuate_EM_Vacuum
+   (bc_attenuate.F90:151-290), Attenuate_EM_Flow with a uniform flow
+   (:16-131), OpenBC_Fld_Left/Right (bc.F90:411-469). */
+void orc_attn_vacuum(const orc_grid *g, orc_fields *f, int faces, const double *pos, const double *scale);
+void orc_attn_flow(const orc_grid *g, orc_fields *f, int side, double pos, double dl, double scale, const double *b,
+                   const double *v);
+void orc_open_fld_right(const orc_grid *g, orc_fields *f, double pos);
+void orc_open_fld_left(const orc_grid *g, orc_fields *f, double pos);
+/* OpenBC_Prtl_Left (side 0) / Right (side 1), bc.F90:478-621, layer width dx. */
+int orc_open_prtl(const orc_grid *g, orc_particles *p, int side, double pos, double dx);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

@@ -102,6 +102,308 @@ __global__ void k_remove_prtl(PartF64 p, const Counters *__restrict__ cnt, int a
     }
 }
 
+// ---------------------------------------------------------------------------
+// Field faces of EnforceBC_Final (bc.F90:292-340) other than 'cond'.
+// Global positions on one rank: x0 = xborders(procxind) - 3 = -3 (likewise
+// y0, z0; z0 = 0 in 2D); the staggered positions of the six components are
+// those of bc_attenuate.F90:36-81 and :184-206.
+// ---------------------------------------------------------------------------
+
+// The cube of t as gfortran evaluates t**3 (t * t * t).
+__device__ __forceinline__ double cube(double t) { return t * t * t; }
+
+// AttenFactorVacuum (bc_attenuate.F90:222-290): the faces' attn_vac_pos p
+// (+-huge for faces that are not 'attn') and attn_scale sc; the z faces only
+// in 3D.  Later faces override earlier ones, as in the reference.
+struct AttnVac {
+    double p[6], sc[6];
+    int ind[6];   // attn_vac_pos_ind
+};
+__device__ double atten_factor_vacuum(const AttnVac &a, bool three_d, double x, double y, double z)
+{
+    const double *p = a.p;
+    double af = 0.0;
+    if (x < p[0]) {
+        if ((y <= (p[3] + p[0] - x)) && (y >= (p[2] - p[0] + x)))
+            if (z <= (p[5] + p[0] - x) && (z >= (p[4] - p[0] + x))) af = cube(fabs(x - p[0]) / a.sc[0]);
+    } else if (x > p[1]) {
+        if ((y <= (p[3] - p[1] + x)) && (y >= (p[2] + p[1] - x)))
+            if ((z <= (p[5] - p[1] + x)) && (z >= (p[4] + p[1] - x))) af = cube(fabs(x - p[1]) / a.sc[1]);
+    }
+    if (y < p[2]) {
+        if ((y < (p[2] - p[0] + x)) && (y < (p[2] + p[1] - x)))
+            if ((z >= (p[4] - p[2] + y)) && (z <= (p[5] + p[2] - y))) af = cube(fabs(y - p[2]) / a.sc[2]);
+    } else if (y > p[3]) {
+        if ((y > (p[3] + p[0] - x)) && (y > (p[3] - p[1] + x)))
+            if ((z >= (p[4] + p[3] - y)) && (z <= (p[5] - p[3] + y))) af = cube(fabs(y - p[3]) / a.sc[3]);
+    }
+    if (three_d) {
+        if (z < p[4]) {
+            if ((z < (p[4] - p[0] + x)) && (z < (p[4] + p[1] - x)))
+                if ((z < (p[4] - p[2] + y)) && (z < (p[4] + p[3] - y))) af = cube(fabs(z - p[4]) / a.sc[4]);
+        } else if (z > p[5]) {
+            if (z > (p[5] + p[0] - x) && (z > (p[5] - p[1] + x)))
+                if ((z > (p[5] + p[2] - y)) && (z > (p[5] - p[3] + y))) af = cube(fabs(z - p[5]) / a.sc[5]);
+        }
+    }
+    af = fmin(1.0, af);
+    af = fmax(0.0, af);
+    return 1.0 - af;
+}
+
+// Attenuate_EM_Vacuum (bc_attenuate.F90:151-220): every cell of the
+// ghosted grid outside the box of attn_vac_pos_ind has its six components
+// scaled by AttenFactorVacuum at their staggered positions.
+__global__ void k_attn_vacuum(GridP g, AttnVac a, double *Ex, double *Ey, double *Ez, double *Bx, double *By,
+                              double *Bz)
+{
+    const long long n = g.ncell;
+    const bool three_d = g.dims == 3;
+    const double x0 = -3.0, y0 = -3.0, z0 = three_d ? -3.0 : 0.0;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long jk = c / g.mx;
+        const int i = (int)(c - jk * g.mx) + 1, j = (int)(jk % g.my) + 1, k = (int)(jk / g.my) + 1;
+        const int ig = i - 3, jg = j - 3, kg = k - 3;
+        const bool inside = ig > a.ind[0] && ig < a.ind[1] && jg > a.ind[2] && jg < a.ind[3] &&
+                            (!three_d || (kg > a.ind[4] && kg < a.ind[5]));
+        if (inside) continue;
+        const double xi = (double)i + x0, yj = (double)j + y0, zk = (double)k + z0;
+        const double xh = (double)i + 0.5 + x0, yh = (double)j + 0.5 + y0, zh = (double)k + 0.5 + z0;
+        Ex[c] = Ex[c] * atten_factor_vacuum(a, three_d, xh, yj, zk);
+        Ey[c] = Ey[c] * atten_factor_vacuum(a, three_d, xi, yh, zk);
+        Ez[c] = Ez[c] * atten_factor_vacuum(a, three_d, xi, yj, zh);
+        Bx[c] = Bx[c] * atten_factor_vacuum(a, three_d, xi, yh, zh);
+        By[c] = By[c] * atten_factor_vacuum(a, three_d, xh, yj, zh);
+        Bz[c] = Bz[c] * atten_factor_vacuum(a, three_d, xh, yh, zk);
+    }
+}
+
+// Attenuate_EM_Flow (bc_attenuate.F90:16-98) for a uniform flow: MagFld and
+// Drift of the face are the constants b and v.  atnn_domain (:117-131) on
+// face side (1..4) with the thickness dl, AttenFactor (:102-115) with the
+// scale length sc.
+struct AttnFlow {
+    double pos, dl, sc, b[3], v[3];
+    int side;
+};
+__device__ __forceinline__ bool atnn_domain(const AttnFlow &a, double xg, double yg)
+{
+    switch (a.side) {
+        case 1: return xg >= a.pos && xg <= a.pos + a.dl;
+        case 2: return xg <= a.pos && xg >= a.pos - a.dl;
+        case 3: return yg >= a.pos && yg <= a.pos + a.dl;
+        default: return yg <= a.pos && yg >= a.pos - a.dl;
+    }
+}
+__device__ __forceinline__ double atten_factor(const AttnFlow &a, double xg, double yg)
+{
+    const double t = a.side <= 2 ? fabs(xg - a.pos) / a.sc : fabs(yg - a.pos) / a.sc;
+    double af = cube(t);
+    af = fmin(1.0, af);
+    af = fmax(0.0, af);
+    return 1.0 - af;
+}
+__global__ void k_attn_flow(GridP g, AttnFlow a, double *Ex, double *Ey, double *Ez, double *Bx, double *By, double *Bz)
+{
+    const long long n = g.ncell;
+    const double x0 = -3.0, y0 = -3.0;
+    // the flow's motional field -v x B, as the reference forms it per component
+    const double fx = a.v[2] * a.b[1] - a.v[1] * a.b[2];
+    const double fy = a.v[0] * a.b[2] - a.v[2] * a.b[0];
+    const double fz = a.v[1] * a.b[0] - a.v[0] * a.b[1];
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long jk = c / g.mx;
+        const int i = (int)(c - jk * g.mx) + 1, j = (int)(jk % g.my) + 1;
+        const double xi = (double)i + x0, yj = (double)j + y0;
+        const double xh = (double)i + 0.5 + x0, yh = (double)j + 0.5 + y0;
+        if (atnn_domain(a, xh, yj)) Ex[c] = (Ex[c] - fx) * atten_factor(a, xh, yj) + fx;
+        if (atnn_domain(a, xi, yh)) Ey[c] = (Ey[c] - fy) * atten_factor(a, xi, yh) + fy;
+        if (atnn_domain(a, xi, yj)) Ez[c] = (Ez[c] - fz) * atten_factor(a, xi, yj) + fz;
+        if (atnn_domain(a, xi, yh)) Bx[c] = (Bx[c] - a.b[0]) * atten_factor(a, xi, yh) + a.b[0];
+        if (atnn_domain(a, xh, yj)) By[c] = (By[c] - a.b[1]) * atten_factor(a, xh, yj) + a.b[1];
+        if (atnn_domain(a, xh, yh)) Bz[c] = (Bz[c] - a.b[2]) * atten_factor(a, xh, yh) + a.b[2];
+    }
+}
+
+// OpenBC_Fld_Right (side 1, bc.F90:411-440) / OpenBC_Fld_Left (side 0,
+// :442-469) at the local layer xl: Ey, Ez halved and Bx copied from layer xl
+// beyond it, Ex, By, Bz halved from xl on (right) or below xl (left).
+__global__ void k_open_fld_x(GridP g, double *Ex, double *Ey, double *Ez, double *Bx, double *By, double *Bz, int xl,
+                             int side)
+{
+    const long long n = g.ncell;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const long long jk = c / g.mx;
+        const int i = (int)(c - jk * g.mx) + 1;
+        const long long src = (long long)(xl - 1) + g.mx * jk;
+        const bool a = side == 1 ? i >= xl + 1 : i <= xl - 1;   // Ey, Ez, Bx
+        const bool b = side == 1 ? i >= xl : i <= xl - 1;       // Ex, By, Bz
+        if (a) {
+            Ey[c] = 0.5 * Ey[c];
+            Ez[c] = 0.5 * Ez[c];
+            Bx[c] = Bx[src];
+        }
+        if (b) {
+            Ex[c] = 0.5 * Ex[c];
+            By[c] = 0.5 * By[c];
+            Bz[c] = 0.5 * Bz[c];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 'open' particle faces along x: OpenBC_Prtl_Right / Left (bc.F90:478-621)
+// with dx = 1 (EnforceBC_Final, :333-334).  The particles beyond the face
+// become holes (DeletePrtl, mem_prtl.F90:7-22); each particle in the layer
+// of width dx inside the face is mirrored across it and appended
+// (InsertNewPrtl, mem_prtl.F90:120-133, in slot order), its u lowered by
+// gamma v0 with v0 the mean x velocity of flavours 1, 2 in its (j, k)
+// column of the layer (OpenBC_MeanPrtlSpeed, bc.F90:603-621; den starts at
+// 1), clamped to <= 0 on the right face and >= 0 on the left one.
+// ---------------------------------------------------------------------------
+
+// den = 1, vel = 0 over the my * mz columns (col[c], col[ncol + c]).
+__global__ void k_open_cols_init(double *col, int ncol)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += gridDim.x * blockDim.x) {
+        col[c] = 1.0;
+        col[ncol + c] = 0.0;
+    }
+}
+
+// Holes beyond the face, layer flags, and the column sums (FP64 atomics: the
+// sums' order, and with it the last bit of v0, follows the atomics).
+__global__ void k_open_prtl_mark(GridP g, PartF64 p, const Counters *__restrict__ cnt, int side, double wall,
+                                 double dx, uint32_t *flag, double *col, double zhole, int *err)
+{
+    const long long used = cnt->used;
+    const int ncol = g.my * g.mz;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used;
+         n += (long long)gridDim.x * blockDim.x) {
+        uint32_t f = 0;
+        if (p.q[n] != 0.0) {
+            const double x = p.x[n];
+            if (side == 1 ? x > wall : x < wall) {
+                p.q[n] = 0.0;
+                p.x[n] = 3.8;
+                p.y[n] = 3.8;
+                p.z[n] = zhole;
+                p.u[n] = 0.0;
+                p.v[n] = 0.0;
+                p.w[n] = 0.0;
+                p.flv[n] = 0;
+            } else if (side == 1 ? (x > wall - dx && x < wall) : (x < wall + dx && x > wall)) {
+                const int j = (int)p.y[n], k = g.dims == 3 ? (int)p.z[n] : 1;
+                if (j < 1 || j > g.my || k < 1 || k > g.mz) {
+                    raise_error(err, PIC_DEVERR_RANGE);
+                } else {
+                    f = 1;
+                    if (p.flv[n] <= 2) {
+                        const double u = p.u[n], v = p.v[n], w = p.w[n];
+                        const double invg = 1.0 / sqrt(1.0 + u * u + v * v + w * w);
+                        const int c = (j - 1) + g.my * (k - 1);
+                        atomicAdd(col + c, 1.0);
+                        atomicAdd(col + ncol + c, u * invg);
+                    }
+                }
+            }
+        }
+        flag[n] = f;
+    }
+}
+
+// vel = vel / den per column.
+__global__ void k_open_cols_mean(double *col, int ncol)
+{
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncol; c += gridDim.x * blockDim.x)
+        col[ncol + c] = col[ncol + c] / col[c];
+}
+
+constexpr int kOpenTile = 4096;   // slots per block of the stable compaction
+
+// Flagged slots per tile of kOpenTile slots below `used`.
+__global__ void __launch_bounds__(256) k_open_tile_counts(const Counters *__restrict__ cnt,
+                                                          const uint32_t *__restrict__ flag, uint32_t *counts)
+{
+    __shared__ uint32_t red[8];
+    const long long used = cnt->used;
+    const long long base = (long long)blockIdx.x * kOpenTile;
+    uint32_t c = 0;
+    for (int r = threadIdx.x; r < kOpenTile; r += 256) {
+        const long long n = base + r;
+        if (n < used) c += flag[n];
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; w++) t += red[w];
+        counts[blockIdx.x] = t;
+    }
+}
+
+// The mirrored copies, appended at used + (rank of the particle among the
+// layer's particles in slot order): block b ranks the flags of its tile
+// from the tile's offset (stable: lanes, warps and chunks in slot order);
+// nothing is written when the copies do not fit.
+__global__ void __launch_bounds__(256) k_open_prtl_insert(GridP g, PartF64 p, const Counters *__restrict__ cnt,
+                                                          int side, double wall, const uint32_t *__restrict__ flag,
+                                                          const uint32_t *__restrict__ offs,
+                                                          const uint32_t *__restrict__ total,
+                                                          const double *__restrict__ col, long long capacity, int *err)
+{
+    __shared__ uint32_t wsum[8];
+    const long long used = cnt->used;
+    const long long m = (long long)*total;
+    if (used + m > capacity) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
+        return;
+    }
+    const int ncol = g.my * g.mz;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t run = offs[blockIdx.x];
+    const long long base = (long long)blockIdx.x * kOpenTile;
+    for (int r = 0; r < kOpenTile; r += 256) {
+        const long long n = base + r + threadIdx.x;
+        const bool f = n < used && flag[n] != 0;
+        const uint32_t bal = __ballot_sync(0xffffffffu, f);
+        if (lane == 0) wsum[warp] = __popc(bal);
+        __syncthreads();
+        uint32_t before = 0, chunk = 0;
+        for (int w = 0; w < 8; w++) {
+            if (w < warp) before += wsum[w];
+            chunk += wsum[w];
+        }
+        if (f) {
+            uint32_t lt;
+            asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
+            const long long d = used + (long long)(run + before + __popc(bal & lt));
+            const double x = p.x[n], y = p.y[n], z = p.z[n], u = p.u[n], v = p.v[n], w = p.w[n];
+            const int j = (int)y, k = g.dims == 3 ? (int)z : 1;
+            double v0 = col[ncol + (j - 1) + g.my * (k - 1)];
+            if (side == 1 ? v0 > 0.0 : v0 < 0.0) v0 = 0.0;
+            const double gamma = sqrt(1.0 + u * u + v * v + w * w);
+            p.x[d] = 2.0 * wall - x;
+            p.y[d] = y;
+            p.z[d] = z;
+            p.u[d] = u - gamma * v0;
+            p.v[d] = v;
+            p.w[d] = w;
+            p.q[d] = p.q[n];
+            p.flv[d] = p.flv[n];
+        }
+        run += chunk;
+        __syncthreads();
+    }
+}
+
+__global__ void k_open_prtl_finish(Counters *cnt, const uint32_t *__restrict__ total, long long capacity)
+{
+    const long long m = (long long)*total;
+    if (cnt->used + m <= capacity) cnt->used += m;
+}
+
 int grid_for(long long n)
 {
     const long long b = (n + kThreads - 1) / kThreads;
@@ -216,6 +518,84 @@ void launch_wall_conducting(const GridP &g, double *const E[3], int side, double
     }
     k_zero_x_layers<<<grid_for((long long)(x1 - x0 + 1) * g.my * g.mz), kThreads, 0, s>>>(g, E[1], E[2], x0, x1);
     count_launches(1);
+}
+
+// Attenuate_EM_Vacuum for the 'attn' faces in the bit mask `faces` (bit n-1
+// = bc_face(n)) at pos[n-1] with attn_scale sc[n-1]; returns without a
+// launch when the whole grid lies inside (bc_attenuate.F90:158-172).
+void launch_bc_attenuate(const GridP &g, double *const E[3], double *const B[3], int faces, const double *pos,
+                         const double *sc, cudaStream_t s)
+{
+    AttnVac a;
+    for (int n = 0; n < 6; n++) {
+        const bool on = (faces >> n) & 1;
+        const bool upper = (n & 1) != 0;   // faces 2, 4, 6
+        a.p[n] = on ? pos[n] : (upper ? 2147483647.0 : -2147483647.0);
+        a.sc[n] = on ? sc[n] : 1.0;
+        a.ind[n] = on ? (upper ? (int)ceil(a.p[n]) + 1 : (int)floor(a.p[n]) - 1) : (upper ? 2147483647 : -2147483647);
+    }
+    const bool inside = 1 - 3 > a.ind[0] && g.mx - 3 < a.ind[1] && 1 - 3 > a.ind[2] && g.my - 3 < a.ind[3] &&
+                        (g.dims == 2 || (1 - 3 > a.ind[4] && g.mz - 3 < a.ind[5]));
+    if (inside) return;
+    k_attn_vacuum<<<grid_for(g.ncell), kThreads, 0, s>>>(g, a, E[0], E[1], E[2], B[0], B[1], B[2]);
+    count_launches(1);
+}
+
+// Attenuate_EM_Flow on face `side` (1..4) with a uniform flow; nothing when
+// the thickness is 0 or the layer lies outside the grid (:33-35).
+void launch_bc_attenuate_flow(const GridP &g, double *const E[3], double *const B[3], int side, double pos, double dl,
+                              double sc, const double *b, const double *v, cudaStream_t s)
+{
+    if (dl == 0.0) return;
+    const double o = -3.0;   // x0 = y0
+    if (side == 1 && (pos + dl) - o < 1) return;
+    if (side == 3 && (pos + dl) - o < 1) return;
+    if (side == 2 && (pos - dl) - o > g.mx) return;
+    if (side == 4 && (pos - dl) - o > g.my) return;
+    AttnFlow a;
+    a.pos = pos;
+    a.dl = dl;
+    a.sc = sc;
+    a.side = side;
+    for (int d = 0; d < 3; d++) {
+        a.b[d] = b[d];
+        a.v[d] = v[d];
+    }
+    k_attn_flow<<<grid_for(g.ncell), kThreads, 0, s>>>(g, a, E[0], E[1], E[2], B[0], B[1], B[2]);
+    count_launches(1);
+}
+
+// OpenBC_Fld_Left (side 0) / OpenBC_Fld_Right (side 1) at `pos`.
+void launch_bc_open_fld_x(const GridP &g, double *const E[3], double *const B[3], int side, double pos, cudaStream_t s)
+{
+    const int xl = (int)ceil(pos - 0.0 + 3);
+    if (side == 1 ? !(xl >= 1 && xl <= g.mx - 1) : !(xl >= 2 && xl <= g.mx)) return;
+    k_open_fld_x<<<grid_for(g.ncell), kThreads, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], xl, side);
+    count_launches(1);
+}
+
+// OpenBC_Prtl_Left (side 0) / OpenBC_Prtl_Right (side 1) at `pos` with
+// dx = 1; col holds 2 my mz doubles; flag (capacity words), counts
+// (capacity / 4096 + 1 words), scan_tmp and total are scratch (the
+// radix-sort buffers, free between reorders).
+void launch_bc_open_prtl_x(const GridP &g, PartF64 &p, Counters *cnt, int side, double pos, double *col,
+                           uint32_t *flag, uint32_t *counts, uint32_t *scan_tmp, uint32_t *total, long long capacity,
+                           int *err, cudaStream_t s)
+{
+    const double wall = pos - 0.0 + 3;
+    if (side == 1 ? !(wall < g.mx - 1) : !(wall > 1)) return;
+    const int ncol = g.my * g.mz;
+    const unsigned tiles = (unsigned)((capacity + kOpenTile - 1) / kOpenTile);
+    k_open_cols_init<<<grid_for(ncol), kThreads, 0, s>>>(col, ncol);
+    k_open_prtl_mark<<<grid_for(capacity), kThreads, 0, s>>>(g, p, cnt, side, wall, 1.0, flag, col,
+                                                             g.dims == 3 ? 3.8 : 1.5, err);
+    k_open_cols_mean<<<grid_for(ncol), kThreads, 0, s>>>(col, ncol);
+    k_open_tile_counts<<<tiles, 256, 0, s>>>(cnt, flag, counts);
+    count_launches(4);
+    scan_exclusive_u32(counts, counts, tiles, scan_tmp, total, s);
+    k_open_prtl_insert<<<tiles, 256, 0, s>>>(g, p, cnt, side, wall, flag, counts, total, col, capacity, err);
+    k_open_prtl_finish<<<1, 1, 0, s>>>(cnt, total, capacity);
+    count_launches(2);
 }
 
 }  // namespace pic

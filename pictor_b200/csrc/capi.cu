@@ -35,6 +35,7 @@ struct pic_handle {
     bool fp32 = false;
     void *E[3] = {}, *B[3] = {}, *J[3] = {};
     void *Jtmp = nullptr;
+    double *open_col = nullptr;   // den, vel per (j, k) column of an 'open' particle face (2 my mz)
     // cylindrical modal form: the fields on modes m = 0, 1, (mx, 3, mz) each;
     // E and B above are kept equal to their theta-gridded synthesis
     bool modal = false;
@@ -1533,6 +1534,55 @@ int pic_bc_remove(pic_handle *h, int32_t face, double pos)
         (h->g.x_external && face <= 2))
         return PIC_ERR_INVALID;
     launch_wall_remove(h->g, h->p64[h->cur], h->cnt, face, pos, h->capacity, h->s);
+    return finish_phase(h);
+}
+
+int pic_bc_attenuate(pic_handle *h, int32_t faces, const double *pos, const double *scale)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || !pos || !scale || faces < 0 ||
+        faces > 63 || (h->g.dims == 2 && (faces & 48)))
+        return PIC_ERR_INVALID;
+    for (int n = 0; n < 6; n++)
+        if (((faces >> n) & 1) && !(scale[n] > 0.0)) return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_bc_attenuate(h->g, E, B, faces, pos, scale, h->s);
+    return finish_phase(h);
+}
+
+int pic_bc_attenuate_flow(pic_handle *h, int32_t face, double pos, double thickness, double scale,
+                          const double *bflow, const double *drift)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || face < 1 || face > 4 || !bflow || !drift ||
+        !(scale > 0.0) || !(thickness >= 0.0) || (h->g.x_external && face <= 2))
+        return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_bc_attenuate_flow(h->g, E, B, face, pos, thickness, scale, bflow, drift, h->s);
+    return finish_phase(h);
+}
+
+int pic_bc_open_x(pic_handle *h, int32_t side, double pos)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || (side != 0 && side != 1))
+        return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_bc_open_fld_x(h->g, E, B, side, pos, h->s);
+    return finish_phase(h);
+}
+
+int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || (side != 0 && side != 1))
+        return PIC_ERR_INVALID;
+    if (!h->open_col) {
+        const int r = dalloc(h, &h->open_col, 2 * (size_t)h->g.my * (size_t)h->g.mz);
+        if (r) return r;
+    }
+    SortScratch &sc = h->sc;
+    launch_bc_open_prtl_x(h->g, h->p64[h->cur], h->cnt, side, pos, h->open_col, sc.key[0], sc.hist, sc.scan_tmp,
+                          sc.scan_tmp + sc.scan_tmp_len - 1, h->capacity, h->err, h->s);
     return finish_phase(h);
 }
 

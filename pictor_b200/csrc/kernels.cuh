@@ -196,6 +196,18 @@ void launch_wall_reflect_y(const GridP &g, PartF64 &p, const Counters *cnt, doub
 void launch_wall_conducting_y(const GridP &g, double *const E[3], int side, double pos, cudaStream_t s);
 void launch_wall_remove(const GridP &g, PartF64 &p, const Counters *cnt, int face, double pos, long long capacity,
                         cudaStream_t s);
+// bc.cu: field faces of EnforceBC_Final (bc.F90:292-340): 'attn' faces
+// (Attenuate_EM_Vacuum), an 'iflw' face with a uniform flow
+// (Attenuate_EM_Flow), 'open' faces along x (OpenBC_Fld_Left/Right)
+void launch_bc_attenuate(const GridP &g, double *const E[3], double *const B[3], int faces, const double *pos,
+                         const double *sc, cudaStream_t s);
+void launch_bc_attenuate_flow(const GridP &g, double *const E[3], double *const B[3], int side, double pos, double dl,
+                              double sc, const double *b, const double *v, cudaStream_t s);
+void launch_bc_open_fld_x(const GridP &g, double *const E[3], double *const B[3], int side, double pos, cudaStream_t s);
+// bc.cu: an 'open' particle face along x (OpenBC_Prtl_Left/Right, bc.F90:478-621)
+void launch_bc_open_prtl_x(const GridP &g, PartF64 &p, Counters *cnt, int side, double pos, double *col,
+                           uint32_t *flag, uint32_t *counts, uint32_t *scan_tmp, uint32_t *total, long long capacity,
+                           int *err, cudaStream_t s);
 // slab.cu: x faces of a slab (fields and particles), see pic_slab_* in the C ABI
 void launch_slab_pack_fields(const GridP &g, int which, double *const F[3], double *to_left, double *to_right,
                              cudaStream_t s);

@@ -142,6 +142,40 @@ module pictor_b200_capi
       end function
    end interface
 
+   ! Field faces of EnforceBC_Final besides 'cond': 'attn' faces
+   ! (Attenuate_EM_Vacuum: faces = bit mask of bc_face(1:6), pos and scale
+   ! hold bc_face(:)%pos_fld and %attn_scale), an 'iflw' face with a uniform
+   ! flow (Attenuate_EM_Flow), 'open' x faces for fields (OpenBC_Fld_*) and
+   ! particles (OpenBC_Prtl_*).
+   interface
+      integer(c_int) function pic_bc_attenuate(h, faces, pos, scale) bind(C, name="pic_bc_attenuate")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: faces
+         real(c_double), intent(in) :: pos(6), scale(6)
+      end function
+      integer(c_int) function pic_bc_attenuate_flow(h, face, pos, thickness, scale, bflow, drift) &
+            bind(C, name="pic_bc_attenuate_flow")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: face
+         real(c_double), value :: pos, thickness, scale
+         real(c_double), intent(in) :: bflow(3), drift(3)
+      end function
+      integer(c_int) function pic_bc_open_x(h, side, pos) bind(C, name="pic_bc_open_x")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+      integer(c_int) function pic_bc_open_prtl_x(h, side, pos) bind(C, name="pic_bc_open_prtl_x")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: side
+         real(c_double), value :: pos
+      end function
+   end interface
+
    ! Slab form (cfg%slab_x = 1): x faces exchanged by the host
    ! between ranks; buffers are device addresses (a CUDA-aware MPI_Sendrecv
    ! takes them as they are), see include/pictor_b200.h.

@@ -258,6 +258,38 @@ class Simulation:
         """RemovePrtl_Left / Right (bc_open.F90:8-62) at face 1..6 (x, y, z; low, high)."""
         check(self.L.pic_bc_remove(self.h, int(face), float(pos)), "pic_bc_remove")
 
+    def Attenuate_EM_Vacuum(self, faces: dict):
+        """Attenuate_EM_Vacuum (bc_attenuate.F90:151-290) for the faces of type
+        'attn': ``faces`` maps bc_face index 1..6 to (pos_fld, attn_scale)."""
+        mask = 0
+        pos = (C.c_double * 6)()
+        sc = (C.c_double * 6)(*([1.0] * 6))
+        for n, (p, s) in faces.items():
+            mask |= 1 << (int(n) - 1)
+            pos[int(n) - 1] = float(p)
+            sc[int(n) - 1] = float(s)
+        check(self.L.pic_bc_attenuate(self.h, mask, pos, sc), "pic_bc_attenuate")
+
+    def Attenuate_EM_Flow(self, face: int, pos: float, thickness: float = 1.0, scale: float = 4.0,
+                          bflow=(0.0, 0.0, 0.0), drift=(0.0, 0.0, 0.0)):
+        """Attenuate_EM_Flow (bc_attenuate.F90:16-131) of an 'iflw' face 1..4
+        with a uniform flow (MagFld = bflow, DriftVelocity = drift); the
+        defaults are SetBC_InflowFld's (bc.F90:163-205)."""
+        b = (C.c_double * 3)(*map(float, bflow))
+        v = (C.c_double * 3)(*map(float, drift))
+        check(self.L.pic_bc_attenuate_flow(self.h, int(face), float(pos), float(thickness), float(scale), b, v),
+              "pic_bc_attenuate_flow")
+
+    def OpenBC_Fld_x(self, side: int, pos: float):
+        """OpenBC_Fld_Left (side 0) / OpenBC_Fld_Right (side 1), bc.F90:411-469."""
+        check(self.L.pic_bc_open_x(self.h, int(side), float(pos)), "pic_bc_open_x")
+
+    def OpenBC_Prtl_x(self, side: int, pos: float):
+        """OpenBC_Prtl_Left (side 0) / OpenBC_Prtl_Right (side 1), bc.F90:478-621,
+        with dx = 1: particles beyond pos removed, the layer inside mirrored
+        and appended with the column's mean x velocity taken out."""
+        check(self.L.pic_bc_open_prtl_x(self.h, int(side), float(pos)), "pic_bc_open_prtl_x")
+
     update_b_half = UpdateBfieldHalfGPU
     move_deposit = MoveDepositPrtlGPU
     exchange_particles = ExchangePrtlGPU

@@ -123,3 +123,9 @@ def test_slab_and_wall_entry_points_validate_without_gpu():
     for fn in (L.pic_bc_reflect_x, L.pic_bc_conducting_x, L.pic_bc_reflect_y, L.pic_bc_conducting_y):
         assert fn(None, 0, 1.5) == -1
     assert L.pic_bc_remove(None, 1, 1.5) == -1
+    six = (C.c_double * 6)(*([1.0] * 6))
+    three = (C.c_double * 3)()
+    assert L.pic_bc_attenuate(None, 1, six, six) == -1
+    assert L.pic_bc_attenuate_flow(None, 2, 30.0, 1.0, 4.0, three, three) == -1
+    assert L.pic_bc_open_x(None, 1, 1.5) == -1
+    assert L.pic_bc_open_prtl_x(None, 1, 1.5) == -1
