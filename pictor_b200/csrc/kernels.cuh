@@ -70,6 +70,8 @@ struct Tiles64 {
     uint32_t *range;              // 2 H per tile: first and past-the-end slot of each row segment
     int *box;                     // 8 per tile: lo[3], hi[3] of the cells its particles occupy (1-based)
     long long *np;                // the live count at the reorder: slots past it were appended since
+    unsigned long long *qmax;     // bits of max |q| over the live particles at the reorder (>= 0 doubles
+                                  // order as their bit patterns): the bound of the fixed-point current box
     int W, H, nsx, ntiles;        // W cells per row segment, H rows per tile
     int smem_bytes;
 };

@@ -24,7 +24,7 @@
 //   * it records the cells its particles move to, which bound the box of the
 //     next step (the particles drift out of their tile between reorders).
 // The current differs from the per-particle mover's only in the order of
-// its FP64 sums.  A particle that leaves the interior is wrapped by the
+// its sums and the fixed-point rounding of each contribution.  A particle that leaves the interior is wrapped by the
 // exchange and appended after the sorted range; those are moved by the
 // per-particle kernel (k_move_f64).  A particle of a tile whose cell lies
 // outside the box, or all particles of a tile whose box does not fit in
@@ -136,35 +136,60 @@ __device__ __forceinline__ void gather_box64(const Box64 &bx, const double *sN, 
     }
 }
 
-// The VecJ entries o of a cell whose box current cell is jb, added into the
-// FP64 box (the scatter offsets of movdep_routines.F90:276-303).
-template <int DIMS>
-__device__ __forceinline__ void deposit_box64(const Box64 &bx, double *sJ, int jb, const double *o)
+// An FP64 value already multiplied by the box's scale, rounded to the
+// nearest integer: adding 1.5 * 2^52 leaves it in the low mantissa bits
+// (exact for |v| < 2^51).
+__device__ __forceinline__ long long fixed64(double v)
 {
-    double *jx = sJ + jb, *jy = sJ + bx.nj + jb, *jz = sJ + 2 * bx.nj + jb;
+    return __double_as_longlong(v + 6755399441055744.0) - 0x4338000000000000ll;
+}
+
+// q added to the 64-bit word w of the fixed-point box with two native 32-bit
+// shared-memory atomics: the low halves, then the high halves with the carry
+// out of the low word, which the add that wrapped it sees in the old value
+// it gets back.  The word then holds the exact sum of every q added (mod 2^64;
+// the scale keeps the sums far inside the signed range).
+__device__ __forceinline__ void add_fixed64(unsigned long long *w, long long q)
+{
+    unsigned *p = reinterpret_cast<unsigned *>(w);
+    const unsigned lo = (unsigned)(unsigned long long)q, hi = (unsigned)((unsigned long long)q >> 32);
+    const unsigned old = atomicAdd(p, lo);
+    const unsigned h = hi + (old + lo < old ? 1u : 0u);
+    if (h) atomicAdd(p + 1, h);
+}
+
+// The VecJ entries o of a cell whose box current cell is jb, added into the
+// fixed-point box (the scatter offsets of movdep_routines.F90:276-303): each
+// entry times the scale S rounded to an integer.
+template <int DIMS>
+__device__ __forceinline__ void deposit_box64(const Box64 &bx, unsigned long long *sJ, int jb, const double *o,
+                                              double S)
+{
+    unsigned long long *jx = sJ + jb, *jy = sJ + bx.nj + jb, *jz = sJ + 2 * bx.nj + jb;
     const int oy = bx.JX, oz = bx.JXY;
+    auto add = [&](unsigned long long *a, double v) { add_fixed64(a, fixed64(v * S)); };
     if (DIMS == 2) {
-        atomicAdd(jx, o[0]);
-        atomicAdd(jx + oy, o[1]);
-        atomicAdd(jy, o[2]);
-        atomicAdd(jy + 1, o[3]);
-        atomicAdd(jz, o[4]);
-        atomicAdd(jz + 1, o[5]);
-        atomicAdd(jz + oy, o[6]);
-        atomicAdd(jz + 1 + oy, o[7]);
+        add(jx, o[0]);
+        add(jx + oy, o[1]);
+        add(jy, o[2]);
+        add(jy + 1, o[3]);
+        add(jz, o[4]);
+        add(jz + 1, o[5]);
+        add(jz + oy, o[6]);
+        add(jz + 1 + oy, o[7]);
     } else {
-        atomicAdd(jx, o[0]);
-        atomicAdd(jx + oy, o[1]);
-        atomicAdd(jx + oz, o[2]);
-        atomicAdd(jx + oy + oz, o[3]);
-        atomicAdd(jy, o[4]);
-        atomicAdd(jy + 1, o[5]);
-        atomicAdd(jy + oz, o[6]);
-        atomicAdd(jy + 1 + oz, o[7]);
-        atomicAdd(jz, o[8]);
-        atomicAdd(jz + 1, o[9]);
-        atomicAdd(jz + oy, o[10]);
-        atomicAdd(jz + 1 + oy, o[11]);
+        add(jx, o[0]);
+        add(jx + oy, o[1]);
+        add(jx + oz, o[2]);
+        add(jx + oy + oz, o[3]);
+        add(jy, o[4]);
+        add(jy + 1, o[5]);
+        add(jy + oz, o[6]);
+        add(jy + 1 + oz, o[7]);
+        add(jz, o[8]);
+        add(jz + 1, o[9]);
+        add(jz + oy, o[10]);
+        add(jz + 1 + oy, o[11]);
     }
 }
 
@@ -244,10 +269,21 @@ __global__ void __launch_bounds__(kT64Threads, 2) k_move_f64_tiled(GridP g, Part
     // tile's particles all take the global path
     const bool use_box = fits(nnode);
     double *sN = smem64;
-    double *sJ = smem64 + 6 * (use_box ? nnode : 0);
+    unsigned long long *sJ = reinterpret_cast<unsigned long long *>(smem64 + 6 * (use_box ? nnode : 0));
+    // fixed-point scale of the current box: a particle adds at most
+    // b = max|q| qi c to a word (its displacement per axis is below c, the
+    // weights at most 1), so with S <= 2^62 / (N b) no sum of the tile's N
+    // particles leaves the signed range, and S <= 2^50 / b keeps every
+    // product within the range of fixed64; one unit is then at most 2^-50 of
+    // b (and N 2^-62 of it for N > 4096), far below the FP64 rounding of J
+    double S = 1.0;
+    {
+        const double b = __longlong_as_double((long long)*T.qmax) * g.qi * g.c;
+        if (b > 0.0) S = 1125899906842624.0 / b * (total > 4096u ? 4096.0 / (double)total : 1.0);
+    }
     if (use_box) {
         const long long sy = g.sy, sz = g.sz;
-        for (int q = tid; q < 3 * bx.nj; q += kT64Threads) sJ[q] = 0.0;
+        for (int q = tid; q < 3 * bx.nj; q += kT64Threads) sJ[q] = 0ull;
         for (int q = tid; q < nnode; q += kT64Threads) {
             const int a = q % bx.NX, r = q / bx.NX, b = r % (bx.C[1] + 1), c = r / (bx.C[1] + 1);
             const long long nd = cidx(g, lo[0] + a, lo[1] + b, DIMS == 3 ? lo[2] + c : 1);
@@ -282,11 +318,9 @@ __global__ void __launch_bounds__(kT64Threads, 2) k_move_f64_tiled(GridP g, Part
     // w takes item 32 (l / 4) + 4 w + l % 4.  The four lanes of a quad read
     // four consecutive slots (one 32-byte sector of each array), and the
     // eight quads of a warp lie 32 items apart, in different cells at the
-    // usual fill.  Shared-memory FP64 atomics are compare-and-swap loops,
-    // which retry while lanes meet at an address: this order puts at most
-    // four lanes of a warp on one cell, where the 32 consecutive items of a
-    // plain grid stride share one or two cells (1.57 -> 1.13 ms on 8.4 M
-    // particles at 16 per cell).
+    // usual fill: lanes whose atomics meet at an address serialise, and this
+    // order puts at most four lanes of a warp on one cell, where the 32
+    // consecutive items of a plain grid stride share one or two cells.
     const uint32_t lane = tid & 31;
     const uint32_t perm = (lane >> 2) * 32 + (uint32_t)(tid >> 5) * 4 + (lane & 3);
     P64 cur;
@@ -356,11 +390,11 @@ __global__ void __launch_bounds__(kT64Threads, 2) k_move_f64_tiled(GridP g, Part
             if (same) {
 #pragma unroll
                 for (int e = 0; e < (DIMS == 3 ? 12 : 8); e++) o[e] = o[e] + o2[e];
-                deposit_box64<DIMS>(bx, sJ, jb0, o);
+                deposit_box64<DIMS>(bx, sJ, jb0, o, S);
             } else {
-                deposit_box64<DIMS>(bx, sJ, jb0, o);
+                deposit_box64<DIMS>(bx, sJ, jb0, o, S);
                 deposit_box64<DIMS>(bx, sJ, jb0 + (ip - ip0) + bx.JX * (jp - jp0) + (DIMS == 3 ? bx.JXY * (kp - kp0) : 0),
-                                    o2);
+                                    o2, S);
             }
         } else {
             scatter<double, DIMS>(g, Jx, Jy, Jz, cidx(g, ip0, jp0, kp0), o);
@@ -389,9 +423,11 @@ __global__ void __launch_bounds__(kT64Threads, 2) k_move_f64_tiled(GridP g, Part
     if (use_box) {
         // the box current onto J (one FP64 atomic per nonzero word)
         const int JY = bx.C[1] + 3;
+        const double inv = 1.0 / S;
         for (int q = tid; q < bx.nj; q += kT64Threads) {
-            const double vx = sJ[q], vy = sJ[bx.nj + q], vz = sJ[2 * bx.nj + q];
-            if (vx == 0.0 && vy == 0.0 && vz == 0.0) continue;
+            const long long ix = (long long)sJ[q], iy = (long long)sJ[bx.nj + q], iz = (long long)sJ[2 * bx.nj + q];
+            if (ix == 0 && iy == 0 && iz == 0) continue;
+            const double vx = (double)ix * inv, vy = (double)iy * inv, vz = (double)iz * inv;
             const int a = q % bx.JX, r = q / bx.JX, b = r % JY, cc = r / JY;
             const long long off = cidx(g, bx.lo[0] - 1 + a, bx.lo[1] - 1 + b, DIMS == 3 ? bx.lo[2] - 1 + cc : 1);
             if (vx != 0.0) atomicAdd(Jx + off, vx);

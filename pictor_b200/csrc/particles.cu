@@ -229,10 +229,11 @@ int sort_key_bits(long long ncell) { return key_bits(ncell); }
 // ReorderPrtlArr (mem_prtl.F90:166-301)
 // ---------------------------------------------------------------------------
 __global__ void k_keys_f64(GridP g, PartF64 p, const long long *__restrict__ used, uint32_t *keys, long long *np,
-                           int *err)
+                           int *err, unsigned long long *qmax)
 {
     const long long n = *used;
     long long live = 0;
+    unsigned long long qm = 0;   // bits of max |q| of this thread's live particles (when qmax is given)
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         uint32_t key = (uint32_t)g.ncell;  // holes sort last (mem_prtl.F90:179 skips them)
         if (p.flv[i] != 0) {
@@ -241,6 +242,7 @@ __global__ void k_keys_f64(GridP g, PartF64 p, const long long *__restrict__ use
             if (ci >= 1 && ci <= g.mx && cj >= 1 && cj <= g.my && ck >= 1 && ck <= g.mz) {
                 key = (uint32_t)cidx(g, ci, cj, ck);
                 live++;
+                if (qmax) qm = max(qm, (unsigned long long)__double_as_longlong(fabs(p.q[i])));
             } else {
                 raise_error(err, PIC_DEVERR_RANGE);
             }
@@ -256,6 +258,10 @@ __global__ void k_keys_f64(GridP g, PartF64 p, const long long *__restrict__ use
         long long t = 0;
         for (int w = 0; w < kThreads / 32; w++) t += red[w];
         atomicAdd((unsigned long long *)np, (unsigned long long)t);
+    }
+    if (qmax) {
+        for (int o = 16; o > 0; o >>= 1) qm = max(qm, __shfl_down_sync(0xffffffffu, qm, o));
+        if ((threadIdx.x & 31) == 0 && qm) atomicMax(qmax, qm);
     }
 }
 
@@ -288,7 +294,9 @@ void launch_reorder_f64(const GridP &g, const PartF64 &p, const PartF64 &out, Co
                         long long capacity, int *err, cudaStream_t s, Tiles64 *tiles)
 {
     cudaMemsetAsync(&cnt->np, 0, sizeof(long long), s);
-    k_keys_f64<<<stream_grid(capacity), kThreads, 0, s>>>(g, p, &cnt->used, sc.key[0], &cnt->np, err);
+    if (tiles) cudaMemsetAsync(tiles->qmax, 0, sizeof(unsigned long long), s);
+    k_keys_f64<<<stream_grid(capacity), kThreads, 0, s>>>(g, p, &cnt->used, sc.key[0], &cnt->np, err,
+                                                          tiles ? tiles->qmax : nullptr);
     count_launches(1);
     const size_t ntiles = sort_tiles(capacity);
     const int r = radix_sort(sc, &cnt->used, key_bits(g.ncell), ntiles, s);
