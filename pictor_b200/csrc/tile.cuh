@@ -139,10 +139,19 @@ __device__ __forceinline__ void red_shared_i(uint32_t a, int v)
 {
     asm volatile("red.shared.add.s32 [%0+%1], %2;" ::"r"(a), "n"(OFF), "r"(v));
 }
+// q added to the 64-bit shared word at a + OFF with two native 32-bit
+// atomics: the low halves (the old value comes back), then the high halves
+// with the carry out of the low word.  Every add's carry is counted once, so
+// the word holds the exact sum of everything added (mod 2^64) once the adds
+// are done; a 64-bit add on shared memory is not a single native atomic.
 template <int OFF>
-__device__ __forceinline__ void red_shared_l(uint32_t a, long long v)
+__device__ __forceinline__ void red_shared_l(uint32_t a, long long q)
 {
-    asm volatile("red.shared.add.u64 [%0+%1], %2;" ::"r"(a), "n"(OFF), "l"(v));
+    const unsigned lo = (unsigned)(unsigned long long)q, hi = (unsigned)((unsigned long long)q >> 32);
+    unsigned old;
+    asm volatile("atom.shared.add.u32 %0, [%1+%2], %3;" : "=r"(old) : "r"(a), "n"(OFF), "r"(lo) : "memory");
+    const unsigned h = hi + (old + lo < old ? 1u : 0u);
+    if (h) asm volatile("red.shared.add.u32 [%0+%1], %2;" ::"r"(a), "n"(OFF + 4), "r"(h) : "memory");
 }
 
 // Shared byte offsets of the current box: component planes and the y / z
