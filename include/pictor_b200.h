@@ -289,6 +289,22 @@ int pic_step_persistent(pic_handle *const *hs, int32_t n, int32_t nsteps, uint32
    filter; returns PIC_ERR_INVALID otherwise. */
 int pic_step_batched(pic_handle *const *hs, int32_t n, int32_t nsteps);
 
+/* The initial electrostatic field, FP64 on the device (no counterpart in the
+   reference, whose setups start from a neutral plasma with E = 0 or set the
+   fields themselves; north_star keeps this solve in FP64 for the FP32 form
+   too).  The particles' CIC charge density rho at the nodes (the rho of the
+   Gauss residual of pic_diagnostics) minus its mean (returned in *rho_mean,
+   a uniform neutralising background on the periodic grid) is the right-hand
+   side of -L phi = rho - mean, L the periodic 7-point (2D: 5-point) Laplacian
+   of the interior nodes, solved by conjugate gradients to a relative residual
+   of `tol` in at most max_iter iterations; E is replaced by -grad(phi)
+   (Ex(i) = phi(i) - phi(i+1) at i + 1/2, ghosts as periodic images, Ez = 0
+   in 2D), whose node divergence (CalcDivE, savedata_routines.F90:310-348) is
+   rho - mean; B is left as it is.  *iters and *rel_residual report the
+   solve.  Cartesian single domain, FP64 or FP32 fields.  PIC_ERR_TIMEOUT when
+   max_iter runs out before tol (E then holds the last iterate). */
+int pic_solve_gauss(pic_handle *h, double tol, int32_t max_iter, int32_t *iters, double *rel_residual,
+                    double *rho_mean);
 /* Diagnostics (savedata_routines.F90:265-348), FP64 accumulation on device:
    out[0] = sum |B|^2, out[1] = sum |E|^2 over the interior (CalcFldEnergy),
    out[2] = max |divE - rho| over interior nodes, out[3] = max |rho_+|,

@@ -1895,6 +1895,27 @@ int pic_diagnostics(pic_handle *h, double masse, double *out, int32_t nout)
     return r;
 }
 
+int pic_solve_gauss(pic_handle *h, double tol, int32_t max_iter, int32_t *iters, double *rel_residual,
+                    double *rho_mean)
+{
+    if (!h || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || !(tol > 0.0) || max_iter < 1) return PIC_ERR_INVALID;
+    const GridP &g = h->g;
+    if (!h->rho) {
+        int r;
+        if ((r = dalloc(h, &h->rho, (size_t)g.ncell)) || (r = dalloc(h, &h->rho_pos, (size_t)g.ncell))) return r;
+    }
+    if (h->fp32) launch_rho_f32(g, h->p32[h->cur], h->cnt, h->rho, h->rho_pos, h->s);
+    else launch_rho_f64(g, h->p64[h->cur], h->cnt, h->rho, h->rho_pos, h->s);
+    int it = 0;
+    double rr = 0.0, mean = 0.0;
+    const int rc = solve_gauss(g, h->E, h->fp32, h->rho, tol, max_iter, h->s, &it, &rr, &mean);
+    if (iters) *iters = it;
+    if (rel_residual) *rel_residual = rr;
+    if (rho_mean) *rho_mean = mean;
+    if (rc != PIC_OK) return rc;
+    return finish(h);
+}
+
 int pic_profile(pic_handle *h, int32_t enable)
 {
     if (!h) return PIC_ERR_INVALID;

@@ -237,6 +237,23 @@ __global__ void __launch_bounds__(kDiagThreads) k_gauss_max(GridP g, const T *__
     }
 }
 
+// The CIC charge density alone (the initial Gauss solve, poisson.cu).
+void launch_rho_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *rho, double *rho_pos, cudaStream_t s)
+{
+    cudaMemsetAsync(rho, 0, (size_t)g.ncell * sizeof(double), s);
+    cudaMemsetAsync(rho_pos, 0, (size_t)g.ncell * sizeof(double), s);
+    k_rho_f64<<<kSMs * 8, 256, 0, s>>>(g, p, cnt, rho, rho_pos);
+    count_launches(1);
+}
+
+void launch_rho_f32(const GridP &g, const PartF32 &p, const Counters *cnt, double *rho, double *rho_pos, cudaStream_t s)
+{
+    cudaMemsetAsync(rho, 0, (size_t)g.ncell * sizeof(double), s);
+    cudaMemsetAsync(rho_pos, 0, (size_t)g.ncell * sizeof(double), s);
+    k_rho_f32<<<kSMs * 8, 256, 0, s>>>(g, p, cnt, rho, rho_pos);
+    count_launches(1);
+}
+
 void launch_gauss_f64(const GridP &g, const PartF64 &p, const Counters *cnt, const double *const E[3], double *rho,
                       double *rho_pos, double *out2, cudaStream_t s)
 {

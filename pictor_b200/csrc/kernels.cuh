@@ -255,6 +255,12 @@ void launch_particle_energy_f64(const GridP &g, const PartF64 &p, const Counters
                                 cudaStream_t s);
 void launch_particle_energy_f32(const GridP &g, const PartF32 &p, const Counters *cnt, double masse, double *out,
                                 cudaStream_t s);
+void launch_rho_f64(const GridP &g, const PartF64 &p, const Counters *cnt, double *rho, double *rho_pos, cudaStream_t s);
+void launch_rho_f32(const GridP &g, const PartF32 &p, const Counters *cnt, double *rho, double *rho_pos, cudaStream_t s);
+// poisson.cu: E = -grad(phi) with the node divergence equal to rho minus its
+// mean (FP64 conjugate gradients); returns a PIC status
+int solve_gauss(const GridP &g, void *const E[3], bool fp32, const double *rho, double tol, int max_iter,
+                cudaStream_t s, int *iters, double *rel_res, double *rho_mean);
 void launch_gauss_f64(const GridP &g, const PartF64 &p, const Counters *cnt, const double *const E[3], double *rho,
                       double *rho_pos, double *out2, cudaStream_t s);
 void launch_gauss_f32(const GridP &g, const PartF32 &p, const Counters *cnt, const float *const E[3], double *rho,

@@ -319,6 +319,16 @@ class Simulation:
         return {"B2": out[0], "E2": out[1], "Benergy": 0.5 * out[0], "Eenergy": 0.5 * out[1],
                 "gauss_linf": out[2], "rho_max": out[3], "kinetic": out[4:].copy()}
 
+    def solve_gauss(self, tol: float = 1e-12, max_iter: int = 20000) -> dict:
+        """The initial electrostatic field (pic_solve_gauss): E = -grad(phi)
+        with the Gauss residual's node divergence equal to the particles' CIC
+        density minus its mean; FP64 conjugate gradients on the device."""
+        it = C.c_int32()
+        rr, mean = C.c_double(), C.c_double()
+        check(self.L.pic_solve_gauss(self.h, float(tol), int(max_iter), C.byref(it), C.byref(rr), C.byref(mean)),
+              "pic_solve_gauss")
+        return {"iters": it.value, "rel_residual": rr.value, "rho_mean": mean.value}
+
     def profile(self, enable: bool = True) -> None:
         check(self.L.pic_profile(self.h, 1 if enable else 0), "pic_profile")
 

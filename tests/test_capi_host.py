@@ -129,3 +129,4 @@ def test_slab_and_wall_entry_points_validate_without_gpu():
     assert L.pic_bc_attenuate_flow(None, 2, 30.0, 1.0, 4.0, three, three) == -1
     assert L.pic_bc_open_x(None, 1, 1.5) == -1
     assert L.pic_bc_open_prtl_x(None, 1, 1.5) == -1
+    assert L.pic_solve_gauss(None, 1e-12, 100, None, None, None) == -1
