@@ -40,8 +40,7 @@ WORKLOADS = {
     # a small case of the headline physics for profiler captures (particles 270 MB > L2)
     "weibel3d_fp32_small": dict(dims=3, nx=128, ny=64, nz=64, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
                                 precision="fp32", horizon=200),
-    # the same small case in the FP64 reference layout with the tiled FP64 mover forced on (by default
-    # the tiles start where the current arrays exceed 48 MB)
+    # the same small case in the FP64 reference layout (the tiled FP64 mover)
     "weibel3d_fp64_small": dict(dims=3, nx=128, ny=64, nz=64, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
                                 precision="fp64", fp64_tiles=1),
     # the batched ensemble: 64 independent 2D Weibel runs, grid 64^2..512^2, 4..32 particles per cell per
@@ -222,14 +221,10 @@ def sum_over_ranks(ws, value: float) -> float:
 
 def mover_kernel(wl: dict, precision: str) -> str:
     """The mover kernel of the timed steps (after a reorder): the FP32 tiled
-    mover, or the FP64 one by tiles where its current arrays exceed 48 MB
-    (or tiles are forced), else the FP64 mover per particle."""
+    mover, or the FP64 one by tiles unless tiles are switched off."""
     if precision == "fp32":
         return "k_move_f32_tiled"
-    mz = wl["nz"] + 5 if wl["dims"] == 3 else 1
-    ncell = (wl["nx"] + 5) * (wl["ny"] + 5) * mz
-    t = wl.get("fp64_tiles", 0)
-    return "k_move_f64_tiled" if t > 0 or (t == 0 and 24.0 * ncell > 48 * 1024 * 1024) else "k_move_f64"
+    return "k_move_f64" if wl.get("fp64_tiles", 0) < 0 else "k_move_f64_tiled"
 
 
 def make_sim(wl: dict, precision: str, extra_capacity: float = 1.04):

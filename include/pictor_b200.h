@@ -95,11 +95,10 @@ typedef struct {
        sort of two records per particle each step.  0 = FP64 atomics into J
        (the sums differ from the serial build's in the last bits). */
     int32_t exact_current;
-    /* FP64 Cartesian form after a reorder: 0 = the mover by tiles of cells
-       (node and current boxes in shared memory) when the grid's current
-       arrays are larger than L2, else one thread per particle with global
-       atomics; 1 = always by tiles; -1 = never.  Positions and momenta are
-       the same either way; the current differs in the order of its sums. */
+    /* FP64 Cartesian form after a reorder: 0 or 1 = the mover by tiles of
+       cells (node and current boxes in shared memory); -1 = one thread per
+       particle with global atomics.  Positions and momenta are the same
+       either way; the current differs in the order of its sums. */
     int32_t fp64_tiles;
     /* FP32 Cartesian form, 3D: 1 = each zigzag segment's current is its
        exact line integral of the bilinear weights (the cross term q dx dy dz

@@ -65,7 +65,6 @@ void launch_move_deposit_f64(const GridP &g, const PartF64 &p, const Counters *c
 // particles the cell-order reorder leaves in H slot ranges.
 constexpr int kTile64SmemBytes = 110 * 1024;   // node box + FP64 current box of one tile (2 CTAs per SM)
 constexpr int kTile64MaxRows = 8;
-constexpr double kTile64MinCurrentBytes = 48.0 * 1024 * 1024;   // the tiles for J (3 FP64 arrays) above this
 struct Tiles64 {
     uint32_t *range;              // 2 H per tile: first and past-the-end slot of each row segment
     int *box;                     // 8 per tile: lo[3], hi[3] of the cells its particles occupy (1-based)

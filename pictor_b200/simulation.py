@@ -56,7 +56,7 @@ class PicConfig:
     cyl_modes: int = 0         # cylindrical: 0 = theta-gridded field solve, 2 = modes m = 0, 1
     slab_x: int = 0            # 1 = one slab of a domain split along x (pictor_b200.slab)
     exact_current: int = 0     # FP64: 1 = current summed in the reference's serial order (bit-exact J)
-    fp64_tiles: int = 0        # FP64 mover: 0 = tiles when J exceeds L2, 1 = always, -1 = never
+    fp64_tiles: int = 0        # FP64 mover after a reorder: 0 or 1 = by tiles, -1 = per particle
     exact_charge: int = 0      # FP32 3D: 1 = exactly charge-conserving deposit, 0 = the reference's weights
 
     def to_struct(self) -> _capi.Config:
