@@ -210,6 +210,37 @@ int pic_bc_open_x(pic_handle *h, int32_t side, double pos);
    the serial sum in the last bit.  PIC_ERR_OVERFLOW (nothing appended) when
    the copies do not fit in the capacity. */
 int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos);
+/* Particle injection at a face of type 'iflw' (SetBC_InflowPrtl, bc.F90:67-153):
+   InjectNewPrtl (bc_inflow.F90:134-256) with 'rndm' placement, called where
+   EnforceBC_PostMovDep calls InflowBC_Prtl (bc.F90:240, after
+   pic_move_deposit).  The trial region is SetInjDomain's: along the face's
+   axis from pos - speed c (or pos - vmax c) to pos + vmax c (or pos + speed
+   c), clipped to the grid, the full interior across; epc times its volume
+   trials (a Poisson draw of that mean below 1000), each at a uniform random
+   position, accepted with probability `density` and only in the layer the
+   flow emptied in one step (beyond pos + drift c on the face's side); each
+   accepted position gets one particle per species (flv, charge, a
+   Maxwellian of temperature temp boosted by the drift: GetVelGamma_MaxBolt
+   and AddDriftVel, prob_dist.F90:13-30, 223-254), appended in trial order.
+   The setup's density and drift functions are uniform here; the random
+   numbers are Philox-4x32-10 keyed by seed, with `call` distinct per call
+   (the step).  FP64 Cartesian single domain; PIC_ERR_OVERFLOW (nothing
+   appended) past the capacity. */
+typedef struct pic_inflow {
+    int32_t face;          /* bc_face index 1..6 (2D: 1..4) */
+    double pos;            /* bc_face(face)%pos_prtl, cells from the first interior cell */
+    double speed;          /* bc_face(face)%speed (InjSpeed), a fraction of c per step */
+    double vmax;           /* the flow's DriftVmax (SetBC_InflowFld default 1) */
+    double epc;            /* trials per cell of unit density */
+    double density;        /* Den, in [0, 1] */
+    double drift[3];       /* DriftVelocity, in units of c */
+    int32_t nspecies;      /* phase-space properties injected at each position, 1..4 */
+    int32_t flv[4];
+    double temp[4];        /* Temperature of each */
+    double charge[4];      /* FlvrCharge(flv) * fraction of each */
+    uint32_t seed, call;
+} pic_inflow;
+int pic_bc_inflow(pic_handle *h, const pic_inflow *inj);
 
 /* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
    with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:

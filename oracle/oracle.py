@@ -68,6 +68,15 @@ class _Fields(C.Structure):
     _fields_ = [(n, C.POINTER(C.c_double)) for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Jy", "Jz")]
 
 
+class Inflow(C.Structure):
+    _fields_ = [
+        ("face", C.c_int32), ("pos", C.c_double), ("speed", C.c_double), ("vmax", C.c_double),
+        ("epc", C.c_double), ("density", C.c_double), ("drift", C.c_double * 3), ("nspecies", C.c_int32),
+        ("flv", C.c_int32 * 4), ("temp", C.c_double * 4), ("charge", C.c_double * 4), ("seed", C.c_uint32),
+        ("call", C.c_uint32),
+    ]
+
+
 class _Weibel(C.Structure):
     _fields_ = [
         ("dims", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
@@ -107,6 +116,8 @@ def _declare(L: C.CDLL) -> None:
         getattr(L, fn).argtypes = [P(Grid), P(_Fields), C.c_double]
     L.orc_open_prtl.argtypes = [P(Grid), P(_Particles), C.c_int, C.c_double, C.c_double]
     L.orc_open_prtl.restype = C.c_int
+    L.orc_inject.argtypes = [P(Grid), P(_Particles), P(Inflow)]
+    L.orc_inject.restype = C.c_int64
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -333,6 +344,20 @@ class Oracle:
         fs = self.f.struct()
         fn = self.L.orc_open_fld_left if side == 0 else self.L.orc_open_fld_right
         fn(C.byref(self.g), C.byref(fs), float(pos))
+
+    def inject(self, face: int, pos: float, species, epc: float, density: float = 1.0, drift=(0.0, 0.0, 0.0),
+               speed: float = 0.0, vmax: float = 1.0, seed: int = 1, call: int = 0) -> int:
+        """InjectNewPrtl at face 1..6; species = [(flv, temperature, charge)]."""
+        f = Inflow()
+        f.face, f.pos, f.speed, f.vmax, f.epc, f.density = int(face), float(pos), float(speed), float(vmax), \
+            float(epc), float(density)
+        for d in range(3):
+            f.drift[d] = float(drift[d])
+        f.nspecies = len(species)
+        for k, (fl, tp, q) in enumerate(species):
+            f.flv[k], f.temp[k], f.charge[k] = int(fl), float(tp), float(q)
+        f.seed, f.call = int(seed) & 0xFFFFFFFF, int(call) & 0xFFFFFFFF
+        return self._call_p(self.L.orc_inject, C.byref(f))
 
     def open_prtl_x(self, side: int, pos: float, dx: float = 1.0) -> int:
         """OpenBC_Prtl_Left (side 0) / OpenBC_Prtl_Right (side 1) at pos."""

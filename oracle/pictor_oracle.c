@@ -1458,3 +1458,92 @@ int64_t orc_load_weibel(const orc_weibel *wb, orc_particles *p)
     }
     return p->used;
 }
+
+/* InjectNewPrtl (bc_inflow.F90:134-189) with SetInjDomain (:191-235),
+   GetIntPoissonDist (prob_dist.F90:194-216), GetNewPrtlPos
+   (bc_inflow.F90:237-256) and InsertPrtl_PSP (init_prtl.F90:138-169) on one
+   rank, for a uniform density and drift; the draws are Philox-4x32-10
+   (counter trial, call, stream; key seed, "INJC"; the Poisson draw at trial
+   0xFFFFFFFF).  Returns the particles appended, or -1 (none appended) past
+   the capacity. */
+int64_t orc_inject(const orc_grid *g, orc_particles *p, const orc_inflow *f)
+{
+    enum { NT = 10000 };
+    static double X[NT], P[NT];
+    orc_maxbolt_table(NT, X, P);
+    const uint32_t key[2] = {f->seed, 0x494E4A43u};
+    double x1 = 3.0, x2 = g->mx - 2, y1 = 3.0, y2 = g->my - 2;
+    double z1 = g->dims == 3 ? 3.0 : 1.0, z2 = g->dims == 3 ? g->mz - 2 : 2.0;
+    const double pos = f->pos, vc = f->vmax * g->c, shift = f->speed * g->c;
+    const int side = f->face;
+    if (side == 1) { x1 = fmax(pos - shift, 0.0) - 0.0 + 3; x2 = fmin(pos + vc, (double)g->nx) - 0.0 + 3; }
+    if (side == 2) { x1 = fmax(pos - vc, 0.0) - 0.0 + 3; x2 = fmin(pos + shift, (double)g->nx) - 0.0 + 3; }
+    if (side == 3) { y1 = fmax(pos - shift, 0.0) - 0.0 + 3; y2 = fmin(pos + vc, (double)g->ny) - 0.0 + 3; }
+    if (side == 4) { y1 = fmax(pos - vc, 0.0) - 0.0 + 3; y2 = fmin(pos + shift, (double)g->ny) - 0.0 + 3; }
+    if (side == 5) { z1 = fmax(pos - shift, 0.0) - 0.0 + 3; z2 = fmin(pos + vc, (double)g->nz) - 0.0 + 3; }
+    if (side == 6) { z1 = fmax(pos - vc, 0.0) - 0.0 + 3; z2 = fmin(pos + shift, (double)g->nz) - 0.0 + 3; }
+    int64_t n = (int64_t)(f->epc * fmax(0.0, x2 - x1) * fmax(0.0, y2 - y1) * fmax(0.0, z2 - z1));
+    if (n <= 0) return 0;
+    if (n < 1000) {
+        uint32_t r[4], ctr[4] = {0xFFFFFFFFu, f->call, 0, 0};
+        orc_philox4x32_10(ctr, key, r);
+        const double r1 = orc_u01(r[0], r[1]);
+        const double mean = (double)n;
+        double sum = exp(-mean), sum_logn = 0;
+        const double log_mean = log(mean);
+        int64_t k = 0;
+        while (sum < r1) {
+            k = k + 1;
+            sum_logn = sum_logn + log((double)k);
+            sum = sum + exp(-mean + (double)k * log_mean - sum_logn);
+            if (k > 10000) break;
+        }
+        n = k;
+    }
+    const int64_t used0 = p->used;
+    for (int64_t t = 0; t < n; t++) {
+        uint32_t r[4], ctr[4] = {(uint32_t)t, f->call, 0, 0};
+        orc_philox4x32_10(ctr, key, r);
+        const double r1 = orc_u01(r[0], r[1]), r2 = orc_u01(r[2], r[3]);
+        ctr[2] = 1;
+        orc_philox4x32_10(ctr, key, r);
+        const double r3 = orc_u01(r[0], r[1]), racpt = orc_u01(r[2], r[3]);
+        const double xl = x1 + r1 * (x2 - x1), yl = y1 + r2 * (y2 - y1), zl = z1 + r3 * (z2 - z1);
+        const double xg = xl + (0.0 - 3.0), yg = yl + (0.0 - 3.0), zg = g->dims == 3 ? zl + (0.0 - 3.0) : zl;
+        int acpt = racpt <= f->density;
+        if (side == 1 && xg > pos + f->drift[0] * g->c) acpt = 0;
+        if (side == 2 && xg < pos + f->drift[0] * g->c) acpt = 0;
+        if (side == 3 && yg > pos + f->drift[1] * g->c) acpt = 0;
+        if (side == 4 && yg < pos + f->drift[1] * g->c) acpt = 0;
+        if (side == 5 && zg > pos + f->drift[2] * g->c) acpt = 0;
+        if (side == 6 && zg < pos + f->drift[2] * g->c) acpt = 0;
+        if (!acpt) continue;
+        for (int sp = 0; sp < f->nspecies; sp++) {
+            ctr[2] = 2 + 2 * sp;
+            orc_philox4x32_10(ctr, key, r);
+            const double rmb = orc_u01(r[0], r[1]), riso2 = orc_u01(r[2], r[3]);
+            ctr[2] = 3 + 2 * sp;
+            orc_philox4x32_10(ctr, key, r);
+            const double riso3 = orc_u01(r[0], r[1]);
+            const int idx = binary_search(NT, P, rmb);
+            double beta = inv_pdf(X, P, rmb, idx);
+            beta = sqrt(beta * f->temp[sp]);
+            if (beta >= 1.0) beta = 0.0;
+            const double gamma = 1.0 / sqrt((1.0 + beta) * (1.0 - beta));
+            const double ct = 2.0 * riso2 - 1.0;
+            const double st = sqrt(1.0 - ct * ct);
+            const double phi = (2.0 * PI_PSN) * riso3;
+            double u = (gamma * beta) * ct;
+            double v = ((gamma * beta) * st) * cos(phi);
+            double w = ((gamma * beta) * st) * sin(phi);
+            add_drift_vel(&u, &v, &w, f->drift[0], f->drift[1], f->drift[2]);
+            if (p->used >= p->capacity) { p->used = used0; return -1; }
+            const int64_t d = p->used++;
+            p->x[d] = xl; p->y[d] = yl; p->z[d] = zl;
+            p->u[d] = u; p->v[d] = v; p->w[d] = w;
+            p->q[d] = f->charge[sp];
+            p->flv[d] = f->flv[sp];
+        }
+    }
+    return p->used - used0;
+}

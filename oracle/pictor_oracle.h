@@ -112,6 +112,15 @@ void orc_open_fld_right(const orc_grid *g, orc_fields *f, double pos);
 void orc_open_fld_left(const orc_grid *g, orc_fields *f, double pos);
 /* OpenBC_Prtl_Left (side 0) / Right (side 1), bc.F90:478-621, layer width dx. */
 int orc_open_prtl(const orc_grid *g, orc_particles *p, int side, double pos, double dx);
+/* InjectNewPrtl (bc_inflow.F90:134-256) for a uniform density and drift. */
+typedef struct {
+    int32_t face;
+    double pos, speed, vmax, epc, density, drift[3];
+    int32_t nspecies, flv[4];
+    double temp[4], charge[4];
+    uint32_t seed, call;
+} orc_inflow;
+int64_t orc_inject(const orc_grid *g, orc_particles *p, const orc_inflow *f);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

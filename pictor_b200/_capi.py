@@ -49,6 +49,16 @@ class Config(C.Structure):
     ]
 
 
+class Inflow(C.Structure):
+    """pic_inflow (include/pictor_b200.h)."""
+    _fields_ = [
+        ("face", C.c_int32), ("pos", C.c_double), ("speed", C.c_double), ("vmax", C.c_double),
+        ("epc", C.c_double), ("density", C.c_double), ("drift", C.c_double * 3), ("nspecies", C.c_int32),
+        ("flv", C.c_int32 * 4), ("temp", C.c_double * 4), ("charge", C.c_double * 4), ("seed", C.c_uint32),
+        ("call", C.c_uint32),
+    ]
+
+
 _LIB = None
 
 
@@ -114,6 +124,7 @@ SIGNATURES = {
     "pic_bc_open_x": (C.c_int, [H, C.c_int32, C.c_double]),
     "pic_bc_open_prtl_x": (C.c_int, [H, C.c_int32, C.c_double]),
     "pic_solve_gauss": (C.c_int, [H, C.c_double, C.c_int32, C.POINTER(C.c_int32), PD, PD]),
+    "pic_bc_inflow": (C.c_int, [H, C.POINTER(Inflow)]),
     "pic_slab_pack_fields": (C.c_int, [H, C.c_int32, C.c_void_p, C.c_void_p]),
     "pic_slab_unpack_fields": (C.c_int, [H, C.c_int32, C.c_void_p, C.c_void_p]),
     "pic_slab_pack_particles": (C.c_int, [H, C.c_void_p, C.c_int64, PI64, PI64]),

@@ -1587,6 +1587,99 @@ int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos)
     return finish_phase(h);
 }
 
+// Philox-4x32-10 on the host (the draw of the injection's Poisson count).
+static void host_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3], k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; r++) {
+        const uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+        const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0, n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        c0 = n0;
+        c1 = (uint32_t)p1;
+        c2 = n2;
+        c3 = (uint32_t)p0;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0;
+    out[1] = c1;
+    out[2] = c2;
+    out[3] = c3;
+}
+
+int pic_bc_inflow(pic_handle *h, const pic_inflow *inj)
+{
+    if (!h || !inj || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external) return PIC_ERR_INVALID;
+    const GridP &g = h->g;
+    const int side = inj->face;
+    if (side < 1 || side > (g.dims == 3 ? 6 : 4) || inj->nspecies < 1 || inj->nspecies > 4 || !(inj->epc > 0.0) ||
+        !(inj->density >= 0.0) || !(inj->vmax >= 0.0) || !(inj->speed >= 0.0))
+        return PIC_ERR_INVALID;
+    for (int sp = 0; sp < inj->nspecies; sp++)
+        if (inj->flv[sp] < 1 || inj->flv[sp] > h->cfg.nflvr || !(inj->temp[sp] >= 0.0)) return PIC_ERR_INVALID;
+    // SetInjDomain (bc_inflow.F90:191-235) on one rank: the borders of the
+    // rank are 0 and n, local = global - 0 + 3; the other axes span
+    // xmin..xmax (subdomains.F90:52-66)
+    InflowParams f;
+    f.x1 = 3.0;
+    f.x2 = g.mx - 2;
+    f.y1 = 3.0;
+    f.y2 = g.my - 2;
+    f.z1 = g.dims == 3 ? 3.0 : 1.0;
+    f.z2 = g.dims == 3 ? (double)(g.mz - 2) : 2.0;
+    const double pos = inj->pos, vc = inj->vmax * g.c, shift = inj->speed * g.c;
+    const double n3[3] = {(double)g.nx, (double)g.ny, (double)g.nz};
+    double *lo[3] = {&f.x1, &f.y1, &f.z1}, *hi[3] = {&f.x2, &f.y2, &f.z2};
+    const int ax = (side - 1) / 2;
+    if (side % 2 == 1) {
+        *lo[ax] = fmax(pos - shift, 0.0) - 0.0 + 3;
+        *hi[ax] = fmin(pos + vc, n3[ax]) - 0.0 + 3;
+    } else {
+        *lo[ax] = fmax(pos - vc, 0.0) - 0.0 + 3;
+        *hi[ax] = fmin(pos + shift, n3[ax]) - 0.0 + 3;
+    }
+    long long n = (long long)(inj->epc * fmax(0.0, f.x2 - f.x1) * fmax(0.0, f.y2 - f.y1) * fmax(0.0, f.z2 - f.z1));
+    if (n <= 0) return PIC_OK;
+    if (n < 1000) {
+        // GetIntPoissonDist (prob_dist.F90:194-216) with mean n
+        const uint32_t ctr[4] = {0xFFFFFFFFu, inj->call, 0u, 0u}, key[2] = {inj->seed, 0x494E4A43u};
+        uint32_t r[4];
+        host_philox(ctr, key, r);
+        const double r1 = (double)((((uint64_t)r[0] << 32) | r[1]) >> 11) * (1.0 / 9007199254740992.0);
+        const double mean = (double)n;
+        double sum = exp(-mean), sum_logn = 0.0;
+        const double log_mean = log(mean);
+        long long k = 0;
+        while (sum < r1) {
+            k = k + 1;
+            sum_logn = sum_logn + log((double)k);
+            sum = sum + exp(-mean + (double)k * log_mean - sum_logn);
+            if (k > 10000) break;
+        }
+        n = k;
+        if (n == 0) return PIC_OK;
+    }
+    if (n >= (1ll << 31)) return PIC_ERR_INVALID;
+    f.density = inj->density;
+    for (int d = 0; d < 3; d++) f.drift[d] = inj->drift[d];
+    f.c = g.c;
+    f.pos = pos;
+    f.side = side;
+    f.dims = g.dims;
+    f.nsp = inj->nspecies;
+    for (int sp = 0; sp < 4; sp++) {
+        f.flv[sp] = sp < inj->nspecies ? inj->flv[sp] : 0;
+        f.temp[sp] = sp < inj->nspecies ? inj->temp[sp] : 0.0;
+        f.charge[sp] = sp < inj->nspecies ? inj->charge[sp] : 0.0;
+    }
+    f.seed = inj->seed;
+    f.call = inj->call;
+    f.ntrial = n;
+    int r = launch_inflow(g, f, h->tab_x, h->tab_p, h->ntab, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s);
+    if (r) return r;
+    return finish_phase(h);
+}
+
 int pic_set_sync(pic_handle *h, int32_t sync)
 {
     if (!h) return PIC_ERR_INVALID;

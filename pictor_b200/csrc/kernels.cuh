@@ -244,6 +244,20 @@ int weibel_with_signs(pic_handle *h, double epc, double density, double drift, d
 int launch_weibel(const GridP &g, const WeibelParams &w, const double *table_x, const double *table_p, int ntable,
                   const PartF64 *p64, const PartF32 *p32, Counters *cnt, SortScratch &sc, long long capacity,
                   int *err, cudaStream_t s);
+// Particle injection at an 'iflw' face (InjectNewPrtl, bc_inflow.F90:134-256):
+// the trial region (local coordinates), the trial count, a uniform density
+// and drift, up to four species per accepted position.
+struct InflowParams {
+    double x1, x2, y1, y2, z1, z2;
+    double density, drift[3], c, pos;
+    int side, dims, nsp;
+    int flv[4];
+    double temp[4], charge[4];
+    uint32_t seed, call;
+    long long ntrial;
+};
+int launch_inflow(const GridP &g, const InflowParams &f, const double *X, const double *P, int nt, PartF64 &p,
+                  Counters *cnt, SortScratch &sc, long long capacity, int *err, cudaStream_t s);
 void scan_exclusive_u32(const uint32_t *in, uint32_t *out, size_t n, uint32_t *tmp, uint32_t *total, cudaStream_t s);
 
 // diag.cu

@@ -775,7 +775,8 @@ __device__ int bsearch_table(int n, const double *A, double val)
 }
 
 __device__ void maxwell_momentum(const double *X, const double *P, int nt, double temp, double rmb, double riso2,
-                                 double riso3, double drift_x, double &u, double &v, double &w)
+                                 double riso3, double drift_x, double drift_y, double drift_z, double &u, double &v,
+                                 double &w)
 {
     // GetVelGamma_MaxBolt (prob_dist.F90:13-30) + InvPDF (:72-83)
     const int idx = bsearch_table(nt, P, rmb);
@@ -791,9 +792,9 @@ __device__ void maxwell_momentum(const double *X, const double *P, int nt, doubl
     u = (gamma * beta) * ct;
     v = ((gamma * beta) * st) * cos(phi);
     w = ((gamma * beta) * st) * sin(phi);
-    // AddDriftVel (:223-254) with the drift along x
-    const double vx = drift_x;
-    const double dr = sqrt((vx * vx + 0.0 * 0.0) + 0.0 * 0.0);
+    // AddDriftVel (:223-254)
+    const double vx = drift_x, vy = drift_y, vz = drift_z;
+    const double dr = sqrt((vx * vx + vy * vy) + vz * vz);
     double db, dg;
     if (fabs(dr) < 1.0) {
         db = dr;
@@ -802,7 +803,7 @@ __device__ void maxwell_momentum(const double *X, const double *P, int nt, doubl
         dg = fabs(dr);
         db = sqrt((dr - 1.0) * (dr + 1.0)) / dr;
     }
-    double d0 = vx, d1 = 0.0, d2 = 0.0;
+    double d0 = vx, d1 = vy, d2 = vz;
     const double mag = sqrt((d0 * d0 + d1 * d1) + d2 * d2);
     if (mag == 0) {
         d0 = d1 = d2 = 0;
@@ -880,7 +881,7 @@ __global__ void __launch_bounds__(256) k_weibel_fill(GridP g, WeibelParams w, co
                 const double riso3 = u01(rr[0], rr[1]);
                 const double sgn = ((call == 0) == (sp == 0)) ? -1.0 : 1.0;
                 double u, v, ww;
-                maxwell_momentum(X, P, nt, w.temp[sp], rmb, riso2, riso3, sgn * w.drift, u, v, ww);
+                maxwell_momentum(X, P, nt, w.temp[sp], rmb, riso2, riso3, sgn * w.drift, 0.0, 0.0, u, v, ww);
                 const long long o = slot + sp;
                 const double q = (1.0 * (sp == 0 ? 1.0 : -1.0)) * 1.0;
                 if (!use32) {
@@ -937,6 +938,148 @@ int launch_weibel(const GridP &g, const WeibelParams &w, const double *X, const 
     count_launches(1);
     k_weibel_finish<<<1, 1, 0, s>>>(cnt, total, capacity);
     count_launches(1);
+    return PIC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Particle injection at an 'iflw' face: InjectNewPrtl (bc_inflow.F90:134-189)
+// with GetNewPrtlPos (:237-256) and InsertPrtl_PSP (init_prtl.F90:138-169)
+// for a uniform density and drift.  Trial n of call k draws from Philox
+// (counter n, k, stream; key seed, "INJC"): streams 0, 1 the position and the
+// acceptance, 2 + 2 sp and 3 + 2 sp the Maxwellian momentum of species sp.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void inflow_draw(const InflowParams &f, uint32_t n, uint32_t stream, double &a, double &b)
+{
+    uint32_t r[4];
+    philox4x32_10(n, f.call, stream, 0, f.seed, 0x494E4A43u, r);
+    a = u01(r[0], r[1]);
+    b = u01(r[2], r[3]);
+}
+
+// The position of trial n (local coordinates) and whether it is accepted:
+// the density, and only the layer the flow emptied in one step
+// (bc_inflow.F90:165-178).
+__device__ __forceinline__ bool inflow_trial(const InflowParams &f, uint32_t n, double &xl, double &yl, double &zl)
+{
+    double r1, r2, r3, racpt;
+    inflow_draw(f, n, 0, r1, r2);
+    inflow_draw(f, n, 1, r3, racpt);
+    xl = f.x1 + r1 * (f.x2 - f.x1);
+    yl = f.y1 + r2 * (f.y2 - f.y1);
+    zl = f.z1 + r3 * (f.z2 - f.z1);
+    const double xg = xl + (0.0 - 3.0), yg = yl + (0.0 - 3.0), zg = f.dims == 3 ? zl + (0.0 - 3.0) : zl;
+    bool acpt = racpt <= f.density;
+    switch (f.side) {
+        case 1: if (xg > f.pos + f.drift[0] * f.c) acpt = false; break;
+        case 2: if (xg < f.pos + f.drift[0] * f.c) acpt = false; break;
+        case 3: if (yg > f.pos + f.drift[1] * f.c) acpt = false; break;
+        case 4: if (yg < f.pos + f.drift[1] * f.c) acpt = false; break;
+        case 5: if (zg > f.pos + f.drift[2] * f.c) acpt = false; break;
+        default: if (zg < f.pos + f.drift[2] * f.c) acpt = false; break;
+    }
+    return acpt;
+}
+
+__global__ void __launch_bounds__(256) k_inflow_count(InflowParams f, uint32_t *counts)
+{
+    __shared__ uint32_t c;
+    if (threadIdx.x == 0) c = 0;
+    __syncthreads();
+    const long long base = (long long)blockIdx.x * kTile;
+    uint32_t mine = 0;
+    for (int r = 0; r < kTile / 256; r++) {
+        const long long t = base + r * 256 + threadIdx.x;
+        double xl, yl, zl;
+        if (t < f.ntrial && inflow_trial(f, (uint32_t)t, xl, yl, zl)) mine++;
+    }
+    atomicAdd(&c, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) counts[blockIdx.x] = c;
+}
+
+// The accepted trials' particles, nsp per trial in species order, appended
+// at used + nsp * (rank of the trial among the accepted ones): the
+// reference's order of InsertParticleAt calls.  Nothing when they do not fit.
+__global__ void __launch_bounds__(256) k_inflow_fill(GridP g, InflowParams f, const double *__restrict__ X,
+                                                     const double *__restrict__ P, int nt, PartF64 p,
+                                                     const Counters *__restrict__ cnt, const uint32_t *__restrict__ offs,
+                                                     const uint32_t *__restrict__ total, long long capacity, int *err)
+{
+    __shared__ uint32_t wh[kTileWarps];
+    const long long used = cnt->used;
+    if (used + (long long)f.nsp * (long long)*total > capacity) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
+        return;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const long long wbase = (long long)blockIdx.x * kTile + (long long)warp * kWarpItems;
+    const uint32_t lt = lanemask_lt();
+    uint32_t mine = 0;
+    for (int r = 0; r < kWarpItems / 32; r++) {
+        const long long t = wbase + r * 32 + lane;
+        double xl, yl, zl;
+        const bool acc = t < f.ntrial && inflow_trial(f, (uint32_t)t, xl, yl, zl);
+        mine += __popc(__ballot_sync(0xffffffffu, acc));
+    }
+    if (lane == 0) wh[warp] = mine;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = offs[blockIdx.x];
+        for (int k = 0; k < kTileWarps; k++) {
+            const uint32_t t = wh[k];
+            wh[k] = run;
+            run += t;
+        }
+    }
+    __syncthreads();
+    uint32_t run = wh[warp];
+    for (int r = 0; r < kWarpItems / 32; r++) {
+        const long long t = wbase + r * 32 + lane;
+        double xl = 0, yl = 0, zl = 0;
+        const bool acc = t < f.ntrial && inflow_trial(f, (uint32_t)t, xl, yl, zl);
+        const uint32_t b = __ballot_sync(0xffffffffu, acc);
+        if (acc) {
+            const long long slot = used + (long long)f.nsp * (long long)(run + __popc(b & lt));
+            for (int sp = 0; sp < f.nsp; sp++) {
+                double rmb, riso2, riso3, unused;
+                inflow_draw(f, (uint32_t)t, 2 + 2 * sp, rmb, riso2);
+                inflow_draw(f, (uint32_t)t, 3 + 2 * sp, riso3, unused);
+                double u, v, w;
+                maxwell_momentum(X, P, nt, f.temp[sp], rmb, riso2, riso3, f.drift[0], f.drift[1], f.drift[2], u, v, w);
+                const long long o = slot + sp;
+                p.x[o] = xl;
+                p.y[o] = yl;
+                p.z[o] = zl;
+                p.u[o] = u;
+                p.v[o] = v;
+                p.w[o] = w;
+                p.q[o] = f.charge[sp];
+                p.flv[o] = f.flv[sp];
+            }
+        }
+        run += __popc(b);
+    }
+}
+
+__global__ void k_inflow_finish(Counters *cnt, const uint32_t *__restrict__ total, int nsp, long long capacity)
+{
+    const long long n = (long long)nsp * (long long)*total;
+    if (cnt->used + n <= capacity) cnt->used += n;
+}
+
+int launch_inflow(const GridP &g, const InflowParams &f, const double *X, const double *P, int nt, PartF64 &p,
+                  Counters *cnt, SortScratch &sc, long long capacity, int *err, cudaStream_t s)
+{
+    if (f.ntrial <= 0) return PIC_OK;
+    const size_t ntiles = (size_t)((f.ntrial + kTile - 1) / kTile);
+    if (ntiles > 256 * sc.ntiles) return PIC_ERR_OVERFLOW;
+    uint32_t *total = sc.scan_tmp + sc.scan_tmp_len - 1;
+    k_inflow_count<<<(unsigned)ntiles, 256, 0, s>>>(f, sc.hist);
+    count_launches(1);
+    scan_exclusive_u32(sc.hist, sc.hist, ntiles, sc.scan_tmp, total, s);
+    k_inflow_fill<<<(unsigned)ntiles, 256, 0, s>>>(g, f, X, P, nt, p, cnt, sc.hist, total, capacity, err);
+    k_inflow_finish<<<1, 1, 0, s>>>(cnt, total, f.nsp, capacity);
+    count_launches(2);
     return PIC_OK;
 }
 

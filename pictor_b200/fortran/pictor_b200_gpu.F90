@@ -26,6 +26,16 @@ module pictor_b200_capi
                             reserved(3)
    end type pic_config
 
+   ! pic_inflow: one 'iflw' face's injection (bc_inflow.F90) with a uniform
+   ! density and drift, up to four phase-space properties
+   type, bind(C) :: pic_inflow_t
+      integer(c_int32_t) :: face
+      real(c_double)     :: pos, speed, vmax, epc, density, drift(3)
+      integer(c_int32_t) :: nspecies, flv(4)
+      real(c_double)     :: temp(4), charge(4)
+      integer(c_int32_t) :: seed, call
+   end type pic_inflow_t
+
    interface
       integer(c_int) function pic_create(cfg, h) bind(C, name="pic_create")
          import :: c_int, c_ptr, pic_config
@@ -173,6 +183,11 @@ module pictor_b200_capi
          type(c_ptr), value :: h
          integer(c_int32_t), value :: side
          real(c_double), value :: pos
+      end function
+      integer(c_int) function pic_bc_inflow(h, inj) bind(C, name="pic_bc_inflow")
+         import :: c_int, c_ptr, pic_inflow_t
+         type(c_ptr), value :: h
+         type(pic_inflow_t), intent(in) :: inj
       end function
    end interface
 

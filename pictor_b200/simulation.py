@@ -319,6 +319,21 @@ class Simulation:
         return {"B2": out[0], "E2": out[1], "Benergy": 0.5 * out[0], "Eenergy": 0.5 * out[1],
                 "gauss_linf": out[2], "rho_max": out[3], "kinetic": out[4:].copy()}
 
+    def InflowBC_Prtl(self, face: int, pos: float, species, epc: float, density: float = 1.0,
+                      drift=(0.0, 0.0, 0.0), speed: float = 0.0, vmax: float = 1.0, seed: int = 1, call: int = 0):
+        """InjectNewPrtl (bc_inflow.F90:134-256) at the 'iflw' face 1..6 for a
+        uniform density and drift; ``species`` lists (flv, temperature, charge)."""
+        f = _capi.Inflow()
+        f.face, f.pos, f.speed, f.vmax, f.epc, f.density = int(face), float(pos), float(speed), float(vmax), \
+            float(epc), float(density)
+        for d in range(3):
+            f.drift[d] = float(drift[d])
+        f.nspecies = len(species)
+        for k, (fl, tp, q) in enumerate(species):
+            f.flv[k], f.temp[k], f.charge[k] = int(fl), float(tp), float(q)
+        f.seed, f.call = int(seed) & 0xFFFFFFFF, int(call) & 0xFFFFFFFF
+        check(self.L.pic_bc_inflow(self.h, C.byref(f)), "pic_bc_inflow")
+
     def solve_gauss(self, tol: float = 1e-12, max_iter: int = 20000) -> dict:
         """The initial electrostatic field (pic_solve_gauss): E = -grad(phi)
         with the Gauss residual's node divergence equal to the particles' CIC

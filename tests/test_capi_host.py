@@ -41,13 +41,15 @@ def test_error_strings_without_gpu():
     assert L.pic_version() >= 10000
 
 
-def test_config_struct_layout_matches_c():
+@pytest.mark.parametrize("cname,pyname", [("pic_config", "Config"), ("pic_inflow", "Inflow")])
+def test_struct_layout_matches_c(cname, pyname):
     from pictor_b200 import _capi
 
-    fields = [f[0] for f in _capi.Config._fields_]
-    prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"pictor_b200.h\"\nint main(){printf(\"%zu\\n\", sizeof(pic_config));"
+    st = getattr(_capi, pyname)
+    fields = [f[0] for f in st._fields_]
+    prog = "#include <stdio.h>\n#include <stddef.h>\n#include \"pictor_b200.h\"\nint main(){printf(\"%zu\\n\", sizeof(" + cname + "));"
     for f in fields:
-        prog += f'printf("%zu\\n", offsetof(pic_config, {f}));'
+        prog += f'printf("%zu\\n", offsetof({cname}, {f}));'
     prog += "return 0;}\n"
     with tempfile.TemporaryDirectory() as d:
         c = os.path.join(d, "t.c")
@@ -55,9 +57,9 @@ def test_config_struct_layout_matches_c():
         open(c, "w").write(prog)
         subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), c, "-o", exe], check=True)
         out = [int(x) for x in subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()]
-    assert out[0] == C.sizeof(_capi.Config)
+    assert out[0] == C.sizeof(st)
     for f, off in zip(fields, out[1:]):
-        assert getattr(_capi.Config, f).offset == off, f
+        assert getattr(st, f).offset == off, f
 
 
 def test_create_without_gpu_fails_cleanly():
@@ -130,3 +132,4 @@ def test_slab_and_wall_entry_points_validate_without_gpu():
     assert L.pic_bc_open_x(None, 1, 1.5) == -1
     assert L.pic_bc_open_prtl_x(None, 1, 1.5) == -1
     assert L.pic_solve_gauss(None, 1e-12, 100, None, None, None) == -1
+    assert L.pic_bc_inflow(None, None) == -1
