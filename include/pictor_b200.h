@@ -241,6 +241,14 @@ typedef struct pic_inflow {
     uint32_t seed, call;
 } pic_inflow;
 int pic_bc_inflow(pic_handle *h, const pic_inflow *inj);
+/* RefPrtlFluidFrameRight (bc_inflow.F90:62-121), which InflowBC_Prtl runs
+   before injecting when bc_face(2) is an 'iflw' particle face with 'rndm'
+   placement: every particle beyond the injector at pos (bc_face(2)%pos_prtl)
+   moved by the flow's drift (x > pos + 3 + drift_x c, local) is reflected
+   in the frame moving with the flow (ReflectPrtlMovingFrameX), mirrored
+   across that layer, and the current of the move added to J
+   (DepositCurrentPIC, deposit.F90:11-103; FP64 atomics).  FP64 Cartesian. */
+int pic_bc_inflow_reflect(pic_handle *h, double pos, double drift_x);
 
 /* Slab form (pic_config.slab_x = 1).  A slab's step is the phase sequence
    with exchanges between the slabs (comm_fld.F90:15-130, loadprtlout.F90:

@@ -118,6 +118,7 @@ def _declare(L: C.CDLL) -> None:
     L.orc_open_prtl.restype = C.c_int
     L.orc_inject.argtypes = [P(Grid), P(_Particles), P(Inflow)]
     L.orc_inject.restype = C.c_int64
+    L.orc_refl_fluid_right.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_double, C.c_double]
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -358,6 +359,11 @@ class Oracle:
             f.flv[k], f.temp[k], f.charge[k] = int(fl), float(tp), float(q)
         f.seed, f.call = int(seed) & 0xFFFFFFFF, int(call) & 0xFFFFFFFF
         return self._call_p(self.L.orc_inject, C.byref(f))
+
+    def reflect_fluid_right(self, pos: float, vx: float):
+        """RefPrtlFluidFrameRight at the right injector pos for the uniform drift vx."""
+        fs = self.f.struct()
+        self._call_p(self.L.orc_refl_fluid_right, C.byref(fs), float(pos), float(vx))
 
     def open_prtl_x(self, side: int, pos: float, dx: float = 1.0) -> int:
         """OpenBC_Prtl_Left (side 0) / OpenBC_Prtl_Right (side 1) at pos."""

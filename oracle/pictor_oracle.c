@@ -1196,6 +1196,88 @@ int orc_open_prtl(const orc_grid *g, orc_particles *p, int side, double pos, dou
     return 0;
 }
 
+/* DepositCurrentPIC (deposit.F90:11-103): the zigzag current of a move from
+   (x0, y0, z0) to (x, y, z) added straight into J. */
+static void deposit_current_pic(const orc_grid *g, orc_fields *f, double x0, double y0, double z0, double x,
+                                double y, double z, double q)
+{
+    const double qthis = q * g->qi;
+    const int i1 = (int)floor(x0), i2 = (int)floor(x), j1 = (int)floor(y0), j2 = (int)floor(y);
+    int k1 = (int)floor(z0), k2 = (int)floor(z);
+    const double xr = fmin((double)((i1 < i2 ? i1 : i2) + 1), fmax((double)(i1 > i2 ? i1 : i2), 0.5 * (x0 + x)));
+    const double yr = fmin((double)((j1 < j2 ? j1 : j2) + 1), fmax((double)(j1 > j2 ? j1 : j2), 0.5 * (y0 + y)));
+    const double zr = fmin((double)((k1 < k2 ? k1 : k2) + 1), fmax((double)(k1 > k2 ? k1 : k2), 0.5 * (z0 + z)));
+    const double Fx1 = qthis * (xr - x0), Fy1 = qthis * (yr - y0), Fz1 = qthis * (zr - z0);
+    const double Wx1 = 0.5 * (x0 + xr) - i1, Wy1 = 0.5 * (y0 + yr) - j1;
+    const double Wx2 = 0.5 * (x + xr) - i2, Wy2 = 0.5 * (y + yr) - j2;
+    double Wz1, Wz2;
+    const int three = g->dims == 3;
+    if (!three) { k1 = 1; k2 = 1; Wz1 = 0.0; Wz2 = 0.0; }
+    else { Wz1 = 0.5 * (z0 + zr) - k1; Wz2 = 0.5 * (z + zr) - k2; }
+    const double Fx2 = qthis * (x - xr), Fy2 = qthis * (y - yr), Fz2 = qthis * (z - zr);
+    double *Jx = f->Jx, *Jy = f->Jy, *Jz = f->Jz;
+    Jx[ID(g, i1, j1, k1)] += Fx1 * (1.0 - Wy1) * (1.0 - Wz1);
+    Jx[ID(g, i1, j1 + 1, k1)] += Fx1 * Wy1 * (1.0 - Wz1);
+    if (three) {
+        Jx[ID(g, i1, j1, k1 + 1)] += Fx1 * (1.0 - Wy1) * Wz1;
+        Jx[ID(g, i1, j1 + 1, k1 + 1)] += Fx1 * Wy1 * Wz1;
+    }
+    Jx[ID(g, i2, j2, k2)] += Fx2 * (1.0 - Wy2) * (1.0 - Wz2);
+    Jx[ID(g, i2, j2 + 1, k2)] += Fx2 * Wy2 * (1.0 - Wz2);
+    if (three) {
+        Jx[ID(g, i2, j2, k2 + 1)] += Fx2 * (1.0 - Wy2) * Wz2;
+        Jx[ID(g, i2, j2 + 1, k2 + 1)] += Fx2 * Wy2 * Wz2;
+    }
+    Jy[ID(g, i1, j1, k1)] += Fy1 * (1.0 - Wx1) * (1.0 - Wz1);
+    Jy[ID(g, i1 + 1, j1, k1)] += Fy1 * Wx1 * (1.0 - Wz1);
+    if (three) {
+        Jy[ID(g, i1, j1, k1 + 1)] += Fy1 * (1.0 - Wx1) * Wz1;
+        Jy[ID(g, i1 + 1, j1, k1 + 1)] += Fy1 * Wx1 * Wz1;
+    }
+    Jy[ID(g, i2, j2, k2)] += Fy2 * (1.0 - Wx2) * (1.0 - Wz2);
+    Jy[ID(g, i2 + 1, j2, k2)] += Fy2 * Wx2 * (1.0 - Wz2);
+    if (three) {
+        Jy[ID(g, i2, j2, k2 + 1)] += Fy2 * (1.0 - Wx2) * Wz2;
+        Jy[ID(g, i2 + 1, j2, k2 + 1)] += Fy2 * Wx2 * Wz2;
+    }
+    Jz[ID(g, i1, j1, k1)] += Fz1 * (1.0 - Wx1) * (1.0 - Wy1);
+    Jz[ID(g, i1 + 1, j1, k1)] += Fz1 * Wx1 * (1.0 - Wy1);
+    Jz[ID(g, i1, j1 + 1, k1)] += Fz1 * (1.0 - Wx1) * Wy1;
+    Jz[ID(g, i1 + 1, j1 + 1, k1)] += Fz1 * Wx1 * Wy1;
+    Jz[ID(g, i2, j2, k2)] += Fz2 * (1.0 - Wx2) * (1.0 - Wy2);
+    Jz[ID(g, i2 + 1, j2, k2)] += Fz2 * Wx2 * (1.0 - Wy2);
+    Jz[ID(g, i2, j2 + 1, k2)] += Fz2 * (1.0 - Wx2) * Wy2;
+    Jz[ID(g, i2 + 1, j2 + 1, k2)] += Fz2 * Wx2 * Wy2;
+}
+
+/* RefPrtlFluidFrameRight (bc_inflow.F90:62-97) with ReflectPrtlMovingFrameX
+   (:100-121) for a uniform drift vx, on one rank. */
+void orc_refl_fluid_right(const orc_grid *g, orc_particles *p, orc_fields *f, double pos, double vx)
+{
+    const double xinj = pos - 0.0 + 3;
+    if (xinj > g->mx - 1) return;
+    const double x1 = xinj + vx * g->c;
+    for (int64_t n = 0; n < p->used; n++) {
+        if (!(p->q[n] != 0 && p->x[n] > x1)) continue;
+        double db, dg;
+        if (fabs(vx) < 1.0) { db = vx; dg = 1.0 / sqrt((1.0 - vx) * (1.0 + vx)); }
+        else { dg = fabs(vx); db = sqrt((vx - 1.0) * (vx + 1.0)) / vx; }
+        double u = p->u[n];
+        const double v = p->v[n], w = p->w[n];
+        double gamma = sqrt(1.0 + u * u + v * v + w * w);
+        db = -db;
+        u = dg * u + dg * db * gamma;
+        u = -u;
+        gamma = sqrt(1.0 + u * u + v * v + w * w);
+        db = -db;
+        u = dg * u + dg * db * gamma;
+        p->u[n] = u;
+        const double x0 = p->x[n], y0 = p->y[n], z0 = p->z[n];
+        p->x[n] = 2.0 * x1 - x0;
+        deposit_current_pic(g, f, x0, y0, z0, p->x[n], p->y[n], p->z[n], p->q[n]);
+    }
+}
+
 /* ------------------------------------------------------------------------- */
 /* One time step, src/MAIN.F90:42-284                                        */
 /* ------------------------------------------------------------------------- */

@@ -121,6 +121,8 @@ typedef struct {
     uint32_t seed, call;
 } orc_inflow;
 int64_t orc_inject(const orc_grid *g, orc_particles *p, const orc_inflow *f);
+/* RefPrtlFluidFrameRight (bc_inflow.F90:62-121) with DepositCurrentPIC. */
+void orc_refl_fluid_right(const orc_grid *g, orc_particles *p, orc_fields *f, double pos, double vx);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

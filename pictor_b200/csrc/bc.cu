@@ -404,6 +404,109 @@ __global__ void k_open_prtl_finish(Counters *cnt, const uint32_t *__restrict__ t
     if (cnt->used + m <= capacity) cnt->used += m;
 }
 
+// ---------------------------------------------------------------------------
+// RefPrtlFluidFrameRight (bc_inflow.F90:62-97) for a uniform drift vx: a
+// particle beyond the drifted injector layer x1 = xinj + vx c is reflected in
+// the frame moving with the flow (ReflectPrtlMovingFrameX, :100-121),
+// mirrored to 2 x1 - x, and the current of that move deposited
+// (DepositCurrentPIC, deposit.F90:11-103, FP64 atomics into J).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void add_j(double *F, long long c, double v) { atomicAdd(F + c, v); }
+
+__global__ void k_refl_fluid_right(GridP g, PartF64 p, const Counters *__restrict__ cnt, double x1, double drift,
+                                   double *Jx, double *Jy, double *Jz, int *err)
+{
+    const long long used = cnt->used;
+    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used;
+         n += (long long)gridDim.x * blockDim.x) {
+        if (p.q[n] == 0.0) continue;
+        const double x0 = p.x[n];
+        if (!(x0 > x1)) continue;
+        const double y0 = p.y[n], z0 = p.z[n];
+        // ReflectPrtlMovingFrameX
+        double db, dg;
+        if (fabs(drift) < 1.0) {
+            db = drift;
+            dg = 1.0 / sqrt((1.0 - drift) * (1.0 + drift));
+        } else {
+            dg = fabs(drift);
+            db = sqrt((drift - 1.0) * (drift + 1.0)) / drift;
+        }
+        double u = p.u[n];
+        const double v = p.v[n], w = p.w[n];
+        double gamma = sqrt(1.0 + u * u + v * v + w * w);
+        db = -db;
+        u = dg * u + dg * db * gamma;
+        u = -u;
+        gamma = sqrt(1.0 + u * u + v * v + w * w);
+        db = -db;
+        u = dg * u + dg * db * gamma;
+        const double x = 2.0 * x1 - x0, y = y0, z = z0;
+        // DepositCurrentPIC
+        const int i1 = (int)floor(x0), i2 = (int)floor(x), j1 = (int)floor(y0), j2 = (int)floor(y);
+        int k1 = (int)floor(z0), k2 = (int)floor(z);
+        const bool three = g.dims == 3;
+        if (i1 < 1 || i1 > g.mx - 1 || i2 < 1 || i2 > g.mx - 1 || j1 < 1 || j1 > g.my - 1 ||
+            (three && (k1 < 1 || k1 > g.mz - 1))) {
+            raise_error(err, PIC_DEVERR_RANGE);
+            continue;
+        }
+        p.u[n] = u;
+        p.x[n] = x;
+        const double qthis = p.q[n] * g.qi;
+        const double xr = fmin((double)(min(i1, i2) + 1), fmax((double)max(i1, i2), 0.5 * (x0 + x)));
+        const double yr = fmin((double)(min(j1, j2) + 1), fmax((double)max(j1, j2), 0.5 * (y0 + y)));
+        const double zr = fmin((double)(min(k1, k2) + 1), fmax((double)max(k1, k2), 0.5 * (z0 + z)));
+        const double Fx1 = qthis * (xr - x0), Fy1 = qthis * (yr - y0), Fz1 = qthis * (zr - z0);
+        const double Wx1 = 0.5 * (x0 + xr) - i1, Wy1 = 0.5 * (y0 + yr) - j1;
+        const double Wx2 = 0.5 * (x + xr) - i2, Wy2 = 0.5 * (y + yr) - j2;
+        double Wz1, Wz2;
+        if (!three) {
+            k1 = 1;
+            k2 = 1;
+            Wz1 = 0.0;
+            Wz2 = 0.0;
+        } else {
+            Wz1 = 0.5 * (z0 + zr) - k1;
+            Wz2 = 0.5 * (z + zr) - k2;
+        }
+        const double Fx2 = qthis * (x - xr), Fy2 = qthis * (y - yr), Fz2 = qthis * (z - zr);
+        auto C = [&](int i, int j, int k) { return cidx(g, i, j, k); };
+        add_j(Jx, C(i1, j1, k1), Fx1 * (1.0 - Wy1) * (1.0 - Wz1));
+        add_j(Jx, C(i1, j1 + 1, k1), Fx1 * Wy1 * (1.0 - Wz1));
+        if (three) {
+            add_j(Jx, C(i1, j1, k1 + 1), Fx1 * (1.0 - Wy1) * Wz1);
+            add_j(Jx, C(i1, j1 + 1, k1 + 1), Fx1 * Wy1 * Wz1);
+        }
+        add_j(Jx, C(i2, j2, k2), Fx2 * (1.0 - Wy2) * (1.0 - Wz2));
+        add_j(Jx, C(i2, j2 + 1, k2), Fx2 * Wy2 * (1.0 - Wz2));
+        if (three) {
+            add_j(Jx, C(i2, j2, k2 + 1), Fx2 * (1.0 - Wy2) * Wz2);
+            add_j(Jx, C(i2, j2 + 1, k2 + 1), Fx2 * Wy2 * Wz2);
+        }
+        add_j(Jy, C(i1, j1, k1), Fy1 * (1.0 - Wx1) * (1.0 - Wz1));
+        add_j(Jy, C(i1 + 1, j1, k1), Fy1 * Wx1 * (1.0 - Wz1));
+        if (three) {
+            add_j(Jy, C(i1, j1, k1 + 1), Fy1 * (1.0 - Wx1) * Wz1);
+            add_j(Jy, C(i1 + 1, j1, k1 + 1), Fy1 * Wx1 * Wz1);
+        }
+        add_j(Jy, C(i2, j2, k2), Fy2 * (1.0 - Wx2) * (1.0 - Wz2));
+        add_j(Jy, C(i2 + 1, j2, k2), Fy2 * Wx2 * (1.0 - Wz2));
+        if (three) {
+            add_j(Jy, C(i2, j2, k2 + 1), Fy2 * (1.0 - Wx2) * Wz2);
+            add_j(Jy, C(i2 + 1, j2, k2 + 1), Fy2 * Wx2 * Wz2);
+        }
+        add_j(Jz, C(i1, j1, k1), Fz1 * (1.0 - Wx1) * (1.0 - Wy1));
+        add_j(Jz, C(i1 + 1, j1, k1), Fz1 * Wx1 * (1.0 - Wy1));
+        add_j(Jz, C(i1, j1 + 1, k1), Fz1 * (1.0 - Wx1) * Wy1);
+        add_j(Jz, C(i1 + 1, j1 + 1, k1), Fz1 * Wx1 * Wy1);
+        add_j(Jz, C(i2, j2, k2), Fz2 * (1.0 - Wx2) * (1.0 - Wy2));
+        add_j(Jz, C(i2 + 1, j2, k2), Fz2 * Wx2 * (1.0 - Wy2));
+        add_j(Jz, C(i2, j2 + 1, k2), Fz2 * (1.0 - Wx2) * Wy2);
+        add_j(Jz, C(i2 + 1, j2 + 1, k2), Fz2 * Wx2 * Wy2);
+    }
+}
+
 int grid_for(long long n)
 {
     const long long b = (n + kThreads - 1) / kThreads;
@@ -596,6 +699,19 @@ void launch_bc_open_prtl_x(const GridP &g, PartF64 &p, Counters *cnt, int side, 
     k_open_prtl_insert<<<tiles, 256, 0, s>>>(g, p, cnt, side, wall, flag, counts, total, col, capacity, err);
     k_open_prtl_finish<<<1, 1, 0, s>>>(cnt, total, capacity);
     count_launches(2);
+}
+
+// RefPrtlFluidFrameRight at the right injector `pos` (bc_face(2)%pos_prtl)
+// for the uniform drift vx; nothing when the injector lies at or beyond the
+// grid's last layer (xinj_local > mx - 1).
+void launch_bc_inflow_reflect(const GridP &g, PartF64 &p, const Counters *cnt, double *const J[3], double pos,
+                              double drift, long long capacity, int *err, cudaStream_t s)
+{
+    const double xinj = pos - 0.0 + 3;
+    if (xinj > g.mx - 1) return;
+    k_refl_fluid_right<<<grid_for(capacity), kThreads, 0, s>>>(g, p, cnt, xinj + drift * g.c, drift, J[0], J[1], J[2],
+                                                               err);
+    count_launches(1);
 }
 
 }  // namespace pic

@@ -1587,6 +1587,16 @@ int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos)
     return finish_phase(h);
 }
 
+int pic_bc_inflow_reflect(pic_handle *h, double pos, double drift_x)
+{
+    if (!h || h->fp32 || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || !(fabs(drift_x) < 1e300))
+        return PIC_ERR_INVALID;
+    double *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    launch_bc_inflow_reflect(h->g, h->p64[h->cur], h->cnt, J, pos, drift_x, h->capacity, h->err, h->s);
+    return finish_phase(h);
+}
+
 // Philox-4x32-10 on the host (the draw of the injection's Poisson count).
 static void host_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4])
 {

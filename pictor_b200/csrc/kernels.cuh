@@ -205,6 +205,9 @@ void launch_bc_attenuate(const GridP &g, double *const E[3], double *const B[3],
 void launch_bc_attenuate_flow(const GridP &g, double *const E[3], double *const B[3], int side, double pos, double dl,
                               double sc, const double *b, const double *v, cudaStream_t s);
 void launch_bc_open_fld_x(const GridP &g, double *const E[3], double *const B[3], int side, double pos, cudaStream_t s);
+// bc.cu: RefPrtlFluidFrameRight (bc_inflow.F90:62-121) with its current
+void launch_bc_inflow_reflect(const GridP &g, PartF64 &p, const Counters *cnt, double *const J[3], double pos,
+                              double drift, long long capacity, int *err, cudaStream_t s);
 // bc.cu: an 'open' particle face along x (OpenBC_Prtl_Left/Right, bc.F90:478-621)
 void launch_bc_open_prtl_x(const GridP &g, PartF64 &p, Counters *cnt, int side, double pos, double *col,
                            uint32_t *flag, uint32_t *counts, uint32_t *scan_tmp, uint32_t *total, long long capacity,

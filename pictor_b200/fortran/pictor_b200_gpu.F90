@@ -189,6 +189,11 @@ module pictor_b200_capi
          type(c_ptr), value :: h
          type(pic_inflow_t), intent(in) :: inj
       end function
+      integer(c_int) function pic_bc_inflow_reflect(h, pos, drift_x) bind(C, name="pic_bc_inflow_reflect")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: h
+         real(c_double), value :: pos, drift_x
+      end function
    end interface
 
    ! Slab form (cfg%slab_x = 1): x faces exchanged by the host

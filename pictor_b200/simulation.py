@@ -334,6 +334,11 @@ class Simulation:
         f.seed, f.call = int(seed) & 0xFFFFFFFF, int(call) & 0xFFFFFFFF
         check(self.L.pic_bc_inflow(self.h, C.byref(f)), "pic_bc_inflow")
 
+    def RefPrtlFluidFrameRight(self, pos: float, drift_x: float):
+        """RefPrtlFluidFrameRight (bc_inflow.F90:62-121) at the right
+        injector pos for the uniform flow drift_x, with its current."""
+        check(self.L.pic_bc_inflow_reflect(self.h, float(pos), float(drift_x)), "pic_bc_inflow_reflect")
+
     def solve_gauss(self, tol: float = 1e-12, max_iter: int = 20000) -> dict:
         """The initial electrostatic field (pic_solve_gauss): E = -grad(phi)
         with the Gauss residual's node divergence equal to the particles' CIC

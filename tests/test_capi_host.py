@@ -133,3 +133,4 @@ def test_slab_and_wall_entry_points_validate_without_gpu():
     assert L.pic_bc_open_prtl_x(None, 1, 1.5) == -1
     assert L.pic_solve_gauss(None, 1e-12, 100, None, None, None) == -1
     assert L.pic_bc_inflow(None, None) == -1
+    assert L.pic_bc_inflow_reflect(None, 20.0, -0.3) == -1

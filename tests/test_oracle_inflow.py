@@ -67,3 +67,45 @@ def test_lower_face_moving_injector_and_poisson_count():
     before = o.p.used
     assert o.inject(1, 10.0, SP, epc=4000.0, density=1.0, drift=(0.2, 0.0, 0.0), speed=0.5, seed=11, call=1) == -1
     assert o.p.used == before
+
+
+def test_fluid_frame_reflection():
+    """RefPrtlFluidFrameRight: a particle beyond the drifted injector layer
+    is reflected in the flow's frame (for a flow at rest, u -> -u), mirrored
+    across the layer, and the current of that move is the zigzag current of
+    DepositCurrentPIC (here a move inside one cell: Jx(i, j) and Jx(i, j+1)
+    share F = q qi dx in the ratio of the midpoint's y weight)."""
+    g = O.make_grid(2, 32, 16, c=0.45, qi=0.01)
+    p = O.Particles(4)
+    rows = [(23.4, 7.25, 0.2, 1.0), (22.6, 7.5, 0.1, 1.0), (23.9, 8.5, -0.1, 0.0)]   # x, y, u, q
+    for n, (x, y, u, q) in enumerate(rows):
+        p.x[n], p.y[n], p.z[n], p.u[n], p.q[n], p.flv[n] = x, y, 1.5, u, q, (1 if q else 0)
+    p.used = 3
+    f = O.Fields(g)
+    o = O.Oracle(g, p, f)
+    o.reflect_fluid_right(20.0, 0.0)                     # layer at 23.0 (local), no flow
+    v = o.p.view()
+    assert v["x"][0] == 2.0 * 23.0 - 23.4 and v["u"][0] == -0.2
+    assert v["x"][1] == 22.6 and v["u"][1] == 0.1          # before the layer: untouched
+    assert v["x"][2] == 23.9                               # a hole (q = 0): untouched
+    # the move 23.4 -> 22.6 crosses x = 23: two segments, Jx of cells 23 and 22 at y weights of 7.25
+    F1, F2 = 0.01 * (23.0 - 23.4), 0.01 * (22.6 - 23.0)
+    np.testing.assert_allclose(o.f.Jx[22, 6, 0], F1 * (1 - 0.25))
+    np.testing.assert_allclose(o.f.Jx[22, 7, 0], F1 * 0.25)
+    np.testing.assert_allclose(o.f.Jx[21, 6, 0], F2 * (1 - 0.25))
+    np.testing.assert_allclose(o.f.Jx[21, 7, 0], F2 * 0.25)
+    assert abs(o.f.Jx.sum() - 0.01 * (22.6 - 23.4)) < 1e-15
+    # a flow drifting at -0.3c: u is reflected in the flow's frame (gamma-boosted), the layer at 23 - 0.135
+    p = O.Particles(2)
+    p.x[0], p.y[0], p.z[0], p.u[0], p.q[0], p.flv[0] = 23.2, 7.5, 1.5, -0.1, 1.0, 1
+    p.used = 1
+    o = O.Oracle(g, p, O.Fields(g))
+    o.reflect_fluid_right(20.0, -0.3)
+    dg, db = 1 / np.sqrt((1 + 0.3) * (1 - 0.3)), -0.3
+    u = -0.1
+    gam = np.sqrt(1 + u * u)
+    u = -(dg * u + dg * (-db) * gam)
+    gam = np.sqrt(1 + u * u)
+    u = dg * u + dg * db * gam
+    np.testing.assert_allclose(o.p.view()["u"][0], u, rtol=1e-15)
+    assert o.p.view()["x"][0] == 2.0 * (23.0 - 0.3 * 0.45) - 23.2
