@@ -223,7 +223,7 @@ def mover_kernel(wl: dict, precision: str) -> str:
     """The mover kernel of the timed steps (after a reorder): the FP32 tiled
     mover, or the FP64 one by tiles unless tiles are switched off."""
     if precision == "fp32":
-        return "k_move_f32_tiled"
+        return "k_move_f32_tiled (timed with the k_node_avg pass it reads from)"
     return "k_move_f64" if wl.get("fp64_tiles", 0) < 0 else "k_move_f64_tiled"
 
 

@@ -1037,6 +1037,11 @@ int pic_create(const pic_config *cfg, pic_handle **out)
             (r = dalloc(h, &bk.scan_tmp, scan_tmp_len(nt + 1))) ||
             (r = dalloc(h, &bk.wmax_bits, 1))) {
         }
+        // the node averages of the Cartesian tiled mover, computed once per
+        // move instead of by every brick for its box
+        if (!r && g.geom == PIC_GEOM_CARTESIAN &&
+            !(r = dalloc(h, (char **)&bk.nodeA, (size_t)g.ncell * sizeof(float4))))
+            r = dalloc(h, (char **)&bk.nodeB, (size_t)g.ncell * sizeof(float2));
     }
     if (!r) r = dalloc(h, &h->cnt, 1);
     if (!r) r = dalloc(h, &h->err, 1);

@@ -99,6 +99,8 @@ struct Bricks {
     uint32_t *src;          // source slot of every brick-grouped slot (capacity)
     uint32_t *scan_tmp;
     uint32_t *wmax_bits;    // max |w| of the live particles (FP32 bits), set by the reorder
+    float4 *nodeA;          // node-averaged Ex, Ey, Ez, Bx (+ bext) at every interior node, or null
+    float2 *nodeB;          // node-averaged By, Bz (+ bext); both written before each tiled move
     int t[3], nb[3], ntiles;
     int smem_floats;
 };

@@ -43,7 +43,7 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // Tiled form: one CTA per brick.
 // ---------------------------------------------------------------------------
 
-template <int DIMS, bool XC>
+template <int DIMS, bool XC, bool PRE>
 __global__ void __launch_bounds__(kTileThreads, 3)
     k_move_f32_tiled(GridP g, PartF32 p, Bricks bk, const float *__restrict__ Ex, const float *__restrict__ Ey,
                      const float *__restrict__ Ez, const float *__restrict__ Bx, const float *__restrict__ By,
@@ -51,7 +51,30 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 {
     extern __shared__ __align__(16) float sm[];
     __shared__ TileShared ts;
-    move_brick<DIMS, XC>(g, p, bk, blockIdx.x, sm, ts, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err);
+    move_brick<DIMS, XC, PRE>(g, p, bk, blockIdx.x, sm, ts, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err);
+}
+
+// The node averages of every interior node (node_avg, the same expressions
+// as the bricks' own staging), for the tiled mover's boxes.
+template <int DIMS>
+__global__ void __launch_bounds__(kThreads) k_node_avg(GridP g, const float *__restrict__ Ex, const float *__restrict__ Ey,
+                                                       const float *__restrict__ Ez, const float *__restrict__ Bx,
+                                                       const float *__restrict__ By, const float *__restrict__ Bz,
+                                                       float4 *nodeA, float2 *nodeB)
+{
+    const long long nint = (long long)g.nx * g.ny * (DIMS == 3 ? g.nz : 1);
+    const int sy = (int)g.sy, sz = (int)g.sz;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
+        const int i = 3 + (int)(t % g.nx);
+        const long long r = t / g.nx;
+        const int j = 3 + (int)(r % g.ny), k = DIMS == 3 ? 3 + (int)(r / g.ny) : 1;
+        const int nd = (int)cidx(g, i, j, k);
+        float4 A;
+        float2 Bv;
+        node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
+        nodeA[nd] = A;
+        nodeB[nd] = Bv;
+    }
 }
 
 // The tiled mover for all runs of a batch in one launch: CTA b takes brick b
@@ -110,20 +133,36 @@ void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Brick
     static bool attr_set = false;
     const int bytes = bk.smem_floats * 4;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_move_f32_tiled<3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
-        cudaFuncSetAttribute(k_move_f32_tiled<3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
-        cudaFuncSetAttribute(k_move_f32_tiled<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<3, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<3, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<2, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<3, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
         attr_set = true;
     }
-    if (g.dims == 3 && g.exact_charge)
-        k_move_f32_tiled<3, true><<<bk.ntiles, kTileThreads, bytes, s>>>(g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2],
-                                                                         J[0], J[1], J[2], err);
-    else if (g.dims == 3)
-        k_move_f32_tiled<3, false><<<bk.ntiles, kTileThreads, bytes, s>>>(g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2],
-                                                                          J[0], J[1], J[2], err);
-    else
-        k_move_f32_tiled<2, false><<<bk.ntiles, kTileThreads, bytes, s>>>(g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2],
-                                                                          J[0], J[1], J[2], err);
+    const bool pre = bk.nodeA != nullptr;
+    if (pre) {
+        const long long nint = (long long)g.nx * g.ny * (g.dims == 3 ? g.nz : 1);
+        long long nb = (nint + kThreads - 1) / kThreads;
+        if (nb > (long long)kSMs * 16) nb = (long long)kSMs * 16;
+        if (g.dims == 3)
+            k_node_avg<3><<<(unsigned)nb, kThreads, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], bk.nodeA, bk.nodeB);
+        else
+            k_node_avg<2><<<(unsigned)nb, kThreads, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], bk.nodeA, bk.nodeB);
+        count_launches(1);
+    }
+#define PIC_MOVE_TILED(D, X, P)                                                                                      \
+    k_move_f32_tiled<D, X, P><<<bk.ntiles, kTileThreads, bytes, s>>>(g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2], J[0], \
+                                                                    J[1], J[2], err)
+    if (g.dims == 3 && g.exact_charge) {
+        if (pre) PIC_MOVE_TILED(3, true, true); else PIC_MOVE_TILED(3, true, false);
+    } else if (g.dims == 3) {
+        if (pre) PIC_MOVE_TILED(3, false, true); else PIC_MOVE_TILED(3, false, false);
+    } else {
+        if (pre) PIC_MOVE_TILED(2, false, true); else PIC_MOVE_TILED(2, false, false);
+    }
+#undef PIC_MOVE_TILED
     count_launches(1);
 }
 

@@ -15,8 +15,11 @@
 // Tiled form (after a reorder): particles are grouped by brick (a block of
 // TX x TY x TZ interior cells, see bricks.cu) and one CTA moves one brick's
 // particles.  The CTA stages the node-averaged E and B of its box in shared
-// memory, so each node value is computed once per brick rather than 8 times
-// per particle.  The box is the bounding box, in cells, of where the brick's
+// memory, so each node value is read once per brick rather than 8 times per
+// particle; the averages themselves are computed once per move for the whole
+// grid (k_node_avg, mover_f32.cu: a streaming pass that writes 24 bytes per
+// node), so the staging is a copy rather than 20 scattered reads per node
+// for a box about twice the brick's size.  The box is the bounding box, in cells, of where the brick's
 // particles were after the previous step (particles drift away from their
 // brick between reorders); it is stored per brick relative to the brick's
 // centre, unwrapped across the periodic boundary, and this kernel writes the
@@ -517,8 +520,9 @@ __device__ __forceinline__ void push_range_tiled(const GridP &g, const PartF32 &
     if (qn) drain_queue<DIMS>(q, qn, tb.jo);
 }
 
-// Move the particles of brick b (one CTA).
-template <int DIMS, bool XC>
+// Move the particles of brick b (one CTA); PRE: the node averages were
+// computed for the whole grid before the launch (bk.nodeA / nodeB).
+template <int DIMS, bool XC, bool PRE = false>
 __device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, const Bricks &bk, int b, float *sm,
                                            TileShared &ts, const float *__restrict__ Ex, const float *__restrict__ Ey,
                                            const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -531,7 +535,8 @@ __device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, con
     int home_lo[3], home_hi[3];
     brick_home<DIMS>(g, bk, b, tb, home_lo, home_hi);
     // a move is below c per axis; the box is the stored bounds (no margin)
-    tile_setup<DIMS, true>(g, bk, b, p1 - p0, 0, g.c_f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By, Bz);
+    tile_setup<DIMS, true, false, PRE>(g, bk, b, p1 - p0, 0, g.c_f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By,
+                                       Bz);
     PackedBounds bd;
     bd.init();
     push_range_tiled<DIMS, XC>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, ts.s_q[threadIdx.x >> 5]);

@@ -3,8 +3,10 @@
 //
 // A CTA moves the particles of one brick (bricks.cu groups them).  It stages
 // the node-averaged E and B of a box of cells around the brick in shared
-// memory (node_avg: each node once per brick instead of 8 times per
-// particle) and sums the brick's current in a shared box of fixed-point
+// memory (each node once per brick instead of 8 times per particle; the
+// Cartesian mover reads them from node arrays that one pass over the grid
+// fills before the move, the cylindrical one averages them itself with
+// node_avg) and sums the brick's current in a shared box of fixed-point
 // words (32-bit; 64-bit for the cylindrical form, whose weights span the
 // radius), added to the global J once at the end.  The box is the
 // bounding box, in cells relative to the brick centre and unwrapped across
@@ -298,7 +300,7 @@ __device__ __forceinline__ void brick_home(const GridP &g, const Bricks &bk, int
 // image, or along a non-periodic x axis (XPER false: the radius of the
 // cylindrical form) the index itself); the current box zeroed and the
 // node-averaged fields staged.
-template <int DIMS, bool XPER, bool WIDE = false>
+template <int DIMS, bool XPER, bool WIDE = false, bool PRE = false>
 __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int b, uint32_t n, int margin, float dmax,
                                            float *sm, TileShared &ts, TileBox &tb, const int home_lo[3],
                                            const int home_hi[3], const float *__restrict__ Ex,
@@ -397,7 +399,12 @@ __device__ __forceinline__ void tile_setup(const GridP &g, const Bricks &bk, int
             const int nd = ts.s_off[0][xx + 1] + ts.s_off[1][yy + 1] + (DIMS == 3 ? ts.s_off[2][zz + 1] : 0);
             float4 A;
             float2 Bv;
-            node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
+            if (PRE) {
+                A = ldro(bk.nodeA + nd);
+                Bv = ldro(bk.nodeB + nd);
+            } else {
+                node_avg<DIMS>(Ex, Ey, Ez, Bx, By, Bz, nd, sy, sz, g.bext_f[0], g.bext_f[1], g.bext_f[2], A, Bv);
+            }
             nA[q] = A;
             nB[q] = Bv;
         }
