@@ -50,7 +50,10 @@ WORKLOADS = {
     # the 2D FP64 Weibel configuration split along x into one slab per rank (strong scaling: the
     # global grid fixed), the slabs exchanging their x faces over NCCL between the phases
     "slab_weibel2d_fp64": dict(dims=2, nx=256, ny=256, nz=1, epc=16, drift=0.5, temp=0.005, c=0.45, c_ompe=2.0,
-                               precision="fp64"),
+                               precision="fp64", cpu_workload="weibel2d_fp64"),
+    # the 3D FP32 Weibel configuration (the headline's) split along x into one slab per rank
+    "slab_weibel3d_fp32": dict(dims=3, nx=512, ny=256, nz=256, epc=8, drift=0.3, temp=8e-4, c=0.45, c_ompe=2.0,
+                               precision="fp32", cpu_workload="weibel3d_fp32"),
     # the differentiable 2D Weibel run: 128^2 cells, 8 particles per cell per species, drift +-0.4c, spread
     # 0.05c, 400 steps, checkpoints every 50, objective sum_t 1/2 sum |B_t|^2 (pictor_b200.adjoint)
     "adjoint128": dict(dims=2, nx=128, ny=128, nz=1, epc=8, drift=0.4, temp=0.005, c=0.45, c_ompe=2.0,
@@ -404,10 +407,11 @@ def parity_weibel2d(wl: dict, horizon: int, every: int = 10) -> dict:
 
 
 def run_slab_bench(args, ws, rank, local, peak, peak_kind):
-    """--workload slab_weibel2d_fp64: the 2D FP64 Weibel grid split along x
-    into one slab per rank (pictor_b200.slab; x faces over NCCL, or copied
-    in place on one rank), each slab loaded by the device loader (seed +
-    rank); the whole step timed with CUDA events, max over ranks."""
+    """--workload slab_weibel2d_fp64 / slab_weibel3d_fp32: the 2D FP64 or the
+    3D FP32 Weibel grid split along x into one slab per rank
+    (pictor_b200.slab; x faces over NCCL, or copied in place on one rank),
+    each slab loaded by the device loader (seed + rank); the whole step timed
+    with CUDA events, max over ranks."""
     import torch
 
     from pictor_b200 import init_scale
@@ -415,11 +419,13 @@ def run_slab_bench(args, ws, rank, local, peak, peak_kind):
 
     wl = WORKLOADS[args.workload]
     sc = init_scale(wl["c"], wl["c_ompe"], wl["epc"])
-    cap = int(2 * wl["epc"] * wl["nx"] * wl["ny"] * 1.04 / ws) + (1 << 16)
+    dims, prec = wl["dims"], wl["precision"]
+    vol = wl["nx"] * wl["ny"] * (wl["nz"] if dims == 3 else 1)
+    cap = int(2 * wl["epc"] * vol * 1.04 / ws) + (1 << 16)
     from pictor_b200 import PicConfig
 
-    cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=1, dims=2, c=wl["c"], qi=sc["qi"], precision="fp64", capacity=cap,
-                    reorder_period=20)
+    cfg = PicConfig(nx=wl["nx"], ny=wl["ny"], nz=wl["nz"] if dims == 3 else 1, dims=dims, c=wl["c"], qi=sc["qi"],
+                    precision=prec, capacity=cap, reorder_period=20)
     dev = torch.device("cuda", local)
     transport = DistTransport() if ws > 1 else LocalTransport()
     dom = SlabDomain([Slab(cfg, rank, ws, dev)], transport, queued=True)
@@ -445,19 +451,21 @@ def run_slab_bench(args, ws, rank, local, peak, peak_kind):
     field = sum_over_ranks(ws, 0.5 * (d["B2"] + d["E2"]))
     dom.close()
     value = n_tot * args.steps / (ms * 1e-3)
-    step_bytes = n_tot * bytes_per_particle(2, "fp64") + wl["nx"] * wl["ny"] * 24 * 8
+    step_bytes = n_tot * bytes_per_particle(dims, prec) + vol * 24 * (8 if prec == "fp64" else 4)
     achieved = step_bytes / (ms / args.steps * 1e-3) / 1e9
-    cpu = None if (args.no_cpu or rank != 0) else cpu_sample(WORKLOADS["weibel2d_fp64"])
+    cpu = None if (args.no_cpu or rank != 0) else cpu_sample(WORKLOADS[wl["cpu_workload"]])
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "global_cells": [wl["nx"], wl["ny"]], "slabs": ws,
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32", "data": "synthetic",
+            "config": {"workload": args.workload,
+                       "global_cells": [wl["nx"], wl["ny"]] + ([wl["nz"]] if dims == 3 else []), "slabs": ws,
                        "slab_cells_x": wl["nx"] // ws, "particles": int(n_tot), "parallelism": f"slab{ws}",
                        "exchange": ("NCCL point-to-point between ranks" if ws > 1 else "x faces copied on the rank")
                        + ", ordered on the library's stream (one host wait per step, for the particle counts)",
-                       "l2": "particles and fields smaller than L2 at this size"},
+                       "l2": ("particles and fields smaller than L2 at this size" if dims == 2 else
+                              "inputs larger than L2 (particle state >> 126 MB)")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                          "traffic": None, "kernel": "whole slab step (phases and host-driven exchanges)",
                          "peak_kind": peak_kind},
@@ -941,7 +949,7 @@ def main():
     if args.workload == "adjoint128":
         peak, peak_kind = measured_peaks()
         return run_adjoint_bench(args, rank, local, peak, peak_kind)
-    if args.workload == "slab_weibel2d_fp64":
+    if args.workload.startswith("slab_"):
         peak, peak_kind = measured_peaks()
         return run_slab_bench(args, ws, rank, local, peak, peak_kind)
     if args.workload.startswith("cyl_wake"):

@@ -84,8 +84,8 @@ typedef struct {
        MPI decomposition with the x neighbours on other ranks): the kernels
        leave the x ghost layers to the pic_slab_* exchanges and particles
        leaving through the x faces to pic_slab_pack_particles; y and z stay
-       periodic on the slab.  FP64 Cartesian, no current filter.  0 = one
-       periodic domain. */
+       periodic on the slab.  Cartesian (FP64 or FP32), no current filter.
+       0 = one periodic domain. */
     int32_t slab_x;
     /* FP64 Cartesian form: 1 = sum the current in the reference's serial
        order (each cell's VecJ entries in particle order, then the cells onto
@@ -272,7 +272,11 @@ int pic_bc_inflow_reflect(pic_handle *h, double pos, double drift_x);
    transfers) and returns the device errors like a synchronous call:
    PIC_ERR_OVERFLOW, with both counts 0 and no particle moved, if more than
    `cap` leave or the appended particles would pass the capacity.  pic_step,
-   pic_step_many and pic_exchange_particles refuse a slab. */
+   pic_step_many and pic_exchange_particles refuse a slab.  The FP32 form
+   uses the same buffers (its fields and particles converted to and from
+   doubles exactly): its mover leaves an x leaver in the ghost cell beside
+   the face, and the particles a slab receives between two reorders are
+   moved one per thread after the bricks. */
 int pic_slab_face_len(pic_handle *h, int64_t *n);
 /* sync = 0: the phase entry points (pic_update_b_half ... pic_reorder and
    the pic_slab_* calls) only enqueue their work on the handle's stream

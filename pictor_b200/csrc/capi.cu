@@ -402,7 +402,7 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 break;
             case PIC_PHASE_MOVE:
                 if (h->sorted)
-                    launch_move_deposit_f32_tiled(g, h->p32[cur], h->bricks, E, B, J, h->err, h->s);
+                    launch_move_deposit_f32_tiled(g, h->p32[cur], h->bricks, h->cnt, E, B, J, h->err, h->s);
                 else
                     launch_move_deposit_f32(g, h->p32[cur], h->cnt, E, B, J, h->err, h->s);
                 break;
@@ -924,12 +924,10 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (c.geom == PIC_GEOM_CYLINDRICAL && (c.dims != 3 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
         return PIC_ERR_INVALID;
     if (c.cyl_modes != 0 && (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4)) return PIC_ERR_INVALID;
-    // the slab form: the reference's FP64 Cartesian step with its x faces on
+    // the slab form: the Cartesian step (FP64 or FP32) with its x faces on
     // neighbouring ranks (no current filter: its passes would need a halo
     // exchange per pass)
-    if (c.slab_x != 0 && (c.slab_x != 1 || c.geom != PIC_GEOM_CARTESIAN || c.precision != PIC_PREC_FP64 ||
-                          c.curr_filter != 0))
-        return PIC_ERR_INVALID;
+    if (c.slab_x != 0 && (c.slab_x != 1 || c.geom != PIC_GEOM_CARTESIAN || c.curr_filter != 0)) return PIC_ERR_INVALID;
     // the exact-order current: FP64 Cartesian, two sorted records per slot
     if (c.exact_current != 0 && (c.exact_current != 1 || c.geom != PIC_GEOM_CARTESIAN ||
                                  c.precision != PIC_PREC_FP64 || c.capacity >= (1ll << 31)))
@@ -1378,7 +1376,7 @@ int pic_move_deposit(pic_handle *h)
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
         if (h->sorted)
-            launch_move_deposit_f32_tiled(h->g, h->p32[h->cur], h->bricks, E, B, J, h->err, h->s);
+            launch_move_deposit_f32_tiled(h->g, h->p32[h->cur], h->bricks, h->cnt, E, B, J, h->err, h->s);
         else
             launch_move_deposit_f32(h->g, h->p32[h->cur], h->cnt, E, B, J, h->err, h->s);
     } else {
@@ -1709,28 +1707,42 @@ int pic_slab_face_len(pic_handle *h, int64_t *n)
     return PIC_OK;
 }
 
+extern "C++" {
+template <typename T>
+static void slab_fields(pic_handle *h, int32_t which, bool pack, double *a, double *b)
+{
+    T *E[3], *B[3], *J[3];
+    field_ptrs(h, E, B, J);
+    T *const *F = which == 0 ? E : which == 1 ? B : J;
+    if (pack) launch_slab_pack_fields<T>(h->g, which, F, a, b, h->s);
+    else launch_slab_unpack_fields<T>(h->g, which, F, a, b, h->s);
+}
+}
+
 int pic_slab_pack_fields(pic_handle *h, int32_t which, double *to_left, double *to_right)
 {
     if (!h || !h->g.x_external || which < 0 || which > 2 || !to_left || !to_right) return PIC_ERR_INVALID;
-    double *E[3], *B[3], *J[3];
-    field_ptrs(h, E, B, J);
-    launch_slab_pack_fields(h->g, which, which == 0 ? E : which == 1 ? B : J, to_left, to_right, h->s);
+    if (h->fp32) slab_fields<float>(h, which, true, to_left, to_right);
+    else slab_fields<double>(h, which, true, to_left, to_right);
     return finish_phase(h);
 }
 
 int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left, const double *from_right)
 {
     if (!h || !h->g.x_external || which < 0 || which > 2 || !from_left || !from_right) return PIC_ERR_INVALID;
-    double *E[3], *B[3], *J[3];
-    field_ptrs(h, E, B, J);
-    launch_slab_unpack_fields(h->g, which, which == 0 ? E : which == 1 ? B : J, from_left, from_right, h->s);
+    if (h->fp32) slab_fields<float>(h, which, false, const_cast<double *>(from_left), const_cast<double *>(from_right));
+    else slab_fields<double>(h, which, false, const_cast<double *>(from_left), const_cast<double *>(from_right));
     return finish_phase(h);
 }
 
 int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_right, int64_t *n_left)
 {
     if (!h || !h->g.x_external || !out || cap < 0 || !n_right || !n_left) return PIC_ERR_INVALID;
-    launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s, out, cap, h->slab_sent);
+    if (h->fp32)
+        launch_slab_pack_f32(h->g, h->p32[h->cur], h->cnt, out, cap, h->sc.hist, h->sc.scan_tmp,
+                             h->sc.scan_tmp + h->sc.scan_tmp_len - 1, h->slab_sent, h->capacity, h->err, h->s);
+    else
+        launch_exchange_f64(h->g, h->p64[h->cur], h->cnt, h->sc, h->capacity, h->err, h->s, out, cap, h->slab_sent);
     uint32_t sent[2] = {0, 0};
     *n_right = 0;
     *n_left = 0;
@@ -1750,7 +1762,8 @@ int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_
 int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n)
 {
     if (!h || !h->g.x_external || n < 0 || (n > 0 && !in)) return PIC_ERR_INVALID;
-    launch_slab_append(h->g, h->p64[h->cur], h->cnt, in, n, h->capacity, h->err, h->s);
+    if (h->fp32) launch_slab_append_f32(h->g, h->p32[h->cur], h->cnt, in, n, h->capacity, h->err, h->s);
+    else launch_slab_append(h->g, h->p64[h->cur], h->cnt, in, n, h->capacity, h->err, h->s);
     return finish_phase(h);
 }
 

@@ -150,8 +150,8 @@ constexpr int kPersistFieldRows = 4;
 void launch_ensemble_persistent(int dims, int fdtd, bool exact_charge, const BatchRun *runs, const int *fstart,
                                 const int *mstart, int n, int nsteps, unsigned *ctl, unsigned spin_limit,
                                 int force_timeout, cudaStream_t s);
-void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
-                                   float *const B[3], float *const J[3], int *err, cudaStream_t s);
+void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, const Counters *cnt,
+                                   float *const E[3], float *const B[3], float *const J[3], int *err, cudaStream_t s);
 // cyl.cu: tiled FP32 cylindrical mover, one CTA per brick (+ the axis current)
 void launch_cyl_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
                                        float *const B[3], float *const J[3], int *err, cudaStream_t s);
@@ -215,10 +215,17 @@ void launch_bc_open_prtl_x(const GridP &g, PartF64 &p, Counters *cnt, int side, 
                            uint32_t *flag, uint32_t *counts, uint32_t *scan_tmp, uint32_t *total, long long capacity,
                            int *err, cudaStream_t s);
 // slab.cu: x faces of a slab (fields and particles), see pic_slab_* in the C ABI
-void launch_slab_pack_fields(const GridP &g, int which, double *const F[3], double *to_left, double *to_right,
-                             cudaStream_t s);
-void launch_slab_unpack_fields(const GridP &g, int which, double *const F[3], const double *from_left,
+template <typename T>
+void launch_slab_pack_fields(const GridP &g, int which, T *const F[3], double *to_left, double *to_right, cudaStream_t s);
+template <typename T>
+void launch_slab_unpack_fields(const GridP &g, int which, T *const F[3], const double *from_left,
                                const double *from_right, cudaStream_t s);
+// the FP32 form's x leavers (slab.cu): to the outbox, and the inbox appended
+void launch_slab_pack_f32(const GridP &g, PartF32 &p, const Counters *cnt, double *out, long long out_cap,
+                          uint32_t *counts, uint32_t *scan_tmp, uint32_t *total, uint32_t *sent, long long capacity,
+                          int *err, cudaStream_t s);
+void launch_slab_append_f32(const GridP &g, PartF32 &p, Counters *cnt, const double *in, long long n,
+                            long long capacity, int *err, cudaStream_t s);
 void launch_slab_append(const GridP &g, PartF64 &p, Counters *cnt, const double *in, long long n, long long capacity,
                         int *err, cudaStream_t s);
 // Stable cell-key reorder (ReorderPrtlArr).  The payload is gathered into

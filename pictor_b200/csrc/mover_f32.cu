@@ -9,33 +9,40 @@ namespace pic {
 // ---------------------------------------------------------------------------
 // Per-particle form (before the first reorder): grid-stride over the array.
 // ---------------------------------------------------------------------------
-template <int DIMS, bool XC>
+// Slots [*first, used) (every slot when first is null): a slab moves the
+// particles it received since its last reorder here, after the tiled launch.
+template <int DIMS, bool XC, bool XS>
 __global__ void __launch_bounds__(kThreads) k_move_f32(GridP g, PartF32 p, const Counters *__restrict__ cnt,
                                                        const float *__restrict__ Ex, const float *__restrict__ Ey,
                                                        const float *__restrict__ Ez, const float *__restrict__ Bx,
                                                        const float *__restrict__ By, const float *__restrict__ Bz,
-                                                       float *Jx, float *Jy, float *Jz, int *err)
+                                                       float *Jx, float *Jy, float *Jz, int *err,
+                                                       const uint32_t *__restrict__ first)
 {
     TileBox tb = {};
     PackedBounds bd;
     const uint32_t step = gridDim.x * blockDim.x;
-    push_range<DIMS, XC>(g, p, blockIdx.x * blockDim.x + threadIdx.x, (uint32_t)cnt->used, step, Ex, Ey, Ez, Bx,
-                            By, Bz, Jx, Jy, Jz, err, tb, bd);
+    const uint32_t n0 = first ? *first : 0u;
+    push_range<DIMS, XC, XS>(g, p, n0 + blockIdx.x * blockDim.x + threadIdx.x, (uint32_t)cnt->used, step, Ex, Ey, Ez,
+                             Bx, By, Bz, Jx, Jy, Jz, err, tb, bd);
 }
 
 void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
                              float *const B[3], float *const J[3], int *err, cudaStream_t s)
 {
     const int grid = kSMs * 16;
-    if (g.dims == 3 && g.exact_charge)
-        k_move_f32<3, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
-                                                     err);
-    else if (g.dims == 3)
-        k_move_f32<3, false><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
-                                                      err);
-    else
-        k_move_f32<2, false><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2],
-                                                      err);
+#define PIC_MOVE_PP(D, X, S)                                                                                         \
+    k_move_f32<D, X, S><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err, \
+                                                   nullptr)
+    const bool xs = g.x_external != 0;
+    if (g.dims == 3 && g.exact_charge) {
+        if (xs) PIC_MOVE_PP(3, true, true); else PIC_MOVE_PP(3, true, false);
+    } else if (g.dims == 3) {
+        if (xs) PIC_MOVE_PP(3, false, true); else PIC_MOVE_PP(3, false, false);
+    } else {
+        if (xs) PIC_MOVE_PP(2, false, true); else PIC_MOVE_PP(2, false, false);
+    }
+#undef PIC_MOVE_PP
     count_launches(1);
 }
 
@@ -43,7 +50,7 @@ void launch_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *c
 // Tiled form: one CTA per brick.
 // ---------------------------------------------------------------------------
 
-template <int DIMS, bool XC, bool PRE>
+template <int DIMS, bool XC, bool PRE, bool XS = false>
 __global__ void __launch_bounds__(kTileThreads, 3)
     k_move_f32_tiled(GridP g, PartF32 p, Bricks bk, const float *__restrict__ Ex, const float *__restrict__ Ey,
                      const float *__restrict__ Ez, const float *__restrict__ Bx, const float *__restrict__ By,
@@ -51,7 +58,7 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 {
     extern __shared__ __align__(16) float sm[];
     __shared__ TileShared ts;
-    move_brick<DIMS, XC, PRE>(g, p, bk, blockIdx.x, sm, ts, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err);
+    move_brick<DIMS, XC, PRE, XS>(g, p, bk, blockIdx.x, sm, ts, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err);
 }
 
 // The node averages of every interior node (node_avg, the same expressions
@@ -127,8 +134,8 @@ void launch_batch_move(int dims, bool exact_charge, const BatchRun *runs, const 
     count_launches(1);
 }
 
-void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, float *const E[3],
-                                   float *const B[3], float *const J[3], int *err, cudaStream_t s)
+void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Bricks &bk, const Counters *cnt,
+                                   float *const E[3], float *const B[3], float *const J[3], int *err, cudaStream_t s)
 {
     static bool attr_set = false;
     const int bytes = bk.smem_floats * 4;
@@ -139,7 +146,42 @@ void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Brick
         cudaFuncSetAttribute(k_move_f32_tiled<3, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
         cudaFuncSetAttribute(k_move_f32_tiled<3, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
         cudaFuncSetAttribute(k_move_f32_tiled<2, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<3, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<3, true, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kBrickSmemBytes);
+        cudaFuncSetAttribute(k_move_f32_tiled<2, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kBrickSmemBytes);
         attr_set = true;
+    }
+    if (g.x_external) {
+        // a slab: the box's x cells include the ghost layers, which the node
+        // arrays (interior nodes only) do not hold, so each brick averages
+        // its own box
+        if (g.dims == 3 && g.exact_charge)
+            k_move_f32_tiled<3, true, false, true><<<bk.ntiles, kTileThreads, bytes, s>>>(
+                g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+        else if (g.dims == 3)
+            k_move_f32_tiled<3, false, false, true><<<bk.ntiles, kTileThreads, bytes, s>>>(
+                g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+        else
+            k_move_f32_tiled<2, false, false, true><<<bk.ntiles, kTileThreads, bytes, s>>>(
+                g, p, bk, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+        // the particles appended since the reorder (received from the
+        // neighbours) are in no brick's range: moved one per thread
+        const uint32_t *first = bk.tile_start + bk.ntiles;
+        const int grid = kSMs * 4;
+        if (g.dims == 3 && g.exact_charge)
+            k_move_f32<3, true, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0],
+                                                               J[1], J[2], err, first);
+        else if (g.dims == 3)
+            k_move_f32<3, false, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0],
+                                                                J[1], J[2], err, first);
+        else
+            k_move_f32<2, false, true><<<grid, kThreads, 0, s>>>(g, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0],
+                                                                J[1], J[2], err, first);
+        count_launches(2);
+        return;
     }
     const bool pre = bk.nodeA != nullptr;
     if (pre) {

@@ -270,7 +270,7 @@ struct PackedBounds {
 // second zigzag segment is then left to the caller (Bq, at box address qa),
 // which deposits those of a warp together.  The cell range is checked where
 // it guards a global access; a cell decoded inside the box is in range.
-template <int DIMS, bool TILED, bool XC = false>
+template <int DIMS, bool TILED, bool XC = false, bool XS = false>
 __device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint32_t n, const PState &s,
                                          const float *__restrict__ Ex, const float *__restrict__ Ey,
                                          const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -291,7 +291,7 @@ __device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint3
     bool inside = false;
     int nb = 0;
     if (TILED) {
-        uo[0] = unwrap_offset(i, tb.hc[0], g.nx);
+        uo[0] = XS ? i - tb.hc[0] : unwrap_offset(i, tb.hc[0], g.nx);
         uo[1] = unwrap_offset(j, tb.hc[1], g.ny);
         if (DIMS == 3) uo[2] = unwrap_offset(k, tb.hc[2], g.nz);
         const int lx = uo[0] - tb.lo[0], ly = uo[1] - tb.lo[1], lz = DIMS == 3 ? uo[2] - tb.lo[2] : 0;
@@ -402,7 +402,9 @@ __device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint3
         bd.add(1, uo[1] + ay);
         if (DIMS == 3) bd.add(2, uo[2] + az);
     }
-    const int ni = wrap_index(i + ax, g.mx), nj = wrap_index(j + ay, g.my);
+    // a slab (XS) leaves an x leaver in the ghost cell beside its face for
+    // the exchange; the single domain wraps it periodically
+    const int ni = XS ? i + ax : wrap_index(i + ax, g.mx), nj = wrap_index(j + ay, g.my);
     const int nk = DIMS == 3 ? wrap_index(k + az, g.mz) : 1;
     p.key[n] = ((uint32_t)flv << kFlvShift) | (uint32_t)((ni - 1) + g.mx * ((nj - 1) + g.my * (nk - 1)));
     p.dx[n] = nx;
@@ -416,7 +418,7 @@ __device__ __forceinline__ bool push_one(const GridP &g, const PartF32 &p, uint3
 
 // Particles [n0, n1) with stride `step`, the next particle prefetched (per-
 // particle form: second segments deposited at once).
-template <int DIMS, bool XC = false>
+template <int DIMS, bool XC = false, bool XS = false>
 __device__ __forceinline__ void push_range(const GridP &g, const PartF32 &p, uint32_t n0, uint32_t n1, uint32_t step,
                                            const float *__restrict__ Ex, const float *__restrict__ Ey,
                                            const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -430,7 +432,7 @@ __device__ __forceinline__ void push_range(const GridP &g, const PartF32 &p, uin
     for (uint32_t n = n0; n < n1; n += step) {
         PState nxt = cur;
         if (n1 - n > step) nxt = load_state<DIMS>(p, n + step);
-        push_one<DIMS, false, XC>(g, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, Bq, qa);
+        push_one<DIMS, false, XC, XS>(g, p, n, cur, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, Bq, qa);
         cur = nxt;
     }
 }
@@ -468,7 +470,7 @@ __device__ __forceinline__ void drain_queue(float (*q)[32], int k, const JOff &j
 // queue and deposited 32 at a time instead of in a branch that nearly every
 // warp would take for a few of its lanes.  The next particle loads while
 // this one moves.
-template <int DIMS, bool XC = false>
+template <int DIMS, bool XC = false, bool XS = false>
 __device__ __forceinline__ void push_range_tiled(const GridP &g, const PartF32 &p, uint32_t p0, uint32_t p1,
                                                  const float *__restrict__ Ex, const float *__restrict__ Ey,
                                                  const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -484,8 +486,8 @@ __device__ __forceinline__ void push_range_tiled(const GridP &g, const PartF32 &
     auto move = [&](const PState &st, uint32_t b) {
         Part Bq;
         uint32_t qa = 0;
-        const bool cross = push_one<DIMS, true, XC>(g, p, b + lane, st, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd,
-                                                Bq, qa);
+        const bool cross = push_one<DIMS, true, XC, XS>(g, p, b + lane, st, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb,
+                                                    bd, Bq, qa);
         const uint32_t m = __ballot_sync(0xffffffffu, cross);
         if (m) {
             const int c = __popc(m);
@@ -521,8 +523,10 @@ __device__ __forceinline__ void push_range_tiled(const GridP &g, const PartF32 &
 }
 
 // Move the particles of brick b (one CTA); PRE: the node averages were
-// computed for the whole grid before the launch (bk.nodeA / nodeB).
-template <int DIMS, bool XC, bool PRE = false>
+// computed for the whole grid before the launch (bk.nodeA / nodeB); XS: the
+// brick belongs to a slab (x not periodic: the box's x cells are the grid's
+// own, ghosts included, and x leavers stay in the ghost layer).
+template <int DIMS, bool XC, bool PRE = false, bool XS = false>
 __device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, const Bricks &bk, int b, float *sm,
                                            TileShared &ts, const float *__restrict__ Ex, const float *__restrict__ Ey,
                                            const float *__restrict__ Ez, const float *__restrict__ Bx,
@@ -535,13 +539,14 @@ __device__ __forceinline__ void move_brick(const GridP &g, const PartF32 &p, con
     int home_lo[3], home_hi[3];
     brick_home<DIMS>(g, bk, b, tb, home_lo, home_hi);
     // a move is below c per axis; the box is the stored bounds (no margin)
-    tile_setup<DIMS, true, false, PRE>(g, bk, b, p1 - p0, 0, g.c_f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By,
-                                       Bz);
+    tile_setup<DIMS, !XS, false, PRE>(g, bk, b, p1 - p0, 0, g.c_f, sm, ts, tb, home_lo, home_hi, Ex, Ey, Ez, Bx, By,
+                                      Bz);
     PackedBounds bd;
     bd.init();
-    push_range_tiled<DIMS, XC>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd, ts.s_q[threadIdx.x >> 5]);
+    push_range_tiled<DIMS, XC, XS>(g, p, p0, p1, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, err, tb, bd,
+                                   ts.s_q[threadIdx.x >> 5]);
     __syncthreads();
-    tile_finish<DIMS, true>(g, bk, b, tb, sm, ts, bd.unpack(), home_lo, home_hi, Jx, Jy, Jz);
+    tile_finish<DIMS, !XS>(g, bk, b, tb, sm, ts, bd.unpack(), home_lo, home_hi, Jx, Jy, Jz);
 }
 
 }  // namespace pic

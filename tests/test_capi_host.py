@@ -102,12 +102,12 @@ def test_cell_decode_division_is_exact():
 
 
 def test_slab_and_wall_entry_points_validate_without_gpu():
-    """The slab form is refused outside the FP64 Cartesian step without a
-    current filter (before any device use), and the slab, wall and sync
+    """The slab form is refused outside the Cartesian step without a current
+    filter (before any device use), and the slab, wall and sync
     entry points reject a null handle and bad arguments."""
     from pictor_b200 import PicConfig, PicError, Simulation, _capi
 
-    for bad in (PicConfig(nx=12, ny=8, slab_x=1, precision="fp32"), PicConfig(nx=12, ny=8, slab_x=2),
+    for bad in (PicConfig(nx=12, ny=8, slab_x=2),
                 PicConfig(nx=12, ny=8, slab_x=1, curr_filter=1),
                 PicConfig(nx=12, ny=8, nz=8, dims=3, slab_x=1, geom="cylindrical")):
         with pytest.raises(PicError) as e:

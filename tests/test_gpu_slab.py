@@ -85,8 +85,8 @@ def test_slabs_track_single_domain(dims, fdtd, nslabs, queued):
 
 def test_slab_refuses_the_periodic_entry_points():
     """A slab's step has exchanges between its phases: pic_step and the
-    single-domain particle exchange refuse it; the slab form is FP64
-    Cartesian without a current filter."""
+    single-domain particle exchange refuse it; the slab form is Cartesian
+    without a current filter."""
     from pictor_b200 import PicError, Simulation
 
     g, cfg = grid_and_config(dims=2, nx=12, ny=8)
@@ -96,8 +96,67 @@ def test_slab_refuses_the_periodic_entry_points():
             s.step(1)
         with pytest.raises(PicError):
             s.exchange_particles()
-    for bad in (dict(precision="fp32"), dict(curr_filter=1)):
+    for bad in (dict(curr_filter=1),):
         g, cfg = grid_and_config(dims=2, nx=12, ny=8, **bad)
         cfg.slab_x = 1
         with pytest.raises(PicError):
             Simulation(cfg)
+
+
+@pytest.mark.parametrize("dims,nslabs", [(3, 2), (2, 3)])
+def test_fp32_slabs_track_single_domain(dims, nslabs):
+    """The FP32 cell-relative form split into slabs: its mover leaves an x
+    leaver in the ghost cell beside the face, the pack sends it in the
+    8-double layout (x in the receiver's coordinates) and leaves a hole, the
+    receiver appends it converted back, and after a reorder the tiled mover
+    moves the bricks while the particles received since then are moved one
+    per thread.  6 steps (reorders at 3 and 6) against the FP32 single
+    periodic domain: the same live particles, positions to 1e-5 of a cell
+    and momenta to 1e-5 (the FP32 currents sum in a different order), E and
+    B to 1e-5 of their scale."""
+    import torch
+
+    from pictor_b200 import Simulation
+    from pictor_b200.slab import join_interior, join_particles, local_domain, split_fields, split_particles
+
+    nx, ny, nz = 24, 8, 8
+    g, cfg = grid_and_config(dims=dims, nx=nx, ny=ny, nz=nz, precision="fp32", capacity=1 << 15, reorder_period=3)
+    f = to_gpu_fields(random_fields(g, seed=73, scale=0.05))
+    p = to_gpu_particles(random_particles(g, n=6000, seed=74, umax=0.8, holes=0.0))
+    with Simulation(cfg) as s:
+        s.load_particles(p)
+        s.load_fields(f)
+        s.step(6)
+        assert s.device_errors() == 0
+        ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096)
+    try:
+        for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
+            sl.sim.load_particles(ps)
+            sl.sim.load_fields(fs)
+        dom.step(6)
+        for sl in dom.slabs:
+            assert sl.sim.device_errors() == 0
+        got_p = join_particles([sl.sim.fetch_particles() for sl in dom.slabs], nx)
+        got_f = [sl.sim.fetch_fields(with_current=False) for sl in dom.slabs]
+    finally:
+        dom.close()
+    lens = (nx, ny, nz if dims == 3 else 0)
+    a, b = _sorted(got_p, lens), _sorted(ref_p, lens)
+    assert len(a["x"]) == len(b["x"]) == 6000
+    np.testing.assert_array_equal(a["flv"], b["flv"])
+    for k, L in zip(("x", "y", "z"), lens):
+        d = a[k] - b[k]
+        if L:
+            d -= L * np.round(d / L)
+        assert np.abs(d).max() <= 1e-5, (k, np.abs(d).max())
+    for k in ("u", "v", "w"):
+        np.testing.assert_allclose(a[k], b[k], rtol=0, atol=1e-5, err_msg=k)
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        ref = getattr(ref_f, n)[2:-3]
+        got = join_interior(got_f, n)
+        if dims == 3:
+            ref, got = ref[:, 2:-3, 2:-3], got[:, 2:-3, 2:-3]
+        else:
+            ref, got = ref[:, 2:-3], got[:, 2:-3]
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5 * max(np.abs(ref).max(), 1e-30), err_msg=n)
