@@ -39,14 +39,24 @@ __device__ __forceinline__ uint32_t lanemask_lt_b()
     return m;
 }
 
+// a / t[d] of a brick axis by multiply-shift (a < 2^28).
+__device__ __forceinline__ uint32_t brick_axis(const Bricks &bk, int d, int a)
+{
+    return bk.t[d] == 1 ? (uint32_t)a : (uint32_t)fast_div((unsigned)a, bk.tmagic[d], bk.tshift[d]);
+}
+
 // Brick of an interior cell (1-based indices 3..n+2), x fastest.
 __device__ __forceinline__ uint32_t brick_of(const Bricks &bk, int i, int j, int k)
 {
-    const int bx = (i - 3) / bk.t[0], by = (j - 3) / bk.t[1], bz = (k - 3) / bk.t[2];
-    return (uint32_t)bx + (uint32_t)bk.nb[0] * ((uint32_t)by + (uint32_t)bk.nb[1] * (uint32_t)bz);
+    const uint32_t bx = brick_axis(bk, 0, i - 3), by = brick_axis(bk, 1, j - 3), bz = brick_axis(bk, 2, k - 3);
+    return bx + (uint32_t)bk.nb[0] * (by + (uint32_t)bk.nb[1] * bz);
 }
 
 constexpr uint32_t kNoBrick = 0xffffffffu;
+
+// Runs of 32 slots a warp loads before it works on them (count and slots
+// passes): the loads of four runs are in flight at once.
+constexpr int kRuns = 4;
 
 // 1. brick id of every slot (kNoBrick for holes) and per-brick counts.
 __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, PartF32 p, const Counters *__restrict__ cnt,
@@ -54,29 +64,36 @@ __global__ void __launch_bounds__(kThreads) k_brick_count(GridP g, Bricks bk, Pa
 {
     const long long used = cnt->used;
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long stride = (long long)gridDim.x * blockDim.x * kRuns;
     uint32_t wmax = 0;   // max |w| bits seen by this thread
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < used; base += stride) {
-        const long long n = base + lane;
-        uint32_t b = kNoBrick, wbits = 0;
-        if (n < used) {
-            const uint32_t key = p.key[n];
-            if ((key >> kFlvShift) != 0) {
-                wbits = __float_as_uint(fabsf(p.w[n]));
+    for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * kRuns; base < used;
+         base += stride) {
+        uint32_t key[kRuns], wb[kRuns];
+#pragma unroll
+        for (int u = 0; u < kRuns; u++) {
+            const long long n = base + 32 * u + lane;
+            key[u] = n < used ? p.key[n] : 0u;
+            wb[u] = n < used ? __float_as_uint(fabsf(p.w[n])) : 0u;
+        }
+#pragma unroll
+        for (int u = 0; u < kRuns; u++) {
+            const long long n = base + 32 * u + lane;
+            uint32_t b = kNoBrick;
+            if ((key[u] >> kFlvShift) != 0) {   // holes and slots past `used` have key 0
                 int i, j, k;
-                decode_cell(g, (int)(key & kCellMask), i, j, k);
+                decode_cell(g, (int)(key[u] & kCellMask), i, j, k);
                 if (i < 3 || i > g.mx - 3 || j < 3 || j > g.my - 3 ||
                     (g.dims == 3 ? (k < 3 || k > g.mz - 3) : k != 1)) {
                     raise_error(err, PIC_DEVERR_RANGE);  // dropped like a hole
                 } else {
                     b = brick_of(bk, i, j, g.dims == 3 ? k : 3);
                 }
+                wmax = max(wmax, wb[u]);   // |w| bit patterns order as integers
             }
-            bid[n] = b;
+            if (n < used) bid[n] = b;
+            const uint32_t peers = __match_any_sync(0xffffffffu, b);
+            if (b != kNoBrick && (peers & lanemask_lt_b()) == 0) atomicAdd(&bk.count[b], (uint32_t)__popc(peers));
         }
-        const uint32_t peers = __match_any_sync(0xffffffffu, b);
-        if (b != kNoBrick && (peers & lanemask_lt_b()) == 0) atomicAdd(&bk.count[b], (uint32_t)__popc(peers));
-        wmax = max(wmax, wbits);   // |w| bit patterns order as integers
     }
     // one atomic per block
     __shared__ uint32_t s_w[kThreads / 32];
@@ -98,18 +115,35 @@ __global__ void __launch_bounds__(kThreads) k_brick_slots(Bricks bk, PartF32 in,
 {
     const long long used = cnt->used;
     const int lane = threadIdx.x & 31;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < used; base += stride) {
-        const long long n = base + lane;
-        const uint32_t b = n < used ? bid[n] : kNoBrick;
-        const uint32_t peers = __match_any_sync(0xffffffffu, b);
-        const int leader = __ffs(peers) - 1;
-        uint32_t slot = 0;
-        if (b != kNoBrick && lane == leader) slot = atomicAdd(&bk.cursor[b], (uint32_t)__popc(peers));
-        slot = __shfl_sync(0xffffffffu, slot, leader) + (uint32_t)__popc(peers & lanemask_lt_b());
-        if (b == kNoBrick) continue;
-        out.key[slot] = in.key[n];
-        bk.src[slot] = (uint32_t)n;
+    const long long stride = (long long)gridDim.x * blockDim.x * kRuns;
+    for (long long base = ((long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31)) * kRuns; base < used;
+         base += stride) {
+        uint32_t bs[kRuns], key[kRuns];
+#pragma unroll
+        for (int u = 0; u < kRuns; u++) {
+            const long long n = base + 32 * u + lane;
+            bs[u] = n < used ? bid[n] : kNoBrick;
+            key[u] = n < used ? in.key[n] : 0u;
+        }
+        // the cursor atomics of all runs issued before any result is used
+        uint32_t peers[kRuns], slot[kRuns];
+#pragma unroll
+        for (int u = 0; u < kRuns; u++) {
+            peers[u] = __match_any_sync(0xffffffffu, bs[u]);
+            slot[u] = 0;
+            if (bs[u] != kNoBrick && (peers[u] & lanemask_lt_b()) == 0)
+                slot[u] = atomicAdd(&bk.cursor[bs[u]], (uint32_t)__popc(peers[u]));
+        }
+#pragma unroll
+        for (int u = 0; u < kRuns; u++) {
+            const long long n = base + 32 * u + lane;
+            const int leader = __ffs(peers[u]) - 1;
+            const uint32_t at = __shfl_sync(0xffffffffu, slot[u], leader) + (uint32_t)__popc(peers[u] & lanemask_lt_b());
+            if (bs[u] != kNoBrick) {
+                out.key[at] = key[u];
+                bk.src[at] = (uint32_t)n;
+            }
+        }
     }
 }
 
@@ -133,19 +167,44 @@ __host__ __device__ inline uint32_t transposed_slot(uint32_t s, uint32_t N, uint
     return col * R + row;
 }
 
+// Payload array a of the FP32 particle record as 32-bit words: key, dx, dy,
+// dz, ux, uy, uz, w.
+__device__ __forceinline__ uint32_t *payload_words(const PartF32 &p, int a)
+{
+    switch (a) {
+        case 0: return p.key;
+        case 1: return reinterpret_cast<uint32_t *>(p.dx);
+        case 2: return reinterpret_cast<uint32_t *>(p.dy);
+        case 3: return reinterpret_cast<uint32_t *>(p.dz);
+        case 4: return reinterpret_cast<uint32_t *>(p.ux);
+        case 5: return reinterpret_cast<uint32_t *>(p.uy);
+        case 6: return reinterpret_cast<uint32_t *>(p.uz);
+        default: return reinterpret_cast<uint32_t *>(p.w);
+    }
+}
+
 constexpr int kOrderThreads = 512;
-// Particles of a brick whose payload the order pass stages through shared
-// memory (a 16-bit final slot and a staging word each); a larger brick
-// writes its slots directly.
-constexpr uint32_t kOrderStage = 8192;
+// Particles of a brick that the order pass orders through shared memory (a
+// 16-bit rank and a source index each; 1.5x the 4096 particles the brick
+// shapes aim at); a larger brick keeps its final slots in bk.bid and writes
+// them directly.  The payload reads of the staged path are served by L1,
+// which gets what shared memory leaves of each SM: at 37 KB per CTA and three
+// CTAs per SM (40 registers at 512 threads) the whole reorder of the 3D
+// Weibel headline takes 18.7 ms; with 8192 staged particles (49 KB per CTA)
+// 20.4 ms, and with 8192 at four CTAs per SM (registers capped at 32) 50 ms.
+constexpr uint32_t kOrderStage = 6144;
+// Payload words a thread has in flight per array in the staged path.
+constexpr int kOrderBatch = 8;
 
 // 5. order brick b by cell and transpose (see the file comment).  Dynamic
-//    shared memory: one counter per cell of the brick, then a staging word
-//    and a 16-bit final slot per particle.  A brick of at most kOrderStage
-//    particles moves each payload array through shared memory: read in the
-//    brick-grouped order (which follows the old order, so reads stay close
-//    to coalesced), placed by final slot, written out contiguously.  A larger
-//    brick keeps its final slots in bk.bid and writes them directly.
+//    shared memory: one counter per cell of the brick, then the source index
+//    of every final slot (the inverse permutation) and a 16-bit rank per
+//    particle.  A brick of at most kOrderStage particles builds the inverse
+//    permutation in shared memory, after which every payload array is
+//    written slot by slot (coalesced) from its source slot, a read that
+//    stays inside the few KB of old slots the brick's particles came from;
+//    the arrays need no barrier between them.  A larger brick keeps its
+//    final slots in bk.bid and scatters each payload word to its final slot.
 __global__ void __launch_bounds__(kOrderThreads) k_brick_order(GridP g, Bricks bk, PartF32 in, PartF32 out, int has_dz)
 {
     extern __shared__ uint32_t s_dyn[];
@@ -155,8 +214,8 @@ __global__ void __launch_bounds__(kOrderThreads) k_brick_order(GridP g, Bricks b
     if (N == 0) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int R = bk.t[0] * bk.t[1] * bk.t[2];
-    uint32_t *s_cnt = s_dyn, *s_st = s_dyn + R;
-    uint16_t *s_m = reinterpret_cast<uint16_t *>(s_st + kOrderStage);
+    uint32_t *s_cnt = s_dyn, *s_inv = s_dyn + R;
+    uint16_t *s_m = reinterpret_cast<uint16_t *>(s_inv + kOrderStage);
     const int bx = b % bk.nb[0], byz = b / bk.nb[0], by = byz % bk.nb[1], bz = byz / bk.nb[1];
     const int lo0 = 3 + bx * bk.t[0], lo1 = 3 + by * bk.t[1], lo2 = 3 + bz * bk.t[2];
     for (int c = tid; c < R; c += kOrderThreads) s_cnt[c] = 0;
@@ -171,14 +230,10 @@ __global__ void __launch_bounds__(kOrderThreads) k_brick_order(GridP g, Bricks b
     const uint32_t *__restrict__ gkey = out.key + p0;   // keys of the brick-grouped slots
     const uint32_t *__restrict__ src = bk.src + p0;
     uint32_t *__restrict__ tmp = bk.bid + p0;
-    // rank within the cell (and the cell, when staged)
+    // rank within the cell
     if (staged) {
 #pragma unroll 4
-        for (uint32_t q = tid; q < N; q += kOrderThreads) {
-            const int c = local_cell(gkey[q]);
-            s_m[q] = (uint16_t)atomicAdd(&s_cnt[c], 1u);
-            s_st[q] = (uint32_t)c;
-        }
+        for (uint32_t q = tid; q < N; q += kOrderThreads) s_m[q] = (uint16_t)atomicAdd(&s_cnt[local_cell(gkey[q])], 1u);
     } else {
         for (uint32_t q = tid; q < N; q += kOrderThreads) tmp[q] = atomicAdd(&s_cnt[local_cell(gkey[q])], 1u);
     }
@@ -207,47 +262,39 @@ __global__ void __launch_bounds__(kOrderThreads) k_brick_order(GridP g, Bricks b
         }
     }
     __syncthreads();
-    const uint32_t *srcs[8] = {in.key,
-                               reinterpret_cast<const uint32_t *>(in.dx),
-                               reinterpret_cast<const uint32_t *>(in.dy),
-                               reinterpret_cast<const uint32_t *>(in.dz),
-                               reinterpret_cast<const uint32_t *>(in.ux),
-                               reinterpret_cast<const uint32_t *>(in.uy),
-                               reinterpret_cast<const uint32_t *>(in.uz),
-                               reinterpret_cast<const uint32_t *>(in.w)};
-    uint32_t *dsts[8] = {out.key,
-                         reinterpret_cast<uint32_t *>(out.dx),
-                         reinterpret_cast<uint32_t *>(out.dy),
-                         reinterpret_cast<uint32_t *>(out.dz),
-                         reinterpret_cast<uint32_t *>(out.ux),
-                         reinterpret_cast<uint32_t *>(out.uy),
-                         reinterpret_cast<uint32_t *>(out.uz),
-                         reinterpret_cast<uint32_t *>(out.w)};
     if (staged) {
+#pragma unroll 4
         for (uint32_t q = tid; q < N; q += kOrderThreads)
-            s_m[q] = (uint16_t)transposed_slot(s_cnt[s_st[q]] + s_m[q], N, (uint32_t)R);
-        __syncthreads();   // every key of the brick read before the key array is rewritten
-#pragma unroll 1
+            s_inv[transposed_slot(s_cnt[local_cell(gkey[q])] + s_m[q], N, (uint32_t)R)] = src[q];
+        __syncthreads();   // the inverse permutation complete, every key of the brick read
+#pragma unroll
         for (int a = 0; a < 8; a++) {
             if (a == 3 && !has_dz) continue;
-            const uint32_t *__restrict__ sa = srcs[a];
-#pragma unroll 4
-            for (uint32_t q = tid; q < N; q += kOrderThreads) s_st[s_m[q]] = sa[src[q]];
-            __syncthreads();
-            uint32_t *__restrict__ da = dsts[a] + p0;
-#pragma unroll 4
-            for (uint32_t t = tid; t < N; t += kOrderThreads) da[t] = s_st[t];
-            __syncthreads();
+            const uint32_t *__restrict__ sa = payload_words(in, a);
+            uint32_t *__restrict__ da = payload_words(out, a) + p0;
+            for (uint32_t t0 = tid; t0 < N; t0 += kOrderBatch * kOrderThreads) {
+                uint32_t v[kOrderBatch];
+#pragma unroll
+                for (int r = 0; r < kOrderBatch; r++) {
+                    const uint32_t t = t0 + r * kOrderThreads;
+                    if (t < N) v[r] = ldro(sa + s_inv[t]);
+                }
+#pragma unroll
+                for (int r = 0; r < kOrderBatch; r++) {
+                    const uint32_t t = t0 + r * kOrderThreads;
+                    if (t < N) da[t] = v[r];
+                }
+            }
         }
     } else {
         for (uint32_t q = tid; q < N; q += kOrderThreads)
             tmp[q] = transposed_slot(s_cnt[local_cell(gkey[q])] + tmp[q], N, (uint32_t)R);
         __syncthreads();   // every key of the brick read before any slot is overwritten
-#pragma unroll 1
+#pragma unroll
         for (int a = 0; a < 8; a++) {
             if (a == 3 && !has_dz) continue;
-            const uint32_t *__restrict__ sa = srcs[a];
-            uint32_t *__restrict__ da = dsts[a] + p0;
+            const uint32_t *__restrict__ sa = payload_words(in, a);
+            uint32_t *__restrict__ da = payload_words(out, a) + p0;
             for (uint32_t q = tid; q < N; q += kOrderThreads) da[tmp[q]] = sa[src[q]];
         }
     }
@@ -342,6 +389,9 @@ bool choose_bricks(const GridP &g, double ppc, const int req[3], Bricks &bk)
     for (int d = 0; d < 3; d++) {
         bk.t[d] = d < g.dims ? (t[d] < n3[d] ? t[d] : n3[d]) : 1;
         bk.nb[d] = d < g.dims ? (n3[d] + bk.t[d] - 1) / bk.t[d] : 1;
+        bk.tmagic[d] = 0;
+        bk.tshift[d] = 0;
+        if (bk.t[d] >= 2) div_magic((unsigned)bk.t[d], bk.tmagic[d], bk.tshift[d]);
     }
     bk.ntiles = bk.nb[0] * bk.nb[1] * bk.nb[2];
     bk.smem_floats = kBrickSmemBytes / 4;

@@ -102,6 +102,8 @@ struct Bricks {
     float4 *nodeA;          // node-averaged Ex, Ey, Ez, Bx (+ bext) at every interior node, or null
     float2 *nodeB;          // node-averaged By, Bz (+ bext); both written before each tiled move
     int t[3], nb[3], ntiles;
+    unsigned int tmagic[3];   // x / t[d] = fast_div(x, tmagic[d], tshift[d]) for t[d] >= 2 (div_magic)
+    int tshift[3];
     int smem_floats;
 };
 // Shared words of a mover box of C cells: (C+1) nodes per axis x 6 field
