@@ -210,6 +210,22 @@ int pic_bc_open_x(pic_handle *h, int32_t side, double pos);
    the serial sum in the last bit.  PIC_ERR_OVERFLOW (nothing appended) when
    the copies do not fit in the capacity. */
 int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos);
+/* Faces of type 'pml' (SetBC_Fld, bc.F90:45-50): the convolutional PML of
+   bc_pml.F90 with SetPMLParameters' profile (n = 4, kappa_max = 1,
+   sigma_max = 1, alpha_max = 9e-4).  pic_bc_pml sets the faces: bit n-1 of
+   `faces` marks bc_face(n) (1, 2 x; 3, 4 y; 5, 6 z, 3D only) at pos[n-1]
+   (pos_fld, cells from the first interior cell) with thickness[n-1]
+   (attn_thickness, SetBC_Fld default 4); the twelve auxiliary grids
+   (pml_E_psi1/2, pml_B_psi1/2) are zeroed on the first call and kept by later
+   ones (moved faces); faces = 0 switches the PML off.  pic_bc_pml_b is
+   UpdateMagFld_PML + SendRecvFlds(B), called after the second
+   pic_update_b_half (MAIN.F90:103-105); pic_bc_pml_e is UpdateElcFld_PML +
+   SendRecvFlds(E), called after pic_update_e (:108-110).  Both do nothing
+   while the grid lies inside the faces (no_pml_this_domain).  FP64 or FP32
+   Cartesian single domain. */
+int pic_bc_pml(pic_handle *h, int32_t faces, const double *pos, const double *thickness);
+int pic_bc_pml_b(pic_handle *h);
+int pic_bc_pml_e(pic_handle *h);
 /* Particle injection at a face of type 'iflw' (SetBC_InflowPrtl, bc.F90:67-153):
    InjectNewPrtl (bc_inflow.F90:134-256) with 'rndm' placement, called where
    EnforceBC_PostMovDep calls InflowBC_Prtl (bc.F90:240, after

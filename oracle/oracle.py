@@ -77,6 +77,35 @@ class Inflow(C.Structure):
     ]
 
 
+class _Pml(C.Structure):
+    _fields_ = [
+        ("faces", C.c_int32), ("pos", C.c_double * 6), ("thickness", C.c_double * 6),
+        ("psiE", C.POINTER(C.c_double) * 6), ("psiB", C.POINTER(C.c_double) * 6),
+    ]
+
+
+class Pml:
+    """The 'pml' faces {n: (pos, thickness)} (n = 1..6) and their twelve
+    convolution arrays (pml_E_psi1/2, pml_B_psi1/2: x, y, z), zero at start."""
+
+    def __init__(self, g: Grid, faces: dict):
+        self.faces = {int(n): (float(p), float(t)) for n, (p, t) in faces.items()}
+        shp = grid_shape(g)
+        self.psiE = [np.zeros(shp, dtype=np.float64, order="F") for _ in range(6)]
+        self.psiB = [np.zeros(shp, dtype=np.float64, order="F") for _ in range(6)]
+
+    def struct(self) -> _Pml:
+        s = _Pml()
+        for n, (p, t) in self.faces.items():
+            s.faces |= 1 << (n - 1)
+            s.pos[n - 1] = p
+            s.thickness[n - 1] = t
+        for c in range(6):
+            s.psiE[c] = _dp(self.psiE[c])
+            s.psiB[c] = _dp(self.psiB[c])
+        return s
+
+
 class _Weibel(C.Structure):
     _fields_ = [
         ("dims", C.c_int), ("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
@@ -119,6 +148,8 @@ def _declare(L: C.CDLL) -> None:
     L.orc_inject.argtypes = [P(Grid), P(_Particles), P(Inflow)]
     L.orc_inject.restype = C.c_int64
     L.orc_refl_fluid_right.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_double, C.c_double]
+    for fn in ("orc_pml_b", "orc_pml_e"):
+        getattr(L, fn).argtypes = [P(Grid), P(_Fields), P(_Pml)]
     L.orc_step.argtypes = [P(Grid), P(_Particles), P(_Fields), C.c_int, C.c_int]
     L.orc_step.restype = C.c_int
     L.orc_field_energy.argtypes = [P(Grid), P(_Fields), P(C.c_double)]
@@ -320,6 +351,16 @@ class Oracle:
         fs = self.f.struct()
         fn = self.L.orc_cond_fld_bottom if side == 0 else self.L.orc_cond_fld_top
         fn(C.byref(self.g), C.byref(fs), float(pos))
+
+    def pml_b(self, pml: "Pml"):
+        """UpdateMagFld_PML (after the second B half step; no halo refresh)."""
+        fs, ps = self.f.struct(), pml.struct()
+        self.L.orc_pml_b(C.byref(self.g), C.byref(fs), C.byref(ps))
+
+    def pml_e(self, pml: "Pml"):
+        """UpdateElcFld_PML (after the E update; no halo refresh)."""
+        fs, ps = self.f.struct(), pml.struct()
+        self.L.orc_pml_e(C.byref(self.g), C.byref(fs), C.byref(ps))
 
     def attenuate_vacuum(self, faces: dict):
         """Attenuate_EM_Vacuum for the 'attn' faces {n: (pos, scale)}, n = 1..6."""

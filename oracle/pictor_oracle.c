@@ -1629,3 +1629,195 @@ int64_t orc_inject(const orc_grid *g, orc_particles *p, const orc_inflow *f)
     }
     return p->used - used0;
 }
+
+/* ---- convolutional PML, bc_pml.F90 ------------------------------------- */
+
+/* The profile of every face: pml_pos / pml_pos_ind of Update_PML_Position
+   (bc_pml.F90:56-71) and pml_params_arr as SetPMLParameters (:42-53) sets a
+   'pml' face; the other faces keep the type's defaults (:6-12) and the
+   +-huge(1) positions.  alpha_max is the default-kind literal 9.0e-4. */
+typedef struct {
+    double pos[6], ind[6], L[6], kmax[6], smax[6], amax[6];
+    int n[6];
+} pml_profile;
+
+static void pml_profile_init(const orc_pml *p, pml_profile *q)
+{
+    const double huge = 2147483647.0;   /* huge(1) */
+    for (int f = 0; f < 6; f++) {
+        const int upper = f & 1;        /* bc_face 2, 4, 6 */
+        q->n[f] = 4;
+        q->kmax[f] = 1.0;
+        if ((p->faces >> f) & 1) {
+            q->L[f] = p->thickness[f];
+            q->smax[f] = 1.0;
+            q->amax[f] = (double)9.0e-4f;
+            q->pos[f] = p->pos[f];
+            q->ind[f] = upper ? ceil(p->pos[f]) + 1.0 : floor(p->pos[f]) - 1.0;
+        } else {
+            q->L[f] = 10.0;
+            q->smax[f] = 0.0;
+            q->amax[f] = 1.0;
+            q->pos[f] = upper ? huge : -huge;
+            q->ind[f] = upper ? huge : -huge;
+        }
+    }
+}
+
+/* x**n for an integer n >= 0 by squaring, as gfortran evaluates a real to a
+   variable integer power. */
+static double ipow(double x, int n)
+{
+    double y = (n & 1) ? x : 1.0;
+    while (n >>= 1) {
+        x = x * x;
+        if (n & 1) y = y * x;
+    }
+    return y;
+}
+
+static double pml_kappa(const pml_profile *q, double d, int f)   /* :330-335 */
+{
+    const double k = 1.0 + ipow(d / q->L[f], q->n[f]) * (q->kmax[f] - 1.0);
+    return q->kmax[f] < k ? q->kmax[f] : k;
+}
+static double pml_sigma(const pml_profile *q, double d, int f)   /* :337-341 */
+{
+    const double s = q->smax[f] * ipow(d / q->L[f], q->n[f]);
+    return q->smax[f] < s ? q->smax[f] : s;
+}
+
+/* pml_c (:271-288) */
+static double pml_c(const pml_profile *q, double fc, double x, int axis)
+{
+    double c = 0.0;
+    const int lo = 2 * axis, hi = 2 * axis + 1;
+    if (x > q->pos[hi]) c = fc * (1.0 / pml_kappa(q, x - q->pos[hi], hi) - 1.0);
+    if (x < q->pos[lo]) c = fc * (1.0 / pml_kappa(q, q->pos[lo] - x, lo) - 1.0);
+    return c;
+}
+
+/* pml_ab (:290-316) */
+static void pml_ab(const pml_profile *q, double x, int axis, double *a, double *b)
+{
+    const int lo = 2 * axis, hi = 2 * axis + 1;
+    *a = 0.0;
+    *b = 0.0;
+    for (int side = 0; side < 2; side++) {
+        const int f = side == 0 ? hi : lo;
+        if (side == 0 ? !(x > q->pos[hi]) : !(x < q->pos[lo])) continue;
+        const double d = side == 0 ? x - q->pos[hi] : q->pos[lo] - x;
+        const double alpha = q->amax[f], sigma = pml_sigma(q, d, f), kappa = pml_kappa(q, d, f);
+        *a = exp(-(sigma / kappa) - alpha);
+        *b = (sigma / (sigma * kappa + alpha * (kappa * kappa))) * (*a - 1.0);
+    }
+}
+
+/* no_pml_this_domain (:67-69) with xborders = yborders = zborders = 0 */
+static int pml_outside_grid(const orc_grid *g, const pml_profile *q)
+{
+    return 1 - 3 > q->ind[0] && g->mx - 3 < q->ind[1] && 1 - 3 > q->ind[2] && g->my - 3 < q->ind[3] &&
+           1 - 3 > q->ind[4] && g->mz - 3 < q->ind[5];
+}
+
+/* beyond the layer of the faces of one axis: x < pos(lo) - L(lo) or x > pos(hi) + L(hi) */
+static int pml_beyond(const pml_profile *q, double x, int axis)
+{
+    return x < q->pos[2 * axis] - q->L[2 * axis] || x > q->pos[2 * axis + 1] + q->L[2 * axis + 1];
+}
+
+/* UpdateElcFld_PML (bc_pml.F90:83-144): E = E + the convolution terms at the
+   cells outside the interior box; E beyond the layers zeroed. */
+void orc_pml_e(const orc_grid *g, orc_fields *f, orc_pml *p)
+{
+    pml_profile q;
+    pml_profile_init(p, &q);
+    if (pml_outside_grid(g, &q)) return;
+    const int three_d = g->dims == 3;
+    const double fc = g->c;
+    double *p1x = p->psiE[0], *p1y = p->psiE[1], *p1z = p->psiE[2];
+    double *p2x = p->psiE[3], *p2y = p->psiE[4], *p2z = p->psiE[5];
+    const int k0 = three_d ? 2 : 1, k1 = three_d ? g->mz - 1 : 1;
+    for (int k = k0; k <= k1; k++)
+        for (int j = 2; j <= g->my - 1; j++)
+            for (int i = 2; i <= g->mx - 1; i++) {
+                const double xg = i - 3, yg = j - 3, zg = k - 3;
+                const int inside = xg > q.ind[0] && xg < q.ind[1] && yg > q.ind[2] && yg < q.ind[3] &&
+                                   zg > q.ind[4] && zg < q.ind[5];
+                if (inside) continue;
+                double ax, bx, ay, by, az, bz;
+                pml_ab(&q, xg, 0, &ax, &bx);
+                pml_ab(&q, yg, 1, &ay, &by);
+                pml_ab(&q, zg, 2, &az, &bz);
+                const double cx = pml_c(&q, fc, xg, 0), cy = pml_c(&q, fc, yg, 1), cz = pml_c(&q, fc, zg, 2);
+                const int64_t c = ID(g, i, j, k), cxm = ID(g, i - 1, j, k), cym = ID(g, i, j - 1, k);
+                const int64_t czm = three_d ? ID(g, i, j, k - 1) : c;
+                p1x[c] = ay * p1x[c] + (by * fc) * (f->Bz[c] - f->Bz[cym]);
+                p1z[c] = ax * p1z[c] + (bx * fc) * (f->By[c] - f->By[cxm]);
+                if (three_d) {
+                    p1y[c] = az * p1y[c] + (bz * fc) * (f->Bx[c] - f->Bx[czm]);
+                    p2x[c] = az * p2x[c] + (bz * fc) * (f->By[c] - f->By[czm]);
+                }
+                p2y[c] = ax * p2y[c] + (bx * fc) * (f->Bz[c] - f->Bz[cxm]);
+                p2z[c] = ay * p2z[c] + (by * fc) * (f->Bx[c] - f->Bx[cym]);
+                if (three_d) {
+                    f->Ex[c] = ((f->Ex[c] + cy * (f->Bz[c] - f->Bz[cym])) - cz * (f->By[c] - f->By[czm])) + p1x[c] - p2x[c];
+                    f->Ey[c] = ((f->Ey[c] + cz * (f->Bx[c] - f->Bx[czm])) - cx * (f->Bz[c] - f->Bz[cxm])) + p1y[c] - p2y[c];
+                } else {
+                    f->Ex[c] = (f->Ex[c] + cy * (f->Bz[c] - f->Bz[cym])) + p1x[c];
+                    f->Ey[c] = (f->Ey[c] - cx * (f->Bz[c] - f->Bz[cxm])) - p2y[c];
+                }
+                f->Ez[c] = ((f->Ez[c] + cx * (f->By[c] - f->By[cxm])) - cy * (f->Bx[c] - f->Bx[cym])) + p1z[c] - p2z[c];
+                if (pml_beyond(&q, xg + 0.5, 0) || pml_beyond(&q, yg, 1) || pml_beyond(&q, zg, 2)) f->Ex[c] = 0.0;
+                if (pml_beyond(&q, xg, 0) || pml_beyond(&q, yg + 0.5, 1) || pml_beyond(&q, zg, 2)) f->Ey[c] = 0.0;
+                if (pml_beyond(&q, xg, 0) || pml_beyond(&q, yg, 1) || pml_beyond(&q, zg + 0.5, 2)) f->Ez[c] = 0.0;
+            }
+}
+
+/* UpdateMagFld_PML (bc_pml.F90:146-264): the same for B at the half-cell
+   positions; the interior test on the integer ones. */
+void orc_pml_b(const orc_grid *g, orc_fields *f, orc_pml *p)
+{
+    pml_profile q;
+    pml_profile_init(p, &q);
+    if (pml_outside_grid(g, &q)) return;
+    const int three_d = g->dims == 3;
+    const double fc = g->c;
+    double *p1x = p->psiB[0], *p1y = p->psiB[1], *p1z = p->psiB[2];
+    double *p2x = p->psiB[3], *p2y = p->psiB[4], *p2z = p->psiB[5];
+    const int k0 = three_d ? 2 : 1, k1 = three_d ? g->mz - 1 : 1;
+    for (int k = k0; k <= k1; k++)
+        for (int j = 2; j <= g->my - 1; j++)
+            for (int i = 2; i <= g->mx - 1; i++) {
+                const int inside = i - 3 > q.ind[0] && i - 3 < q.ind[1] && j - 3 > q.ind[2] && j - 3 < q.ind[3] &&
+                                   k - 3 > q.ind[4] && k - 3 < q.ind[5];
+                if (inside) continue;
+                const double xg = (i - 3) + 0.5, yg = (j - 3) + 0.5, zg = (k - 3) + 0.5;
+                double ax, bx, ay, by, az, bz;
+                pml_ab(&q, xg, 0, &ax, &bx);
+                pml_ab(&q, yg, 1, &ay, &by);
+                pml_ab(&q, zg, 2, &az, &bz);
+                const double cx = pml_c(&q, fc, xg, 0), cy = pml_c(&q, fc, yg, 1), cz = pml_c(&q, fc, zg, 2);
+                const int64_t c = ID(g, i, j, k), cxp = ID(g, i + 1, j, k), cyp = ID(g, i, j + 1, k);
+                const int64_t czp = three_d ? ID(g, i, j, k + 1) : c;
+                p1x[c] = ay * p1x[c] + (by * fc) * (f->Ez[cyp] - f->Ez[c]);
+                p1z[c] = ax * p1z[c] + (bx * fc) * (f->Ey[cxp] - f->Ey[c]);
+                if (three_d) {
+                    p1y[c] = az * p1y[c] + (bz * fc) * (f->Ex[czp] - f->Ex[c]);
+                    p2x[c] = az * p2x[c] + (bz * fc) * (f->Ey[czp] - f->Ey[c]);
+                }
+                p2y[c] = ax * p2y[c] + (bx * fc) * (f->Ez[cxp] - f->Ez[c]);
+                p2z[c] = ay * p2z[c] + (by * fc) * (f->Ex[cyp] - f->Ex[c]);
+                if (three_d) {
+                    f->Bx[c] = ((f->Bx[c] - cy * (f->Ez[cyp] - f->Ez[c])) + cz * (f->Ey[czp] - f->Ey[c])) - p1x[c] + p2x[c];
+                    f->By[c] = ((f->By[c] - cz * (f->Ex[czp] - f->Ex[c])) + cx * (f->Ez[cxp] - f->Ez[c])) - p1y[c] + p2y[c];
+                } else {
+                    f->Bx[c] = (f->Bx[c] - cy * (f->Ez[cyp] - f->Ez[c])) - p1x[c];
+                    f->By[c] = (f->By[c] + cx * (f->Ez[cxp] - f->Ez[c])) + p2y[c];
+                }
+                f->Bz[c] = ((f->Bz[c] - cx * (f->Ey[cxp] - f->Ey[c])) + cy * (f->Ex[cyp] - f->Ex[c])) - p1z[c] + p2z[c];
+                if (pml_beyond(&q, xg - 0.5, 0) || pml_beyond(&q, yg, 1) || pml_beyond(&q, zg, 2)) f->Bx[c] = 0.0;
+                if (pml_beyond(&q, xg, 0) || pml_beyond(&q, yg - 0.5, 1) || pml_beyond(&q, zg, 2)) f->By[c] = 0.0;
+                if (pml_beyond(&q, xg, 0) || pml_beyond(&q, yg, 1) || pml_beyond(&q, zg - 0.5, 2)) f->Bz[c] = 0.0;
+            }
+}

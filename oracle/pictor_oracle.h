@@ -123,6 +123,21 @@ typedef struct {
 int64_t orc_inject(const orc_grid *g, orc_particles *p, const orc_inflow *f);
 /* RefPrtlFluidFrameRight (bc_inflow.F90:62-121) with DepositCurrentPIC. */
 void orc_refl_fluid_right(const orc_grid *g, orc_particles *p, orc_fields *f, double pos, double vx);
+/* Convolutional PML (bc_pml.F90): bit n-1 of `faces` marks bc_face(n) as
+   'pml' at pos[n-1] with attn_thickness thickness[n-1] (SetBC_Fld default 4),
+   with SetPMLParameters' profile (n = 4, kappa_max = 1, sigma_max = 1,
+   alpha_max = 9e-4); psiE / psiB are pml_E_psi1 x, y, z, pml_E_psi2 x, y, z
+   and the same for B, each a zeroed ghosted grid.  orc_pml_b is
+   UpdateMagFld_PML (:146-264), called after the second B half step;
+   orc_pml_e is UpdateElcFld_PML (:83-144), after the E update.  Neither
+   refreshes the halo: SendRecvFlds follows each in MAIN.F90:104-110. */
+typedef struct {
+    int32_t faces;
+    double pos[6], thickness[6];
+    double *psiE[6], *psiB[6];
+} orc_pml;
+void orc_pml_b(const orc_grid *g, orc_fields *f, orc_pml *p);
+void orc_pml_e(const orc_grid *g, orc_fields *f, orc_pml *p);
 
 /* mem_prtl.F90 ReorderPrtlArr: stable counting sort by cell key; holes dropped.
    If perm is non-NULL it receives, for each output slot, the input slot. */

@@ -36,6 +36,13 @@ struct pic_handle {
     void *E[3] = {}, *B[3] = {}, *J[3] = {};
     void *Jtmp = nullptr;
     double *open_col = nullptr;   // den, vel per (j, k) column of an 'open' particle face (2 my mz)
+    // convolutional PML: per-axis tables (6 doubles and a flag per index),
+    // twelve psi grids in the handle's precision (E psi1 x,y,z, psi2 x,y,z,
+    // then B), kept across pic_bc_pml calls as the reference keeps them
+    double *pml_coef = nullptr;
+    uint8_t *pml_flag = nullptr;
+    void *pml_psi = nullptr;
+    bool pml_on = false;
     // cylindrical modal form: the fields on modes m = 0, 1, (mx, 3, mz) each;
     // E and B above are kept equal to their theta-gridded synthesis
     bool modal = false;
@@ -1589,6 +1596,66 @@ int pic_bc_open_prtl_x(pic_handle *h, int32_t side, double pos)
                           sc.scan_tmp + sc.scan_tmp_len - 1, h->capacity, h->err, h->s);
     return finish_phase(h);
 }
+
+int pic_bc_pml(pic_handle *h, int32_t faces, const double *pos, const double *thickness)
+{
+    if (!h || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || h->modal || faces < 0 || faces > 63 ||
+        (h->g.dims == 2 && (faces & 0x30)) || (faces && (!pos || !thickness)))
+        return PIC_ERR_INVALID;
+    for (int f = 0; f < 6; f++)
+        if (((faces >> f) & 1) && !(thickness[f] > 0.0 && std::fabs(pos[f]) < 1e9)) return PIC_ERR_INVALID;
+    const GridP &g = h->g;
+    const size_t rows = (size_t)g.mx + g.my + g.mz;
+    std::vector<double> coef(6 * rows);
+    std::vector<uint8_t> flag(rows);
+    h->pml_on = faces != 0 && pml_tables(g, faces, pos, thickness, coef.data(), flag.data());
+    if (!h->pml_on) return PIC_OK;
+    if (!h->pml_psi) {   // InitPMLArr: zeroed on first use
+        const size_t bytes = 12 * (size_t)g.ncell * (h->fp32 ? sizeof(float) : sizeof(double));
+        int r = dalloc(h, &h->pml_coef, 6 * rows);
+        if (!r) r = dalloc(h, &h->pml_flag, rows);
+        if (!r) r = dalloc(h, reinterpret_cast<uint8_t **>(&h->pml_psi), bytes);
+        if (r) {
+            h->pml_on = false;
+            return r;
+        }
+        CK(cudaMemsetAsync(h->pml_psi, 0, bytes, h->s));
+    }
+    CK(cudaMemcpyAsync(h->pml_coef, coef.data(), coef.size() * sizeof(double), cudaMemcpyHostToDevice, h->s));
+    CK(cudaMemcpyAsync(h->pml_flag, flag.data(), flag.size(), cudaMemcpyHostToDevice, h->s));
+    return finish(h);   // the host tables go out of scope
+}
+
+static int pml_phase(pic_handle *h, int which)
+{
+    if (!h || h->g.geom != PIC_GEOM_CARTESIAN || h->g.x_external || h->modal) return PIC_ERR_INVALID;
+    if (!h->pml_on) return PIC_OK;
+    const GridP &g = h->g;
+    PmlP P;
+    int off = 0;
+    const int m[3] = {g.mx, g.my, g.mz};
+    for (int a = 0; a < 3; a++) {
+        P.coef[a] = h->pml_coef + 6 * (size_t)off;
+        P.flag[a] = h->pml_flag + off;
+        off += m[a];
+    }
+    P.fc = g.fc;
+    if (h->fp32) {
+        float *E[3], *B[3], *J[3], *psi[6];
+        field_ptrs(h, E, B, J);
+        for (int c = 0; c < 6; c++) psi[c] = (float *)h->pml_psi + (size_t)(which == 0 ? 6 + c : c) * g.ncell;
+        launch_pml<float>(g, P, which, E, B, psi, h->s);
+    } else {
+        double *E[3], *B[3], *J[3], *psi[6];
+        field_ptrs(h, E, B, J);
+        for (int c = 0; c < 6; c++) psi[c] = (double *)h->pml_psi + (size_t)(which == 0 ? 6 + c : c) * g.ncell;
+        launch_pml<double>(g, P, which, E, B, psi, h->s);
+    }
+    return finish_phase(h);
+}
+
+int pic_bc_pml_b(pic_handle *h) { return pml_phase(h, 0); }
+int pic_bc_pml_e(pic_handle *h) { return pml_phase(h, 1); }
 
 int pic_bc_inflow_reflect(pic_handle *h, double pos, double drift_x)
 {

@@ -216,6 +216,23 @@ void launch_bc_inflow_reflect(const GridP &g, PartF64 &p, const Counters *cnt, d
 void launch_bc_open_prtl_x(const GridP &g, PartF64 &p, Counters *cnt, int side, double pos, double *col,
                            uint32_t *flag, uint32_t *counts, uint32_t *scan_tmp, uint32_t *total, long long capacity,
                            int *err, cudaStream_t s);
+// pml.cu: the convolutional PML (bc_pml.F90).  Per axis and 1-based index a
+// (a = 1..m): coef[axis][6 (a-1) + 0..2] = a, b, c at position a - 3 (the E
+// update), [+3..5] at a - 3 + 0.5 (the B update); flag bits below.
+constexpr uint8_t kPmlInside = 1;       // a - 3 strictly between the axis's pml_pos_ind
+constexpr uint8_t kPmlBeyond = 2;       // a - 3 beyond the axis's layers (zeroed)
+constexpr uint8_t kPmlBeyondHalf = 4;   // a - 3 + 0.5 beyond them
+struct PmlP {
+    const double *coef[3];
+    const uint8_t *flag[3];
+    double fc;
+};
+// Host: the tables of (mx + my + mz) rows (6 doubles and one flag each, x
+// rows first); false when the whole grid lies inside (no_pml_this_domain).
+bool pml_tables(const GridP &g, int faces, const double *pos, const double *thickness, double *coef, uint8_t *flag);
+// which 0: UpdateMagFld_PML + halo(B); 1: UpdateElcFld_PML + halo(E)
+template <typename T>
+void launch_pml(const GridP &g, const PmlP &P, int which, T *const E[3], T *const B[3], T *const psi[6], cudaStream_t s);
 // slab.cu: x faces of a slab (fields and particles), see pic_slab_* in the C ABI
 template <typename T>
 void launch_slab_pack_fields(const GridP &g, int which, T *const F[3], double *to_left, double *to_right, cudaStream_t s);

@@ -194,6 +194,24 @@ module pictor_b200_capi
          type(c_ptr), value :: h
          real(c_double), value :: pos, drift_x
       end function
+      ! 'pml' faces (bc_pml.F90): faces = bit mask of bc_face(1:6), pos and
+      ! thickness hold bc_face(:)%pos_fld and %attn_thickness; then
+      ! pic_bc_pml_b where MAIN calls UpdateMagFld_PML and pic_bc_pml_e where
+      ! it calls UpdateElcFld_PML
+      integer(c_int) function pic_bc_pml(h, faces, pos, thickness) bind(C, name="pic_bc_pml")
+         import :: c_int, c_ptr, c_int32_t, c_double
+         type(c_ptr), value :: h
+         integer(c_int32_t), value :: faces
+         real(c_double), intent(in) :: pos(6), thickness(6)
+      end function
+      integer(c_int) function pic_bc_pml_b(h) bind(C, name="pic_bc_pml_b")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
+      integer(c_int) function pic_bc_pml_e(h) bind(C, name="pic_bc_pml_e")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: h
+      end function
    end interface
 
    ! Slab form (cfg%slab_x = 1): x faces exchanged by the host

@@ -270,6 +270,29 @@ class Simulation:
             sc[int(n) - 1] = float(s)
         check(self.L.pic_bc_attenuate(self.h, mask, pos, sc), "pic_bc_attenuate")
 
+    def SetBC_PML(self, faces: dict):
+        """The faces of type 'pml' (SetBC_Fld, bc.F90:45-50; bc_pml.F90):
+        ``faces`` maps bc_face index 1..6 to (pos_fld, attn_thickness), the
+        thickness 4 by default; an empty dict switches the PML off.  The
+        auxiliary grids are zeroed on the first call and kept by later ones."""
+        mask = 0
+        pos = (C.c_double * 6)()
+        th = (C.c_double * 6)(*([4.0] * 6))
+        for n, v in faces.items():
+            p, t = (v, 4.0) if isinstance(v, (int, float)) else v
+            mask |= 1 << (int(n) - 1)
+            pos[int(n) - 1] = float(p)
+            th[int(n) - 1] = float(t)
+        check(self.L.pic_bc_pml(self.h, mask, pos, th), "pic_bc_pml")
+
+    def UpdateMagFld_PML(self):
+        """UpdateMagFld_PML + SendRecvFlds(B), after the second B half step."""
+        check(self.L.pic_bc_pml_b(self.h), "pic_bc_pml_b")
+
+    def UpdateElcFld_PML(self):
+        """UpdateElcFld_PML + SendRecvFlds(E), after the E update."""
+        check(self.L.pic_bc_pml_e(self.h), "pic_bc_pml_e")
+
     def Attenuate_EM_Flow(self, face: int, pos: float, thickness: float = 1.0, scale: float = 4.0,
                           bflow=(0.0, 0.0, 0.0), drift=(0.0, 0.0, 0.0)):
         """Attenuate_EM_Flow (bc_attenuate.F90:16-131) of an 'iflw' face 1..4

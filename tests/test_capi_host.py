@@ -134,3 +134,7 @@ def test_slab_and_wall_entry_points_validate_without_gpu():
     assert L.pic_solve_gauss(None, 1e-12, 100, None, None, None) == -1
     assert L.pic_bc_inflow(None, None) == -1
     assert L.pic_bc_inflow_reflect(None, 20.0, -0.3) == -1
+    six = (C.c_double * 6)()
+    assert L.pic_bc_pml(None, 1, six, six) == -1
+    assert L.pic_bc_pml_b(None) == -1
+    assert L.pic_bc_pml_e(None) == -1
