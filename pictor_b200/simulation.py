@@ -169,8 +169,16 @@ class Simulation:
     def load_current(self, Jx: np.ndarray, Jy: np.ndarray, Jz: np.ndarray) -> None:
         check(self.L.pic_load_current(self.h, dptr(Jx), dptr(Jy), dptr(Jz)), "pic_load_current")
 
-    def fetch_fields(self, with_current: bool = True) -> Fields:
-        f = Fields.zeros(self.cfg.shape)
+    def fetch_fields(self, with_current: bool = True, out: Fields | None = None) -> Fields:
+        """The fields in the reference layout; into the arrays of ``out`` when
+        given (Fortran-ordered float64 of the grid's shape, e.g. views of
+        pinned buffers, which the device writes at the full link rate)."""
+        f = out if out is not None else Fields.zeros(self.cfg.shape)
+        names = ("Ex", "Ey", "Ez", "Bx", "By", "Bz") + (("Jx", "Jy", "Jz") if with_current else ())
+        for n in names:
+            a = getattr(f, n)
+            if a.shape != tuple(self.cfg.shape) or a.dtype != np.float64 or not a.flags["F_CONTIGUOUS"]:
+                raise ValueError(f"fetch_fields: {n} must be a Fortran-ordered float64 array of shape {self.cfg.shape}")
         J = (dptr(f.Jx), dptr(f.Jy), dptr(f.Jz)) if with_current else (None, None, None)
         check(self.L.pic_fetch_fields(self.h, dptr(f.Ex), dptr(f.Ey), dptr(f.Ez), dptr(f.Bx), dptr(f.By), dptr(f.Bz), *J),
               "pic_fetch_fields")

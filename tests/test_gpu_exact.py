@@ -117,3 +117,29 @@ def test_exact_current_is_reproducible():
             out.append(s.fetch_fields(with_current=False))
     for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
         assert np.array_equal(getattr(out[0], n), getattr(out[1], n)), n
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_fetch_fields_into_caller_arrays(precision):
+    """pic_fetch_fields into arrays the caller owns (here views of one
+    reused buffer, as a host with pinned output buffers passes them) equals
+    the fetch into fresh arrays; arrays of the wrong shape or order are
+    refused before anything is written."""
+    from pictor_b200 import Fields
+
+    g, cfg = grid_and_config(dims=3, nx=12, ny=10, nz=8, precision=precision)
+    f = random_fields(g, seed=77)
+    shape = tuple(cfg.shape)
+    n = int(np.prod(shape))
+    buf = np.full(9 * n, np.nan)
+    out = Fields(*(buf[c * n:(c + 1) * n].reshape(shape, order="F") for c in range(9)))
+    with _sim(cfg) as s:
+        s.load_fields(to_gpu_fields(f))
+        ref = s.fetch_fields()
+        got = s.fetch_fields(out=out)
+        assert got is out
+        bad = Fields(*(np.zeros(shape) for _ in range(9)))          # C order
+        with pytest.raises(ValueError):
+            s.fetch_fields(out=bad)
+    for k in ("Ex", "Ey", "Ez", "Bx", "By", "Bz", "Jx", "Jy", "Jz"):
+        assert np.array_equal(getattr(out, k), getattr(ref, k)), k
