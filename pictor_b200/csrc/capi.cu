@@ -344,7 +344,8 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 else launch_cyl_bhalf(g, E, B, h->s);
                 break;
             case PIC_PHASE_MOVE:  // cyl_movdep_strang.F90:14-378
-                launch_cyl_move_deposit(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s);
+                launch_cyl_move_deposit(g, h->p64[cur], h->cnt, E, B, J, h->err, h->s,
+                                        h->tiled64 && h->sorted ? &h->t64 : nullptr);
                 break;
             case PIC_PHASE_EXCHANGE:
                 launch_exchange_f64(g, h->p64[cur], h->cnt, h->sc, h->capacity, h->err, h->s);
@@ -361,7 +362,8 @@ int enqueue_phase(pic_handle *h, int cur, bool reorder, int phase)
                 break;
             case PIC_PHASE_REORDER:
                 if (reorder)
-                    launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s);
+                    launch_reorder_f64(g, h->p64[cur], h->p64[cur ^ 1], h->cnt, h->sc, h->capacity, h->err, h->s,
+                                       h->tiled64 ? &h->t64 : nullptr);
                 break;
         }
         return (int)g_launches;
@@ -1062,13 +1064,13 @@ int pic_create(const pic_config *cfg, pic_handle **out)
             (r = dalloc(h, &sc.scan_tmp, sc.scan_tmp_len))) {
         }
     }
-    // the tiles of the FP64 Cartesian mover (faster than the per-particle
-    // mover's global FP64 atomics on every grid measured: 0.15 against 0.26
-    // ms per move on the 256^2 grid of 2.1 M particles, 44 against 69 ms on
+    // the tiles of the FP64 movers (faster than the per-particle mover's
+    // global FP64 atomics on every grid measured: 0.15 against 0.26 ms per
+    // move on the 256^2 grid of 2.1 M particles, 44 against 69 ms on
     // 512 x 256 x 256); the exact-order current keeps the per-particle
     // mover, whose records it sorts anyway
-    if (!r && c.geom == PIC_GEOM_CARTESIAN && c.precision == PIC_PREC_FP64 && !c.exact_current &&
-        c.fp64_tiles >= 0) {
+    if (!r && (c.geom == PIC_GEOM_CARTESIAN || c.geom == PIC_GEOM_CYLINDRICAL) && c.precision == PIC_PREC_FP64 &&
+        !c.exact_current && c.fp64_tiles >= 0) {
         Tiles64 &T = h->t64;
         choose_tiles64(g, T);
         if (!(r = dalloc(h, &T.range, 2 * (size_t)T.H * (size_t)T.ntiles)) &&
@@ -1378,7 +1380,8 @@ int pic_move_deposit(pic_handle *h)
     } else if (h->g.geom == PIC_GEOM_CYLINDRICAL) {
         double *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);
-        launch_cyl_move_deposit(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s);
+        launch_cyl_move_deposit(h->g, h->p64[h->cur], h->cnt, E, B, J, h->err, h->s,
+                                h->tiled64 && h->sorted ? &h->t64 : nullptr);
     } else if (h->fp32) {
         float *E[3], *B[3], *J[3];
         field_ptrs(h, E, B, J);

@@ -16,6 +16,7 @@
 // momenta and positions equal the serial CPU build bit for bit.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "tile64.cuh"
 #include "particle_math.cuh"
 #include "tile.cuh"
 
@@ -395,169 +396,236 @@ __device__ void deposit_pic(const GridP &g, double *Jx, double *Jy, double *Jz, 
 
 constexpr int kMaxSubsteps = 100000;
 
-template <int DUMMY>
+// One particle of the cylindrical mover (cyl_movdep_strang.F90:14-378, the
+// near-axis sub-stepper :404-566).  interp(x, y, z, pE, pB) is
+// Interp_VecEM_GridPoints at a position; dep(i, j, k, o, far) adds the VecJ
+// entries o of the zigzag at start cell (i, j, k), far when the particle
+// crossed more than one cell along an axis.  Returns false when the particle
+// keeps its state (range or non-finite momenta); nc receives its new cell.
+template <class Interp, class Dep>
+__device__ __forceinline__ bool cyl_move_one(const GridP &g, const CylP &cp, const PartF64 &p, long long n,
+                                             int flv, double qn, double x0, double y0, double z0, double ui,
+                                             double vi, double wi, const double *__restrict__ Ex,
+                                             const double *__restrict__ Ey, const double *__restrict__ Ez,
+                                             const double *__restrict__ Bx, const double *__restrict__ By,
+                                             const double *__restrict__ Bz, double *Jx, double *Jy, double *Jz,
+                                             int *err, Interp &&interp, Dep &&dep, int *nc)
+{
+    const double c = g.c, sqc = g.sqc, cinv = g.cinv;
+    const double r_proc = cp.rmin - 3.0;  // xborders + rshift - xmin
+    if (flv < 0 || flv > PIC_MAX_FLVR || !(x0 >= 2.5 && x0 < (double)(g.mx - 1)) ||
+        !(y0 >= 2.0 && y0 < (double)(g.my - 1)) || !(z0 >= 2.0 && z0 < (double)(g.mz - 1))) {
+        raise_error(err, PIC_DEVERR_RANGE);
+        return false;
+    }
+    if (flv == 0) return false;  // a hole moves nowhere and deposits zero
+    double qthis = qn * g.qi;
+    const double qm = g.qm[flv] * 0.25;  // cyl_movdep_strang.F90:100
+    const int ip0 = (int)x0, jp0 = (int)y0, kp0 = (int)z0;
+    double pE[3], pB[3];
+    interp(x0, y0, z0, pE, pB);
+    for (int d = 0; d < 3; d++) {
+        pE[d] = pE[d] * qm;
+        pB[d] = pB[d] * qm;
+    }
+    double u0 = c * ui + pE[0], v0 = c * vi + pE[1], w0 = c * wi + pE[2];
+    half_boris_d(sqc, pE, pB, u0, v0, w0);
+    if (!finite3(u0, v0, w0)) {   // the particle keeps its state (see finite3)
+        raise_error(err, PIC_DEVERR_NAN);
+        return false;
+    }
+    double u1 = u0 * cinv, v1 = v0 * cinv;
+    const double gg = sqc / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
+    const double r0 = (x0 + r_proc) * 1.0;
+    const double xx1 = r0 + u1 * gg, yy1 = v1 * gg;
+    double r1 = sqrt(xx1 * xx1 + yy1 * yy1);
+    double xn = r1 * 1.0 - r_proc;
+    double yn = y0 + atan(yy1 / xx1) * cp.inv_dtheta;
+    double zn = z0 + (wi * gg) * 1.0;  // z moves with this step's initial w (:202)
+    r1 = 1.0 / r1;
+    u1 = (r0 * u0 + ((u0 * u1) * gg + v0 * yy1)) * r1;
+    v1 = (v0 * r0) * r1;
+    if (x0 >= 4.5 && (!(xn >= 2.0 && xn < (double)(g.mx - 1)) || !(yn >= 2.0 && yn < (double)(g.my - 1)) ||
+                      !(zn >= 2.0 && zn < (double)(g.mz - 1)))) {
+        raise_error(err, PIC_DEVERR_RANGE);  // the azimuthal step left the ghost frame
+        return false;
+    }
+    const int ip = (int)xn, jp = (int)yn, kp = (int)zn;
+    if (x0 >= 4.5) {
+        interp(xn, yn, zn, pE, pB);
+    } else {
+        pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.0;  // redone by the sub-stepper below
+    }
+    for (int d = 0; d < 3; d++) {
+        pE[d] = pE[d] * qm;
+        pB[d] = pB[d] * qm;
+    }
+    u0 = u1 + pE[0];
+    v0 = v1 + pE[1];
+    w0 = w0 + pE[2];
+    half_boris_d(sqc, pE, pB, u0, v0, w0);
+    double un = u0 * cinv, vn = v0 * cinv, wn = w0 * cinv;
+    if (x0 < 4.5) {
+        // SubStepMovDep (:404-438) from the step's initial state
+        qthis = 0.0;
+        xn = x0; yn = y0; zn = z0; un = ui; vn = vi; wn = wi;
+        double t = 0.0, dt = 1.0, sx0 = x0, sy0 = y0, sz0 = z0;
+        int tries = 0;
+        while (t < 1.0) {
+            if (++tries > kMaxSubsteps) {
+                raise_error(err, PIC_DEVERR_SUBSTEP);
+                break;
+            }
+            const double delt = (t + dt > 1.0) ? 1.0 - t : dt;
+            // MovePrtlAxis (:462-566)
+            interp3(g, Ex, Ey, Ez, Bx, By, Bz, sx0, sy0, sz0, pE, pB);
+            for (int d = 0; d < 3; d++) {
+                pE[d] = (pE[d] * qm) * delt;
+                pB[d] = (pB[d] * qm) * delt;
+            }
+            double a0 = c * un + pE[0], b0 = c * vn + pE[1], c0 = c * wn + pE[2];
+            half_boris_d(sqc, pE, pB, a0, b0, c0);
+            if (!finite3(a0, b0, c0)) {
+                raise_error(err, PIC_DEVERR_NAN);
+                return false;   // the particle keeps its state
+            }
+            double a1 = a0 * cinv, b1 = b0 * cinv;
+            const double c1 = c0 * cinv;
+            const double g2 = sqc / sqrt(((sqc + a0 * a0) + b0 * b0) + c0 * c0);
+            const double rr0 = (sx0 - 3.5) * 1.0;
+            const double X1 = rr0 + (a1 * g2) * delt;
+            const double Y1 = (b1 * g2) * delt;
+            const double R1 = sqrt(X1 * X1 + Y1 * Y1);
+            const double dy = X1 > 0 ? atan(Y1 / X1) * cp.inv_dtheta : 0.0;
+            if (fabs(dy) > 0.45) {
+                dt = dt * 0.5;
+                continue;
+            }
+            double nx;
+            if (X1 > 0) {
+                nx = R1 / 1.0 + 3.5;
+                a1 = (rr0 * a0 + ((a0 * a1) * g2 * delt + b0 * Y1)) / R1;
+                b1 = (b0 * rr0) / R1;
+            } else {
+                nx = X1 / 1.0 + 3.5;
+            }
+            const double ny = yn + dy;
+            const double nz = zn + ((c1 * g2) * delt) * 1.0;
+            interp3(g, Ex, Ey, Ez, Bx, By, Bz, nx, ny, nz, pE, pB);
+            for (int d = 0; d < 3; d++) {
+                pE[d] = (pE[d] * qm) * delt;
+                pB[d] = (pB[d] * qm) * delt;
+            }
+            a0 = a1 + pE[0];
+            b0 = b1 + pE[1];
+            c0 = c0 + pE[2];
+            half_boris_d(sqc, pE, pB, a0, b0, c0);
+            xn = nx; yn = ny; zn = nz;
+            un = a0 * cinv; vn = b0 * cinv; wn = c0 * cinv;
+            t = t + delt;
+            deposit_pic(g, Jx, Jy, Jz, sx0, sy0, sz0, xn, yn, zn, qn);
+            // PrtlAxisBC (:450-460)
+            if (xn < 3.5) {
+                xn = 3.5 + (3.5 - xn);
+                yn = yn + g.ny / 2.0;
+                un = -un;
+                vn = -vn;
+            }
+            if (yn > g.ymax) yn = yn - g.ylen;
+            if (yn < g.ymin) yn = yn + g.ylen;
+            dt = dt * 1.7;
+            sx0 = xn; sy0 = yn; sz0 = zn;
+        }
+    }
+    // zigzag deposit; both segments use the start cell (:341)
+    if (qthis != 0.0) {
+        const double xr = fmin((double)(min(ip0, ip) + 1), fmax((double)max(ip0, ip), 0.5 * (x0 + xn)));
+        const double yr = fmin((double)(min(jp0, jp) + 1), fmax((double)max(jp0, jp), 0.5 * (y0 + yn)));
+        const double zr = fmin((double)(min(kp0, kp) + 1), fmax((double)max(kp0, kp), 0.5 * (z0 + zn)));
+        double o[12], o2[12];
+        segment<double, 3>(qthis * (xr - x0), qthis * (yr - y0), qthis * (zr - z0), 0.5 * (x0 + xr) - ip0,
+                           0.5 * (y0 + yr) - jp0, 0.5 * (z0 + zr) - kp0, o);
+        segment<double, 3>(qthis * (xn - xr), qthis * (yn - yr), qthis * (zn - zr), 0.5 * (xn + xr) - ip,
+                           0.5 * (yn + yr) - jp, 0.5 * (zn + zr) - kp, o2);
+        for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
+        dep(ip0, jp0, kp0, o, abs(ip - ip0) > 1 || abs(jp - jp0) > 1 || abs(kp - kp0) > 1);
+    }
+    p.x[n] = xn;
+    p.y[n] = yn;
+    p.z[n] = zn;
+    p.u[n] = un;
+    p.v[n] = vn;
+    p.w[n] = wn;
+    nc[0] = (int)xn;
+    nc[1] = (int)yn;
+    nc[2] = (int)zn;
+    return true;
+}
+
+// The per-particle mover over slots first .. used - 1 (first: all of them
+// when null; after a reorder of the tiled form, the particles appended since).
 __global__ void __launch_bounds__(kThreads) k_cyl_move(GridP g, CylP cp, PartF64 p, const Counters *__restrict__ cnt,
+                                                       const long long *__restrict__ first,
                                                        const double *__restrict__ Ex, const double *__restrict__ Ey,
                                                        const double *__restrict__ Ez, const double *__restrict__ Bx,
                                                        const double *__restrict__ By, const double *__restrict__ Bz,
                                                        double *Jx, double *Jy, double *Jz, int *err)
 {
-    const long long used = cnt->used;
-    const double c = g.c, sqc = g.sqc, cinv = g.cinv;
-    const double r_proc = cp.rmin - 3.0;  // xborders + rshift - xmin
-    const double ylen = g.ylen;
-    for (long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used; n += (long long)gridDim.x * blockDim.x) {
-        const int flv = p.flv[n];
-        const double x0 = p.x[n], y0 = p.y[n], z0 = p.z[n];
-        if (flv < 0 || flv > PIC_MAX_FLVR || !(x0 >= 2.5 && x0 < (double)(g.mx - 1)) ||
-            !(y0 >= 2.0 && y0 < (double)(g.my - 1)) || !(z0 >= 2.0 && z0 < (double)(g.mz - 1))) {
-            raise_error(err, PIC_DEVERR_RANGE);
-            continue;
-        }
-        if (flv == 0) continue;  // a hole moves nowhere and deposits zero
-        double qthis = p.q[n] * g.qi;
-        const double ui = p.u[n], vi = p.v[n], wi = p.w[n];
-        const double qm = g.qm[flv] * 0.25;  // cyl_movdep_strang.F90:100
-        const int ip0 = (int)x0, jp0 = (int)y0, kp0 = (int)z0;
-        double pE[3], pB[3];
-        interp3(g, Ex, Ey, Ez, Bx, By, Bz, x0, y0, z0, pE, pB);
-        for (int d = 0; d < 3; d++) {
-            pE[d] = pE[d] * qm;
-            pB[d] = pB[d] * qm;
-        }
-        double u0 = c * ui + pE[0], v0 = c * vi + pE[1], w0 = c * wi + pE[2];
-        half_boris_d(sqc, pE, pB, u0, v0, w0);
-        if (!finite3(u0, v0, w0)) {   // the particle keeps its state (see finite3)
-            raise_error(err, PIC_DEVERR_NAN);
-            continue;
-        }
-        double u1 = u0 * cinv, v1 = v0 * cinv;
-        const double gg = sqc / sqrt(((sqc + u0 * u0) + v0 * v0) + w0 * w0);
-        const double r0 = (x0 + r_proc) * 1.0;
-        const double xx1 = r0 + u1 * gg, yy1 = v1 * gg;
-        double r1 = sqrt(xx1 * xx1 + yy1 * yy1);
-        double xn = r1 * 1.0 - r_proc;
-        double yn = y0 + atan(yy1 / xx1) * cp.inv_dtheta;
-        double zn = z0 + (wi * gg) * 1.0;  // z moves with this step's initial w (:202)
-        r1 = 1.0 / r1;
-        u1 = (r0 * u0 + ((u0 * u1) * gg + v0 * yy1)) * r1;
-        v1 = (v0 * r0) * r1;
-        if (x0 >= 4.5 && (!(xn >= 2.0 && xn < (double)(g.mx - 1)) || !(yn >= 2.0 && yn < (double)(g.my - 1)) ||
-                          !(zn >= 2.0 && zn < (double)(g.mz - 1)))) {
-            raise_error(err, PIC_DEVERR_RANGE);  // the azimuthal step left the ghost frame
-            continue;
-        }
-        const int ip = (int)xn, jp = (int)yn, kp = (int)zn;
-        if (x0 >= 4.5) {
-            interp3(g, Ex, Ey, Ez, Bx, By, Bz, xn, yn, zn, pE, pB);
-        } else {
-            pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.0;  // redone by the sub-stepper below
-        }
-        for (int d = 0; d < 3; d++) {
-            pE[d] = pE[d] * qm;
-            pB[d] = pB[d] * qm;
-        }
-        u0 = u1 + pE[0];
-        v0 = v1 + pE[1];
-        w0 = w0 + pE[2];
-        half_boris_d(sqc, pE, pB, u0, v0, w0);
-        double un = u0 * cinv, vn = v0 * cinv, wn = w0 * cinv;
-        if (x0 < 4.5) {
-            // SubStepMovDep (:404-438) from the step's initial state
-            qthis = 0.0;
-            xn = x0; yn = y0; zn = z0; un = ui; vn = vi; wn = wi;
-            double t = 0.0, dt = 1.0, sx0 = x0, sy0 = y0, sz0 = z0;
-            int tries = 0;
-            bool bad = false;
-            while (t < 1.0) {
-                if (++tries > kMaxSubsteps) {
-                    raise_error(err, PIC_DEVERR_SUBSTEP);
-                    break;
-                }
-                const double delt = (t + dt > 1.0) ? 1.0 - t : dt;
-                // MovePrtlAxis (:462-566)
-                interp3(g, Ex, Ey, Ez, Bx, By, Bz, sx0, sy0, sz0, pE, pB);
-                for (int d = 0; d < 3; d++) {
-                    pE[d] = (pE[d] * qm) * delt;
-                    pB[d] = (pB[d] * qm) * delt;
-                }
-                double a0 = c * un + pE[0], b0 = c * vn + pE[1], c0 = c * wn + pE[2];
-                half_boris_d(sqc, pE, pB, a0, b0, c0);
-                if (!finite3(a0, b0, c0)) {
-                    raise_error(err, PIC_DEVERR_NAN);
-                    bad = true;
-                    break;
-                }
-                double a1 = a0 * cinv, b1 = b0 * cinv;
-                const double c1 = c0 * cinv;
-                const double g2 = sqc / sqrt(((sqc + a0 * a0) + b0 * b0) + c0 * c0);
-                const double rr0 = (sx0 - 3.5) * 1.0;
-                const double X1 = rr0 + (a1 * g2) * delt;
-                const double Y1 = (b1 * g2) * delt;
-                const double R1 = sqrt(X1 * X1 + Y1 * Y1);
-                const double dy = X1 > 0 ? atan(Y1 / X1) * cp.inv_dtheta : 0.0;
-                if (fabs(dy) > 0.45) {
-                    dt = dt * 0.5;
-                    continue;
-                }
-                double nx;
-                if (X1 > 0) {
-                    nx = R1 / 1.0 + 3.5;
-                    a1 = (rr0 * a0 + ((a0 * a1) * g2 * delt + b0 * Y1)) / R1;
-                    b1 = (b0 * rr0) / R1;
-                } else {
-                    nx = X1 / 1.0 + 3.5;
-                }
-                const double ny = yn + dy;
-                const double nz = zn + ((c1 * g2) * delt) * 1.0;
-                interp3(g, Ex, Ey, Ez, Bx, By, Bz, nx, ny, nz, pE, pB);
-                for (int d = 0; d < 3; d++) {
-                    pE[d] = (pE[d] * qm) * delt;
-                    pB[d] = (pB[d] * qm) * delt;
-                }
-                a0 = a1 + pE[0];
-                b0 = b1 + pE[1];
-                c0 = c0 + pE[2];
-                half_boris_d(sqc, pE, pB, a0, b0, c0);
-                xn = nx; yn = ny; zn = nz;
-                un = a0 * cinv; vn = b0 * cinv; wn = c0 * cinv;
-                t = t + delt;
-                deposit_pic(g, Jx, Jy, Jz, sx0, sy0, sz0, xn, yn, zn, p.q[n]);
-                // PrtlAxisBC (:450-460)
-                if (xn < 3.5) {
-                    xn = 3.5 + (3.5 - xn);
-                    yn = yn + g.ny / 2.0;
-                    un = -un;
-                    vn = -vn;
-                }
-                if (yn > g.ymax) yn = yn - g.ylen;
-                if (yn < g.ymin) yn = yn + g.ylen;
-                dt = dt * 1.7;
-                sx0 = xn; sy0 = yn; sz0 = zn;
-            }
-            if (bad) continue;   // the particle keeps its state
-        }
-        // zigzag deposit; both segments use the start cell (:341)
-        const double xr = fmin((double)(min(ip0, ip) + 1), fmax((double)max(ip0, ip), 0.5 * (x0 + xn)));
-        const double yr = fmin((double)(min(jp0, jp) + 1), fmax((double)max(jp0, jp), 0.5 * (y0 + yn)));
-        const double zr = fmin((double)(min(kp0, kp) + 1), fmax((double)max(kp0, kp), 0.5 * (z0 + zn)));
-        if (qthis != 0.0) {
-            const long long cell = cidx(g, ip0, jp0, kp0);
-            double o[12], o2[12];
-            segment<double, 3>(qthis * (xr - x0), qthis * (yr - y0), qthis * (zr - z0), 0.5 * (x0 + xr) - ip0,
-                               0.5 * (y0 + yr) - jp0, 0.5 * (z0 + zr) - kp0, o);
-            segment<double, 3>(qthis * (xn - xr), qthis * (yn - yr), qthis * (zn - zr), 0.5 * (xn + xr) - ip,
-                               0.5 * (yn + yr) - jp, 0.5 * (zn + zr) - kp, o2);
-            for (int e = 0; e < 12; e++) o[e] = o[e] + o2[e];
-            scatter<double, 3>(g, Jx, Jy, Jz, cell, o);
-        }
-        p.x[n] = xn;
-        p.y[n] = yn;
-        p.z[n] = zn;
-        p.u[n] = un;
-        p.v[n] = vn;
-        p.w[n] = wn;
+    const long long used = cnt->used, n0 = first ? *first : 0;
+    auto interp = [&](double x, double y, double z, double pE[3], double pB[3]) {
+        interp3(g, Ex, Ey, Ez, Bx, By, Bz, x, y, z, pE, pB);
+    };
+    auto dep = [&](int i, int j, int k, const double *o, bool) { scatter<double, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o); };
+    for (long long n = n0 + (long long)blockIdx.x * blockDim.x + threadIdx.x; n < used;
+         n += (long long)gridDim.x * blockDim.x) {
+        int nc[3];
+        cyl_move_one(g, cp, p, n, p.flv[n], p.q[n], p.x[n], p.y[n], p.z[n], p.u[n], p.v[n], p.w[n], Ex, Ey, Ez, Bx,
+                     By, Bz, Jx, Jy, Jz, err, interp, dep, nc);
     }
+}
+
+// The tiled form after a reorder: tile64.cuh's boxes, widened by one cell so
+// that the gather at the moved position (the second half of the Strang
+// split) finds its nodes; a particle within one cell of its start deposits
+// into the fixed-point box (two segments of at most one cell per axis add at
+// most 2 q qi to a word), the rest (near-axis sub-steps, long azimuthal
+// steps, cells outside the box) through global memory.
+__global__ void __launch_bounds__(kT64Threads, 2) k_cyl_move_tiled(GridP g, CylP cp, PartF64 p, Tiles64 T,
+                                                                   const double *__restrict__ Ex,
+                                                                   const double *__restrict__ Ey,
+                                                                   const double *__restrict__ Ez,
+                                                                   const double *__restrict__ Bx,
+                                                                   const double *__restrict__ By,
+                                                                   const double *__restrict__ Bz, double *Jx,
+                                                                   double *Jy, double *Jz, int *err)
+{
+    extern __shared__ __align__(16) double smem64[];
+    move_tile64<3, 1>(g, p, T, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz, 2.0, smem64,
+                      [&](const P64 &s, uint32_t n, const Tile64Ctx &ctx, int *nc) {
+        auto interp = [&](double x, double y, double z, double pE[3], double pB[3]) {
+            const int i = (int)x, j = (int)y, k = (int)z;
+            int nb;
+            if (ctx.use_box && in_box<3>(ctx.bx, i, j, k, nb)) {
+                double wt[8];
+                weights<double, 3>(x - i, y - j, z - k, wt);
+                gather_box64<3>(ctx.bx, ctx.sN, nb, wt, pE, pB);
+            } else {
+                interp3(g, Ex, Ey, Ez, Bx, By, Bz, x, y, z, pE, pB);
+            }
+        };
+        auto dep = [&](int i, int j, int k, const double *o, bool far) {
+            int nb;
+            if (!far && ctx.use_box && in_box<3>(ctx.bx, i, j, k, nb))
+                deposit_box64<3>(ctx.bx, ctx.sJ, ctx.jcell<3>(i, j, k), o, ctx.S);
+            else
+                scatter<double, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o);
+        };
+        if (!cyl_move_one(g, cp, p, n, s.flv, s.q, s.x, s.y, s.z, s.u, s.v, s.w, Ex, Ey, Ez, Bx, By, Bz, Jx, Jy, Jz,
+                          err, interp, dep, nc))
+            return false;
+        // the particles that stay in the interior bound the next box
+        return nc[0] >= 3 && nc[0] <= g.mx - 3 && nc[1] >= 3 && nc[1] <= g.my - 3 && nc[2] >= 3 && nc[2] <= g.mz - 3;
+    });
 }
 
 // AxisCurrentBC (cyl_movdep_strang.F90:570-584), all j, k.
@@ -575,10 +643,22 @@ __global__ void k_cyl_axis_current(GridP g, T *Jx, T *Jy, T *Jz)
 }
 
 void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
-                             double *const B[3], double *const J[3], int *err, cudaStream_t s)
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s, const Tiles64 *T)
 {
     const CylP cp = cyl_params(g);
-    k_cyl_move<0><<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2], err);
+    if (T) {
+        static bool attr_set = false;
+        if (!attr_set) {
+            cudaFuncSetAttribute(k_cyl_move_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize, kTile64SmemBytes);
+            attr_set = true;
+        }
+        k_cyl_move_tiled<<<T->ntiles, kT64Threads, T->smem_bytes, s>>>(g, cp, p, *T, E[0], E[1], E[2], B[0], B[1],
+                                                                        B[2], J[0], J[1], J[2], err);
+        count_launches(1);
+    }
+    // every particle, or the ones appended since the reorder
+    k_cyl_move<<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, T ? T->np : nullptr, E[0], E[1], E[2], B[0], B[1], B[2],
+                                             J[0], J[1], J[2], err);
     k_cyl_axis_current<double><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
     count_launches(2);
 }

@@ -46,8 +46,10 @@ template <typename T>
 void launch_modal_synth(const GridP &g, T *const Fm[3], T *const F[3], cudaStream_t s);
 template <typename T>
 void launch_modal_project(const GridP &g, T *const F[3], T *const Fm[3], cudaStream_t s);
+struct Tiles64;
 void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *cnt, double *const E[3],
-                             double *const B[3], double *const J[3], int *err, cudaStream_t s);
+                             double *const B[3], double *const J[3], int *err, cudaStream_t s,
+                             const Tiles64 *T = nullptr);
 void launch_cyl_move_deposit_f32(const GridP &g, const PartF32 &p, const Counters *cnt, float *const E[3],
                                  float *const B[3], float *const J[3], int *err, cudaStream_t s);
 
