@@ -95,9 +95,9 @@ typedef struct {
        sort of two records per particle each step.  0 = FP64 atomics into J
        (the sums differ from the serial build's in the last bits). */
     int32_t exact_current;
-    /* FP64 Cartesian form after a reorder: 0 or 1 = the mover by tiles of
-       cells (node and current boxes in shared memory); -1 = one thread per
-       particle with global atomics.  Positions and momenta are the same
+    /* FP64 form (Cartesian or cylindrical) after a reorder: 0 or 1 = the
+       mover by tiles of cells (node and current boxes in shared memory); -1
+       = one thread per particle with global atomics.  Positions and momenta are the same
        either way; the current differs in the order of its sums. */
     int32_t fp64_tiles;
     /* FP32 Cartesian form, 3D: 1 = each zigzag segment's current is its
