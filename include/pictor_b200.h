@@ -84,8 +84,12 @@ typedef struct {
        MPI decomposition with the x neighbours on other ranks): the kernels
        leave the x ghost layers to the pic_slab_* exchanges and particles
        leaving through the x faces to pic_slab_pack_particles; y and z stay
-       periodic on the slab.  Cartesian (FP64 or FP32), no current filter.
-       0 = one periodic domain. */
+       periodic on the slab.  Cartesian (FP64 or FP32) or cylindrical (FP64,
+       theta-gridded: a slab of radii; inc_axis on the slab holding the axis,
+       whose low face then has no neighbour, rmin >= 2.5 on the others), no
+       current filter.  2 = the same for the cylindrical slab whose high face
+       is the outer radius (no neighbour: leavers are dropped, its ghosts are
+       neither packed nor unpacked).  0 = one domain. */
     int32_t slab_x;
     /* FP64 Cartesian form: 1 = sum the current in the reference's serial
        order (each cell's VecJ entries in particle order, then the cells onto

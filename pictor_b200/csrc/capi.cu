@@ -927,16 +927,25 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     const pic_config &c = *cfg;
     if (c.dims != 2 && c.dims != 3) return PIC_ERR_INVALID;
     if (c.geom != PIC_GEOM_CARTESIAN && c.geom != PIC_GEOM_CYLINDRICAL) return PIC_ERR_INVALID;
-    // the cylindrical step: 3D, with the axis on this rank, no current filter;
-    // the reference's FP64 form or the FP32 cell-relative one, each with the
-    // theta-gridded or the modal (m = 0, 1) field solve
-    if (c.geom == PIC_GEOM_CYLINDRICAL && (c.dims != 3 || !c.inc_axis || c.curr_filter != 0 || (c.ny % 2) != 0))
+    // the cylindrical step: 3D, no current filter; the reference's FP64 form
+    // or the FP32 cell-relative one, each with the theta-gridded or the modal
+    // (m = 0, 1) field solve.  The rank holding the axis has it at x = 3.5
+    // (rmin = rshift = -0.5, cyl_common.F90:23); a slab away from the axis
+    // starts at least 2.5 cells out, so that every radius its stencils use,
+    // ghosts included, is positive.
+    if (c.geom == PIC_GEOM_CYLINDRICAL &&
+        (c.dims != 3 || c.curr_filter != 0 || (c.ny % 2) != 0 || (c.inc_axis != 0 && c.inc_axis != 1) ||
+         (c.inc_axis ? c.rmin != -0.5 : (c.slab_x == 0 || !(c.rmin >= 2.5)))))
         return PIC_ERR_INVALID;
     if (c.cyl_modes != 0 && (c.geom != PIC_GEOM_CYLINDRICAL || c.cyl_modes != 2 || c.ny < 4)) return PIC_ERR_INVALID;
-    // the slab form: the Cartesian step (FP64 or FP32) with its x faces on
-    // neighbouring ranks (no current filter: its passes would need a halo
-    // exchange per pass)
-    if (c.slab_x != 0 && (c.slab_x != 1 || c.geom != PIC_GEOM_CARTESIAN || c.curr_filter != 0)) return PIC_ERR_INVALID;
+    // the slab form: the Cartesian step (FP64 or FP32) or the FP64
+    // theta-gridded cylindrical one with its x faces on neighbouring ranks
+    // (no current filter: its passes would need a halo exchange per pass);
+    // 2 = the high x face is the outer radius of a cylinder
+    if (c.slab_x < 0 || c.slab_x > 2 || (c.slab_x != 0 && c.curr_filter != 0) ||
+        (c.slab_x == 2 && c.geom != PIC_GEOM_CYLINDRICAL) ||
+        (c.slab_x != 0 && c.geom == PIC_GEOM_CYLINDRICAL && (c.precision != PIC_PREC_FP64 || c.cyl_modes != 0)))
+        return PIC_ERR_INVALID;
     // the exact-order current: FP64 Cartesian, two sorted records per slot
     if (c.exact_current != 0 && (c.exact_current != 1 || c.geom != PIC_GEOM_CARTESIAN ||
                                  c.precision != PIC_PREC_FP64 || c.capacity >= (1ll << 31)))
@@ -987,8 +996,14 @@ int pic_create(const pic_config *cfg, pic_handle **out)
     if (c.geom == PIC_GEOM_CYLINDRICAL) cyl_lehe_coefficients(c.c, c.ny, g.lehe);
     else lehe_coefficients(c.dims, c.c, g.lehe);
     g.geom = c.geom;
-    g.closed_x = c.geom == PIC_GEOM_CYLINDRICAL;
-    g.x_external = c.slab_x;
+    // a cylinder's x faces: the axis and the outer radius have no neighbour;
+    // a slab exchanges the others
+    g.closed_x = c.geom != PIC_GEOM_CYLINDRICAL ? 0
+                 : c.slab_x == 0                ? 3
+                                                : (c.inc_axis ? 1 : 0) | (c.slab_x == 2 ? 2 : 0);
+    g.inc_axis = c.geom == PIC_GEOM_CYLINDRICAL && c.inc_axis;
+    g.rmin = c.rmin;
+    g.x_external = c.slab_x != 0;
     g.exact_charge = c.exact_charge != 0;
     g.qm[0] = 0.0;
     for (int f = 1; f <= PIC_MAX_FLVR; f++) g.qm[f] = f <= c.nflvr ? c.qm[f] : 0.0;

@@ -30,7 +30,10 @@ struct GridP {
     // particle bounds (subdomains.F90:52-67)
     double xmin, xmax, ymin, ymax, zmin, zmax, xlen, ylen, zlen;
     int geom;                         // PIC_GEOM_*
-    int closed_x;                     // x faces not periodic (cylinder): leavers are dropped
+    int closed_x;                     // bit 0 / bit 1: the low / high x face has no neighbour (a cylinder's
+                                      // axis or outer radius): leavers through it are dropped
+    int inc_axis;                     // cylindrical: the axis is this grid's low x face
+    double rmin;                      // cylindrical: r of the first interior cell's inner edge (xborders + rshift)
     int x_external;                   // slab form: x faces exchanged with neighbouring slabs (no x images)
     int exact_charge;                 // FP32 3D: exactly charge-conserving segment currents (pic_config)
     unsigned int mx_magic, my_magic;  // n / m = umulhi(n, magic) >> shift, exact for n < 2^28 (div_magic)

@@ -79,11 +79,13 @@ __device__ __forceinline__ T lgz(const GridP &g, const T *F, long long c0)
 // earlier and come from L1 rather than L2.
 constexpr int kCylZChunk = 16;
 
+// i from 4 on the rank holding the axis (its cells 3 take the axis
+// updates), from 1 elsewhere (cyl_em_update.F90:49-51).
 template <typename T, int FDTD>
 __global__ void k_cyl_bhalf(GridP g, CylP cp, const T *__restrict__ Ex, const T *__restrict__ Ey,
                             const T *__restrict__ Ez, T *Bx, T *By, T *Bz)
 {
-    const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (g.inc_axis ? 4 : 1) + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
     if (i > g.mx - 1 || j > g.my - 1) return;
     const int k0 = (FDTD == PIC_FDTD_LEHE ? 2 : 1) + blockIdx.z * kCylZChunk;
@@ -156,13 +158,14 @@ __global__ void k_cyl_e_axis(GridP g, T *Ex, T *Ey, T *Ez)
 }
 
 // UpdateEfield (MODE 0, cyl_em_update.F90:24-41) or AddCurrent (MODE 2,
-// :128-137): i 4..mx-3, j, k 3..m-3.
+// :128-137): i 4..mx-3 on the rank holding the axis, 3..mx-3 elsewhere;
+// j, k 3..m-3.
 template <typename T, int MODE>
 __global__ void k_cyl_e(GridP g, CylP cp, T *Ex, T *Ey, T *Ez, const T *__restrict__ Bx, const T *__restrict__ By,
                         const T *__restrict__ Bz, const T *__restrict__ Jx, const T *__restrict__ Jy,
                         const T *__restrict__ Jz)
 {
-    const int i = 4 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = (g.inc_axis ? 4 : 3) + blockIdx.x * blockDim.x + threadIdx.x;
     const int j = 3 + blockIdx.y * blockDim.y + threadIdx.y;
     const int k = 3 + blockIdx.z;
     if (i > g.mx - 3 || j > g.my - 3) return;
@@ -239,7 +242,7 @@ static CylP cyl_params(const GridP &g)
     c.dtheta = 2.0 * pi / g.ny;
     c.ax_perm_area = 4.0 / g.ny;
     c.inv_dtheta = 1.0 / c.dtheta;
-    c.rmin = 0.0 + -0.5;  // xborders(0) + rshift
+    c.rmin = g.rmin;  // xborders(procxind) + rshift: -0.5 on the rank holding the axis
     return c;
 }
 
@@ -258,14 +261,18 @@ void launch_cyl_bhalf(const GridP &g, T *const E[3], T *const B[3], cudaStream_t
 {
     const CylP cp = cyl_params(g);
     const int nk = g.fdtd == PIC_FDTD_LEHE ? g.mz - 3 : g.mz - 1;
-    const dim3 grid((g.mx - 4 + 31) / 32, (g.my - 1 + 3) / 4, (nk + kCylZChunk - 1) / kCylZChunk), block(32, 4, 1);
+    const int ni = g.mx - (g.inc_axis ? 4 : 1);   // i .. mx-1
+    const dim3 grid((ni + 31) / 32, (g.my - 1 + 3) / 4, (nk + kCylZChunk - 1) / kCylZChunk), block(32, 4, 1);
     if (g.fdtd == PIC_FDTD_LEHE)
         k_cyl_bhalf<T, PIC_FDTD_LEHE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
     else
         k_cyl_bhalf<T, PIC_FDTD_YEE><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2]);
-    k_cyl_bz_axis<T><<<(g.mz + 127) / 128, 128, 0, s>>>(g, cp, E[1], B[2]);
-    k_cyl_b_axis<T><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, B[0], B[1], B[2]);
-    count_launches(3);
+    count_launches(1);
+    if (g.inc_axis) {   // cyl_em_update.F90:85-105
+        k_cyl_bz_axis<T><<<(g.mz + 127) / 128, 128, 0, s>>>(g, cp, E[1], B[2]);
+        k_cyl_b_axis<T><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, B[0], B[1], B[2]);
+        count_launches(2);
+    }
     halo<T>(g, B, s);
 }
 
@@ -273,11 +280,15 @@ template <typename T>
 void launch_cyl_efield(const GridP &g, int mode, T *const E[3], T *const B[3], T *const J[3], cudaStream_t s)
 {
     const CylP cp = cyl_params(g);
-    const dim3 grid((g.mx - 6 + 31) / 32, (g.my - 5 + 7) / 8, g.mz - 5), block(32, 8, 1);
+    const int ni = g.mx - 2 - (g.inc_axis ? 4 : 3);   // i .. mx-3
+    const dim3 grid((ni + 31) / 32, (g.my - 5 + 7) / 8, g.mz - 5), block(32, 8, 1);
     if (mode == 0) k_cyl_e<T, 0><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
     else k_cyl_e<T, 2><<<grid, block, 0, s>>>(g, cp, E[0], E[1], E[2], B[0], B[1], B[2], J[0], J[1], J[2]);
-    k_cyl_e_axis<T><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, E[0], E[1], E[2]);
-    count_launches(2);
+    count_launches(1);
+    if (g.inc_axis) {   // UpdateEFldAxis
+        k_cyl_e_axis<T><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, E[0], E[1], E[2]);
+        count_launches(1);
+    }
     halo<T>(g, E, s);
 }
 
@@ -421,6 +432,9 @@ __device__ __forceinline__ bool cyl_move_one(const GridP &g, const CylP &cp, con
     if (flv == 0) return false;  // a hole moves nowhere and deposits zero
     double qthis = qn * g.qi;
     const double qm = g.qm[flv] * 0.25;  // cyl_movdep_strang.F90:100
+    // MovDepAxis re-moves the particles within 1.5 cells of the axis on the
+    // rank holding it (:296, 390-402)
+    const bool near_axis = g.inc_axis && x0 < 4.5;
     const int ip0 = (int)x0, jp0 = (int)y0, kp0 = (int)z0;
     double pE[3], pB[3];
     interp(x0, y0, z0, pE, pB);
@@ -445,13 +459,13 @@ __device__ __forceinline__ bool cyl_move_one(const GridP &g, const CylP &cp, con
     r1 = 1.0 / r1;
     u1 = (r0 * u0 + ((u0 * u1) * gg + v0 * yy1)) * r1;
     v1 = (v0 * r0) * r1;
-    if (x0 >= 4.5 && (!(xn >= 2.0 && xn < (double)(g.mx - 1)) || !(yn >= 2.0 && yn < (double)(g.my - 1)) ||
+    if (!near_axis && (!(xn >= 2.0 && xn < (double)(g.mx - 1)) || !(yn >= 2.0 && yn < (double)(g.my - 1)) ||
                       !(zn >= 2.0 && zn < (double)(g.mz - 1)))) {
         raise_error(err, PIC_DEVERR_RANGE);  // the azimuthal step left the ghost frame
         return false;
     }
     const int ip = (int)xn, jp = (int)yn, kp = (int)zn;
-    if (x0 >= 4.5) {
+    if (!near_axis) {
         interp(xn, yn, zn, pE, pB);
     } else {
         pE[0] = pE[1] = pE[2] = pB[0] = pB[1] = pB[2] = 0.0;  // redone by the sub-stepper below
@@ -465,7 +479,7 @@ __device__ __forceinline__ bool cyl_move_one(const GridP &g, const CylP &cp, con
     w0 = w0 + pE[2];
     half_boris_d(sqc, pE, pB, u0, v0, w0);
     double un = u0 * cinv, vn = v0 * cinv, wn = w0 * cinv;
-    if (x0 < 4.5) {
+    if (near_axis) {
         // SubStepMovDep (:404-438) from the step's initial state
         qthis = 0.0;
         xn = x0; yn = y0; zn = z0; un = ui; vn = vi; wn = wi;
@@ -659,8 +673,11 @@ void launch_cyl_move_deposit(const GridP &g, const PartF64 &p, const Counters *c
     // every particle, or the ones appended since the reorder
     k_cyl_move<<<kSMs * 8, kThreads, 0, s>>>(g, cp, p, cnt, T ? T->np : nullptr, E[0], E[1], E[2], B[0], B[1], B[2],
                                              J[0], J[1], J[2], err);
-    k_cyl_axis_current<double><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
-    count_launches(2);
+    count_launches(1);
+    if (g.inc_axis) {   // AxisCurrentBC on the rank holding the axis
+        k_cyl_axis_current<double><<<dim3((g.my + 127) / 128, g.mz), 128, 0, s>>>(g, J[0], J[1], J[2]);
+        count_launches(1);
+    }
 }
 
 // ---------------------------------------------------------------------------

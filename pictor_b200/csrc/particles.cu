@@ -350,7 +350,7 @@ __device__ __forceinline__ int outlier_face(const GridP &g, double x, double y, 
 // neighbour is MPI_PROC_NULL (the r faces of a cylinder) append nothing.
 __device__ __forceinline__ int append_slot(const GridP &g, int face)
 {
-    if (face == 0 || (g.closed_x && face <= 2)) return -1;
+    if (face == 0 || (face <= 2 && ((g.closed_x >> (face - 1)) & 1))) return -1;
     return (face - 1) ^ 1;
 }
 

@@ -259,11 +259,12 @@ template <typename T>
 void launch_slab_pack_fields(const GridP &g, int which, T *const F[3], double *to_left, double *to_right, cudaStream_t s)
 {
     for (int side = 0; side < 2; side++) {
+        if ((g.closed_x >> side) & 1) continue;   // no neighbour on that face: nothing leaves
         const FaceLayers fl = send_layers(g.mx, which, side);
         k_slab_pack<T><<<face_grid(g, fl.n), kThreads, 0, s>>>(g, which, F[0], F[1], F[2],
                                                                 side == 0 ? to_left : to_right, fl);
+        count_launches(1);
     }
-    count_launches(2);
 }
 
 template <typename T>
@@ -271,11 +272,12 @@ void launch_slab_unpack_fields(const GridP &g, int which, T *const F[3], const d
                                const double *from_right, cudaStream_t s)
 {
     for (int side = 0; side < 2; side++) {
+        if ((g.closed_x >> side) & 1) continue;   // no neighbour: the face's ghosts stay this grid's
         const FaceLayers fl = recv_layers(g.mx, which, side);
         k_slab_unpack<T><<<face_grid(g, fl.n), kThreads, 0, s>>>(g, which, F[0], F[1], F[2],
                                                                   side == 0 ? from_left : from_right, fl);
+        count_launches(1);
     }
-    count_launches(2);
 }
 template void launch_slab_pack_fields<double>(const GridP &, int, double *const[3], double *, double *, cudaStream_t);
 template void launch_slab_pack_fields<float>(const GridP &, int, float *const[3], double *, double *, cudaStream_t);

@@ -16,6 +16,14 @@ A ``Transport`` moves the face buffers: ``DistTransport`` between ranks
 (torch.distributed point-to-point, NCCL between GPUs over NVLink, gloo on
 CPU), ``LocalTransport`` between slabs that share a process (device
 copies).  The left neighbour of slab 0 is slab S-1 (the periodic x axis).
+
+A cylindrical domain (FP64, theta-gridded) splits along r the same way: slab
+0 holds the axis (``inc_axis``), slab s starts at r = rmin + s w, and the
+last slab's high face is the outer radius (``slab_x = 2``).  Those two
+faces have no neighbour: the library drops what leaves through them and
+neither packs nor unpacks them, so the ring transports carry the chain
+unchanged (what slab 0 and slab S-1 exchange across the ring's seam is
+ignored on both sides).
 """
 from __future__ import annotations
 
@@ -207,7 +215,12 @@ class Slab:
         self.index, self.nslabs = index, nslabs
         self.w = slab_width(cfg.nx, nslabs)
         self.x0 = index * self.w
-        self.cfg = dataclasses.replace(cfg, nx=self.w, slab_x=1)
+        if cfg.geom == "cylindrical":
+            # r of the slab's first cell; the axis on slab 0, the outer radius on the last
+            self.cfg = dataclasses.replace(cfg, nx=self.w, slab_x=2 if index == nslabs - 1 else 1,
+                                           rmin=cfg.rmin + self.x0, inc_axis=cfg.inc_axis if index == 0 else 0)
+        else:
+            self.cfg = dataclasses.replace(cfg, nx=self.w, slab_x=1)
         self.sim = Simulation(self.cfg)
         self.device = device if device is not None else torch.device("cuda", torch.cuda.current_device())
         n = C.c_int64()

@@ -102,14 +102,24 @@ def test_cell_decode_division_is_exact():
 
 
 def test_slab_and_wall_entry_points_validate_without_gpu():
-    """The slab form is refused outside the Cartesian step without a current
-    filter (before any device use), and the slab, wall and sync
+    """The slab form is refused (before any device use) with a current
+    filter, for the FP32 or modal cylindrical step, with the outer-radius
+    form (slab_x = 2) outside a cylinder, and for a cylindrical slab whose
+    radii would not all be positive; a cylinder without the axis must be a
+    slab, one with it must have it at x = 3.5.  The slab, wall and sync
     entry points reject a null handle and bad arguments."""
     from pictor_b200 import PicConfig, PicError, Simulation, _capi
 
+    cyl = dict(nx=12, ny=8, nz=8, dims=3, geom="cylindrical")
     for bad in (PicConfig(nx=12, ny=8, slab_x=2),
+                PicConfig(nx=12, ny=8, slab_x=3),
                 PicConfig(nx=12, ny=8, slab_x=1, curr_filter=1),
-                PicConfig(nx=12, ny=8, nz=8, dims=3, slab_x=1, geom="cylindrical")):
+                PicConfig(**cyl, slab_x=1),                                    # rmin 0, no axis
+                PicConfig(**cyl, slab_x=1, rmin=2.0),                          # ghost radii <= 0
+                PicConfig(**cyl, slab_x=1, rmin=11.5, precision="fp32"),
+                PicConfig(**cyl, slab_x=1, rmin=-0.5, inc_axis=1, cyl_modes=2),
+                PicConfig(**cyl, rmin=11.5),                                   # no axis, one domain
+                PicConfig(**cyl, rmin=0.0, inc_axis=1)):
         with pytest.raises(PicError) as e:
             Simulation(bad)
         assert e.value.code == -1

@@ -160,3 +160,70 @@ def test_fp32_slabs_track_single_domain(dims, nslabs):
         else:
             ref, got = ref[:, 2:-3], got[:, 2:-3]
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5 * max(np.abs(ref).max(), 1e-30), err_msg=n)
+
+
+@pytest.mark.parametrize("nslabs", [2, 3])
+def test_cylindrical_slabs_track_single_domain(nslabs):
+    """The FP64 cylindrical step split along r: slab 0 holds the axis (the
+    near-axis sub-steps, the axis field and current conditions), the last
+    slab's high face is the outer radius, the faces between them are
+    exchanged; 6 steps with a reorder at step 3 (the tiled mover after it)
+    of r-weighted electrons and ions with a few particles crossing the axis
+    region equal the single domain's: the same live particles (positions and
+    momenta to 1e-11), E and B to 1e-11 of their scale."""
+    import torch
+
+    from oracle import oracle as O
+    from pictor_b200 import PicConfig, Simulation
+    from pictor_b200.slab import join_interior, join_particles, local_domain, split_fields, split_particles
+
+    nx, ny, nz = 24, 8, 10
+    cfg = PicConfig(nx=nx, ny=ny, nz=nz, dims=3, c=0.45, qi=0.01, qm=(1.0, -1.0), geom="cylindrical",
+                    capacity=1 << 15, reorder_period=3, rmin=-0.5, inc_axis=1)
+    g = O.make_grid(3, nx, ny, nz, c=0.45, qi=0.01, qm=(1.0, -1.0))
+    op = O.cyl_load_uniform(g, 1, 1, 1, 1.0, 2e-3, -1.0, 2, 5, 1 << 14)
+    rng = np.random.default_rng(5)
+    idx = rng.choice(op.used, 60, replace=False)
+    op.x[idx] = 3.5 + rng.uniform(0.05, 1.0, 60)          # near the axis, moving through it
+    op.u[idx] = rng.uniform(-0.6, 0.6, 60)
+    op.v[idx] = rng.uniform(-0.6, 0.6, 60)
+    out_idx = rng.choice(op.used, 200, replace=False)       # some fast radial movers near the slab faces
+    op.u[out_idx] = rng.uniform(-0.9, 0.9, 200)
+    op.flv[idx[:30]] = 1
+    op.q[idx[:30]] *= -1.0
+    p = to_gpu_particles(op)
+    f = to_gpu_fields(random_fields(g, seed=73, scale=0.02))
+    with Simulation(cfg) as s:
+        s.load_particles(p)
+        s.load_fields(f)
+        s.step(6)
+        assert s.device_errors() == 0
+        ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096)
+    try:
+        for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
+            sl.sim.load_particles(ps)
+            sl.sim.load_fields(fs)
+        dom.step(6)
+        for sl in dom.slabs:
+            assert sl.sim.device_errors() == 0
+        got_p = join_particles([sl.sim.fetch_particles() for sl in dom.slabs], nx)
+        got_f = [sl.sim.fetch_fields(with_current=False) for sl in dom.slabs]
+    finally:
+        dom.close()
+    lens = (0, ny, nz)          # r is not periodic
+    a, b = _sorted(got_p, lens), _sorted(ref_p, lens)
+    assert len(a["x"]) == len(b["x"])
+    np.testing.assert_array_equal(a["flv"], b["flv"])
+    np.testing.assert_array_equal(a["q"], b["q"])
+    for k, L in zip(("x", "y", "z"), lens):
+        d = a[k] - b[k]
+        if L:
+            d -= L * np.round(d / L)
+        assert np.abs(d).max() <= 1e-11, k
+    for k in ("u", "v", "w"):
+        np.testing.assert_allclose(a[k], b[k], rtol=0, atol=1e-11, err_msg=k)
+    for n in ("Ex", "Ey", "Ez", "Bx", "By", "Bz"):
+        ref = getattr(ref_f, n)[2:-3][:, 2:-3, 2:-3]
+        got = join_interior(got_f, n)[:, 2:-3, 2:-3]
+        np.testing.assert_allclose(got, ref, rtol=0, atol=1e-11 * max(np.abs(ref).max(), 1e-30), err_msg=n)
