@@ -428,7 +428,10 @@ def run_slab_bench(args, ws, rank, local, peak, peak_kind):
                     precision=prec, capacity=cap, reorder_period=20)
     dev = torch.device("cuda", local)
     transport = DistTransport() if ws > 1 else LocalTransport()
-    dom = SlabDomain([Slab(cfg, rank, ws, dev)], transport, queued=True)
+    # fixed-size particle boxes (the counts travel on the device, no host
+    # wait in a step) of half an x layer of the slab at the configured fill
+    box = cap // (wl["nx"] // ws) // 2 + 4096
+    dom = SlabDomain([Slab(cfg, rank, ws, dev, out_capacity=box)], transport, queued=True, fixed=True)
     sim = dom.slabs[0].sim
     n_p = sim.init_weibel(wl["epc"], 0.5, wl["drift"], wl["temp"], wl["temp"], SEED + rank)
     sim.reorder()
@@ -463,7 +466,8 @@ def run_slab_bench(args, ws, rank, local, peak, peak_kind):
                        "global_cells": [wl["nx"], wl["ny"]] + ([wl["nz"]] if dims == 3 else []), "slabs": ws,
                        "slab_cells_x": wl["nx"] // ws, "particles": int(n_tot), "parallelism": f"slab{ws}",
                        "exchange": ("NCCL point-to-point between ranks" if ws > 1 else "x faces copied on the rank")
-                       + ", ordered on the library's stream (one host wait per step, for the particle counts)",
+                       + ", ordered on the library's stream; particles in fixed-size boxes of "
+                       + f"{box} (their counts on the device): no host wait in a step",
                        "l2": ("particles and fields smaller than L2 at this size" if dims == 2 else
                               "inputs larger than L2 (particle state >> 126 MB)")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

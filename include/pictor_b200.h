@@ -309,6 +309,18 @@ int pic_slab_pack_fields(pic_handle *h, int32_t which, double *to_left, double *
 int pic_slab_unpack_fields(pic_handle *h, int32_t which, const double *from_left, const double *from_right);
 int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_right, int64_t *n_left);
 int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n);
+/* The same exchange with the counts on the device, so that a slab's step
+   never waits on the host: each direction's particles go in a box of
+   cap + 1 records of 8 doubles (record 0 holds the count in its first word,
+   the particles follow), and the boxes travel whole (a fixed size each
+   step).  pic_slab_pack_particles_fixed fills to_left and to_right (all
+   leavers or, when they exceed cap in total, none: the device error word
+   gets PIC_DEVERR_OVERFLOW and both counts are 0); the neighbours' boxes
+   go to pic_slab_unpack_particles_fixed, which appends from the left, then
+   from the right, and ignores the box of a face without neighbour.  Both
+   only enqueue their work under pic_set_sync(h, 0). */
+int pic_slab_pack_particles_fixed(pic_handle *h, double *to_left, double *to_right, int64_t cap);
+int pic_slab_unpack_particles_fixed(pic_handle *h, const double *from_left, const double *from_right, int64_t cap);
 
 /* nsteps full steps of MAIN.F90:42-284 (reorder every reorder_period steps,
    counted from the handle's step counter), captured once as a CUDA graph. */

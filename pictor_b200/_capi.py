@@ -127,6 +127,8 @@ SIGNATURES = {
     "pic_bc_inflow": (C.c_int, [H, C.POINTER(Inflow)]),
     "pic_bc_inflow_reflect": (C.c_int, [H, C.c_double, C.c_double]),
     "pic_bc_pml": (C.c_int, [H, C.c_int32, PD, PD]),
+    "pic_slab_pack_particles_fixed": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_int64]),
+    "pic_slab_unpack_particles_fixed": (C.c_int, [H, C.c_void_p, C.c_void_p, C.c_int64]),
     "pic_bc_pml_b": (C.c_int, [H]),
     "pic_bc_pml_e": (C.c_int, [H]),
     "pic_slab_pack_fields": (C.c_int, [H, C.c_int32, C.c_void_p, C.c_void_p]),

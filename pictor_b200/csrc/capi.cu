@@ -1844,6 +1844,22 @@ int pic_slab_pack_particles(pic_handle *h, double *out, int64_t cap, int64_t *n_
     return PIC_OK;
 }
 
+int pic_slab_pack_particles_fixed(pic_handle *h, double *to_left, double *to_right, int64_t cap)
+{
+    if (!h || !h->g.x_external || !to_left || !to_right || cap < 0) return PIC_ERR_INVALID;
+    launch_slab_pack_fixed(h->g, h->fp32, h->p64[h->cur], h->p32[h->cur], h->cnt, h->sc, to_left, to_right, cap,
+                           h->slab_sent, h->capacity, h->err, h->s);
+    return finish_phase(h);
+}
+
+int pic_slab_unpack_particles_fixed(pic_handle *h, const double *from_left, const double *from_right, int64_t cap)
+{
+    if (!h || !h->g.x_external || !from_left || !from_right || cap < 0) return PIC_ERR_INVALID;
+    launch_slab_append_fixed(h->g, h->fp32, h->p64[h->cur], h->p32[h->cur], h->cnt, from_left, from_right, cap,
+                             h->capacity, h->err, h->s);
+    return finish_phase(h);
+}
+
 int pic_slab_unpack_particles(pic_handle *h, const double *in, int64_t n)
 {
     if (!h || !h->g.x_external || n < 0 || (n > 0 && !in)) return PIC_ERR_INVALID;

@@ -247,6 +247,14 @@ void launch_slab_pack_f32(const GridP &g, PartF32 &p, const Counters *cnt, doubl
                           int *err, cudaStream_t s);
 void launch_slab_append_f32(const GridP &g, PartF32 &p, Counters *cnt, const double *in, long long n,
                             long long capacity, int *err, cudaStream_t s);
+// slab.cu: the x leavers through fixed-size boxes (cap + 1 records of 8
+// doubles, record 0 the count), with no count on the host
+void launch_slab_pack_fixed(const GridP &g, bool fp32, PartF64 &p64, PartF32 &p32, Counters *cnt, SortScratch &sc,
+                            double *to_left, double *to_right, long long cap, uint32_t *sent, long long capacity,
+                            int *err, cudaStream_t s);
+void launch_slab_append_fixed(const GridP &g, bool fp32, PartF64 &p64, PartF32 &p32, Counters *cnt,
+                              const double *from_left, const double *from_right, long long cap, long long capacity,
+                              int *err, cudaStream_t s);
 void launch_slab_append(const GridP &g, PartF64 &p, Counters *cnt, const double *in, long long n, long long capacity,
                         int *err, cudaStream_t s);
 // Stable cell-key reorder (ReorderPrtlArr).  The payload is gathered into

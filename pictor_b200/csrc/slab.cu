@@ -81,6 +81,20 @@ __global__ void k_slab_unpack(GridP g, int which, T *F0, T *F1, T *F2, const dou
     }
 }
 
+// One received particle (8 doubles: q, x, y, z, u, v, w, flv, already in
+// this slab's coordinates) into slot d of the reference layout.
+__device__ __forceinline__ void append_record_f64(const PartF64 &p, long long d, const double *o)
+{
+    p.q[d] = o[0];
+    p.x[d] = o[1];
+    p.y[d] = o[2];
+    p.z[d] = o[3];
+    p.u[d] = o[4];
+    p.v[d] = o[5];
+    p.w[d] = o[6];
+    p.flv[d] = (int)o[7];
+}
+
 // AppendParticles (comm_prtl.F90:11-30) of n received particles (8 doubles
 // each, already in this slab's coordinates) after the used slots.
 __global__ void k_slab_append(PartF64 p, Counters *cnt, const double *__restrict__ in, long long n, long long capacity,
@@ -91,18 +105,8 @@ __global__ void k_slab_append(PartF64 p, Counters *cnt, const double *__restrict
         if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
         return;
     }
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const double *o = in + 8 * t;
-        const long long d = used + t;
-        p.q[d] = o[0];
-        p.x[d] = o[1];
-        p.y[d] = o[2];
-        p.z[d] = o[3];
-        p.u[d] = o[4];
-        p.v[d] = o[5];
-        p.w[d] = o[6];
-        p.flv[d] = (int)o[7];
-    }
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        append_record_f64(p, used + t, in + 8 * t);
 }
 
 __global__ void k_slab_append_finish(Counters *cnt, long long n, long long capacity)
@@ -123,35 +127,54 @@ __device__ __forceinline__ int f32_side(const GridP &g, uint32_t key)
 {
     if ((key >> kFlvShift) == 0) return -1;
     const int cell = (int)(key & kCellMask);
-    const int ci = cell % g.mx + 1;
+    const int ci = cell - fast_div((unsigned)cell, g.mx_magic, g.mx_shift) * g.mx + 1;
     return ci >= g.mx - 2 ? 0 : (ci <= 2 ? 1 : -1);   // 0 right-bound, 1 left-bound
+}
+
+// Each thread takes kSlabPer consecutive slots of a tile (16-byte loads of
+// the keys, four at a time).
+constexpr int kSlabPer = kSlabTile / 256;
+
+__device__ __forceinline__ void load_tile_keys(const uint32_t *__restrict__ key, long long n0, long long used,
+                                               uint32_t k[kSlabPer])
+{
+    if (n0 + kSlabPer <= used) {
+#pragma unroll
+        for (int v = 0; v < kSlabPer / 4; v++) {
+            const uint4 q = *reinterpret_cast<const uint4 *>(key + n0 + 4 * v);
+            k[4 * v] = q.x; k[4 * v + 1] = q.y; k[4 * v + 2] = q.z; k[4 * v + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int e = 0; e < kSlabPer; e++) k[e] = n0 + e < used ? key[n0 + e] : 0u;
+    }
 }
 
 __global__ void __launch_bounds__(256) k_slab_count_f32(GridP g, PartF32 p, const Counters *__restrict__ cnt,
                                                         uint32_t *counts, int ntiles)
 {
-    __shared__ uint32_t c[2];
-    if (threadIdx.x < 2) c[threadIdx.x] = 0;
-    __syncthreads();
-    const long long used = cnt->used, base = (long long)blockIdx.x * kSlabTile;
+    __shared__ uint32_t c[2][8];
+    const long long used = cnt->used, n0 = (long long)blockIdx.x * kSlabTile + (long long)threadIdx.x * kSlabPer;
+    uint32_t k[kSlabPer];
+    load_tile_keys(p.key, n0, used, k);
     uint32_t r = 0, l = 0;
-    for (int q = threadIdx.x; q < kSlabTile; q += 256) {
-        const long long n = base + q;
-        if (n >= used) break;
-        const int sd = f32_side(g, p.key[n]);
+#pragma unroll
+    for (int e = 0; e < kSlabPer; e++) {
+        const int sd = f32_side(g, k[e]);
         r += sd == 0;
         l += sd == 1;
     }
     r = __reduce_add_sync(0xffffffffu, r);
     l = __reduce_add_sync(0xffffffffu, l);
     if ((threadIdx.x & 31) == 0) {
-        atomicAdd(&c[0], r);
-        atomicAdd(&c[1], l);
+        c[0][threadIdx.x >> 5] = r;
+        c[1][threadIdx.x >> 5] = l;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-        counts[blockIdx.x] = c[0];
-        counts[ntiles + blockIdx.x] = c[1];
+    if (threadIdx.x < 2) {
+        uint32_t t = 0;
+        for (int w = 0; w < 8; w++) t += c[threadIdx.x][w];
+        counts[(size_t)threadIdx.x * ntiles + blockIdx.x] = t;
     }
 }
 
@@ -165,50 +188,90 @@ __global__ void __launch_bounds__(256) k_slab_scatter_f32(GridP g, PartF32 p, co
         if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
         return;
     }
-    const long long used = cnt->used, base = (long long)blockIdx.x * kSlabTile;
+    const long long used = cnt->used, n0 = (long long)blockIdx.x * kSlabTile + (long long)threadIdx.x * kSlabPer;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t lt;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(lt));
-    uint32_t run[2] = {offs[blockIdx.x], offs[ntiles + blockIdx.x]};
-    const double len = g.xlen;
-    for (int r0 = 0; r0 < kSlabTile; r0 += 256) {
-        const long long n = base + r0 + threadIdx.x;
-        const int sd = n < used ? f32_side(g, p.key[n]) : -1;
-        const uint32_t b0 = __ballot_sync(0xffffffffu, sd == 0), b1 = __ballot_sync(0xffffffffu, sd == 1);
-        if (lane == 0) {
-            wsum[0][warp] = __popc(b0);
-            wsum[1][warp] = __popc(b1);
-        }
-        __syncthreads();
-        uint32_t before[2] = {0, 0}, chunk[2] = {0, 0};
-        for (int w = 0; w < 8; w++)
-            for (int k = 0; k < 2; k++) {
-                if (w < warp) before[k] += wsum[k][w];
-                chunk[k] += wsum[k][w];
-            }
-        if (sd >= 0) {
-            const uint32_t pos = run[sd] + before[sd] + __popc((sd == 0 ? b0 : b1) & lt);
-            const uint32_t key = p.key[n];
-            const int flv = (int)(key >> kFlvShift), cell = (int)(key & kCellMask);
-            const int ci = cell % g.mx + 1, jk = cell / g.mx, cj = jk % g.my + 1, ck = jk / g.my + 1;
-            // CopyTransferPrtl / InsertPrtls (subdomains.F90:720-740): a right
-            // leaver -len, a left one +len
-            const double x = (double)ci + (double)p.dx[n];
-            double *o = out + 8 * (size_t)pos;
-            o[0] = (double)p.w[n];
-            o[1] = sd == 0 ? (x - len) + 0.0 : (x - 0.0) + len;
-            o[2] = (double)cj + (double)p.dy[n];
-            o[3] = g.dims == 3 ? (double)ck + (double)p.dz[n] : 1.5;
-            o[4] = (double)p.ux[n];
-            o[5] = (double)p.uy[n];
-            o[6] = (double)p.uz[n];
-            o[7] = (double)flv;
-            p.key[n] = 0u;   // a hole
-        }
-        run[0] += chunk[0];
-        run[1] += chunk[1];
-        __syncthreads();
+    uint32_t k[kSlabPer];
+    load_tile_keys(p.key, n0, used, k);
+    int sd[kSlabPer];
+    uint32_t cr = 0, cl = 0;
+#pragma unroll
+    for (int e = 0; e < kSlabPer; e++) {
+        sd[e] = f32_side(g, k[e]);
+        cr += sd[e] == 0;
+        cl += sd[e] == 1;
     }
+    // the thread's first position per side: the tile's offset, the lower
+    // warps' and the lower lanes' leavers (slot order within each side)
+    uint32_t ir = cr, il = cl;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t vr = __shfl_up_sync(0xffffffffu, ir, o), vl = __shfl_up_sync(0xffffffffu, il, o);
+        if (lane >= o) {
+            ir += vr;
+            il += vl;
+        }
+    }
+    if (lane == 31) {
+        wsum[0][warp] = ir;
+        wsum[1][warp] = il;
+    }
+    __syncthreads();
+    if ((__ballot_sync(0xffffffffu, cr + cl != 0)) == 0) return;   // no leaver in the warp's slots
+    uint32_t pr = offs[blockIdx.x] + ir - cr, pl = offs[ntiles + blockIdx.x] + il - cl;
+    for (int w = 0; w < warp; w++) {
+        pr += wsum[0][w];
+        pl += wsum[1][w];
+    }
+    const double len = g.xlen;
+#pragma unroll
+    for (int e = 0; e < kSlabPer; e++) {
+        if (sd[e] < 0) continue;
+        const long long n = n0 + e;
+        const uint32_t key = k[e];
+        const int flv = (int)(key >> kFlvShift);
+        int ci, cj, ck;
+        decode_cell(g, (int)(key & kCellMask), ci, cj, ck);
+        // CopyTransferPrtl / InsertPrtls (subdomains.F90:720-740): a right
+        // leaver -len, a left one +len
+        const double x = (double)ci + (double)p.dx[n];
+        double *o = out + 8 * (size_t)(sd[e] == 0 ? pr++ : pl++);
+        o[0] = (double)p.w[n];
+        o[1] = sd[e] == 0 ? (x - len) + 0.0 : (x - 0.0) + len;
+        o[2] = (double)cj + (double)p.dy[n];
+        o[3] = g.dims == 3 ? (double)ck + (double)p.dz[n] : 1.5;
+        o[4] = (double)p.ux[n];
+        o[5] = (double)p.uy[n];
+        o[6] = (double)p.uz[n];
+        o[7] = (double)flv;
+        p.key[n] = 0u;   // a hole
+    }
+}
+
+// One received particle (8 doubles, the FP64 layout) into slot d of the FP32
+// form: its cell and offsets, FP32 momenta and weight; a particle outside
+// the slab's interior in x (or its ghost frame in y, z) leaves a hole.
+__device__ __forceinline__ void append_record_f32(const GridP &g, const PartF32 &p, long long d, const double *o,
+                                                  int *err)
+{
+    const int flv = (int)o[7];
+    const double x = o[1], y = o[2], z = o[3];
+    const double fx = floor(x), fy = floor(y), fz = g.dims == 3 ? floor(z) : 1.0;
+    uint32_t key = 0;
+    if (flv < 1 || flv > 15 || !(x >= 3.0 && x < (double)(g.mx - 2) && y >= 2.0 && y < (double)(g.my - 1) &&
+                                  (g.dims == 2 || (z >= 2.0 && z < (double)(g.mz - 1))))) {
+        raise_error(err, PIC_DEVERR_RANGE);   // left a hole
+    } else {
+        const int ci = (int)fx, cj = wrap_index((int)fy, g.my), ck = g.dims == 3 ? wrap_index((int)fz, g.mz) : 1;
+        key = ((uint32_t)flv << kFlvShift) | (uint32_t)cidx(g, ci, cj, ck);
+    }
+    p.key[d] = key;
+    p.dx[d] = (float)(x - fx);
+    p.dy[d] = (float)(y - fy);
+    if (g.dims == 3) p.dz[d] = (float)(z - fz);
+    p.ux[d] = (float)o[4];
+    p.uy[d] = (float)o[5];
+    p.uz[d] = (float)o[6];
+    p.w[d] = (float)o[0];
 }
 
 // The received particles (8 doubles each, in this slab's coordinates)
@@ -221,30 +284,69 @@ __global__ void k_slab_append_f32(GridP g, PartF32 p, Counters *cnt, const doubl
         if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
         return;
     }
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x)
+        append_record_f32(g, p, used + t, in + 8 * t, err);
+}
+
+// --- fixed-size boxes ------------------------------------------------------
+// A box of cap particles is cap + 1 records of 8 doubles: record 0 holds the
+// count (word 0), the particles follow.  Nothing about the exchange then
+// needs the host: the counts travel with the particles.
+struct Inbox2 {
+    const double *l, *r;   // from the left and from the right neighbour
+    long long cap;
+    int closed;            // GridP::closed_x: a face without neighbour receives nothing
+};
+__device__ __forceinline__ void inbox_counts(const Inbox2 &ib, long long &nl, long long &nr)
+{
+    nl = (ib.closed & 1) ? 0 : (long long)ib.l[0];
+    nr = (ib.closed & 2) ? 0 : (long long)ib.r[0];
+    nl = nl < 0 ? 0 : (nl > ib.cap ? ib.cap : nl);
+    nr = nr < 0 ? 0 : (nr > ib.cap ? ib.cap : nr);
+}
+
+// After the pack into to_right's payload (right-bound records, then the
+// left-bound ones): both headers, and the left-bound records moved to
+// to_left's payload.  A pack that overflowed moved nothing: both counts 0.
+__global__ void k_slab_split(const uint32_t *__restrict__ sent, double *to_left, double *to_right, long long cap)
+{
+    const long long all = (long long)sent[1];
+    const bool ok = all <= cap;
+    const long long nr = ok ? (long long)sent[0] : 0, nl = ok ? all - (long long)sent[0] : 0;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x, stride = (long long)gridDim.x * blockDim.x;
+    if (tid < 8) {
+        to_right[tid] = tid == 0 ? (double)nr : 0.0;
+        to_left[tid] = tid == 0 ? (double)nl : 0.0;
+    }
+    for (long long w = tid; w < 8 * nl; w += stride) to_left[8 + w] = to_right[8 + 8 * nr + w];
+}
+
+// AppendParticles of both inboxes: from the left, then from the right.
+template <bool F32>
+__global__ void k_slab_append_fixed(GridP g, PartF64 p64, PartF32 p32, Counters *cnt, Inbox2 ib, long long capacity,
+                                    int *err)
+{
+    long long nl, nr;
+    inbox_counts(ib, nl, nr);
+    const long long n = nl + nr, used = cnt->used;
+    if (used + n > capacity) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) raise_error(err, PIC_DEVERR_OVERFLOW);
+        return;
+    }
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const double *o = in + 8 * t;
-        const long long d = used + t;
-        const int flv = (int)o[7];
-        const double x = o[1], y = o[2], z = o[3];
-        const double fx = floor(x), fy = floor(y), fz = g.dims == 3 ? floor(z) : 1.0;
-        uint32_t key = 0;
-        if (flv < 1 || flv > 15 || !(x >= 3.0 && x < (double)(g.mx - 2) && y >= 2.0 && y < (double)(g.my - 1) &&
-                                      (g.dims == 2 || (z >= 2.0 && z < (double)(g.mz - 1))))) {
-            raise_error(err, PIC_DEVERR_RANGE);   // left a hole
-        } else {
-            const int ci = (int)fx, cj = wrap_index((int)fy, g.my), ck = g.dims == 3 ? wrap_index((int)fz, g.mz) : 1;
-            key = ((uint32_t)flv << kFlvShift) | (uint32_t)cidx(g, ci, cj, ck);
-        }
-        p.key[d] = key;
-        p.dx[d] = (float)(x - fx);
-        p.dy[d] = (float)(y - fy);
-        if (g.dims == 3) p.dz[d] = (float)(z - fz);
-        p.ux[d] = (float)o[4];
-        p.uy[d] = (float)o[5];
-        p.uz[d] = (float)o[6];
-        p.w[d] = (float)o[0];
+        const double *o = t < nl ? ib.l + 8 * (t + 1) : ib.r + 8 * (t - nl + 1);
+        if (F32) append_record_f32(g, p32, used + t, o, err);
+        else append_record_f64(p64, used + t, o);
     }
 }
+
+__global__ void k_slab_append_fixed_finish(Counters *cnt, Inbox2 ib, long long capacity)
+{
+    long long nl, nr;
+    inbox_counts(ib, nl, nr);
+    if (cnt->used + nl + nr <= capacity) cnt->used += nl + nr;
+}
+
 
 int face_grid(const GridP &g, int nl)
 {
@@ -311,6 +413,33 @@ void launch_slab_pack_f32(const GridP &g, PartF32 &p, const Counters *cnt, doubl
     count_launches(1);
     cudaMemcpyAsync(sent, counts + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
     cudaMemcpyAsync(sent + 1, total, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s);
+}
+
+// The x leavers into fixed-size boxes (record 0: the count; FP64 or FP32
+// form): the pack writes right- then left-bound records into to_right's
+// payload, the split moves the left-bound ones to to_left's.
+void launch_slab_pack_fixed(const GridP &g, bool fp32, PartF64 &p64, PartF32 &p32, Counters *cnt, SortScratch &sc,
+                            double *to_left, double *to_right, long long cap, uint32_t *sent, long long capacity,
+                            int *err, cudaStream_t s)
+{
+    if (fp32)
+        launch_slab_pack_f32(g, p32, cnt, to_right + 8, cap, sc.hist, sc.scan_tmp, sc.scan_tmp + sc.scan_tmp_len - 1,
+                             sent, capacity, err, s);
+    else
+        launch_exchange_f64(g, p64, cnt, sc, capacity, err, s, to_right + 8, cap, sent);
+    k_slab_split<<<kSMs, kThreads, 0, s>>>(sent, to_left, to_right, cap);
+    count_launches(1);
+}
+
+void launch_slab_append_fixed(const GridP &g, bool fp32, PartF64 &p64, PartF32 &p32, Counters *cnt,
+                              const double *from_left, const double *from_right, long long cap, long long capacity,
+                              int *err, cudaStream_t s)
+{
+    const Inbox2 ib{from_left, from_right, cap, g.closed_x};
+    if (fp32) k_slab_append_fixed<true><<<kSMs * 4, kThreads, 0, s>>>(g, p64, p32, cnt, ib, capacity, err);
+    else k_slab_append_fixed<false><<<kSMs * 4, kThreads, 0, s>>>(g, p64, p32, cnt, ib, capacity, err);
+    k_slab_append_fixed_finish<<<1, 1, 0, s>>>(cnt, ib, capacity);
+    count_launches(2);
 }
 
 void launch_slab_append_f32(const GridP &g, PartF32 &p, Counters *cnt, const double *in, long long n,

@@ -232,6 +232,17 @@ class Slab:
         # layer at the configured fill, with a factor 2 for the fluctuations
         self.out_capacity = int(out_capacity or 4 * (self.cfg.capacity // self.w) + 4096)
         self.out = torch.zeros(P_WORDS * self.out_capacity, dtype=torch.float64, device=self.device)
+        self._boxes = None
+
+    def boxes(self):
+        """The fixed-size particle boxes (to_left, to_right, from_left,
+        from_right): out_capacity particles and a count record each."""
+        import torch
+
+        if self._boxes is None:
+            n = P_WORDS * (self.out_capacity + 1)
+            self._boxes = tuple(torch.zeros(n, dtype=torch.float64, device=self.device) for _ in range(4))
+        return self._boxes
 
     def close(self):
         self.sim.close()
@@ -260,6 +271,16 @@ class Slab:
             check(self.sim.L.pic_slab_unpack_particles(self.sim.h, buf.data_ptr(), int(n)),
                   "pic_slab_unpack_particles")
 
+    def pack_particles_fixed(self):
+        tl, tr, _, _ = self.boxes()
+        check(self.sim.L.pic_slab_pack_particles_fixed(self.sim.h, tl.data_ptr(), tr.data_ptr(), self.out_capacity),
+              "pic_slab_pack_particles_fixed")
+
+    def unpack_particles_fixed(self):
+        _, _, fl, fr = self.boxes()
+        check(self.sim.L.pic_slab_unpack_particles_fixed(self.sim.h, fl.data_ptr(), fr.data_ptr(), self.out_capacity),
+              "pic_slab_unpack_particles_fixed")
+
 
 class SlabDomain:
     """The slabs of this process and the transport between them: MAIN.F90's
@@ -271,17 +292,22 @@ class SlabDomain:
     kernels, the unpack kernels after the transfers), so a step waits on the
     host only for the particle counts; several slabs in one process
     synchronise the device around each exchange instead of after every
-    call."""
+    call.
+
+    fixed=True: the particles cross in fixed-size boxes that carry their
+    counts (pic_slab_*_particles_fixed), so no count comes back to the host:
+    queued with one slab, a step enqueues all its work and never waits."""
 
     E, B, J = 0, 1, 2
 
-    def __init__(self, slabs: list[Slab], transport, queued: bool = False):
+    def __init__(self, slabs: list[Slab], transport, queued: bool = False, fixed: bool = False):
         import torch
 
         self.slabs = slabs
         self.transport = transport
         self.t = 0
         self.queued = queued
+        self.fixed = fixed
         self._stream = None
         if queued:
             for s in slabs:
@@ -320,6 +346,14 @@ class SlabDomain:
     def exchange_particles(self):
         import torch
 
+        if self.fixed:
+            for s in self.slabs:
+                s.pack_particles_fixed()
+            self._transfer(lambda: self.transport.exchange([s.boxes()[:2] for s in self.slabs],
+                                                           [s.boxes()[2:] for s in self.slabs]))
+            for s in self.slabs:
+                s.unpack_particles_fixed()
+            return
         packed = [s.pack_particles() for s in self.slabs]
         outs = [(tl, tr) for (tl, _), (tr, _) in packed]
         counts = [(nl, nr) for (_, nl), (_, nr) in packed]
@@ -361,13 +395,15 @@ class SlabDomain:
 
 
 def local_domain(cfg: PicConfig, nslabs: int, device=None, out_capacity: int | None = None,
-                 queued: bool = False) -> SlabDomain:
+                 queued: bool = False, fixed: bool = False) -> SlabDomain:
     """All slabs of a domain split along x in this process (one GPU)."""
-    return SlabDomain([Slab(cfg, s, nslabs, device, out_capacity) for s in range(nslabs)], LocalTransport(), queued)
+    return SlabDomain([Slab(cfg, s, nslabs, device, out_capacity) for s in range(nslabs)], LocalTransport(), queued,
+                      fixed)
 
 
-def distributed_slab(cfg: PicConfig, group=None, out_capacity: int | None = None, queued: bool = True) -> SlabDomain:
+def distributed_slab(cfg: PicConfig, group=None, out_capacity: int | None = None, queued: bool = True,
+                     fixed: bool = False) -> SlabDomain:
     """This rank's slab of a domain split along x over the ranks of the
     process group (one GPU per rank, the current CUDA device)."""
     t = DistTransport(group)
-    return SlabDomain([Slab(cfg, t.rank, t.world, None, out_capacity)], t, queued)
+    return SlabDomain([Slab(cfg, t.rank, t.world, None, out_capacity)], t, queued, fixed)

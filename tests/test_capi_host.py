@@ -131,6 +131,8 @@ def test_slab_and_wall_entry_points_validate_without_gpu():
     assert L.pic_slab_unpack_fields(None, 0, None, None) == -1
     assert L.pic_slab_pack_particles(None, None, 0, C.byref(a), C.byref(b)) == -1
     assert L.pic_slab_unpack_particles(None, None, 0) == -1
+    assert L.pic_slab_pack_particles_fixed(None, None, None, 0) == -1
+    assert L.pic_slab_unpack_particles_fixed(None, None, None, 0) == -1
     assert L.pic_set_sync(None, 0) == -1
     for fn in (L.pic_bc_reflect_x, L.pic_bc_conducting_x, L.pic_bc_reflect_y, L.pic_bc_conducting_y):
         assert fn(None, 0, 1.5) == -1

@@ -25,9 +25,11 @@ def _sorted(p, lens):
     return {k: v[o] for k, v in out.items()}
 
 
-@pytest.mark.parametrize("dims,fdtd,nslabs,queued", [(3, "yee", 2, False), (3, "lehe", 3, True), (2, "yee", 3, False),
-                                                      (2, "lehe", 2, True), (3, "yee", 1, True)])
-def test_slabs_track_single_domain(dims, fdtd, nslabs, queued):
+@pytest.mark.parametrize("dims,fdtd,nslabs,queued,fixed", [(3, "yee", 2, False, False), (3, "lehe", 3, True, False),
+                                                            (2, "yee", 3, False, False), (2, "lehe", 2, True, False),
+                                                            (3, "yee", 1, True, False), (3, "yee", 2, False, True),
+                                                            (2, "lehe", 3, True, True), (3, "yee", 1, True, True)])
+def test_slabs_track_single_domain(dims, fdtd, nslabs, queued, fixed):
     """6 steps (a reorder at step 3) of a 24-cell-wide domain as one
     periodic domain and as 1, 2 or 3 slabs (the library's phase calls
     waiting for their work, or queued with the exchanges ordered on the
@@ -49,7 +51,7 @@ def test_slabs_track_single_domain(dims, fdtd, nslabs, queued):
         s.step(6)
         assert s.device_errors() == 0
         ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
-    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096, queued=queued)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096, queued=queued, fixed=fixed)
     try:
         for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
             sl.sim.load_particles(ps)
@@ -103,8 +105,8 @@ def test_slab_refuses_the_periodic_entry_points():
             Simulation(cfg)
 
 
-@pytest.mark.parametrize("dims,nslabs", [(3, 2), (2, 3)])
-def test_fp32_slabs_track_single_domain(dims, nslabs):
+@pytest.mark.parametrize("dims,nslabs,fixed", [(3, 2, False), (2, 3, False), (3, 2, True)])
+def test_fp32_slabs_track_single_domain(dims, nslabs, fixed):
     """The FP32 cell-relative form split into slabs: its mover leaves an x
     leaver in the ghost cell beside the face, the pack sends it in the
     8-double layout (x in the receiver's coordinates) and leaves a hole, the
@@ -129,7 +131,7 @@ def test_fp32_slabs_track_single_domain(dims, nslabs):
         s.step(6)
         assert s.device_errors() == 0
         ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
-    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096, fixed=fixed)
     try:
         for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
             sl.sim.load_particles(ps)
@@ -162,8 +164,8 @@ def test_fp32_slabs_track_single_domain(dims, nslabs):
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-5 * max(np.abs(ref).max(), 1e-30), err_msg=n)
 
 
-@pytest.mark.parametrize("nslabs", [2, 3])
-def test_cylindrical_slabs_track_single_domain(nslabs):
+@pytest.mark.parametrize("nslabs,fixed", [(2, False), (3, False), (3, True)])
+def test_cylindrical_slabs_track_single_domain(nslabs, fixed):
     """The FP64 cylindrical step split along r: slab 0 holds the axis (the
     near-axis sub-steps, the axis field and current conditions), the last
     slab's high face is the outer radius, the faces between them are
@@ -199,7 +201,7 @@ def test_cylindrical_slabs_track_single_domain(nslabs):
         s.step(6)
         assert s.device_errors() == 0
         ref_p, ref_f = s.fetch_particles(), s.fetch_fields(with_current=False)
-    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096)
+    dom = local_domain(cfg, nslabs, device=torch.device("cuda", 0), out_capacity=4096, fixed=fixed)
     try:
         for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, nslabs), split_fields(f, nx, nslabs)):
             sl.sim.load_particles(ps)
@@ -227,3 +229,35 @@ def test_cylindrical_slabs_track_single_domain(nslabs):
         ref = getattr(ref_f, n)[2:-3][:, 2:-3, 2:-3]
         got = join_interior(got_f, n)[:, 2:-3, 2:-3]
         np.testing.assert_allclose(got, ref, rtol=0, atol=1e-11 * max(np.abs(ref).max(), 1e-30), err_msg=n)
+
+
+def test_fixed_boxes_overflow_moves_nothing():
+    """Fixed-size boxes too small for the particles leaving a slab: the pack
+    moves nothing (both counts 0, the leavers stay where the mover left
+    them) and returns PIC_ERR_OVERFLOW."""
+    import torch
+
+    from pictor_b200 import PicError
+    from pictor_b200.slab import local_domain, split_fields, split_particles
+
+    nx, ny, nz = 24, 8, 8
+    g, cfg = grid_and_config(dims=3, nx=nx, ny=ny, nz=nz, capacity=1 << 15)
+    p = to_gpu_particles(random_particles(g, n=6000, seed=74, umax=0.8))
+    f = to_gpu_fields(random_fields(g, seed=75, scale=0.05))
+    dom = local_domain(cfg, 2, device=torch.device("cuda", 0), out_capacity=2, fixed=True)
+    try:
+        for sl, ps, fs in zip(dom.slabs, split_particles(p, nx, 2), split_fields(f, nx, 2)):
+            sl.sim.load_particles(ps)
+            sl.sim.load_fields(fs)
+        sl = dom.slabs[0]
+        n0 = sl.sim.particle_count()
+        sl.sim.update_b_half()
+        sl.sim.move_deposit()
+        with pytest.raises(PicError) as e:
+            sl.pack_particles_fixed()
+        assert e.value.code == -3                           # PIC_ERR_OVERFLOW
+        tl, tr, _, _ = sl.boxes()
+        assert tl[0].item() == 0.0 and tr[0].item() == 0.0
+        assert sl.sim.particle_count() == n0
+    finally:
+        dom.close()
