@@ -62,19 +62,21 @@ __global__ void __launch_bounds__(kTileThreads, 3)
 }
 
 // The node averages of every interior node (node_avg, the same expressions
-// as the bricks' own staging), for the tiled mover's boxes.
+// as the bricks' own staging), for the tiled mover's boxes.  A (32, 8) block
+// covers 32 x 8 nodes of kNodeKz consecutive z planes (3D).
+constexpr int kNodeKz = 4;
 template <int DIMS>
 __global__ void __launch_bounds__(kThreads) k_node_avg(GridP g, const float *__restrict__ Ex, const float *__restrict__ Ey,
                                                        const float *__restrict__ Ez, const float *__restrict__ Bx,
                                                        const float *__restrict__ By, const float *__restrict__ Bz,
                                                        float4 *nodeA, float2 *nodeB)
 {
-    const long long nint = (long long)g.nx * g.ny * (DIMS == 3 ? g.nz : 1);
     const int sy = (int)g.sy, sz = (int)g.sz;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < nint; t += (long long)gridDim.x * blockDim.x) {
-        const int i = 3 + (int)(t % g.nx);
-        const long long r = t / g.nx;
-        const int j = 3 + (int)(r % g.ny), k = DIMS == 3 ? 3 + (int)(r / g.ny) : 1;
+    const int i = 3 + blockIdx.x * 32 + threadIdx.x, j = 3 + blockIdx.y * 8 + threadIdx.y;
+    if (i > g.nx + 2 || j > g.ny + 2) return;
+    for (int z = 0; z < (DIMS == 3 ? kNodeKz : 1); z++) {
+        const int k = DIMS == 3 ? 3 + blockIdx.z * kNodeKz + z : 1;
+        if (DIMS == 3 && k > g.nz + 2) break;
         const int nd = (int)cidx(g, i, j, k);
         float4 A;
         float2 Bv;
@@ -185,13 +187,13 @@ void launch_move_deposit_f32_tiled(const GridP &g, const PartF32 &p, const Brick
     }
     const bool pre = bk.nodeA != nullptr;
     if (pre) {
-        const long long nint = (long long)g.nx * g.ny * (g.dims == 3 ? g.nz : 1);
-        long long nb = (nint + kThreads - 1) / kThreads;
-        if (nb > (long long)kSMs * 16) nb = (long long)kSMs * 16;
+        const dim3 grid((unsigned)((g.nx + 31) / 32), (unsigned)((g.ny + 7) / 8),
+                        (unsigned)(g.dims == 3 ? (g.nz + kNodeKz - 1) / kNodeKz : 1)),
+            block(32, 8, 1);
         if (g.dims == 3)
-            k_node_avg<3><<<(unsigned)nb, kThreads, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], bk.nodeA, bk.nodeB);
+            k_node_avg<3><<<grid, block, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], bk.nodeA, bk.nodeB);
         else
-            k_node_avg<2><<<(unsigned)nb, kThreads, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], bk.nodeA, bk.nodeB);
+            k_node_avg<2><<<grid, block, 0, s>>>(g, E[0], E[1], E[2], B[0], B[1], B[2], bk.nodeA, bk.nodeB);
         count_launches(1);
     }
 #define PIC_MOVE_TILED(D, X, P)                                                                                      \
