@@ -1088,7 +1088,7 @@ int pic_create(const pic_config *cfg, pic_handle **out)
         !c.exact_current && c.fp64_tiles >= 0) {
         Tiles64 &T = h->t64;
         choose_tiles64(g, T);
-        if (!(r = dalloc(h, &T.range, 2 * (size_t)T.H * (size_t)T.ntiles)) &&
+        if (!(r = dalloc(h, &T.range, 2 * (size_t)T.H * (size_t)T.D * (size_t)T.ntiles)) &&
             !(r = dalloc(h, &T.box, 8 * (size_t)T.ntiles)) && !(r = dalloc(h, &T.np, 1)) &&
             !(r = dalloc(h, &T.qmax, 1)))
             h->tiled64 = true;

@@ -628,8 +628,7 @@ __global__ void __launch_bounds__(kT64Threads, 2) k_cyl_move_tiled(GridP g, CylP
             }
         };
         auto dep = [&](int i, int j, int k, const double *o, bool far) {
-            int nb;
-            if (!far && ctx.use_box && in_box<3>(ctx.bx, i, j, k, nb))
+            if (!far && ctx.use_box && ctx.in_jbox<3>(i, j, k))
                 deposit_box64<3>(ctx.bx, ctx.sJ, ctx.jcell<3>(i, j, k), o, ctx.S);
             else
                 scatter<double, 3>(g, Jx, Jy, Jz, cidx(g, i, j, k), o);

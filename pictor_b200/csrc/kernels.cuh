@@ -74,6 +74,9 @@ struct Tiles64 {
     unsigned long long *qmax;     // bits of max |q| over the live particles at the reorder (>= 0 doubles
                                   // order as their bit patterns): the bound of the fixed-point current box
     int W, H, nsx, ntiles;        // W cells per row segment, H rows per tile
+    int D;                        // z planes per tile (3D; H D row segments, at most kTile64MaxRows)
+    int jfirst;                   // rows of the first row group (H, or 2: the low ghost rows alone, so
+                                  // that the next groups start at the first interior row)
     int smem_bytes;
 };
 void choose_tiles64(const GridP &g, Tiles64 &T);

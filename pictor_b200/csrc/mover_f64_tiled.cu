@@ -42,24 +42,26 @@ __global__ void k_tile_starts(GridP g, Tiles64 T, const uint32_t *__restrict__ k
     const long long np = cnt->np;
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T.ntiles; t += gridDim.x * blockDim.x) {
         if (t == 0) *T.np = np;
-        int x0, x1, j0, nrow, k;
-        tile_cells(g, T, t, x0, x1, j0, nrow, k);
-        uint32_t *rg = T.range + 2 * (size_t)T.H * t;
-        for (int r = 0; r < T.H; r++) {
-            uint32_t b = 0, e = 0;
-            if (r < nrow) {
-                b = lower_bound_key(keys, np, (uint32_t)cidx(g, x0, j0 + r, k));
-                e = lower_bound_key(keys, np, (uint32_t)cidx(g, x1, j0 + r, k));
+        int x0, x1, j0, nrow, k0, nk;
+        tile_cells(g, T, t, x0, x1, j0, nrow, k0, nk);
+        uint32_t *rg = T.range + 2 * (size_t)T.H * T.D * t;
+        for (int q = 0; q < T.D; q++)
+            for (int r = 0; r < T.H; r++) {
+                uint32_t b = 0, e = 0;
+                if (r < nrow && q < nk) {
+                    b = lower_bound_key(keys, np, (uint32_t)cidx(g, x0, j0 + r, k0 + q));
+                    e = lower_bound_key(keys, np, (uint32_t)cidx(g, x1, j0 + r, k0 + q));
+                }
+                rg[2 * (q * T.H + r)] = b;
+                rg[2 * (q * T.H + r) + 1] = e;
             }
-            rg[2 * r] = b;
-            rg[2 * r + 1] = e;
-        }
         // the box of the first move: the tile's interior cells (a tile of
         // ghost cells only gets an empty box: its rare particles take the
         // global path)
         int *bx = T.box + 8 * (size_t)t;
-        bx[0] = max(x0, 3); bx[1] = max(j0, 3); bx[2] = g.dims == 3 ? max(k, 3) : 1;
-        bx[3] = min(x1 - 1, g.mx - 3); bx[4] = min(j0 + nrow - 1, g.my - 3); bx[5] = g.dims == 3 ? min(k, g.mz - 3) : 1;
+        bx[0] = max(x0, 3); bx[1] = max(j0, 3); bx[2] = g.dims == 3 ? max(k0, 3) : 1;
+        bx[3] = min(x1 - 1, g.mx - 3); bx[4] = min(j0 + nrow - 1, g.my - 3);
+        bx[5] = g.dims == 3 ? min(k0 + nk - 1, g.mz - 3) : 1;
     }
 }
 
@@ -161,9 +163,18 @@ void choose_tiles64(const GridP &g, Tiles64 &T)
     if (T.W > g.mx) T.W = g.mx;
     T.H = g.dims == 3 ? 4 : 2;
     if (T.H > g.my) T.H = g.my;
+    T.D = 1;
+    T.jfirst = T.H;
+    if (g.geom == PIC_GEOM_CYLINDRICAL) {
+        // a theta grid of a few cells: row groups aligned to the interior
+        // rows (the two low ghost rows alone) and two z planes per tile, so
+        // that a tile stages fewer nodes per particle
+        T.D = 2;
+        T.jfirst = 2;
+    }
     T.nsx = (g.mx + T.W - 1) / T.W;
-    const int nry = (g.my + T.H - 1) / T.H;
-    T.ntiles = T.nsx * nry * (g.dims == 3 ? g.mz : 1);
+    const int nry = tile_row_groups(g, T);
+    T.ntiles = T.nsx * nry * (g.dims == 3 ? (g.mz + T.D - 1) / T.D : 1);
     T.smem_bytes = kTile64SmemBytes;
 }
 

@@ -36,29 +36,41 @@ namespace pic {
 constexpr int kT64Threads = 256;   // 8 warps: the item order below covers 256 items
 
 // Tile t -> its row segments: cells x0 .. x1 - 1 (1-based) of rows j0 ..
-// j0 + nrow - 1 in plane k.  The tiles cover every cell of the ghosted
+// j0 + nrow - 1 in planes k0 .. k0 + nk - 1 (segment p H + r: row j0 + r of
+// plane k0 + p).  The tiles cover every cell of the ghosted
 // grid, not only the interior: the exchange sends a particle that left
 // through an edge or a corner through one face per step (the diagonal-face
 // rule of LoadPrtlOutliers), so a reorder can find it in a ghost cell, and
 // it must still belong to a tile (the range check of the move raises
 // PIC_ERR_RANGE for a cell outside the ghost frame, before any access).
+__host__ __device__ inline int tile_row_groups(const GridP &g, const Tiles64 &T)
+{
+    return 1 + (g.my - T.jfirst + T.H - 1) / T.H;
+}
 __device__ __forceinline__ void tile_cells(const GridP &g, const Tiles64 &T, int t, int &x0, int &x1, int &j0,
-                                           int &nrow, int &k)
+                                           int &nrow, int &k0, int &nk)
 {
     const int sx = t % T.nsx, r = t / T.nsx;
-    const int nry = (g.my + T.H - 1) / T.H;   // row groups per plane
+    const int nry = tile_row_groups(g, T);
     x0 = 1 + sx * T.W;
     x1 = min(x0 + T.W, g.mx + 1);
     const int ry = r % nry;
-    j0 = 1 + ry * T.H;
-    nrow = min(T.H, g.my + 1 - j0);
-    k = g.dims == 3 ? 1 + r / nry : 1;
+    j0 = ry == 0 ? 1 : 1 + T.jfirst + (ry - 1) * T.H;
+    nrow = max(0, min(ry == 0 ? T.jfirst : T.H, g.my + 1 - j0));
+    if (g.dims == 3) {
+        k0 = 1 + (r / nry) * T.D;
+        nk = min(T.D, g.mz + 1 - k0);
+    } else {
+        k0 = 1;
+        nk = 1;
+    }
 }
 
 struct Box64 {
-    int lo[3], C[3];      // box cells: lo .. lo + C - 1 per axis (z: 1 cell in 2D)
+    int lo[3], C[3];      // node box cells: lo .. lo + C - 1 per axis (z: 1 cell in 2D)
     int NX, NXY;          // node strides (C + 1 per axis)
-    int JX, JXY, nj;      // current strides (C + 3 per axis) and words per component
+    int jlo[3], jC[3];    // current box cells jlo .. jlo + jC - 1: the node box without its margin
+    int JX, JXY, nj;      // current strides (jC + 3 per axis) and words per component
 };
 
 template <int DIMS>
@@ -174,11 +186,18 @@ struct Tile64Ctx {
     unsigned long long *sJ;  // fixed-point current, 3 components of bx.nj words
     double S;                // fixed-point scale
     bool use_box;
-    // box current cell of cell (i, j, k) of the box
+    // box current cell of cell (i, j, k) of the current box
     template <int DIMS>
     __device__ __forceinline__ int jcell(int i, int j, int k) const
     {
-        return (i - bx.lo[0] + 1) + bx.JX * (j - bx.lo[1] + 1) + (DIMS == 3 ? bx.JXY * (k - bx.lo[2] + 1) : 0);
+        return (i - bx.jlo[0] + 1) + bx.JX * (j - bx.jlo[1] + 1) + (DIMS == 3 ? bx.JXY * (k - bx.jlo[2] + 1) : 0);
+    }
+    // cell (i, j, k) lies in the current box (its deposit's words then do)
+    template <int DIMS>
+    __device__ __forceinline__ bool in_jbox(int i, int j, int k) const
+    {
+        return (unsigned)(i - bx.jlo[0]) < (unsigned)bx.jC[0] && (unsigned)(j - bx.jlo[1]) < (unsigned)bx.jC[1] &&
+               (DIMS == 2 || (unsigned)(k - bx.jlo[2]) < (unsigned)bx.jC[2]);
     }
 };
 
@@ -187,7 +206,9 @@ struct Tile64Ctx {
 // nc when that cell bounds the next box.  MARGIN widens the staged box by
 // cells on each side (a body that gathers at the moved position too); bound
 // is the largest VecJ entry a particle of charge q adds to one word, over
-// q qi.  Shared memory: T.smem_bytes dynamic; smem64 the dynamic array.
+// q qi.  The current box covers the cells of the box without MARGIN (the
+// start cells; a deposit beyond them by one cell lands in its +-1 frame).
+// Shared memory: T.smem_bytes dynamic; smem64 the dynamic array.
 template <int DIMS, int MARGIN, class Body>
 __device__ __forceinline__ void move_tile64(const GridP &g, const PartF64 &p, const Tiles64 &T,
                                             const double *__restrict__ Ex, const double *__restrict__ Ey,
@@ -199,31 +220,36 @@ __device__ __forceinline__ void move_tile64(const GridP &g, const PartF64 &p, co
     __shared__ int s_red[kT64Threads / 32][6];
     __shared__ uint32_t s_rg[2 * kTile64MaxRows];
     const int t = blockIdx.x, tid = threadIdx.x;
-    if (tid < 2 * T.H) s_rg[tid] = T.range[2 * (size_t)T.H * t + tid];
+    const int nseg = T.H * T.D;
+    if (tid < 2 * nseg) s_rg[tid] = T.range[2 * (size_t)nseg * t + tid];
     __syncthreads();
-    // the tile's particles: item i -> slot, over the H ranges in order
+    // the tile's particles: item i -> slot, over the H D ranges in order
     uint32_t total = 0;
-    for (int r = 0; r < T.H; r++) total += s_rg[2 * r + 1] - s_rg[2 * r];
+    for (int r = 0; r < nseg; r++) total += s_rg[2 * r + 1] - s_rg[2 * r];
     if (total == 0) return;   // uniform across the CTA
     int *gbox = T.box + 8 * (size_t)t;
     Tile64Ctx ctx;
     Box64 &bx = ctx.bx;
     int lo[3] = {gbox[0] - MARGIN, gbox[1] - MARGIN, DIMS == 3 ? gbox[2] - MARGIN : 1};
     int hi[3] = {gbox[3] + MARGIN, gbox[4] + MARGIN, DIMS == 3 ? gbox[5] + MARGIN : 1};
+    int margin = MARGIN;
     auto set_box = [&]() {
         for (int d = 0; d < 3; d++) {
+            const int m = (DIMS == 2 && d == 2) ? 0 : margin;
             bx.lo[d] = lo[d];
             bx.C[d] = hi[d] - lo[d] + 1;
+            bx.jlo[d] = lo[d] + m;
+            bx.jC[d] = bx.C[d] - 2 * m;
         }
         bx.NX = bx.C[0] + 1;
         bx.NXY = bx.NX * (bx.C[1] + 1);
-        bx.JX = bx.C[0] + 3;
-        bx.JXY = bx.JX * (bx.C[1] + 3);
-        bx.nj = bx.JXY * (DIMS == 3 ? bx.C[2] + 3 : 1);
+        bx.JX = bx.jC[0] + 3;
+        bx.JXY = bx.JX * (bx.jC[1] + 3);
+        bx.nj = bx.JXY * (DIMS == 3 ? bx.jC[2] + 3 : 1);
         return bx.NXY * (DIMS == 3 ? bx.C[2] + 1 : 1);
     };
     auto fits = [&](int nn) {
-        return bx.C[0] >= 1 && bx.C[1] >= 1 && bx.C[2] >= 1 && lo[0] >= 2 && hi[0] <= g.mx - 2 && lo[1] >= 2 &&
+        return bx.jC[0] >= 1 && bx.jC[1] >= 1 && bx.jC[2] >= 1 && lo[0] >= 2 && hi[0] <= g.mx - 2 && lo[1] >= 2 &&
                hi[1] <= g.my - 2 && (DIMS == 2 || (lo[2] >= 2 && hi[2] <= g.mz - 2)) &&
                8ll * (6ll * nn + 3ll * bx.nj) <= (long long)T.smem_bytes;
     };
@@ -232,11 +258,12 @@ __device__ __forceinline__ void move_tile64(const GridP &g, const PartF64 &p, co
         // the particles spread further than shared memory holds: the tile's
         // own cells plus one on each side (clamped to the ghost frame), the
         // particles beyond it through global memory
-        int x0, x1, j0, nrow, k;
-        tile_cells(g, T, t, x0, x1, j0, nrow, k);
+        int x0, x1, j0, nrow, k0, nk;
+        tile_cells(g, T, t, x0, x1, j0, nrow, k0, nk);
         lo[0] = max(x0 - 1, 2); hi[0] = min(x1, g.mx - 2);
         lo[1] = max(j0 - 1, 2); hi[1] = min(j0 + nrow, g.my - 2);
-        if (DIMS == 3) { lo[2] = max(k - 1, 2); hi[2] = min(k + 1, g.mz - 2); }
+        if (DIMS == 3) { lo[2] = max(k0 - 1, 2); hi[2] = min(k0 + nk, g.mz - 2); }
+        margin = 0;   // the current box is the node box here
         nnode = set_box();
     }
     // the box fits (and lies where the kernel may read and write) or the
@@ -282,7 +309,7 @@ __device__ __forceinline__ void move_tile64(const GridP &g, const PartF64 &p, co
     __syncthreads();
     int blo[3] = {0x3fffffff, 0x3fffffff, 0x3fffffff}, bhi[3] = {-0x3fffffff, -0x3fffffff, -0x3fffffff};
     auto slot_of = [&](uint32_t i) {
-        for (int r = 0; r < T.H; r++) {
+        for (int r = 0; r < nseg; r++) {
             const uint32_t len = s_rg[2 * r + 1] - s_rg[2 * r];
             if (i < len) return s_rg[2 * r] + i;
             i -= len;
@@ -329,14 +356,14 @@ __device__ __forceinline__ void move_tile64(const GridP &g, const PartF64 &p, co
     __syncthreads();
     if (ctx.use_box) {
         // the box current onto J (one FP64 atomic per nonzero word)
-        const int JY = bx.C[1] + 3;
+        const int JY = bx.jC[1] + 3;
         const double inv = 1.0 / ctx.S;
         for (int q = tid; q < bx.nj; q += kT64Threads) {
             const long long ix = (long long)sJ[q], iy = (long long)sJ[bx.nj + q], iz = (long long)sJ[2 * bx.nj + q];
             if (ix == 0 && iy == 0 && iz == 0) continue;
             const double vx = (double)ix * inv, vy = (double)iy * inv, vz = (double)iz * inv;
             const int a = q % bx.JX, r = q / bx.JX, b = r % JY, cc = r / JY;
-            const long long off = cidx(g, bx.lo[0] - 1 + a, bx.lo[1] - 1 + b, DIMS == 3 ? bx.lo[2] - 1 + cc : 1);
+            const long long off = cidx(g, bx.jlo[0] - 1 + a, bx.jlo[1] - 1 + b, DIMS == 3 ? bx.jlo[2] - 1 + cc : 1);
             if (vx != 0.0) atomicAdd(Jx + off, vx);
             if (vy != 0.0) atomicAdd(Jy + off, vy);
             if (vz != 0.0) atomicAdd(Jz + off, vz);
